@@ -1,0 +1,262 @@
+"""What Enzo does around the hydro call, restated for tests and benchmarks.
+
+Enzo's hierarchy, boundary exchange and initialisers are outside the hot path;
+this module provides just enough of them to drive ``grid::SolvePPM_DE``-style
+calls: grid geometry with 3 ghost zones, the hydro parameter defaults of
+``SetDefaultGlobalValues.C``, ghost-zone fill (outflow = copy of the nearest
+active cell, periodic = wrap; ``ExternalBoundary_SetExternalBoundaryIO.C``
+:201-209, :378-386), and seeded synthetic initial conditions.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+
+import numpy as np
+
+NGHOST = 3
+FIELD_NAMES = ("d", "te", "v1", "v2", "v3", "ge")
+
+
+@dataclasses.dataclass
+class Grid:
+    """One Enzo grid: GridRank, GridDimension, GridStartIndex, GridEndIndex."""
+
+    rank: int
+    dims: tuple
+    start: tuple
+    end: tuple
+    cellwidth: tuple  # per-dim arrays of length dims[d] (CellWidth)
+
+    @staticmethod
+    def uniform(active, width=1.0, ghosts=NGHOST):
+        """active: tuple of active cells per dim (len = rank); domain width per dim."""
+        rank = len(active)
+        dims, start, end, cw = [], [], [], []
+        for d in range(3):
+            if d < rank:
+                n = int(active[d])
+                dims.append(n + 2 * ghosts)
+                start.append(ghosts)
+                end.append(ghosts + n - 1)
+                w = width[d] if isinstance(width, (tuple, list)) else width
+                cw.append(np.full(n + 2 * ghosts, w / n, dtype=np.float64))
+            else:
+                dims.append(1)
+                start.append(0)
+                end.append(0)
+                cw.append(np.ones(1, dtype=np.float64))
+        return Grid(rank, tuple(dims), tuple(start), tuple(end), tuple(cw))
+
+    @property
+    def shape(self):
+        """numpy shape (z, y, x) of one field, x fastest."""
+        return (self.dims[2], self.dims[1], self.dims[0])
+
+    @property
+    def size(self):
+        return self.dims[0] * self.dims[1] * self.dims[2]
+
+    @property
+    def active_cells(self):
+        n = 1
+        for d in range(self.rank):
+            n *= self.end[d] - self.start[d] + 1
+        return n
+
+    def centers(self, d, left=0.0):
+        """Cell-centre coordinates along dim d (ghosts included)."""
+        w = self.cellwidth[d]
+        edges = left + np.concatenate([[0.0], np.cumsum(w)]) - self.start[d] * w[0]
+        return 0.5 * (edges[:-1] + edges[1:])
+
+    def active_slices(self):
+        return tuple(
+            slice(self.start[d], self.end[d] + 1) for d in (2, 1, 0)
+        )
+
+
+@dataclasses.dataclass
+class HydroParams:
+    """Hydro globals consumed by the PPM-DE path (SetDefaultGlobalValues.C)."""
+
+    gamma: float = 5.0 / 3.0          # Gamma (:194)
+    cfl: float = 0.6                  # CourantSafetyNumber (:181)
+    dual: bool = False                # DualEnergyFormalism
+    eta1: float = 0.001               # DualEnergyFormalismEta1 (:425)
+    eta2: float = 0.1                 # DualEnergyFormalismEta2 (:426)
+    small_rho: float = 1e-30          # SmallRho (:803)
+    tiny_number: float = 1e-20        # tiny_number -> MinimumPressure
+    min_support: float = 0.0          # MinimumSupportEnergyCoefficient
+    gravity: bool = False             # GravityOn
+    pressure_free: bool = False       # PressureFree (:195)
+    fallback: bool = True             # RiemannSolverFallback (:809)
+
+
+def new_fields(grid, dual):
+    f = {n: np.zeros(grid.shape, dtype=np.float64) for n in FIELD_NAMES if n != "ge" or dual}
+    return f
+
+
+def _index_map(grid, d, bc):
+    n = grid.dims[d]
+    s, e = grid.start[d], grid.end[d]
+    idx = np.arange(n)
+    if n == 1:
+        return idx
+    if bc == "periodic":
+        return s + (idx - s) % (e - s + 1)
+    if bc == "outflow":
+        return np.clip(idx, s, e)
+    raise ValueError(bc)
+
+
+def fill_ghosts(grid, fields, bc="periodic"):
+    """Ghost-zone fill on host arrays (in place); bc per dim or one string."""
+    bcs = bc if isinstance(bc, (tuple, list)) else (bc,) * 3
+    ix = _index_map(grid, 0, bcs[0])
+    iy = _index_map(grid, 1, bcs[1])
+    iz = _index_map(grid, 2, bcs[2])
+    for k, a in fields.items():
+        if a is None:
+            continue
+        a[...] = a[np.ix_(iz, iy, ix)]
+
+
+# ---------------------------------------------------------------- initial conditions
+
+def shock_tube(grid, hp, x0, left, right, dim=0):
+    """Grid_HydroShockTubesInitializeGrid.C:72-116 (x <= x0 takes the left state).
+
+    left/right: (rho, v, p) with v along `dim`."""
+    f = new_fields(grid, hp.dual)
+    xc = grid.centers(dim)
+    shp = [1, 1, 1]
+    shp[2 - dim] = grid.dims[dim]
+    mask = (xc <= x0).reshape(shp)
+    vel = ("v1", "v2", "v3")[dim]
+    for (rho, v, p), m in ((left, mask), (right, ~mask)):
+        etot = p / ((hp.gamma - 1.0) * rho) + 0.5 * (v * v)
+        mb = np.broadcast_to(m, grid.shape)
+        f["d"][mb] = rho
+        f[vel][mb] = v
+        f["te"][mb] = etot
+        if hp.dual:
+            f["ge"][mb] = etot - 0.5 * (v * v)
+    return f
+
+
+def _grf(n, slope, rng):
+    """Unit-variance periodic Gaussian random field on n^3 with P(k) ~ k^slope."""
+    k = np.fft.fftfreq(n) * n
+    kx, ky, kz = np.meshgrid(k, k, k[: n // 2 + 1], indexing="ij")
+    kk = np.sqrt(kx * kx + ky * ky + kz * kz)
+    amp = np.zeros_like(kk)
+    nz = kk > 0
+    amp[nz] = kk[nz] ** (slope / 2.0)
+    noise = rng.standard_normal(kk.shape) + 1j * rng.standard_normal(kk.shape)
+    g = np.fft.irfftn(noise * amp, s=(n, n, n))
+    g -= g.mean()
+    g /= g.std()
+    return g
+
+
+def _solenoidal(n, slope, rng):
+    k = np.fft.fftfreq(n) * n
+    kx, ky, kz = np.meshgrid(k, k, k[: n // 2 + 1], indexing="ij")
+    kk2 = kx * kx + ky * ky + kz * kz
+    kk = np.sqrt(kk2)
+    amp = np.zeros_like(kk)
+    nz = kk > 0
+    amp[nz] = kk[nz] ** (slope / 2.0)
+    comps = [
+        (rng.standard_normal(kk.shape) + 1j * rng.standard_normal(kk.shape)) * amp
+        for _ in range(3)
+    ]
+    kv = (kx, ky, kz)
+    div = sum(c * kc for c, kc in zip(comps, kv))
+    safe = np.where(nz, kk2, 1.0)
+    comps = [c - kc * div / safe for c, kc in zip(comps, kv)]
+    out = [np.fft.irfftn(c, s=(n, n, n)) for c in comps]
+    return out
+
+
+def turbulence(grid, hp, mach=3.0, sigma_lnrho=0.5, seed=1234):
+    """Decaying supersonic turbulence IC on a periodic cube.
+
+    Density lognormal (sigma_ln rho) from a seeded GRF with P(k) ~ k^-2, normalised to
+    <rho> = 1; velocity a solenoidal GRF with P(k) ~ k^-4 scaled to rms Mach `mach`
+    at c_s = 1; uniform pressure p = 1/gamma."""
+    assert grid.rank == 3
+    n = grid.end[0] - grid.start[0] + 1
+    assert all(grid.end[d] - grid.start[d] + 1 == n for d in range(3))
+    rng = np.random.default_rng(seed)
+    g = _grf(n, -2.0, rng)
+    rho = np.exp(sigma_lnrho * g - 0.5 * sigma_lnrho ** 2)
+    rho /= rho.mean()
+    vx, vy, vz = _solenoidal(n, -4.0, rng)
+    vrms = np.sqrt(np.mean(vx * vx + vy * vy + vz * vz))
+    scale = mach / vrms
+    # fields are stored (z, y, x); the generator's axes are (x, y, z)
+    to_zyx = lambda a: np.ascontiguousarray(np.transpose(a, (2, 1, 0)))
+    p0 = 1.0 / hp.gamma
+    f = new_fields(grid, hp.dual)
+    act = grid.active_slices()
+    f["d"][act] = to_zyx(rho)
+    f["v1"][act] = to_zyx(vx * scale)
+    f["v2"][act] = to_zyx(vy * scale)
+    f["v3"][act] = to_zyx(vz * scale)
+    eint = p0 / ((hp.gamma - 1.0) * f["d"][act])
+    ke = 0.5 * (f["v1"][act] ** 2 + f["v2"][act] ** 2 + f["v3"][act] ** 2)
+    f["te"][act] = eint + ke
+    if hp.dual:
+        f["ge"][act] = eint
+    fill_ghosts(grid, f, "periodic")
+    return f
+
+
+def sedov(grid, hp, e_blast=1.0, rho0=1.0, p0=1e-5):
+    """Point blast: E deposited as thermal energy in the central 2^3 active cells."""
+    assert grid.rank == 3
+    f = new_fields(grid, hp.dual)
+    f["d"][...] = rho0
+    eint0 = p0 / ((hp.gamma - 1.0) * rho0)
+    f["te"][...] = eint0
+    if hp.dual:
+        f["ge"][...] = eint0
+    c = [grid.start[d] + (grid.end[d] - grid.start[d] + 1) // 2 for d in range(3)]
+    vol = grid.cellwidth[0][0] * grid.cellwidth[1][0] * grid.cellwidth[2][0]
+    e_spec = e_blast / (8.0 * vol * rho0)
+    sl = (slice(c[2] - 1, c[2] + 1), slice(c[1] - 1, c[1] + 1), slice(c[0] - 1, c[0] + 1))
+    f["te"][sl] += e_spec
+    if hp.dual:
+        f["ge"][sl] += e_spec
+    return f
+
+
+def pressure_np(grid, hp, fields):
+    """grid::ComputePressure (time == Time) in numpy, for diagnostics."""
+    g = hp.gamma
+    if hp.dual:
+        ge = fields["ge"]
+    else:
+        v2 = fields["v1"] ** 2
+        if grid.rank > 1:
+            v2 = v2 + fields["v2"] ** 2
+        if grid.rank > 2:
+            v2 = v2 + fields["v3"] ** 2
+        ge = fields["te"] - 0.5 * v2
+    p = (g - 1.0) * fields["d"] * ge
+    return np.maximum(p, hp.tiny_number)
+
+
+def max_signal_dt(grid, hp, fields):
+    """CFL dt (calc_dt.F, ihydro=0) times the Courant factor, numpy version."""
+    p = pressure_np(grid, hp, fields)
+    act = grid.active_slices()
+    cs = np.maximum(np.sqrt(hp.gamma * p[act] / fields["d"][act]), 1e-20)
+    s = 0.0
+    names = ("v1", "v2", "v3")
+    for d in range(grid.rank):
+        s = s + (cs + np.abs(fields[names[d]][act])) / grid.cellwidth[d][0]
+    return hp.cfl / float(np.max(s))

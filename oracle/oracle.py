@@ -1,0 +1,217 @@
+"""ctypes front end of the CPU oracle (TEST INFRASTRUCTURE ONLY).
+
+The oracle is a plain-C FP64 restatement of Enzo's PPM-DE hot path
+(``ppm_oracle.c``; see its header for the reference file:line map).  Only the
+tests, ``__graft_entry__.smoke()`` and the CPU-baseline leg of ``bench.py``
+load it -- always as the checker or the timed CPU reference, never as part of
+the product path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "_build" / "libppm_oracle.so"
+
+FIELD_NAMES = ("d", "te", "v1", "v2", "v3", "ge")
+
+
+class OraParams(C.Structure):
+    _fields_ = [
+        ("rank", C.c_int),
+        ("dims", C.c_int * 3),
+        ("start", C.c_int * 3),
+        ("end", C.c_int * 3),
+        ("gamma", C.c_double),
+        ("dt", C.c_double),
+        ("eta1", C.c_double),
+        ("eta2", C.c_double),
+        ("small_rho", C.c_double),
+        ("tiny_number", C.c_double),
+        ("min_support", C.c_double),
+        ("dual", C.c_int),
+        ("gravity", C.c_int),
+        ("pressure_free", C.c_int),
+        ("fallback", C.c_int),
+        ("max_velocity_index", C.c_int),
+    ]
+
+
+class OraFluxes(C.Structure):
+    _fields_ = [
+        ("left_start", (C.c_longlong * 3) * 3),
+        ("left_end", (C.c_longlong * 3) * 3),
+        ("right_start", (C.c_longlong * 3) * 3),
+        ("right_end", (C.c_longlong * 3) * 3),
+        ("left", (C.POINTER(C.c_double) * 3) * 6),
+        ("right", (C.POINTER(C.c_double) * 3) * 6),
+    ]
+
+
+class OraStats(C.Structure):
+    _fields_ = [
+        ("interfaces", C.c_longlong),
+        ("newton_iters", C.c_longlong),
+        ("newton_hist", C.c_longlong * 8),
+        ("fallbacks", C.c_longlong),
+        ("fatal", C.c_int),
+    ]
+
+    def as_dict(self):
+        return {
+            "interfaces": int(self.interfaces),
+            "newton_iters": int(self.newton_iters),
+            "newton_hist": [int(x) for x in self.newton_hist],
+            "fallbacks": int(self.fallbacks),
+            "fatal": int(self.fatal),
+        }
+
+
+_lib = None
+
+
+def build() -> Path:
+    """Compile the oracle (make in oracle/)."""
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+    return LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            build()
+        L = C.CDLL(str(LIB_PATH))
+        dp = C.POINTER(C.c_double)
+        L.ora_solve_ppm_de.argtypes = [C.POINTER(OraParams), C.c_int, dp * 6, dp * 3, dp * 3,
+                                       C.c_int, C.POINTER(OraFluxes), C.c_longlong * 3,
+                                       C.POINTER(OraStats), C.c_int]
+        L.ora_solve_ppm_de.restype = C.c_int
+        L.ora_sweep.argtypes = [C.c_int, C.POINTER(OraParams), dp * 6, dp, dp * 3, dp * 3,
+                                C.c_int, C.POINTER(OraFluxes), C.c_longlong * 3,
+                                C.POINTER(OraStats), C.c_int]
+        L.ora_sweep.restype = C.c_int
+        L.ora_compute_pressure.argtypes = [C.POINTER(OraParams), dp * 6, dp]
+        L.ora_compute_pressure.restype = None
+        L.ora_calc_dt.argtypes = [C.POINTER(OraParams), dp * 6, dp, dp * 3, C.c_double,
+                                  C.c_double * 3]
+        L.ora_calc_dt.restype = C.c_double
+        L.ora_twoshock_point.argtypes = [C.c_double * 6, C.c_double, C.c_double, C.c_double,
+                                         dp, dp, C.POINTER(C.c_int)]
+        L.ora_twoshock_point.restype = None
+        _lib = L
+    return _lib
+
+
+def _ptr(a):
+    if a is None:
+        return C.POINTER(C.c_double)()
+    assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def make_params(grid, hp, dt) -> OraParams:
+    """grid: object with rank, dims(3), start(3), end(3); hp: HydroParams-like."""
+    P = OraParams()
+    P.rank = grid.rank
+    for d in range(3):
+        P.dims[d] = grid.dims[d]
+        P.start[d] = grid.start[d]
+        P.end[d] = grid.end[d]
+    P.gamma = hp.gamma
+    P.dt = dt
+    P.eta1 = hp.eta1
+    P.eta2 = hp.eta2
+    P.small_rho = hp.small_rho
+    P.tiny_number = hp.tiny_number
+    P.min_support = hp.min_support
+    P.dual = int(hp.dual)
+    P.gravity = int(hp.gravity)
+    P.pressure_free = int(hp.pressure_free)
+    P.fallback = int(hp.fallback)
+    P.max_velocity_index = grid.rank
+    return P
+
+
+def _fields6(fields):
+    arr = (C.POINTER(C.c_double) * 6)()
+    for i, n in enumerate(FIELD_NAMES):
+        arr[i] = _ptr(fields.get(n))
+    return arr
+
+
+def _cw3(cellwidth):
+    arr = (C.POINTER(C.c_double) * 3)()
+    for d in range(3):
+        arr[d] = _ptr(cellwidth[d] if d < len(cellwidth) else None)
+    return arr
+
+
+def solve_ppm_de(grid, hp, dt, cycle, fields, cellwidth, accel=None, subgrids=None,
+                 ggs=(0, 0, 0), nthreads=1):
+    """Advance `fields` (dict of float64 arrays, x fastest) by one split step in place.
+
+    Returns (rc, stats dict).  subgrids: list of OraFluxes (filled in place)."""
+    L = lib()
+    P = make_params(grid, hp, dt)
+    acc = (C.POINTER(C.c_double) * 3)()
+    if accel is not None:
+        for d in range(3):
+            acc[d] = _ptr(accel[d] if d < len(accel) else None)
+    st = OraStats()
+    nsub = 0 if not subgrids else len(subgrids)
+    subarr = None
+    if nsub:
+        subarr = (OraFluxes * nsub)(*subgrids)
+    g = (C.c_longlong * 3)(*ggs)
+    rc = L.ora_solve_ppm_de(C.byref(P), int(cycle), _fields6(fields), acc, _cw3(cellwidth), nsub,
+                            subarr, g, C.byref(st), int(nthreads))
+    if nsub:
+        for i in range(nsub):
+            subgrids[i] = subarr[i]
+    return rc, st.as_dict()
+
+
+def sweep(dim, grid, hp, dt, fields, pressure, cellwidth, accel=None, nthreads=1):
+    L = lib()
+    P = make_params(grid, hp, dt)
+    acc = (C.POINTER(C.c_double) * 3)()
+    if accel is not None:
+        for d in range(3):
+            acc[d] = _ptr(accel[d])
+    st = OraStats()
+    g = (C.c_longlong * 3)(0, 0, 0)
+    rc = L.ora_sweep(int(dim), C.byref(P), _fields6(fields), _ptr(pressure), acc,
+                     _cw3(cellwidth), 0, None, g, C.byref(st), int(nthreads))
+    return rc, st.as_dict()
+
+
+def compute_pressure(grid, hp, fields):
+    L = lib()
+    P = make_params(grid, hp, 0.0)
+    p = np.zeros_like(fields["d"])
+    L.ora_compute_pressure(C.byref(P), _fields6(fields), _ptr(p))
+    return p
+
+
+def calc_dt(grid, hp, fields, pressure, cellwidth, aye=1.0, vgrid=(0.0, 0.0, 0.0)):
+    """calc_dt (without the Courant factor)."""
+    L = lib()
+    P = make_params(grid, hp, 0.0)
+    return L.ora_calc_dt(C.byref(P), _fields6(fields), _ptr(pressure), _cw3(cellwidth),
+                         float(aye), (C.c_double * 3)(*vgrid))
+
+
+def twoshock_point(states6, gamma, pmin, guess=0.0):
+    L = lib()
+    pb = C.c_double()
+    ub = C.c_double()
+    it = C.c_int()
+    L.ora_twoshock_point((C.c_double * 6)(*states6), gamma, pmin, guess, C.byref(pb),
+                         C.byref(ub), C.byref(it))
+    return pb.value, ub.value, it.value

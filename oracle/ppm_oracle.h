@@ -1,0 +1,110 @@
+/*
+ * ppm_oracle.h -- CPU oracle for the PPM-DE hydro hot path (TEST INFRASTRUCTURE).
+ *
+ * This is a plain-C, FP64 restatement of Enzo's directionally split PPM
+ * "Direct Eulerian" solver (HydroMethod = 0), kept in the reference's
+ * Fortran evaluation order and built without floating-point contraction.
+ * It exists only to check the CUDA implementation: tests, the smoke check
+ * and the CPU-baseline leg of the benchmark call it; the product library
+ * never links or calls it.
+ *
+ * Reference routines restated (paths relative to the enzo-dev tree):
+ *   grid::SolvePPM_DE          src/enzo/Grid_SolvePPM_DE.C:36-164
+ *   grid::{x,y,z}EulerSweep    src/enzo/Grid_{x,y,z}EulerSweep.C
+ *   inteuler / intvar          src/enzo/inteuler.F:5-566, intvar.F:5-179
+ *   twoshock                   src/enzo/twoshock.F:5-276
+ *   flux_twoshock / flux_hll   src/enzo/flux_twoshock.F:6-490, flux_hll.F:6-415
+ *   euler                      src/enzo/euler.F:7-285
+ *   pgas2d_dual                src/enzo/pgas2d_dual.F:4-122
+ *   grid::ComputePressure      src/enzo/Grid_ComputePressure.C:36-164
+ *   calc_dt (PPM branch)       src/enzo/calc_dt.F:6-181
+ *
+ * Parity anchors: the reference's analytic shock-tube answer tests
+ * (run/Hydro/Hydro-1D/{SodShockTube,Toro-*}) at the reference's own
+ * tolerances; no bit-level golden output of the Fortran exists in the tree
+ * and no Fortran compiler is available, so bit-level parity of this
+ * restatement against the Fortran itself is unpinned.
+ */
+#ifndef PPM_ORACLE_H
+#define PPM_ORACLE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* field slots, in BaryonField roles */
+enum { ORA_D = 0, ORA_TE = 1, ORA_V1 = 2, ORA_V2 = 3, ORA_V3 = 4, ORA_GE = 5, ORA_NFIELD = 6 };
+
+typedef struct {
+  int rank;            /* GridRank (1..3) */
+  int dims[3];         /* GridDimension, ghosts included */
+  int start[3];        /* GridStartIndex, 0-based */
+  int end[3];          /* GridEndIndex, 0-based inclusive */
+  double gamma;        /* Gamma */
+  double dt;           /* dtFixed */
+  double eta1, eta2;   /* DualEnergyFormalismEta1/2 */
+  double small_rho;    /* SmallRho: density floor applied in euler */
+  double tiny_number;  /* tiny_number: MinimumPressure of the sweeps */
+  double min_support;  /* MinimumSupportEnergyCoefficient (ComputePressure) */
+  int dual;            /* DualEnergyFormalism */
+  int gravity;         /* GravityOn */
+  int pressure_free;   /* PressureFree */
+  int fallback;        /* RiemannSolverFallback */
+  int max_velocity_index; /* MaxVelocityIndex used by ComputePressure */
+} ora_params;
+
+/* struct fluxes (src/enzo/Fluxes.h:29-37), restricted to the six hydro slots */
+typedef struct {
+  long long left_start[3][3], left_end[3][3];
+  long long right_start[3][3], right_end[3][3];
+  double *left[ORA_NFIELD][3];
+  double *right[ORA_NFIELD][3];
+} ora_fluxes;
+
+typedef struct {
+  long long interfaces;      /* Riemann problems solved */
+  long long newton_iters;    /* total Newton updates */
+  long long newton_hist[8];  /* [n] = interfaces that took n Newton updates (1..7) */
+  long long fallbacks;       /* cells whose fluxes were recomputed with HLL */
+  int fatal;                 /* 1 if a state the reference aborts on was met */
+} ora_stats;
+
+/* Optional hook: called for every Riemann problem with the six interface
+   states and the converged pbar (training-data logging). */
+typedef void (*ora_riemann_log_fn)(void *ctx, const double st[6], double pbar, int iters);
+
+/* grid::ComputePressure at time == Time (Grid_ComputePressure.C:96-164). */
+void ora_compute_pressure(const ora_params *P, double *const fields[ORA_NFIELD], double *pressure);
+
+/* One directional sweep over all slices of the grid (dim 0,1,2), i.e. the
+   `for k ... xEulerSweep(k)` loop of Grid_SolvePPM_DE.C:91-97 and its y/z
+   siblings.  accel may be NULL when gravity is off. */
+int ora_sweep(int dim, const ora_params *P, double *const fields[ORA_NFIELD],
+              const double *pressure, double *const accel[3],
+              double *const cellwidth[3], int nsub, ora_fluxes *sub,
+              const long long ggs[3], ora_stats *st, int nthreads);
+
+/* grid::SolvePPM_DE (Grid_SolvePPM_DE.C:36-164), EOSType = 0. */
+int ora_solve_ppm_de(const ora_params *P, int cycle, double *const fields[ORA_NFIELD],
+                     double *const accel[3], double *const cellwidth[3],
+                     int nsub, ora_fluxes *sub, const long long ggs[3],
+                     ora_stats *st, int nthreads);
+
+/* calc_dt (rank 1..3, ihydro = 0) on a pressure field; returns dt without
+   the Courant factor (calc_dt.F:6-181). */
+double ora_calc_dt(const ora_params *P, double *const fields[ORA_NFIELD],
+                   const double *pressure, double *const cellwidth[3],
+                   double aye, const double vgrid[3]);
+
+/* A single two-shock Riemann problem (twoshock.F:115-254 for one interface).
+   st = {dl, dr, pl, pr, ul, ur}. If guess > 0 it replaces the acoustic
+   starting pressure (learned-guess semantics; guess <= 0 = reference). */
+void ora_twoshock_point(const double st[6], double gamma, double pmin, double guess,
+                        double *pbar, double *ubar, int *iters);
+
+void ora_set_riemann_log(ora_riemann_log_fn fn, void *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
