@@ -1,0 +1,418 @@
+// ppm_device.cuh -- per-point FP64 physics of the PPM-DE sweep, as device functions.
+//
+// Each function is one stencil point of a reference Fortran loop, written with the
+// reference's operand order (left-to-right association, x**2 = x*x, x**3 = (x*x)*x,
+// MAX/MIN as a compare-select).  The library is compiled with -fmad=false, so every
+// product and sum is rounded separately, and CUDA's FP64 '/' and sqrt are IEEE
+// correctly rounded: the results are bit-identical to a plain x86-64 build of the
+// same expressions.  The sweep kernels (ppm_sweep.cu) only schedule these points.
+#pragma once
+
+#include <cstdint>
+
+namespace ppm {
+
+constexpr double kTiny = 1.0e-20;        // fortran_types.def: tiny (CONFIG_PFLOAT_8)
+constexpr double kFt = 4.0 / 3.0;        // intvar.F:62, inteuler.F:127
+constexpr double kTolerance = 1.0e-14;   // twoshock.F:97-100 (CONFIG_BFLOAT_8)
+constexpr int kNumIter = 8;              // twoshock.F:105-106
+
+__device__ __forceinline__ double dmax(double a, double b) { return a > b ? a : b; }
+__device__ __forceinline__ double dmin(double a, double b) { return a < b ? a : b; }
+
+struct Phys {
+  double gamma, dt, eta1, eta2, small_rho, pmin;
+  double qa;      // (gamma + 1)/(2 gamma)   twoshock.F:115, flux_twoshock.F:73
+  double gp1;     // gamma + 1
+  double gm1;     // gamma - 1
+};
+
+// ---------------------------------------------------------------- inteuler.F:197-208
+struct Prep {
+  double char1, char2, cm, c0, cp;
+};
+
+__device__ __forceinline__ Prep cell_prep(double d, double p, double u, double dx2i,
+                                          const Phys& P) {
+  Prep r;
+  double cs = sqrt(P.gamma * p / d);
+  r.char1 = dmax(0.0, P.dt * (u + cs)) * dx2i;
+  r.char2 = dmax(0.0, -(P.dt * (u - cs))) * dx2i;
+  r.cm = P.dt * (u - cs) * dx2i;
+  r.c0 = P.dt * (u) * dx2i;
+  r.cp = P.dt * (u + cs) * dx2i;
+  return r;
+}
+
+// ---------------------------------------------------------------- intvar.F:82-94
+__device__ __forceinline__ double pm_slope(double qm, double q0, double qp, double c1, double c2) {
+  double qplus = qp - q0;
+  double qmnus = q0 - qm;
+  double qcent = c1 * qplus + c2 * qmnus;
+  double qvanl = 2.0 * qplus * qmnus / (qmnus + qplus);
+  double temp1 = dmin(dmin(dmin(fabs(qcent), fabs(qvanl)), 2.0 * fabs(qmnus)), 2.0 * fabs(qplus));
+  double r = temp1 * copysign(1.0, qcent);
+  return (qplus * qmnus > 0.0) ? r : 0.0;
+}
+
+// ---------------------------------------------------------------- intvar.F:98-102
+__device__ __forceinline__ double pm_edge(double qm, double q0, double dqm, double dq0, double c3,
+                                          double c4, double c5, double c6) {
+  return c3 * qm + c4 * q0 + c5 * dqm + c6 * dq0;
+}
+
+// ------------------------------------------- intvar.F:117-160 (no steepening/flattening)
+struct Para {
+  double ql, qr, q6, dq;
+};
+
+__device__ __forceinline__ Para pm_parabola(double qm, double q0, double qp, double ql, double qr) {
+  double temp1 = (qr - q0) * (q0 - ql);
+  double temp2 = qr - ql;
+  double temp3 = 6.0 * (q0 - 0.5 * (qr + ql));
+  if (temp1 <= 0.0) {
+    ql = q0;
+    qr = q0;
+  }
+  double temp22 = temp2 * temp2;
+  double temp23 = temp2 * temp3;
+  if (temp22 < temp23) ql = 3.0 * q0 - 2.0 * qr;
+  if (temp22 < -temp23) qr = 3.0 * q0 - 2.0 * ql;
+  // CHECK_LR, intvar.F:145-153
+  ql = dmax(dmin(q0, qm), ql);
+  ql = dmin(dmax(q0, qm), ql);
+  qr = dmax(dmin(q0, qp), qr);
+  qr = dmin(dmax(q0, qp), qr);
+  Para r;
+  r.q6 = 6.0 * (q0 - 0.5 * (ql + qr));
+  r.dq = qr - ql;
+  r.ql = ql;
+  r.qr = qr;
+  return r;
+}
+
+// characteristic averages, intvar.F:162-174 and inteuler.F:304-316
+// A: qla (x = char1), ql0 (c0), plm/ulm (cm), plp/ulp (cp) from the cell left of a face
+__device__ __forceinline__ double pm_A(const Para& a, double x) {
+  return a.qr - x * (a.dq - (1.0 - kFt * x) * a.q6);
+}
+// B: qr0 (c0), prm/urm (cm), prp/urp (cp) from the cell right of a face
+__device__ __forceinline__ double pm_B(const Para& a, double x) {
+  return a.ql - x * (a.dq + (1.0 + kFt * x) * a.q6);
+}
+// C: qra (x = char2)
+__device__ __forceinline__ double pm_C(const Para& a, double x) {
+  return a.ql + x * (a.dq + (1.0 - kFt * x) * a.q6);
+}
+
+// What a face needs from the cell on its left / right.
+struct Lside {
+  double dla, dl0, pla, pl0, plm, plp, ula, ul0, ulm, ulp, vla, vl0, wla, wl0, gela, gel0;
+  double cm, c0, cp;
+};
+struct Rside {
+  double dra, dr0, pra, pr0, prm, prp, ura, ur0, urm, urp, vra, vr0, wra, wr0, gera, ger0;
+  double cm, c0, cp;
+};
+
+struct FaceState {
+  double dl, dr, pl, pr, ul, ur, vl, vr, wl, wr, gel, ger;
+};
+
+// ------------------------------------------------------- inteuler.F:320-551 for one face
+// gsum = grslice(i-1) + grslice(i) (only read when GRAV); ul_cell/ur_cell = uslice(i-1)/(i)
+template <bool DUAL, bool GRAV>
+__device__ __forceinline__ FaceState face_assemble(const Lside& L, const Rside& R, double ul_cell,
+                                                   double ur_cell, double gsum, const Phys& P) {
+  FaceState s;
+  double cla = sqrt(dmax(P.gamma * L.pla * L.dla, 0.0));
+  double cra = sqrt(dmax(P.gamma * R.pra * R.dra, 0.0));
+  // a) left side
+  double f1 = 1.0 / cla;
+  double betalp = (L.ula - L.ulp) + (L.pla - L.plp) * f1;
+  double betalm = (L.ula - L.ulm) - (L.pla - L.plm) * f1;
+  double betal0 = (L.pla - L.pl0) * (f1 * f1) + 1.0 / L.dla - 1.0 / L.dl0;
+  double gterm = 0.0;
+  if (GRAV) {
+    gterm = 0.25 * P.dt * gsum;
+    betalp = betalp - gterm;
+    betalm = betalm - gterm;
+  }
+  f1 = 0.5 / cla;
+  betalp = -(betalp * f1);
+  betalm = +betalm * f1;
+  if (L.cp <= 0.0) betalp = 0.0;
+  if (L.cm <= 0.0) betalm = 0.0;
+  if (L.c0 <= 0.0) betal0 = 0.0;
+  // b) right side
+  f1 = 1.0 / cra;
+  double betarp = (R.ura - R.urp) + (R.pra - R.prp) * f1;
+  double betarm = (R.ura - R.urm) - (R.pra - R.prm) * f1;
+  double betar0 = (R.pra - R.pr0) * (f1 * f1) + 1.0 / R.dra - 1.0 / R.dr0;
+  if (GRAV) {
+    betarp = betarp - gterm;
+    betarm = betarm - gterm;
+  }
+  f1 = 0.5 / cra;
+  betarp = -(betarp * f1);
+  betarm = +betarm * f1;
+  if (R.cp >= 0.0) betarp = 0.0;
+  if (R.cm >= 0.0) betarm = 0.0;
+  if (R.c0 >= 0.0) betar0 = 0.0;
+  // eq. 3.6
+  s.pl = L.pla + (betalp + betalm) * (cla * cla);
+  s.pr = R.pra + (betarp + betarm) * (cra * cra);
+  s.ul = L.ula + (betalp - betalm) * cla;
+  s.ur = R.ura + (betarp - betarm) * cra;
+  s.dl = 1.0 / (1.0 / L.dla - (betal0 + betalp + betalm));
+  s.dr = 1.0 / (1.0 / R.dra - (betar0 + betarp + betarm));
+  // advected quantities, inteuler.F:414-434
+  if (ul_cell <= 0.0) {
+    s.vl = L.vla; s.wl = L.wla; s.gel = L.gela;
+  } else {
+    s.vl = L.vl0; s.wl = L.wl0; s.gel = L.gel0;
+  }
+  if (ur_cell >= 0.0) {
+    s.vr = R.vra; s.wr = R.wra; s.ger = R.gera;
+  } else {
+    s.vr = R.vr0; s.wr = R.wr0; s.ger = R.ger0;
+  }
+  // dual-energy hypersonic override, inteuler.F:493-521
+  if (DUAL) {
+    double ml = dmax(dmax(fabs(L.cm), fabs(L.c0)), fabs(L.cp));
+    if (P.gamma * L.pla / L.dla < P.eta2 * (L.ula * L.ula) || ml < 1.0e-3 || s.dl / L.dla > 5.0) {
+      s.pl = L.pla; s.ul = L.ula; s.dl = L.dla;
+    }
+    double mr = dmax(dmax(fabs(R.cm), fabs(R.c0)), fabs(R.cp));
+    if (P.gamma * R.pra / R.dra < P.eta2 * (R.ura * R.ura) || mr < 1.0e-3 || s.dr / R.dra > 5.0) {
+      s.pr = R.pra; s.ur = R.ura; s.dr = R.dra;
+    }
+  }
+  // floors, inteuler.F:540-545
+  s.pl = dmax(s.pl, kTiny);
+  s.pr = dmax(s.pr, kTiny);
+  s.dl = dmax(s.dl, kTiny);
+  s.dr = dmax(s.dr, kTiny);
+  return s;
+}
+
+// ---------------------------------------------- twoshock.F:156-254 for one interface
+// The acoustic starting pressure of twoshock.F:156-170, or `guess` when guess > 0.
+struct Riemann {
+  double pbar, ubar;
+  int iters;      // Newton updates performed (1..7)
+  bool converged; // reached |dp/p| < tolerance within numiter - 1 updates
+};
+
+__device__ __forceinline__ double acoustic_guess(const FaceState& s, double cl, double cr,
+                                                 const Phys& P) {
+  double ps = (cr * s.pl + cl * s.pr + cr * cl * (s.ul - s.ur)) / (cr + cl);
+  if (ps < P.pmin) ps = P.pmin;
+  return ps;
+}
+
+__device__ __forceinline__ Riemann twoshock_newton(const FaceState& s, double cl, double cr,
+                                                   double ps, const Phys& P) {
+  double old_ps = ps, ubl = 0.0, ubr = 0.0, dpdul = 0.0, dpdur = 0.0;
+  int it = 0;
+  bool active = true;
+#pragma unroll 1
+  for (int n = 2; n <= kNumIter; n++) {
+    if (active) {
+      double zl = cl * sqrt((1.0 + P.qa * (ps / s.pl - 1.0)));
+      double zr = cr * sqrt((1.0 + P.qa * (ps / s.pr - 1.0)));
+      ubl = s.ul - (ps - s.pl) / zl;
+      ubr = s.ur + (ps - s.pr) / zr;
+      dpdul = -(4.0 * (zl * zl * zl) / s.dl / (4.0 * (zl * zl) / s.dl - P.gp1 * (ps - s.pl)));
+      dpdur = 4.0 * (zr * zr * zr) / s.dr / (4.0 * (zr * zr) / s.dr - P.gp1 * (ps - s.pr));
+      ps = ps + (ubr - ubl) * dpdur * dpdul / (dpdur - dpdul);
+      if (ps < P.pmin) ps = P.pmin;
+      double delta_ps = ps - old_ps;
+      old_ps = ps;
+      it++;
+      if (fabs(delta_ps / ps) < kTolerance) active = false;
+    }
+  }
+  Riemann r;
+  if (ps < P.pmin) ps = dmin(s.pl, s.pr);
+  r.pbar = ps;
+  r.ubar = ubl + (ubr - ubl) * dpdur / (dpdur - dpdul);
+  r.iters = it;
+  r.converged = !active;
+  return r;
+}
+
+// ------------------------------------ flux_twoshock.F:84-396 for one face (RAREFACTION2)
+struct Flux {
+  double df, ef, uf, vf, wf, gef, ub;
+};
+
+template <bool DUAL>
+__device__ __forceinline__ Flux flux_twoshock(const FaceState& s, double pbar, double ubar,
+                                              double qc, const Phys& P) {
+  const double gamma = P.gamma;
+  double sn = copysign(1.0, -ubar);
+  double u0, p0, d0;
+  if (sn < 0.0) {
+    u0 = s.ul; p0 = s.pl; d0 = s.dl;
+  } else {
+    u0 = s.ur; p0 = s.pr; d0 = s.dr;
+  }
+  double c0 = sqrt(dmax(gamma * p0 / d0, kTiny));
+  double z0 = c0 * d0 * sqrt(dmax(1.0 + P.qa * (pbar / p0 - 1.0), kTiny));
+  double dbar = 1.0 / (1.0 / d0 - (pbar - p0) / dmax(z0 * z0, kTiny));
+  double cbar = sqrt(dmax(gamma * pbar / dbar, kTiny));
+  double l0, lbar;
+  if (pbar < p0) {
+    l0 = u0 * sn + c0;
+    lbar = sn * ubar + cbar;
+  } else {
+    l0 = u0 * sn + z0 / d0;
+    lbar = l0;
+  }
+  double frac = l0 - lbar;
+  if (frac < kTiny) frac = kTiny;
+  frac = (0.0 - lbar) / frac;
+  frac = dmin(dmax(frac, 0.0), 1.0);
+  double pb = p0 * frac + pbar * (1.0 - frac);
+  double db = d0 * frac + dbar * (1.0 - frac);
+  double ub = u0 * frac + ubar * (1.0 - frac);
+  if (lbar >= 0.0) {
+    pb = pbar; db = dbar; ub = ubar;
+  }
+  if (l0 < 0.0) {
+    pb = p0; db = d0; ub = u0;
+  }
+  double vb, wb, geb;
+  if (ub > 0.0) {
+    vb = s.vl; wb = s.wl; geb = s.gel;
+  } else {
+    vb = s.vr; wb = s.wr; geb = s.ger;
+  }
+  double eb = pb / (P.gm1 * db) + 0.5 * (ub * ub + vb * vb + wb * wb);
+  double upb = pb * ub;
+  double dub = ub * db;
+  double duub = dub * ub;
+  double duvb = dub * vb;
+  double duwb = dub * wb;
+  double dueb = dub * eb;
+  Flux f;
+  f.df = qc * dub;
+  f.ef = qc * (dueb + upb);
+  f.uf = qc * (duub + pb);
+  f.vf = qc * duvb;
+  f.wf = qc * duwb;
+  f.gef = DUAL ? qc * (dub * geb) : 0.0;
+  f.ub = ub;
+  return f;
+}
+
+// ------------------------------------------ flux_hll.F:111-258 for one face (no diffusion)
+struct HllFace {
+  double sl, sr, gesl, gesr;
+  double df, uf, vf, wf, ef, gef;  // before the dt/dx factor
+};
+
+template <bool DUAL>
+__device__ __forceinline__ HllFace hll_face(const FaceState& s, const Phys& P) {
+  const double gamma = P.gamma;
+  const double gamma1 = gamma - 1.0;
+  const double gamma1i = 1.0 / gamma1;
+  double sqrtdl = sqrt(s.dl);
+  double sqrtdr = sqrt(s.dr);
+  double isdlpdr = 1.0 / (sqrtdl + sqrtdr);
+  double vroe1 = (sqrtdl * s.ul + sqrtdr * s.ur) * isdlpdr;
+  double vroe2 = (sqrtdl * s.vl + sqrtdr * s.vr) * isdlpdr;
+  double vroe3 = (sqrtdl * s.wl + sqrtdr * s.wr) * isdlpdr;
+  double v2 = vroe1 * vroe1 + vroe2 * vroe2 + vroe3 * vroe3;
+  double el = gamma1i * s.pl + 0.5 * s.dl * (s.ul * s.ul + s.vl * s.vl + s.wl * s.wl);
+  double er = gamma1i * s.pr + 0.5 * s.dr * (s.ur * s.ur + s.vr * s.vr + s.wr * s.wr);
+  double hroe = ((el + s.pl) / sqrtdl + (er + s.pr) / sqrtdr) * isdlpdr;
+  double cs = sqrt(gamma1 * dmax((hroe - 0.5 * v2), kTiny));
+  double char1 = vroe1 - cs;
+  double char2 = vroe1 + cs;
+  double csl0 = sqrt(gamma * s.pl / s.dl);
+  double csr0 = sqrt(gamma * s.pr / s.dr);
+  double csl = dmin(s.ul - csl0, char1);
+  double csr = dmax(s.ur + csr0, char2);
+  double bm = dmin(csl, 0.0);
+  double bp = dmax(csr, 0.0);
+  double bm0 = s.ul - bm;
+  double bp0 = s.ur - bp;
+  double q1 = (bp + bm) / (bp - bm);
+  HllFace h;
+  h.sl = 0.5 * (1.0 + q1);
+  h.sr = 0.5 * (1.0 - q1);
+  h.gesl = bm0;
+  h.gesr = bp0;
+  double dubl = s.dl * s.ul;
+  double dubr = s.dr * s.ur;
+  double dfl = s.dl * bm0, dfr = s.dr * bp0;
+  double ufl = dubl * bm0 + s.pl, ufr = dubr * bp0 + s.pr;
+  double vfl = s.dl * s.vl * bm0, vfr = s.dr * s.vr * bp0;
+  double wfl = s.dl * s.wl * bm0, wfr = s.dr * s.wr * bp0;
+  double efl = el * bm0 + s.pl * s.ul, efr = er * bp0 + s.pr * s.ur;
+  h.df = h.sl * dfl + h.sr * dfr + 0.0;
+  h.uf = h.sl * ufl + h.sr * ufr + 0.0;
+  h.vf = h.sl * vfl + h.sr * vfr + 0.0;
+  h.wf = h.sl * wfl + h.sr * wfr + 0.0;
+  h.ef = h.sl * efl + h.sr * efr + 0.0;
+  if (DUAL) {
+    double gefl = bm0 * s.gel * s.dl;
+    double gefr = bp0 * s.ger * s.dr;
+    h.gef = h.sl * gefl + h.sr * gefr + 0.0;
+  } else {
+    h.gef = 0.0;
+  }
+  return h;
+}
+
+// -------------------------------------------------------------- euler.F:126-279 (one cell)
+struct Cell {
+  double d, e, u, v, w, ge;
+};
+
+template <bool DUAL, bool GRAV>
+__device__ __forceinline__ Cell euler_update(const Cell& c, const Flux& F0, const Flux& F1,
+                                             double ges, double gr, const Phys& P, bool& fatal) {
+  Cell o;
+  double dnu = c.d + (F0.df - F1.df);
+  double dnuinv = 1.0 / dnu;
+  if (P.small_rho > 0.0) {
+    dnu = dmax(dnu, P.small_rho);
+    dnuinv = 1.0 / dnu;
+  }
+  double uold = c.u;
+  o.u = (c.u * c.d + (F0.uf - F1.uf)) * dnuinv;
+  o.v = (c.v * c.d + (F0.vf - F1.vf)) * dnuinv;
+  o.w = (c.w * c.d + (F0.wf - F1.wf)) * dnuinv;
+  o.e = dmax(0.1 * c.e, (c.e * c.d + (F0.ef - F1.ef)) * dnuinv);
+  if (DUAL) {
+    o.ge = dmax((c.ge * c.d + (F0.gef - F1.gef) + ges) * dnuinv, 0.5 * c.ge);
+    if (o.ge < 0.0) fatal = true;
+  } else {
+    o.ge = c.ge;
+  }
+  if (GRAV) {
+    o.u = o.u + P.dt * gr * 0.5 * (c.d * dnuinv + 1.0);
+    o.e = o.e + P.dt * gr * 0.5 * (o.u + uold * c.d * dnuinv);
+    o.e = dmax(o.e, kTiny);
+  }
+  o.d = dnu;
+  return o;
+}
+
+// ----------------------------------------------------- pgas2d_dual.F:70-117 (one cell)
+// de_m / de_p: dslice*eslice of the clamped left / right neighbours, the left one
+// already rewritten by this routine (the loop is sequential along the pencil).
+__device__ __forceinline__ void pgas2d_dual(Cell& c, double de_m, double de_p, const Phys& P) {
+  double ke = 0.5 * (c.u * c.u + c.v * c.v + c.w * c.w);
+  double ge1 = c.e - ke;
+  double demax = dmax(dmax(c.d * c.e, de_m), de_p);
+  if (ge1 * c.d / demax > P.eta2) c.ge = ge1;
+  double ge2 = (ge1 / c.e > P.eta1) ? ge1 : c.ge;
+  ge2 = dmax(ge2, P.pmin / (P.gm1 * c.d));
+  c.e = c.e - ge1 + ge2;
+}
+
+}  // namespace ppm

@@ -1,0 +1,71 @@
+// ppm_sweep.cuh -- launch arguments shared by the sweep kernels and the host driver.
+#pragma once
+
+#include <cstdint>
+
+namespace ppm {
+
+// Per-cell coefficients along one sweep axis, precomputed by the host from the
+// cell widths exactly as inteuler.F:140-158 computes them (same expressions, FP64).
+struct Coef {
+  double c1, c2, c3, c4, c5, c6, dx2i, dx;
+};
+
+// Subgrid-flux capture request for one pencil: flux of face `face` goes to
+// `dst_offset` of capture slot `slot` (a contiguous range of the capture buffer).
+struct FluxCapture {
+  int64_t pencil;     // linear pencil id
+  int32_t face;       // face index along the pencil (left face of cell `face`)
+  int32_t pad;
+  int64_t dst;        // base offset (in doubles) of this request in the capture buffer
+};
+
+enum { kMaxCounters = 16 };
+// device counters (unsigned long long), see ppm_b200_stats
+enum {
+  kCntInterfaces = 0,
+  kCntNewton = 1,
+  kCntHist0 = 2,  // 2..9 : newton_hist[0..7]
+  kCntFallbacks = 10,
+  kCntFatal = 11,
+  kCntGuessRejected = 12,
+  kCntNonFinite = 13,
+};
+
+struct SweepArgs {
+  // geometry: pencils are indexed p = t2 * n1 + t1; cell a of pencil (t1, t2)
+  // sits at element t1 * s1 + t2 * s2 + a * sa of every field array.
+  int n;                 // pencil length (GridDimension[dim])
+  int is, ie;            // active range along the pencil, 0-based inclusive
+  int n1, n2;            // pencils along the two transverse axes
+  int64_t s1, s2, sa;    // element strides
+  int64_t npencils;
+  // fields: d, e, u(sweep velocity), v, w, ge -- input and output sets (distinct)
+  const double* __restrict__ in_d;
+  const double* __restrict__ in_e;
+  const double* __restrict__ in_u;
+  const double* __restrict__ in_v;   // may be null (rank < 3): read as 0, not written
+  const double* __restrict__ in_w;
+  const double* __restrict__ in_ge;  // may be null unless dual
+  const double* __restrict__ pres;   // pressure of this SolvePPM_DE call (stale across sweeps)
+  const double* __restrict__ grav;   // acceleration along the sweep axis (GRAV only)
+  double* __restrict__ out_d;
+  double* __restrict__ out_e;
+  double* __restrict__ out_u;
+  double* __restrict__ out_v;
+  double* __restrict__ out_w;
+  double* __restrict__ out_ge;
+  const Coef* __restrict__ coef;     // n entries
+  // physics
+  double gamma, dt, eta1, eta2, small_rho, pmin;
+  const double* dt_device;           // if non-null, *dt_device replaces dt
+  int fallback;                      // RiemannSolverFallback
+  // diagnostics
+  unsigned long long* counters;      // kMaxCounters
+  // subgrid flux capture (optional)
+  const FluxCapture* captures;       // sorted by pencil
+  int64_t ncaptures;
+  double* capture_buf;               // 6 doubles per request: df, ef, uf, vf, wf, gef
+};
+
+}  // namespace ppm

@@ -1,0 +1,301 @@
+"""ctypes binding of the C ABI in include/ppm_b200.h (libppm_b200.so).
+
+This is the Python mirror of the reference's call site: ``Context.solve_ppm_de``
+takes what ``grid::SolvePPM_DE`` takes (cycle number, subgrid flux boxes, the
+grid's global start) and fields in Enzo's BaryonField layout, either as host
+numpy arrays (copied in and out inside the call) or as device tensors.
+The library is required: there is no CPU fallback on this path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+from . import build as _build
+
+OK = 0
+ERR_UNSUPPORTED = -1
+ERR_INVALID = -2
+ERR_CUDA = -3
+ERR_NEGATIVE = -4
+ERR_NONFINITE = -5
+ERR_TOO_LARGE = -6
+MEM_HOST = 0
+MEM_DEVICE = 1
+RIEMANN_TWOSHOCK = 5
+RECONSTRUCTION_PPM = 1
+
+EXPORTS = (
+    "ppm_b200_create", "ppm_b200_destroy", "ppm_b200_solve_ppm_de", "ppm_b200_euler_sweep",
+    "ppm_b200_compute_pressure", "ppm_b200_compute_timestep", "ppm_b200_set_boundary",
+    "ppm_b200_synchronize", "ppm_b200_launch_count", "ppm_b200_error_string",
+    "ppm_b200_version",
+)
+
+_dp = C.POINTER(C.c_double)
+
+
+class Params(C.Structure):
+    _fields_ = [
+        ("gamma", C.c_double), ("dt", C.c_double), ("eta1", C.c_double), ("eta2", C.c_double),
+        ("small_rho", C.c_double), ("tiny_number", C.c_double), ("min_support", C.c_double),
+        ("dual_energy", C.c_int), ("gravity", C.c_int), ("pressure_free", C.c_int),
+        ("riemann_solver", C.c_int), ("riemann_fallback", C.c_int), ("reconstruction", C.c_int),
+        ("steepening", C.c_int), ("flattening", C.c_int), ("diffusion", C.c_int),
+        ("conservative_rec", C.c_int), ("positive_rec", C.c_int), ("eos_type", C.c_int),
+        ("number_of_colours", C.c_int), ("learned_guess", C.c_int),
+        ("dt_device", C.c_void_p), ("reserved", C.c_int * 6),
+    ]
+
+
+class GridDesc(C.Structure):
+    _fields_ = [
+        ("rank", C.c_int), ("dims", C.c_int * 3), ("start", C.c_int * 3), ("end", C.c_int * 3),
+        ("density", C.c_void_p), ("total_energy", C.c_void_p), ("velocity", C.c_void_p * 3),
+        ("gas_energy", C.c_void_p), ("acceleration", C.c_void_p * 3),
+        ("cell_width", C.c_void_p * 3),
+    ]
+
+
+class Fluxes(C.Structure):
+    _fields_ = [
+        ("left_start", (C.c_longlong * 3) * 3), ("left_end", (C.c_longlong * 3) * 3),
+        ("right_start", (C.c_longlong * 3) * 3), ("right_end", (C.c_longlong * 3) * 3),
+        ("left", (C.c_void_p * 3) * 6), ("right", (C.c_void_p * 3) * 6),
+    ]
+
+
+class Stats(C.Structure):
+    _fields_ = [
+        ("interfaces", C.c_longlong), ("newton_iters", C.c_longlong),
+        ("newton_hist", C.c_longlong * 8), ("fallbacks", C.c_longlong),
+        ("fatal_cells", C.c_longlong), ("guess_rejected", C.c_longlong),
+    ]
+
+    def as_dict(self):
+        return {
+            "interfaces": int(self.interfaces), "newton_iters": int(self.newton_iters),
+            "newton_hist": [int(x) for x in self.newton_hist], "fallbacks": int(self.fallbacks),
+            "fatal_cells": int(self.fatal_cells), "guess_rejected": int(self.guess_rejected),
+        }
+
+
+class PPMError(RuntimeError):
+    def __init__(self, code, what=""):
+        self.code = code
+        super().__init__(f"{what}: ppm_b200 error {code} ({error_string(code)})")
+
+
+_lib = None
+
+
+def library_path() -> Path:
+    return _build.LIB
+
+
+def lib(build_if_missing: bool = True):
+    """Load libppm_b200.so (building it when missing and nvcc is available)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not _build.LIB.exists():
+        if not build_if_missing:
+            raise RuntimeError(f"{_build.LIB} is missing; run python -m ppm_b200.build")
+        _build.build()
+    L = C.CDLL(str(_build.LIB))
+    vp = C.c_void_p
+    L.ppm_b200_create.argtypes = [C.c_int, vp, C.POINTER(vp)]
+    L.ppm_b200_destroy.argtypes = [vp]
+    L.ppm_b200_solve_ppm_de.argtypes = [vp, C.POINTER(Params), C.c_int, C.POINTER(GridDesc),
+                                        C.c_int, C.c_int, C.POINTER(Fluxes),
+                                        C.POINTER(C.c_longlong), C.POINTER(Stats)]
+    L.ppm_b200_euler_sweep.argtypes = [vp, C.c_int, C.POINTER(Params), C.POINTER(GridDesc),
+                                       vp, C.c_int, C.c_int, C.POINTER(Fluxes),
+                                       C.POINTER(C.c_longlong), C.POINTER(Stats)]
+    L.ppm_b200_compute_pressure.argtypes = [vp, C.POINTER(Params), C.POINTER(GridDesc), vp,
+                                            C.c_int]
+    L.ppm_b200_compute_timestep.argtypes = [vp, C.POINTER(Params), C.POINTER(GridDesc), C.c_int,
+                                            C.c_double, C.c_double, C.POINTER(C.c_double),
+                                            vp, C.POINTER(C.c_double)]
+    L.ppm_b200_set_boundary.argtypes = [vp, C.POINTER(GridDesc), C.c_int, C.POINTER(C.c_int)]
+    L.ppm_b200_synchronize.argtypes = [vp, C.POINTER(Stats)]
+    L.ppm_b200_launch_count.argtypes = [vp]
+    L.ppm_b200_launch_count.restype = C.c_longlong
+    L.ppm_b200_error_string.argtypes = [C.c_int]
+    L.ppm_b200_error_string.restype = C.c_char_p
+    L.ppm_b200_version.argtypes = []
+    for name in EXPORTS:
+        fn = getattr(L, name)
+        if name not in ("ppm_b200_launch_count", "ppm_b200_error_string"):
+            fn.restype = C.c_int
+    _lib = L
+    return L
+
+
+def error_string(code: int) -> str:
+    return lib().ppm_b200_error_string(int(code)).decode()
+
+
+def _addr(x):
+    """Address of a host numpy array or a device tensor (None -> NULL)."""
+    if x is None:
+        return None
+    if isinstance(x, np.ndarray):
+        assert x.dtype == np.float64 and x.flags["C_CONTIGUOUS"], "float64 C-contiguous required"
+        return x.ctypes.data
+    # torch tensor
+    assert x.dtype.__str__() == "torch.float64" and x.is_contiguous()
+    return x.data_ptr()
+
+
+def make_params(hp, dt, learned_guess=False, dt_device=None) -> Params:
+    P = Params()
+    P.gamma = hp.gamma
+    P.dt = float(dt)
+    P.eta1 = hp.eta1
+    P.eta2 = hp.eta2
+    P.small_rho = hp.small_rho
+    P.tiny_number = hp.tiny_number
+    P.min_support = hp.min_support
+    P.dual_energy = int(hp.dual)
+    P.gravity = int(hp.gravity)
+    P.pressure_free = int(hp.pressure_free)
+    P.riemann_solver = RIEMANN_TWOSHOCK
+    P.riemann_fallback = int(hp.fallback)
+    P.reconstruction = RECONSTRUCTION_PPM
+    P.learned_guess = int(learned_guess)
+    P.dt_device = _addr(dt_device) if dt_device is not None else None
+    return P
+
+
+def make_grid(grid, fields, accel=None):
+    """Returns (GridDesc, keepalive list)."""
+    G = GridDesc()
+    G.rank = grid.rank
+    for d in range(3):
+        G.dims[d] = grid.dims[d]
+        G.start[d] = grid.start[d]
+        G.end[d] = grid.end[d]
+    G.density = _addr(fields["d"])
+    G.total_energy = _addr(fields["te"])
+    for d, n in enumerate(("v1", "v2", "v3")):
+        G.velocity[d] = _addr(fields.get(n)) if d < grid.rank else None
+    G.gas_energy = _addr(fields.get("ge"))
+    keep = []
+    for d in range(3):
+        if accel is not None and d < len(accel) and accel[d] is not None:
+            G.acceleration[d] = _addr(accel[d])
+        cw = np.ascontiguousarray(grid.cellwidth[d], dtype=np.float64)
+        keep.append(cw)
+        G.cell_width[d] = cw.ctypes.data
+    return G, keep
+
+
+def make_fluxes(box):
+    """box: dict with left_start/left_end/right_start/right_end (3x3) and arrays
+    left[slot][dim], right[slot][dim] (numpy, may be None). Returns Fluxes."""
+    F = Fluxes()
+    for key in ("left_start", "left_end", "right_start", "right_end"):
+        arr = getattr(F, key)
+        for i in range(3):
+            for j in range(3):
+                arr[i][j] = int(box[key][i][j])
+    for side in ("left", "right"):
+        arr = getattr(F, side)
+        for s in range(6):
+            for d in range(3):
+                a = box[side][s][d]
+                arr[s][d] = _addr(a) if a is not None else None
+    return F
+
+
+class Context:
+    """One ppm_b200_context (one per rank / device)."""
+
+    def __init__(self, device: int = 0, stream=None):
+        self.L = lib()
+        h = C.c_void_p()
+        rc = self.L.ppm_b200_create(int(device), stream, C.byref(h))
+        if rc != OK:
+            raise PPMError(rc, "ppm_b200_create")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.ppm_b200_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def launches(self) -> int:
+        return int(self.L.ppm_b200_launch_count(self.h))
+
+    def solve_ppm_de(self, grid, hp, dt, cycle, fields, memory=MEM_HOST, accel=None,
+                     subgrids=None, ggs=(0, 0, 0), want_stats=True, learned_guess=False,
+                     dt_device=None, check=True):
+        P = make_params(hp, dt, learned_guess, dt_device)
+        G, keep = make_grid(grid, fields, accel)
+        st = Stats()
+        nsub = 0 if not subgrids else len(subgrids)
+        sub = None
+        if nsub:
+            sub = (Fluxes * nsub)(*[make_fluxes(b) for b in subgrids])
+        g = (C.c_longlong * 3)(*[int(x) for x in ggs])
+        rc = self.L.ppm_b200_solve_ppm_de(self.h, C.byref(P), int(cycle), C.byref(G), int(memory),
+                                          nsub, sub, g, C.byref(st) if want_stats else None)
+        if check and rc != OK:
+            raise PPMError(rc, "ppm_b200_solve_ppm_de")
+        return rc, st.as_dict()
+
+    def euler_sweep(self, dim, grid, hp, dt, fields, pressure, memory=MEM_HOST, accel=None,
+                    check=True):
+        P = make_params(hp, dt)
+        G, keep = make_grid(grid, fields, accel)
+        st = Stats()
+        g = (C.c_longlong * 3)(0, 0, 0)
+        rc = self.L.ppm_b200_euler_sweep(self.h, int(dim), C.byref(P), C.byref(G),
+                                         _addr(pressure), int(memory), 0, None, g, C.byref(st))
+        if check and rc != OK:
+            raise PPMError(rc, "ppm_b200_euler_sweep")
+        return rc, st.as_dict()
+
+    def compute_pressure(self, grid, hp, fields, out, memory=MEM_HOST):
+        P = make_params(hp, 0.0)
+        G, keep = make_grid(grid, fields)
+        rc = self.L.ppm_b200_compute_pressure(self.h, C.byref(P), C.byref(G), _addr(out),
+                                              int(memory))
+        if rc != OK:
+            raise PPMError(rc, "ppm_b200_compute_pressure")
+
+    def compute_timestep(self, grid, hp, fields, memory=MEM_HOST, courant=None, aye=1.0,
+                         vgrid=(0.0, 0.0, 0.0), dt_device=None, want_host=True):
+        P = make_params(hp, 0.0)
+        G, keep = make_grid(grid, fields)
+        vg = (C.c_double * 3)(*vgrid)
+        out = C.c_double(0.0)
+        cf = hp.cfl if courant is None else courant
+        rc = self.L.ppm_b200_compute_timestep(self.h, C.byref(P), C.byref(G), int(memory),
+                                              float(cf), float(aye), vg,
+                                              _addr(dt_device) if dt_device is not None else None,
+                                              C.byref(out) if want_host else None)
+        if rc != OK:
+            raise PPMError(rc, "ppm_b200_compute_timestep")
+        return out.value
+
+    def set_boundary(self, grid, fields, dual, bc=("periodic",) * 3):
+        G, keep = make_grid(grid, fields)
+        codes = (C.c_int * 3)(*[0 if b == "periodic" else 1 for b in bc])
+        rc = self.L.ppm_b200_set_boundary(self.h, C.byref(G), int(bool(dual)), codes)
+        if rc != OK:
+            raise PPMError(rc, "ppm_b200_set_boundary")
+
+    def synchronize(self):
+        st = Stats()
+        rc = self.L.ppm_b200_synchronize(self.h, C.byref(st))
+        return rc, st.as_dict()

@@ -1,0 +1,173 @@
+/*
+ * ppm_b200.h -- C ABI of the B200 PPM-DE hydro library.
+ *
+ * Drop-in replacement for the directionally split PPM "Direct Eulerian"
+ * solver of Enzo (HydroMethod = 0).  The entry points mirror the reference's
+ * own seam: grid::SolvePPM_DE (src/enzo/Grid_SolvePPM_DE.C:36) and the
+ * per-direction sweep loops it runs (Grid_SolvePPM_DE.C:86-146, each a loop of
+ * grid::{x,y,z}EulerSweep, src/enzo/Grid_xEulerSweep.C:33), and the
+ * UseCUDA branch that the reference reserves for a GPU solver
+ * (cuPPMInitParameter / cuPPMInitData / cuPPMSweep / cuPPMSaveSubgridFluxes /
+ * cuPPMGetBaryon / cuPPMDestroy, src/enzo/cuPPM.h, called from
+ * Grid_SolvePPM_DE.C:63-153).
+ *
+ * All arithmetic is FP64.  Fields keep Enzo's BaryonField layout: one array
+ * per field, x fastest, index (k*GD1 + j)*GD0 + i, ghost zones included.
+ * Subgrid fluxes keep the layout of struct fluxes (src/enzo/Fluxes.h:29-37).
+ *
+ * Plain pointers and sizes only: no C++ or CUDA types cross this boundary.
+ * Every call returns PPM_B200_OK (0) or a negative PPM_B200_ERR_* code and
+ * never exits or traps the GPU.
+ */
+#ifndef PPM_B200_H
+#define PPM_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PPM_B200_VERSION 100
+
+/* return codes */
+#define PPM_B200_OK 0
+#define PPM_B200_ERR_UNSUPPORTED (-1)  /* configuration this library does not cover: caller keeps the Fortran path */
+#define PPM_B200_ERR_INVALID (-2)      /* bad arguments (NULL field, ghost zones != 3, ...) */
+#define PPM_B200_ERR_CUDA (-3)         /* a CUDA runtime call failed */
+#define PPM_B200_ERR_NEGATIVE (-4)     /* a state the reference aborts on (flux_twoshock.F:440-443, flux_hll.F:336-383, euler.F:203-215) */
+#define PPM_B200_ERR_NONFINITE (-5)    /* non-finite output detected */
+#define PPM_B200_ERR_TOO_LARGE (-6)    /* size beyond a fixed limit of the entry point */
+
+/* memory kinds of the field pointers */
+#define PPM_B200_MEM_HOST 0   /* fields in host memory: copied in and out inside the call (like cuPPMSetBaryon/GetBaryon) */
+#define PPM_B200_MEM_DEVICE 1 /* fields already resident in device memory */
+
+/* Riemann solver / reconstruction enums, values as in Enzo's typedefs.h */
+#define PPM_B200_RIEMANN_TWOSHOCK 5
+#define PPM_B200_RECONSTRUCTION_PPM 1
+
+/* Hydro globals consumed by the sweeps (global_data.h, defaults in
+   SetDefaultGlobalValues.C).  POD, filled by the caller from the same globals
+   the Fortran path reads. */
+typedef struct ppm_b200_params {
+  double gamma;             /* Gamma */
+  double dt;                /* dtFixed of the grid */
+  double eta1, eta2;        /* DualEnergyFormalismEta1 / Eta2 */
+  double small_rho;         /* SmallRho (density floor of euler.F:141-144) */
+  double tiny_number;       /* tiny_number = MinimumPressure of the sweeps */
+  double min_support;       /* MinimumSupportEnergyCoefficient (ComputePressure) */
+  int dual_energy;          /* DualEnergyFormalism */
+  int gravity;              /* GravityOn (AccelerationField used) */
+  int pressure_free;        /* PressureFree: unsupported, must be 0 */
+  int riemann_solver;       /* RiemannSolver: PPM_B200_RIEMANN_TWOSHOCK */
+  int riemann_fallback;     /* RiemannSolverFallback */
+  int reconstruction;       /* ReconstructionMethod: PPM_B200_RECONSTRUCTION_PPM */
+  int steepening;           /* PPMSteepeningParameter: must be 0 */
+  int flattening;           /* PPMFlatteningParameter: must be 0 */
+  int diffusion;            /* PPMDiffusionParameter: must be 0 */
+  int conservative_rec;     /* ConservativeReconstruction: must be 0 */
+  int positive_rec;         /* PositiveReconstruction: must be 0 */
+  int eos_type;             /* EOSType: must be 0 */
+  int number_of_colours;    /* NumberOfColours: must be 0 */
+  int learned_guess;        /* 1: start twoshock's Newton iteration from the learned p* guess */
+  const double *dt_device;  /* optional: device pointer holding dtFixed (overrides dt) */
+  int reserved[6];
+} ppm_b200_params;
+
+/* One grid.  Field pointers are host or device memory as the call says.
+   velocity[d] may be NULL for d >= rank; gas_energy may be NULL unless
+   dual_energy; acceleration[] is read only when gravity. */
+typedef struct ppm_b200_grid {
+  int rank;                 /* GridRank */
+  int dims[3];              /* GridDimension (ghosts included) */
+  int start[3];             /* GridStartIndex (0-based) */
+  int end[3];               /* GridEndIndex (0-based, inclusive) */
+  double *density;          /* BaryonField[DensNum] */
+  double *total_energy;     /* BaryonField[TENum] */
+  double *velocity[3];      /* BaryonField[Vel1Num..Vel3Num] */
+  double *gas_energy;       /* BaryonField[GENum] */
+  const double *acceleration[3]; /* AccelerationField[dim] */
+  const double *cell_width[3];   /* CellWidthTemp[dim]: HOST arrays of dims[dim] values */
+} ppm_b200_grid;
+
+/* struct fluxes (Fluxes.h:29-37) restricted to the six hydro slots.
+   Slot order: density, total energy, velocity1, velocity2, velocity3, gas
+   energy.  Arrays are HOST memory, allocated and zeroed by the caller
+   (Grid_SolveHydroEquations.C:320-369); NULL slots are skipped. */
+typedef struct ppm_b200_fluxes {
+  long long left_start[3][3], left_end[3][3];
+  long long right_start[3][3], right_end[3][3];
+  double *left[6][3];
+  double *right[6][3];
+} ppm_b200_fluxes;
+
+typedef struct ppm_b200_stats {
+  long long interfaces;     /* Riemann problems solved */
+  long long newton_iters;   /* Newton updates performed */
+  long long newton_hist[8]; /* interfaces by Newton updates taken (1..7) */
+  long long fallbacks;      /* cells recomputed with the HLL fallback */
+  long long fatal_cells;    /* cells in a state the reference aborts on */
+  long long guess_rejected; /* learned guesses that did not converge (plain guess reused) */
+} ppm_b200_stats;
+
+typedef struct ppm_b200_context ppm_b200_context;
+
+/* Context: one per MPI rank / device (InitGPU selects rank % ngpu,
+   CUDAUtil.cu:19-31).  Owns the stream, persistent device scratch (grown on
+   demand, never reallocated per call) and device-side status counters.
+   stream may be NULL (the context creates its own non-blocking stream). */
+int ppm_b200_create(int device, void *cuda_stream, ppm_b200_context **ctx);
+int ppm_b200_destroy(ppm_b200_context *ctx);
+
+/* grid::SolvePPM_DE (Grid_SolvePPM_DE.C:36-164) for EOSType 0: pressure once,
+   then the x/y/z sweeps in the order rotated by cycle_number % rank, each over
+   every pencil including transverse ghost pencils, with subgrid flux capture.
+   memory = PPM_B200_MEM_HOST: synchronous, like the Fortran path.
+   memory = PPM_B200_MEM_DEVICE: asynchronous on the context stream when
+   nsub == 0 and stats == NULL; call ppm_b200_synchronize for the status. */
+int ppm_b200_solve_ppm_de(ppm_b200_context *ctx, const ppm_b200_params *params,
+                          int cycle_number, ppm_b200_grid *grid, int memory, int nsub,
+                          ppm_b200_fluxes *subgrid_fluxes, const long long grid_global_start[3],
+                          ppm_b200_stats *stats);
+
+/* One direction: the `for k ... xEulerSweep(k)` loop (Grid_SolvePPM_DE.C:89-97)
+   or its y (:108-116) / z (:127-136) sibling, with a caller-supplied pressure
+   field (same memory kind as the fields). */
+int ppm_b200_euler_sweep(ppm_b200_context *ctx, int dim, const ppm_b200_params *params,
+                         ppm_b200_grid *grid, const double *pressure, int memory, int nsub,
+                         ppm_b200_fluxes *subgrid_fluxes, const long long grid_global_start[3],
+                         ppm_b200_stats *stats);
+
+/* grid::ComputePressure at time == Time (Grid_ComputePressure.C:96-164). */
+int ppm_b200_compute_pressure(ppm_b200_context *ctx, const ppm_b200_params *params,
+                              ppm_b200_grid *grid, double *pressure, int memory);
+
+/* Courant time step of grid::ComputeTimeStep for PPM (Grid_ComputeTimeStep.C
+   :146-209 with calc_dt.F ihydro = 0): pressure on the fly, min over active
+   cells of aye / sum_d (c_s + |v_d - vgrid_d|)/dx_d, times courant.
+   Writes the result to *dt_device (device pointer, may be NULL) without a host
+   sync, and to *dt_host (may be NULL; synchronises). */
+int ppm_b200_compute_timestep(ppm_b200_context *ctx, const ppm_b200_params *params,
+                              ppm_b200_grid *grid, int memory, double courant, double aye,
+                              const double vgrid[3], double *dt_device, double *dt_host);
+
+/* Ghost-zone fill of one grid on device memory (periodic = 0 / outflow = 1
+   per dimension); the external-boundary part of SetBoundaryConditions for a
+   single grid (ExternalBoundary_SetExternalBoundaryIO.C:201-209, :378-386). */
+int ppm_b200_set_boundary(ppm_b200_context *ctx, ppm_b200_grid *grid, int dual_energy,
+                          const int bc_type[3]);
+
+/* Waits for all work queued on the context and returns the first error code
+   recorded by device work since the last call; accumulates device counters
+   into *stats (may be NULL). */
+int ppm_b200_synchronize(ppm_b200_context *ctx, ppm_b200_stats *stats);
+
+/* Number of kernels this library has launched on the context since creation. */
+long long ppm_b200_launch_count(ppm_b200_context *ctx);
+
+const char *ppm_b200_error_string(int code);
+int ppm_b200_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PPM_B200_H */
