@@ -1,0 +1,363 @@
+#!/usr/bin/env python
+"""Benchmark of the PPM-DE hydro hot path (zone-updates/s) on B200.
+
+Workload (one grid per GPU): decaying supersonic turbulence on a 256^3 periodic
+grid (+3 ghost zones per side), FP64, gamma = 5/3, dual-energy formalism on,
+density lognormal (sigma_ln rho = 0.5) from a seeded Gaussian random field with
+P(k) ~ k^-2, solenoidal velocity with P(k) ~ k^-4 at rms Mach 3, uniform
+pressure; seeded synthetic data generated here (no external dataset).
+
+One step = what Enzo's level-0 cycle does around the hydro call for one grid:
+Courant time step (ComputeTimeStep/calc_dt, on device), grid::SolvePPM_DE
+(pressure + x/y/z sweeps in the cycle-rotated order), ghost-zone fill
+(periodic).  With N GPUs every rank advances its own grid (weak scaling) and the
+time step is the minimum over ranks (one 8-byte NCCL all-reduce, as
+SetLevelTimeStep.C does with MPI).  A zone-update is one active cell advanced
+through one full split step.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+REPO = Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO / "enzo-dev_b200"))
+
+from ppm_b200 import harness as H  # noqa: E402
+
+METRIC = "zone-updates/s on 1 B200: batched+learned vs plain GPU PPM at 1e-10 rel; % HBM"
+UNIT = "zone-updates/s"
+# Algorithmic HBM bytes per zone-update (FP64, dual energy, no gravity, no colours):
+# ComputePressure reads rho, ge and writes p (24 B); each sweep reads rho, E, u, v, w,
+# ge, p (56 B) and writes rho, E, u, v, w, ge (48 B).
+BYTES_PER_SWEEP_CELL = 104
+BYTES_PER_ZONE_UPDATE = 24 + 3 * BYTES_PER_SWEEP_CELL
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--size", type=int, default=256, help="active cells per dimension")
+    ap.add_argument("--seed", type=int, default=20240611)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def workload_config(args):
+    return {
+        "workload": f"decaying supersonic turbulence {args.size}^3 periodic (+3 ghosts), "
+                    "Mach 3, gamma 5/3, dual energy, FP64 PPM-DE (plain two-shock guess)",
+        "grid": [args.size + 6] * 3,
+        "active_cells_per_gpu": args.size ** 3,
+        "step": "calc_dt (device) + SolvePPM_DE (pressure, 3 sweeps) + periodic ghost fill",
+        "l2": "inputs larger than L2 (13 fields x 144 MB resident per GPU)",
+        "bytes_per_zone_update": BYTES_PER_ZONE_UPDATE,
+    }
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", str(rank)))
+    return rank, world, local
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons while the timed region runs."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nme, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(nme)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak_hbm():
+    f = REPO / "MEASURED_PEAKS.json"
+    if f.exists():
+        d = json.loads(f.read_text())
+        return float(d["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    return 6650.0, "fallback 6.65 TB/s"
+
+
+def committed_traffic():
+    """Per-zone-sweep DRAM bytes of the sweep kernel from the committed ncu summary."""
+    f = REPO / "profiles" / "sweep_kernel_traffic.json"
+    if f.exists():
+        try:
+            d = json.loads(f.read_text())
+            return float(d["dram_bytes_per_cell_sweep"]), d.get("source", "")
+        except Exception:
+            return None, ""
+    return None, ""
+
+
+# ---------------------------------------------------------------- CPU reference (oracle port)
+def cpu_reference_rate(size, seed, steps, nthreads):
+    """Times the C restatement of the Fortran path (the oracle) on the host cores."""
+    sys.path.insert(0, str(REPO / "oracle"))
+    import oracle as O  # the CPU baseline leg is the one place bench.py runs the oracle
+    hp = H.HydroParams(gamma=5.0 / 3.0, cfl=0.4, dual=True)
+    g = H.Grid.uniform((size, size, size))
+    f = H.turbulence(g, hp, mach=3.0, seed=seed)
+    times = []
+    for cyc in range(steps):
+        p = O.compute_pressure(g, hp, f)
+        dt = hp.cfl * O.calc_dt(g, hp, f, p, g.cellwidth)
+        t0 = time.perf_counter()
+        rc, _ = O.solve_ppm_de(g, hp, dt, cyc, f, g.cellwidth, nthreads=nthreads)
+        times.append(time.perf_counter() - t0)
+        if rc != 0:
+            raise RuntimeError("oracle step failed")
+        H.fill_ghosts(g, f, "periodic")
+    return g.active_cells * steps / sum(times), sum(times)
+
+
+def run_reference(args):
+    rank, world, local = dist_env()
+    if rank != 0:
+        return 0
+    nthreads = os.cpu_count() or 1
+    # a bounded sample of the same workload: a 128^3 grid of the same generator
+    sample = min(args.size, 128)
+    rates = []
+    hp = H.HydroParams(gamma=5.0 / 3.0, cfl=0.4, dual=True)
+    sys.path.insert(0, str(REPO / "oracle"))
+    import oracle as O
+    g = H.Grid.uniform((sample,) * 3)
+    f = H.turbulence(g, hp, mach=3.0, seed=args.seed)
+    total = 0.0
+    for cyc in range(args.warmup + args.steps):
+        p = O.compute_pressure(g, hp, f)
+        dt = hp.cfl * O.calc_dt(g, hp, f, p, g.cellwidth)
+        t0 = time.perf_counter()
+        rc, _ = O.solve_ppm_de(g, hp, dt, cyc, f, g.cellwidth, nthreads=nthreads)
+        el = time.perf_counter() - t0
+        H.fill_ghosts(g, f, "periodic")
+        if cyc >= args.warmup:
+            total += el
+    value = g.active_cells * args.steps / total
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+        "config": dict(workload_config(args),
+                       reference_sample=f"{sample}^3 grid of the same turbulence generator"),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": nthreads, "kind": "port",
+                         "sample": f"{sample}^3 turbulence, {args.steps} SolvePPM_DE steps, "
+                                   f"OpenMP over slices, {nthreads} threads; C restatement of "
+                                   "the Fortran (no Fortran compiler on the box)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------- GPU arm
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    from ppm_b200 import capi
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+    # one explicit stream for the library's kernels, torch's copies and the timing events
+    stream = torch.cuda.Stream(device=dev)
+    torch.cuda.set_stream(stream)
+    ctx = capi.Context(local, stream=stream.cuda_stream)
+
+    hp = H.HydroParams(gamma=5.0 / 3.0, cfl=0.4, dual=True)
+    g = H.Grid.uniform((args.size,) * 3)
+    f_host = H.turbulence(g, hp, mach=3.0, seed=args.seed + rank)
+    fields = {k: torch.from_numpy(v).to(dev) for k, v in f_host.items()}
+    dt_dev = torch.zeros(1, dtype=torch.float64, device=dev)
+    periodic = ("periodic",) * 3
+
+    def step(cyc):
+        ctx.compute_timestep(g, hp, fields, memory=capi.MEM_DEVICE, dt_device=dt_dev,
+                             want_host=False)
+        if world > 1:
+            dist.all_reduce(dt_dev, op=dist.ReduceOp.MIN)
+        ctx.solve_ppm_de(g, hp, 0.0, cyc, fields, memory=capi.MEM_DEVICE, want_stats=False,
+                         dt_device=dt_dev)
+        ctx.set_boundary(g, fields, hp.dual, periodic)
+
+    cyc = 0
+    for _ in range(args.warmup):
+        step(cyc)
+        cyc += 1
+    torch.cuda.synchronize()
+    rc, st = ctx.synchronize()
+    if rc != 0:
+        raise RuntimeError(f"warm-up failed: {capi.error_string(rc)}")
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = ctx.launches()
+    ctx.profile(True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step(cyc)
+        cyc += 1
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = sampler.stop()
+    ctx.profile(False)
+    launches = ctx.launches() - launches0
+    sweep_ms, nsweep = ctx.profile_read()
+    rc, st = ctx.synchronize()
+    if rc != 0:
+        raise RuntimeError(f"timed steps failed: {capi.error_string(rc)}")
+    ms = ev0.elapsed_time(ev1)
+    if world > 1:
+        t = torch.tensor([ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    cells = g.active_cells
+    value = cells * world * args.steps / (ms * 1e-3)
+
+    # roofline of the dominant kernel (the fused sweep): algorithmic bytes per launch
+    # = 104 B x active cells, over its average event-timed duration
+    peak, peak_src = measured_peak_hbm()
+    avg_sweep_s = sweep_ms * 1e-3 / max(nsweep, 1)
+    achieved = BYTES_PER_SWEEP_CELL * cells / avg_sweep_s / 1e9
+    tr, tr_src = committed_traffic()
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": (tr * cells if tr else None),
+                "kernel": "sweep_kernel<DUAL=1,GRAV=0>", "avg_launch_ms": avg_sweep_s * 1e3,
+                "sweep_share_of_step": sweep_ms / ms, "peak_source": peak_src,
+                "traffic_source": tr_src or None}
+
+    # end to end through the public API with host buffers (pinned), copies inside the timing
+    e2e = None
+    if not args.no_e2e:
+        pinned = {k: torch.from_numpy(v).pin_memory().numpy() for k, v in f_host.items()}
+        dt_fixed = float(dt_dev.item())
+        ne = max(1, min(args.steps, 5))
+        ctx.solve_ppm_de(g, hp, dt_fixed, 0, pinned, memory=capi.MEM_HOST)  # warm
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for k in range(ne):
+            ctx.solve_ppm_de(g, hp, dt_fixed, k, pinned, memory=capi.MEM_HOST)
+        el = time.perf_counter() - t0
+        if world > 1:
+            t = torch.tensor([el], dtype=torch.float64, device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            el = float(t.item())
+        nbytes = sum(a.nbytes for a in pinned.values())
+        e2e = {"value": cells * world * ne / el, "unit": UNIT, "h2d_bytes_per_step": nbytes,
+               "d2h_bytes_per_step": nbytes, "steps": ne,
+               "api": "ppm_b200_solve_ppm_de(MEM_HOST), pinned host fields"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        nthreads = os.cpu_count() or 1
+        sample = min(args.size, 128)
+        rate, secs = cpu_reference_rate(sample, args.seed, 2, nthreads)
+        cpu = {"value": rate, "unit": UNIT, "cores": nthreads, "kind": "port",
+               "sample": f"{sample}^3 turbulence, 2 SolvePPM_DE steps, {nthreads} threads "
+                         f"({secs:.1f} s); C restatement of the Fortran path"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded turbulence generator)",
+            "config": dict(workload_config(args), parallelism=f"grid per GPU x{world}"),
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+            "clocks": clocks,
+            "newton_iters_per_interface": (st["newton_iters"] / st["interfaces"]
+                                           if st["interfaces"] else None),
+            "hll_fallbacks": st["fallbacks"],
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -59,6 +59,10 @@ struct ppm_b200_context {
   DevBuf captures;
   DevBuf capture_buf;
   std::vector<double> capture_host;
+  // event timing of sweep launches
+  bool profiling = false;
+  std::vector<cudaEvent_t> ev_pool;
+  size_t ev_used = 0;
 };
 
 namespace {
@@ -288,9 +292,21 @@ int run_sweep(ppm_b200_context* ctx, int dim, const ppm_b200_params* p, const pp
     a.capture_buf = (double*)ctx->capture_buf.p;
   }
 
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  if (ctx->profiling) {
+    while (ctx->ev_pool.size() < ctx->ev_used + 2) {
+      cudaEvent_t e;
+      CK(cudaEventCreate(&e));
+      ctx->ev_pool.push_back(e);
+    }
+    ev0 = ctx->ev_pool[ctx->ev_used++];
+    ev1 = ctx->ev_pool[ctx->ev_used++];
+    CK(cudaEventRecord(ev0, ctx->stream));
+  }
   ppm::launch_sweep(a, p->dual_energy != 0, p->gravity != 0, ctx->stream);
   ctx->launches += 1;
   CK(cudaGetLastError());
+  if (ev1) CK(cudaEventRecord(ev1, ctx->stream));
 
   if (!reqs.empty()) {
     ctx->capture_host.resize(reqs.size() * 6);
@@ -416,12 +432,35 @@ int ppm_b200_destroy(ppm_b200_context* ctx) {
   fr(ctx->misc);
   fr(ctx->captures);
   fr(ctx->capture_buf);
+  for (auto e : ctx->ev_pool) cudaEventDestroy(e);
   if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
   return PPM_B200_OK;
 }
 
 long long ppm_b200_launch_count(ppm_b200_context* ctx) { return ctx ? ctx->launches : -1; }
+
+int ppm_b200_profile(ppm_b200_context* ctx, int enable) {
+  if (!ctx) return PPM_B200_ERR_INVALID;
+  ctx->profiling = enable != 0;
+  return PPM_B200_OK;
+}
+
+int ppm_b200_profile_read(ppm_b200_context* ctx, double* sweep_ms, long long* sweep_launches) {
+  if (!ctx) return PPM_B200_ERR_INVALID;
+  CK(cudaSetDevice(ctx->device));
+  CK(cudaStreamSynchronize(ctx->stream));
+  double total = 0.0;
+  for (size_t k = 0; k + 1 < ctx->ev_used; k += 2) {
+    float ms = 0.0f;
+    CK(cudaEventElapsedTime(&ms, ctx->ev_pool[k], ctx->ev_pool[k + 1]));
+    total += ms;
+  }
+  if (sweep_ms) *sweep_ms = total;
+  if (sweep_launches) *sweep_launches = (long long)(ctx->ev_used / 2);
+  ctx->ev_used = 0;
+  return PPM_B200_OK;
+}
 
 int ppm_b200_synchronize(ppm_b200_context* ctx, ppm_b200_stats* stats) {
   if (!ctx) return PPM_B200_ERR_INVALID;

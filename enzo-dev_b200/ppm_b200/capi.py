@@ -31,7 +31,7 @@ EXPORTS = (
     "ppm_b200_create", "ppm_b200_destroy", "ppm_b200_solve_ppm_de", "ppm_b200_euler_sweep",
     "ppm_b200_compute_pressure", "ppm_b200_compute_timestep", "ppm_b200_set_boundary",
     "ppm_b200_synchronize", "ppm_b200_launch_count", "ppm_b200_error_string",
-    "ppm_b200_version",
+    "ppm_b200_version", "ppm_b200_profile", "ppm_b200_profile_read",
 )
 
 _dp = C.POINTER(C.c_double)
@@ -126,6 +126,8 @@ def lib(build_if_missing: bool = True):
     L.ppm_b200_error_string.argtypes = [C.c_int]
     L.ppm_b200_error_string.restype = C.c_char_p
     L.ppm_b200_version.argtypes = []
+    L.ppm_b200_profile.argtypes = [vp, C.c_int]
+    L.ppm_b200_profile_read.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]
     for name in EXPORTS:
         fn = getattr(L, name)
         if name not in ("ppm_b200_launch_count", "ppm_b200_error_string"):
@@ -294,6 +296,17 @@ class Context:
         rc = self.L.ppm_b200_set_boundary(self.h, C.byref(G), int(bool(dual)), codes)
         if rc != OK:
             raise PPMError(rc, "ppm_b200_set_boundary")
+
+    def profile(self, enable=True):
+        self.L.ppm_b200_profile(self.h, int(bool(enable)))
+
+    def profile_read(self):
+        ms = C.c_double(0.0)
+        n = C.c_longlong(0)
+        rc = self.L.ppm_b200_profile_read(self.h, C.byref(ms), C.byref(n))
+        if rc != OK:
+            raise PPMError(rc, "ppm_b200_profile_read")
+        return ms.value, n.value
 
     def synchronize(self):
         st = Stats()

@@ -164,6 +164,14 @@ int ppm_b200_synchronize(ppm_b200_context *ctx, ppm_b200_stats *stats);
 /* Number of kernels this library has launched on the context since creation. */
 long long ppm_b200_launch_count(ppm_b200_context *ctx);
 
+/* Kernel timing with CUDA events recorded on the context stream around every sweep
+   launch (the per-direction timers of the reference's EnzoTiming sections,
+   Grid_SolveHydroEquations.C:68 / :632, at kernel granularity).  enable = 0 stops.
+   ppm_b200_profile_read synchronises, returns the summed sweep-kernel time in ms
+   and the number of timed sweep launches since the last read, and resets them. */
+int ppm_b200_profile(ppm_b200_context *ctx, int enable);
+int ppm_b200_profile_read(ppm_b200_context *ctx, double *sweep_ms, long long *sweep_launches);
+
 const char *ppm_b200_error_string(int code);
 int ppm_b200_version(void);
 
