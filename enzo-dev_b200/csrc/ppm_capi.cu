@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <cstdint>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -14,7 +15,7 @@
 
 // launchers defined in ppm_kernels.cu
 namespace ppm {
-void launch_sweep(const SweepArgs& a, bool dual, bool grav, cudaStream_t st);
+void launch_sweep_split(const SweepArgs& a, bool dual, bool grav, cudaStream_t st);
 void launch_pressure_plain(const double* d, const double* te, const double* v1, const double* v2,
                            const double* v3, const double* ge, double* p, int64_t size,
                            double gamma, double tiny_number, double min_support, int sms,
@@ -59,6 +60,7 @@ struct ppm_b200_context {
   DevBuf captures;
   DevBuf capture_buf;
   std::vector<double> capture_host;
+  DevBuf face_scratch;      // interface states and fluxes of the three-stage sweep
   // event timing of sweep launches
   bool profiling = false;
   std::vector<cudaEvent_t> ev_pool;
@@ -303,8 +305,14 @@ int run_sweep(ppm_b200_context* ctx, int dim, const ppm_b200_params* p, const pp
     ev1 = ctx->ev_pool[ctx->ev_used++];
     CK(cudaEventRecord(ev0, ctx->stream));
   }
-  ppm::launch_sweep(a, p->dual_energy != 0, p->gravity != 0, ctx->stream);
-  ctx->launches += 1;
+  a.plane = (int64_t)(a.ie - a.is + 2) * a.npencils;
+  const size_t need = (size_t)(ppm::kFaceVars + ppm::kFluxVars) * (size_t)a.plane * sizeof(double);
+  rc = ensure(ctx, ctx->face_scratch, need);
+  if (rc) return rc;
+  a.fstate = (double*)ctx->face_scratch.p;
+  a.fflux = a.fstate + (size_t)ppm::kFaceVars * (size_t)a.plane;
+  ppm::launch_sweep_split(a, p->dual_energy != 0, p->gravity != 0, ctx->stream);
+  ctx->launches += 3;
   CK(cudaGetLastError());
   if (ev1) CK(cudaEventRecord(ev1, ctx->stream));
 
@@ -401,6 +409,7 @@ int ppm_b200_create(int device, void* cuda_stream, ppm_b200_context** out) {
     }
     ctx->own_stream = true;
   }
+
   int rc = ensure(ctx, ctx->counters, ppm::kMaxCounters * sizeof(unsigned long long));
   if (!rc) rc = ensure(ctx, ctx->misc, 4 * sizeof(double));
   if (!rc) rc = cuda_fail(ctx, cudaMemset(ctx->counters.p, 0, ctx->counters.bytes), "cudaMemset");
@@ -432,6 +441,7 @@ int ppm_b200_destroy(ppm_b200_context* ctx) {
   fr(ctx->misc);
   fr(ctx->captures);
   fr(ctx->capture_buf);
+  fr(ctx->face_scratch);
   for (auto e : ctx->ev_pool) cudaEventDestroy(e);
   if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;

@@ -1,0 +1,499 @@
+// ppm_split.cu -- one directional sweep as three sm_100a kernels sharing a face scratch.
+//
+//   reconstruct_kernel  (thread per pencil, marching)  inteuler + intvar: the 12 corrected
+//                       interface states of every face -> fstate
+//   riemann_kernel      (thread per face)               twoshock + flux_twoshock -> fflux
+//   update_kernel       (thread per pencil, marching)  flux_twoshock's negative-state check
+//                       with the per-cell flux_hll fallback, euler, pgas2d_dual
+//
+// Splitting the chain at the interface states keeps each kernel's live state small.
+// The Riemann stage -- a divergent Newton iteration with a serial chain of divides and
+// square roots per face -- runs face-parallel at full occupancy instead of inside a
+// register-heavy marching pipeline.  The two marching stages keep the reference's
+// sequential semantics along a pencil: the fallback of cell i rewrites faces i and
+// i+1 before cell i+1 is checked and before cell i-1 is updated, and pgas2d_dual
+// reads its already-updated left neighbour.
+// Scratch planes are laid out face-major with the pencil index fastest, so every
+// warp's scratch accesses are contiguous.
+#include <cuda_runtime.h>
+
+#include "ppm_device.cuh"
+#include "ppm_sweep.cuh"
+
+namespace ppm {
+namespace split {
+
+enum { VD = 0, VP = 1, VU = 2, VV = 3, VW = 4, VGE = 5 };
+enum { SDL = 0, SDR, SPL, SPR, SUL, SUR, SVL, SVR, SWL, SWR, SGEL, SGER };
+enum { XDF = 0, XEF, XUF, XVF, XWF, XGEF, XUB };
+
+__device__ __forceinline__ double ldg0(const double* __restrict__ p, int64_t off) {
+  return p ? __ldg(p + off) : 0.0;
+}
+
+__device__ __forceinline__ Phys make_phys(const SweepArgs& a) {
+  Phys P;
+  P.gamma = a.gamma;
+  P.dt = a.dt_device ? *a.dt_device : a.dt;
+  P.eta1 = a.eta1;
+  P.eta2 = a.eta2;
+  P.small_rho = a.small_rho;
+  P.pmin = a.pmin;
+  P.qa = (a.gamma + 1.0) / (2.0 * a.gamma);
+  P.gp1 = a.gamma + 1.0;
+  P.gm1 = a.gamma - 1.0;
+  return P;
+}
+
+template <bool DUAL>
+__device__ __forceinline__ Lside make_left(const Para (&pa)[6], const Prep& pr) {
+  Lside L;
+  L.dla = pm_A(pa[VD], pr.char1);
+  L.dl0 = pm_A(pa[VD], pr.c0);
+  L.pla = pm_A(pa[VP], pr.char1);
+  L.pl0 = pm_A(pa[VP], pr.c0);
+  L.plm = pm_A(pa[VP], pr.cm);
+  L.plp = pm_A(pa[VP], pr.cp);
+  L.ula = pm_A(pa[VU], pr.char1);
+  L.ul0 = pm_A(pa[VU], pr.c0);
+  L.ulm = pm_A(pa[VU], pr.cm);
+  L.ulp = pm_A(pa[VU], pr.cp);
+  L.vla = pm_A(pa[VV], pr.char1);
+  L.vl0 = pm_A(pa[VV], pr.c0);
+  L.wla = pm_A(pa[VW], pr.char1);
+  L.wl0 = pm_A(pa[VW], pr.c0);
+  L.gela = DUAL ? pm_A(pa[VGE], pr.char1) : 0.0;
+  L.gel0 = DUAL ? pm_A(pa[VGE], pr.c0) : 0.0;
+  L.cm = pr.cm;
+  L.c0 = pr.c0;
+  L.cp = pr.cp;
+  return L;
+}
+
+template <bool DUAL>
+__device__ __forceinline__ Rside make_right(const Para (&pa)[6], const Prep& pr) {
+  Rside R;
+  R.dra = pm_C(pa[VD], pr.char2);
+  R.dr0 = pm_B(pa[VD], pr.c0);
+  R.pra = pm_C(pa[VP], pr.char2);
+  R.pr0 = pm_B(pa[VP], pr.c0);
+  R.prm = pm_B(pa[VP], pr.cm);
+  R.prp = pm_B(pa[VP], pr.cp);
+  R.ura = pm_C(pa[VU], pr.char2);
+  R.ur0 = pm_B(pa[VU], pr.c0);
+  R.urm = pm_B(pa[VU], pr.cm);
+  R.urp = pm_B(pa[VU], pr.cp);
+  R.vra = pm_C(pa[VV], pr.char2);
+  R.vr0 = pm_B(pa[VV], pr.c0);
+  R.wra = pm_C(pa[VW], pr.char2);
+  R.wr0 = pm_B(pa[VW], pr.c0);
+  R.gera = DUAL ? pm_C(pa[VGE], pr.char2) : 0.0;
+  R.ger0 = DUAL ? pm_B(pa[VGE], pr.c0) : 0.0;
+  R.cm = pr.cm;
+  R.c0 = pr.c0;
+  R.cp = pr.cp;
+  return R;
+}
+
+// ------------------------------------------------------------------ stage 1
+template <bool DUAL, bool GRAV>
+__global__ void __launch_bounds__(128) reconstruct_kernel(const __grid_constant__ SweepArgs a) {
+  constexpr int NV = DUAL ? 6 : 5;
+  const int64_t pid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (pid >= a.npencils) return;
+  const Phys P = make_phys(a);
+  const int64_t base = (pid % a.n1) * a.s1 + (pid / a.n1) * a.s2;
+  const int64_t sa = a.sa;
+  const int is = a.is, ie = a.ie;
+  const int64_t np = a.npencils, plane = a.plane;
+
+  double wq0[6], wq1[6], wq2[6];  // cells t-3, t-2, t-1
+  double dqm1[6], qlm1[6];        // dq(t-2), ql(t-2)
+#pragma unroll
+  for (int v = 0; v < 6; ++v) wq0[v] = wq1[v] = wq2[v] = dqm1[v] = qlm1[v] = 0.0;
+  double wg0 = 0.0, wg1 = 0.0, wg2 = 0.0;
+  Prep prA = {0, 0, 0, 0, 0}, prB = {0, 0, 0, 0, 0};  // cells t-2, t-1
+  Lside Lp = {};                                      // left data of face t-2
+
+  const int tend = ie + 3;  // the last face, ie+1, is assembled at t = ie+3
+#pragma unroll 1
+  for (int t = 0; t <= tend; ++t) {
+    double nq[6];
+    const int64_t off = base + (int64_t)t * sa;
+    nq[VD] = __ldg(a.in_d + off);
+    nq[VP] = __ldg(a.pres + off);
+    nq[VU] = ldg0(a.in_u, off);
+    nq[VV] = ldg0(a.in_v, off);
+    nq[VW] = ldg0(a.in_w, off);
+    nq[VGE] = DUAL ? __ldg(a.in_ge + off) : 0.0;
+    const double ng = GRAV ? __ldg(a.grav + off) : 0.0;
+    // characteristic distances of cell t (inteuler.F:197-208)
+    Prep prC = prB;
+    if (t >= is - 1 && t <= ie + 1) prC = cell_prep(nq[VD], nq[VP], nq[VU], a.coef[t].dx2i, P);
+    // slope and left edge of cell t-1 (intvar.F:82-102)
+    double dqN[6], qlN[6];
+#pragma unroll
+    for (int v = 0; v < 6; ++v) dqN[v] = qlN[v] = 0.0;
+    {
+      const int c = t - 1;
+      if (c >= is - 2 && c <= ie + 2) {
+        const Coef cf = a.coef[c];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) dqN[v] = pm_slope(wq1[v], wq2[v], nq[v], cf.c1, cf.c2);
+        if (c >= is - 1) {
+#pragma unroll
+          for (int v = 0; v < NV; ++v)
+            qlN[v] = pm_edge(wq1[v], wq2[v], dqm1[v], dqN[v], cf.c3, cf.c4, cf.c5, cf.c6);
+        }
+      }
+    }
+    // parabola of cell t-2, its face contributions, and face t-2 (inteuler.F:304-551)
+    Lside Ln = Lp;
+    {
+      const int c = t - 2;
+      if (c >= is - 1 && c <= ie + 1) {
+        Para pa[6];
+#pragma unroll
+        for (int v = 0; v < 6; ++v) pa[v] = Para{0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+        for (int v = 0; v < NV; ++v) pa[v] = pm_parabola(wq0[v], wq1[v], wq2[v], qlm1[v], qlN[v]);
+        if (c >= is) {
+          const Rside Rc = make_right<DUAL>(pa, prA);
+          const double gsum = GRAV ? (wg0 + wg1) : 0.0;
+          const FaceState s = face_assemble<DUAL, GRAV>(Lp, Rc, wq0[VU], wq1[VU], gsum, P);
+          double* o = a.fstate + (int64_t)(c - is) * np + pid;
+          o[SDL * plane] = s.dl;
+          o[SDR * plane] = s.dr;
+          o[SPL * plane] = s.pl;
+          o[SPR * plane] = s.pr;
+          o[SUL * plane] = s.ul;
+          o[SUR * plane] = s.ur;
+          o[SVL * plane] = s.vl;
+          o[SVR * plane] = s.vr;
+          o[SWL * plane] = s.wl;
+          o[SWR * plane] = s.wr;
+          if (DUAL) {
+            o[SGEL * plane] = s.gel;
+            o[SGER * plane] = s.ger;
+          }
+        }
+        if (c <= ie) Ln = make_left<DUAL>(pa, prA);
+      }
+    }
+#pragma unroll
+    for (int v = 0; v < 6; ++v) {
+      wq0[v] = wq1[v];
+      wq1[v] = wq2[v];
+      wq2[v] = nq[v];
+      dqm1[v] = dqN[v];
+      qlm1[v] = qlN[v];
+    }
+    wg0 = wg1;
+    wg1 = wg2;
+    wg2 = ng;
+    prA = prB;
+    prB = prC;
+    Lp = Ln;
+  }
+}
+
+template <bool DUAL>
+__device__ __forceinline__ FaceState load_face(const SweepArgs& a, int64_t idx) {
+  const double* s = a.fstate + idx;
+  const int64_t pl = a.plane;
+  FaceState f;
+  f.dl = s[SDL * pl];
+  f.dr = s[SDR * pl];
+  f.pl = s[SPL * pl];
+  f.pr = s[SPR * pl];
+  f.ul = s[SUL * pl];
+  f.ur = s[SUR * pl];
+  f.vl = s[SVL * pl];
+  f.vr = s[SVR * pl];
+  f.wl = s[SWL * pl];
+  f.wr = s[SWR * pl];
+  f.gel = DUAL ? s[SGEL * pl] : 0.0;
+  f.ger = DUAL ? s[SGER * pl] : 0.0;
+  return f;
+}
+
+// ------------------------------------------------------------------ stage 2
+// grid: x over pencils, y over faces (fi = face - is)
+template <bool DUAL>
+__global__ void __launch_bounds__(256) riemann_kernel(const __grid_constant__ SweepArgs a) {
+  __shared__ unsigned int s_hist[8];
+  __shared__ unsigned int s_newton;
+  if (threadIdx.x < 8) s_hist[threadIdx.x] = 0u;
+  if (threadIdx.x == 0) s_newton = 0u;
+  __syncthreads();
+  const int64_t pid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int fi = blockIdx.y;
+  if (pid < a.npencils) {
+    const Phys P = make_phys(a);
+    const int64_t idx = (int64_t)fi * a.npencils + pid;
+    const FaceState s = load_face<DUAL>(a, idx);
+    const double cl = sqrt(P.gamma * s.pl * s.dl);
+    const double cr = sqrt(P.gamma * s.pr * s.dr);
+    const double ps = acoustic_guess(s, cl, cr, P);
+    const Riemann rs = twoshock_newton(s, cl, cr, ps, P);
+    const double qc = P.dt / a.coef[a.is + fi].dx;
+    const Flux F = flux_twoshock<DUAL>(s, rs.pbar, rs.ubar, qc, P);
+    double* o = a.fflux + idx;
+    const int64_t pl = a.plane;
+    o[XDF * pl] = F.df;
+    o[XEF * pl] = F.ef;
+    o[XUF * pl] = F.uf;
+    o[XVF * pl] = F.vf;
+    o[XWF * pl] = F.wf;
+    if (DUAL) o[XGEF * pl] = F.gef;
+    o[XUB * pl] = F.ub;
+    atomicAdd(&s_hist[rs.iters & 7], 1u);
+    atomicAdd(&s_newton, (unsigned)rs.iters);
+  }
+  __syncthreads();
+  if (threadIdx.x < 8 && s_hist[threadIdx.x])
+    atomicAdd(&a.counters[kCntHist0 + threadIdx.x], (unsigned long long)s_hist[threadIdx.x]);
+  if (threadIdx.x == 8 && s_newton) {
+    unsigned long long nif = 0;
+    for (int h = 0; h < 8; ++h) nif += s_hist[h];
+    atomicAdd(&a.counters[kCntInterfaces], nif);
+    atomicAdd(&a.counters[kCntNewton], (unsigned long long)s_newton);
+  }
+}
+
+__device__ __forceinline__ Flux load_flux(const SweepArgs& a, int64_t idx) {
+  const double* s = a.fflux + idx;
+  const int64_t pl = a.plane;
+  Flux f;
+  f.df = s[XDF * pl];
+  f.ef = s[XEF * pl];
+  f.uf = s[XUF * pl];
+  f.vf = s[XVF * pl];
+  f.wf = s[XWF * pl];
+  f.gef = s[XGEF * pl];
+  f.ub = s[XUB * pl];
+  return f;
+}
+
+template <bool DUAL>
+__device__ __forceinline__ Cell load_cell(const SweepArgs& a, int64_t off) {
+  Cell c;
+  c.d = __ldg(a.in_d + off);
+  c.e = __ldg(a.in_e + off);
+  c.u = ldg0(a.in_u, off);
+  c.v = ldg0(a.in_v, off);
+  c.w = ldg0(a.in_w, off);
+  c.ge = DUAL ? __ldg(a.in_ge + off) : 0.0;
+  return c;
+}
+
+// flux_hll for cell c (flux_hll.F with i1 = i2 = c): replaces the fluxes of faces c and
+// c+1 and returns ges(c); ges(c+1), which the single-cell call leaves to its unset
+// locals at index c+2, is defined from the HLL state of face c+2 when that face exists.
+template <bool DUAL>
+__device__ __noinline__ void hll_fallback(const SweepArgs& a, int64_t pid, int64_t base, int c,
+                                          const Cell& cell, const Phys& P, Flux& F0, Flux& F1,
+                                          double& ges_c, double& ges_c1, bool& fatal) {
+  const int is = a.is, ie = a.ie;
+  const int64_t np = a.npencils;
+  const FaceState s0 = load_face<DUAL>(a, (int64_t)(c - is) * np + pid);
+  const FaceState s1 = load_face<DUAL>(a, (int64_t)(c + 1 - is) * np + pid);
+  const HllFace h0 = hll_face<DUAL>(s0, P);
+  const HllFace h1 = hll_face<DUAL>(s1, P);
+  HllFace h2 = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+  if (c + 2 <= ie + 1) h2 = hll_face<DUAL>(load_face<DUAL>(a, (int64_t)(c + 2 - is) * np + pid), P);
+  const double qcc = P.dt / a.coef[c].dx;
+  const double qc1 = P.dt / a.coef[c + 1].dx;
+  if (DUAL) {
+    const int64_t off1 = base + (int64_t)(c + 1) * a.sa;
+    const double pc0 = dmax(P.gm1 * cell.ge * cell.d, kTiny);
+    const double pc1 = dmax(P.gm1 * __ldg(a.in_ge + off1) * __ldg(a.in_d + off1), kTiny);
+    ges_c = qcc * pc0 * (h0.sl * h0.gesl + h0.sr * h0.gesr - h1.sl * h1.gesl - h1.sr * h1.gesr);
+    ges_c1 = qc1 * pc1 * (h1.sl * h1.gesl + h1.sr * h1.gesr - h2.sl * h2.gesl - h2.sr * h2.gesr);
+  }
+  F0.df = qcc * h0.df;
+  F0.uf = qcc * h0.uf;
+  F0.vf = qcc * h0.vf;
+  F0.wf = qcc * h0.wf;
+  F0.ef = qcc * h0.ef;
+  F0.gef = DUAL ? P.dt / a.coef[c].dx * h0.gef : 0.0;
+  F1.df = qc1 * h1.df;
+  F1.uf = qc1 * h1.uf;
+  F1.vf = qc1 * h1.vf;
+  F1.wf = qc1 * h1.wf;
+  F1.ef = qc1 * h1.ef;
+  F1.gef = DUAL ? P.dt / a.coef[c + 1].dx * h1.gef : 0.0;
+  if (cell.d + F0.df - F1.df <= 0.0) fatal = true;  // flux_hll.F:336-383
+}
+
+// ------------------------------------------------------------------ stage 3
+// Marching order per step t: (1) check cell t (flux_twoshock.F:401-456) and apply its
+// fallback, which may rewrite faces t and t+1; face t is then final; (2) conservative
+// update of cell t-1 from faces t-1 and t (euler.F); (3) dual-energy select of cell
+// t-2 (pgas2d_dual.F, which needs the post-euler state of t-1) and store.  This is
+// the reference's order: all checks and fallbacks of a pencil precede its update, and
+// a fallback of cell i changes the right face of cell i-1.
+template <bool DUAL, bool GRAV>
+__global__ void __launch_bounds__(128) update_kernel(const __grid_constant__ SweepArgs a) {
+  __shared__ unsigned long long s_cnt[4];
+  if (threadIdx.x < 4) s_cnt[threadIdx.x] = 0ull;
+  __syncthreads();
+  const int64_t pid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (pid < a.npencils) {
+    const Phys P = make_phys(a);
+    const int64_t base = (pid % a.n1) * a.s1 + (pid / a.n1) * a.s2;
+    const int64_t sa = a.sa, np = a.npencils;
+    const int n = a.n, is = a.is, ie = a.ie;
+
+    int64_t cap = 0, cap_end = 0;
+    if (a.ncaptures > 0) {
+      int64_t lo = 0, hi = a.ncaptures;
+      while (lo < hi) {
+        int64_t mid = (lo + hi) >> 1;
+        if (a.captures[mid].pencil < pid) lo = mid + 1; else hi = mid;
+      }
+      cap = cap_end = lo;
+      while (cap_end < a.ncaptures && a.captures[cap_end].pencil == pid) ++cap_end;
+    }
+
+    Flux Fm = {0, 0, 0, 0, 0, 0, 0};  // final flux at face t-1
+    Flux F0 = load_flux(a, pid);      // flux at face t (face is at t = is)
+    Cell Cm = {0, 0, 0, 0, 0, 0};     // input state of cell t-1
+    double ges_m = 0.0;               // final ges of cell t-1
+    bool gov = false;                 // ges(t) was set by the fallback of cell t-1
+    double govv = 0.0;
+    Cell PEm = {0, 0, 0, 0, 0, 0};    // post-euler state of cell t-2
+    double dep = 0.0;                 // post-pgas d*e of cell t-3
+    unsigned int c_fb = 0, c_fatal = 0, c_nonfin = 0;
+
+#pragma unroll 1
+    for (int t = 0; t <= n; ++t) {
+      Cell Cn = Cm;
+      double ges_n = 0.0;
+      Flux F1 = F0;
+      bool gov_next = false;
+      double govv_next = 0.0;
+      // (1) check of cell t
+      if (t < n) {
+        const int64_t off = base + (int64_t)t * sa;
+        Cn = load_cell<DUAL>(a, off);
+        if (t >= is && t <= ie) {
+          F1 = load_flux(a, (int64_t)(t + 1 - is) * np + pid);
+          if (DUAL) {
+            const double pcent = dmax(P.gm1 * Cn.ge * Cn.d, kTiny);
+            ges_n = gov ? govv : P.dt / a.coef[t].dx * pcent * (F0.ub - F1.ub);
+          }
+          if (Cn.d + (F0.df - F1.df) <= 0.0 || Cn.e < 0.0) {
+            if (a.fallback == 0) {
+              c_fatal += 1;
+            } else {
+              bool fatal = false;
+              c_fb += 1;
+              hll_fallback<DUAL>(a, pid, base, t, Cn, P, F0, F1, ges_n, govv_next, fatal);
+              gov_next = DUAL;
+              if (fatal) c_fatal += 1;
+            }
+          }
+          // subgrid flux capture: faces t (and ie+1 after the last check) are final
+          while (cap < cap_end && a.captures[cap].face <= t + (t == ie ? 1 : 0)) {
+            const FluxCapture& rq = a.captures[cap];
+            const Flux& F = (rq.face == t) ? F0 : F1;
+            double* dst = a.capture_buf + rq.dst;
+            dst[0] = F.df; dst[1] = F.ef; dst[2] = F.uf;
+            dst[3] = F.vf; dst[4] = F.wf; dst[5] = DUAL ? F.gef : 0.0;
+            ++cap;
+          }
+        }
+      }
+      // (2) conservative update of cell t-1
+      Cell PEn = Cm;
+      {
+        const int c = t - 1;
+        if (c >= is && c <= ie) {
+          bool fatal = false;
+          PEn = euler_update<DUAL, GRAV>(Cm, Fm, F0, ges_m,
+                                         GRAV ? __ldg(a.grav + base + (int64_t)c * sa) : 0.0, P,
+                                         fatal);
+          if (fatal) c_fatal += 1;
+        }
+      }
+      // (3) dual-energy select of cell t-2 and store
+      {
+        const int c = t - 2;
+        if (c >= 0) {
+          Cell o = PEm;
+          if (DUAL) {
+            const double own = o.d * o.e;
+            const double de_m = (c == 0) ? own : dep;
+            const double de_p = (c == n - 1) ? own : PEn.d * PEn.e;
+            pgas2d_dual(o, de_m, de_p, P);
+            dep = o.d * o.e;
+          }
+          if (!isfinite(o.d) || !isfinite(o.e)) c_nonfin += 1;
+          const int64_t off = base + (int64_t)c * sa;
+          a.out_d[off] = o.d;
+          a.out_e[off] = o.e;
+          if (a.out_u) a.out_u[off] = o.u;
+          if (a.out_v) a.out_v[off] = o.v;
+          if (a.out_w) a.out_w[off] = o.w;
+          if (DUAL) a.out_ge[off] = o.ge;
+        }
+      }
+      Fm = F0;
+      F0 = F1;
+      Cm = Cn;
+      ges_m = ges_n;
+      gov = gov_next;
+      govv = govv_next;
+      PEm = PEn;
+    }
+    // the loop's last step (t = n) leaves cell n-1 unstored; it is a ghost cell, whose
+    // post-euler state is its input, selected against itself and its left neighbour
+    {
+      const int c = n - 1;
+      Cell o = PEm;
+      if (DUAL) {
+        const double own = o.d * o.e;
+        pgas2d_dual(o, (c == 0) ? own : dep, own, P);
+      }
+      if (!isfinite(o.d) || !isfinite(o.e)) c_nonfin += 1;
+      const int64_t off = base + (int64_t)c * sa;
+      a.out_d[off] = o.d;
+      a.out_e[off] = o.e;
+      if (a.out_u) a.out_u[off] = o.u;
+      if (a.out_v) a.out_v[off] = o.v;
+      if (a.out_w) a.out_w[off] = o.w;
+      if (DUAL) a.out_ge[off] = o.ge;
+    }
+    if (c_fb) atomicAdd(&s_cnt[0], (unsigned long long)c_fb);
+    if (c_fatal) atomicAdd(&s_cnt[1], (unsigned long long)c_fatal);
+    if (c_nonfin) atomicAdd(&s_cnt[2], (unsigned long long)c_nonfin);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    if (s_cnt[0]) atomicAdd(&a.counters[kCntFallbacks], s_cnt[0]);
+    if (s_cnt[1]) atomicAdd(&a.counters[kCntFatal], s_cnt[1]);
+    if (s_cnt[2]) atomicAdd(&a.counters[kCntNonFinite], s_cnt[2]);
+  }
+}
+
+template <bool DUAL, bool GRAV>
+void launch3(const SweepArgs& a, cudaStream_t st) {
+  const unsigned b1 = (unsigned)((a.npencils + 127) / 128);
+  reconstruct_kernel<DUAL, GRAV><<<b1, 128, 0, st>>>(a);
+  dim3 g2((unsigned)((a.npencils + 255) / 256), (unsigned)(a.ie - a.is + 2));
+  riemann_kernel<DUAL><<<g2, 256, 0, st>>>(a);
+  update_kernel<DUAL, GRAV><<<b1, 128, 0, st>>>(a);
+}
+
+}  // namespace split
+
+// Three launches; the caller provides a.fstate / a.fflux / a.plane.
+void launch_sweep_split(const SweepArgs& a, bool dual, bool grav, cudaStream_t st) {
+  if (dual && grav) split::launch3<true, true>(a, st);
+  else if (dual) split::launch3<true, false>(a, st);
+  else if (grav) split::launch3<false, true>(a, st);
+  else split::launch3<false, false>(a, st);
+}
+
+}  // namespace ppm

@@ -66,6 +66,13 @@ struct SweepArgs {
   const FluxCapture* captures;       // sorted by pencil
   int64_t ncaptures;
   double* capture_buf;               // 6 doubles per request: df, ef, uf, vf, wf, gef
+  // face scratch of the three-stage sweep: plane v holds one value per (face, pencil),
+  // element fi * npencils + pencil with fi = face - is in [0, ie - is + 1]
+  double* fstate;                    // kFaceVars planes: dl dr pl pr ul ur vl vr wl wr gel ger
+  double* fflux;                     // kFluxVars planes: df ef uf vf wf gef ub
+  int64_t plane;                     // elements per plane = (ie - is + 2) * npencils
 };
+
+enum { kFaceVars = 12, kFluxVars = 7 };
 
 }  // namespace ppm

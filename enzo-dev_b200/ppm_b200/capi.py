@@ -9,6 +9,7 @@ The library is required: there is no CPU fallback on this path.
 from __future__ import annotations
 
 import ctypes as C
+import os
 from pathlib import Path
 
 import numpy as np
@@ -92,7 +93,9 @@ _lib = None
 
 
 def library_path() -> Path:
-    return _build.LIB
+    """libppm_b200.so to load: $PPM_B200_LIB when set, else the in-tree build."""
+    env = os.environ.get("PPM_B200_LIB")
+    return Path(env) if env else _build.LIB
 
 
 def lib(build_if_missing: bool = True):
@@ -100,11 +103,12 @@ def lib(build_if_missing: bool = True):
     global _lib
     if _lib is not None:
         return _lib
-    if not _build.LIB.exists():
-        if not build_if_missing:
-            raise RuntimeError(f"{_build.LIB} is missing; run python -m ppm_b200.build")
+    path = library_path()
+    if not path.exists():
+        if not build_if_missing or path != _build.LIB:
+            raise RuntimeError(f"{path} is missing; run python -m ppm_b200.build")
         _build.build()
-    L = C.CDLL(str(_build.LIB))
+    L = C.CDLL(str(path))
     vp = C.c_void_p
     L.ppm_b200_create.argtypes = [C.c_int, vp, C.POINTER(vp)]
     L.ppm_b200_destroy.argtypes = [vp]
