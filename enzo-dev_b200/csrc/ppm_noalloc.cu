@@ -1,0 +1,235 @@
+// ppm_noalloc.cu -- ppm_b200_euler_sweep_static: one directional sweep that allocates
+// nothing.
+//
+// Some callers cannot allocate device memory at the moment they want to advance a
+// grid: code that runs under a memory pool or arena that owns all device memory and
+// forbids further cudaMalloc calls, code inside a callback where allocating could
+// synchronise the device or deadlock, or embedded drivers that reserve all memory up
+// front.  Such a caller still provides its own input and output arrays; this entry
+// point takes the sweep's scratch (the interface-state and flux planes, the inteuler
+// coefficient table and the status counters) from a fixed array compiled into the
+// library instead of from cudaMalloc.
+//
+// Properties a caller must know:
+//  * Limit: the face planes fit kStaticPlaneBytes (48 MiB), i.e.
+//    19 * 8 * (active cells along the sweep + 1) * (pencils) bytes; this covers grids
+//    up to 64^3 active cells (70^3 with ghosts) in every direction.  Larger grids and
+//    pencils longer than 1031 cells are rejected with PPM_B200_ERR_TOO_LARGE before
+//    any device work.
+//  * Every GPU that loads the library holds the array (about 48.1 MiB) until the
+//    process exits.
+//  * Set-up: the first call on a device, with that device current, looks up the
+//    array's device address (cudaGetSymbolAddress).  Make that first call before any
+//    stream capture.
+//  * The array is shared by every call on a device and keeps the last call's
+//    contents.  Calls that overlap on the GPU (different streams, or different host
+//    threads) race on it; serialise them.
+//  * The call is synchronous: it waits for its own stream to read the status.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "ppm_b200.h"
+#include "ppm_sweep.cuh"
+
+namespace ppm {
+void launch_sweep_split(const SweepArgs& a, bool dual, bool grav, cudaStream_t st);
+}
+
+namespace {
+
+constexpr size_t kStaticCounterBytes = 256;                       // kMaxCounters counters
+constexpr int kStaticCoefEntries = 1031;                          // longest pencil (fortran.def:1)
+constexpr size_t kStaticCoefBytes = 66560;                        // >= 1031 * sizeof(Coef), 256-aligned
+constexpr size_t kStaticPlaneBytes = size_t(48) << 20;            // interface states + fluxes
+constexpr size_t kStaticBytes = kStaticCounterBytes + kStaticCoefBytes + kStaticPlaneBytes;
+static_assert(kStaticCoefEntries * sizeof(ppm::Coef) <= kStaticCoefBytes, "coef area");
+
+constexpr int kMaxDevices = 64;
+
+struct DeviceSlot {
+  bool ready = false;
+  unsigned char* base = nullptr;
+};
+DeviceSlot g_slots[kMaxDevices];
+std::mutex g_setup_mutex;
+
+}  // namespace
+
+// The scratch itself.  Host code must not use this name as an address: it is a
+// host-side stand-in for the device array; the device address comes from
+// cudaGetSymbolAddress below.
+static __device__ __align__(256) unsigned char g_sweep_scratch[kStaticBytes];
+
+namespace {
+
+// Once per device, with that device current: look up the array's device address.
+int static_setup(int device, unsigned char** base) {
+  if (device < 0 || device >= kMaxDevices) return PPM_B200_ERR_INVALID;
+  std::lock_guard<std::mutex> lock(g_setup_mutex);
+  DeviceSlot& s = g_slots[device];
+  if (!s.ready) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_sweep_scratch);
+    if (e != cudaSuccess || p == nullptr) {
+      fprintf(stderr, "ppm_b200: cudaGetSymbolAddress failed: %s\n", cudaGetErrorString(e));
+      return PPM_B200_ERR_CUDA;
+    }
+    s.base = static_cast<unsigned char*>(p);
+    s.ready = true;
+  }
+  *base = s.base;
+  return PPM_B200_OK;
+}
+
+// inteuler.F:140-158 on the host (same expressions as the context path).
+void coef_table(const double* dxi_in, int n, int is0, int ie0, std::vector<ppm::Coef>& out) {
+  out.assign(n, ppm::Coef{0, 0, 0, 0, 0, 0, 0, 0});
+  auto dxi = [&](int i) { return dxi_in[i - 1]; };
+  const int i1 = is0 + 1, i2 = ie0 + 1;
+  for (int i = 1; i <= n; ++i) out[i - 1].dx = dxi(i);
+  for (int i = i1 - 2; i <= i2 + 2; i++) {
+    double qa = dxi(i) / (dxi(i - 1) + dxi(i) + dxi(i + 1));
+    out[i - 1].c1 = qa * (2.0 * dxi(i - 1) + dxi(i)) / (dxi(i + 1) + dxi(i));
+    out[i - 1].c2 = qa * (2.0 * dxi(i + 1) + dxi(i)) / (dxi(i - 1) + dxi(i));
+  }
+  for (int i = i1 - 1; i <= i2 + 2; i++) {
+    double qa = dxi(i - 2) + dxi(i - 1) + dxi(i) + dxi(i + 1);
+    double qb = dxi(i - 1) / (dxi(i - 1) + dxi(i));
+    double qc = (dxi(i - 2) + dxi(i - 1)) / (2.0 * dxi(i - 1) + dxi(i));
+    double qd = (dxi(i + 1) + dxi(i)) / (2.0 * dxi(i) + dxi(i - 1));
+    qb = qb + 2.0 * dxi(i) * qb / qa * (qc - qd);
+    out[i - 1].c3 = 1.0 - qb;
+    out[i - 1].c4 = qb;
+    out[i - 1].c5 = dxi(i) / qa * qd;
+    out[i - 1].c6 = -(dxi(i - 1) / qa * qc);
+    out[i - 1].dx2i = 0.5 / dxi(i);
+  }
+}
+
+int fail_cuda(cudaError_t e, const char* what) {
+  fprintf(stderr, "ppm_b200: %s failed: %s\n", what, cudaGetErrorString(e));
+  return PPM_B200_ERR_CUDA;
+}
+
+}  // namespace
+
+extern "C" int ppm_b200_euler_sweep_static(int dim, const ppm_b200_params* p,
+                                           const ppm_b200_grid* in, const double* pressure,
+                                           ppm_b200_grid* out, void* cuda_stream,
+                                           ppm_b200_stats* stats) {
+  // ---- argument checks (no device work yet)
+  if (!p || !in || !out || !pressure || dim < 0 || dim > 2) return PPM_B200_ERR_INVALID;
+  if (p->pressure_free || p->steepening || p->flattening || p->diffusion || p->conservative_rec ||
+      p->positive_rec || p->eos_type != 0 || p->number_of_colours != 0 || p->learned_guess ||
+      p->riemann_solver != PPM_B200_RIEMANN_TWOSHOCK ||
+      p->reconstruction != PPM_B200_RECONSTRUCTION_PPM)
+    return PPM_B200_ERR_UNSUPPORTED;
+  if (in->rank < 1 || in->rank > 3 || dim >= in->rank) return PPM_B200_ERR_INVALID;
+  for (int d = 0; d < 3; ++d)
+    if (out->dims[d] != in->dims[d] || (d >= in->rank && in->dims[d] != 1))
+      return PPM_B200_ERR_INVALID;
+  if (in->start[dim] != 3 || in->dims[dim] - 1 - in->end[dim] != 3 || !in->cell_width[dim])
+    return PPM_B200_ERR_INVALID;
+  if (!in->density || !in->total_energy || !in->velocity[0] || !out->density ||
+      !out->total_energy || !out->velocity[0])
+    return PPM_B200_ERR_INVALID;
+  for (int d = 1; d < in->rank; ++d)
+    if (!in->velocity[d] || !out->velocity[d]) return PPM_B200_ERR_INVALID;
+  if (p->dual_energy && (!in->gas_energy || !out->gas_energy)) return PPM_B200_ERR_INVALID;
+  if (p->gravity && !in->acceleration[dim]) return PPM_B200_ERR_INVALID;
+
+  const int GD0 = in->dims[0], GD1 = in->dims[1], GD2 = in->dims[2];
+  ppm::SweepArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.n = in->dims[dim];
+  a.is = in->start[dim];
+  a.ie = in->end[dim];
+  if (dim == 0) {
+    a.n1 = GD1; a.n2 = GD2; a.s1 = GD0; a.s2 = (int64_t)GD0 * GD1; a.sa = 1;
+  } else if (dim == 1) {
+    a.n1 = GD0; a.n2 = GD2; a.s1 = 1; a.s2 = (int64_t)GD0 * GD1; a.sa = GD0;
+  } else {
+    a.n1 = GD0; a.n2 = GD1; a.s1 = 1; a.s2 = GD0; a.sa = (int64_t)GD0 * GD1;
+  }
+  a.npencils = (int64_t)a.n1 * a.n2;
+  a.plane = (int64_t)(a.ie - a.is + 2) * a.npencils;
+  const size_t plane_bytes =
+      (size_t)(ppm::kFaceVars + ppm::kFluxVars) * (size_t)a.plane * sizeof(double);
+  if (a.n > kStaticCoefEntries || plane_bytes > kStaticPlaneBytes) return PPM_B200_ERR_TOO_LARGE;
+
+  // ---- set-up of this device (first call only), with the caller's device current
+  int device = 0;
+  cudaError_t e = cudaGetDevice(&device);
+  if (e != cudaSuccess) return fail_cuda(e, "cudaGetDevice");
+  unsigned char* base = nullptr;
+  int rc = static_setup(device, &base);
+  if (rc) return rc;
+  unsigned long long* counters = reinterpret_cast<unsigned long long*>(base);
+  ppm::Coef* coef = reinterpret_cast<ppm::Coef*>(base + kStaticCounterBytes);
+  double* planes = reinterpret_cast<double*>(base + kStaticCounterBytes + kStaticCoefBytes);
+  cudaStream_t st = static_cast<cudaStream_t>(cuda_stream);
+
+  // ---- per-call contents: counters start at zero, the coefficient table is rewritten
+  e = cudaMemsetAsync(counters, 0, kStaticCounterBytes, st);
+  if (e != cudaSuccess) return fail_cuda(e, "cudaMemsetAsync");
+  std::vector<ppm::Coef> table;
+  coef_table(in->cell_width[dim], a.n, a.is, a.ie, table);
+  e = cudaMemcpyAsync(coef, table.data(), table.size() * sizeof(ppm::Coef),
+                      cudaMemcpyHostToDevice, st);
+  if (e != cudaSuccess) return fail_cuda(e, "cudaMemcpyAsync");
+
+  const int vu = dim, vv = (dim + 1) % 3, vw = (dim + 2) % 3;
+  auto vin = [&](int c) -> const double* { return c < in->rank ? in->velocity[c] : nullptr; };
+  auto vout = [&](int c) -> double* { return c < in->rank ? out->velocity[c] : nullptr; };
+  a.in_d = in->density;
+  a.in_e = in->total_energy;
+  a.in_u = vin(vu);
+  a.in_v = vin(vv);
+  a.in_w = vin(vw);
+  a.in_ge = p->dual_energy ? in->gas_energy : nullptr;
+  a.out_d = out->density;
+  a.out_e = out->total_energy;
+  a.out_u = vout(vu);
+  a.out_v = vout(vv);
+  a.out_w = vout(vw);
+  a.out_ge = p->dual_energy ? out->gas_energy : nullptr;
+  a.pres = pressure;
+  a.grav = p->gravity ? in->acceleration[dim] : nullptr;
+  a.coef = coef;
+  a.gamma = p->gamma;
+  a.dt = p->dt;
+  a.dt_device = p->dt_device;
+  a.eta1 = p->eta1;
+  a.eta2 = p->eta2;
+  a.small_rho = p->small_rho;
+  a.pmin = p->tiny_number;
+  a.fallback = p->riemann_fallback;
+  a.counters = counters;
+  a.fstate = planes;
+  a.fflux = planes + (size_t)ppm::kFaceVars * (size_t)a.plane;
+  ppm::launch_sweep_split(a, p->dual_energy != 0, p->gravity != 0, st);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return fail_cuda(e, "sweep launch");
+
+  // ---- status
+  unsigned long long c[ppm::kMaxCounters];
+  e = cudaMemcpyAsync(c, counters, sizeof(c), cudaMemcpyDeviceToHost, st);
+  if (e != cudaSuccess) return fail_cuda(e, "cudaMemcpyAsync");
+  e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return fail_cuda(e, "cudaStreamSynchronize");
+  if (stats) {
+    stats->interfaces += (long long)c[ppm::kCntInterfaces];
+    stats->newton_iters += (long long)c[ppm::kCntNewton];
+    for (int h = 0; h < 8; ++h) stats->newton_hist[h] += (long long)c[ppm::kCntHist0 + h];
+    stats->fallbacks += (long long)c[ppm::kCntFallbacks];
+    stats->fatal_cells += (long long)c[ppm::kCntFatal];
+  }
+  if (c[ppm::kCntFatal]) return PPM_B200_ERR_NEGATIVE;
+  if (c[ppm::kCntNonFinite]) return PPM_B200_ERR_NONFINITE;
+  return PPM_B200_OK;
+}

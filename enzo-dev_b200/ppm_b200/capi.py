@@ -33,6 +33,7 @@ EXPORTS = (
     "ppm_b200_compute_pressure", "ppm_b200_compute_timestep", "ppm_b200_set_boundary",
     "ppm_b200_synchronize", "ppm_b200_launch_count", "ppm_b200_error_string",
     "ppm_b200_version", "ppm_b200_profile", "ppm_b200_profile_read",
+    "ppm_b200_euler_sweep_static",
 )
 
 _dp = C.POINTER(C.c_double)
@@ -130,6 +131,8 @@ def lib(build_if_missing: bool = True):
     L.ppm_b200_error_string.argtypes = [C.c_int]
     L.ppm_b200_error_string.restype = C.c_char_p
     L.ppm_b200_version.argtypes = []
+    L.ppm_b200_euler_sweep_static.argtypes = [C.c_int, C.POINTER(Params), C.POINTER(GridDesc),
+                                              vp, C.POINTER(GridDesc), vp, C.POINTER(Stats)]
     L.ppm_b200_profile.argtypes = [vp, C.c_int]
     L.ppm_b200_profile_read.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]
     for name in EXPORTS:
@@ -215,6 +218,25 @@ def make_fluxes(box):
                 a = box[side][s][d]
                 arr[s][d] = _addr(a) if a is not None else None
     return F
+
+
+def euler_sweep_static(dim, grid, hp, dt, fields_in, pressure, fields_out, stream=None,
+                       accel=None):
+    """ppm_b200_euler_sweep_static: one sweep with no device allocation.
+
+    For callers that cannot allocate device memory when they advance a grid (a
+    memory arena owns the device, or the call happens where an allocation could
+    synchronise).  fields_in / fields_out / pressure are device tensors owned by the
+    caller; the sweep's scratch is a fixed array inside the library (grids up to
+    64^3 active cells).  Returns (rc, stats dict); no exception on a nonzero rc."""
+    L = lib()
+    P = make_params(hp, dt)
+    Gi, keep_i = make_grid(grid, fields_in, accel)
+    Go, keep_o = make_grid(grid, fields_out)
+    st = Stats()
+    rc = L.ppm_b200_euler_sweep_static(int(dim), C.byref(P), C.byref(Gi), _addr(pressure),
+                                       C.byref(Go), stream, C.byref(st))
+    return rc, st.as_dict()
 
 
 class Context:

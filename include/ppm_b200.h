@@ -172,6 +172,22 @@ long long ppm_b200_launch_count(ppm_b200_context *ctx);
 int ppm_b200_profile(ppm_b200_context *ctx, int enable);
 int ppm_b200_profile_read(ppm_b200_context *ctx, double *sweep_ms, long long *sweep_launches);
 
+/* One directional sweep that allocates nothing (no counterpart in the reference).
+   For callers that cannot call cudaMalloc when they advance a grid -- code running
+   under a memory arena that owns all device memory, or inside a callback where an
+   allocation could synchronise or deadlock.  `in` and `out` are caller-owned DEVICE
+   arrays (out must not alias in; cell widths stay host arrays), `pressure` a device
+   array; the sweep's scratch comes from a fixed array compiled into the library.
+   Limit: 19 * 8 * (active cells along dim + 1) * pencils bytes <= 48 MiB (grids up
+   to 64^3 active cells) and pencils of at most 1031 cells; larger sizes return
+   PPM_B200_ERR_TOO_LARGE.  The first call on a device (which must be current) looks
+   up the array's address; make it before any stream capture.  The array is shared
+   by all calls on a device: calls that overlap on the GPU race.  Synchronous on
+   cuda_stream (NULL = default stream); no subgrid flux capture. */
+int ppm_b200_euler_sweep_static(int dim, const ppm_b200_params *params,
+                                const ppm_b200_grid *in, const double *pressure,
+                                ppm_b200_grid *out, void *cuda_stream, ppm_b200_stats *stats);
+
 const char *ppm_b200_error_string(int code);
 int ppm_b200_version(void);
 
