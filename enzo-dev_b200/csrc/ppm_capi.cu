@@ -306,13 +306,15 @@ int run_sweep(ppm_b200_context* ctx, int dim, const ppm_b200_params* p, const pp
     CK(cudaEventRecord(ev0, ctx->stream));
   }
   a.plane = (int64_t)(a.ie - a.is + 2) * a.npencils;
-  const size_t need = (size_t)(ppm::kFaceVars + ppm::kFluxVars) * (size_t)a.plane * sizeof(double);
+  const size_t planes = (size_t)(ppm::kFaceVars + ppm::kFluxVars) * (size_t)a.plane;
+  const size_t need = planes * sizeof(double) + (size_t)a.npencils * sizeof(int64_t);
   rc = ensure(ctx, ctx->face_scratch, need);
   if (rc) return rc;
   a.fstate = (double*)ctx->face_scratch.p;
   a.fflux = a.fstate + (size_t)ppm::kFaceVars * (size_t)a.plane;
+  a.flagged = (int64_t*)(a.fstate + planes);
   ppm::launch_sweep_split(a, p->dual_energy != 0, p->gravity != 0, ctx->stream);
-  ctx->launches += 3;
+  ctx->launches += 4;
   CK(cudaGetLastError());
   if (ev1) CK(cudaEventRecord(ev1, ctx->stream));
 

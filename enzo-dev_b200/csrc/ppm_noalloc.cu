@@ -12,7 +12,7 @@
 //
 // Properties a caller must know:
 //  * Limit: the face planes fit kStaticPlaneBytes (48 MiB), i.e.
-//    19 * 8 * (active cells along the sweep + 1) * (pencils) bytes; this covers grids
+//    (19 * 8 * (active cells along the sweep + 1) + 8) * (pencils) bytes; this covers grids
 //    up to 64^3 active cells (70^3 with ghosts) in every direction.  Larger grids and
 //    pencils longer than 1031 cells are rejected with PPM_B200_ERR_TOO_LARGE before
 //    any device work.
@@ -159,7 +159,8 @@ extern "C" int ppm_b200_euler_sweep_static(int dim, const ppm_b200_params* p,
   a.npencils = (int64_t)a.n1 * a.n2;
   a.plane = (int64_t)(a.ie - a.is + 2) * a.npencils;
   const size_t plane_bytes =
-      (size_t)(ppm::kFaceVars + ppm::kFluxVars) * (size_t)a.plane * sizeof(double);
+      (size_t)(ppm::kFaceVars + ppm::kFluxVars) * (size_t)a.plane * sizeof(double) +
+      (size_t)a.npencils * sizeof(int64_t);
   if (a.n > kStaticCoefEntries || plane_bytes > kStaticPlaneBytes) return PPM_B200_ERR_TOO_LARGE;
 
   // ---- set-up of this device (first call only), with the caller's device current
@@ -212,6 +213,8 @@ extern "C" int ppm_b200_euler_sweep_static(int dim, const ppm_b200_params* p,
   a.counters = counters;
   a.fstate = planes;
   a.fflux = planes + (size_t)ppm::kFaceVars * (size_t)a.plane;
+  a.flagged = reinterpret_cast<int64_t*>(planes + (size_t)(ppm::kFaceVars + ppm::kFluxVars) *
+                                                      (size_t)a.plane);
   ppm::launch_sweep_split(a, p->dual_energy != 0, p->gravity != 0, st);
   e = cudaGetLastError();
   if (e != cudaSuccess) return fail_cuda(e, "sweep launch");

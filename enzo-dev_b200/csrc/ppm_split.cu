@@ -333,162 +333,211 @@ __device__ __noinline__ void hll_fallback(const SweepArgs& a, int64_t pid, int64
 // t-2 (pgas2d_dual.F, which needs the post-euler state of t-1) and store.  This is
 // the reference's order: all checks and fallbacks of a pencil precede its update, and
 // a fallback of cell i changes the right face of cell i-1.
+//
+// FALLBACK = false is the hot pass: it stops at the first cell that fails its check
+// and flags the pencil; FALLBACK = true re-runs flagged pencils with the per-cell HLL
+// fallback.  Sweeps are out of place, so the re-run reads untouched inputs and
+// rewrites every output (and subgrid-flux capture) of the pencil.
+struct UpdateCounts {
+  unsigned int fallbacks, fatal, nonfinite;
+};
+
+template <bool DUAL, bool GRAV, bool FALLBACK>
+__device__ __forceinline__ bool update_pencil(const SweepArgs& a, int64_t pid, const Phys& P,
+                                              UpdateCounts& cnt) {
+  const int64_t base = (pid % a.n1) * a.s1 + (pid / a.n1) * a.s2;
+  const int64_t sa = a.sa, np = a.npencils;
+  const int n = a.n, is = a.is, ie = a.ie;
+
+  int64_t cap = 0, cap_end = 0;
+  if (a.ncaptures > 0) {
+    int64_t lo = 0, hi = a.ncaptures;
+    while (lo < hi) {
+      int64_t mid = (lo + hi) >> 1;
+      if (a.captures[mid].pencil < pid) lo = mid + 1; else hi = mid;
+    }
+    cap = cap_end = lo;
+    while (cap_end < a.ncaptures && a.captures[cap_end].pencil == pid) ++cap_end;
+  }
+
+  Flux Fm = {0, 0, 0, 0, 0, 0, 0};  // final flux at face t-1
+  Flux F0 = load_flux(a, pid);      // flux at face t (face is while t <= is)
+  Cell Cm = {0, 0, 0, 0, 0, 0};     // input state of cell t-1
+  double ges_m = 0.0;               // final ges of cell t-1
+  bool gov = false;                 // ges(t) was set by the fallback of cell t-1
+  double govv = 0.0;
+  Cell PEm = {0, 0, 0, 0, 0, 0};    // post-euler state of cell t-2
+  double dep = 0.0;                 // post-pgas d*e of cell t-3
+  unsigned int nonfin = 0;
+  // one-step prefetch of cell t and face t+1
+  Cell Cpf = load_cell<DUAL>(a, base);
+  Flux Fpf = (0 >= is && 0 <= ie) ? load_flux(a, (int64_t)(1 - is) * np + pid) : F0;
+
+#pragma unroll 1
+  for (int t = 0; t <= n; ++t) {
+    Cell Cn = Cm;
+    double ges_n = 0.0;
+    Flux F1 = F0;
+    bool gov_next = false;
+    double govv_next = 0.0;
+    // (1) check of cell t
+    if (t < n) {
+      Cn = Cpf;
+      if (t >= is && t <= ie) F1 = Fpf;
+      if (t + 1 < n) {
+        Cpf = load_cell<DUAL>(a, base + (int64_t)(t + 1) * sa);
+        if (t + 1 >= is && t + 1 <= ie) Fpf = load_flux(a, (int64_t)(t + 2 - is) * np + pid);
+      }
+      if (t >= is && t <= ie) {
+        if (DUAL) {
+          const double pcent = dmax(P.gm1 * Cn.ge * Cn.d, kTiny);
+          ges_n = gov ? govv : P.dt / a.coef[t].dx * pcent * (F0.ub - F1.ub);
+        }
+        if (Cn.d + (F0.df - F1.df) <= 0.0 || Cn.e < 0.0) {
+          if (!FALLBACK) return true;  // hand the pencil to the fallback pass
+          if (a.fallback == 0) {
+            cnt.fatal += 1;
+          } else {
+            bool fatal = false;
+            cnt.fallbacks += 1;
+            hll_fallback<DUAL>(a, pid, base, t, Cn, P, F0, F1, ges_n, govv_next, fatal);
+            gov_next = DUAL;
+            if (fatal) cnt.fatal += 1;
+          }
+        }
+        // subgrid flux capture: faces t (and ie+1 after the last check) are final
+        while (cap < cap_end && a.captures[cap].face <= t + (t == ie ? 1 : 0)) {
+          const FluxCapture& rq = a.captures[cap];
+          const Flux& F = (rq.face == t) ? F0 : F1;
+          double* dst = a.capture_buf + rq.dst;
+          dst[0] = F.df; dst[1] = F.ef; dst[2] = F.uf;
+          dst[3] = F.vf; dst[4] = F.wf; dst[5] = DUAL ? F.gef : 0.0;
+          ++cap;
+        }
+      }
+    }
+    // (2) conservative update of cell t-1
+    Cell PEn = Cm;
+    {
+      const int c = t - 1;
+      if (c >= is && c <= ie) {
+        bool fatal = false;
+        PEn = euler_update<DUAL, GRAV>(Cm, Fm, F0, ges_m,
+                                       GRAV ? __ldg(a.grav + base + (int64_t)c * sa) : 0.0, P,
+                                       fatal);
+        if (fatal) cnt.fatal += 1;
+      }
+    }
+    // (3) dual-energy select of cell t-2 and store
+    {
+      const int c = t - 2;
+      if (c >= 0) {
+        Cell o = PEm;
+        if (DUAL) {
+          const double own = o.d * o.e;
+          const double de_m = (c == 0) ? own : dep;
+          const double de_p = (c == n - 1) ? own : PEn.d * PEn.e;
+          pgas2d_dual(o, de_m, de_p, P);
+          dep = o.d * o.e;
+        }
+        if (!isfinite(o.d) || !isfinite(o.e)) nonfin += 1;
+        const int64_t off = base + (int64_t)c * sa;
+        a.out_d[off] = o.d;
+        a.out_e[off] = o.e;
+        if (a.out_u) a.out_u[off] = o.u;
+        if (a.out_v) a.out_v[off] = o.v;
+        if (a.out_w) a.out_w[off] = o.w;
+        if (DUAL) a.out_ge[off] = o.ge;
+      }
+    }
+    Fm = F0;
+    F0 = F1;
+    Cm = Cn;
+    ges_m = ges_n;
+    gov = gov_next;
+    govv = govv_next;
+    PEm = PEn;
+  }
+  // the last step (t = n) leaves cell n-1 unstored; it is a ghost cell, whose
+  // post-euler state is its input, selected against itself and its left neighbour
+  {
+    const int c = n - 1;
+    Cell o = PEm;
+    if (DUAL) {
+      const double own = o.d * o.e;
+      pgas2d_dual(o, (c == 0) ? own : dep, own, P);
+    }
+    if (!isfinite(o.d) || !isfinite(o.e)) nonfin += 1;
+    const int64_t off = base + (int64_t)c * sa;
+    a.out_d[off] = o.d;
+    a.out_e[off] = o.e;
+    if (a.out_u) a.out_u[off] = o.u;
+    if (a.out_v) a.out_v[off] = o.v;
+    if (a.out_w) a.out_w[off] = o.w;
+    if (DUAL) a.out_ge[off] = o.ge;
+  }
+  cnt.nonfinite += nonfin;
+  return false;
+}
+
+#ifndef PPM_UPDATE_MINBLOCKS
+#define PPM_UPDATE_MINBLOCKS 3
+#endif
+
 template <bool DUAL, bool GRAV>
-__global__ void __launch_bounds__(128) update_kernel(const __grid_constant__ SweepArgs a) {
-  __shared__ unsigned long long s_cnt[4];
-  if (threadIdx.x < 4) s_cnt[threadIdx.x] = 0ull;
+__global__ void __launch_bounds__(128, PPM_UPDATE_MINBLOCKS)
+    update_kernel(const __grid_constant__ SweepArgs a) {
+  __shared__ unsigned long long s_cnt[2];
+  if (threadIdx.x < 2) s_cnt[threadIdx.x] = 0ull;
   __syncthreads();
   const int64_t pid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (pid < a.npencils) {
     const Phys P = make_phys(a);
-    const int64_t base = (pid % a.n1) * a.s1 + (pid / a.n1) * a.s2;
-    const int64_t sa = a.sa, np = a.npencils;
-    const int n = a.n, is = a.is, ie = a.ie;
-
-    int64_t cap = 0, cap_end = 0;
-    if (a.ncaptures > 0) {
-      int64_t lo = 0, hi = a.ncaptures;
-      while (lo < hi) {
-        int64_t mid = (lo + hi) >> 1;
-        if (a.captures[mid].pencil < pid) lo = mid + 1; else hi = mid;
-      }
-      cap = cap_end = lo;
-      while (cap_end < a.ncaptures && a.captures[cap_end].pencil == pid) ++cap_end;
+    UpdateCounts cnt = {0, 0, 0};
+    if (update_pencil<DUAL, GRAV, false>(a, pid, P, cnt)) {
+      const unsigned long long slot = atomicAdd(&a.counters[kCntFlagged], 1ull);
+      a.flagged[slot] = pid;
+    } else {
+      if (cnt.fatal) atomicAdd(&s_cnt[0], (unsigned long long)cnt.fatal);
+      if (cnt.nonfinite) atomicAdd(&s_cnt[1], (unsigned long long)cnt.nonfinite);
     }
-
-    Flux Fm = {0, 0, 0, 0, 0, 0, 0};  // final flux at face t-1
-    Flux F0 = load_flux(a, pid);      // flux at face t (face is at t = is)
-    Cell Cm = {0, 0, 0, 0, 0, 0};     // input state of cell t-1
-    double ges_m = 0.0;               // final ges of cell t-1
-    bool gov = false;                 // ges(t) was set by the fallback of cell t-1
-    double govv = 0.0;
-    Cell PEm = {0, 0, 0, 0, 0, 0};    // post-euler state of cell t-2
-    double dep = 0.0;                 // post-pgas d*e of cell t-3
-    unsigned int c_fb = 0, c_fatal = 0, c_nonfin = 0;
-
-#pragma unroll 1
-    for (int t = 0; t <= n; ++t) {
-      Cell Cn = Cm;
-      double ges_n = 0.0;
-      Flux F1 = F0;
-      bool gov_next = false;
-      double govv_next = 0.0;
-      // (1) check of cell t
-      if (t < n) {
-        const int64_t off = base + (int64_t)t * sa;
-        Cn = load_cell<DUAL>(a, off);
-        if (t >= is && t <= ie) {
-          F1 = load_flux(a, (int64_t)(t + 1 - is) * np + pid);
-          if (DUAL) {
-            const double pcent = dmax(P.gm1 * Cn.ge * Cn.d, kTiny);
-            ges_n = gov ? govv : P.dt / a.coef[t].dx * pcent * (F0.ub - F1.ub);
-          }
-          if (Cn.d + (F0.df - F1.df) <= 0.0 || Cn.e < 0.0) {
-            if (a.fallback == 0) {
-              c_fatal += 1;
-            } else {
-              bool fatal = false;
-              c_fb += 1;
-              hll_fallback<DUAL>(a, pid, base, t, Cn, P, F0, F1, ges_n, govv_next, fatal);
-              gov_next = DUAL;
-              if (fatal) c_fatal += 1;
-            }
-          }
-          // subgrid flux capture: faces t (and ie+1 after the last check) are final
-          while (cap < cap_end && a.captures[cap].face <= t + (t == ie ? 1 : 0)) {
-            const FluxCapture& rq = a.captures[cap];
-            const Flux& F = (rq.face == t) ? F0 : F1;
-            double* dst = a.capture_buf + rq.dst;
-            dst[0] = F.df; dst[1] = F.ef; dst[2] = F.uf;
-            dst[3] = F.vf; dst[4] = F.wf; dst[5] = DUAL ? F.gef : 0.0;
-            ++cap;
-          }
-        }
-      }
-      // (2) conservative update of cell t-1
-      Cell PEn = Cm;
-      {
-        const int c = t - 1;
-        if (c >= is && c <= ie) {
-          bool fatal = false;
-          PEn = euler_update<DUAL, GRAV>(Cm, Fm, F0, ges_m,
-                                         GRAV ? __ldg(a.grav + base + (int64_t)c * sa) : 0.0, P,
-                                         fatal);
-          if (fatal) c_fatal += 1;
-        }
-      }
-      // (3) dual-energy select of cell t-2 and store
-      {
-        const int c = t - 2;
-        if (c >= 0) {
-          Cell o = PEm;
-          if (DUAL) {
-            const double own = o.d * o.e;
-            const double de_m = (c == 0) ? own : dep;
-            const double de_p = (c == n - 1) ? own : PEn.d * PEn.e;
-            pgas2d_dual(o, de_m, de_p, P);
-            dep = o.d * o.e;
-          }
-          if (!isfinite(o.d) || !isfinite(o.e)) c_nonfin += 1;
-          const int64_t off = base + (int64_t)c * sa;
-          a.out_d[off] = o.d;
-          a.out_e[off] = o.e;
-          if (a.out_u) a.out_u[off] = o.u;
-          if (a.out_v) a.out_v[off] = o.v;
-          if (a.out_w) a.out_w[off] = o.w;
-          if (DUAL) a.out_ge[off] = o.ge;
-        }
-      }
-      Fm = F0;
-      F0 = F1;
-      Cm = Cn;
-      ges_m = ges_n;
-      gov = gov_next;
-      govv = govv_next;
-      PEm = PEn;
-    }
-    // the loop's last step (t = n) leaves cell n-1 unstored; it is a ghost cell, whose
-    // post-euler state is its input, selected against itself and its left neighbour
-    {
-      const int c = n - 1;
-      Cell o = PEm;
-      if (DUAL) {
-        const double own = o.d * o.e;
-        pgas2d_dual(o, (c == 0) ? own : dep, own, P);
-      }
-      if (!isfinite(o.d) || !isfinite(o.e)) c_nonfin += 1;
-      const int64_t off = base + (int64_t)c * sa;
-      a.out_d[off] = o.d;
-      a.out_e[off] = o.e;
-      if (a.out_u) a.out_u[off] = o.u;
-      if (a.out_v) a.out_v[off] = o.v;
-      if (a.out_w) a.out_w[off] = o.w;
-      if (DUAL) a.out_ge[off] = o.ge;
-    }
-    if (c_fb) atomicAdd(&s_cnt[0], (unsigned long long)c_fb);
-    if (c_fatal) atomicAdd(&s_cnt[1], (unsigned long long)c_fatal);
-    if (c_nonfin) atomicAdd(&s_cnt[2], (unsigned long long)c_nonfin);
   }
   __syncthreads();
   if (threadIdx.x == 0) {
-    if (s_cnt[0]) atomicAdd(&a.counters[kCntFallbacks], s_cnt[0]);
-    if (s_cnt[1]) atomicAdd(&a.counters[kCntFatal], s_cnt[1]);
-    if (s_cnt[2]) atomicAdd(&a.counters[kCntNonFinite], s_cnt[2]);
+    if (s_cnt[0]) atomicAdd(&a.counters[kCntFatal], s_cnt[0]);
+    if (s_cnt[1]) atomicAdd(&a.counters[kCntNonFinite], s_cnt[1]);
+  }
+}
+
+// The fallback pass: a fixed grid that walks the list of flagged pencils.
+template <bool DUAL, bool GRAV>
+__global__ void __launch_bounds__(128) fallback_kernel(const __grid_constant__ SweepArgs a) {
+  const unsigned long long nflag = *(volatile unsigned long long*)&a.counters[kCntFlagged];
+  const Phys P = make_phys(a);
+  for (unsigned long long k = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+       k < nflag; k += (unsigned long long)gridDim.x * blockDim.x) {
+    UpdateCounts cnt = {0, 0, 0};
+    update_pencil<DUAL, GRAV, true>(a, a.flagged[k], P, cnt);
+    if (cnt.fallbacks) atomicAdd(&a.counters[kCntFallbacks], (unsigned long long)cnt.fallbacks);
+    if (cnt.fatal) atomicAdd(&a.counters[kCntFatal], (unsigned long long)cnt.fatal);
+    if (cnt.nonfinite) atomicAdd(&a.counters[kCntNonFinite], (unsigned long long)cnt.nonfinite);
   }
 }
 
 template <bool DUAL, bool GRAV>
 void launch3(const SweepArgs& a, cudaStream_t st) {
   const unsigned b1 = (unsigned)((a.npencils + 127) / 128);
+  cudaMemsetAsync(a.counters + kCntFlagged, 0, sizeof(unsigned long long), st);
   reconstruct_kernel<DUAL, GRAV><<<b1, 128, 0, st>>>(a);
   dim3 g2((unsigned)((a.npencils + 255) / 256), (unsigned)(a.ie - a.is + 2));
   riemann_kernel<DUAL><<<g2, 256, 0, st>>>(a);
   update_kernel<DUAL, GRAV><<<b1, 128, 0, st>>>(a);
+  fallback_kernel<DUAL, GRAV><<<64, 128, 0, st>>>(a);
 }
 
 }  // namespace split
 
-// Three launches; the caller provides a.fstate / a.fflux / a.plane.
+// Four launches; the caller provides a.fstate / a.fflux / a.plane / a.flagged.
 void launch_sweep_split(const SweepArgs& a, bool dual, bool grav, cudaStream_t st) {
   if (dual && grav) split::launch3<true, true>(a, st);
   else if (dual) split::launch3<true, false>(a, st);

@@ -30,6 +30,7 @@ enum {
   kCntFatal = 11,
   kCntGuessRejected = 12,
   kCntNonFinite = 13,
+  kCntFlagged = 14,  // pencils handed to the fallback pass (index into SweepArgs::flagged)
 };
 
 struct SweepArgs {
@@ -71,6 +72,7 @@ struct SweepArgs {
   double* fstate;                    // kFaceVars planes: dl dr pl pr ul ur vl vr wl wr gel ger
   double* fflux;                     // kFluxVars planes: df ef uf vf wf gef ub
   int64_t plane;                     // elements per plane = (ie - is + 2) * npencils
+  int64_t* flagged;                  // npencils slots: pencils needing the fallback pass
 };
 
 enum { kFaceVars = 12, kFluxVars = 7 };
