@@ -314,7 +314,7 @@ int run_sweep(ppm_b200_context* ctx, int dim, const ppm_b200_params* p, const pp
   a.fflux = a.fstate + (size_t)ppm::kFaceVars * (size_t)a.plane;
   a.flagged = (int64_t*)(a.fstate + planes);
   ppm::launch_sweep_split(a, p->dual_energy != 0, p->gravity != 0, ctx->stream);
-  ctx->launches += 4;
+  ctx->launches += 5;
   CK(cudaGetLastError());
   if (ev1) CK(cudaEventRecord(ev1, ctx->stream));
 

@@ -105,29 +105,40 @@ __device__ __forceinline__ double pm_C(const Para& a, double x) {
   return a.ql + x * (a.dq + (1.0 - kFt * x) * a.q6);
 }
 
-// What a face needs from the cell on its left / right.
-struct Lside {
-  double dla, dl0, pla, pl0, plm, plp, ula, ul0, ulm, ulp, vla, vl0, wla, wl0, gela, gel0;
-  double cm, c0, cp;
-};
-struct Rside {
-  double dra, dr0, pra, pr0, prm, prp, ura, ur0, urm, urp, vra, vr0, wra, wr0, gera, ger0;
-  double cm, c0, cp;
-};
-
 struct FaceState {
   double dl, dr, pl, pr, ul, ur, vl, vr, wl, wr, gel, ger;
 };
 
 // ------------------------------------------------------- inteuler.F:320-551 for one face
-// gsum = grslice(i-1) + grslice(i) (only read when GRAV); ul_cell/ur_cell = uslice(i-1)/(i)
+// The corrected states of one face split into two independent groups: density,
+// pressure and normal velocity (characteristic corrections, dual-energy override,
+// floors) and the advected transverse velocities and gas energy (upwind selection).
+struct CoreL {
+  double dla, dl0, pla, pl0, plm, plp, ula, ul0, ulm, ulp, cm, c0, cp;
+};
+struct CoreR {
+  double dra, dr0, pra, pr0, prm, prp, ura, ur0, urm, urp, cm, c0, cp;
+};
+struct CoreState {
+  double dl, dr, pl, pr, ul, ur;
+};
+struct AdvL {
+  double vla, vl0, wla, wl0, gela, gel0;
+};
+struct AdvR {
+  double vra, vr0, wra, wr0, gera, ger0;
+};
+struct AdvState {
+  double vl, vr, wl, wr, gel, ger;
+};
+
+// inteuler.F:320-410, 493-551 (d, p, u); gsum = grslice(i-1) + grslice(i) (GRAV only)
 template <bool DUAL, bool GRAV>
-__device__ __forceinline__ FaceState face_assemble(const Lside& L, const Rside& R, double ul_cell,
-                                                   double ur_cell, double gsum, const Phys& P) {
-  FaceState s;
+__device__ __forceinline__ CoreState face_core(const CoreL& L, const CoreR& R, double gsum,
+                                               const Phys& P) {
+  CoreState s;
   double cla = sqrt(dmax(P.gamma * L.pla * L.dla, 0.0));
   double cra = sqrt(dmax(P.gamma * R.pra * R.dra, 0.0));
-  // a) left side
   double f1 = 1.0 / cla;
   double betalp = (L.ula - L.ulp) + (L.pla - L.plp) * f1;
   double betalm = (L.ula - L.ulm) - (L.pla - L.plm) * f1;
@@ -144,7 +155,6 @@ __device__ __forceinline__ FaceState face_assemble(const Lside& L, const Rside& 
   if (L.cp <= 0.0) betalp = 0.0;
   if (L.cm <= 0.0) betalm = 0.0;
   if (L.c0 <= 0.0) betal0 = 0.0;
-  // b) right side
   f1 = 1.0 / cra;
   double betarp = (R.ura - R.urp) + (R.pra - R.prp) * f1;
   double betarm = (R.ura - R.urm) - (R.pra - R.prm) * f1;
@@ -159,25 +169,12 @@ __device__ __forceinline__ FaceState face_assemble(const Lside& L, const Rside& 
   if (R.cp >= 0.0) betarp = 0.0;
   if (R.cm >= 0.0) betarm = 0.0;
   if (R.c0 >= 0.0) betar0 = 0.0;
-  // eq. 3.6
   s.pl = L.pla + (betalp + betalm) * (cla * cla);
   s.pr = R.pra + (betarp + betarm) * (cra * cra);
   s.ul = L.ula + (betalp - betalm) * cla;
   s.ur = R.ura + (betarp - betarm) * cra;
   s.dl = 1.0 / (1.0 / L.dla - (betal0 + betalp + betalm));
   s.dr = 1.0 / (1.0 / R.dra - (betar0 + betarp + betarm));
-  // advected quantities, inteuler.F:414-434
-  if (ul_cell <= 0.0) {
-    s.vl = L.vla; s.wl = L.wla; s.gel = L.gela;
-  } else {
-    s.vl = L.vl0; s.wl = L.wl0; s.gel = L.gel0;
-  }
-  if (ur_cell >= 0.0) {
-    s.vr = R.vra; s.wr = R.wra; s.ger = R.gera;
-  } else {
-    s.vr = R.vr0; s.wr = R.wr0; s.ger = R.ger0;
-  }
-  // dual-energy hypersonic override, inteuler.F:493-521
   if (DUAL) {
     double ml = dmax(dmax(fabs(L.cm), fabs(L.c0)), fabs(L.cp));
     if (P.gamma * L.pla / L.dla < P.eta2 * (L.ula * L.ula) || ml < 1.0e-3 || s.dl / L.dla > 5.0) {
@@ -188,11 +185,27 @@ __device__ __forceinline__ FaceState face_assemble(const Lside& L, const Rside& 
       s.pr = R.pra; s.ur = R.ura; s.dr = R.dra;
     }
   }
-  // floors, inteuler.F:540-545
   s.pl = dmax(s.pl, kTiny);
   s.pr = dmax(s.pr, kTiny);
   s.dl = dmax(s.dl, kTiny);
   s.dr = dmax(s.dr, kTiny);
+  return s;
+}
+
+// inteuler.F:414-434: ul_cell / ur_cell = uslice(i-1) / uslice(i)
+__device__ __forceinline__ AdvState face_advected(const AdvL& L, const AdvR& R, double ul_cell,
+                                                  double ur_cell) {
+  AdvState s;
+  if (ul_cell <= 0.0) {
+    s.vl = L.vla; s.wl = L.wla; s.gel = L.gela;
+  } else {
+    s.vl = L.vl0; s.wl = L.wl0; s.gel = L.gel0;
+  }
+  if (ur_cell >= 0.0) {
+    s.vr = R.vra; s.wr = R.wra; s.ger = R.gera;
+  } else {
+    s.vr = R.vr0; s.wr = R.wr0; s.ger = R.ger0;
+  }
   return s;
 }
 

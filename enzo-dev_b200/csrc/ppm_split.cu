@@ -1,7 +1,7 @@
 // ppm_split.cu -- one directional sweep as three sm_100a kernels sharing a face scratch.
 //
-//   reconstruct_kernel  (thread per pencil, marching)  inteuler + intvar: the 12 corrected
-//                       interface states of every face -> fstate
+//   reconstruct_kernel  (thread per pencil, marching, two roles)  inteuler + intvar: the
+//                       12 corrected interface states of every face -> fstate
 //   riemann_kernel      (thread per face)               twoshock + flux_twoshock -> fflux
 //   update_kernel       (thread per pencil, marching)  flux_twoshock's negative-state check
 //                       with the per-cell flux_hll fallback, euler, pgas2d_dual
@@ -45,60 +45,20 @@ __device__ __forceinline__ Phys make_phys(const SweepArgs& a) {
   return P;
 }
 
-template <bool DUAL>
-__device__ __forceinline__ Lside make_left(const Para (&pa)[6], const Prep& pr) {
-  Lside L;
-  L.dla = pm_A(pa[VD], pr.char1);
-  L.dl0 = pm_A(pa[VD], pr.c0);
-  L.pla = pm_A(pa[VP], pr.char1);
-  L.pl0 = pm_A(pa[VP], pr.c0);
-  L.plm = pm_A(pa[VP], pr.cm);
-  L.plp = pm_A(pa[VP], pr.cp);
-  L.ula = pm_A(pa[VU], pr.char1);
-  L.ul0 = pm_A(pa[VU], pr.c0);
-  L.ulm = pm_A(pa[VU], pr.cm);
-  L.ulp = pm_A(pa[VU], pr.cp);
-  L.vla = pm_A(pa[VV], pr.char1);
-  L.vl0 = pm_A(pa[VV], pr.c0);
-  L.wla = pm_A(pa[VW], pr.char1);
-  L.wl0 = pm_A(pa[VW], pr.c0);
-  L.gela = DUAL ? pm_A(pa[VGE], pr.char1) : 0.0;
-  L.gel0 = DUAL ? pm_A(pa[VGE], pr.c0) : 0.0;
-  L.cm = pr.cm;
-  L.c0 = pr.c0;
-  L.cp = pr.cp;
-  return L;
-}
-
-template <bool DUAL>
-__device__ __forceinline__ Rside make_right(const Para (&pa)[6], const Prep& pr) {
-  Rside R;
-  R.dra = pm_C(pa[VD], pr.char2);
-  R.dr0 = pm_B(pa[VD], pr.c0);
-  R.pra = pm_C(pa[VP], pr.char2);
-  R.pr0 = pm_B(pa[VP], pr.c0);
-  R.prm = pm_B(pa[VP], pr.cm);
-  R.prp = pm_B(pa[VP], pr.cp);
-  R.ura = pm_C(pa[VU], pr.char2);
-  R.ur0 = pm_B(pa[VU], pr.c0);
-  R.urm = pm_B(pa[VU], pr.cm);
-  R.urp = pm_B(pa[VU], pr.cp);
-  R.vra = pm_C(pa[VV], pr.char2);
-  R.vr0 = pm_B(pa[VV], pr.c0);
-  R.wra = pm_C(pa[VW], pr.char2);
-  R.wr0 = pm_B(pa[VW], pr.c0);
-  R.gera = DUAL ? pm_C(pa[VGE], pr.char2) : 0.0;
-  R.ger0 = DUAL ? pm_B(pa[VGE], pr.c0) : 0.0;
-  R.cm = pr.cm;
-  R.c0 = pr.c0;
-  R.cp = pr.cp;
-  return R;
-}
-
 // ------------------------------------------------------------------ stage 1
-template <bool DUAL, bool GRAV>
-__global__ void __launch_bounds__(128) reconstruct_kernel(const __grid_constant__ SweepArgs a) {
-  constexpr int NV = DUAL ? 6 : 5;
+// Two roles march the same pencil independently: ROLE 0 reconstructs density,
+// pressure and normal velocity and applies inteuler's characteristic corrections,
+// dual-energy override and floors; ROLE 1 reconstructs the transverse velocities and
+// the gas energy and selects their upwind states.  Each writes its own six planes.
+// Splitting the face this way halves the live state of a marching thread.
+#ifndef PPM_RECON_MINBLOCKS
+#define PPM_RECON_MINBLOCKS 1
+#endif
+
+template <bool DUAL, bool GRAV, int ROLE>
+__global__ void __launch_bounds__(128, PPM_RECON_MINBLOCKS)
+    reconstruct_kernel(const __grid_constant__ SweepArgs a) {
+  constexpr int NV = (ROLE == 0) ? 3 : (DUAL ? 3 : 2);
   const int64_t pid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (pid >= a.npencils) return;
   const Phys P = make_phys(a);
@@ -106,34 +66,42 @@ __global__ void __launch_bounds__(128) reconstruct_kernel(const __grid_constant_
   const int64_t sa = a.sa;
   const int is = a.is, ie = a.ie;
   const int64_t np = a.npencils, plane = a.plane;
+  // the role's variables: ROLE 0 (d, p, u), ROLE 1 (v, w, ge)
+  const double* q0p = ROLE == 0 ? a.in_d : a.in_v;
+  const double* q1p = ROLE == 0 ? a.pres : a.in_w;
+  const double* q2p = ROLE == 0 ? a.in_u : (DUAL ? a.in_ge : nullptr);
 
-  double wq0[6], wq1[6], wq2[6];  // cells t-3, t-2, t-1
-  double dqm1[6], qlm1[6];        // dq(t-2), ql(t-2)
+  double wq0[3], wq1[3], wq2[3];  // cells t-3, t-2, t-1
+  double dqm1[3], qlm1[3];        // dq(t-2), ql(t-2)
 #pragma unroll
-  for (int v = 0; v < 6; ++v) wq0[v] = wq1[v] = wq2[v] = dqm1[v] = qlm1[v] = 0.0;
-  double wg0 = 0.0, wg1 = 0.0, wg2 = 0.0;
+  for (int v = 0; v < 3; ++v) wq0[v] = wq1[v] = wq2[v] = dqm1[v] = qlm1[v] = 0.0;
+  double wu0 = 0.0, wu1 = 0.0, wu2 = 0.0;  // normal velocity of cells t-3, t-2, t-1
+  double wg0 = 0.0, wg1 = 0.0, wg2 = 0.0;  // acceleration (ROLE 0, GRAV)
   Prep prA = {0, 0, 0, 0, 0}, prB = {0, 0, 0, 0, 0};  // cells t-2, t-1
-  Lside Lp = {};                                      // left data of face t-2
+  CoreL cLp = {};  // left data of face t-2 (ROLE 0)
+  AdvL aLp = {};   // left data of face t-2 (ROLE 1)
 
   const int tend = ie + 3;  // the last face, ie+1, is assembled at t = ie+3
 #pragma unroll 1
   for (int t = 0; t <= tend; ++t) {
-    double nq[6];
     const int64_t off = base + (int64_t)t * sa;
-    nq[VD] = __ldg(a.in_d + off);
-    nq[VP] = __ldg(a.pres + off);
-    nq[VU] = ldg0(a.in_u, off);
-    nq[VV] = ldg0(a.in_v, off);
-    nq[VW] = ldg0(a.in_w, off);
-    nq[VGE] = DUAL ? __ldg(a.in_ge + off) : 0.0;
-    const double ng = GRAV ? __ldg(a.grav + off) : 0.0;
+    double nq[3];
+    nq[0] = ldg0(q0p, off);
+    nq[1] = ldg0(q1p, off);
+    nq[2] = ldg0(q2p, off);
+    const double nu = ROLE == 0 ? nq[2] : ldg0(a.in_u, off);
+    const double ng = (GRAV && ROLE == 0) ? __ldg(a.grav + off) : 0.0;
     // characteristic distances of cell t (inteuler.F:197-208)
     Prep prC = prB;
-    if (t >= is - 1 && t <= ie + 1) prC = cell_prep(nq[VD], nq[VP], nq[VU], a.coef[t].dx2i, P);
+    if (t >= is - 1 && t <= ie + 1) {
+      const double nd = ROLE == 0 ? nq[0] : __ldg(a.in_d + off);
+      const double npr = ROLE == 0 ? nq[1] : __ldg(a.pres + off);
+      prC = cell_prep(nd, npr, nu, a.coef[t].dx2i, P);
+    }
     // slope and left edge of cell t-1 (intvar.F:82-102)
-    double dqN[6], qlN[6];
+    double dqN[3], qlN[3];
 #pragma unroll
-    for (int v = 0; v < 6; ++v) dqN[v] = qlN[v] = 0.0;
+    for (int v = 0; v < 3; ++v) dqN[v] = qlN[v] = 0.0;
     {
       const int c = t - 1;
       if (c >= is - 2 && c <= ie + 2) {
@@ -148,52 +116,104 @@ __global__ void __launch_bounds__(128) reconstruct_kernel(const __grid_constant_
       }
     }
     // parabola of cell t-2, its face contributions, and face t-2 (inteuler.F:304-551)
-    Lside Ln = Lp;
+    CoreL cLn = cLp;
+    AdvL aLn = aLp;
     {
       const int c = t - 2;
       if (c >= is - 1 && c <= ie + 1) {
-        Para pa[6];
+        Para pa[3];
 #pragma unroll
-        for (int v = 0; v < 6; ++v) pa[v] = Para{0.0, 0.0, 0.0, 0.0};
+        for (int v = 0; v < 3; ++v) pa[v] = Para{0.0, 0.0, 0.0, 0.0};
 #pragma unroll
         for (int v = 0; v < NV; ++v) pa[v] = pm_parabola(wq0[v], wq1[v], wq2[v], qlm1[v], qlN[v]);
-        if (c >= is) {
-          const Rside Rc = make_right<DUAL>(pa, prA);
-          const double gsum = GRAV ? (wg0 + wg1) : 0.0;
-          const FaceState s = face_assemble<DUAL, GRAV>(Lp, Rc, wq0[VU], wq1[VU], gsum, P);
-          double* o = a.fstate + (int64_t)(c - is) * np + pid;
-          o[SDL * plane] = s.dl;
-          o[SDR * plane] = s.dr;
-          o[SPL * plane] = s.pl;
-          o[SPR * plane] = s.pr;
-          o[SUL * plane] = s.ul;
-          o[SUR * plane] = s.ur;
-          o[SVL * plane] = s.vl;
-          o[SVR * plane] = s.vr;
-          o[SWL * plane] = s.wl;
-          o[SWR * plane] = s.wr;
-          if (DUAL) {
-            o[SGEL * plane] = s.gel;
-            o[SGER * plane] = s.ger;
+        double* o = a.fstate + (int64_t)(c - is) * np + pid;
+        if (ROLE == 0) {
+          if (c >= is) {
+            CoreR R;
+            R.dra = pm_C(pa[0], prA.char2);
+            R.dr0 = pm_B(pa[0], prA.c0);
+            R.pra = pm_C(pa[1], prA.char2);
+            R.pr0 = pm_B(pa[1], prA.c0);
+            R.prm = pm_B(pa[1], prA.cm);
+            R.prp = pm_B(pa[1], prA.cp);
+            R.ura = pm_C(pa[2], prA.char2);
+            R.ur0 = pm_B(pa[2], prA.c0);
+            R.urm = pm_B(pa[2], prA.cm);
+            R.urp = pm_B(pa[2], prA.cp);
+            R.cm = prA.cm;
+            R.c0 = prA.c0;
+            R.cp = prA.cp;
+            const CoreState s = face_core<DUAL, GRAV>(cLp, R, GRAV ? (wg0 + wg1) : 0.0, P);
+            o[SDL * plane] = s.dl;
+            o[SDR * plane] = s.dr;
+            o[SPL * plane] = s.pl;
+            o[SPR * plane] = s.pr;
+            o[SUL * plane] = s.ul;
+            o[SUR * plane] = s.ur;
+          }
+          if (c <= ie) {
+            cLn.dla = pm_A(pa[0], prA.char1);
+            cLn.dl0 = pm_A(pa[0], prA.c0);
+            cLn.pla = pm_A(pa[1], prA.char1);
+            cLn.pl0 = pm_A(pa[1], prA.c0);
+            cLn.plm = pm_A(pa[1], prA.cm);
+            cLn.plp = pm_A(pa[1], prA.cp);
+            cLn.ula = pm_A(pa[2], prA.char1);
+            cLn.ul0 = pm_A(pa[2], prA.c0);
+            cLn.ulm = pm_A(pa[2], prA.cm);
+            cLn.ulp = pm_A(pa[2], prA.cp);
+            cLn.cm = prA.cm;
+            cLn.c0 = prA.c0;
+            cLn.cp = prA.cp;
+          }
+        } else {
+          if (c >= is) {
+            AdvR R;
+            R.vra = pm_C(pa[0], prA.char2);
+            R.vr0 = pm_B(pa[0], prA.c0);
+            R.wra = pm_C(pa[1], prA.char2);
+            R.wr0 = pm_B(pa[1], prA.c0);
+            R.gera = DUAL ? pm_C(pa[2], prA.char2) : 0.0;
+            R.ger0 = DUAL ? pm_B(pa[2], prA.c0) : 0.0;
+            const AdvState s = face_advected(aLp, R, wu0, wu1);
+            o[SVL * plane] = s.vl;
+            o[SVR * plane] = s.vr;
+            o[SWL * plane] = s.wl;
+            o[SWR * plane] = s.wr;
+            if (DUAL) {
+              o[SGEL * plane] = s.gel;
+              o[SGER * plane] = s.ger;
+            }
+          }
+          if (c <= ie) {
+            aLn.vla = pm_A(pa[0], prA.char1);
+            aLn.vl0 = pm_A(pa[0], prA.c0);
+            aLn.wla = pm_A(pa[1], prA.char1);
+            aLn.wl0 = pm_A(pa[1], prA.c0);
+            aLn.gela = DUAL ? pm_A(pa[2], prA.char1) : 0.0;
+            aLn.gel0 = DUAL ? pm_A(pa[2], prA.c0) : 0.0;
           }
         }
-        if (c <= ie) Ln = make_left<DUAL>(pa, prA);
       }
     }
 #pragma unroll
-    for (int v = 0; v < 6; ++v) {
+    for (int v = 0; v < 3; ++v) {
       wq0[v] = wq1[v];
       wq1[v] = wq2[v];
       wq2[v] = nq[v];
       dqm1[v] = dqN[v];
       qlm1[v] = qlN[v];
     }
+    wu0 = wu1;
+    wu1 = wu2;
+    wu2 = nu;
     wg0 = wg1;
     wg1 = wg2;
     wg2 = ng;
     prA = prB;
     prB = prC;
-    Lp = Ln;
+    cLp = cLn;
+    aLp = aLn;
   }
 }
 
@@ -528,7 +548,8 @@ template <bool DUAL, bool GRAV>
 void launch3(const SweepArgs& a, cudaStream_t st) {
   const unsigned b1 = (unsigned)((a.npencils + 127) / 128);
   cudaMemsetAsync(a.counters + kCntFlagged, 0, sizeof(unsigned long long), st);
-  reconstruct_kernel<DUAL, GRAV><<<b1, 128, 0, st>>>(a);
+  reconstruct_kernel<DUAL, GRAV, 0><<<b1, 128, 0, st>>>(a);
+  reconstruct_kernel<DUAL, GRAV, 1><<<b1, 128, 0, st>>>(a);
   dim3 g2((unsigned)((a.npencils + 255) / 256), (unsigned)(a.ie - a.is + 2));
   riemann_kernel<DUAL><<<g2, 256, 0, st>>>(a);
   update_kernel<DUAL, GRAV><<<b1, 128, 0, st>>>(a);
@@ -537,7 +558,7 @@ void launch3(const SweepArgs& a, cudaStream_t st) {
 
 }  // namespace split
 
-// Four launches; the caller provides a.fstate / a.fflux / a.plane / a.flagged.
+// Five launches; the caller provides a.fstate / a.fflux / a.plane / a.flagged.
 void launch_sweep_split(const SweepArgs& a, bool dual, bool grav, cudaStream_t st) {
   if (dual && grav) split::launch3<true, true>(a, st);
   else if (dual) split::launch3<true, false>(a, st);
