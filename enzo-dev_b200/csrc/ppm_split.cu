@@ -51,8 +51,9 @@ __device__ __forceinline__ Phys make_phys(const SweepArgs& a) {
 // dual-energy override and floors; ROLE 1 reconstructs the transverse velocities and
 // the gas energy and selects their upwind states.  Each writes its own six planes.
 // Splitting the face this way halves the live state of a marching thread.
+// Four resident blocks per SM keep a 256^3 sweep's pencils in a single wave.
 #ifndef PPM_RECON_MINBLOCKS
-#define PPM_RECON_MINBLOCKS 1
+#define PPM_RECON_MINBLOCKS 4
 #endif
 
 template <bool DUAL, bool GRAV, int ROLE>
