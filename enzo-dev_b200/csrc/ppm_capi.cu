@@ -1,36 +1,65 @@
 // ppm_capi.cu -- the C ABI of include/ppm_b200.h: context, persistent device scratch,
-// coefficient tables, and the grid::SolvePPM_DE driver (pressure once, then the three
-// sweeps in the order rotated by CycleNumber % GridRank, Grid_SolvePPM_DE.C:53-146).
+// batch descriptors, and the grid::SolvePPM_DE driver (pressure once, then the sweeps
+// in the order rotated by CycleNumber % GridRank, Grid_SolvePPM_DE.C:53-146).
+//
+// Every call runs on a batch of grids: a single grid (ppm_b200_solve_ppm_de,
+// ppm_b200_euler_sweep) or all grids of an AMR level (ppm_b200_solve_level).  Each
+// kernel stage is one launch over the whole batch; the per-grid records and block
+// prefix tables it reads are uploaded only when their contents change, so a
+// device-resident time loop issues no host-to-device copies after its first step and
+// can be replayed as a CUDA graph.
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
+#include <string>
 #include <vector>
 
 #include "ppm_b200.h"
 #include "ppm_sweep.cuh"
 
-// launchers defined in ppm_kernels.cu
 namespace ppm {
-void launch_sweep_split(const SweepArgs& a, bool dual, bool grav, cudaStream_t st);
-void launch_pressure_plain(const double* d, const double* te, const double* v1, const double* v2,
-                           const double* v3, const double* ge, double* p, int64_t size,
-                           double gamma, double tiny_number, double min_support, int sms,
+// element-wise batch records, defined with the kernels in ppm_kernels.cu
+struct ElemGrid {
+  const double* d;
+  const double* te;
+  const double* v[3];
+  const double* ge;
+  double* p;
+  double* f[6];
+  const double* cw[3];
+  int rank;
+  int dims[3], start[3], end[3];
+  int bc[3];
+  int64_t size;
+  int64_t active;
+};
+struct ElemBatch {
+  const ElemGrid* grids;
+  int ngrids;
+  const int64_t* size_prefix;
+  const int64_t* active_prefix;
+  double gamma, tiny_number, min_support;
+  double aye, vg[3];
+  unsigned long long* min_bits;
+};
+void launch_sweep_batch(const BatchArgs& B, int64_t march_blocks, int64_t riemann_blocks,
+                        bool dual, bool grav, cudaStream_t st, cudaEvent_t* ev = nullptr);
+void launch_pressure_batch(const ElemBatch& B, int64_t blocks, cudaStream_t st);
+void launch_timestep_batch(const ElemBatch& B, int64_t blocks, double courant, double* dt_out,
                            cudaStream_t st);
-void launch_timestep_plain(const double* d, const double* te, const double* const v[3],
-                           const double* ge, int rank, const int dims[3], const int start[3],
-                           const int end[3], double gamma, double tiny_number, double min_support,
-                           double aye, const double vg[3], const double* const cw[3],
-                           unsigned long long* min_bits, double courant, double* dt_out, int sms,
-                           cudaStream_t st);
-void launch_boundary_plain(double* const* f, int nf, const int dims[3], const int start[3],
-                           const int end[3], const int bc[3], int sms, cudaStream_t st);
+void launch_boundary_batch(const ElemBatch& B, int64_t blocks, cudaStream_t st);
 }  // namespace ppm
 
+using ppm::BatchArgs;
 using ppm::Coef;
+using ppm::ElemBatch;
+using ppm::ElemGrid;
 using ppm::FluxCapture;
 using ppm::SweepArgs;
 
@@ -38,6 +67,31 @@ struct DevBuf {
   void* p = nullptr;
   size_t bytes = 0;
 };
+
+// A device copy of a host byte image, re-uploaded only when the image changes.
+struct Mirror {
+  DevBuf dev;
+  std::vector<unsigned char> host;
+  uint64_t version = 0;
+};
+
+// descriptor slots: one per sweep direction and position, per element kernel and per
+// table, so a time loop that repeats the same calls uploads nothing after its first step
+enum {
+  kSlotSweep0 = 0,     // 0..8: sweep records + block prefixes, per (direction, position
+                       //       of the sweep in the rotated order): the ring buffers a
+                       //       sweep reads and writes depend on both
+  kSlotPressure = 9,   // element records of the pressure kernel
+  kSlotCoef0 = 10,     // 10..12: inteuler coefficient tables per direction
+  kSlotCw = 13,        // cell widths of the time-step kernel
+  kSlotTimestep = 14,  // element records of the time-step kernel
+  kSlotBoundary = 15,  // element records of the ghost-fill kernel
+  kSlotCount = 16
+};
+// captured level graphs kept at most (a changed grid list leaves the old ones unused)
+constexpr size_t kMaxGraphs = 16;
+// events around a timed sweep: before each of its five kernels and after the last
+constexpr int kSweepEvents = 6;
 
 struct ppm_b200_context {
   int device = 0;
@@ -47,24 +101,25 @@ struct ppm_b200_context {
   long long launches = 0;
   int sticky_error = 0;
   // persistent device scratch, grown on demand
-  DevBuf field_set[2][6];   // two ring sets of d, e, v1, v2, v3, ge
-  DevBuf host_set[6];       // device copies of host-memory fields
+  DevBuf host_set[6];       // device copies of host-memory fields (single grid)
   DevBuf host_acc[3];       // device copies of host-memory accelerations
-  DevBuf pressure;
-  DevBuf coef[3];
-  std::vector<Coef> coef_host[3];
-  DevBuf cw_dev[3];
-  std::vector<double> cw_host[3];
+  DevBuf ring;              // two ring sets of the six updated fields, every grid of the batch
+  DevBuf pressure;          // pressure of every grid of the batch
+  DevBuf face_scratch;      // interface states, fluxes and the flagged-pencil list
   DevBuf counters;          // kMaxCounters unsigned long long
   DevBuf misc;              // [0] min_bits, [1] dt
   DevBuf captures;
   DevBuf capture_buf;
   std::vector<double> capture_host;
-  DevBuf face_scratch;      // interface states and fluxes of the three-stage sweep
+  Mirror mirror[kSlotCount];
   // event timing of sweep launches
   bool profiling = false;
-  std::vector<cudaEvent_t> ev_pool;
+  std::vector<cudaEvent_t> ev_pool;  // kSweepEvents per timed sweep
   size_t ev_used = 0;
+  double stage_ms[5] = {0, 0, 0, 0, 0};  // per-kernel totals of the last profile read
+  // CUDA graphs of level solves, keyed by everything a launch takes by value
+  bool use_graphs = false;
+  std::map<std::string, cudaGraphExec_t> graphs;
 };
 
 namespace {
@@ -82,6 +137,11 @@ int cuda_fail(ppm_b200_context* ctx, cudaError_t e, const char* what) {
     if (_e != cudaSuccess) return cuda_fail(ctx, _e, #call);  \
   } while (0)
 
+void drop_graphs(ppm_b200_context* ctx) {
+  for (auto& kv : ctx->graphs) cudaGraphExecDestroy(kv.second);
+  ctx->graphs.clear();
+}
+
 int ensure(ppm_b200_context* ctx, DevBuf& b, size_t bytes) {
   if (b.bytes >= bytes) return PPM_B200_OK;
   if (b.p) {
@@ -89,14 +149,44 @@ int ensure(ppm_b200_context* ctx, DevBuf& b, size_t bytes) {
     CK(cudaFree(b.p));
     b.p = nullptr;
     b.bytes = 0;
+    drop_graphs(ctx);  // captured graphs may reference the old allocation
   }
   CK(cudaMalloc(&b.p, bytes));
   b.bytes = bytes;
   return PPM_B200_OK;
 }
 
+// Upload `img` into mirror slot m unless the device copy already holds it.
+int mirror_put(ppm_b200_context* ctx, Mirror& m, const std::vector<unsigned char>& img) {
+  if (m.host.size() == img.size() && m.dev.p &&
+      std::memcmp(m.host.data(), img.data(), img.size()) == 0)
+    return PPM_B200_OK;
+  int rc = ensure(ctx, m.dev, std::max<size_t>(img.size(), 256));
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(ctx->stream));  // the previous contents may still be in use
+  CK(cudaMemcpy(m.dev.p, img.data(), img.size(), cudaMemcpyHostToDevice));
+  m.host = img;
+  m.version += 1;
+  return PPM_B200_OK;
+}
+
+template <class T>
+void append(std::vector<unsigned char>& img, const T* p, size_t n) {
+  const size_t at = img.size();
+  img.resize(at + n * sizeof(T));
+  if (n) std::memcpy(img.data() + at, p, n * sizeof(T));
+}
+
+size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
 int64_t grid_size(const ppm_b200_grid* g) {
   return (int64_t)g->dims[0] * g->dims[1] * g->dims[2];
+}
+
+int64_t grid_active(const ppm_b200_grid* g) {
+  int64_t n = 1;
+  for (int d = 0; d < g->rank; ++d) n *= g->end[d] - g->start[d] + 1;
+  return n;
 }
 
 // inteuler.F:140-158 on the host, same expressions, 1-based i mapped to entry i-1.
@@ -124,34 +214,6 @@ void build_coef(const double* dxi_in, int n, int is0, int ie0, std::vector<Coef>
   }
 }
 
-int upload_coef(ppm_b200_context* ctx, int dim, const ppm_b200_grid* g) {
-  const int n = g->dims[dim];
-  std::vector<Coef> c;
-  build_coef(g->cell_width[dim], n, g->start[dim], g->end[dim], c);
-  auto& cache = ctx->coef_host[dim];
-  if (cache.size() == c.size() && std::memcmp(cache.data(), c.data(), c.size() * sizeof(Coef)) == 0)
-    return PPM_B200_OK;
-  int rc = ensure(ctx, ctx->coef[dim], c.size() * sizeof(Coef));
-  if (rc) return rc;
-  CK(cudaStreamSynchronize(ctx->stream));  // the previous table may still be in use
-  CK(cudaMemcpy(ctx->coef[dim].p, c.data(), c.size() * sizeof(Coef), cudaMemcpyHostToDevice));
-  cache = c;
-  return PPM_B200_OK;
-}
-
-int upload_cw(ppm_b200_context* ctx, int dim, const ppm_b200_grid* g) {
-  const int n = g->dims[dim];
-  std::vector<double> c(g->cell_width[dim], g->cell_width[dim] + n);
-  auto& cache = ctx->cw_host[dim];
-  if (cache == c) return PPM_B200_OK;
-  int rc = ensure(ctx, ctx->cw_dev[dim], n * sizeof(double));
-  if (rc) return rc;
-  CK(cudaStreamSynchronize(ctx->stream));
-  CK(cudaMemcpy(ctx->cw_dev[dim].p, c.data(), n * sizeof(double), cudaMemcpyHostToDevice));
-  cache = c;
-  return PPM_B200_OK;
-}
-
 int check_supported(const ppm_b200_params* p) {
   if (!p) return PPM_B200_ERR_INVALID;
   if (p->pressure_free || p->steepening || p->flattening || p->diffusion ||
@@ -173,6 +235,7 @@ int check_grid(const ppm_b200_grid* g, const ppm_b200_params* p) {
         // the sweep needs exactly three ghost zones on each side (NumberOfGhostZones = 3)
         if (g->start[d] != 3 || g->dims[d] - 1 - g->end[d] != 3) return PPM_B200_ERR_INVALID;
         if (!g->cell_width[d]) return PPM_B200_ERR_INVALID;
+        if (g->dims[d] > 1031) return PPM_B200_ERR_TOO_LARGE;  // fortran.def:1
       }
       if (d > 0 && !g->velocity[d]) return PPM_B200_ERR_INVALID;
       if (p->gravity && !g->acceleration[d]) return PPM_B200_ERR_INVALID;
@@ -187,6 +250,15 @@ struct FieldSet {
   double* f[6];  // d, e, v1, v2, v3, ge
 };
 
+// Device pointers of one grid for one call.
+struct GridIO {
+  const ppm_b200_grid* g;
+  FieldSet user;            // the grid's fields (device)
+  FieldSet ring[2];         // scratch ring sets
+  const double* acc[3];
+  double* pres;
+};
+
 // One capture request on the host: where the 6 captured values of a request go.
 struct HostCapture {
   int sub;     // subgrid
@@ -194,159 +266,300 @@ struct HostCapture {
   int64_t offset;
 };
 
-int run_sweep(ppm_b200_context* ctx, int dim, const ppm_b200_params* p, const ppm_b200_grid* g,
-              const FieldSet& in, const FieldSet& out, const double* pressure,
-              const double* const acc[3], int nsub, ppm_b200_fluxes* sub, const long long ggs[3]) {
-  int rc = upload_coef(ctx, dim, g);
-  if (rc) return rc;
-  const int GD0 = g->dims[0], GD1 = g->dims[1], GD2 = g->dims[2];
-  SweepArgs a;
-  std::memset(&a, 0, sizeof(a));
-  a.n = g->dims[dim];
-  a.is = g->start[dim];
-  a.ie = g->end[dim];
-  int ax1, ax2;  // transverse axes: t1 (fast), t2
-  if (dim == 0) {
-    a.n1 = GD1; a.n2 = GD2; a.s1 = GD0; a.s2 = (int64_t)GD0 * GD1; a.sa = 1; ax1 = 1; ax2 = 2;
-  } else if (dim == 1) {
-    a.n1 = GD0; a.n2 = GD2; a.s1 = 1; a.s2 = (int64_t)GD0 * GD1; a.sa = GD0; ax1 = 0; ax2 = 2;
-  } else {
-    a.n1 = GD0; a.n2 = GD1; a.s1 = 1; a.s2 = GD0; a.sa = (int64_t)GD0 * GD1; ax1 = 0; ax2 = 1;
-  }
-  a.npencils = (int64_t)a.n1 * a.n2;
-  const int vu = dim, vv = (dim + 1) % 3, vw = (dim + 2) % 3;
-  auto vel_in = [&](int c) -> const double* { return c < g->rank ? in.f[2 + c] : nullptr; };
-  auto vel_out = [&](int c) -> double* { return c < g->rank ? out.f[2 + c] : nullptr; };
-  a.in_d = in.f[0];
-  a.in_e = in.f[1];
-  a.in_u = vel_in(vu);
-  a.in_v = vel_in(vv);
-  a.in_w = vel_in(vw);
-  a.in_ge = p->dual_energy ? in.f[5] : nullptr;
-  a.out_d = out.f[0];
-  a.out_e = out.f[1];
-  a.out_u = vel_out(vu);
-  a.out_v = vel_out(vv);
-  a.out_w = vel_out(vw);
-  a.out_ge = p->dual_energy ? out.f[5] : nullptr;
-  a.pres = pressure;
-  a.grav = p->gravity ? acc[dim] : nullptr;
-  a.coef = (const Coef*)ctx->coef[dim].p;
-  a.gamma = p->gamma;
-  a.dt = p->dt;
-  a.dt_device = p->dt_device;
-  a.eta1 = p->eta1;
-  a.eta2 = p->eta2;
-  a.small_rho = p->small_rho;
-  a.pmin = p->tiny_number;
-  a.fallback = p->riemann_fallback;
-  a.counters = (unsigned long long*)ctx->counters.p;
+// Per-grid coefficient tables of one direction, deduplicated by content.
+struct CoefTables {
+  std::vector<Coef> all;
+  std::vector<int64_t> offset;  // per grid, entries into `all`
+};
 
-  // subgrid flux capture requests (Grid_xEulerSweep.C:313-377 and y/z siblings)
-  std::vector<FluxCapture> reqs;
-  std::vector<HostCapture> hreq;
-  if (nsub > 0 && sub) {
-    for (int s = 0; s < nsub; ++s) {
-      const ppm_b200_fluxes& fx = sub[s];
-      // flux-plane axes as the reference names them: (idim, jdim)
-      int ia = (dim == 0) ? 1 : 0;
-      int ja = (dim == 2) ? 1 : 2;
-      long long fi0 = fx.right_start[dim][ia] - ggs[ia];
-      long long fi1 = fx.right_end[dim][ia] - ggs[ia];
-      long long fj0 = fx.right_start[dim][ja] - ggs[ja];
-      long long fj1 = fx.right_end[dim][ja] - ggs[ja];
-      long long nfi = fi1 - fi0 + 1;
-      long long lface = fx.left_start[dim][dim] - ggs[dim];
-      long long rface = fx.right_start[dim][dim] - ggs[dim] + 1;
-      if (lface < a.is || rface > a.ie + 1) return PPM_B200_ERR_INVALID;
-      for (long long cj = fj0; cj <= fj1; ++cj)
-        for (long long ci = fi0; ci <= fi1; ++ci) {
-          long long c[3];
-          c[ia] = ci;
-          c[ja] = cj;
-          int64_t t1 = c[ax1], t2 = c[ax2];
-          if (t1 < 0 || t1 >= a.n1 || t2 < 0 || t2 >= a.n2) return PPM_B200_ERR_INVALID;
-          int64_t pencil = t2 * a.n1 + t1;
-          long long offset = (ci - fi0) + (cj - fj0) * nfi;
-          for (int side = 0; side < 2; ++side) {
-            FluxCapture r;
-            r.pencil = pencil;
-            r.face = (int)(side == 0 ? lface : rface);
-            r.pad = (int)hreq.size();
-            r.dst = 0;
-            reqs.push_back(r);
-            hreq.push_back(HostCapture{s, side, offset});
-          }
-        }
+void build_coef_tables(int dim, const std::vector<GridIO>& io, CoefTables& ct) {
+  ct.all.clear();
+  ct.offset.assign(io.size(), 0);
+  std::map<std::vector<double>, int64_t> seen;
+  for (size_t k = 0; k < io.size(); ++k) {
+    const ppm_b200_grid* g = io[k].g;
+    const int n = g->dims[dim];
+    std::vector<double> key(g->cell_width[dim], g->cell_width[dim] + n);
+    key.push_back((double)g->start[dim]);
+    key.push_back((double)g->end[dim]);
+    auto it = seen.find(key);
+    if (it != seen.end()) {
+      ct.offset[k] = it->second;
+      continue;
     }
-    std::sort(reqs.begin(), reqs.end(), [](const FluxCapture& x, const FluxCapture& y) {
-      return x.pencil != y.pencil ? x.pencil < y.pencil : x.face < y.face;
-    });
-    for (size_t k = 0; k < reqs.size(); ++k) reqs[k].dst = (int64_t)k * 6;
-    rc = ensure(ctx, ctx->captures, reqs.size() * sizeof(FluxCapture));
-    if (rc) return rc;
-    rc = ensure(ctx, ctx->capture_buf, reqs.size() * 6 * sizeof(double));
-    if (rc) return rc;
-    CK(cudaMemcpyAsync(ctx->captures.p, reqs.data(), reqs.size() * sizeof(FluxCapture),
+    std::vector<Coef> c;
+    build_coef(g->cell_width[dim], n, g->start[dim], g->end[dim], c);
+    ct.offset[k] = (int64_t)ct.all.size();
+    seen[key] = ct.offset[k];
+    ct.all.insert(ct.all.end(), c.begin(), c.end());
+  }
+}
+
+// Everything one directional sweep of a batch needs on the device.
+struct SweepPlan {
+  BatchArgs B;
+  int64_t march_blocks = 0, riemann_blocks = 0;
+  std::vector<FluxCapture> reqs;    // single-grid subgrid-flux capture
+  std::vector<HostCapture> hreq;
+  int64_t cap_offset = 0;           // this sweep's first request in the capture buffers
+};
+
+// Subgrid flux capture requests of one sweep of a single grid (Grid_xEulerSweep.C:313-377
+// and its y/z siblings): one request per (flux-plane cell, side), sorted by pencil.
+int build_captures(const ppm_b200_grid* g, int dim, int nsub, const ppm_b200_fluxes* sub,
+                   const long long ggs[3], SweepPlan& plan) {
+  plan.reqs.clear();
+  plan.hreq.clear();
+  if (nsub <= 0 || !sub) return PPM_B200_OK;
+  const int is = g->start[dim], ie = g->end[dim];
+  int n1, n2, ax1, ax2;
+  if (dim == 0) { n1 = g->dims[1]; n2 = g->dims[2]; ax1 = 1; ax2 = 2; }
+  else if (dim == 1) { n1 = g->dims[0]; n2 = g->dims[2]; ax1 = 0; ax2 = 2; }
+  else { n1 = g->dims[0]; n2 = g->dims[1]; ax1 = 0; ax2 = 1; }
+  for (int s = 0; s < nsub; ++s) {
+    const ppm_b200_fluxes& fx = sub[s];
+    // flux-plane axes as the reference names them: (idim, jdim)
+    const int ia = (dim == 0) ? 1 : 0;
+    const int ja = (dim == 2) ? 1 : 2;
+    const long long fi0 = fx.right_start[dim][ia] - ggs[ia];
+    const long long fi1 = fx.right_end[dim][ia] - ggs[ia];
+    const long long fj0 = fx.right_start[dim][ja] - ggs[ja];
+    const long long fj1 = fx.right_end[dim][ja] - ggs[ja];
+    const long long nfi = fi1 - fi0 + 1;
+    const long long lface = fx.left_start[dim][dim] - ggs[dim];
+    const long long rface = fx.right_start[dim][dim] - ggs[dim] + 1;
+    if (lface < is || rface > ie + 1) return PPM_B200_ERR_INVALID;
+    for (long long cj = fj0; cj <= fj1; ++cj)
+      for (long long ci = fi0; ci <= fi1; ++ci) {
+        long long c[3] = {0, 0, 0};
+        c[ia] = ci;
+        c[ja] = cj;
+        const int64_t t1 = c[ax1], t2 = c[ax2];
+        if (t1 < 0 || t1 >= n1 || t2 < 0 || t2 >= n2) return PPM_B200_ERR_INVALID;
+        const int64_t pencil = t2 * n1 + t1;
+        const long long offset = (ci - fi0) + (cj - fj0) * nfi;
+        for (int side = 0; side < 2; ++side) {
+          FluxCapture r;
+          r.pencil = pencil;
+          r.face = (int)(side == 0 ? lface : rface);
+          r.pad = (int)plan.hreq.size();
+          r.dst = 0;
+          plan.reqs.push_back(r);
+          plan.hreq.push_back(HostCapture{s, side, offset});
+        }
+      }
+  }
+  std::sort(plan.reqs.begin(), plan.reqs.end(), [](const FluxCapture& x, const FluxCapture& y) {
+    return x.pencil != y.pencil ? x.pencil < y.pencil : x.face < y.face;
+  });
+  return PPM_B200_OK;
+}
+
+// Places the capture requests of several sweeps one after another in the capture
+// buffers (sized before any sweep is queued, so no buffer moves under queued work).
+int reserve_captures(ppm_b200_context* ctx, SweepPlan* plans, int n) {
+  int64_t total = 0;
+  for (int s = 0; s < n; ++s) {
+    plans[s].cap_offset = total;
+    total += (int64_t)plans[s].reqs.size();
+  }
+  if (total == 0) return PPM_B200_OK;
+  int rc = ensure(ctx, ctx->captures, (size_t)total * sizeof(FluxCapture));
+  if (rc) return rc;
+  return ensure(ctx, ctx->capture_buf, (size_t)total * 6 * sizeof(double));
+}
+
+// Face scratch of one directional sweep of a batch: 19 planes of (active cells along
+// the sweep + 1) x pencils per grid, then one flagged-pencil slot per pencil.  The
+// size differs between directions for non-cubic grids.
+size_t sweep_scratch_bytes(int dim, const std::vector<GridIO>& io) {
+  size_t doubles = 0, pencils = 0;
+  for (const auto& x : io) {
+    const ppm_b200_grid* g = x.g;
+    const size_t np = (size_t)grid_size(g) / (size_t)g->dims[dim];
+    doubles += (size_t)(ppm::kFaceVars + ppm::kFluxVars) *
+               (size_t)(g->end[dim] - g->start[dim] + 2) * np;
+    pencils += np;
+  }
+  return doubles * sizeof(double) + pencils * sizeof(int64_t);
+}
+
+int prepare_sweep(ppm_b200_context* ctx, int dim, int position, const ppm_b200_params* p,
+                  const std::vector<GridIO>& io, const std::vector<int>& src,
+                  const std::vector<int>& dst, SweepPlan& plan) {
+  const int ng = (int)io.size();
+  // coefficient tables (deduplicated), uploaded into this direction's table slot
+  CoefTables ct;
+  build_coef_tables(dim, io, ct);
+  std::vector<unsigned char> timg;
+  append(timg, ct.all.data(), ct.all.size());
+  int rc = mirror_put(ctx, ctx->mirror[kSlotCoef0 + dim], timg);
+  if (rc) return rc;
+  const Coef* coef_dev = (const Coef*)ctx->mirror[kSlotCoef0 + dim].dev.p;
+
+  // face scratch: planes of every grid, then the flagged-pencil list
+  std::vector<SweepArgs> rec(ng);
+  std::vector<int64_t> mpre(ng + 1, 0), rpre(ng + 1, 0);
+  size_t scratch_doubles = 0;
+  int64_t total_pencils = 0;
+  for (int k = 0; k < ng; ++k) {
+    const ppm_b200_grid* g = io[k].g;
+    const int GD0 = g->dims[0], GD1 = g->dims[1], GD2 = g->dims[2];
+    SweepArgs& a = rec[k];
+    std::memset(&a, 0, sizeof(a));
+    a.n = g->dims[dim];
+    a.is = g->start[dim];
+    a.ie = g->end[dim];
+    if (dim == 0) {
+      a.n1 = GD1; a.n2 = GD2; a.s1 = GD0; a.s2 = (int64_t)GD0 * GD1; a.sa = 1;
+    } else if (dim == 1) {
+      a.n1 = GD0; a.n2 = GD2; a.s1 = 1; a.s2 = (int64_t)GD0 * GD1; a.sa = GD0;
+    } else {
+      a.n1 = GD0; a.n2 = GD1; a.s1 = 1; a.s2 = GD0; a.sa = (int64_t)GD0 * GD1;
+    }
+    a.npencils = (int64_t)a.n1 * a.n2;
+    a.plane = (int64_t)(a.ie - a.is + 2) * a.npencils;
+    scratch_doubles += (size_t)(ppm::kFaceVars + ppm::kFluxVars) * (size_t)a.plane;
+    total_pencils += a.npencils;
+    const int64_t mb = (a.npencils + ppm::kMarchThreads - 1) / ppm::kMarchThreads;
+    const int64_t rb = (int64_t)(a.ie - a.is + 2) *
+                       ((a.npencils + ppm::kRiemannThreads - 1) / ppm::kRiemannThreads);
+    mpre[k + 1] = mpre[k] + mb;
+    rpre[k + 1] = rpre[k] + rb;
+  }
+  // callers that queue several sweeps size the scratch for all of them first, so this
+  // never moves the buffer under a sweep prepared earlier
+  rc = ensure(ctx, ctx->face_scratch,
+              scratch_doubles * sizeof(double) + (size_t)total_pencils * sizeof(int64_t));
+  if (rc) return rc;
+  double* scratch = (double*)ctx->face_scratch.p;
+  size_t at = 0;
+  const int vu = dim, vv = (dim + 1) % 3, vw = (dim + 2) % 3;
+  for (int k = 0; k < ng; ++k) {
+    const ppm_b200_grid* g = io[k].g;
+    const FieldSet& in = src[k] < 0 ? io[k].user : io[k].ring[src[k]];
+    const FieldSet& out = dst[k] < 0 ? io[k].user : io[k].ring[dst[k]];
+    auto vin = [&](int c) -> const double* { return c < g->rank ? in.f[2 + c] : nullptr; };
+    auto vout = [&](int c) -> double* { return c < g->rank ? out.f[2 + c] : nullptr; };
+    SweepArgs& a = rec[k];
+    a.in_d = in.f[0];
+    a.in_e = in.f[1];
+    a.in_u = vin(vu);
+    a.in_v = vin(vv);
+    a.in_w = vin(vw);
+    a.in_ge = p->dual_energy ? in.f[5] : nullptr;
+    a.out_d = out.f[0];
+    a.out_e = out.f[1];
+    a.out_u = vout(vu);
+    a.out_v = vout(vv);
+    a.out_w = vout(vw);
+    a.out_ge = p->dual_energy ? out.f[5] : nullptr;
+    a.pres = io[k].pres;
+    a.grav = p->gravity ? io[k].acc[dim] : nullptr;
+    a.coef = coef_dev + ct.offset[k];
+    a.gamma = p->gamma;
+    a.dt = p->dt;
+    a.dt_device = p->dt_device;
+    a.eta1 = p->eta1;
+    a.eta2 = p->eta2;
+    a.small_rho = p->small_rho;
+    a.pmin = p->tiny_number;
+    a.fallback = p->riemann_fallback;
+    a.fstate = scratch + at;
+    a.fflux = a.fstate + (size_t)ppm::kFaceVars * (size_t)a.plane;
+    at += (size_t)(ppm::kFaceVars + ppm::kFluxVars) * (size_t)a.plane;
+  }
+
+  // subgrid flux capture (single grid): requests built by build_captures, buffers
+  // placed by reserve_captures
+  if (!plan.reqs.empty()) {
+    SweepArgs& a = rec[0];
+    for (size_t k = 0; k < plan.reqs.size(); ++k)
+      plan.reqs[k].dst = (plan.cap_offset + (int64_t)k) * 6;
+    FluxCapture* dev_reqs = (FluxCapture*)ctx->captures.p + plan.cap_offset;
+    CK(cudaMemcpyAsync(dev_reqs, plan.reqs.data(), plan.reqs.size() * sizeof(FluxCapture),
                        cudaMemcpyHostToDevice, ctx->stream));
-    a.captures = (const FluxCapture*)ctx->captures.p;
-    a.ncaptures = (int64_t)reqs.size();
+    a.captures = dev_reqs;
+    a.ncaptures = (int64_t)plan.reqs.size();
     a.capture_buf = (double*)ctx->capture_buf.p;
   }
 
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-  if (ctx->profiling) {
-    while (ctx->ev_pool.size() < ctx->ev_used + 2) {
+  // descriptor image: records | march prefix | riemann prefix
+  std::vector<unsigned char> img;
+  append(img, rec.data(), rec.size());
+  const size_t off_m = align256(img.size());
+  img.resize(off_m);
+  append(img, mpre.data(), mpre.size());
+  const size_t off_r = align256(img.size());
+  img.resize(off_r);
+  append(img, rpre.data(), rpre.size());
+  const int slot = kSlotSweep0 + 3 * dim + position;
+  rc = mirror_put(ctx, ctx->mirror[slot], img);
+  if (rc) return rc;
+  unsigned char* base = (unsigned char*)ctx->mirror[slot].dev.p;
+  std::memset(&plan.B.one, 0, sizeof(plan.B.one));
+  if (ng == 1) plan.B.one = rec[0];
+  plan.B.grids = (const SweepArgs*)base;
+  plan.B.ngrids = ng;
+  plan.B.march_prefix = (const int64_t*)(base + off_m);
+  plan.B.riemann_prefix = (const int64_t*)(base + off_r);
+  plan.B.counters = (unsigned long long*)ctx->counters.p;
+  plan.B.flagged = (int64_t*)(scratch + scratch_doubles);
+  plan.march_blocks = mpre[ng];
+  plan.riemann_blocks = rpre[ng];
+  return PPM_B200_OK;
+}
+
+int enqueue_sweep(ppm_b200_context* ctx, const SweepPlan& plan, const ppm_b200_params* p,
+                  bool capturing) {
+  cudaEvent_t* ev = nullptr;
+  if (ctx->profiling && !capturing) {
+    while (ctx->ev_pool.size() < ctx->ev_used + kSweepEvents) {
       cudaEvent_t e;
       CK(cudaEventCreate(&e));
       ctx->ev_pool.push_back(e);
     }
-    ev0 = ctx->ev_pool[ctx->ev_used++];
-    ev1 = ctx->ev_pool[ctx->ev_used++];
-    CK(cudaEventRecord(ev0, ctx->stream));
+    ev = &ctx->ev_pool[ctx->ev_used];
+    ctx->ev_used += kSweepEvents;
   }
-  a.plane = (int64_t)(a.ie - a.is + 2) * a.npencils;
-  const size_t planes = (size_t)(ppm::kFaceVars + ppm::kFluxVars) * (size_t)a.plane;
-  const size_t need = planes * sizeof(double) + (size_t)a.npencils * sizeof(int64_t);
-  rc = ensure(ctx, ctx->face_scratch, need);
-  if (rc) return rc;
-  a.fstate = (double*)ctx->face_scratch.p;
-  a.fflux = a.fstate + (size_t)ppm::kFaceVars * (size_t)a.plane;
-  a.flagged = (int64_t*)(a.fstate + planes);
-  ppm::launch_sweep_split(a, p->dual_energy != 0, p->gravity != 0, ctx->stream);
+  ppm::launch_sweep_batch(plan.B, plan.march_blocks, plan.riemann_blocks, p->dual_energy != 0,
+                          p->gravity != 0, ctx->stream, ev);
   ctx->launches += 5;
   CK(cudaGetLastError());
-  if (ev1) CK(cudaEventRecord(ev1, ctx->stream));
+  return PPM_B200_OK;
+}
 
-  if (!reqs.empty()) {
-    ctx->capture_host.resize(reqs.size() * 6);
-    CK(cudaMemcpyAsync(ctx->capture_host.data(), ctx->capture_buf.p,
-                       reqs.size() * 6 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
-    // active extents for the transverse-velocity rule (nxz/nyz/nzz > 1)
-    long long nact[3];
-    for (int d = 0; d < 3; ++d) nact[d] = d < g->rank ? g->end[d] - g->start[d] + 1 : 1;
-    // capture slot order: df, ef, uf, vf, wf, gef -> BaryonField slots
-    const int slot_of_role[3] = {2 + vu, 2 + vv, 2 + vw};
-    for (size_t k = 0; k < reqs.size(); ++k) {
-      const HostCapture& h = hreq[reqs[k].pad];
-      ppm_b200_fluxes& fx = sub[h.sub];
-      double* const* dst = h.side == 0 ? &fx.left[0][0] : &fx.right[0][0];
-      auto put = [&](int slot, double v) {
-        double* arr = dst[slot * 3 + dim];
-        if (arr) arr[h.offset] = v;
-      };
-      const double* v = &ctx->capture_host[k * 6];
-      put(0, v[0]);
-      put(1, v[1]);
-      for (int r = 0; r < 3; ++r) {
-        int comp = slot_of_role[r] - 2;
-        if (r != 0 && nact[comp] <= 1) continue;
-        if (comp >= g->rank) continue;
-        put(slot_of_role[r], v[2 + r]);
-      }
-      if (p->dual_energy) put(5, v[5]);
+int scatter_captures(ppm_b200_context* ctx, int dim, const ppm_b200_params* p,
+                     const ppm_b200_grid* g, const SweepPlan& plan, ppm_b200_fluxes* sub) {
+  if (plan.reqs.empty()) return PPM_B200_OK;
+  ctx->capture_host.resize(plan.reqs.size() * 6);
+  CK(cudaMemcpyAsync(ctx->capture_host.data(), (double*)ctx->capture_buf.p + plan.cap_offset * 6,
+                     plan.reqs.size() * 6 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  // active extents for the transverse-velocity rule (nxz/nyz/nzz > 1)
+  long long nact[3];
+  for (int d = 0; d < 3; ++d) nact[d] = d < g->rank ? g->end[d] - g->start[d] + 1 : 1;
+  const int vu = dim, vv = (dim + 1) % 3, vw = (dim + 2) % 3;
+  // capture slot order: df, ef, uf, vf, wf, gef -> BaryonField slots
+  const int slot_of_role[3] = {2 + vu, 2 + vv, 2 + vw};
+  for (size_t k = 0; k < plan.reqs.size(); ++k) {
+    const HostCapture& h = plan.hreq[plan.reqs[k].pad];
+    ppm_b200_fluxes& fx = sub[h.sub];
+    double* const* dst = h.side == 0 ? &fx.left[0][0] : &fx.right[0][0];
+    auto put = [&](int slot, double v) {
+      double* arr = dst[slot * 3 + dim];
+      if (arr) arr[h.offset] = v;
+    };
+    const double* v = &ctx->capture_host[k * 6];
+    put(0, v[0]);
+    put(1, v[1]);
+    for (int r = 0; r < 3; ++r) {
+      int comp = slot_of_role[r] - 2;
+      if (r != 0 && nact[comp] <= 1) continue;
+      if (comp >= g->rank) continue;
+      put(slot_of_role[r], v[2 + r]);
     }
+    if (p->dual_energy) put(5, v[5]);
   }
   return PPM_B200_OK;
 }
@@ -369,6 +582,307 @@ int read_counters(ppm_b200_context* ctx, ppm_b200_stats* st, int* status) {
   else if (c[ppm::kCntNonFinite]) s = PPM_B200_ERR_NONFINITE;
   if (status) *status = s;
   return PPM_B200_OK;
+}
+
+// Element descriptors of a batch (pressure, time step, ghost fill), one image slot.
+struct ElemPlan {
+  ElemBatch B;
+  int64_t size_blocks = 0, active_blocks = 0;
+};
+
+int prepare_elem(ppm_b200_context* ctx, int slot, const ppm_b200_params* p,
+                 const std::vector<GridIO>& io, bool with_cw, const int* bc, ElemPlan& plan) {
+  const int ng = (int)io.size();
+  std::vector<ElemGrid> rec(ng);
+  std::vector<int64_t> spre(ng + 1, 0), apre(ng + 1, 0);
+  // cell widths (time step only), deduplicated, in their own slot
+  std::vector<std::array<int64_t, 3>> cwoff(ng, std::array<int64_t, 3>{{-1, -1, -1}});
+  if (with_cw) {
+    std::vector<double> cws;
+    std::map<std::vector<double>, int64_t> seen;
+    for (int k = 0; k < ng; ++k)
+      for (int d = 0; d < io[k].g->rank; ++d) {
+        const ppm_b200_grid* g = io[k].g;
+        std::vector<double> key(g->cell_width[d], g->cell_width[d] + g->dims[d]);
+        auto it = seen.find(key);
+        if (it != seen.end()) {
+          cwoff[k][d] = it->second;
+        } else {
+          cwoff[k][d] = (int64_t)cws.size();
+          seen[key] = cwoff[k][d];
+          cws.insert(cws.end(), key.begin(), key.end());
+        }
+      }
+    std::vector<unsigned char> cimg;
+    append(cimg, cws.data(), cws.size());
+    int rc = mirror_put(ctx, ctx->mirror[kSlotCw], cimg);
+    if (rc) return rc;
+  }
+  const double* cw_dev = (const double*)ctx->mirror[kSlotCw].dev.p;
+  for (int k = 0; k < ng; ++k) {
+    const ppm_b200_grid* g = io[k].g;
+    ElemGrid& e = rec[k];
+    std::memset(&e, 0, sizeof(e));
+    e.d = io[k].user.f[0];
+    e.te = io[k].user.f[1];
+    e.v[0] = io[k].user.f[2];
+    e.v[1] = g->rank > 1 ? io[k].user.f[3] : nullptr;
+    e.v[2] = g->rank > 2 ? io[k].user.f[4] : nullptr;
+    e.ge = p->dual_energy ? io[k].user.f[5] : nullptr;
+    e.p = io[k].pres;
+    for (int n = 0; n < 6; ++n) e.f[n] = io[k].user.f[n];
+    if (!p->dual_energy) e.f[5] = nullptr;
+    for (int d = 0; d < 3; ++d) {
+      e.cw[d] = (with_cw && cwoff[k][d] >= 0) ? cw_dev + cwoff[k][d] : nullptr;
+      e.dims[d] = g->dims[d];
+      e.start[d] = g->start[d];
+      e.end[d] = g->end[d];
+      e.bc[d] = bc ? bc[d] : 0;
+    }
+    e.rank = g->rank;
+    e.size = grid_size(g);
+    e.active = grid_active(g);
+    spre[k + 1] = spre[k] + (e.size + 255) / 256;
+    apre[k + 1] = apre[k] + (e.active + 255) / 256;
+  }
+  std::vector<unsigned char> img;
+  append(img, rec.data(), rec.size());
+  const size_t off_s = align256(img.size());
+  img.resize(off_s);
+  append(img, spre.data(), spre.size());
+  const size_t off_a = align256(img.size());
+  img.resize(off_a);
+  append(img, apre.data(), apre.size());
+  int rc = mirror_put(ctx, ctx->mirror[slot], img);
+  if (rc) return rc;
+  unsigned char* base = (unsigned char*)ctx->mirror[slot].dev.p;
+  plan.B.grids = (const ElemGrid*)base;
+  plan.B.ngrids = ng;
+  plan.B.size_prefix = (const int64_t*)(base + off_s);
+  plan.B.active_prefix = (const int64_t*)(base + off_a);
+  plan.B.gamma = p->gamma;
+  plan.B.tiny_number = p->tiny_number;
+  plan.B.min_support = p->min_support;
+  plan.B.aye = 1.0;
+  plan.B.vg[0] = plan.B.vg[1] = plan.B.vg[2] = 0.0;
+  plan.B.min_bits = (unsigned long long*)ctx->misc.p;
+  plan.size_blocks = spre[ng];
+  plan.active_blocks = apre[ng];
+  return PPM_B200_OK;
+}
+
+// Resolve the device field set of a grid: device pointers as given, or the context's
+// device copies of host fields (copied in here; single grid only).
+int stage_in(ppm_b200_context* ctx, const ppm_b200_params* p, ppm_b200_grid* g, int memory,
+             FieldSet& fs, const double* acc[3]) {
+  double* src[6] = {g->density, g->total_energy, g->velocity[0],
+                    g->rank > 1 ? g->velocity[1] : nullptr,
+                    g->rank > 2 ? g->velocity[2] : nullptr,
+                    p->dual_energy ? g->gas_energy : nullptr};
+  const size_t bytes = (size_t)grid_size(g) * sizeof(double);
+  for (int k = 0; k < 3; ++k) acc[k] = nullptr;
+  if (memory == PPM_B200_MEM_DEVICE) {
+    for (int k = 0; k < 6; ++k) fs.f[k] = src[k];
+    for (int k = 0; k < g->rank; ++k) acc[k] = p->gravity ? g->acceleration[k] : nullptr;
+    return PPM_B200_OK;
+  }
+  if (memory != PPM_B200_MEM_HOST) return PPM_B200_ERR_INVALID;
+  for (int k = 0; k < 6; ++k) {
+    fs.f[k] = nullptr;
+    if (!src[k]) continue;
+    int rc = ensure(ctx, ctx->host_set[k], bytes);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(ctx->host_set[k].p, src[k], bytes, cudaMemcpyHostToDevice, ctx->stream));
+    fs.f[k] = (double*)ctx->host_set[k].p;
+  }
+  if (p->gravity) {
+    for (int k = 0; k < g->rank; ++k) {
+      int rc = ensure(ctx, ctx->host_acc[k], bytes);
+      if (rc) return rc;
+      CK(cudaMemcpyAsync(ctx->host_acc[k].p, g->acceleration[k], bytes, cudaMemcpyHostToDevice,
+                         ctx->stream));
+      acc[k] = (const double*)ctx->host_acc[k].p;
+    }
+  }
+  return PPM_B200_OK;
+}
+
+int stage_out(ppm_b200_context* ctx, const ppm_b200_params* p, ppm_b200_grid* g,
+              const FieldSet& fs) {
+  double* dst[6] = {g->density, g->total_energy, g->velocity[0],
+                    g->rank > 1 ? g->velocity[1] : nullptr,
+                    g->rank > 2 ? g->velocity[2] : nullptr,
+                    p->dual_energy ? g->gas_energy : nullptr};
+  const size_t bytes = (size_t)grid_size(g) * sizeof(double);
+  for (int k = 0; k < 6; ++k)
+    if (dst[k] && fs.f[k])
+      CK(cudaMemcpyAsync(dst[k], fs.f[k], bytes, cudaMemcpyDeviceToHost, ctx->stream));
+  return PPM_B200_OK;
+}
+
+// Ring sets and pressure of every grid in one allocation each.
+int assign_scratch(ppm_b200_context* ctx, std::vector<GridIO>& io) {
+  size_t ring_doubles = 0, pres_doubles = 0;
+  for (auto& x : io) {
+    int nf = 0;
+    for (int k = 0; k < 6; ++k) nf += x.user.f[k] ? 1 : 0;
+    ring_doubles += 2 * (size_t)nf * (size_t)grid_size(x.g);
+    pres_doubles += (size_t)grid_size(x.g);
+  }
+  int rc = ensure(ctx, ctx->ring, std::max<size_t>(ring_doubles, 1) * sizeof(double));
+  if (rc) return rc;
+  rc = ensure(ctx, ctx->pressure, std::max<size_t>(pres_doubles, 1) * sizeof(double));
+  if (rc) return rc;
+  double* r = (double*)ctx->ring.p;
+  double* pr = (double*)ctx->pressure.p;
+  for (auto& x : io) {
+    const size_t n = (size_t)grid_size(x.g);
+    for (int s = 0; s < 2; ++s)
+      for (int k = 0; k < 6; ++k) {
+        x.ring[s].f[k] = nullptr;
+        if (!x.user.f[k]) continue;
+        x.ring[s].f[k] = r;
+        r += n;
+      }
+    x.pres = pr;
+    pr += n;
+  }
+  return PPM_B200_OK;
+}
+
+// The sweep order of Grid_SolvePPM_DE.C:53, :86-146 (all grids of a batch share rank).
+int sweep_order(const ppm_b200_grid* g, int cycle, int order[3]) {
+  const int rank = g->rank;
+  const int nact[3] = {g->end[0] - g->start[0] + 1, rank > 1 ? g->end[1] - g->start[1] + 1 : 1,
+                       rank > 2 ? g->end[2] - g->start[2] + 1 : 1};
+  int n = 0;
+  const int ixyz = cycle % rank;
+  for (int k = ixyz; k < ixyz + rank; ++k) {
+    const int dim = k % rank;
+    if (nact[dim] > 1) order[n++] = dim;
+  }
+  return n;
+}
+
+// Plans for pressure + the sweeps of one SolvePPM_DE over a batch; captures only for a
+// single grid.  Ring: user -> S0 [-> S1] -> user; a single sweep is copied back.
+struct SolvePlan {
+  ElemPlan pressure;
+  SweepPlan sweep[3];
+  int order[3];
+  int nsweeps = 0;
+};
+
+int prepare_solve(ppm_b200_context* ctx, const ppm_b200_params* p, int cycle,
+                  std::vector<GridIO>& io, int nsub, ppm_b200_fluxes* sub, const long long ggs[3],
+                  SolvePlan& sp) {
+  int rc = assign_scratch(ctx, io);
+  if (rc) return rc;
+  rc = prepare_elem(ctx, kSlotPressure, p, io, false, nullptr, sp.pressure);
+  if (rc) return rc;
+  sp.nsweeps = sweep_order(io[0].g, cycle, sp.order);
+  for (size_t k = 1; k < io.size(); ++k) {
+    int o2[3];
+    const int n2 = sweep_order(io[k].g, cycle, o2);
+    if (n2 != sp.nsweeps) return PPM_B200_ERR_INVALID;
+    for (int s = 0; s < n2; ++s)
+      if (o2[s] != sp.order[s]) return PPM_B200_ERR_INVALID;
+  }
+  const int ng = (int)io.size();
+  for (int s = 0; s < sp.nsweeps; ++s) {
+    rc = build_captures(io[0].g, sp.order[s], ng == 1 ? nsub : 0, sub, ggs, sp.sweep[s]);
+    if (rc) return rc;
+  }
+  rc = reserve_captures(ctx, sp.sweep, sp.nsweeps);
+  if (rc) return rc;
+  // one face scratch serves the sweeps in turn: size it for the largest before any
+  // sweep records its pointers
+  size_t scratch = 0;
+  for (int s = 0; s < sp.nsweeps; ++s)
+    scratch = std::max(scratch, sweep_scratch_bytes(sp.order[s], io));
+  rc = ensure(ctx, ctx->face_scratch, scratch);
+  if (rc) return rc;
+  const void* scratch_base = ctx->face_scratch.p;
+  for (int s = 0; s < sp.nsweeps; ++s) {
+    const int in_set = (s == 0) ? -1 : (s - 1) % 2;
+    const int out_set = (s == sp.nsweeps - 1 && sp.nsweeps >= 2) ? -1 : s % 2;
+    std::vector<int> src(ng, in_set), dst(ng, out_set);
+    rc = prepare_sweep(ctx, sp.order[s], s, p, io, src, dst, sp.sweep[s]);
+    if (rc) return rc;
+  }
+  if (ctx->face_scratch.p != scratch_base) {  // would leave earlier sweeps on freed memory
+    fprintf(stderr, "ppm_b200: face scratch moved while sweeps were prepared\n");
+    return PPM_B200_ERR_CUDA;
+  }
+  return PPM_B200_OK;
+}
+
+int enqueue_solve(ppm_b200_context* ctx, const ppm_b200_params* p, const std::vector<GridIO>& io,
+                  const SolvePlan& sp, bool capturing) {
+  ppm::launch_pressure_batch(sp.pressure.B, sp.pressure.size_blocks, ctx->stream);
+  ctx->launches += 1;
+  CK(cudaGetLastError());
+  for (int s = 0; s < sp.nsweeps; ++s) {
+    int rc = enqueue_sweep(ctx, sp.sweep[s], p, capturing);
+    if (rc) return rc;
+  }
+  if (sp.nsweeps == 1) {
+    for (const auto& x : io) {
+      const size_t bytes = (size_t)grid_size(x.g) * sizeof(double);
+      for (int k = 0; k < 6; ++k)
+        if (x.user.f[k])
+          CK(cudaMemcpyAsync(x.user.f[k], x.ring[0].f[k], bytes, cudaMemcpyDeviceToDevice,
+                             ctx->stream));
+    }
+  }
+  return PPM_B200_OK;
+}
+
+// Graph key: the by-value launch arguments of a level solve (kernel parameter structs,
+// block counts, flags) and the versions of the sweep descriptor images, which hold the
+// field pointers that a one-sweep solve also copies by value.  Descriptor and table
+// contents are read by the kernels when the graph runs, so they need no key.
+template <class T>
+void key_put(std::string& k, const T& v) {
+  k.append(reinterpret_cast<const char*>(&v), sizeof(T));
+}
+
+std::string graph_key(ppm_b200_context* ctx, const ppm_b200_params* p, const SolvePlan& sp) {
+  std::string k;
+  key_put(k, p->dual_energy);
+  key_put(k, p->gravity);
+  key_put(k, sp.nsweeps);
+  const ElemBatch& e = sp.pressure.B;
+  key_put(k, e.grids);
+  key_put(k, e.ngrids);
+  key_put(k, e.size_prefix);
+  key_put(k, e.active_prefix);
+  key_put(k, e.gamma);
+  key_put(k, e.tiny_number);
+  key_put(k, e.min_support);
+  key_put(k, e.min_bits);
+  key_put(k, sp.pressure.size_blocks);
+  for (int s = 0; s < sp.nsweeps; ++s) {
+    const BatchArgs& b = sp.sweep[s].B;
+    key_put(k, sp.order[s]);
+    key_put(k, b.grids);
+    key_put(k, b.ngrids);
+    key_put(k, b.march_prefix);
+    key_put(k, b.riemann_prefix);
+    key_put(k, b.counters);
+    key_put(k, b.flagged);
+    key_put(k, sp.sweep[s].march_blocks);
+    key_put(k, sp.sweep[s].riemann_blocks);
+    key_put(k, ctx->mirror[kSlotSweep0 + 3 * sp.order[s] + s].version);
+  }
+  return k;
+}
+
+int finish_status(ppm_b200_context* ctx, ppm_b200_stats* stats) {
+  int status = PPM_B200_OK;
+  int rc = read_counters(ctx, stats, &status);
+  if (rc) return rc;
+  return status;
 }
 
 }  // namespace
@@ -411,7 +925,6 @@ int ppm_b200_create(int device, void* cuda_stream, ppm_b200_context** out) {
     }
     ctx->own_stream = true;
   }
-
   int rc = ensure(ctx, ctx->counters, ppm::kMaxCounters * sizeof(unsigned long long));
   if (!rc) rc = ensure(ctx, ctx->misc, 4 * sizeof(double));
   if (!rc) rc = cuda_fail(ctx, cudaMemset(ctx->counters.p, 0, ctx->counters.bytes), "cudaMemset");
@@ -427,23 +940,22 @@ int ppm_b200_destroy(ppm_b200_context* ctx) {
   if (!ctx) return PPM_B200_OK;
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  drop_graphs(ctx);
   auto fr = [](DevBuf& b) {
     if (b.p) cudaFree(b.p);
     b.p = nullptr;
     b.bytes = 0;
   };
-  for (auto& s : ctx->field_set)
-    for (auto& b : s) fr(b);
   for (auto& b : ctx->host_set) fr(b);
   for (auto& b : ctx->host_acc) fr(b);
+  fr(ctx->ring);
   fr(ctx->pressure);
-  for (auto& b : ctx->coef) fr(b);
-  for (auto& b : ctx->cw_dev) fr(b);
+  fr(ctx->face_scratch);
   fr(ctx->counters);
   fr(ctx->misc);
   fr(ctx->captures);
   fr(ctx->capture_buf);
-  fr(ctx->face_scratch);
+  for (auto& m : ctx->mirror) fr(m.dev);
   for (auto e : ctx->ev_pool) cudaEventDestroy(e);
   if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
@@ -463,14 +975,33 @@ int ppm_b200_profile_read(ppm_b200_context* ctx, double* sweep_ms, long long* sw
   CK(cudaSetDevice(ctx->device));
   CK(cudaStreamSynchronize(ctx->stream));
   double total = 0.0;
-  for (size_t k = 0; k + 1 < ctx->ev_used; k += 2) {
-    float ms = 0.0f;
-    CK(cudaEventElapsedTime(&ms, ctx->ev_pool[k], ctx->ev_pool[k + 1]));
-    total += ms;
+  double stage[kSweepEvents - 1] = {0, 0, 0, 0, 0};
+  for (size_t k = 0; k + kSweepEvents <= ctx->ev_used; k += kSweepEvents) {
+    for (int j = 0; j + 1 < kSweepEvents; ++j) {
+      float ms = 0.0f;
+      CK(cudaEventElapsedTime(&ms, ctx->ev_pool[k + j], ctx->ev_pool[k + j + 1]));
+      stage[j] += ms;
+      total += ms;
+    }
   }
   if (sweep_ms) *sweep_ms = total;
-  if (sweep_launches) *sweep_launches = (long long)(ctx->ev_used / 2);
+  if (sweep_launches) *sweep_launches = (long long)(ctx->ev_used / kSweepEvents);
+  for (int j = 0; j + 1 < kSweepEvents; ++j) ctx->stage_ms[j] = stage[j];
   ctx->ev_used = 0;
+  return PPM_B200_OK;
+}
+
+int ppm_b200_profile_stages(ppm_b200_context* ctx, double stage_ms[5]) {
+  if (!ctx || !stage_ms) return PPM_B200_ERR_INVALID;
+  for (int j = 0; j < 5; ++j) stage_ms[j] = ctx->stage_ms[j];
+  return PPM_B200_OK;
+}
+
+int ppm_b200_set_graphs(ppm_b200_context* ctx, int enable) {
+  if (!ctx) return PPM_B200_ERR_INVALID;
+  if (!enable && !ctx->graphs.empty()) CK(cudaStreamSynchronize(ctx->stream));
+  ctx->use_graphs = enable != 0;
+  if (!ctx->use_graphs) drop_graphs(ctx);
   return PPM_B200_OK;
 }
 
@@ -489,80 +1020,6 @@ int ppm_b200_synchronize(ppm_b200_context* ctx, ppm_b200_stats* stats) {
   return status;
 }
 
-// Resolve the device field set of a call: device pointers as given, or the context's
-// device copies of host fields (copied in here).
-static int stage_in(ppm_b200_context* ctx, const ppm_b200_params* p, ppm_b200_grid* g, int memory,
-                    FieldSet& fs, const double* acc[3]) {
-  double* src[6] = {g->density, g->total_energy, g->velocity[0],
-                    g->rank > 1 ? g->velocity[1] : nullptr,
-                    g->rank > 2 ? g->velocity[2] : nullptr,
-                    p->dual_energy ? g->gas_energy : nullptr};
-  const size_t bytes = (size_t)grid_size(g) * sizeof(double);
-  for (int k = 0; k < 3; ++k) acc[k] = nullptr;
-  if (memory == PPM_B200_MEM_DEVICE) {
-    for (int k = 0; k < 6; ++k) fs.f[k] = src[k];
-    for (int k = 0; k < g->rank; ++k) acc[k] = p->gravity ? g->acceleration[k] : nullptr;
-    return PPM_B200_OK;
-  }
-  if (memory != PPM_B200_MEM_HOST) return PPM_B200_ERR_INVALID;
-  for (int k = 0; k < 6; ++k) {
-    fs.f[k] = nullptr;
-    if (!src[k]) continue;
-    int rc = ensure(ctx, ctx->host_set[k], bytes);
-    if (rc) return rc;
-    CK(cudaMemcpyAsync(ctx->host_set[k].p, src[k], bytes, cudaMemcpyHostToDevice, ctx->stream));
-    fs.f[k] = (double*)ctx->host_set[k].p;
-  }
-  if (p->gravity) {
-    for (int k = 0; k < g->rank; ++k) {
-      int rc = ensure(ctx, ctx->host_acc[k], bytes);
-      if (rc) return rc;
-      CK(cudaMemcpyAsync(ctx->host_acc[k].p, g->acceleration[k], bytes, cudaMemcpyHostToDevice,
-                         ctx->stream));
-      acc[k] = (const double*)ctx->host_acc[k].p;
-    }
-  }
-  return PPM_B200_OK;
-}
-
-static int stage_out(ppm_b200_context* ctx, const ppm_b200_params* p, ppm_b200_grid* g,
-                     const FieldSet& fs) {
-  double* dst[6] = {g->density, g->total_energy, g->velocity[0],
-                    g->rank > 1 ? g->velocity[1] : nullptr,
-                    g->rank > 2 ? g->velocity[2] : nullptr,
-                    p->dual_energy ? g->gas_energy : nullptr};
-  const size_t bytes = (size_t)grid_size(g) * sizeof(double);
-  for (int k = 0; k < 6; ++k)
-    if (dst[k] && fs.f[k])
-      CK(cudaMemcpyAsync(dst[k], fs.f[k], bytes, cudaMemcpyDeviceToHost, ctx->stream));
-  return PPM_B200_OK;
-}
-
-static int scratch_sets(ppm_b200_context* ctx, const ppm_b200_params* p, const ppm_b200_grid* g,
-                        const FieldSet& user, FieldSet out[2]) {
-  const size_t bytes = (size_t)grid_size(g) * sizeof(double);
-  for (int s = 0; s < 2; ++s)
-    for (int k = 0; k < 6; ++k) {
-      out[s].f[k] = nullptr;
-      if (!user.f[k]) continue;
-      int rc = ensure(ctx, ctx->field_set[s][k], bytes);
-      if (rc) return rc;
-      out[s].f[k] = (double*)ctx->field_set[s][k].p;
-    }
-  return PPM_B200_OK;
-}
-
-static int pressure_into(ppm_b200_context* ctx, const ppm_b200_params* p, const ppm_b200_grid* g,
-                         const FieldSet& fs, double* pres) {
-  ppm::launch_pressure_plain(fs.f[0], fs.f[1], fs.f[2], g->rank > 1 ? fs.f[3] : nullptr,
-                             g->rank > 2 ? fs.f[4] : nullptr, p->dual_energy ? fs.f[5] : nullptr,
-                             pres, grid_size(g), p->gamma, p->tiny_number, p->min_support,
-                             ctx->sms, ctx->stream);
-  ctx->launches += 1;
-  CK(cudaGetLastError());
-  return PPM_B200_OK;
-}
-
 int ppm_b200_solve_ppm_de(ppm_b200_context* ctx, const ppm_b200_params* p, int cycle_number,
                           ppm_b200_grid* g, int memory, int nsub, ppm_b200_fluxes* sub,
                           const long long ggs_in[3], ppm_b200_stats* stats) {
@@ -575,57 +1032,83 @@ int ppm_b200_solve_ppm_de(ppm_b200_context* ctx, const ppm_b200_params* p, int c
   CK(cudaSetDevice(ctx->device));
   const long long zero3[3] = {0, 0, 0};
   const long long* ggs = ggs_in ? ggs_in : zero3;
-
-  FieldSet user;
-  const double* acc[3];
-  rc = stage_in(ctx, p, g, memory, user, acc);
+  std::vector<GridIO> io(1);
+  io[0].g = g;
+  rc = stage_in(ctx, p, g, memory, io[0].user, io[0].acc);
   if (rc) return rc;
-  FieldSet ring[2];
-  rc = scratch_sets(ctx, p, g, user, ring);
+  SolvePlan sp;
+  rc = prepare_solve(ctx, p, cycle_number, io, nsub, sub, ggs, sp);
   if (rc) return rc;
-  rc = ensure(ctx, ctx->pressure, (size_t)grid_size(g) * sizeof(double));
+  rc = enqueue_solve(ctx, p, io, sp, false);
   if (rc) return rc;
-  double* pres = (double*)ctx->pressure.p;
-  rc = pressure_into(ctx, p, g, user, pres);
-  if (rc) return rc;
-
-  // sweep order rotation, Grid_SolvePPM_DE.C:53 and :86-146
-  const int rank = g->rank;
-  const int nact[3] = {g->end[0] - g->start[0] + 1, rank > 1 ? g->end[1] - g->start[1] + 1 : 1,
-                       rank > 2 ? g->end[2] - g->start[2] + 1 : 1};
-  int order[3], nsweeps = 0;
-  const int ixyz = cycle_number % rank;
-  for (int n = ixyz; n < ixyz + rank; ++n) {
-    const int dim = n % rank;
-    if (nact[dim] > 1) order[nsweeps++] = dim;
-  }
-  // out-of-place ring: user -> S0 [-> S1] -> user; the last of two or three sweeps
-  // writes the caller's arrays directly, a single sweep is copied back.
-  const FieldSet* cur = &user;
-  for (int s = 0; s < nsweeps; ++s) {
-    const FieldSet* dst;
-    if (s == nsweeps - 1 && nsweeps >= 2) dst = &user;
-    else dst = &ring[s % 2];
-    rc = run_sweep(ctx, order[s], p, g, *cur, *dst, pres, acc, nsub, sub, ggs);
+  for (int s = 0; s < sp.nsweeps; ++s) {
+    rc = scatter_captures(ctx, sp.order[s], p, g, sp.sweep[s], sub);
     if (rc) return rc;
-    cur = dst;
-  }
-  if (cur != &user) {
-    const size_t bytes = (size_t)grid_size(g) * sizeof(double);
-    for (int k = 0; k < 6; ++k)
-      if (user.f[k])
-        CK(cudaMemcpyAsync(user.f[k], cur->f[k], bytes, cudaMemcpyDeviceToDevice, ctx->stream));
   }
   if (memory == PPM_B200_MEM_HOST) {
-    rc = stage_out(ctx, p, g, user);
+    rc = stage_out(ctx, p, g, io[0].user);
     if (rc) return rc;
   }
-  if (memory == PPM_B200_MEM_HOST || stats || nsub > 0) {
-    int status = PPM_B200_OK;
-    rc = read_counters(ctx, stats, &status);
+  if (memory == PPM_B200_MEM_HOST || stats || nsub > 0) return finish_status(ctx, stats);
+  return PPM_B200_OK;
+}
+
+int ppm_b200_solve_level(ppm_b200_context* ctx, const ppm_b200_params* p, int cycle_number,
+                         ppm_b200_grid* grids, int ngrids, ppm_b200_stats* stats) {
+  if (!ctx || !p || !grids || ngrids <= 0) return PPM_B200_ERR_INVALID;
+  int rc = check_supported(p);
+  if (rc) return rc;
+  for (int k = 0; k < ngrids; ++k) {
+    rc = check_grid(&grids[k], p);
     if (rc) return rc;
-    return status;
+    if (grids[k].rank != grids[0].rank) return PPM_B200_ERR_INVALID;
   }
+  CK(cudaSetDevice(ctx->device));
+  // largest grids first: the block scheduler then starts the longest pencils first
+  std::vector<int> idx(ngrids);
+  for (int k = 0; k < ngrids; ++k) idx[k] = k;
+  std::stable_sort(idx.begin(), idx.end(),
+                   [&](int x, int y) { return grid_size(&grids[x]) > grid_size(&grids[y]); });
+  std::vector<GridIO> io(ngrids);
+  for (int k = 0; k < ngrids; ++k) {
+    io[k].g = &grids[idx[k]];
+    rc = stage_in(ctx, p, &grids[idx[k]], PPM_B200_MEM_DEVICE, io[k].user, io[k].acc);
+    if (rc) return rc;
+  }
+  SolvePlan sp;
+  rc = prepare_solve(ctx, p, cycle_number, io, 0, nullptr, nullptr, sp);
+  if (rc) return rc;
+  // graph replay needs every per-step value on the device (dt included)
+  const bool graph = ctx->use_graphs && p->dt_device != nullptr && !ctx->profiling;
+  if (graph) {
+    const std::string key = graph_key(ctx, p, sp);
+    auto it = ctx->graphs.find(key);
+    if (it == ctx->graphs.end()) {
+      if (ctx->graphs.size() >= kMaxGraphs) {
+        CK(cudaStreamSynchronize(ctx->stream));
+        drop_graphs(ctx);
+      }
+      cudaGraph_t gr;
+      CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+      const long long before = ctx->launches;
+      rc = enqueue_solve(ctx, p, io, sp, true);
+      cudaError_t e = cudaStreamEndCapture(ctx->stream, &gr);
+      if (rc) return rc;
+      if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaStreamEndCapture");
+      cudaGraphExec_t ex;
+      e = cudaGraphInstantiate(&ex, gr, 0);
+      cudaGraphDestroy(gr);
+      if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaGraphInstantiate");
+      ctx->launches = before;  // counted when the graph runs
+      it = ctx->graphs.emplace(key, ex).first;
+    }
+    CK(cudaGraphLaunch(it->second, ctx->stream));
+    ctx->launches += 1 + 5 * sp.nsweeps;
+  } else {
+    rc = enqueue_solve(ctx, p, io, sp, false);
+    if (rc) return rc;
+  }
+  if (stats) return finish_status(ctx, stats);
   return PPM_B200_OK;
 }
 
@@ -641,37 +1124,40 @@ int ppm_b200_euler_sweep(ppm_b200_context* ctx, int dim, const ppm_b200_params* 
   CK(cudaSetDevice(ctx->device));
   const long long zero3[3] = {0, 0, 0};
   const long long* ggs = ggs_in ? ggs_in : zero3;
-  FieldSet user;
-  const double* acc[3];
-  rc = stage_in(ctx, p, g, memory, user, acc);
+  std::vector<GridIO> io(1);
+  io[0].g = g;
+  rc = stage_in(ctx, p, g, memory, io[0].user, io[0].acc);
   if (rc) return rc;
-  FieldSet ring[2];
-  rc = scratch_sets(ctx, p, g, user, ring);
+  rc = assign_scratch(ctx, io);
   if (rc) return rc;
-  const double* pres = pressure;
   if (memory == PPM_B200_MEM_HOST) {
-    rc = ensure(ctx, ctx->pressure, (size_t)grid_size(g) * sizeof(double));
-    if (rc) return rc;
-    CK(cudaMemcpyAsync(ctx->pressure.p, pressure, (size_t)grid_size(g) * sizeof(double),
+    CK(cudaMemcpyAsync(io[0].pres, pressure, (size_t)grid_size(g) * sizeof(double),
                        cudaMemcpyHostToDevice, ctx->stream));
-    pres = (const double*)ctx->pressure.p;
+  } else {
+    io[0].pres = const_cast<double*>(pressure);
   }
-  rc = run_sweep(ctx, dim, p, g, user, ring[0], pres, acc, nsub, sub, ggs);
+  SweepPlan plan;
+  rc = build_captures(g, dim, nsub, sub, ggs, plan);
+  if (rc) return rc;
+  rc = reserve_captures(ctx, &plan, 1);
+  if (rc) return rc;
+  std::vector<int> src(1, -1), dst(1, 0);
+  rc = prepare_sweep(ctx, dim, 0, p, io, src, dst, plan);
+  if (rc) return rc;
+  rc = enqueue_sweep(ctx, plan, p, false);
+  if (rc) return rc;
+  rc = scatter_captures(ctx, dim, p, g, plan, sub);
   if (rc) return rc;
   const size_t bytes = (size_t)grid_size(g) * sizeof(double);
   for (int k = 0; k < 6; ++k)
-    if (user.f[k])
-      CK(cudaMemcpyAsync(user.f[k], ring[0].f[k], bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+    if (io[0].user.f[k])
+      CK(cudaMemcpyAsync(io[0].user.f[k], io[0].ring[0].f[k], bytes, cudaMemcpyDeviceToDevice,
+                         ctx->stream));
   if (memory == PPM_B200_MEM_HOST) {
-    rc = stage_out(ctx, p, g, user);
+    rc = stage_out(ctx, p, g, io[0].user);
     if (rc) return rc;
   }
-  if (memory == PPM_B200_MEM_HOST || stats || nsub > 0) {
-    int status = PPM_B200_OK;
-    rc = read_counters(ctx, stats, &status);
-    if (rc) return rc;
-    return status;
-  }
+  if (memory == PPM_B200_MEM_HOST || stats || nsub > 0) return finish_status(ctx, stats);
   return PPM_B200_OK;
 }
 
@@ -681,21 +1167,50 @@ int ppm_b200_compute_pressure(ppm_b200_context* ctx, const ppm_b200_params* p, p
   int rc = check_grid(g, p);
   if (rc) return rc;
   CK(cudaSetDevice(ctx->device));
-  FieldSet user;
-  const double* acc[3];
-  rc = stage_in(ctx, p, g, memory, user, acc);
+  std::vector<GridIO> io(1);
+  io[0].g = g;
+  rc = stage_in(ctx, p, g, memory, io[0].user, io[0].acc);
   if (rc) return rc;
-  double* out = pressure;
   if (memory == PPM_B200_MEM_HOST) {
     rc = ensure(ctx, ctx->pressure, (size_t)grid_size(g) * sizeof(double));
     if (rc) return rc;
-    out = (double*)ctx->pressure.p;
+    io[0].pres = (double*)ctx->pressure.p;
+  } else {
+    io[0].pres = pressure;
   }
-  rc = pressure_into(ctx, p, g, user, out);
+  ElemPlan ep;
+  rc = prepare_elem(ctx, kSlotPressure, p, io, false, nullptr, ep);
   if (rc) return rc;
+  ppm::launch_pressure_batch(ep.B, ep.size_blocks, ctx->stream);
+  ctx->launches += 1;
+  CK(cudaGetLastError());
   if (memory == PPM_B200_MEM_HOST) {
-    CK(cudaMemcpyAsync(pressure, out, (size_t)grid_size(g) * sizeof(double),
+    CK(cudaMemcpyAsync(pressure, io[0].pres, (size_t)grid_size(g) * sizeof(double),
                        cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+  }
+  return PPM_B200_OK;
+}
+
+static int timestep_batch(ppm_b200_context* ctx, const ppm_b200_params* p,
+                          std::vector<GridIO>& io, double courant, double aye,
+                          const double vgrid_in[3], double* dt_device, double* dt_host) {
+  for (auto& x : io)
+    for (int d = 0; d < x.g->rank; ++d)
+      if (!x.g->cell_width[d]) return PPM_B200_ERR_INVALID;
+  ElemPlan ep;
+  int rc = prepare_elem(ctx, kSlotTimestep, p, io, true, nullptr, ep);
+  if (rc) return rc;
+  const double zero3[3] = {0.0, 0.0, 0.0};
+  const double* vg = vgrid_in ? vgrid_in : zero3;
+  ep.B.aye = aye;
+  for (int d = 0; d < 3; ++d) ep.B.vg[d] = vg[d];
+  double* dt_slot = dt_device ? dt_device : ((double*)ctx->misc.p) + 1;
+  ppm::launch_timestep_batch(ep.B, ep.active_blocks, courant, dt_slot, ctx->stream);
+  ctx->launches += 2;
+  CK(cudaGetLastError());
+  if (dt_host) {
+    CK(cudaMemcpyAsync(dt_host, dt_slot, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
   }
   return PPM_B200_OK;
@@ -708,54 +1223,66 @@ int ppm_b200_compute_timestep(ppm_b200_context* ctx, const ppm_b200_params* p, p
   int rc = check_grid(g, p);
   if (rc) return rc;
   CK(cudaSetDevice(ctx->device));
-  FieldSet user;
-  const double* acc[3];
-  rc = stage_in(ctx, p, g, memory, user, acc);
+  std::vector<GridIO> io(1);
+  io[0].g = g;
+  rc = stage_in(ctx, p, g, memory, io[0].user, io[0].acc);
   if (rc) return rc;
-  const double* cw[3] = {nullptr, nullptr, nullptr};
-  for (int d = 0; d < g->rank; ++d) {
-    if (!g->cell_width[d]) return PPM_B200_ERR_INVALID;
-    rc = upload_cw(ctx, d, g);
+  return timestep_batch(ctx, p, io, courant, aye, vgrid_in, dt_device, dt_host);
+}
+
+int ppm_b200_compute_timestep_level(ppm_b200_context* ctx, const ppm_b200_params* p,
+                                    ppm_b200_grid* grids, int ngrids, double courant, double aye,
+                                    const double vgrid[3], double* dt_device, double* dt_host) {
+  if (!ctx || !p || !grids || ngrids <= 0) return PPM_B200_ERR_INVALID;
+  CK(cudaSetDevice(ctx->device));
+  std::vector<GridIO> io(ngrids);
+  for (int k = 0; k < ngrids; ++k) {
+    int rc = check_grid(&grids[k], p);
     if (rc) return rc;
-    cw[d] = (const double*)ctx->cw_dev[d].p;
+    io[k].g = &grids[k];
+    rc = stage_in(ctx, p, &grids[k], PPM_B200_MEM_DEVICE, io[k].user, io[k].acc);
+    if (rc) return rc;
   }
-  const double zero3[3] = {0.0, 0.0, 0.0};
-  const double* vg = vgrid_in ? vgrid_in : zero3;
-  unsigned long long* min_bits = (unsigned long long*)ctx->misc.p;
-  double* dt_slot = dt_device ? dt_device : ((double*)ctx->misc.p) + 1;
-  const double* vel[3] = {user.f[2], g->rank > 1 ? user.f[3] : nullptr,
-                          g->rank > 2 ? user.f[4] : nullptr};
-  ppm::launch_timestep_plain(user.f[0], user.f[1], vel, p->dual_energy ? user.f[5] : nullptr,
-                             g->rank, g->dims, g->start, g->end, p->gamma, p->tiny_number,
-                             p->min_support, aye, vg, cw, min_bits, courant, dt_slot, ctx->sms,
-                             ctx->stream);
-  ctx->launches += 2;
+  return timestep_batch(ctx, p, io, courant, aye, vgrid, dt_device, dt_host);
+}
+
+static int boundary_batch(ppm_b200_context* ctx, ppm_b200_grid* grids, int ngrids,
+                          int dual_energy, const int bc_type[3]) {
+  if (!ctx || !grids || ngrids <= 0 || !bc_type) return PPM_B200_ERR_INVALID;
+  for (int d = 0; d < 3; ++d)
+    if (bc_type[d] != 0 && bc_type[d] != 1) return PPM_B200_ERR_INVALID;
+  CK(cudaSetDevice(ctx->device));
+  ppm_b200_params p;
+  std::memset(&p, 0, sizeof(p));
+  p.dual_energy = dual_energy;
+  std::vector<GridIO> io(ngrids);
+  for (int k = 0; k < ngrids; ++k) {
+    ppm_b200_grid* g = &grids[k];
+    if (!g->density || !g->total_energy || !g->velocity[0]) return PPM_B200_ERR_INVALID;
+    for (int d = 1; d < g->rank; ++d)
+      if (!g->velocity[d]) return PPM_B200_ERR_INVALID;
+    if (dual_energy && !g->gas_energy) return PPM_B200_ERR_INVALID;
+    io[k].g = g;
+    int rc = stage_in(ctx, &p, g, PPM_B200_MEM_DEVICE, io[k].user, io[k].acc);
+    if (rc) return rc;
+  }
+  ElemPlan ep;
+  int rc = prepare_elem(ctx, kSlotBoundary, &p, io, false, bc_type, ep);
+  if (rc) return rc;
+  ppm::launch_boundary_batch(ep.B, ep.size_blocks, ctx->stream);
+  ctx->launches += 1;
   CK(cudaGetLastError());
-  if (dt_host) {
-    CK(cudaMemcpyAsync(dt_host, dt_slot, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
-  }
   return PPM_B200_OK;
 }
 
 int ppm_b200_set_boundary(ppm_b200_context* ctx, ppm_b200_grid* g, int dual_energy,
                           const int bc_type[3]) {
-  if (!ctx || !g || !bc_type) return PPM_B200_ERR_INVALID;
-  CK(cudaSetDevice(ctx->device));
-  double* f[6];
-  int nf = 0;
-  f[nf++] = g->density;
-  f[nf++] = g->total_energy;
-  for (int d = 0; d < g->rank; ++d) f[nf++] = g->velocity[d];
-  if (dual_energy) f[nf++] = g->gas_energy;
-  for (int k = 0; k < nf; ++k)
-    if (!f[k]) return PPM_B200_ERR_INVALID;
-  for (int d = 0; d < 3; ++d)
-    if (bc_type[d] != 0 && bc_type[d] != 1) return PPM_B200_ERR_INVALID;
-  ppm::launch_boundary_plain(f, nf, g->dims, g->start, g->end, bc_type, ctx->sms, ctx->stream);
-  ctx->launches += 1;
-  CK(cudaGetLastError());
-  return PPM_B200_OK;
+  return boundary_batch(ctx, g, 1, dual_energy, bc_type);
+}
+
+int ppm_b200_set_boundary_level(ppm_b200_context* ctx, ppm_b200_grid* grids, int ngrids,
+                                int dual_energy, const int bc_type[3]) {
+  return boundary_batch(ctx, grids, ngrids, dual_energy, bc_type);
 }
 
 }  // extern "C"

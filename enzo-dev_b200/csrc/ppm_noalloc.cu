@@ -7,7 +7,7 @@
 // synchronise the device or deadlock, or embedded drivers that reserve all memory up
 // front.  Such a caller still provides its own input and output arrays; this entry
 // point takes the sweep's scratch (the interface-state and flux planes, the inteuler
-// coefficient table and the status counters) from a fixed array compiled into the
+// coefficient table, the grid record the kernels read and the status counters) from a fixed array compiled into the
 // library instead of from cudaMalloc.
 //
 // Properties a caller must know:
@@ -37,7 +37,8 @@
 #include "ppm_sweep.cuh"
 
 namespace ppm {
-void launch_sweep_split(const SweepArgs& a, bool dual, bool grav, cudaStream_t st);
+void launch_sweep_batch(const BatchArgs& B, int64_t march_blocks, int64_t riemann_blocks,
+                        bool dual, bool grav, cudaStream_t st, cudaEvent_t* ev);
 }
 
 namespace {
@@ -45,9 +46,12 @@ namespace {
 constexpr size_t kStaticCounterBytes = 256;                       // kMaxCounters counters
 constexpr int kStaticCoefEntries = 1031;                          // longest pencil (fortran.def:1)
 constexpr size_t kStaticCoefBytes = 66560;                        // >= 1031 * sizeof(Coef), 256-aligned
+constexpr size_t kStaticDescBytes = 1024;                         // grid record + block prefixes
 constexpr size_t kStaticPlaneBytes = size_t(48) << 20;            // interface states + fluxes
-constexpr size_t kStaticBytes = kStaticCounterBytes + kStaticCoefBytes + kStaticPlaneBytes;
+constexpr size_t kStaticBytes =
+    kStaticCounterBytes + kStaticCoefBytes + kStaticDescBytes + kStaticPlaneBytes;
 static_assert(kStaticCoefEntries * sizeof(ppm::Coef) <= kStaticCoefBytes, "coef area");
+static_assert(sizeof(ppm::SweepArgs) <= 512, "descriptor area");
 
 constexpr int kMaxDevices = 64;
 
@@ -172,7 +176,8 @@ extern "C" int ppm_b200_euler_sweep_static(int dim, const ppm_b200_params* p,
   if (rc) return rc;
   unsigned long long* counters = reinterpret_cast<unsigned long long*>(base);
   ppm::Coef* coef = reinterpret_cast<ppm::Coef*>(base + kStaticCounterBytes);
-  double* planes = reinterpret_cast<double*>(base + kStaticCounterBytes + kStaticCoefBytes);
+  unsigned char* desc = base + kStaticCounterBytes + kStaticCoefBytes;
+  double* planes = reinterpret_cast<double*>(desc + kStaticDescBytes);
   cudaStream_t st = static_cast<cudaStream_t>(cuda_stream);
 
   // ---- per-call contents: counters start at zero, the coefficient table is rewritten
@@ -210,12 +215,32 @@ extern "C" int ppm_b200_euler_sweep_static(int dim, const ppm_b200_params* p,
   a.small_rho = p->small_rho;
   a.pmin = p->tiny_number;
   a.fallback = p->riemann_fallback;
-  a.counters = counters;
   a.fstate = planes;
   a.fflux = planes + (size_t)ppm::kFaceVars * (size_t)a.plane;
-  a.flagged = reinterpret_cast<int64_t*>(planes + (size_t)(ppm::kFaceVars + ppm::kFluxVars) *
+
+  // a batch of one grid: its record and block prefix tables go into the descriptor area
+  const int64_t march_blocks = (a.npencils + ppm::kMarchThreads - 1) / ppm::kMarchThreads;
+  const int64_t riemann_blocks =
+      (int64_t)(a.ie - a.is + 2) * ((a.npencils + ppm::kRiemannThreads - 1) / ppm::kRiemannThreads);
+  unsigned char img[kStaticDescBytes];
+  std::memset(img, 0, sizeof(img));
+  std::memcpy(img, &a, sizeof(a));
+  const int64_t mpre[2] = {0, march_blocks}, rpre[2] = {0, riemann_blocks};
+  std::memcpy(img + 512, mpre, sizeof(mpre));
+  std::memcpy(img + 768, rpre, sizeof(rpre));
+  e = cudaMemcpyAsync(desc, img, sizeof(img), cudaMemcpyHostToDevice, st);
+  if (e != cudaSuccess) return fail_cuda(e, "cudaMemcpyAsync");
+  ppm::BatchArgs B;
+  B.one = a;
+  B.grids = reinterpret_cast<const ppm::SweepArgs*>(desc);
+  B.ngrids = 1;
+  B.march_prefix = reinterpret_cast<const int64_t*>(desc + 512);
+  B.riemann_prefix = reinterpret_cast<const int64_t*>(desc + 768);
+  B.counters = counters;
+  B.flagged = reinterpret_cast<int64_t*>(planes + (size_t)(ppm::kFaceVars + ppm::kFluxVars) *
                                                       (size_t)a.plane);
-  ppm::launch_sweep_split(a, p->dual_energy != 0, p->gravity != 0, st);
+  ppm::launch_sweep_batch(B, march_blocks, riemann_blocks, p->dual_energy != 0, p->gravity != 0,
+                          st, nullptr);
   e = cudaGetLastError();
   if (e != cudaSuccess) return fail_cuda(e, "sweep launch");
 

@@ -31,6 +31,35 @@ __device__ __forceinline__ double ldg0(const double* __restrict__ p, int64_t off
   return p ? __ldg(p + off) : 0.0;
 }
 
+// Every thread of a block works on the same grid.  A batch of one grid (ONE) reads its
+// record from the kernel parameters, where the compiler uses the fields as constant
+// operands; a larger batch copies the block's record from the device array into shared
+// memory once per block.  (Reading the record through a reference into global memory
+// or as a by-value copy measured slower: the marching loops then hold the fields in
+// registers and spill.)
+__device__ __forceinline__ void load_record(SweepArgs& dst, const SweepArgs* src) {
+  const unsigned long long* s = reinterpret_cast<const unsigned long long*>(src);
+  unsigned long long* d = reinterpret_cast<unsigned long long*>(&dst);
+  for (int i = threadIdx.x; i < (int)(sizeof(SweepArgs) / 8); i += blockDim.x) d[i] = __ldg(s + i);
+}
+
+template <bool ONE>
+__device__ __forceinline__ int locate(const int64_t* prefix, int ngrids, int64_t& lb) {
+  if (ONE) {
+    lb = blockIdx.x;
+    return 0;
+  }
+  return batch_locate(prefix, ngrids, blockIdx.x, lb);
+}
+
+#define PPM_BIND_RECORD(name, g)           \
+  __shared__ SweepArgs s_rec_;             \
+  if (!ONE) {                              \
+    load_record(s_rec_, B.grids + (g));    \
+    __syncthreads();                       \
+  }                                        \
+  const SweepArgs& name = ONE ? B.one : s_rec_;
+
 __device__ __forceinline__ Phys make_phys(const SweepArgs& a) {
   Phys P;
   P.gamma = a.gamma;
@@ -56,11 +85,14 @@ __device__ __forceinline__ Phys make_phys(const SweepArgs& a) {
 #define PPM_RECON_MINBLOCKS 4
 #endif
 
-template <bool DUAL, bool GRAV, int ROLE>
-__global__ void __launch_bounds__(128, PPM_RECON_MINBLOCKS)
-    reconstruct_kernel(const __grid_constant__ SweepArgs a) {
+template <bool DUAL, bool GRAV, int ROLE, bool ONE>
+__global__ void __launch_bounds__(kMarchThreads, PPM_RECON_MINBLOCKS)
+    reconstruct_kernel(const __grid_constant__ BatchArgs B) {
   constexpr int NV = (ROLE == 0) ? 3 : (DUAL ? 3 : 2);
-  const int64_t pid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  int64_t lb;
+  const int g = locate<ONE>(B.march_prefix, B.ngrids, lb);
+  PPM_BIND_RECORD(a, g)
+  const int64_t pid = lb * kMarchThreads + threadIdx.x;
   if (pid >= a.npencils) return;
   const Phys P = make_phys(a);
   const int64_t base = (pid % a.n1) * a.s1 + (pid / a.n1) * a.s2;
@@ -239,16 +271,20 @@ __device__ __forceinline__ FaceState load_face(const SweepArgs& a, int64_t idx) 
 }
 
 // ------------------------------------------------------------------ stage 2
-// grid: x over pencils, y over faces (fi = face - is)
-template <bool DUAL>
-__global__ void __launch_bounds__(256) riemann_kernel(const __grid_constant__ SweepArgs a) {
+// per grid, blocks over (face plane fi = face - is) x (chunks of pencils)
+template <bool DUAL, bool ONE>
+__global__ void __launch_bounds__(kRiemannThreads) riemann_kernel(const __grid_constant__ BatchArgs B) {
   __shared__ unsigned int s_hist[8];
   __shared__ unsigned int s_newton;
   if (threadIdx.x < 8) s_hist[threadIdx.x] = 0u;
   if (threadIdx.x == 0) s_newton = 0u;
-  __syncthreads();
-  const int64_t pid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const int fi = blockIdx.y;
+  int64_t lb;
+  const int g = locate<ONE>(B.riemann_prefix, B.ngrids, lb);
+  PPM_BIND_RECORD(a, g)
+  if (ONE) __syncthreads();
+  const int64_t chunks = (a.npencils + kRiemannThreads - 1) / kRiemannThreads;
+  const int fi = (int)(lb / chunks);
+  const int64_t pid = (lb - (int64_t)fi * chunks) * kRiemannThreads + threadIdx.x;
   if (pid < a.npencils) {
     const Phys P = make_phys(a);
     const int64_t idx = (int64_t)fi * a.npencils + pid;
@@ -273,12 +309,12 @@ __global__ void __launch_bounds__(256) riemann_kernel(const __grid_constant__ Sw
   }
   __syncthreads();
   if (threadIdx.x < 8 && s_hist[threadIdx.x])
-    atomicAdd(&a.counters[kCntHist0 + threadIdx.x], (unsigned long long)s_hist[threadIdx.x]);
+    atomicAdd(&B.counters[kCntHist0 + threadIdx.x], (unsigned long long)s_hist[threadIdx.x]);
   if (threadIdx.x == 8 && s_newton) {
     unsigned long long nif = 0;
     for (int h = 0; h < 8; ++h) nif += s_hist[h];
-    atomicAdd(&a.counters[kCntInterfaces], nif);
-    atomicAdd(&a.counters[kCntNewton], (unsigned long long)s_newton);
+    atomicAdd(&B.counters[kCntInterfaces], nif);
+    atomicAdd(&B.counters[kCntNewton], (unsigned long long)s_newton);
   }
 }
 
@@ -505,19 +541,22 @@ __device__ __forceinline__ bool update_pencil(const SweepArgs& a, int64_t pid, c
 #define PPM_UPDATE_MINBLOCKS 3
 #endif
 
-template <bool DUAL, bool GRAV>
-__global__ void __launch_bounds__(128, PPM_UPDATE_MINBLOCKS)
-    update_kernel(const __grid_constant__ SweepArgs a) {
+template <bool DUAL, bool GRAV, bool ONE>
+__global__ void __launch_bounds__(kMarchThreads, PPM_UPDATE_MINBLOCKS)
+    update_kernel(const __grid_constant__ BatchArgs B) {
   __shared__ unsigned long long s_cnt[2];
   if (threadIdx.x < 2) s_cnt[threadIdx.x] = 0ull;
-  __syncthreads();
-  const int64_t pid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  int64_t lb;
+  const int g = locate<ONE>(B.march_prefix, B.ngrids, lb);
+  PPM_BIND_RECORD(a, g)
+  if (ONE) __syncthreads();
+  const int64_t pid = lb * kMarchThreads + threadIdx.x;
   if (pid < a.npencils) {
     const Phys P = make_phys(a);
     UpdateCounts cnt = {0, 0, 0};
     if (update_pencil<DUAL, GRAV, false>(a, pid, P, cnt)) {
-      const unsigned long long slot = atomicAdd(&a.counters[kCntFlagged], 1ull);
-      a.flagged[slot] = pid;
+      const unsigned long long slot = atomicAdd(&B.counters[kCntFlagged], 1ull);
+      B.flagged[slot] = ((int64_t)g << 40) | pid;
     } else {
       if (cnt.fatal) atomicAdd(&s_cnt[0], (unsigned long long)cnt.fatal);
       if (cnt.nonfinite) atomicAdd(&s_cnt[1], (unsigned long long)cnt.nonfinite);
@@ -525,46 +564,67 @@ __global__ void __launch_bounds__(128, PPM_UPDATE_MINBLOCKS)
   }
   __syncthreads();
   if (threadIdx.x == 0) {
-    if (s_cnt[0]) atomicAdd(&a.counters[kCntFatal], s_cnt[0]);
-    if (s_cnt[1]) atomicAdd(&a.counters[kCntNonFinite], s_cnt[1]);
+    if (s_cnt[0]) atomicAdd(&B.counters[kCntFatal], s_cnt[0]);
+    if (s_cnt[1]) atomicAdd(&B.counters[kCntNonFinite], s_cnt[1]);
   }
 }
 
 // The fallback pass: a fixed grid that walks the list of flagged pencils.
-template <bool DUAL, bool GRAV>
-__global__ void __launch_bounds__(128) fallback_kernel(const __grid_constant__ SweepArgs a) {
-  const unsigned long long nflag = *(volatile unsigned long long*)&a.counters[kCntFlagged];
-  const Phys P = make_phys(a);
+template <bool DUAL, bool GRAV, bool ONE>
+__global__ void __launch_bounds__(128) fallback_kernel(const __grid_constant__ BatchArgs B) {
+  const unsigned long long nflag = *(volatile unsigned long long*)&B.counters[kCntFlagged];
   for (unsigned long long k = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
        k < nflag; k += (unsigned long long)gridDim.x * blockDim.x) {
+    const int64_t code = B.flagged[k];
+    const SweepArgs& a = ONE ? B.one : B.grids[(int)(code >> 40)];
+    const Phys P = make_phys(a);
     UpdateCounts cnt = {0, 0, 0};
-    update_pencil<DUAL, GRAV, true>(a, a.flagged[k], P, cnt);
-    if (cnt.fallbacks) atomicAdd(&a.counters[kCntFallbacks], (unsigned long long)cnt.fallbacks);
-    if (cnt.fatal) atomicAdd(&a.counters[kCntFatal], (unsigned long long)cnt.fatal);
-    if (cnt.nonfinite) atomicAdd(&a.counters[kCntNonFinite], (unsigned long long)cnt.nonfinite);
+    update_pencil<DUAL, GRAV, true>(a, code & ((int64_t(1) << 40) - 1), P, cnt);
+    if (cnt.fallbacks) atomicAdd(&B.counters[kCntFallbacks], (unsigned long long)cnt.fallbacks);
+    if (cnt.fatal) atomicAdd(&B.counters[kCntFatal], (unsigned long long)cnt.fatal);
+    if (cnt.nonfinite) atomicAdd(&B.counters[kCntNonFinite], (unsigned long long)cnt.nonfinite);
   }
 }
 
+template <bool DUAL, bool GRAV, bool ONE>
+void launch_stages(const BatchArgs& B, int64_t march_blocks, int64_t riemann_blocks,
+                   cudaStream_t st, cudaEvent_t* ev) {
+  auto mark = [&](int k) {
+    if (ev) cudaEventRecord(ev[k], st);
+  };
+  mark(0);
+  cudaMemsetAsync(B.counters + kCntFlagged, 0, sizeof(unsigned long long), st);
+  reconstruct_kernel<DUAL, GRAV, 0, ONE><<<(unsigned)march_blocks, kMarchThreads, 0, st>>>(B);
+  mark(1);
+  reconstruct_kernel<DUAL, GRAV, 1, ONE><<<(unsigned)march_blocks, kMarchThreads, 0, st>>>(B);
+  mark(2);
+  riemann_kernel<DUAL, ONE><<<(unsigned)riemann_blocks, kRiemannThreads, 0, st>>>(B);
+  mark(3);
+  update_kernel<DUAL, GRAV, ONE><<<(unsigned)march_blocks, kMarchThreads, 0, st>>>(B);
+  mark(4);
+  fallback_kernel<DUAL, GRAV, ONE><<<64, 128, 0, st>>>(B);
+  mark(5);
+}
+
 template <bool DUAL, bool GRAV>
-void launch3(const SweepArgs& a, cudaStream_t st) {
-  const unsigned b1 = (unsigned)((a.npencils + 127) / 128);
-  cudaMemsetAsync(a.counters + kCntFlagged, 0, sizeof(unsigned long long), st);
-  reconstruct_kernel<DUAL, GRAV, 0><<<b1, 128, 0, st>>>(a);
-  reconstruct_kernel<DUAL, GRAV, 1><<<b1, 128, 0, st>>>(a);
-  dim3 g2((unsigned)((a.npencils + 255) / 256), (unsigned)(a.ie - a.is + 2));
-  riemann_kernel<DUAL><<<g2, 256, 0, st>>>(a);
-  update_kernel<DUAL, GRAV><<<b1, 128, 0, st>>>(a);
-  fallback_kernel<DUAL, GRAV><<<64, 128, 0, st>>>(a);
+void launch_any(const BatchArgs& B, int64_t march_blocks, int64_t riemann_blocks,
+                cudaStream_t st, cudaEvent_t* ev) {
+  if (B.ngrids == 1) launch_stages<DUAL, GRAV, true>(B, march_blocks, riemann_blocks, st, ev);
+  else launch_stages<DUAL, GRAV, false>(B, march_blocks, riemann_blocks, st, ev);
 }
 
 }  // namespace split
 
-// Five launches; the caller provides a.fstate / a.fflux / a.plane / a.flagged.
-void launch_sweep_split(const SweepArgs& a, bool dual, bool grav, cudaStream_t st) {
-  if (dual && grav) split::launch3<true, true>(a, st);
-  else if (dual) split::launch3<true, false>(a, st);
-  else if (grav) split::launch3<false, true>(a, st);
-  else split::launch3<false, false>(a, st);
+// One directional sweep of every grid of a batch: five launches.  The caller provides
+// each grid's fstate / fflux / plane, the prefix tables and the flagged list, and for a
+// batch of one grid also B.one (a copy of that grid's record).  ev (optional): six
+// events recorded before each kernel and after the last.
+void launch_sweep_batch(const BatchArgs& B, int64_t march_blocks, int64_t riemann_blocks,
+                        bool dual, bool grav, cudaStream_t st, cudaEvent_t* ev) {
+  if (dual && grav) split::launch_any<true, true>(B, march_blocks, riemann_blocks, st, ev);
+  else if (dual) split::launch_any<true, false>(B, march_blocks, riemann_blocks, st, ev);
+  else if (grav) split::launch_any<false, true>(B, march_blocks, riemann_blocks, st, ev);
+  else split::launch_any<false, false>(B, march_blocks, riemann_blocks, st, ev);
 }
 
 }  // namespace ppm

@@ -30,7 +30,7 @@ enum {
   kCntFatal = 11,
   kCntGuessRejected = 12,
   kCntNonFinite = 13,
-  kCntFlagged = 14,  // pencils handed to the fallback pass (index into SweepArgs::flagged)
+  kCntFlagged = 14,  // pencils handed to the fallback pass (index into BatchArgs::flagged)
 };
 
 struct SweepArgs {
@@ -61,8 +61,6 @@ struct SweepArgs {
   double gamma, dt, eta1, eta2, small_rho, pmin;
   const double* dt_device;           // if non-null, *dt_device replaces dt
   int fallback;                      // RiemannSolverFallback
-  // diagnostics
-  unsigned long long* counters;      // kMaxCounters
   // subgrid flux capture (optional)
   const FluxCapture* captures;       // sorted by pencil
   int64_t ncaptures;
@@ -72,9 +70,39 @@ struct SweepArgs {
   double* fstate;                    // kFaceVars planes: dl dr pl pr ul ur vl vr wl wr gel ger
   double* fflux;                     // kFluxVars planes: df ef uf vf wf gef ub
   int64_t plane;                     // elements per plane = (ie - is + 2) * npencils
-  int64_t* flagged;                  // npencils slots: pencils needing the fallback pass
 };
 
 enum { kFaceVars = 12, kFluxVars = 7 };
+
+// Threads per block of the marching stages and of the face-parallel Riemann stage.
+enum { kMarchThreads = 128, kRiemannThreads = 256 };
+
+// One launch over a batch of grids (an AMR level, or a single grid).  Every block
+// belongs to one grid: grid g owns blocks [prefix[g], prefix[g+1]) of a stage; a
+// block finds its grid by binary search over the prefix table.
+//   marching stages: ceil(npencils / kMarchThreads) blocks per grid
+//   Riemann stage:   (ie - is + 2) * ceil(npencils / kRiemannThreads) blocks per grid
+struct BatchArgs {
+  SweepArgs one;                     // the record itself when ngrids == 1 (read from the
+                                     // kernel parameter space, like a plain launch)
+  const SweepArgs* grids;            // device array, ngrids records
+  int ngrids;
+  const int64_t* march_prefix;       // ngrids + 1
+  const int64_t* riemann_prefix;     // ngrids + 1
+  unsigned long long* counters;      // kMaxCounters, shared by the batch
+  int64_t* flagged;                  // pencils needing the fallback pass: (grid << 40) | pencil
+};
+
+// Grid that owns block b of a stage, and the block's index inside that grid.
+__device__ __forceinline__ int batch_locate(const int64_t* prefix, int ngrids, int64_t b,
+                                            int64_t& local) {
+  int lo = 0, hi = ngrids - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (prefix[mid] <= b) lo = mid; else hi = mid - 1;
+  }
+  local = b - prefix[lo];
+  return lo;
+}
 
 }  // namespace ppm

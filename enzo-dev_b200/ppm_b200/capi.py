@@ -33,8 +33,13 @@ EXPORTS = (
     "ppm_b200_compute_pressure", "ppm_b200_compute_timestep", "ppm_b200_set_boundary",
     "ppm_b200_synchronize", "ppm_b200_launch_count", "ppm_b200_error_string",
     "ppm_b200_version", "ppm_b200_profile", "ppm_b200_profile_read",
-    "ppm_b200_euler_sweep_static",
+    "ppm_b200_euler_sweep_static", "ppm_b200_solve_level", "ppm_b200_set_graphs",
+    "ppm_b200_compute_timestep_level", "ppm_b200_set_boundary_level",
+    "ppm_b200_profile_stages",
 )
+
+# the five kernels of one sweep, in launch order (ppm_b200_profile_stages)
+SWEEP_STAGES = ("reconstruct_dpu", "reconstruct_vwge", "riemann", "update", "fallback")
 
 _dp = C.POINTER(C.c_double)
 
@@ -134,6 +139,16 @@ def lib(build_if_missing: bool = True):
     L.ppm_b200_euler_sweep_static.argtypes = [C.c_int, C.POINTER(Params), C.POINTER(GridDesc),
                                               vp, C.POINTER(GridDesc), vp, C.POINTER(Stats)]
     L.ppm_b200_profile.argtypes = [vp, C.c_int]
+    L.ppm_b200_profile_stages.argtypes = [vp, C.POINTER(C.c_double)]
+    L.ppm_b200_solve_level.argtypes = [vp, C.POINTER(Params), C.c_int, C.POINTER(GridDesc),
+                                       C.c_int, C.POINTER(Stats)]
+    L.ppm_b200_set_graphs.argtypes = [vp, C.c_int]
+    L.ppm_b200_compute_timestep_level.argtypes = [vp, C.POINTER(Params), C.POINTER(GridDesc),
+                                                  C.c_int, C.c_double, C.c_double,
+                                                  C.POINTER(C.c_double), vp,
+                                                  C.POINTER(C.c_double)]
+    L.ppm_b200_set_boundary_level.argtypes = [vp, C.POINTER(GridDesc), C.c_int, C.c_int,
+                                              C.POINTER(C.c_int)]
     L.ppm_b200_profile_read.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]
     for name in EXPORTS:
         fn = getattr(L, name)
@@ -323,6 +338,57 @@ class Context:
         if rc != OK:
             raise PPMError(rc, "ppm_b200_set_boundary")
 
+    def _level(self, grids, fields_list, accels=None):
+        """GridDesc array for a level: grids[k] with device fields fields_list[k]."""
+        n = len(grids)
+        arr = (GridDesc * n)()
+        keep = []
+        for k in range(n):
+            acc = accels[k] if accels is not None else None
+            G, kp = make_grid(grids[k], fields_list[k], acc)
+            arr[k] = G
+            keep.append(kp)
+        return arr, keep
+
+    def solve_level(self, grids, hp, dt, cycle, fields_list, accels=None, want_stats=False,
+                    dt_device=None, check=True):
+        """SolvePPM_DE of every grid of a level in one batch (device tensors)."""
+        P = make_params(hp, dt, False, dt_device)
+        arr, keep = self._level(grids, fields_list, accels)
+        st = Stats()
+        rc = self.L.ppm_b200_solve_level(self.h, C.byref(P), int(cycle), arr, len(grids),
+                                         C.byref(st) if want_stats else None)
+        if check and rc != OK:
+            raise PPMError(rc, "ppm_b200_solve_level")
+        return rc, st.as_dict()
+
+    def set_graphs(self, enable=True):
+        rc = self.L.ppm_b200_set_graphs(self.h, int(bool(enable)))
+        if rc != OK:
+            raise PPMError(rc, "ppm_b200_set_graphs")
+
+    def compute_timestep_level(self, grids, hp, fields_list, courant=None, aye=1.0,
+                               vgrid=(0.0, 0.0, 0.0), dt_device=None, want_host=True):
+        P = make_params(hp, 0.0)
+        arr, keep = self._level(grids, fields_list)
+        vg = (C.c_double * 3)(*vgrid)
+        out = C.c_double(0.0)
+        cf = hp.cfl if courant is None else courant
+        rc = self.L.ppm_b200_compute_timestep_level(
+            self.h, C.byref(P), arr, len(grids), float(cf), float(aye), vg,
+            _addr(dt_device) if dt_device is not None else None,
+            C.byref(out) if want_host else None)
+        if rc != OK:
+            raise PPMError(rc, "ppm_b200_compute_timestep_level")
+        return out.value
+
+    def set_boundary_level(self, grids, fields_list, dual, bc=("periodic",) * 3):
+        arr, keep = self._level(grids, fields_list)
+        codes = (C.c_int * 3)(*[0 if b == "periodic" else 1 for b in bc])
+        rc = self.L.ppm_b200_set_boundary_level(self.h, arr, len(grids), int(bool(dual)), codes)
+        if rc != OK:
+            raise PPMError(rc, "ppm_b200_set_boundary_level")
+
     def profile(self, enable=True):
         self.L.ppm_b200_profile(self.h, int(bool(enable)))
 
@@ -333,6 +399,14 @@ class Context:
         if rc != OK:
             raise PPMError(rc, "ppm_b200_profile_read")
         return ms.value, n.value
+
+    def profile_stages(self):
+        """{stage: ms} of the five sweep kernels, summed over the last profile_read."""
+        arr = (C.c_double * 5)()
+        rc = self.L.ppm_b200_profile_stages(self.h, arr)
+        if rc != OK:
+            raise PPMError(rc, "ppm_b200_profile_stages")
+        return dict(zip(SWEEP_STAGES, list(arr)))
 
     def synchronize(self):
         st = Stats()

@@ -234,6 +234,40 @@ def sedov(grid, hp, e_blast=1.0, rho0=1.0, p0=1e-5):
     return f
 
 
+def amr_level(hp, npatch=600, lo=16, hi=128, seed=2024, sedov_fraction=0.5, source_n=128,
+              mach=3.0):
+    """One AMR level of `npatch` patches for batched solves.
+
+    Edge lengths are drawn independently per axis, log-uniform in [lo, hi] (non-cubic
+    patches), every patch with 3 ghost zones and the level's cell width 1/source_n.
+    A patch holds either a Sedov blast (E = 1 in its central 2^3 cells, rho = 1,
+    p = 1e-5) or a periodic crop, ghosts included, of one turbulence field of
+    source_n^3 cells (the generator of `turbulence`, rms Mach `mach`).
+    Returns (grids, fields) lists."""
+    rng = np.random.default_rng(seed)
+    src_grid = Grid.uniform((source_n,) * 3)
+    src = turbulence(src_grid, hp, mach=mach, seed=seed + 1)
+    act = src_grid.active_slices()
+    src = {k: np.ascontiguousarray(v[act]) for k, v in src.items()}
+    grids, fields = [], []
+    for _ in range(npatch):
+        edges = np.floor(np.exp(rng.uniform(np.log(lo), np.log(hi + 1), size=3))).astype(int)
+        edges = np.clip(edges, lo, hi)
+        g = Grid.uniform(tuple(int(e) for e in edges),
+                         width=tuple(float(e) / source_n for e in edges))
+        if rng.random() < sedov_fraction:
+            f = sedov(g, hp)
+        else:
+            off = rng.integers(0, source_n, size=3)
+            idx = [(off[d] - NGHOST + np.arange(g.dims[d])) % source_n for d in range(3)]
+            f = new_fields(g, hp.dual)
+            for k in f:
+                f[k][...] = src[k][np.ix_(idx[2], idx[1], idx[0])]
+        grids.append(g)
+        fields.append(f)
+    return grids, fields
+
+
 def pressure_np(grid, hp, fields):
     """grid::ComputePressure (time == Time) in numpy, for diagnostics."""
     g = hp.gamma

@@ -156,6 +156,37 @@ int ppm_b200_compute_timestep(ppm_b200_context *ctx, const ppm_b200_params *para
 int ppm_b200_set_boundary(ppm_b200_context *ctx, ppm_b200_grid *grid, int dual_energy,
                           const int bc_type[3]);
 
+/* --- AMR level entry points: every grid of a level in one batch (DEVICE memory) ---
+   The reference advances a level one grid at a time: the grid loop of
+   EvolveLevel.C:569-585 calls grid::SolveHydroEquations -> SolvePPM_DE per grid,
+   and SetLevelTimeStep.C:66 takes the min of grid::ComputeTimeStep over the grids.
+   These run each stage of that loop as ONE kernel launch over all grids (largest
+   first); results are bit-identical to calling the single-grid entry points on
+   each grid in turn.  All grids share rank and physics parameters. */
+
+/* SolvePPM_DE of every grid of a level (no subgrid flux capture).  Asynchronous
+   unless stats != NULL.  With graphs enabled (ppm_b200_set_graphs) and
+   params->dt_device set, the level's launches are captured once into a CUDA graph
+   per sweep rotation and replayed while the grid list and parameters stay the
+   same. */
+int ppm_b200_solve_level(ppm_b200_context *ctx, const ppm_b200_params *params,
+                         int cycle_number, ppm_b200_grid *grids, int ngrids,
+                         ppm_b200_stats *stats);
+
+/* enable != 0: replay level solves from CUDA graphs (see ppm_b200_solve_level). */
+int ppm_b200_set_graphs(ppm_b200_context *ctx, int enable);
+
+/* min over the grids of the hydro Courant time step (SetLevelTimeStep.C:66 over
+   grid::ComputeTimeStep), one reduction for the whole level. */
+int ppm_b200_compute_timestep_level(ppm_b200_context *ctx, const ppm_b200_params *params,
+                                    ppm_b200_grid *grids, int ngrids, double courant,
+                                    double aye, const double vgrid[3], double *dt_device,
+                                    double *dt_host);
+
+/* ppm_b200_set_boundary on every grid of a list, one launch. */
+int ppm_b200_set_boundary_level(ppm_b200_context *ctx, ppm_b200_grid *grids, int ngrids,
+                                int dual_energy, const int bc_type[3]);
+
 /* Waits for all work queued on the context and returns the first error code
    recorded by device work since the last call; accumulates device counters
    into *stats (may be NULL). */
@@ -171,6 +202,9 @@ long long ppm_b200_launch_count(ppm_b200_context *ctx);
    and the number of timed sweep launches since the last read, and resets them. */
 int ppm_b200_profile(ppm_b200_context *ctx, int enable);
 int ppm_b200_profile_read(ppm_b200_context *ctx, double *sweep_ms, long long *sweep_launches);
+/* Per-kernel split of the last ppm_b200_profile_read: summed ms of the five kernels of
+   a sweep (reconstruct d/p/u, reconstruct v/w/ge, Riemann, update, HLL fallback pass). */
+int ppm_b200_profile_stages(ppm_b200_context *ctx, double stage_ms[5]);
 
 /* One directional sweep that allocates nothing (no counterpart in the reference).
    For callers that cannot call cudaMalloc when they advance a grid -- code running
