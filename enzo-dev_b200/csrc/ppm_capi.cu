@@ -68,11 +68,18 @@ struct DevBuf {
   size_t bytes = 0;
 };
 
-// A device copy of a host byte image, re-uploaded only when the image changes.
+// A device copy of a host byte image, re-uploaded only when the image changes.  The
+// upload is queued on the context stream from pinned staging memory, so it neither
+// waits for the device nor races kernels queued before it (they read the old image).
+constexpr int kStages = 4;  // staging buffers per slot, reused round robin
 struct Mirror {
   DevBuf dev;
   std::vector<unsigned char> host;
   uint64_t version = 0;
+  void* stage[kStages] = {nullptr, nullptr, nullptr, nullptr};
+  size_t stage_bytes[kStages] = {0, 0, 0, 0};
+  cudaEvent_t done[kStages] = {nullptr, nullptr, nullptr, nullptr};  // copy out of stage k
+  int next = 0;
 };
 
 // descriptor slots: one per sweep direction and position, per element kernel and per
@@ -163,11 +170,39 @@ int mirror_put(ppm_b200_context* ctx, Mirror& m, const std::vector<unsigned char
     return PPM_B200_OK;
   int rc = ensure(ctx, m.dev, std::max<size_t>(img.size(), 256));
   if (rc) return rc;
-  CK(cudaStreamSynchronize(ctx->stream));  // the previous contents may still be in use
-  CK(cudaMemcpy(m.dev.p, img.data(), img.size(), cudaMemcpyHostToDevice));
+  const int k = m.next;
+  m.next = (m.next + 1) % kStages;
+  if (m.done[k]) {
+    CK(cudaEventSynchronize(m.done[k]));  // the copy that last used this staging buffer
+  } else {
+    CK(cudaEventCreateWithFlags(&m.done[k], cudaEventDisableTiming));
+  }
+  if (m.stage_bytes[k] < img.size()) {
+    if (m.stage[k]) CK(cudaFreeHost(m.stage[k]));
+    m.stage[k] = nullptr;
+    m.stage_bytes[k] = 0;
+    const size_t cap = std::max<size_t>(img.size() + img.size() / 2, 4096);
+    CK(cudaMallocHost(&m.stage[k], cap));
+    m.stage_bytes[k] = cap;
+  }
+  if (!img.empty()) {
+    std::memcpy(m.stage[k], img.data(), img.size());
+    CK(cudaMemcpyAsync(m.dev.p, m.stage[k], img.size(), cudaMemcpyHostToDevice, ctx->stream));
+  }
+  CK(cudaEventRecord(m.done[k], ctx->stream));
   m.host = img;
   m.version += 1;
   return PPM_B200_OK;
+}
+
+void mirror_free(Mirror& m) {
+  for (int k = 0; k < kStages; ++k) {
+    if (m.done[k]) cudaEventDestroy(m.done[k]);
+    if (m.stage[k]) cudaFreeHost(m.stage[k]);
+    m.done[k] = nullptr;
+    m.stage[k] = nullptr;
+    m.stage_bytes[k] = 0;
+  }
 }
 
 template <class T>
@@ -955,7 +990,10 @@ int ppm_b200_destroy(ppm_b200_context* ctx) {
   fr(ctx->misc);
   fr(ctx->captures);
   fr(ctx->capture_buf);
-  for (auto& m : ctx->mirror) fr(m.dev);
+  for (auto& m : ctx->mirror) {
+    fr(m.dev);
+    mirror_free(m);
+  }
   for (auto e : ctx->ev_pool) cudaEventDestroy(e);
   if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
