@@ -143,7 +143,7 @@ def measured_peak_hbm():
 
 def committed_traffic():
     """Per-zone-sweep DRAM bytes of the sweep kernel from the committed ncu summary."""
-    f = REPO / "profiles" / "sweep_kernel_traffic.json"
+    f = REPO / "profiles" / "sweep_traffic_turbulence128.json"
     if f.exists():
         try:
             d = json.loads(f.read_text())
