@@ -21,6 +21,7 @@
 #include <vector>
 
 #include "ppm_b200.h"
+#include "ppm_guess.cuh"
 #include "ppm_sweep.cuh"
 
 namespace ppm {
@@ -49,7 +50,17 @@ struct ElemBatch {
   unsigned long long* min_bits;
 };
 void launch_sweep_batch(const BatchArgs& B, int64_t march_blocks, int64_t riemann_blocks,
-                        bool dual, bool grav, cudaStream_t st, cudaEvent_t* ev = nullptr);
+                        bool dual, bool grav, cudaStream_t st, cudaEvent_t* ev, bool learned);
+// learned-start training and evaluation (ppm_mlp.cu)
+cudaError_t launch_guess_features(const double* rec, int64_t n, double gamma, double pmin,
+                                  float* out, cudaStream_t st);
+cudaError_t launch_guess_grad(const float* W, const float* samples, const int64_t* index,
+                              int64_t n, float inv_count, float* grad, double* loss, int blocks,
+                              cudaStream_t st);
+cudaError_t launch_guess_adam(float* W, float* grad, float* m, float* v, int step, float lr,
+                              float beta1, float beta2, float eps, cudaStream_t st);
+cudaError_t launch_guess_eval(const uint32_t* packed, const float* feats, int64_t n, float* y,
+                              cudaStream_t st);
 void launch_pressure_batch(const ElemBatch& B, int64_t blocks, cudaStream_t st);
 void launch_timestep_batch(const ElemBatch& B, int64_t blocks, double courant, double* dt_out,
                            cudaStream_t st);
@@ -124,6 +135,14 @@ struct ppm_b200_context {
   std::vector<cudaEvent_t> ev_pool;  // kSweepEvents per timed sweep
   size_t ev_used = 0;
   double stage_ms[5] = {0, 0, 0, 0, 0};  // per-kernel totals of the last profile read
+  // learned Newton start: packed inference weights (ppm_b200_set_guess)
+  DevBuf guess;
+  bool has_guess = false;
+  // log of sampled Riemann problems of the plain solver (ppm_b200_riemann_log)
+  double* log = nullptr;
+  long long log_cap = 0;
+  int log_stride = 0;
+  DevBuf log_count;
   // CUDA graphs of level solves, keyed by everything a launch takes by value
   bool use_graphs = false;
   std::map<std::string, cudaGraphExec_t> graphs;
@@ -256,7 +275,6 @@ int check_supported(const ppm_b200_params* p) {
     return PPM_B200_ERR_UNSUPPORTED;
   if (p->riemann_solver != PPM_B200_RIEMANN_TWOSHOCK) return PPM_B200_ERR_UNSUPPORTED;
   if (p->reconstruction != PPM_B200_RECONSTRUCTION_PPM) return PPM_B200_ERR_UNSUPPORTED;
-  if (p->learned_guess) return PPM_B200_ERR_UNSUPPORTED;
   return PPM_B200_OK;
 }
 
@@ -279,6 +297,61 @@ int check_grid(const ppm_b200_grid* g, const ppm_b200_params* p) {
     }
   }
   return PPM_B200_OK;
+}
+
+// A learned start needs weights (ppm_b200_set_guess) on this context.
+int check_guess(const ppm_b200_context* ctx, const ppm_b200_params* p) {
+  if (p->learned_guess && !ctx->has_guess) return PPM_B200_ERR_INVALID;
+  return PPM_B200_OK;
+}
+
+// Host: FP32 master weights -> BF16 B fragments of mma.m16n8k16 + FP32 biases, in the
+// order guess_mlp_warp reads them (ppm_guess.cuh).
+uint16_t bf16_bits(float x) {
+  uint32_t u;
+  std::memcpy(&u, &x, 4);
+  u += 0x7FFFu + ((u >> 16) & 1u);  // round to nearest even (finite inputs)
+  return (uint16_t)(u >> 16);
+}
+
+uint32_t bf16_pair(float lo, float hi) {
+  return (uint32_t)bf16_bits(lo) | ((uint32_t)bf16_bits(hi) << 16);
+}
+
+void pack_guess(const float* w, std::vector<uint32_t>& out) {
+  using namespace ppm;
+  out.assign(kPackWords, 0u);
+  auto w1 = [&](int k, int n) { return k < kGuessIn ? w[kOffW1 + k * kGuessHidden + n] : 0.0f; };
+  auto w2 = [&](int k, int n) { return w[kOffW2 + k * kGuessHidden + n]; };
+  for (int lane = 0; lane < 32; ++lane) {
+    const int g = lane >> 2, t = lane & 3;
+    for (int n = 0; n < 8; ++n) {
+      const int col = 8 * n + g;
+      uint32_t* o = &out[kPackL1 + (n * 32 + lane) * 2];
+      o[0] = bf16_pair(w1(2 * t, col), w1(2 * t + 1, col));
+      o[1] = bf16_pair(w1(2 * t + 8, col), w1(2 * t + 9, col));
+    }
+    for (int kk = 0; kk < 4; ++kk)
+      for (int n = 0; n < 8; ++n) {
+        const int col = 8 * n + g, r0 = 16 * kk + 2 * t;
+        uint32_t* o = &out[kPackL2 + ((kk * 8 + n) * 32 + lane) * 2];
+        o[0] = bf16_pair(w2(r0, col), w2(r0 + 1, col));
+        o[1] = bf16_pair(w2(r0 + 8, col), w2(r0 + 9, col));
+      }
+    for (int kk = 0; kk < 4; ++kk) {
+      const int r0 = 16 * kk + 2 * t;
+      uint32_t* o = &out[kPackL3 + (kk * 32 + lane) * 2];
+      if (g == 0) {
+        o[0] = bf16_pair(w[kOffW3 + r0], w[kOffW3 + r0 + 1]);
+        o[1] = bf16_pair(w[kOffW3 + r0 + 8], w[kOffW3 + r0 + 9]);
+      }
+    }
+  }
+  for (int j = 0; j < kGuessHidden; ++j) {
+    std::memcpy(&out[kPackB1 + j], &w[kOffB1 + j], 4);
+    std::memcpy(&out[kPackB2 + j], &w[kOffB2 + j], 4);
+  }
+  std::memcpy(&out[kPackB3], &w[kOffB3], 4);
 }
 
 struct FieldSet {
@@ -500,6 +573,13 @@ int prepare_sweep(ppm_b200_context* ctx, int dim, int position, const ppm_b200_p
     a.small_rho = p->small_rho;
     a.pmin = p->tiny_number;
     a.fallback = p->riemann_fallback;
+    a.guess = p->learned_guess ? (const uint32_t*)ctx->guess.p : nullptr;
+    if (ctx->log && !p->learned_guess) {
+      a.log = ctx->log;
+      a.log_count = (unsigned long long*)ctx->log_count.p;
+      a.log_cap = ctx->log_cap;
+      a.log_stride = ctx->log_stride;
+    }
     a.fstate = scratch + at;
     a.fflux = a.fstate + (size_t)ppm::kFaceVars * (size_t)a.plane;
     at += (size_t)(ppm::kFaceVars + ppm::kFluxVars) * (size_t)a.plane;
@@ -558,7 +638,7 @@ int enqueue_sweep(ppm_b200_context* ctx, const SweepPlan& plan, const ppm_b200_p
     ctx->ev_used += kSweepEvents;
   }
   ppm::launch_sweep_batch(plan.B, plan.march_blocks, plan.riemann_blocks, p->dual_energy != 0,
-                          p->gravity != 0, ctx->stream, ev);
+                          p->gravity != 0, ctx->stream, ev, p->learned_guess != 0);
   ctx->launches += 5;
   CK(cudaGetLastError());
   return PPM_B200_OK;
@@ -884,6 +964,7 @@ void key_put(std::string& k, const T& v) {
 
 std::string graph_key(ppm_b200_context* ctx, const ppm_b200_params* p, const SolvePlan& sp) {
   std::string k;
+  key_put(k, p->learned_guess);
   key_put(k, p->dual_energy);
   key_put(k, p->gravity);
   key_put(k, sp.nsweeps);
@@ -990,6 +1071,8 @@ int ppm_b200_destroy(ppm_b200_context* ctx) {
   fr(ctx->misc);
   fr(ctx->captures);
   fr(ctx->capture_buf);
+  fr(ctx->guess);
+  fr(ctx->log_count);
   for (auto& m : ctx->mirror) {
     fr(m.dev);
     mirror_free(m);
@@ -1066,6 +1149,8 @@ int ppm_b200_solve_ppm_de(ppm_b200_context* ctx, const ppm_b200_params* p, int c
   if (rc) return rc;
   rc = check_grid(g, p);
   if (rc) return rc;
+  rc = check_guess(ctx, p);
+  if (rc) return rc;
   if (nsub > 0 && !sub) return PPM_B200_ERR_INVALID;
   CK(cudaSetDevice(ctx->device));
   const long long zero3[3] = {0, 0, 0};
@@ -1101,6 +1186,8 @@ int ppm_b200_solve_level(ppm_b200_context* ctx, const ppm_b200_params* p, int cy
     if (rc) return rc;
     if (grids[k].rank != grids[0].rank) return PPM_B200_ERR_INVALID;
   }
+  rc = check_guess(ctx, p);
+  if (rc) return rc;
   CK(cudaSetDevice(ctx->device));
   // largest grids first: the block scheduler then starts the longest pencils first
   std::vector<int> idx(ngrids);
@@ -1159,6 +1246,8 @@ int ppm_b200_euler_sweep(ppm_b200_context* ctx, int dim, const ppm_b200_params* 
   rc = check_grid(g, p);
   if (rc) return rc;
   if (dim >= g->rank) return PPM_B200_ERR_INVALID;
+  rc = check_guess(ctx, p);
+  if (rc) return rc;
   CK(cudaSetDevice(ctx->device));
   const long long zero3[3] = {0, 0, 0};
   const long long* ggs = ggs_in ? ggs_in : zero3;
@@ -1310,6 +1399,94 @@ static int boundary_batch(ppm_b200_context* ctx, ppm_b200_grid* grids, int ngrid
   ppm::launch_boundary_batch(ep.B, ep.size_blocks, ctx->stream);
   ctx->launches += 1;
   CK(cudaGetLastError());
+  return PPM_B200_OK;
+}
+
+int ppm_b200_set_guess(ppm_b200_context* ctx, const float* weights) {
+  if (!ctx) return PPM_B200_ERR_INVALID;
+  CK(cudaSetDevice(ctx->device));
+  if (!weights) {
+    ctx->has_guess = false;
+    return PPM_B200_OK;
+  }
+  std::vector<uint32_t> packed;
+  pack_guess(weights, packed);
+  int rc = ensure(ctx, ctx->guess, packed.size() * sizeof(uint32_t));
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(ctx->stream));  // a queued solve may still read the old weights
+  CK(cudaMemcpy(ctx->guess.p, packed.data(), packed.size() * sizeof(uint32_t),
+                cudaMemcpyHostToDevice));
+  ctx->has_guess = true;
+  return PPM_B200_OK;
+}
+
+int ppm_b200_riemann_log(ppm_b200_context* ctx, double* records, long long capacity,
+                         int stride) {
+  if (!ctx || capacity < 0 || stride < 0) return PPM_B200_ERR_INVALID;
+  CK(cudaSetDevice(ctx->device));
+  if (!records || capacity == 0 || stride == 0) {
+    ctx->log = nullptr;
+    ctx->log_cap = 0;
+    ctx->log_stride = 0;
+    return PPM_B200_OK;
+  }
+  int rc = ensure(ctx, ctx->log_count, sizeof(unsigned long long));
+  if (rc) return rc;
+  CK(cudaMemsetAsync(ctx->log_count.p, 0, sizeof(unsigned long long), ctx->stream));
+  ctx->log = records;
+  ctx->log_cap = capacity;
+  ctx->log_stride = stride;
+  return PPM_B200_OK;
+}
+
+int ppm_b200_riemann_log_count(ppm_b200_context* ctx, long long* count) {
+  if (!ctx || !count) return PPM_B200_ERR_INVALID;
+  CK(cudaSetDevice(ctx->device));
+  unsigned long long c = 0;
+  if (ctx->log_count.p) {
+    CK(cudaMemcpyAsync(&c, ctx->log_count.p, sizeof(c), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+  }
+  *count = (long long)std::min<unsigned long long>(c, (unsigned long long)ctx->log_cap);
+  return PPM_B200_OK;
+}
+
+int ppm_b200_guess_features(ppm_b200_context* ctx, const double* records, long long n,
+                            double gamma, double pmin, float* samples) {
+  if (!ctx || n < 0 || (n > 0 && (!records || !samples))) return PPM_B200_ERR_INVALID;
+  CK(cudaSetDevice(ctx->device));
+  CK(ppm::launch_guess_features(records, n, gamma, pmin, samples, ctx->stream));
+  ctx->launches += 1;
+  return PPM_B200_OK;
+}
+
+int ppm_b200_guess_grad(ppm_b200_context* ctx, const float* weights, const float* samples,
+                        const long long* index, long long n, float* grad, double* loss) {
+  if (!ctx || n < 0 || !weights || !grad || !loss || (n > 0 && !samples))
+    return PPM_B200_ERR_INVALID;
+  CK(cudaSetDevice(ctx->device));
+  if (n == 0) return PPM_B200_OK;
+  CK(ppm::launch_guess_grad(weights, samples, (const int64_t*)index, n, 1.0f / (float)n, grad,
+                            loss, ctx->sms, ctx->stream));
+  ctx->launches += 1;
+  return PPM_B200_OK;
+}
+
+int ppm_b200_guess_adam(ppm_b200_context* ctx, float* weights, float* grad, float* m, float* v,
+                        int step, float lr, float beta1, float beta2, float eps) {
+  if (!ctx || !weights || !grad || !m || !v || step < 1) return PPM_B200_ERR_INVALID;
+  CK(cudaSetDevice(ctx->device));
+  CK(ppm::launch_guess_adam(weights, grad, m, v, step, lr, beta1, beta2, eps, ctx->stream));
+  ctx->launches += 1;
+  return PPM_B200_OK;
+}
+
+int ppm_b200_guess_eval(ppm_b200_context* ctx, const float* features, long long n, float* y) {
+  if (!ctx || n < 0 || (n > 0 && (!features || !y))) return PPM_B200_ERR_INVALID;
+  if (!ctx->has_guess) return PPM_B200_ERR_INVALID;
+  CK(cudaSetDevice(ctx->device));
+  CK(ppm::launch_guess_eval((const uint32_t*)ctx->guess.p, features, n, y, ctx->stream));
+  ctx->launches += 1;
   return PPM_B200_OK;
 }
 

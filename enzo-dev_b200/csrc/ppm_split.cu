@@ -18,6 +18,7 @@
 #include <cuda_runtime.h>
 
 #include "ppm_device.cuh"
+#include "ppm_guess.cuh"
 #include "ppm_sweep.cuh"
 
 namespace ppm {
@@ -272,12 +273,20 @@ __device__ __forceinline__ FaceState load_face(const SweepArgs& a, int64_t idx) 
 
 // ------------------------------------------------------------------ stage 2
 // per grid, blocks over (face plane fi = face - is) x (chunks of pencils)
-template <bool DUAL, bool ONE>
+// LEARNED: the Newton iteration starts from the MLP's pressure (ppm_guess.cuh) and falls
+// back to the acoustic start, i.e. the plain solver, when it does not converge.
+// Without LEARNED, a sample of the faces can be logged (states + converged p*) as
+// training data for that net.
+template <bool DUAL, bool ONE, bool LEARNED>
 __global__ void __launch_bounds__(kRiemannThreads) riemann_kernel(const __grid_constant__ BatchArgs B) {
   __shared__ unsigned int s_hist[8];
   __shared__ unsigned int s_newton;
+  __shared__ unsigned int s_rejected;
   if (threadIdx.x < 8) s_hist[threadIdx.x] = 0u;
-  if (threadIdx.x == 0) s_newton = 0u;
+  if (threadIdx.x == 0) {
+    s_newton = 0u;
+    s_rejected = 0u;
+  }
   int64_t lb;
   const int g = locate<ONE>(B.riemann_prefix, B.ngrids, lb);
   PPM_BIND_RECORD(a, g)
@@ -285,14 +294,51 @@ __global__ void __launch_bounds__(kRiemannThreads) riemann_kernel(const __grid_c
   const int64_t chunks = (a.npencils + kRiemannThreads - 1) / kRiemannThreads;
   const int fi = (int)(lb / chunks);
   const int64_t pid = (lb - (int64_t)fi * chunks) * kRiemannThreads + threadIdx.x;
-  if (pid < a.npencils) {
-    const Phys P = make_phys(a);
-    const int64_t idx = (int64_t)fi * a.npencils + pid;
-    const FaceState s = load_face<DUAL>(a, idx);
+  const bool valid = pid < a.npencils;
+  const Phys P = make_phys(a);
+  const int64_t idx = (int64_t)fi * a.npencils + pid;
+  FaceState s;
+  if (valid) {
+    s = load_face<DUAL>(a, idx);
+  } else {
+    s = FaceState{1.0, 1.0, 1.0, 1.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  }
+  float y = 0.0f, d2 = 0.0f;
+  if (LEARNED) {  // warp-collective: every lane takes part, with or without a face
+    float f[6];
+    d2 = guess_features(s.dl, s.dr, s.pl, s.pr, s.ul, s.ur, P.gamma, f);
+    y = guess_mlp_warp(a.guess, f);
+  }
+  if (valid) {
     const double cl = sqrt(P.gamma * s.pl * s.dl);
     const double cr = sqrt(P.gamma * s.pr * s.dr);
     const double ps = acoustic_guess(s, cl, cr, P);
-    const Riemann rs = twoshock_newton(s, cl, cr, ps, P);
+    Riemann rs;
+    unsigned spent = 0;
+    if (LEARNED) {
+      rs = twoshock_newton(s, cl, cr, guess_pressure(ps, y, d2, P.pmin), P);
+      if (!rs.converged) {
+        spent = (unsigned)rs.iters;
+        rs = twoshock_newton(s, cl, cr, ps, P);
+        atomicAdd(&s_rejected, 1u);
+      }
+    } else {
+      rs = twoshock_newton(s, cl, cr, ps, P);
+      if (a.log && a.log_stride > 0) {
+        const unsigned long long h =
+            ((unsigned long long)idx + 0x9E3779B97F4A7C15ull * (unsigned long long)(g + 1)) *
+            0xD1B54A32D192ED03ull;
+        if ((h >> 40) % (unsigned long long)a.log_stride == 0) {
+          const unsigned long long slot = atomicAdd(a.log_count, 1ull);
+          if (slot < (unsigned long long)a.log_cap) {
+            double* r = a.log + slot * 8;
+            r[0] = s.dl; r[1] = s.dr; r[2] = s.pl; r[3] = s.pr;
+            r[4] = s.ul; r[5] = s.ur; r[6] = rs.pbar;
+            r[7] = rs.converged ? (double)rs.iters : -(double)rs.iters;
+          }
+        }
+      }
+    }
     const double qc = P.dt / a.coef[a.is + fi].dx;
     const Flux F = flux_twoshock<DUAL>(s, rs.pbar, rs.ubar, qc, P);
     double* o = a.fflux + idx;
@@ -305,7 +351,7 @@ __global__ void __launch_bounds__(kRiemannThreads) riemann_kernel(const __grid_c
     if (DUAL) o[XGEF * pl] = F.gef;
     o[XUB * pl] = F.ub;
     atomicAdd(&s_hist[rs.iters & 7], 1u);
-    atomicAdd(&s_newton, (unsigned)rs.iters);
+    atomicAdd(&s_newton, (unsigned)rs.iters + spent);
   }
   __syncthreads();
   if (threadIdx.x < 8 && s_hist[threadIdx.x])
@@ -316,6 +362,8 @@ __global__ void __launch_bounds__(kRiemannThreads) riemann_kernel(const __grid_c
     atomicAdd(&B.counters[kCntInterfaces], nif);
     atomicAdd(&B.counters[kCntNewton], (unsigned long long)s_newton);
   }
+  if (LEARNED && threadIdx.x == 9 && s_rejected)
+    atomicAdd(&B.counters[kCntGuessRejected], (unsigned long long)s_rejected);
 }
 
 __device__ __forceinline__ Flux load_flux(const SweepArgs& a, int64_t idx) {
@@ -588,7 +636,7 @@ __global__ void __launch_bounds__(128) fallback_kernel(const __grid_constant__ B
 
 template <bool DUAL, bool GRAV, bool ONE>
 void launch_stages(const BatchArgs& B, int64_t march_blocks, int64_t riemann_blocks,
-                   cudaStream_t st, cudaEvent_t* ev) {
+                   cudaStream_t st, cudaEvent_t* ev, bool learned) {
   auto mark = [&](int k) {
     if (ev) cudaEventRecord(ev[k], st);
   };
@@ -598,7 +646,10 @@ void launch_stages(const BatchArgs& B, int64_t march_blocks, int64_t riemann_blo
   mark(1);
   reconstruct_kernel<DUAL, GRAV, 1, ONE><<<(unsigned)march_blocks, kMarchThreads, 0, st>>>(B);
   mark(2);
-  riemann_kernel<DUAL, ONE><<<(unsigned)riemann_blocks, kRiemannThreads, 0, st>>>(B);
+  if (learned)
+    riemann_kernel<DUAL, ONE, true><<<(unsigned)riemann_blocks, kRiemannThreads, 0, st>>>(B);
+  else
+    riemann_kernel<DUAL, ONE, false><<<(unsigned)riemann_blocks, kRiemannThreads, 0, st>>>(B);
   mark(3);
   update_kernel<DUAL, GRAV, ONE><<<(unsigned)march_blocks, kMarchThreads, 0, st>>>(B);
   mark(4);
@@ -608,9 +659,11 @@ void launch_stages(const BatchArgs& B, int64_t march_blocks, int64_t riemann_blo
 
 template <bool DUAL, bool GRAV>
 void launch_any(const BatchArgs& B, int64_t march_blocks, int64_t riemann_blocks,
-                cudaStream_t st, cudaEvent_t* ev) {
-  if (B.ngrids == 1) launch_stages<DUAL, GRAV, true>(B, march_blocks, riemann_blocks, st, ev);
-  else launch_stages<DUAL, GRAV, false>(B, march_blocks, riemann_blocks, st, ev);
+                cudaStream_t st, cudaEvent_t* ev, bool learned) {
+  if (B.ngrids == 1)
+    launch_stages<DUAL, GRAV, true>(B, march_blocks, riemann_blocks, st, ev, learned);
+  else
+    launch_stages<DUAL, GRAV, false>(B, march_blocks, riemann_blocks, st, ev, learned);
 }
 
 }  // namespace split
@@ -618,13 +671,14 @@ void launch_any(const BatchArgs& B, int64_t march_blocks, int64_t riemann_blocks
 // One directional sweep of every grid of a batch: five launches.  The caller provides
 // each grid's fstate / fflux / plane, the prefix tables and the flagged list, and for a
 // batch of one grid also B.one (a copy of that grid's record).  ev (optional): six
-// events recorded before each kernel and after the last.
+// events recorded before each kernel and after the last.  learned: start the Newton
+// iteration from the MLP guess (every record's `guess` must point at packed weights).
 void launch_sweep_batch(const BatchArgs& B, int64_t march_blocks, int64_t riemann_blocks,
-                        bool dual, bool grav, cudaStream_t st, cudaEvent_t* ev) {
-  if (dual && grav) split::launch_any<true, true>(B, march_blocks, riemann_blocks, st, ev);
-  else if (dual) split::launch_any<true, false>(B, march_blocks, riemann_blocks, st, ev);
-  else if (grav) split::launch_any<false, true>(B, march_blocks, riemann_blocks, st, ev);
-  else split::launch_any<false, false>(B, march_blocks, riemann_blocks, st, ev);
+                        bool dual, bool grav, cudaStream_t st, cudaEvent_t* ev, bool learned) {
+  if (dual && grav) split::launch_any<true, true>(B, march_blocks, riemann_blocks, st, ev, learned);
+  else if (dual) split::launch_any<true, false>(B, march_blocks, riemann_blocks, st, ev, learned);
+  else if (grav) split::launch_any<false, true>(B, march_blocks, riemann_blocks, st, ev, learned);
+  else split::launch_any<false, false>(B, march_blocks, riemann_blocks, st, ev, learned);
 }
 
 }  // namespace ppm

@@ -70,6 +70,14 @@ struct SweepArgs {
   double* fstate;                    // kFaceVars planes: dl dr pl pr ul ur vl vr wl wr gel ger
   double* fflux;                     // kFluxVars planes: df ef uf vf wf gef ub
   int64_t plane;                     // elements per plane = (ie - is + 2) * npencils
+  // learned Newton start (ppm_guess.cuh): packed BF16 weights, used by the LEARNED kernels
+  const uint32_t* guess;
+  // optional log of sampled faces of the plain solver: 8 doubles per record
+  // (dl dr pl pr ul ur p* +-iterations, negative when Newton did not converge)
+  double* log;
+  unsigned long long* log_count;     // records claimed (may exceed log_cap)
+  int64_t log_cap;
+  int log_stride;                    // about one face in log_stride is logged; 0 = off
 };
 
 enum { kFaceVars = 12, kFluxVars = 7 };

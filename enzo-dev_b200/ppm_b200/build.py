@@ -22,7 +22,7 @@ OUT_DIR = ROOT / "_build"
 LIB = OUT_DIR / "libppm_b200.so"
 INCLUDE = REPO / "include"
 
-SOURCES = ["ppm_kernels.cu", "ppm_split.cu", "ppm_capi.cu", "ppm_noalloc.cu"]
+SOURCES = ["ppm_kernels.cu", "ppm_split.cu", "ppm_capi.cu", "ppm_noalloc.cu", "ppm_mlp.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-fmad=false",
               "-Xcompiler", "-fPIC,-ffp-contract=off", "--expt-relaxed-constexpr"]

@@ -35,8 +35,12 @@ EXPORTS = (
     "ppm_b200_version", "ppm_b200_profile", "ppm_b200_profile_read",
     "ppm_b200_euler_sweep_static", "ppm_b200_solve_level", "ppm_b200_set_graphs",
     "ppm_b200_compute_timestep_level", "ppm_b200_set_boundary_level",
-    "ppm_b200_profile_stages",
+    "ppm_b200_profile_stages", "ppm_b200_set_guess", "ppm_b200_riemann_log",
+    "ppm_b200_riemann_log_count", "ppm_b200_guess_features", "ppm_b200_guess_grad",
+    "ppm_b200_guess_adam", "ppm_b200_guess_eval",
 )
+
+GUESS_WEIGHTS = 4673  # W1[6][64] b1[64] W2[64][64] b2[64] w3[64] b3
 
 # the five kernels of one sweep, in launch order (ppm_b200_profile_stages)
 SWEEP_STAGES = ("reconstruct_dpu", "reconstruct_vwge", "riemann", "update", "fallback")
@@ -143,6 +147,15 @@ def lib(build_if_missing: bool = True):
     L.ppm_b200_solve_level.argtypes = [vp, C.POINTER(Params), C.c_int, C.POINTER(GridDesc),
                                        C.c_int, C.POINTER(Stats)]
     L.ppm_b200_set_graphs.argtypes = [vp, C.c_int]
+    fp = C.POINTER(C.c_float)
+    L.ppm_b200_set_guess.argtypes = [vp, vp]
+    L.ppm_b200_riemann_log.argtypes = [vp, vp, C.c_longlong, C.c_int]
+    L.ppm_b200_riemann_log_count.argtypes = [vp, C.POINTER(C.c_longlong)]
+    L.ppm_b200_guess_features.argtypes = [vp, vp, C.c_longlong, C.c_double, C.c_double, vp]
+    L.ppm_b200_guess_grad.argtypes = [vp, vp, vp, vp, C.c_longlong, vp, vp]
+    L.ppm_b200_guess_adam.argtypes = [vp, vp, vp, vp, vp, C.c_int, C.c_float, C.c_float,
+                                      C.c_float, C.c_float]
+    L.ppm_b200_guess_eval.argtypes = [vp, vp, C.c_longlong, vp]
     L.ppm_b200_compute_timestep_level.argtypes = [vp, C.POINTER(Params), C.POINTER(GridDesc),
                                                   C.c_int, C.c_double, C.c_double,
                                                   C.POINTER(C.c_double), vp,
@@ -297,8 +310,8 @@ class Context:
         return rc, st.as_dict()
 
     def euler_sweep(self, dim, grid, hp, dt, fields, pressure, memory=MEM_HOST, accel=None,
-                    check=True):
-        P = make_params(hp, dt)
+                    check=True, learned_guess=False):
+        P = make_params(hp, dt, learned_guess)
         G, keep = make_grid(grid, fields, accel)
         st = Stats()
         g = (C.c_longlong * 3)(0, 0, 0)
@@ -351,9 +364,9 @@ class Context:
         return arr, keep
 
     def solve_level(self, grids, hp, dt, cycle, fields_list, accels=None, want_stats=False,
-                    dt_device=None, check=True):
+                    dt_device=None, check=True, learned_guess=False):
         """SolvePPM_DE of every grid of a level in one batch (device tensors)."""
-        P = make_params(hp, dt, False, dt_device)
+        P = make_params(hp, dt, learned_guess, dt_device)
         arr, keep = self._level(grids, fields_list, accels)
         st = Stats()
         rc = self.L.ppm_b200_solve_level(self.h, C.byref(P), int(cycle), arr, len(grids),
@@ -399,6 +412,60 @@ class Context:
         if rc != OK:
             raise PPMError(rc, "ppm_b200_profile_read")
         return ms.value, n.value
+
+    # ---- learned Newton start
+    def set_guess(self, weights):
+        """weights: host float32 array of GUESS_WEIGHTS values (None clears)."""
+        if weights is None:
+            rc = self.L.ppm_b200_set_guess(self.h, None)
+        else:
+            w = np.ascontiguousarray(weights, dtype=np.float32)
+            assert w.size == GUESS_WEIGHTS
+            rc = self.L.ppm_b200_set_guess(self.h, w.ctypes.data)
+        if rc != OK:
+            raise PPMError(rc, "ppm_b200_set_guess")
+
+    def riemann_log(self, records, stride):
+        """records: device float64 tensor (capacity, 8) or None to stop."""
+        if records is None:
+            rc = self.L.ppm_b200_riemann_log(self.h, None, 0, 0)
+        else:
+            rc = self.L.ppm_b200_riemann_log(self.h, records.data_ptr(), records.shape[0],
+                                             int(stride))
+        if rc != OK:
+            raise PPMError(rc, "ppm_b200_riemann_log")
+
+    def riemann_log_count(self):
+        n = C.c_longlong(0)
+        rc = self.L.ppm_b200_riemann_log_count(self.h, C.byref(n))
+        if rc != OK:
+            raise PPMError(rc, "ppm_b200_riemann_log_count")
+        return n.value
+
+    def guess_features(self, records, n, gamma, pmin, samples):
+        rc = self.L.ppm_b200_guess_features(self.h, records.data_ptr(), int(n), float(gamma),
+                                            float(pmin), samples.data_ptr())
+        if rc != OK:
+            raise PPMError(rc, "ppm_b200_guess_features")
+
+    def guess_grad(self, weights, samples, index, n, grad, loss):
+        rc = self.L.ppm_b200_guess_grad(self.h, weights.data_ptr(), samples.data_ptr(),
+                                        index.data_ptr() if index is not None else None,
+                                        int(n), grad.data_ptr(), loss.data_ptr())
+        if rc != OK:
+            raise PPMError(rc, "ppm_b200_guess_grad")
+
+    def guess_adam(self, weights, grad, m, v, step, lr, beta1=0.9, beta2=0.999, eps=1e-8):
+        rc = self.L.ppm_b200_guess_adam(self.h, weights.data_ptr(), grad.data_ptr(),
+                                        m.data_ptr(), v.data_ptr(), int(step), float(lr),
+                                        float(beta1), float(beta2), float(eps))
+        if rc != OK:
+            raise PPMError(rc, "ppm_b200_guess_adam")
+
+    def guess_eval(self, features, n, y):
+        rc = self.L.ppm_b200_guess_eval(self.h, features.data_ptr(), int(n), y.data_ptr())
+        if rc != OK:
+            raise PPMError(rc, "ppm_b200_guess_eval")
 
     def profile_stages(self):
         """{stage: ms} of the five sweep kernels, summed over the last profile_read."""

@@ -68,7 +68,8 @@ typedef struct ppm_b200_params {
   int positive_rec;         /* PositiveReconstruction: must be 0 */
   int eos_type;             /* EOSType: must be 0 */
   int number_of_colours;    /* NumberOfColours: must be 0 */
-  int learned_guess;        /* 1: start twoshock's Newton iteration from the learned p* guess */
+  int learned_guess;        /* 1: start twoshock's Newton iteration from the learned p* guess
+                               (weights from ppm_b200_set_guess) */
   const double *dt_device;  /* optional: device pointer holding dtFixed (overrides dt) */
   int reserved[6];
 } ppm_b200_params;
@@ -205,6 +206,47 @@ int ppm_b200_profile_read(ppm_b200_context *ctx, double *sweep_ms, long long *sw
 /* Per-kernel split of the last ppm_b200_profile_read: summed ms of the five kernels of
    a sweep (reconstruct d/p/u, reconstruct v/w/ge, Riemann, update, HLL fallback pass). */
 int ppm_b200_profile_stages(ppm_b200_context *ctx, double stage_ms[5]);
+
+/* --- learned starting pressure of twoshock's Newton iteration (twoshock.F:156-170) ---
+   A 6 -> 64 -> 64 -> 1 MLP predicts ln(p* / p_acoustic) from the two interface states;
+   with params->learned_guess = 1 the Riemann kernel evaluates it on the tensor cores
+   (BF16 operands, FP32 accumulation), starts Newton from that pressure, iterates to the
+   reference tolerance, and re-solves from the acoustic start (the plain solver) any
+   face that does not converge (counted in stats->guess_rejected).  The fields then
+   agree with the plain solver to round-off, not bit for bit.
+   Weights: 4673 floats, W1[6][64] b1[64] W2[64][64] b2[64] w3[64] b3 (row = input).
+   All pointers below are DEVICE memory unless stated; calls queue on the context
+   stream and return without waiting, except where noted. */
+
+/* Host weights for the learned start (NULL: forget them).  Synchronises. */
+int ppm_b200_set_guess(ppm_b200_context *ctx, const float *weights_host);
+
+/* Log about one in `stride` Riemann problems of later plain solves on this context:
+   8 doubles per record (dl dr pl pr ul ur p* iterations, the count negative when
+   Newton did not converge), at most `capacity` records.  NULL / 0 stops logging. */
+int ppm_b200_riemann_log(ppm_b200_context *ctx, double *records, long long capacity,
+                         int stride);
+/* Records written so far (synchronises). */
+int ppm_b200_riemann_log_count(ppm_b200_context *ctx, long long *count);
+
+/* Training samples from log records: 8 floats each (the 6 inputs, the target
+   ln(p* / p_acoustic), 1 if usable else 0 -- unconverged or non-finite). */
+int ppm_b200_guess_features(ppm_b200_context *ctx, const double *records, long long n,
+                            double gamma, double pmin, float *samples);
+
+/* Forward + backward over samples[index[0..n-1]] (index may be NULL: the first n):
+   adds d(loss)/d(weights) to grad (4673 floats, zero it first) and the summed squared
+   error to *loss (one double), loss = mean squared error of the n samples. */
+int ppm_b200_guess_grad(ppm_b200_context *ctx, const float *weights, const float *samples,
+                        const long long *index, long long n, float *grad, double *loss);
+
+/* One Adam step (step counts from 1) on the FP32 master weights; zeroes grad. */
+int ppm_b200_guess_adam(ppm_b200_context *ctx, float *weights, float *grad, float *m,
+                        float *v, int step, float lr, float beta1, float beta2, float eps);
+
+/* The tensor-core inference of the Riemann kernel on given inputs (6 floats each),
+   with the weights of ppm_b200_set_guess: y[i] = predicted ln(p* / p_acoustic). */
+int ppm_b200_guess_eval(ppm_b200_context *ctx, const float *features, long long n, float *y);
 
 /* One directional sweep that allocates nothing (no counterpart in the reference).
    For callers that cannot call cudaMalloc when they advance a grid -- code running
