@@ -155,7 +155,7 @@ def _grf(n, slope, rng):
     nz = kk > 0
     amp[nz] = kk[nz] ** (slope / 2.0)
     noise = rng.standard_normal(kk.shape) + 1j * rng.standard_normal(kk.shape)
-    g = np.fft.irfftn(noise * amp, s=(n, n, n))
+    g = np.fft.irfftn(noise * amp, s=(n, n, n), axes=(0, 1, 2))
     g -= g.mean()
     g /= g.std()
     return g
@@ -177,7 +177,7 @@ def _solenoidal(n, slope, rng):
     div = sum(c * kc for c, kc in zip(comps, kv))
     safe = np.where(nz, kk2, 1.0)
     comps = [c - kc * div / safe for c, kc in zip(comps, kv)]
-    out = [np.fft.irfftn(c, s=(n, n, n)) for c in comps]
+    out = [np.fft.irfftn(c, s=(n, n, n), axes=(0, 1, 2)) for c in comps]
     return out
 
 
@@ -212,6 +212,84 @@ def turbulence(grid, hp, mach=3.0, sigma_lnrho=0.5, seed=1234):
     if hp.dual:
         f["ge"][act] = eint
     fill_ghosts(grid, f, "periodic")
+    return f
+
+
+def turbulence_device(grid, hp, mach=3.0, sigma_lnrho=0.5, seed=1234, device="cuda"):
+    """`turbulence` generated on the GPU with torch (for grids of 512^3 and more, where
+    the host FFTs take minutes): the same spectra, normalisations and uniform pressure,
+    from torch's seeded generator (a different realisation than the numpy one).
+    Returns device float64 tensors with periodic ghosts, in the BaryonField layout."""
+    import torch
+
+    assert grid.rank == 3
+    n = grid.end[0] - grid.start[0] + 1
+    gen = torch.Generator(device=device)
+    gen.manual_seed(seed)
+    k = torch.fft.fftfreq(n, device=device, dtype=torch.float64) * n
+    kz = torch.fft.rfftfreq(n, device=device, dtype=torch.float64) * n
+    kx, ky, kzz = torch.meshgrid(k, k, kz, indexing="ij")
+    kk2 = kx * kx + ky * ky + kzz * kzz
+    nz = kk2 > 0
+
+    def amp(slope):
+        a = torch.zeros_like(kk2)
+        a[nz] = kk2[nz] ** (slope / 4.0)  # |k|^(slope/2)
+        return a
+
+    def noise():
+        re = torch.randn(kk2.shape, generator=gen, device=device, dtype=torch.float64)
+        im = torch.randn(kk2.shape, generator=gen, device=device, dtype=torch.float64)
+        return torch.complex(re, im)
+
+    g = torch.fft.irfftn(noise() * amp(-2.0), s=(n, n, n), dim=(0, 1, 2))
+    g = (g - g.mean()) / g.std()
+    rho = torch.exp(sigma_lnrho * g - 0.5 * sigma_lnrho ** 2)
+    rho = rho / rho.mean()
+    del g
+    a4 = amp(-4.0)
+    comps = [noise() * a4 for _ in range(3)]
+    kv = (kx, ky, kzz)
+    div = sum(c * kc for c, kc in zip(comps, kv))
+    safe = torch.where(nz, kk2, torch.ones_like(kk2))
+    vel = []
+    for c, kc in zip(comps, kv):
+        vel.append(torch.fft.irfftn(c - kc * div / safe, s=(n, n, n), dim=(0, 1, 2)))
+    del comps, div, safe, kx, ky, kzz, kk2, a4
+    vrms = torch.sqrt(torch.mean(vel[0] ** 2 + vel[1] ** 2 + vel[2] ** 2))
+    scale = mach / vrms
+    p0 = 1.0 / hp.gamma
+    shape = grid.shape
+    f = {}
+    for name in ("d", "te", "v1", "v2", "v3") + (("ge",) if hp.dual else ()):
+        f[name] = torch.zeros(shape, dtype=torch.float64, device=device)
+    act = grid.active_slices()
+    to_zyx = lambda a: a.permute(2, 1, 0).contiguous()
+    f["d"][act] = to_zyx(rho)
+    for name, v in zip(("v1", "v2", "v3"), vel):
+        f[name][act] = to_zyx(v * scale)
+    eint = p0 / ((hp.gamma - 1.0) * f["d"][act])
+    ke = 0.5 * (f["v1"][act] ** 2 + f["v2"][act] ** 2 + f["v3"][act] ** 2)
+    f["te"][act] = eint + ke
+    if hp.dual:
+        f["ge"][act] = eint
+    # periodic ghosts
+    gz = grid.start[0]
+    for ax in range(3):
+        dim = 2 - ax
+        s, e = grid.start[dim], grid.end[dim]
+        for name in f:
+            t = f[name]
+            lo = [slice(None)] * 3
+            hi = [slice(None)] * 3
+            src_lo = [slice(None)] * 3
+            src_hi = [slice(None)] * 3
+            lo[ax] = slice(0, s)
+            src_lo[ax] = slice(e + 1 - gz, e + 1)
+            hi[ax] = slice(e + 1, e + 1 + gz)
+            src_hi[ax] = slice(s, s + gz)
+            t[tuple(lo)] = t[tuple(src_lo)]
+            t[tuple(hi)] = t[tuple(src_hi)]
     return f
 
 
