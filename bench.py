@@ -57,6 +57,8 @@ def parse():
     ap.add_argument("--no-level", action="store_true",
                     help="skip the batched AMR-level measurement")
     ap.add_argument("--level-patches", type=int, default=600)
+    ap.add_argument("--no-learned", action="store_true",
+                    help="skip the learned-Newton-start comparison")
     return ap.parse_args()
 
 
@@ -215,6 +217,69 @@ def run_reference(args):
     return 0
 
 
+# ---------------------------------------------------------------- learned Newton start
+def run_learned(ctx, g, hp, f_host, args, stream):
+    """Plain vs learned starting pressure of the Newton iteration on the bench workload:
+    zone-updates/s (event-timed), Newton iterations per interface, the Riemann kernel's
+    time per sweep, and the largest relative field difference after the steps."""
+    import torch
+    from ppm_b200 import capi
+    from ppm_b200 import learned as LRN
+
+    ctx.set_guess(LRN.default_weights())
+    dev = torch.device("cuda", torch.cuda.current_device())
+    steps = max(1, min(args.steps, 5))
+    out = {"steps": steps, "warmup": 2}
+    finals = {}
+    for mode in ("plain", "learned"):
+        f = {k: torch.from_numpy(v).to(dev) for k, v in f_host.items()}
+        dtd = torch.zeros(1, dtype=torch.float64, device=dev)
+        torch.cuda.synchronize()
+
+        def step(cyc):
+            ctx.compute_timestep(g, hp, f, memory=capi.MEM_DEVICE, dt_device=dtd,
+                                 want_host=False)
+            ctx.solve_ppm_de(g, hp, 0.0, cyc, f, memory=capi.MEM_DEVICE, want_stats=False,
+                             dt_device=dtd, learned_guess=(mode == "learned"))
+            ctx.set_boundary(g, f, hp.dual, ("periodic",) * 3)
+
+        for c in range(2):
+            step(c)
+        ctx.synchronize()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ctx.profile(True)
+        ev0.record(stream)
+        for c in range(2, 2 + steps):
+            step(c)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        sweep_ms, nsweep = ctx.profile_read()
+        stages = ctx.profile_stages()
+        ctx.profile(False)
+        rc, st = ctx.synchronize()
+        if rc != 0:
+            raise RuntimeError(f"{mode} steps failed: {capi.error_string(rc)}")
+        ms = ev0.elapsed_time(ev1) / steps
+        out[mode] = {"ms_per_step": ms, "zone_updates_per_s": g.active_cells / (ms * 1e-3),
+                     "newton_per_interface": st["newton_iters"] / max(st["interfaces"], 1),
+                     "riemann_ms_per_sweep": stages["riemann"] / max(nsweep, 1),
+                     "guess_rejected": st["guess_rejected"]}
+        finals[mode] = f
+    act = g.active_slices()
+    worst = 0.0
+    for k in finals["plain"]:
+        a = finals["plain"][k][act]
+        b = finals["learned"][k][act]
+        worst = max(worst, float((a - b).abs().max() / a.abs().max().clamp_min(1e-300)))
+    out["max_rel_field_difference"] = worst
+    out["speedup_learned_vs_plain"] = (out["learned"]["zone_updates_per_s"] /
+                                       out["plain"]["zone_updates_per_s"])
+    del finals
+    torch.cuda.empty_cache()
+    return out
+
+
 # ---------------------------------------------------------------- AMR level (batched)
 def run_level(ctx, args, stream):
     """One AMR level of 600 patches (edges log-uniform in 16-128 per axis, 3 ghost zones,
@@ -238,12 +303,15 @@ def run_level(ctx, args, stream):
            "contents": "Sedov blasts (E=1 in 2^3 cells) and Mach-3 turbulence crops",
            "steps": steps, "warmup": 3}
     digests = {}
-    for mode in ("batched_graph", "per_patch_loop"):
+    from ppm_b200 import learned as LRN
+    ctx.set_guess(LRN.default_weights())
+    for mode in ("batched_graph", "per_patch_loop", "batched_graph_learned"):
         f = [{k: torch.from_numpy(v).to(dev) for k, v in fh.items()} for fh in host]
         arr, keep = ctx._level(grids, f)
-        P = capi.make_params(hp, 0.0, False, dtd)
+        P = capi.make_params(hp, 0.0, mode == "batched_graph_learned", dtd)
         ggs = (C.c_longlong * 3)(0, 0, 0)
-        ctx.set_graphs(mode == "batched_graph")
+        ctx.set_graphs(mode != "per_patch_loop")
+        torch.cuda.synchronize()
         L = ctx.L
 
         def step(cyc):
@@ -263,6 +331,7 @@ def run_level(ctx, args, stream):
         for c in range(3):
             step(c)
         torch.cuda.synchronize()
+        ctx.synchronize()
         ev0 = torch.cuda.Event(enable_timing=True)
         ev1 = torch.cuda.Event(enable_timing=True)
         ev0.record(stream)
@@ -270,21 +339,26 @@ def run_level(ctx, args, stream):
             step(c)
         ev1.record(stream)
         torch.cuda.synchronize()
-        rc, _ = ctx.synchronize()
+        rc, st = ctx.synchronize()
         if rc != 0:
             raise RuntimeError(f"level steps failed: {capi.error_string(rc)}")
         ms = ev0.elapsed_time(ev1) / steps
+        newton = st["newton_iters"] / max(st["interfaces"], 1)
         h = hashlib.sha1()
         for fk in f:
             for name in sorted(fk):
                 h.update(fk[name].cpu().numpy().tobytes())
         digests[mode] = h.hexdigest()
-        out[mode] = {"ms_per_step": ms, "zone_updates_per_s": active / (ms * 1e-3)}
+        out[mode] = {"ms_per_step": ms, "zone_updates_per_s": active / (ms * 1e-3),
+                     "newton_per_interface": newton}
         del f, arr, keep
         torch.cuda.empty_cache()
     ctx.set_graphs(False)
     out["speedup_batched_vs_loop"] = (out["batched_graph"]["zone_updates_per_s"] /
                                       out["per_patch_loop"]["zone_updates_per_s"])
+    out["speedup_batched_learned_vs_loop"] = (
+        out["batched_graph_learned"]["zone_updates_per_s"] /
+        out["per_patch_loop"]["zone_updates_per_s"])
     out["bit_identical"] = digests["batched_graph"] == digests["per_patch_loop"]
     return out
 
@@ -404,6 +478,11 @@ def run_ours(args):
                "d2h_bytes_per_step": nbytes, "steps": ne,
                "api": "ppm_b200_solve_ppm_de(MEM_HOST), pinned host fields"}
 
+    # the learned Newton start on the same workload (same state, a few steps each way)
+    learned = None
+    if world == 1 and not args.no_learned:
+        learned = run_learned(ctx, g, hp, f_host, args, stream)
+
     level = None
     if world == 1 and not args.no_level:
         level = run_level(ctx, args, stream)
@@ -430,6 +509,7 @@ def run_ours(args):
                                            if st["interfaces"] else None),
             "hll_fallbacks": st["fallbacks"],
             "amr_level": level,
+            "learned_start": learned,
         }
         print(json.dumps(line), flush=True)
     ctx.close()

@@ -33,6 +33,11 @@ namespace ppm {
 
 enum { kGuessIn = 6, kGuessHidden = 64 };
 
+// Below this |x|^2 for all 32 faces of a warp the net is not evaluated: the acoustic
+// start is then already within about |x|^2 |r| (|r| of order 0.1) of p*, which leaves
+// too little for the net to save to pay for its evaluation.
+constexpr float kGuessMinJump = 1.0e-4f;
+
 // FP32 master weights, flat: W1 [6][64] (input-major), b1 [64], W2 [64][64], b2 [64],
 // w3 [64], b3 [1]
 enum {

@@ -304,10 +304,13 @@ __global__ void __launch_bounds__(kRiemannThreads) riemann_kernel(const __grid_c
     s = FaceState{1.0, 1.0, 1.0, 1.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
   }
   float y = 0.0f, d2 = 0.0f;
-  if (LEARNED) {  // warp-collective: every lane takes part, with or without a face
+  if (LEARNED) {
     float f[6];
     d2 = guess_features(s.dl, s.dr, s.pl, s.pr, s.ul, s.ur, P.gamma, f);
-    y = guess_mlp_warp(a.guess, f);
+    if (!valid) d2 = 0.0f;
+    // warp-collective (every lane takes part, with or without a face); a warp whose
+    // jumps are all weak keeps the acoustic start, which is then within ~|x|^2 of p*
+    if (__any_sync(0xffffffffu, d2 > kGuessMinJump)) y = guess_mlp_warp(a.guess, f);
   }
   if (valid) {
     const double cl = sqrt(P.gamma * s.pl * s.dl);
