@@ -1377,7 +1377,7 @@ static int boundary_batch(ppm_b200_context* ctx, ppm_b200_grid* grids, int ngrid
                           int dual_energy, const int bc_type[3]) {
   if (!ctx || !grids || ngrids <= 0 || !bc_type) return PPM_B200_ERR_INVALID;
   for (int d = 0; d < 3; ++d)
-    if (bc_type[d] != 0 && bc_type[d] != 1) return PPM_B200_ERR_INVALID;
+    if (bc_type[d] < 0 || bc_type[d] > 2) return PPM_B200_ERR_INVALID;
   CK(cudaSetDevice(ctx->device));
   ppm_b200_params p;
   std::memset(&p, 0, sizeof(p));

@@ -27,7 +27,7 @@ struct ElemGrid {
   const double* cw[3];  // device cell widths (time-step kernel)
   int rank;
   int dims[3], start[3], end[3];
-  int bc[3];            // 0 periodic, 1 outflow
+  int bc[3];            // 0 periodic, 1 outflow, 2 left alone
   int64_t size;         // cells incl. ghosts
   int64_t active;       // active cells
 };
@@ -130,6 +130,7 @@ __global__ void timestep_finalize_kernel(const unsigned long long* min_bits, dou
 // ------------------------------------------------------------------ ghost-zone fill
 __device__ __forceinline__ int bc_map(int i, int s, int e, int bc) {
   if (i >= s && i <= e) return i;
+  if (bc == 2) return i;  // left alone: filled by a halo exchange
   if (bc == 0) {
     const int nn = e - s + 1;
     int r = (i - s) % nn;
@@ -139,9 +140,10 @@ __device__ __forceinline__ int bc_map(int i, int s, int e, int bc) {
   return i < s ? s : e;
 }
 
-// One thread per cell of the padded grid: every ghost cell copies the active cell it
-// maps to (sources are always active cells, so the in-place fill has no
-// read-after-write hazard); active cells return immediately.
+// One thread per cell of the padded grid: every ghost cell copies the cell it maps to.
+// Sources are cells that map to themselves (active cells, or ghosts of a face left to a
+// halo exchange), which this kernel never writes, so the in-place fill has no
+// read-after-write hazard.
 __global__ void __launch_bounds__(256) boundary_kernel(const __grid_constant__ ElemBatch B) {
   int64_t lb;
   const ElemGrid& G = B.grids[batch_locate(B.size_prefix, B.ngrids, blockIdx.x, lb)];

@@ -41,6 +41,7 @@ EXPORTS = (
 )
 
 GUESS_WEIGHTS = 4673  # W1[6][64] b1[64] W2[64][64] b2[64] w3[64] b3
+BC_CODES = {"periodic": 0, "outflow": 1, "none": 2}  # ppm_b200_set_boundary bc_type
 
 # the five kernels of one sweep, in launch order (ppm_b200_profile_stages)
 SWEEP_STAGES = ("reconstruct_dpu", "reconstruct_vwge", "riemann", "update", "fallback")
@@ -346,7 +347,7 @@ class Context:
 
     def set_boundary(self, grid, fields, dual, bc=("periodic",) * 3):
         G, keep = make_grid(grid, fields)
-        codes = (C.c_int * 3)(*[0 if b == "periodic" else 1 for b in bc])
+        codes = (C.c_int * 3)(*[BC_CODES[b] for b in bc])
         rc = self.L.ppm_b200_set_boundary(self.h, C.byref(G), int(bool(dual)), codes)
         if rc != OK:
             raise PPMError(rc, "ppm_b200_set_boundary")
@@ -397,7 +398,7 @@ class Context:
 
     def set_boundary_level(self, grids, fields_list, dual, bc=("periodic",) * 3):
         arr, keep = self._level(grids, fields_list)
-        codes = (C.c_int * 3)(*[0 if b == "periodic" else 1 for b in bc])
+        codes = (C.c_int * 3)(*[BC_CODES[b] for b in bc])
         rc = self.L.ppm_b200_set_boundary_level(self.h, arr, len(grids), int(bool(dual)), codes)
         if rc != OK:
             raise PPMError(rc, "ppm_b200_set_boundary_level")

@@ -108,6 +108,8 @@ def _index_map(grid, d, bc):
         return s + (idx - s) % (e - s + 1)
     if bc == "outflow":
         return np.clip(idx, s, e)
+    if bc == "none":  # ghosts filled elsewhere (e.g. a halo exchange)
+        return idx
     raise ValueError(bc)
 
 

@@ -151,9 +151,10 @@ int ppm_b200_compute_timestep(ppm_b200_context *ctx, const ppm_b200_params *para
                               ppm_b200_grid *grid, int memory, double courant, double aye,
                               const double vgrid[3], double *dt_device, double *dt_host);
 
-/* Ghost-zone fill of one grid on device memory (periodic = 0 / outflow = 1
-   per dimension); the external-boundary part of SetBoundaryConditions for a
-   single grid (ExternalBoundary_SetExternalBoundaryIO.C:201-209, :378-386). */
+/* Ghost-zone fill of one grid on device memory (periodic = 0 / outflow = 1 /
+   2 = leave alone, for faces a halo exchange fills, per dimension); the
+   external-boundary part of SetBoundaryConditions for a single grid
+   (ExternalBoundary_SetExternalBoundaryIO.C:201-209, :378-386). */
 int ppm_b200_set_boundary(ppm_b200_context *ctx, ppm_b200_grid *grid, int dual_energy,
                           const int bc_type[3]);
 
