@@ -50,7 +50,8 @@ struct ElemBatch {
   unsigned long long* min_bits;
 };
 void launch_sweep_batch(const BatchArgs& B, int64_t march_blocks, int64_t riemann_blocks,
-                        bool dual, bool grav, cudaStream_t st, cudaEvent_t* ev, bool learned);
+                        bool dual, bool grav, cudaStream_t st, cudaEvent_t* ev, bool learned,
+                        bool contiguous);
 // learned-start training and evaluation (ppm_mlp.cu)
 cudaError_t launch_guess_features(const double* rec, int64_t n, double gamma, double pmin,
                                   float* out, cudaStream_t st);
@@ -410,6 +411,7 @@ struct SweepPlan {
   std::vector<FluxCapture> reqs;    // single-grid subgrid-flux capture
   std::vector<HostCapture> hreq;
   int64_t cap_offset = 0;           // this sweep's first request in the capture buffers
+  bool contiguous = false;          // x sweep: pencils along the contiguous axis
 };
 
 // Subgrid flux capture requests of one sweep of a single grid (Grid_xEulerSweep.C:313-377
@@ -622,6 +624,7 @@ int prepare_sweep(ppm_b200_context* ctx, int dim, int position, const ppm_b200_p
   plan.B.flagged = (int64_t*)(scratch + scratch_doubles);
   plan.march_blocks = mpre[ng];
   plan.riemann_blocks = rpre[ng];
+  plan.contiguous = dim == 0;
   return PPM_B200_OK;
 }
 
@@ -638,7 +641,8 @@ int enqueue_sweep(ppm_b200_context* ctx, const SweepPlan& plan, const ppm_b200_p
     ctx->ev_used += kSweepEvents;
   }
   ppm::launch_sweep_batch(plan.B, plan.march_blocks, plan.riemann_blocks, p->dual_energy != 0,
-                          p->gravity != 0, ctx->stream, ev, p->learned_guess != 0);
+                          p->gravity != 0, ctx->stream, ev, p->learned_guess != 0,
+                          plan.contiguous);
   ctx->launches += 5;
   CK(cudaGetLastError());
   return PPM_B200_OK;
@@ -989,6 +993,7 @@ std::string graph_key(ppm_b200_context* ctx, const ppm_b200_params* p, const Sol
     key_put(k, b.flagged);
     key_put(k, sp.sweep[s].march_blocks);
     key_put(k, sp.sweep[s].riemann_blocks);
+    key_put(k, sp.sweep[s].contiguous);
     key_put(k, ctx->mirror[kSlotSweep0 + 3 * sp.order[s] + s].version);
   }
   return k;

@@ -38,7 +38,8 @@
 
 namespace ppm {
 void launch_sweep_batch(const BatchArgs& B, int64_t march_blocks, int64_t riemann_blocks,
-                        bool dual, bool grav, cudaStream_t st, cudaEvent_t* ev, bool learned);
+                        bool dual, bool grav, cudaStream_t st, cudaEvent_t* ev, bool learned,
+                        bool contiguous);
 }
 
 namespace {
@@ -240,7 +241,7 @@ extern "C" int ppm_b200_euler_sweep_static(int dim, const ppm_b200_params* p,
   B.flagged = reinterpret_cast<int64_t*>(planes + (size_t)(ppm::kFaceVars + ppm::kFluxVars) *
                                                       (size_t)a.plane);
   ppm::launch_sweep_batch(B, march_blocks, riemann_blocks, p->dual_energy != 0, p->gravity != 0,
-                          st, nullptr, false);
+                          st, nullptr, false, dim == 0);
   e = cudaGetLastError();
   if (e != cudaSuccess) return fail_cuda(e, "sweep launch");
 

@@ -450,10 +450,47 @@ struct UpdateCounts {
   unsigned int fallbacks, fatal, nonfinite;
 };
 
-template <bool DUAL, bool GRAV, bool FALLBACK>
+// Output staging of the x sweep.  Its pencils run along the contiguous axis, so a warp
+// storing one cell per pencil writes 32 separate sectors; instead every thread stores
+// its cells into shared memory, and every kStageCells cells the block writes them out
+// with consecutive lanes on consecutive cells of a pencil.  Layout [field][cell][pencil]
+// with a padded row (kStageLd) so that the flush reads hit distinct banks.
+enum { kStageCells = 4, kStageLd = kMarchThreads + 8 };
+constexpr int kStageField = kStageCells * kStageLd;
+
+template <bool DUAL>
+__device__ __forceinline__ void flush_stage(const SweepArgs& a, const double* stage,
+                                            int64_t pid0, int c0, int ncells) {
+  __syncthreads();  // every thread has staged its cells
+  for (int q = threadIdx.x; q < kMarchThreads * kStageCells; q += kMarchThreads) {
+    const int j = q % kStageCells, p = q / kStageCells;
+    const int64_t pid = pid0 + p;
+    if (j < ncells && pid < a.npencils) {
+      const int64_t off = (pid % a.n1) * a.s1 + (pid / a.n1) * a.s2 + (c0 + j);  // sa == 1
+      const double* sp = stage + j * kStageLd + p;
+      a.out_d[off] = sp[0];
+      a.out_e[off] = sp[kStageField];
+      if (a.out_u) a.out_u[off] = sp[2 * kStageField];
+      if (a.out_v) a.out_v[off] = sp[3 * kStageField];
+      if (a.out_w) a.out_w[off] = sp[4 * kStageField];
+      if (DUAL) a.out_ge[off] = sp[5 * kStageField];
+    }
+  }
+  __syncthreads();  // the staging buffer may be refilled
+}
+
+//
+// STAGED (x sweep, hot pass only): every thread of the block runs the same steps,
+// including threads without a pencil (valid = false) and threads whose pencil was
+// flagged, since the block flushes the staged outputs together; those threads skip all
+// loads and computation.  A flagged pencil's partial outputs are rewritten by the
+// fallback pass.
+template <bool DUAL, bool GRAV, bool FALLBACK, bool STAGED = false>
 __device__ __forceinline__ bool update_pencil(const SweepArgs& a, int64_t pid, const Phys& P,
-                                              UpdateCounts& cnt) {
-  const int64_t base = (pid % a.n1) * a.s1 + (pid / a.n1) * a.s2;
+                                              UpdateCounts& cnt, bool valid = true,
+                                              double* stage = nullptr, int64_t pid0 = 0) {
+  bool live = valid, flagged = false;
+  const int64_t base = live ? (pid % a.n1) * a.s1 + (pid / a.n1) * a.s2 : 0;
   const int64_t sa = a.sa, np = a.npencils;
   const int n = a.n, is = a.is, ie = a.ie;
 
@@ -469,7 +506,8 @@ __device__ __forceinline__ bool update_pencil(const SweepArgs& a, int64_t pid, c
   }
 
   Flux Fm = {0, 0, 0, 0, 0, 0, 0};  // final flux at face t-1
-  Flux F0 = load_flux(a, pid);      // flux at face t (face is while t <= is)
+  Flux F0 = Fm;                     // flux at face t (face is while t <= is)
+  if (live) F0 = load_flux(a, pid);
   Cell Cm = {0, 0, 0, 0, 0, 0};     // input state of cell t-1
   double ges_m = 0.0;               // final ges of cell t-1
   bool gov = false;                 // ges(t) was set by the fallback of cell t-1
@@ -478,8 +516,12 @@ __device__ __forceinline__ bool update_pencil(const SweepArgs& a, int64_t pid, c
   double dep = 0.0;                 // post-pgas d*e of cell t-3
   unsigned int nonfin = 0;
   // one-step prefetch of cell t and face t+1
-  Cell Cpf = load_cell<DUAL>(a, base);
-  Flux Fpf = (0 >= is && 0 <= ie) ? load_flux(a, (int64_t)(1 - is) * np + pid) : F0;
+  Cell Cpf = Cm;
+  Flux Fpf = F0;
+  if (live) {
+    Cpf = load_cell<DUAL>(a, base);
+    if (0 >= is && 0 <= ie) Fpf = load_flux(a, (int64_t)(1 - is) * np + pid);
+  }
 
 #pragma unroll 1
   for (int t = 0; t <= n; ++t) {
@@ -489,7 +531,7 @@ __device__ __forceinline__ bool update_pencil(const SweepArgs& a, int64_t pid, c
     bool gov_next = false;
     double govv_next = 0.0;
     // (1) check of cell t
-    if (t < n) {
+    if (live && t < n) {
       Cn = Cpf;
       if (t >= is && t <= ie) F1 = Fpf;
       if (t + 1 < n) {
@@ -502,7 +544,13 @@ __device__ __forceinline__ bool update_pencil(const SweepArgs& a, int64_t pid, c
           ges_n = gov ? govv : P.dt / a.coef[t].dx * pcent * (F0.ub - F1.ub);
         }
         if (Cn.d + (F0.df - F1.df) <= 0.0 || Cn.e < 0.0) {
-          if (!FALLBACK) return true;  // hand the pencil to the fallback pass
+          if (!FALLBACK && !STAGED) return true;  // hand the pencil to the fallback pass
+          if (!FALLBACK) {  // STAGED: stop computing, keep joining the block's flushes
+            live = false;
+            flagged = true;
+          }
+        }
+        if (live && (Cn.d + (F0.df - F1.df) <= 0.0 || Cn.e < 0.0)) {
           if (a.fallback == 0) {
             cnt.fatal += 1;
           } else {
@@ -526,7 +574,7 @@ __device__ __forceinline__ bool update_pencil(const SweepArgs& a, int64_t pid, c
     }
     // (2) conservative update of cell t-1
     Cell PEn = Cm;
-    {
+    if (live) {
       const int c = t - 1;
       if (c >= is && c <= ie) {
         bool fatal = false;
@@ -539,7 +587,7 @@ __device__ __forceinline__ bool update_pencil(const SweepArgs& a, int64_t pid, c
     // (3) dual-energy select of cell t-2 and store
     {
       const int c = t - 2;
-      if (c >= 0) {
+      if (live && c >= 0) {
         Cell o = PEm;
         if (DUAL) {
           const double own = o.d * o.e;
@@ -549,14 +597,27 @@ __device__ __forceinline__ bool update_pencil(const SweepArgs& a, int64_t pid, c
           dep = o.d * o.e;
         }
         if (!isfinite(o.d) || !isfinite(o.e)) nonfin += 1;
-        const int64_t off = base + (int64_t)c * sa;
-        a.out_d[off] = o.d;
-        a.out_e[off] = o.e;
-        if (a.out_u) a.out_u[off] = o.u;
-        if (a.out_v) a.out_v[off] = o.v;
-        if (a.out_w) a.out_w[off] = o.w;
-        if (DUAL) a.out_ge[off] = o.ge;
+        if (STAGED) {
+          double* sp = stage + (c % kStageCells) * kStageLd + threadIdx.x;
+          sp[0] = o.d;
+          sp[kStageField] = o.e;
+          sp[2 * kStageField] = o.u;
+          sp[3 * kStageField] = o.v;
+          sp[4 * kStageField] = o.w;
+          if (DUAL) sp[5 * kStageField] = o.ge;
+        } else {
+          const int64_t off = base + (int64_t)c * sa;
+          a.out_d[off] = o.d;
+          a.out_e[off] = o.e;
+          if (a.out_u) a.out_u[off] = o.u;
+          if (a.out_v) a.out_v[off] = o.v;
+          if (a.out_w) a.out_w[off] = o.w;
+          if (DUAL) a.out_ge[off] = o.ge;
+        }
       }
+      // block-wide: the same steps on every thread
+      if (STAGED && c >= 0 && c % kStageCells == kStageCells - 1)
+        flush_stage<DUAL>(a, stage, pid0, c - (kStageCells - 1), kStageCells);
     }
     Fm = F0;
     F0 = F1;
@@ -570,42 +631,62 @@ __device__ __forceinline__ bool update_pencil(const SweepArgs& a, int64_t pid, c
   // post-euler state is its input, selected against itself and its left neighbour
   {
     const int c = n - 1;
-    Cell o = PEm;
-    if (DUAL) {
-      const double own = o.d * o.e;
-      pgas2d_dual(o, (c == 0) ? own : dep, own, P);
+    if (live) {
+      Cell o = PEm;
+      if (DUAL) {
+        const double own = o.d * o.e;
+        pgas2d_dual(o, (c == 0) ? own : dep, own, P);
+      }
+      if (!isfinite(o.d) || !isfinite(o.e)) nonfin += 1;
+      if (STAGED) {
+        double* sp = stage + (c % kStageCells) * kStageLd + threadIdx.x;
+        sp[0] = o.d;
+        sp[kStageField] = o.e;
+        sp[2 * kStageField] = o.u;
+        sp[3 * kStageField] = o.v;
+        sp[4 * kStageField] = o.w;
+        if (DUAL) sp[5 * kStageField] = o.ge;
+      } else {
+        const int64_t off = base + (int64_t)c * sa;
+        a.out_d[off] = o.d;
+        a.out_e[off] = o.e;
+        if (a.out_u) a.out_u[off] = o.u;
+        if (a.out_v) a.out_v[off] = o.v;
+        if (a.out_w) a.out_w[off] = o.w;
+        if (DUAL) a.out_ge[off] = o.ge;
+      }
     }
-    if (!isfinite(o.d) || !isfinite(o.e)) nonfin += 1;
-    const int64_t off = base + (int64_t)c * sa;
-    a.out_d[off] = o.d;
-    a.out_e[off] = o.e;
-    if (a.out_u) a.out_u[off] = o.u;
-    if (a.out_v) a.out_v[off] = o.v;
-    if (a.out_w) a.out_w[off] = o.w;
-    if (DUAL) a.out_ge[off] = o.ge;
+    if (STAGED) {  // the partial last chunk, cells c0 .. n-1
+      const int c0 = c - c % kStageCells;
+      flush_stage<DUAL>(a, stage, pid0, c0, c - c0 + 1);
+    }
   }
   cnt.nonfinite += nonfin;
-  return false;
+  return flagged;
 }
 
 #ifndef PPM_UPDATE_MINBLOCKS
 #define PPM_UPDATE_MINBLOCKS 3
 #endif
 
-template <bool DUAL, bool GRAV, bool ONE>
+// STAGED: the x sweep (pencils along the contiguous axis) with staged outputs.
+template <bool DUAL, bool GRAV, bool ONE, bool STAGED>
 __global__ void __launch_bounds__(kMarchThreads, PPM_UPDATE_MINBLOCKS)
     update_kernel(const __grid_constant__ BatchArgs B) {
   __shared__ unsigned long long s_cnt[2];
+  __shared__ double s_stage[STAGED ? 6 * kStageField : 1];
   if (threadIdx.x < 2) s_cnt[threadIdx.x] = 0ull;
   int64_t lb;
   const int g = locate<ONE>(B.march_prefix, B.ngrids, lb);
   PPM_BIND_RECORD(a, g)
   if (ONE) __syncthreads();
-  const int64_t pid = lb * kMarchThreads + threadIdx.x;
-  if (pid < a.npencils) {
+  const int64_t pid0 = lb * kMarchThreads;
+  const int64_t pid = pid0 + threadIdx.x;
+  const bool valid = pid < a.npencils;
+  if (STAGED || valid) {
     const Phys P = make_phys(a);
     UpdateCounts cnt = {0, 0, 0};
-    if (update_pencil<DUAL, GRAV, false>(a, pid, P, cnt)) {
+    if (update_pencil<DUAL, GRAV, false, STAGED>(a, pid, P, cnt, valid, s_stage, pid0)) {
       const unsigned long long slot = atomicAdd(&B.counters[kCntFlagged], 1ull);
       B.flagged[slot] = ((int64_t)g << 40) | pid;
     } else {
@@ -639,7 +720,7 @@ __global__ void __launch_bounds__(128) fallback_kernel(const __grid_constant__ B
 
 template <bool DUAL, bool GRAV, bool ONE>
 void launch_stages(const BatchArgs& B, int64_t march_blocks, int64_t riemann_blocks,
-                   cudaStream_t st, cudaEvent_t* ev, bool learned) {
+                   cudaStream_t st, cudaEvent_t* ev, bool learned, bool staged) {
   auto mark = [&](int k) {
     if (ev) cudaEventRecord(ev[k], st);
   };
@@ -654,7 +735,10 @@ void launch_stages(const BatchArgs& B, int64_t march_blocks, int64_t riemann_blo
   else
     riemann_kernel<DUAL, ONE, false><<<(unsigned)riemann_blocks, kRiemannThreads, 0, st>>>(B);
   mark(3);
-  update_kernel<DUAL, GRAV, ONE><<<(unsigned)march_blocks, kMarchThreads, 0, st>>>(B);
+  if (staged)
+    update_kernel<DUAL, GRAV, ONE, true><<<(unsigned)march_blocks, kMarchThreads, 0, st>>>(B);
+  else
+    update_kernel<DUAL, GRAV, ONE, false><<<(unsigned)march_blocks, kMarchThreads, 0, st>>>(B);
   mark(4);
   fallback_kernel<DUAL, GRAV, ONE><<<64, 128, 0, st>>>(B);
   mark(5);
@@ -662,11 +746,11 @@ void launch_stages(const BatchArgs& B, int64_t march_blocks, int64_t riemann_blo
 
 template <bool DUAL, bool GRAV>
 void launch_any(const BatchArgs& B, int64_t march_blocks, int64_t riemann_blocks,
-                cudaStream_t st, cudaEvent_t* ev, bool learned) {
+                cudaStream_t st, cudaEvent_t* ev, bool learned, bool staged) {
   if (B.ngrids == 1)
-    launch_stages<DUAL, GRAV, true>(B, march_blocks, riemann_blocks, st, ev, learned);
+    launch_stages<DUAL, GRAV, true>(B, march_blocks, riemann_blocks, st, ev, learned, staged);
   else
-    launch_stages<DUAL, GRAV, false>(B, march_blocks, riemann_blocks, st, ev, learned);
+    launch_stages<DUAL, GRAV, false>(B, march_blocks, riemann_blocks, st, ev, learned, staged);
 }
 
 }  // namespace split
@@ -676,12 +760,16 @@ void launch_any(const BatchArgs& B, int64_t march_blocks, int64_t riemann_blocks
 // batch of one grid also B.one (a copy of that grid's record).  ev (optional): six
 // events recorded before each kernel and after the last.  learned: start the Newton
 // iteration from the MLP guess (every record's `guess` must point at packed weights).
+// contiguous: every grid's pencils run along the contiguous axis (sa == 1, the x
+// sweep); the update kernel then stages its stores.
 void launch_sweep_batch(const BatchArgs& B, int64_t march_blocks, int64_t riemann_blocks,
-                        bool dual, bool grav, cudaStream_t st, cudaEvent_t* ev, bool learned) {
-  if (dual && grav) split::launch_any<true, true>(B, march_blocks, riemann_blocks, st, ev, learned);
-  else if (dual) split::launch_any<true, false>(B, march_blocks, riemann_blocks, st, ev, learned);
-  else if (grav) split::launch_any<false, true>(B, march_blocks, riemann_blocks, st, ev, learned);
-  else split::launch_any<false, false>(B, march_blocks, riemann_blocks, st, ev, learned);
+                        bool dual, bool grav, cudaStream_t st, cudaEvent_t* ev, bool learned,
+                        bool contiguous) {
+  const int64_t mb = march_blocks, rb = riemann_blocks;
+  if (dual && grav) split::launch_any<true, true>(B, mb, rb, st, ev, learned, contiguous);
+  else if (dual) split::launch_any<true, false>(B, mb, rb, st, ev, learned, contiguous);
+  else if (grav) split::launch_any<false, true>(B, mb, rb, st, ev, learned, contiguous);
+  else split::launch_any<false, false>(B, mb, rb, st, ev, learned, contiguous);
 }
 
 }  // namespace ppm
