@@ -450,13 +450,51 @@ struct UpdateCounts {
   unsigned int fallbacks, fatal, nonfinite;
 };
 
-// Output staging of the x sweep.  Its pencils run along the contiguous axis, so a warp
-// storing one cell per pencil writes 32 separate sectors; instead every thread stores
-// its cells into shared memory, and every kStageCells cells the block writes them out
-// with consecutive lanes on consecutive cells of a pencil.  Layout [field][cell][pencil]
+// Staging of the x sweep's cells.  Its pencils run along the contiguous axis, so a warp
+// touching one cell per pencil touches 32 separate sectors; instead the block moves
+// kStageCells cells of all its pencils at a time between global and shared memory,
+// with consecutive lanes on consecutive cells of a pencil, and every thread reads and
+// writes its own cells in shared memory.  Layout [field][cell][pencil]
 // with a padded row (kStageLd) so that the flush reads hit distinct banks.
 enum { kStageCells = 4, kStageLd = kMarchThreads + 8 };
 constexpr int kStageField = kStageCells * kStageLd;
+
+// The matching input side: the block reads the next kStageCells cells of all its
+// pencils with consecutive lanes on consecutive cells, so the x sweep's loads do not
+// depend on L1 holding a line per pencil and field.
+template <bool DUAL>
+__device__ __forceinline__ void fill_stage(const SweepArgs& a, double* stage, int64_t pid0,
+                                           int c0, int ncells) {
+  __syncthreads();  // every thread is done with the previous chunk
+  for (int q = threadIdx.x; q < kMarchThreads * kStageCells; q += kMarchThreads) {
+    const int j = q % kStageCells, p = q / kStageCells;
+    const int64_t pid = pid0 + p;
+    if (j < ncells && pid < a.npencils) {
+      const int64_t off = (pid % a.n1) * a.s1 + (pid / a.n1) * a.s2 + (c0 + j);  // sa == 1
+      double* sp = stage + j * kStageLd + p;
+      sp[0] = __ldg(a.in_d + off);
+      sp[kStageField] = __ldg(a.in_e + off);
+      sp[2 * kStageField] = ldg0(a.in_u, off);
+      sp[3 * kStageField] = ldg0(a.in_v, off);
+      sp[4 * kStageField] = ldg0(a.in_w, off);
+      if (DUAL) sp[5 * kStageField] = __ldg(a.in_ge + off);
+    }
+  }
+  __syncthreads();
+}
+
+template <bool DUAL>
+__device__ __forceinline__ Cell staged_cell(const double* stage, int c) {
+  const double* sp = stage + (c % kStageCells) * kStageLd + threadIdx.x;
+  Cell r;
+  r.d = sp[0];
+  r.e = sp[kStageField];
+  r.u = sp[2 * kStageField];
+  r.v = sp[3 * kStageField];
+  r.w = sp[4 * kStageField];
+  r.ge = DUAL ? sp[5 * kStageField] : 0.0;
+  return r;
+}
 
 template <bool DUAL>
 __device__ __forceinline__ void flush_stage(const SweepArgs& a, const double* stage,
@@ -488,7 +526,8 @@ __device__ __forceinline__ void flush_stage(const SweepArgs& a, const double* st
 template <bool DUAL, bool GRAV, bool FALLBACK, bool STAGED = false>
 __device__ __forceinline__ bool update_pencil(const SweepArgs& a, int64_t pid, const Phys& P,
                                               UpdateCounts& cnt, bool valid = true,
-                                              double* stage = nullptr, int64_t pid0 = 0) {
+                                              double* stage = nullptr, int64_t pid0 = 0,
+                                              double* stage_in = nullptr) {
   bool live = valid, flagged = false;
   const int64_t base = live ? (pid % a.n1) * a.s1 + (pid / a.n1) * a.s2 : 0;
   const int64_t sa = a.sa, np = a.npencils;
@@ -519,7 +558,7 @@ __device__ __forceinline__ bool update_pencil(const SweepArgs& a, int64_t pid, c
   Cell Cpf = Cm;
   Flux Fpf = F0;
   if (live) {
-    Cpf = load_cell<DUAL>(a, base);
+    if (!STAGED) Cpf = load_cell<DUAL>(a, base);
     if (0 >= is && 0 <= ie) Fpf = load_flux(a, (int64_t)(1 - is) * np + pid);
   }
 
@@ -530,12 +569,15 @@ __device__ __forceinline__ bool update_pencil(const SweepArgs& a, int64_t pid, c
     Flux F1 = F0;
     bool gov_next = false;
     double govv_next = 0.0;
+    // block-wide: the next chunk of input cells (same steps on every thread)
+    if (STAGED && t < n && t % kStageCells == 0)
+      fill_stage<DUAL>(a, stage_in, pid0, t, min(kStageCells, n - t));
     // (1) check of cell t
     if (live && t < n) {
-      Cn = Cpf;
+      Cn = STAGED ? staged_cell<DUAL>(stage_in, t) : Cpf;
       if (t >= is && t <= ie) F1 = Fpf;
       if (t + 1 < n) {
-        Cpf = load_cell<DUAL>(a, base + (int64_t)(t + 1) * sa);
+        if (!STAGED) Cpf = load_cell<DUAL>(a, base + (int64_t)(t + 1) * sa);
         if (t + 1 >= is && t + 1 <= ie) Fpf = load_flux(a, (int64_t)(t + 2 - is) * np + pid);
       }
       if (t >= is && t <= ie) {
@@ -674,7 +716,10 @@ template <bool DUAL, bool GRAV, bool ONE, bool STAGED>
 __global__ void __launch_bounds__(kMarchThreads, PPM_UPDATE_MINBLOCKS)
     update_kernel(const __grid_constant__ BatchArgs B) {
   __shared__ unsigned long long s_cnt[2];
-  __shared__ double s_stage[STAGED ? 6 * kStageField : 1];
+  // STAGED: output and input staging buffers in dynamic shared memory (2 x 6 fields)
+  extern __shared__ __align__(16) unsigned char s_dyn[];
+  double* s_stage = reinterpret_cast<double*>(s_dyn);
+  double* s_stage_in = s_stage + 6 * kStageField;
   if (threadIdx.x < 2) s_cnt[threadIdx.x] = 0ull;
   int64_t lb;
   const int g = locate<ONE>(B.march_prefix, B.ngrids, lb);
@@ -686,7 +731,8 @@ __global__ void __launch_bounds__(kMarchThreads, PPM_UPDATE_MINBLOCKS)
   if (STAGED || valid) {
     const Phys P = make_phys(a);
     UpdateCounts cnt = {0, 0, 0};
-    if (update_pencil<DUAL, GRAV, false, STAGED>(a, pid, P, cnt, valid, s_stage, pid0)) {
+    if (update_pencil<DUAL, GRAV, false, STAGED>(a, pid, P, cnt, valid, s_stage, pid0,
+                                                 s_stage_in)) {
       const unsigned long long slot = atomicAdd(&B.counters[kCntFlagged], 1ull);
       B.flagged[slot] = ((int64_t)g << 40) | pid;
     } else {
@@ -735,8 +781,12 @@ void launch_stages(const BatchArgs& B, int64_t march_blocks, int64_t riemann_blo
   else
     riemann_kernel<DUAL, ONE, false><<<(unsigned)riemann_blocks, kRiemannThreads, 0, st>>>(B);
   mark(3);
-  if (staged)
-    update_kernel<DUAL, GRAV, ONE, true><<<(unsigned)march_blocks, kMarchThreads, 0, st>>>(B);
+  if (staged) {
+    constexpr int smem = 2 * 6 * kStageField * (int)sizeof(double);  // above 48 KB: opt in
+    cudaFuncSetAttribute(update_kernel<DUAL, GRAV, ONE, true>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    update_kernel<DUAL, GRAV, ONE, true><<<(unsigned)march_blocks, kMarchThreads, smem, st>>>(B);
+  }
   else
     update_kernel<DUAL, GRAV, ONE, false><<<(unsigned)march_blocks, kMarchThreads, 0, st>>>(B);
   mark(4);
