@@ -450,57 +450,25 @@ struct UpdateCounts {
   unsigned int fallbacks, fatal, nonfinite;
 };
 
-// Staging of the x sweep's cells.  Its pencils run along the contiguous axis, so a warp
-// touching one cell per pencil touches 32 separate sectors; instead the block moves
-// kStageCells cells of all its pencils at a time between global and shared memory,
-// with consecutive lanes on consecutive cells of a pencil, and every thread reads and
-// writes its own cells in shared memory.  Layout [field][cell][pencil]
-// with a padded row (kStageLd) so that the flush reads hit distinct banks.
-enum { kStageCells = 4, kStageLd = kMarchThreads + 8 };
+// Output staging of the x sweep.  Its pencils run along the contiguous axis, so a warp
+// storing one cell per pencil writes 32 separate sectors; instead every thread stores
+// its cells into shared memory, and every kStageCells cells each warp writes out its
+// 32 pencils' cells with consecutive lanes on consecutive cells of a pencil (warp-local:
+// no block barrier).  Layout per warp [field][cell][lane], the cell row padded
+// (kStageLd) so that the flush reads hit distinct banks.
+enum { kStageCells = 4, kStageLd = 32 + 8 };
 constexpr int kStageField = kStageCells * kStageLd;
+constexpr int kStageWarp = 6 * kStageField;  // doubles per warp
 
-// The matching input side: the block reads the next kStageCells cells of all its
-// pencils with consecutive lanes on consecutive cells, so the x sweep's loads do not
-// depend on L1 holding a line per pencil and field.
-template <bool DUAL>
-__device__ __forceinline__ void fill_stage(const SweepArgs& a, double* stage, int64_t pid0,
-                                           int c0, int ncells) {
-  __syncthreads();  // every thread is done with the previous chunk
-  for (int q = threadIdx.x; q < kMarchThreads * kStageCells; q += kMarchThreads) {
-    const int j = q % kStageCells, p = q / kStageCells;
-    const int64_t pid = pid0 + p;
-    if (j < ncells && pid < a.npencils) {
-      const int64_t off = (pid % a.n1) * a.s1 + (pid / a.n1) * a.s2 + (c0 + j);  // sa == 1
-      double* sp = stage + j * kStageLd + p;
-      sp[0] = __ldg(a.in_d + off);
-      sp[kStageField] = __ldg(a.in_e + off);
-      sp[2 * kStageField] = ldg0(a.in_u, off);
-      sp[3 * kStageField] = ldg0(a.in_v, off);
-      sp[4 * kStageField] = ldg0(a.in_w, off);
-      if (DUAL) sp[5 * kStageField] = __ldg(a.in_ge + off);
-    }
-  }
-  __syncthreads();
-}
-
-template <bool DUAL>
-__device__ __forceinline__ Cell staged_cell(const double* stage, int c) {
-  const double* sp = stage + (c % kStageCells) * kStageLd + threadIdx.x;
-  Cell r;
-  r.d = sp[0];
-  r.e = sp[kStageField];
-  r.u = sp[2 * kStageField];
-  r.v = sp[3 * kStageField];
-  r.w = sp[4 * kStageField];
-  r.ge = DUAL ? sp[5 * kStageField] : 0.0;
-  return r;
-}
-
+// stage: this warp's buffer; pid0: the warp's first pencil
 template <bool DUAL>
 __device__ __forceinline__ void flush_stage(const SweepArgs& a, const double* stage,
                                             int64_t pid0, int c0, int ncells) {
-  __syncthreads();  // every thread has staged its cells
-  for (int q = threadIdx.x; q < kMarchThreads * kStageCells; q += kMarchThreads) {
+  __syncwarp();  // every lane has staged its cells
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int r = 0; r < kStageCells; ++r) {
+    const int q = lane + 32 * r;
     const int j = q % kStageCells, p = q / kStageCells;
     const int64_t pid = pid0 + p;
     if (j < ncells && pid < a.npencils) {
@@ -514,20 +482,18 @@ __device__ __forceinline__ void flush_stage(const SweepArgs& a, const double* st
       if (DUAL) a.out_ge[off] = sp[5 * kStageField];
     }
   }
-  __syncthreads();  // the staging buffer may be refilled
+  __syncwarp();  // the buffer may be refilled
 }
 
 //
-// STAGED (x sweep, hot pass only): every thread of the block runs the same steps,
-// including threads without a pencil (valid = false) and threads whose pencil was
-// flagged, since the block flushes the staged outputs together; those threads skip all
-// loads and computation.  A flagged pencil's partial outputs are rewritten by the
+// STAGED (x sweep, hot pass only): every lane of a warp runs the same steps, including
+// lanes without a pencil (valid = false) and lanes whose pencil was flagged, since the
+// warp flushes the staged outputs together; those lanes skip all loads and computation.  A flagged pencil's partial outputs are rewritten by the
 // fallback pass.
 template <bool DUAL, bool GRAV, bool FALLBACK, bool STAGED = false>
 __device__ __forceinline__ bool update_pencil(const SweepArgs& a, int64_t pid, const Phys& P,
                                               UpdateCounts& cnt, bool valid = true,
-                                              double* stage = nullptr, int64_t pid0 = 0,
-                                              double* stage_in = nullptr) {
+                                              double* stage = nullptr, int64_t pid0 = 0) {
   bool live = valid, flagged = false;
   const int64_t base = live ? (pid % a.n1) * a.s1 + (pid / a.n1) * a.s2 : 0;
   const int64_t sa = a.sa, np = a.npencils;
@@ -558,7 +524,7 @@ __device__ __forceinline__ bool update_pencil(const SweepArgs& a, int64_t pid, c
   Cell Cpf = Cm;
   Flux Fpf = F0;
   if (live) {
-    if (!STAGED) Cpf = load_cell<DUAL>(a, base);
+    Cpf = load_cell<DUAL>(a, base);
     if (0 >= is && 0 <= ie) Fpf = load_flux(a, (int64_t)(1 - is) * np + pid);
   }
 
@@ -569,15 +535,12 @@ __device__ __forceinline__ bool update_pencil(const SweepArgs& a, int64_t pid, c
     Flux F1 = F0;
     bool gov_next = false;
     double govv_next = 0.0;
-    // block-wide: the next chunk of input cells (same steps on every thread)
-    if (STAGED && t < n && t % kStageCells == 0)
-      fill_stage<DUAL>(a, stage_in, pid0, t, min(kStageCells, n - t));
     // (1) check of cell t
     if (live && t < n) {
-      Cn = STAGED ? staged_cell<DUAL>(stage_in, t) : Cpf;
+      Cn = Cpf;
       if (t >= is && t <= ie) F1 = Fpf;
       if (t + 1 < n) {
-        if (!STAGED) Cpf = load_cell<DUAL>(a, base + (int64_t)(t + 1) * sa);
+        Cpf = load_cell<DUAL>(a, base + (int64_t)(t + 1) * sa);
         if (t + 1 >= is && t + 1 <= ie) Fpf = load_flux(a, (int64_t)(t + 2 - is) * np + pid);
       }
       if (t >= is && t <= ie) {
@@ -640,7 +603,7 @@ __device__ __forceinline__ bool update_pencil(const SweepArgs& a, int64_t pid, c
         }
         if (!isfinite(o.d) || !isfinite(o.e)) nonfin += 1;
         if (STAGED) {
-          double* sp = stage + (c % kStageCells) * kStageLd + threadIdx.x;
+          double* sp = stage + (c % kStageCells) * kStageLd + (threadIdx.x & 31);
           sp[0] = o.d;
           sp[kStageField] = o.e;
           sp[2 * kStageField] = o.u;
@@ -657,7 +620,7 @@ __device__ __forceinline__ bool update_pencil(const SweepArgs& a, int64_t pid, c
           if (DUAL) a.out_ge[off] = o.ge;
         }
       }
-      // block-wide: the same steps on every thread
+      // warp-wide: the same steps on every lane
       if (STAGED && c >= 0 && c % kStageCells == kStageCells - 1)
         flush_stage<DUAL>(a, stage, pid0, c - (kStageCells - 1), kStageCells);
     }
@@ -681,7 +644,7 @@ __device__ __forceinline__ bool update_pencil(const SweepArgs& a, int64_t pid, c
       }
       if (!isfinite(o.d) || !isfinite(o.e)) nonfin += 1;
       if (STAGED) {
-        double* sp = stage + (c % kStageCells) * kStageLd + threadIdx.x;
+        double* sp = stage + (c % kStageCells) * kStageLd + (threadIdx.x & 31);
         sp[0] = o.d;
         sp[kStageField] = o.e;
         sp[2 * kStageField] = o.u;
@@ -716,23 +679,20 @@ template <bool DUAL, bool GRAV, bool ONE, bool STAGED>
 __global__ void __launch_bounds__(kMarchThreads, PPM_UPDATE_MINBLOCKS)
     update_kernel(const __grid_constant__ BatchArgs B) {
   __shared__ unsigned long long s_cnt[2];
-  // STAGED: output and input staging buffers in dynamic shared memory (2 x 6 fields)
-  extern __shared__ __align__(16) unsigned char s_dyn[];
-  double* s_stage = reinterpret_cast<double*>(s_dyn);
-  double* s_stage_in = s_stage + 6 * kStageField;
+  __shared__ double s_stage[STAGED ? (kMarchThreads / 32) * kStageWarp : 1];  // per warp
   if (threadIdx.x < 2) s_cnt[threadIdx.x] = 0ull;
   int64_t lb;
   const int g = locate<ONE>(B.march_prefix, B.ngrids, lb);
   PPM_BIND_RECORD(a, g)
   if (ONE) __syncthreads();
-  const int64_t pid0 = lb * kMarchThreads;
-  const int64_t pid = pid0 + threadIdx.x;
+  const int64_t pid = lb * kMarchThreads + threadIdx.x;
+  const int64_t wpid0 = pid - (threadIdx.x & 31);  // first pencil of this warp
   const bool valid = pid < a.npencils;
   if (STAGED || valid) {
     const Phys P = make_phys(a);
     UpdateCounts cnt = {0, 0, 0};
-    if (update_pencil<DUAL, GRAV, false, STAGED>(a, pid, P, cnt, valid, s_stage, pid0,
-                                                 s_stage_in)) {
+    if (update_pencil<DUAL, GRAV, false, STAGED>(
+            a, pid, P, cnt, valid, s_stage + (threadIdx.x >> 5) * kStageWarp, wpid0)) {
       const unsigned long long slot = atomicAdd(&B.counters[kCntFlagged], 1ull);
       B.flagged[slot] = ((int64_t)g << 40) | pid;
     } else {
@@ -781,12 +741,8 @@ void launch_stages(const BatchArgs& B, int64_t march_blocks, int64_t riemann_blo
   else
     riemann_kernel<DUAL, ONE, false><<<(unsigned)riemann_blocks, kRiemannThreads, 0, st>>>(B);
   mark(3);
-  if (staged) {
-    constexpr int smem = 2 * 6 * kStageField * (int)sizeof(double);  // above 48 KB: opt in
-    cudaFuncSetAttribute(update_kernel<DUAL, GRAV, ONE, true>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    update_kernel<DUAL, GRAV, ONE, true><<<(unsigned)march_blocks, kMarchThreads, smem, st>>>(B);
-  }
+  if (staged)
+    update_kernel<DUAL, GRAV, ONE, true><<<(unsigned)march_blocks, kMarchThreads, 0, st>>>(B);
   else
     update_kernel<DUAL, GRAV, ONE, false><<<(unsigned)march_blocks, kMarchThreads, 0, st>>>(B);
   mark(4);
