@@ -450,68 +450,15 @@ struct UpdateCounts {
   unsigned int fallbacks, fatal, nonfinite;
 };
 
-// Staging of the x sweep.  Its pencils run along the contiguous axis, so a warp that
-// loads or stores one cell per pencil touches 32 separate sectors.  Instead each warp
-// moves kStageCells cells of its 32 pencils at a time, consecutive lanes on consecutive
-// cells of a pencil, between global and shared memory, and every lane reads and writes
-// its own cells in shared memory (warp-local: no block barrier):
-//   input:  double-buffered chunks filled with cp.async one chunk ahead of use,
-//           layout [buffer][field][cell][lane];
-//   output: one chunk written out when full, layout [field][cell][lane], the cell row
-//           padded to kStageLd so that the write-out reads mostly hit distinct banks.
-enum { kStageCells = 4, kStageLd = 33 };
+// Output staging of the x sweep.  Its pencils run along the contiguous axis, so a warp
+// storing one cell per pencil writes 32 separate sectors; instead every thread stores
+// its cells into shared memory, and every kStageCells cells each warp writes out its
+// 32 pencils' cells with consecutive lanes on consecutive cells of a pencil (warp-local:
+// no block barrier).  Layout per warp [field][cell][lane], the cell row padded
+// (kStageLd) so that the flush reads hit distinct banks.
+enum { kStageCells = 4, kStageLd = 32 + 8 };
 constexpr int kStageField = kStageCells * kStageLd;
-constexpr int kStageWarp = 6 * kStageField;         // output doubles per warp
-constexpr int kStageInField = kStageCells * 32;
-constexpr int kStageInWarp = 2 * 6 * kStageInField;  // input doubles per warp
-constexpr int kStageBytes = (kMarchThreads / 32) * (kStageWarp + kStageInWarp) * 8;
-
-__device__ __forceinline__ void cp_async8(double* dst, const double* src) {
-  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() {
-  asm volatile("cp.async.commit_group;\n" ::: "memory");
-}
-__device__ __forceinline__ void cp_async_wait_1() {
-  asm volatile("cp.async.wait_group 1;\n" ::: "memory");
-}
-
-// Queue the copies of cells c0 .. c0 + ncells - 1 of the warp's pencils into `buf`.
-template <bool DUAL>
-__device__ __forceinline__ void fill_chunk(const SweepArgs& a, double* buf, int64_t pid0, int c0,
-                                           int ncells) {
-  const int lane = threadIdx.x & 31;
-#pragma unroll
-  for (int r = 0; r < kStageCells; ++r) {
-    const int q = lane + 32 * r;
-    const int j = q % kStageCells, p = q / kStageCells;
-    const int64_t pid = pid0 + p;
-    if (j < ncells && pid < a.npencils) {
-      const int64_t off = (pid % a.n1) * a.s1 + (pid / a.n1) * a.s2 + (c0 + j);  // sa == 1
-      double* d = buf + j * 32 + p;
-      cp_async8(d, a.in_d + off);
-      cp_async8(d + kStageInField, a.in_e + off);
-      if (a.in_u) cp_async8(d + 2 * kStageInField, a.in_u + off);
-      if (a.in_v) cp_async8(d + 3 * kStageInField, a.in_v + off);
-      if (a.in_w) cp_async8(d + 4 * kStageInField, a.in_w + off);
-      if (DUAL) cp_async8(d + 5 * kStageInField, a.in_ge + off);
-    }
-  }
-}
-
-template <bool DUAL>
-__device__ __forceinline__ Cell staged_cell(const SweepArgs& a, const double* buf, int j) {
-  const double* sp = buf + j * 32 + (threadIdx.x & 31);
-  Cell r;
-  r.d = sp[0];
-  r.e = sp[kStageInField];
-  r.u = a.in_u ? sp[2 * kStageInField] : 0.0;
-  r.v = a.in_v ? sp[3 * kStageInField] : 0.0;
-  r.w = a.in_w ? sp[4 * kStageInField] : 0.0;
-  r.ge = DUAL ? sp[5 * kStageInField] : 0.0;
-  return r;
-}
+constexpr int kStageWarp = 6 * kStageField;  // doubles per warp
 
 // stage: this warp's buffer; pid0: the warp's first pencil
 template <bool DUAL>
@@ -546,8 +493,7 @@ __device__ __forceinline__ void flush_stage(const SweepArgs& a, const double* st
 template <bool DUAL, bool GRAV, bool FALLBACK, bool STAGED = false>
 __device__ __forceinline__ bool update_pencil(const SweepArgs& a, int64_t pid, const Phys& P,
                                               UpdateCounts& cnt, bool valid = true,
-                                              double* stage = nullptr, int64_t pid0 = 0,
-                                              double* stage_in = nullptr) {
+                                              double* stage = nullptr, int64_t pid0 = 0) {
   bool live = valid, flagged = false;
   const int64_t base = live ? (pid % a.n1) * a.s1 + (pid / a.n1) * a.s2 : 0;
   const int64_t sa = a.sa, np = a.npencils;
@@ -578,12 +524,8 @@ __device__ __forceinline__ bool update_pencil(const SweepArgs& a, int64_t pid, c
   Cell Cpf = Cm;
   Flux Fpf = F0;
   if (live) {
-    if (!STAGED) Cpf = load_cell<DUAL>(a, base);
+    Cpf = load_cell<DUAL>(a, base);
     if (0 >= is && 0 <= ie) Fpf = load_flux(a, (int64_t)(1 - is) * np + pid);
-  }
-  if (STAGED) {  // warp-wide: the first chunk of input cells
-    fill_chunk<DUAL>(a, stage_in, pid0, 0, min((int)kStageCells, n));
-    cp_async_commit();
   }
 
 #pragma unroll 1
@@ -593,26 +535,12 @@ __device__ __forceinline__ bool update_pencil(const SweepArgs& a, int64_t pid, c
     Flux F1 = F0;
     bool gov_next = false;
     double govv_next = 0.0;
-    // warp-wide (same steps on every lane): at a chunk start, queue the next chunk into
-    // the other buffer (its previous contents are consumed) and wait for this one
-    if (STAGED && t < n && t % kStageCells == 0) {
-      __syncwarp();
-      const int k = t / kStageCells;
-      if (t + kStageCells < n)
-        fill_chunk<DUAL>(a, stage_in + ((k + 1) & 1) * 6 * kStageInField, pid0,
-                         t + kStageCells, min((int)kStageCells, n - t - kStageCells));
-      cp_async_commit();
-      cp_async_wait_1();
-      __syncwarp();
-    }
     // (1) check of cell t
     if (live && t < n) {
-      Cn = STAGED ? staged_cell<DUAL>(a, stage_in + ((t / kStageCells) & 1) * 6 * kStageInField,
-                                      t % kStageCells)
-                  : Cpf;
+      Cn = Cpf;
       if (t >= is && t <= ie) F1 = Fpf;
       if (t + 1 < n) {
-        if (!STAGED) Cpf = load_cell<DUAL>(a, base + (int64_t)(t + 1) * sa);
+        Cpf = load_cell<DUAL>(a, base + (int64_t)(t + 1) * sa);
         if (t + 1 >= is && t + 1 <= ie) Fpf = load_flux(a, (int64_t)(t + 2 - is) * np + pid);
       }
       if (t >= is && t <= ie) {
@@ -751,9 +679,7 @@ template <bool DUAL, bool GRAV, bool ONE, bool STAGED>
 __global__ void __launch_bounds__(kMarchThreads, PPM_UPDATE_MINBLOCKS)
     update_kernel(const __grid_constant__ BatchArgs B) {
   __shared__ unsigned long long s_cnt[2];
-  // STAGED: per warp an output buffer and a double input buffer (dynamic shared memory)
-  extern __shared__ __align__(16) double s_dyn[];
-  double* s_stage = s_dyn + (threadIdx.x >> 5) * (kStageWarp + kStageInWarp);
+  __shared__ double s_stage[STAGED ? (kMarchThreads / 32) * kStageWarp : 1];  // per warp
   if (threadIdx.x < 2) s_cnt[threadIdx.x] = 0ull;
   int64_t lb;
   const int g = locate<ONE>(B.march_prefix, B.ngrids, lb);
@@ -765,8 +691,8 @@ __global__ void __launch_bounds__(kMarchThreads, PPM_UPDATE_MINBLOCKS)
   if (STAGED || valid) {
     const Phys P = make_phys(a);
     UpdateCounts cnt = {0, 0, 0};
-    if (update_pencil<DUAL, GRAV, false, STAGED>(a, pid, P, cnt, valid, s_stage, wpid0,
-                                                 s_stage + kStageWarp)) {
+    if (update_pencil<DUAL, GRAV, false, STAGED>(
+            a, pid, P, cnt, valid, s_stage + (threadIdx.x >> 5) * kStageWarp, wpid0)) {
       const unsigned long long slot = atomicAdd(&B.counters[kCntFlagged], 1ull);
       B.flagged[slot] = ((int64_t)g << 40) | pid;
     } else {
@@ -815,12 +741,8 @@ void launch_stages(const BatchArgs& B, int64_t march_blocks, int64_t riemann_blo
   else
     riemann_kernel<DUAL, ONE, false><<<(unsigned)riemann_blocks, kRiemannThreads, 0, st>>>(B);
   mark(3);
-  if (staged) {
-    cudaFuncSetAttribute(update_kernel<DUAL, GRAV, ONE, true>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize, kStageBytes);
-    update_kernel<DUAL, GRAV, ONE, true>
-        <<<(unsigned)march_blocks, kMarchThreads, kStageBytes, st>>>(B);
-  }
+  if (staged)
+    update_kernel<DUAL, GRAV, ONE, true><<<(unsigned)march_blocks, kMarchThreads, 0, st>>>(B);
   else
     update_kernel<DUAL, GRAV, ONE, false><<<(unsigned)march_blocks, kMarchThreads, 0, st>>>(B);
   mark(4);
