@@ -34,6 +34,7 @@ struct ElemGrid {
   double* p;
   double* f[6];
   const double* cw[3];
+  const double* old[6];
   int rank;
   int dims[3], start[3], end[3];
   int bc[3];
@@ -48,7 +49,10 @@ struct ElemBatch {
   double gamma, tiny_number, min_support;
   double aye, vg[3];
   unsigned long long* min_bits;
+  double expansion, coef_new, coef_old;
+  int interpolate;
 };
+void launch_expansion_batch(const ElemBatch& B, int64_t blocks, cudaStream_t st);
 void launch_sweep_batch(const BatchArgs& B, int64_t march_blocks, int64_t riemann_blocks,
                         bool dual, bool grav, cudaStream_t st, cudaEvent_t* ev, bool learned,
                         bool contiguous);
@@ -105,7 +109,8 @@ enum {
   kSlotCw = 13,        // cell widths of the time-step kernel
   kSlotTimestep = 14,  // element records of the time-step kernel
   kSlotBoundary = 15,  // element records of the ghost-fill kernel
-  kSlotCount = 16
+  kSlotExpansion = 16, // element records of the comoving-expansion kernel
+  kSlotCount = 17
 };
 // captured level graphs kept at most (a changed grid list leaves the old ones unused)
 constexpr size_t kMaxGraphs = 16;
@@ -122,6 +127,7 @@ struct ppm_b200_context {
   // persistent device scratch, grown on demand
   DevBuf host_set[6];       // device copies of host-memory fields (single grid)
   DevBuf host_acc[3];       // device copies of host-memory accelerations
+  DevBuf host_old[6];       // device copies of host-memory fields at OldTime
   DevBuf ring;              // two ring sets of the six updated fields, every grid of the batch
   DevBuf pressure;          // pressure of every grid of the batch
   DevBuf face_scratch;      // interface states, fluxes and the flagged-pencil list
@@ -710,7 +716,8 @@ struct ElemPlan {
 };
 
 int prepare_elem(ppm_b200_context* ctx, int slot, const ppm_b200_params* p,
-                 const std::vector<GridIO>& io, bool with_cw, const int* bc, ElemPlan& plan) {
+                 const std::vector<GridIO>& io, bool with_cw, const int* bc, ElemPlan& plan,
+                 const std::vector<FieldSet>* old = nullptr) {
   const int ng = (int)io.size();
   std::vector<ElemGrid> rec(ng);
   std::vector<int64_t> spre(ng + 1, 0), apre(ng + 1, 0);
@@ -758,6 +765,8 @@ int prepare_elem(ppm_b200_context* ctx, int slot, const ppm_b200_params* p,
       e.end[d] = g->end[d];
       e.bc[d] = bc ? bc[d] : 0;
     }
+    if (old)
+      for (int n = 0; n < 6; ++n) e.old[n] = (*old)[k].f[n];
     e.rank = g->rank;
     e.size = grid_size(g);
     e.active = grid_active(g);
@@ -785,6 +794,8 @@ int prepare_elem(ppm_b200_context* ctx, int slot, const ppm_b200_params* p,
   plan.B.aye = 1.0;
   plan.B.vg[0] = plan.B.vg[1] = plan.B.vg[2] = 0.0;
   plan.B.min_bits = (unsigned long long*)ctx->misc.p;
+  plan.B.expansion = plan.B.coef_new = plan.B.coef_old = 0.0;
+  plan.B.interpolate = 0;
   plan.size_blocks = spre[ng];
   plan.active_blocks = apre[ng];
   return PPM_B200_OK;
@@ -1069,6 +1080,7 @@ int ppm_b200_destroy(ppm_b200_context* ctx) {
   };
   for (auto& b : ctx->host_set) fr(b);
   for (auto& b : ctx->host_acc) fr(b);
+  for (auto& b : ctx->host_old) fr(b);
   fr(ctx->ring);
   fr(ctx->pressure);
   fr(ctx->face_scratch);
@@ -1405,6 +1417,110 @@ static int boundary_batch(ppm_b200_context* ctx, ppm_b200_grid* grids, int ngrid
   ctx->launches += 1;
   CK(cudaGetLastError());
   return PPM_B200_OK;
+}
+
+// Old fields of a grid on the device: device pointers as given, or copies of host arrays.
+static int stage_old(ppm_b200_context* ctx, const ppm_b200_params* p, const ppm_b200_grid* g,
+                     const ppm_b200_grid* old, int memory, FieldSet& fs) {
+  const double* src[6] = {old->density, old->total_energy, old->velocity[0],
+                          g->rank > 1 ? old->velocity[1] : nullptr,
+                          g->rank > 2 ? old->velocity[2] : nullptr,
+                          p->dual_energy ? old->gas_energy : nullptr};
+  if (!src[0] || !src[1] || !src[2] || (g->rank > 1 && !src[3]) || (g->rank > 2 && !src[4]) ||
+      (p->dual_energy && !src[5]))
+    return PPM_B200_ERR_INVALID;
+  for (int d = 0; d < 3; ++d)
+    if (old->dims[d] != g->dims[d]) return PPM_B200_ERR_INVALID;
+  const size_t bytes = (size_t)grid_size(g) * sizeof(double);
+  for (int k = 0; k < 6; ++k) {
+    fs.f[k] = nullptr;
+    if (!src[k]) continue;
+    if (memory == PPM_B200_MEM_DEVICE) {
+      fs.f[k] = const_cast<double*>(src[k]);
+    } else {
+      int rc = ensure(ctx, ctx->host_old[k], bytes);
+      if (rc) return rc;
+      CK(cudaMemcpyAsync(ctx->host_old[k].p, src[k], bytes, cudaMemcpyHostToDevice,
+                         ctx->stream));
+      fs.f[k] = (double*)ctx->host_old[k].p;
+    }
+  }
+  return PPM_B200_OK;
+}
+
+// grid::ComovingExpansionTerms over a batch (see ppm_b200_expansion_terms).
+static int expansion_batch(ppm_b200_context* ctx, const ppm_b200_params* p,
+                           std::vector<GridIO>& io, const std::vector<FieldSet>* old,
+                           double time, double old_time, double coefficient) {
+  ElemPlan ep;
+  int rc = prepare_elem(ctx, kSlotExpansion, p, io, false, nullptr, ep, old);
+  if (rc) return rc;
+  ep.B.expansion = coefficient;
+  // Grid_ComovingExpansionTerms.C:84-89 and Grid_ComputePressure.C:51-58: the mid time
+  // between OldTime and Time, as an interpolation weight of the current fields
+  ep.B.interpolate = 0;
+  if (old) {
+    const double ptime = 0.5 * (time + old_time);
+    if (ptime != time) {
+      double coef = 1.0;
+      if (time - old_time > 0) coef = (ptime - old_time) / (time - old_time);
+      ep.B.coef_new = coef;
+      ep.B.coef_old = 1 - coef;
+      ep.B.interpolate = 1;
+    }
+  }
+  ppm::launch_expansion_batch(ep.B, ep.size_blocks, ctx->stream);
+  ctx->launches += 1;
+  CK(cudaGetLastError());
+  return PPM_B200_OK;
+}
+
+int ppm_b200_expansion_terms(ppm_b200_context* ctx, const ppm_b200_params* p, ppm_b200_grid* g,
+                             const ppm_b200_grid* old, double time, double old_time,
+                             double coefficient, int memory) {
+  if (!ctx || !p || !g) return PPM_B200_ERR_INVALID;
+  int rc = check_grid(g, p);
+  if (rc) return rc;
+  CK(cudaSetDevice(ctx->device));
+  std::vector<GridIO> io(1);
+  io[0].g = g;
+  rc = stage_in(ctx, p, g, memory, io[0].user, io[0].acc);
+  if (rc) return rc;
+  std::vector<FieldSet> ofs(1);
+  if (old) {
+    rc = stage_old(ctx, p, g, old, memory, ofs[0]);
+    if (rc) return rc;
+  }
+  rc = expansion_batch(ctx, p, io, old ? &ofs : nullptr, time, old_time, coefficient);
+  if (rc) return rc;
+  if (memory == PPM_B200_MEM_HOST) {
+    rc = stage_out(ctx, p, g, io[0].user);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(ctx->stream));
+  }
+  return PPM_B200_OK;
+}
+
+int ppm_b200_expansion_terms_level(ppm_b200_context* ctx, const ppm_b200_params* p,
+                                   ppm_b200_grid* grids, const ppm_b200_grid* olds,
+                                   int ngrids, double time, double old_time,
+                                   double coefficient) {
+  if (!ctx || !p || !grids || ngrids <= 0) return PPM_B200_ERR_INVALID;
+  CK(cudaSetDevice(ctx->device));
+  std::vector<GridIO> io(ngrids);
+  std::vector<FieldSet> ofs(ngrids);
+  for (int k = 0; k < ngrids; ++k) {
+    int rc = check_grid(&grids[k], p);
+    if (rc) return rc;
+    io[k].g = &grids[k];
+    rc = stage_in(ctx, p, &grids[k], PPM_B200_MEM_DEVICE, io[k].user, io[k].acc);
+    if (rc) return rc;
+    if (olds) {
+      rc = stage_old(ctx, p, &grids[k], &olds[k], PPM_B200_MEM_DEVICE, ofs[k]);
+      if (rc) return rc;
+    }
+  }
+  return expansion_batch(ctx, p, io, olds ? &ofs : nullptr, time, old_time, coefficient);
 }
 
 int ppm_b200_set_guess(ppm_b200_context* ctx, const float* weights) {

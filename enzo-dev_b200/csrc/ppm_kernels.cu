@@ -25,6 +25,7 @@ struct ElemGrid {
   double* p;            // pressure output (pressure kernel)
   double* f[6];         // fields filled by the ghost-zone kernel (null entries skipped)
   const double* cw[3];  // device cell widths (time-step kernel)
+  const double* old[6]; // fields at OldTime: d, te, v1, v2, v3, ge (expansion kernel)
   int rank;
   int dims[3], start[3], end[3];
   int bc[3];            // 0 periodic, 1 outflow, 2 left alone
@@ -40,6 +41,9 @@ struct ElemBatch {
   double gamma, tiny_number, min_support;
   double aye, vg[3];
   unsigned long long* min_bits;  // running minimum of dt1 (positive doubles order as integers)
+  // expansion kernel: dt * adot / a, and the pressure's interpolation weights
+  double expansion, coef_new, coef_old;
+  int interpolate;
 };
 
 // grid::ComputePressure at time == Time (Grid_ComputePressure.C:96-164)
@@ -162,6 +166,61 @@ __global__ void __launch_bounds__(256) boundary_kernel(const __grid_constant__ E
     if (G.f[n]) G.f[n][g] = G.f[n][src];
 }
 
+// ------------------------------------------------------------------ comoving expansion
+// grid::ComovingExpansionTerms for PPM (Grid_ComovingExpansionTerms.C:36-99 with
+// expand_terms.F, ENERGY_METHOD3 / VELOCITY_METHOD3) over every cell of every grid:
+// the pressure at the mid time, interpolated between the old and current fields
+// (Grid_ComputePressure.C:168-223) or at the current time, with
+// MinimumSupportEnergyCoefficient 0 (ComputePressure's default); then the gas energy,
+// total energy and velocity terms of the cell.
+__device__ __forceinline__ double cell_pressure_interp(const ElemGrid& G, int64_t i,
+                                                       const ElemBatch& B) {
+  const double coef = B.coef_new, coefold = B.coef_old;
+  double velocity2 = 0.0, velocity3 = 0.0, gas_energy;
+  const double total_energy = coef * __ldg(G.te + i) + coefold * __ldg(G.old[1] + i);
+  const double density = coef * __ldg(G.d + i) + coefold * __ldg(G.old[0] + i);
+  const double velocity1 = coef * __ldg(G.v[0] + i) + coefold * __ldg(G.old[2] + i);
+  if (G.v[1]) velocity2 = coef * __ldg(G.v[1] + i) + coefold * __ldg(G.old[3] + i);
+  if (G.v[2]) velocity3 = coef * __ldg(G.v[2] + i) + coefold * __ldg(G.old[4] + i);
+  if (!G.ge) {
+    const double kineticE =
+        0.5 * (velocity1 * velocity1 + velocity2 * velocity2 + velocity3 * velocity3);
+    gas_energy = total_energy - kineticE;
+  } else {
+    gas_energy = coef * __ldg(G.ge + i) + coefold * __ldg(G.old[5] + i);
+  }
+  const double gm1 = B.gamma - 1.0;
+  double p = gm1 * density * gas_energy;
+  if (p < B.tiny_number) p = B.tiny_number;
+  const double min_pressure = 0.0 * gm1 * density * density;  // coefficient 0
+  if (p < min_pressure) p = min_pressure;
+  return p;
+}
+
+__global__ void __launch_bounds__(256) expansion_kernel(const __grid_constant__ ElemBatch B) {
+  int64_t lb;
+  const ElemGrid& G = B.grids[batch_locate(B.size_prefix, B.ngrids, blockIdx.x, lb)];
+  const int64_t i = lb * 256 + threadIdx.x;
+  if (i >= G.size) return;
+  const double p = B.interpolate ? cell_pressure_interp(G, i, B)
+                                 : cell_pressure(G, i, B.gamma, B.tiny_number, 0.0);
+  const double coef = B.expansion;
+  double* d = G.f[0];
+  double* e = G.f[1];
+  if (G.f[5]) {  // gas energy (idual = 1)
+    double* ge = G.f[5];
+    ge[i] = ge[i] * (1.0 - coef) / (1.0 + coef);
+  }
+  double en = e[i] * (1.0 - coef) / (1.0 + coef);
+  const double a = en - coef * (3.0 - 2.0 / (B.gamma - 1.0)) * p / d[i];
+  const double b = 0.5 * en;
+  e[i] = a > b ? a : b;
+  for (int c = 0; c < G.rank; ++c) {
+    double* vel = G.f[2 + c];
+    vel[i] = vel[i] * (1.0 - 0.5 * coef) / (1.0 + 0.5 * coef);
+  }
+}
+
 // ------------------------------------------------------------------ launchers
 void launch_pressure_batch(const ElemBatch& B, int64_t blocks, cudaStream_t st) {
   pressure_kernel<<<(unsigned)blocks, 256, 0, st>>>(B);
@@ -172,6 +231,10 @@ void launch_timestep_batch(const ElemBatch& B, int64_t blocks, double courant, d
   cudaMemsetAsync(B.min_bits, 0xFF, sizeof(unsigned long long), st);
   timestep_kernel<<<(unsigned)blocks, 256, 0, st>>>(B);
   timestep_finalize_kernel<<<1, 32, 0, st>>>(B.min_bits, courant, dt_out);
+}
+
+void launch_expansion_batch(const ElemBatch& B, int64_t blocks, cudaStream_t st) {
+  expansion_kernel<<<(unsigned)blocks, 256, 0, st>>>(B);
 }
 
 void launch_boundary_batch(const ElemBatch& B, int64_t blocks, cudaStream_t st) {

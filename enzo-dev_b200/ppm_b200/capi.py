@@ -37,7 +37,8 @@ EXPORTS = (
     "ppm_b200_compute_timestep_level", "ppm_b200_set_boundary_level",
     "ppm_b200_profile_stages", "ppm_b200_set_guess", "ppm_b200_riemann_log",
     "ppm_b200_riemann_log_count", "ppm_b200_guess_features", "ppm_b200_guess_grad",
-    "ppm_b200_guess_adam", "ppm_b200_guess_eval",
+    "ppm_b200_guess_adam", "ppm_b200_guess_eval", "ppm_b200_expansion_terms",
+    "ppm_b200_expansion_terms_level",
 )
 
 GUESS_WEIGHTS = 4673  # W1[6][64] b1[64] W2[64][64] b2[64] w3[64] b3
@@ -150,6 +151,12 @@ def lib(build_if_missing: bool = True):
     L.ppm_b200_set_graphs.argtypes = [vp, C.c_int]
     fp = C.POINTER(C.c_float)
     L.ppm_b200_set_guess.argtypes = [vp, vp]
+    L.ppm_b200_expansion_terms.argtypes = [vp, C.POINTER(Params), C.POINTER(GridDesc),
+                                           C.POINTER(GridDesc), C.c_double, C.c_double,
+                                           C.c_double, C.c_int]
+    L.ppm_b200_expansion_terms_level.argtypes = [vp, C.POINTER(Params), C.POINTER(GridDesc),
+                                                 C.POINTER(GridDesc), C.c_int, C.c_double,
+                                                 C.c_double, C.c_double]
     L.ppm_b200_riemann_log.argtypes = [vp, vp, C.c_longlong, C.c_int]
     L.ppm_b200_riemann_log_count.argtypes = [vp, C.POINTER(C.c_longlong)]
     L.ppm_b200_guess_features.argtypes = [vp, vp, C.c_longlong, C.c_double, C.c_double, vp]
@@ -413,6 +420,31 @@ class Context:
         if rc != OK:
             raise PPMError(rc, "ppm_b200_profile_read")
         return ms.value, n.value
+
+    # ---- comoving expansion terms
+    def expansion_terms(self, grid, hp, fields, old, time, old_time, coefficient,
+                        memory=MEM_HOST):
+        """grid::ComovingExpansionTerms (in place); old: fields at OldTime or None."""
+        P = make_params(hp, 0.0)
+        G, keep = make_grid(grid, fields)
+        Og, keep2 = make_grid(grid, old) if old is not None else (None, None)
+        rc = self.L.ppm_b200_expansion_terms(self.h, C.byref(P), C.byref(G),
+                                             C.byref(Og) if Og is not None else None,
+                                             float(time), float(old_time), float(coefficient),
+                                             int(memory))
+        if rc != OK:
+            raise PPMError(rc, "ppm_b200_expansion_terms")
+
+    def expansion_terms_level(self, grids, hp, fields_list, olds, time, old_time,
+                              coefficient):
+        P = make_params(hp, 0.0)
+        arr, keep = self._level(grids, fields_list)
+        oarr, keep2 = self._level(grids, olds) if olds is not None else (None, None)
+        rc = self.L.ppm_b200_expansion_terms_level(self.h, C.byref(P), arr, oarr, len(grids),
+                                                   float(time), float(old_time),
+                                                   float(coefficient))
+        if rc != OK:
+            raise PPMError(rc, "ppm_b200_expansion_terms_level")
 
     # ---- learned Newton start
     def set_guess(self, weights):

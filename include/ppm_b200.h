@@ -208,6 +208,23 @@ int ppm_b200_profile_read(ppm_b200_context *ctx, double *sweep_ms, long long *sw
    a sweep (reconstruct d/p/u, reconstruct v/w/ge, Riemann, update, HLL fallback pass). */
 int ppm_b200_profile_stages(ppm_b200_context *ctx, double stage_ms[5]);
 
+/* grid::ComovingExpansionTerms for PPM (Grid_ComovingExpansionTerms.C:36-99 with
+   expand_terms.F, ENERGY_METHOD3 / VELOCITY_METHOD3), called after the hydro step of
+   a grid when ComovingCoordinates (EvolveLevel.C:753-754): the pressure at
+   0.5*(time + old_time), interpolated between `old` (the fields at OldTime,
+   OldBaryonField) and the current fields, or at `time` when old is NULL; then the
+   expansion terms of the gas energy, total energy and velocities in every cell.
+   coefficient = dtFixed * (da/dt) / a at the mid time (CosmologyComputeExpansionFactor,
+   the caller's).  Same memory kind for grid and old. */
+int ppm_b200_expansion_terms(ppm_b200_context *ctx, const ppm_b200_params *params,
+                             ppm_b200_grid *grid, const ppm_b200_grid *old, double time,
+                             double old_time, double coefficient, int memory);
+/* The same for every grid of a level (DEVICE memory; olds may be NULL). */
+int ppm_b200_expansion_terms_level(ppm_b200_context *ctx, const ppm_b200_params *params,
+                                   ppm_b200_grid *grids, const ppm_b200_grid *olds,
+                                   int ngrids, double time, double old_time,
+                                   double coefficient);
+
 /* --- learned starting pressure of twoshock's Newton iteration (twoshock.F:156-170) ---
    A 6 -> 64 -> 64 -> 1 MLP predicts ln(p* / p_acoustic) from the two interface states;
    with params->learned_guess = 1 the Riemann kernel evaluates it on the tensor cores

@@ -104,6 +104,9 @@ def lib():
         L.ora_twoshock_point.argtypes = [C.c_double * 6, C.c_double, C.c_double, C.c_double,
                                          dp, dp, C.POINTER(C.c_int)]
         L.ora_twoshock_point.restype = None
+        L.ora_expansion_terms.argtypes = [C.POINTER(OraParams), dp * 6, C.c_void_p, C.c_double,
+                                          C.c_double, C.c_double]
+        L.ora_expansion_terms.restype = None
         _lib = L
     return _lib
 
@@ -215,3 +218,12 @@ def twoshock_point(states6, gamma, pmin, guess=0.0):
     L.ora_twoshock_point((C.c_double * 6)(*states6), gamma, pmin, guess, C.byref(pb),
                          C.byref(ub), C.byref(it))
     return pb.value, ub.value, it.value
+
+def expansion_terms(grid, hp, fields, old, time, old_time, coefficient):
+    """grid::ComovingExpansionTerms on host fields (in place); old: fields at OldTime
+    or None."""
+    L = lib()
+    P = make_params(grid, hp, 0.0)
+    F = _fields6(fields)
+    O = C.cast(_fields6(old), C.c_void_p) if old is not None else None
+    L.ora_expansion_terms(C.byref(P), F, O, float(time), float(old_time), float(coefficient))

@@ -1061,3 +1061,83 @@ double ora_calc_dt(const ora_params *P, double *const F[ORA_NFIELD], const doubl
       }
   return dt;
 }
+
+/* ------------------------------------------------------------------------ */
+/* comoving expansion terms                                                  */
+/* ------------------------------------------------------------------------ */
+
+/* Grid_ComputePressure.C:51-58 and :168-223 (time strictly between OldTime and Time). */
+static void pressure_interpolated(const ora_params *P, double *const F[ORA_NFIELD],
+                                  double *const O[ORA_NFIELD], double time, double Time,
+                                  double OldTime, double *pressure) {
+  size_t size = 1;
+  for (int dim = 0; dim < P->rank; dim++) size *= (size_t)P->dims[dim];
+  const double Gamma = P->gamma;
+  double coef, coefold;
+  if (Time - OldTime > 0)
+    coef = (time - OldTime) / (Time - OldTime);
+  else
+    coef = 1;
+  coefold = 1 - coef;
+  for (size_t i = 0; i < size; i++) {
+    double velocity2 = 0.0, velocity3 = 0.0, gas_energy;
+    double total_energy = coef * F[ORA_TE][i] + coefold * O[ORA_TE][i];
+    double density = coef * F[ORA_D][i] + coefold * O[ORA_D][i];
+    double velocity1 = coef * F[ORA_V1][i] + coefold * O[ORA_V1][i];
+    if (P->max_velocity_index > 1) velocity2 = coef * F[ORA_V2][i] + coefold * O[ORA_V2][i];
+    if (P->max_velocity_index > 2) velocity3 = coef * F[ORA_V3][i] + coefold * O[ORA_V3][i];
+    if (P->dual == 0) {
+      double kineticE = 0.5 * (velocity1 * velocity1 + velocity2 * velocity2 +
+                               velocity3 * velocity3);
+      gas_energy = total_energy - kineticE;
+    } else {
+      gas_energy = coef * F[ORA_GE][i] + coefold * O[ORA_GE][i];
+    }
+    pressure[i] = (Gamma - 1.0) * density * gas_energy;
+    if (pressure[i] < P->tiny_number) pressure[i] = P->tiny_number;
+    double min_pressure = P->min_support * (Gamma - 1.0) * density * density;
+    if (pressure[i] < min_pressure) pressure[i] = min_pressure;
+  }
+}
+
+void ora_expansion_terms(const ora_params *P, double *const F[ORA_NFIELD],
+                         double *const O[ORA_NFIELD], double Time, double OldTime,
+                         double coefficient) {
+  size_t size = 1;
+  for (int dim = 0; dim < P->rank; dim++) size *= (size_t)P->dims[dim];
+  double *p = (double *)malloc(size * sizeof(double));
+  /* Grid_ComovingExpansionTerms.C:84-89: the pressure at the mid time when the old
+     fields exist, else at Time; ComputePressure's MinimumSupportEnergyCoefficient keeps
+     its default 0 here (Grid.h:576-578) */
+  ora_params Q = *P;
+  Q.min_support = 0.0;
+  if (O != NULL) {
+    double PressureTime = 0.5 * (Time + OldTime);
+    if (PressureTime == Time)
+      ora_compute_pressure(&Q, F, p);
+    else
+      pressure_interpolated(&Q, F, O, PressureTime, Time, OldTime, p);
+  } else {
+    ora_compute_pressure(&Q, F, p);
+  }
+  const double coef = coefficient, gamma = P->gamma;
+  double *d = F[ORA_D], *e = F[ORA_TE], *ge = F[ORA_GE];
+  double *u = F[ORA_V1], *v = F[ORA_V2], *w = F[ORA_V3];
+  /* expand_terms.F: gas energy, ENERGY_METHOD3 */
+  if (P->dual == 1)
+    for (size_t i = 0; i < size; i++) ge[i] = ge[i] * (1.0 - coef) / (1.0 + coef);
+  /* total energy, ENERGY_METHOD3 (imethod != 2, no cosmic rays) */
+  for (size_t i = 0; i < size; i++) {
+    e[i] = e[i] * (1.0 - coef) / (1.0 + coef);
+    double a = e[i] - coef * (3.0 - 2.0 / (gamma - 1.0)) * p[i] / d[i];
+    double b = 0.5 * e[i];
+    e[i] = a > b ? a : b; /* max(a, b) */
+  }
+  /* velocities, VELOCITY_METHOD3 */
+  for (size_t i = 0; i < size; i++) {
+    u[i] = u[i] * (1.0 - 0.5 * coef) / (1.0 + 0.5 * coef);
+    if (P->rank > 1) v[i] = v[i] * (1.0 - 0.5 * coef) / (1.0 + 0.5 * coef);
+    if (P->rank > 2) w[i] = w[i] * (1.0 - 0.5 * coef) / (1.0 + 0.5 * coef);
+  }
+  free(p);
+}

@@ -104,6 +104,15 @@ void ora_twoshock_point(const double st[6], double gamma, double pmin, double gu
 
 void ora_set_riemann_log(ora_riemann_log_fn fn, void *ctx);
 
+/* grid::ComovingExpansionTerms for PPM (Grid_ComovingExpansionTerms.C:36-99 with
+   expand_terms.F, ENERGY_METHOD3 and VELOCITY_METHOD3): pressure at
+   0.5*(time + old_time) interpolated between old and current fields
+   (Grid_ComputePressure.C:51-58, :168-223) when old != NULL, else at time; then the
+   expansion terms over every cell.  coefficient = dtFixed * adot / a. */
+void ora_expansion_terms(const ora_params *P, double *const fields[ORA_NFIELD],
+                         double *const old[ORA_NFIELD], double time, double old_time,
+                         double coefficient);
+
 #ifdef __cplusplus
 }
 #endif
