@@ -143,6 +143,18 @@ def measured_peak_hbm():
     return 6650.0, "fallback 6.65 TB/s"
 
 
+def committed_fp64():
+    """FP64 warp-instructions per active cell and sweep from the committed ncu summary."""
+    f = REPO / "profiles" / "sweep_fp64_turbulence256.json"
+    if f.exists():
+        try:
+            d = json.loads(f.read_text())
+            return float(d["fp64_warp_inst_per_cell_sweep"]), d.get("source", "")
+        except Exception:
+            return None, ""
+    return None, ""
+
+
 def committed_traffic():
     """Per-zone-sweep DRAM bytes of the sweep kernel from the committed ncu summary."""
     f = REPO / "profiles" / "sweep_traffic_turbulence128.json"
@@ -454,6 +466,17 @@ def run_ours(args):
                 "stage_ms_per_sweep": {k: v / max(nsweep, 1) for k, v in stages.items()},
                 "sweep_share_of_step": sweep_ms / ms, "peak_source": peak_src,
                 "traffic_source": tr_src or None}
+    # the bound that is active: FP64 issue (64 FP64 lanes = 2 warp-instructions per SM
+    # and clock), from the committed per-cell instruction count and the sampled clock
+    fp, fp_src = committed_fp64()
+    if fp:
+        sms = torch.cuda.get_device_properties(dev).multi_processor_count
+        mhz = clocks.get("sm_mhz") or clocks.get("sm_max_mhz") or 1965.0
+        fp_peak = sms * 2 * mhz * 1e6
+        fp_achieved = fp * cells / avg_sweep_s
+        roofline["fp64"] = {"bound": "fp64 issue", "achieved": fp_achieved, "peak": fp_peak,
+                            "unit": "warp-instructions/s", "frac": fp_achieved / fp_peak,
+                            "inst_per_cell_sweep": fp, "source": fp_src}
 
     # end to end through the public API with host buffers (pinned), copies inside the timing
     e2e = None
