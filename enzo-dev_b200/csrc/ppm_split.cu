@@ -83,11 +83,15 @@ __device__ __forceinline__ Phys make_phys(const SweepArgs& a) {
 // Splitting the face this way halves the live state of a marching thread.
 // Four resident blocks per SM keep a 256^3 sweep's pencils in a single wave.
 #ifndef PPM_RECON_MINBLOCKS
-#define PPM_RECON_MINBLOCKS 4
+#define PPM_RECON_MINBLOCKS (4 * 128 / PPM_MARCH_THREADS)
 #endif
 
+#ifndef PPM_RECON0_MINBLOCKS
+#define PPM_RECON0_MINBLOCKS PPM_RECON_MINBLOCKS
+#endif
 template <bool DUAL, bool GRAV, int ROLE, bool ONE>
-__global__ void __launch_bounds__(kMarchThreads, PPM_RECON_MINBLOCKS)
+__global__ void __launch_bounds__(kMarchThreads,
+                                  ROLE == 0 ? PPM_RECON0_MINBLOCKS : PPM_RECON_MINBLOCKS)
     reconstruct_kernel(const __grid_constant__ BatchArgs B) {
   constexpr int NV = (ROLE == 0) ? 3 : (DUAL ? 3 : 2);
   int64_t lb;
@@ -671,7 +675,7 @@ __device__ __forceinline__ bool update_pencil(const SweepArgs& a, int64_t pid, c
 }
 
 #ifndef PPM_UPDATE_MINBLOCKS
-#define PPM_UPDATE_MINBLOCKS 3
+#define PPM_UPDATE_MINBLOCKS (3 * 128 / PPM_MARCH_THREADS)
 #endif
 
 // STAGED: the x sweep (pencils along the contiguous axis) with staged outputs.

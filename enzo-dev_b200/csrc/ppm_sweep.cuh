@@ -83,7 +83,16 @@ struct SweepArgs {
 enum { kFaceVars = 12, kFluxVars = 7 };
 
 // Threads per block of the marching stages and of the face-parallel Riemann stage.
-enum { kMarchThreads = 128, kRiemannThreads = 256 };
+// (Riemann blocks of 128 faces leave fewer idle lanes at the end of each face plane of
+// the small grids of a level than 256: -18 % Riemann time on a 600-patch level, and
+// slightly faster on 256^3.)
+#ifndef PPM_RIEMANN_THREADS
+#define PPM_RIEMANN_THREADS 128
+#endif
+#ifndef PPM_MARCH_THREADS
+#define PPM_MARCH_THREADS 128
+#endif
+enum { kMarchThreads = PPM_MARCH_THREADS, kRiemannThreads = PPM_RIEMANN_THREADS };
 
 // One launch over a batch of grids (an AMR level, or a single grid).  Every block
 // belongs to one grid: grid g owns blocks [prefix[g], prefix[g+1]) of a stage; a
