@@ -53,6 +53,9 @@ struct ElemBatch {
   int interpolate;
 };
 void launch_expansion_batch(const ElemBatch& B, int64_t blocks, cudaStream_t st);
+void launch_cfl_reset(unsigned long long* min_bits, cudaStream_t st);
+void launch_cfl_finalize(const unsigned long long* min_bits, double courant, double* dt_out,
+                         cudaStream_t st);
 void launch_sweep_batch(const BatchArgs& B, int64_t march_blocks, int64_t riemann_blocks,
                         bool dual, bool grav, cudaStream_t st, cudaEvent_t* ev, bool learned,
                         bool contiguous);
@@ -110,7 +113,8 @@ enum {
   kSlotTimestep = 14,  // element records of the time-step kernel
   kSlotBoundary = 15,  // element records of the ghost-fill kernel
   kSlotExpansion = 16, // element records of the comoving-expansion kernel
-  kSlotCount = 17
+  kSlotCflCw = 17,     // cell widths read by the time step folded into the last sweep
+  kSlotCount = 18
 };
 // captured level graphs kept at most (a changed grid list leaves the old ones unused)
 constexpr size_t kMaxGraphs = 16;
@@ -132,7 +136,7 @@ struct ppm_b200_context {
   DevBuf pressure;          // pressure of every grid of the batch
   DevBuf face_scratch;      // interface states, fluxes and the flagged-pencil list
   DevBuf counters;          // kMaxCounters unsigned long long
-  DevBuf misc;              // [0] min_bits, [1] dt
+  DevBuf misc;              // [0] min_bits, [1] dt, [2] min_bits of the folded time step
   DevBuf captures;
   DevBuf capture_buf;
   std::vector<double> capture_host;
@@ -142,6 +146,9 @@ struct ppm_b200_context {
   std::vector<cudaEvent_t> ev_pool;  // kSweepEvents per timed sweep
   size_t ev_used = 0;
   double stage_ms[5] = {0, 0, 0, 0, 0};  // per-kernel totals of the last profile read
+  // time step of the next cycle, folded into each solve's last sweep (ppm_b200_set_cfl)
+  double* cfl_dt = nullptr;
+  double cfl_courant = 1.0, cfl_aye = 1.0, cfl_vg[3] = {0.0, 0.0, 0.0};
   // learned Newton start: packed inference weights (ppm_b200_set_guess)
   DevBuf guess;
   bool has_guess = false;
@@ -502,8 +509,33 @@ size_t sweep_scratch_bytes(int dim, const std::vector<GridIO>& io) {
 
 int prepare_sweep(ppm_b200_context* ctx, int dim, int position, const ppm_b200_params* p,
                   const std::vector<GridIO>& io, const std::vector<int>& src,
-                  const std::vector<int>& dst, SweepPlan& plan) {
+                  const std::vector<int>& dst, SweepPlan& plan, bool cfl = false) {
   const int ng = (int)io.size();
+  // the folded time step reads the transverse cell widths: one deduplicated table
+  std::vector<std::array<int64_t, 3>> cwoff(ng, std::array<int64_t, 3>{{-1, -1, -1}});
+  const double* cw_dev = nullptr;
+  if (cfl) {
+    std::vector<double> cws;
+    std::map<std::vector<double>, int64_t> seen;
+    for (int k = 0; k < ng; ++k)
+      for (int d = 0; d < io[k].g->rank; ++d) {
+        const ppm_b200_grid* g = io[k].g;
+        std::vector<double> key(g->cell_width[d], g->cell_width[d] + g->dims[d]);
+        auto it = seen.find(key);
+        if (it != seen.end()) {
+          cwoff[k][d] = it->second;
+        } else {
+          cwoff[k][d] = (int64_t)cws.size();
+          seen[key] = cwoff[k][d];
+          cws.insert(cws.end(), key.begin(), key.end());
+        }
+      }
+    std::vector<unsigned char> cimg;
+    append(cimg, cws.data(), cws.size());
+    int rc0 = mirror_put(ctx, ctx->mirror[kSlotCflCw], cimg);
+    if (rc0) return rc0;
+    cw_dev = (const double*)ctx->mirror[kSlotCflCw].dev.p;
+  }
   // coefficient tables (deduplicated), uploaded into this direction's table slot
   CoefTables ct;
   build_coef_tables(dim, io, ct);
@@ -591,6 +623,21 @@ int prepare_sweep(ppm_b200_context* ctx, int dim, int position, const ppm_b200_p
     a.fstate = scratch + at;
     a.fflux = a.fstate + (size_t)ppm::kFaceVars * (size_t)a.plane;
     at += (size_t)(ppm::kFaceVars + ppm::kFluxVars) * (size_t)a.plane;
+    a.dim = dim;
+    a.rank = g->rank;
+    if (cfl) {
+      const int ax1 = dim == 0 ? 1 : 0, ax2 = dim == 2 ? 1 : 2;
+      a.cfl_min_bits = ((unsigned long long*)ctx->misc.p) + 2;
+      a.cw1 = cwoff[k][ax1] >= 0 ? cw_dev + cwoff[k][ax1] : nullptr;
+      a.cw2 = cwoff[k][ax2] >= 0 ? cw_dev + cwoff[k][ax2] : nullptr;
+      a.ts1 = g->start[ax1];
+      a.te1 = g->end[ax1];
+      a.ts2 = g->start[ax2];
+      a.te2 = g->end[ax2];
+      a.aye = ctx->cfl_aye;
+      for (int d = 0; d < 3; ++d) a.vg[d] = ctx->cfl_vg[d];
+      a.min_support = p->min_support;
+    }
   }
 
   // subgrid flux capture (single grid): requests built by build_captures, buffers
@@ -937,7 +984,8 @@ int prepare_solve(ppm_b200_context* ctx, const ppm_b200_params* p, int cycle,
     const int in_set = (s == 0) ? -1 : (s - 1) % 2;
     const int out_set = (s == sp.nsweeps - 1 && sp.nsweeps >= 2) ? -1 : s % 2;
     std::vector<int> src(ng, in_set), dst(ng, out_set);
-    rc = prepare_sweep(ctx, sp.order[s], s, p, io, src, dst, sp.sweep[s]);
+    const bool cfl = ctx->cfl_dt != nullptr && s == sp.nsweeps - 1;
+    rc = prepare_sweep(ctx, sp.order[s], s, p, io, src, dst, sp.sweep[s], cfl);
     if (rc) return rc;
   }
   if (ctx->face_scratch.p != scratch_base) {  // would leave earlier sweeps on freed memory
@@ -952,9 +1000,17 @@ int enqueue_solve(ppm_b200_context* ctx, const ppm_b200_params* p, const std::ve
   ppm::launch_pressure_batch(sp.pressure.B, sp.pressure.size_blocks, ctx->stream);
   ctx->launches += 1;
   CK(cudaGetLastError());
+  unsigned long long* cfl_bits = ((unsigned long long*)ctx->misc.p) + 2;
   for (int s = 0; s < sp.nsweeps; ++s) {
+    const bool cfl = ctx->cfl_dt != nullptr && s == sp.nsweeps - 1;
+    if (cfl) ppm::launch_cfl_reset(cfl_bits, ctx->stream);
     int rc = enqueue_sweep(ctx, sp.sweep[s], p, capturing);
     if (rc) return rc;
+    if (cfl) {
+      ppm::launch_cfl_finalize(cfl_bits, ctx->cfl_courant, ctx->cfl_dt, ctx->stream);
+      ctx->launches += 1;
+      CK(cudaGetLastError());
+    }
   }
   if (sp.nsweeps == 1) {
     for (const auto& x : io) {
@@ -979,6 +1035,8 @@ void key_put(std::string& k, const T& v) {
 
 std::string graph_key(ppm_b200_context* ctx, const ppm_b200_params* p, const SolvePlan& sp) {
   std::string k;
+  key_put(k, ctx->cfl_dt);
+  key_put(k, ctx->cfl_courant);
   key_put(k, p->learned_guess);
   key_put(k, p->dual_energy);
   key_put(k, p->gravity);
@@ -1521,6 +1579,16 @@ int ppm_b200_expansion_terms_level(ppm_b200_context* ctx, const ppm_b200_params*
     }
   }
   return expansion_batch(ctx, p, io, olds ? &ofs : nullptr, time, old_time, coefficient);
+}
+
+int ppm_b200_set_cfl(ppm_b200_context* ctx, double* dt_device, double courant, double aye,
+                     const double vgrid[3]) {
+  if (!ctx) return PPM_B200_ERR_INVALID;
+  ctx->cfl_dt = dt_device;
+  ctx->cfl_courant = courant;
+  ctx->cfl_aye = aye;
+  for (int d = 0; d < 3; ++d) ctx->cfl_vg[d] = vgrid ? vgrid[d] : 0.0;
+  return PPM_B200_OK;
 }
 
 int ppm_b200_set_guess(ppm_b200_context* ctx, const float* weights) {

@@ -233,6 +233,16 @@ void launch_timestep_batch(const ElemBatch& B, int64_t blocks, double courant, d
   timestep_finalize_kernel<<<1, 32, 0, st>>>(B.min_bits, courant, dt_out);
 }
 
+// The time step folded into a solve's last sweep: reset before it, finalise after it.
+void launch_cfl_reset(unsigned long long* min_bits, cudaStream_t st) {
+  cudaMemsetAsync(min_bits, 0xFF, sizeof(unsigned long long), st);
+}
+
+void launch_cfl_finalize(const unsigned long long* min_bits, double courant, double* dt_out,
+                         cudaStream_t st) {
+  timestep_finalize_kernel<<<1, 32, 0, st>>>(min_bits, courant, dt_out);
+}
+
 void launch_expansion_batch(const ElemBatch& B, int64_t blocks, cudaStream_t st) {
   expansion_kernel<<<(unsigned)blocks, 256, 0, st>>>(B);
 }

@@ -452,7 +452,47 @@ __device__ __noinline__ void hll_fallback(const SweepArgs& a, int64_t pid, int64
 // rewrites every output (and subgrid-flux capture) of the pencil.
 struct UpdateCounts {
   unsigned int fallbacks, fatal, nonfinite;
+  double dtmin;  // smallest calc_dt dt1 of the pencil's active cells (cfl_min_bits set)
 };
+
+// calc_dt.F:136-153 for one updated cell (the cell of pencil position c), with the
+// pressure of grid::ComputePressure at the new time (Grid_ComputePressure.C:96-164):
+// the time step of the next cycle, computed where the final state is first known.
+// Roles -> axes: the sweep velocity u is v[dim], v is v[dim+1], w is v[dim+2].
+template <bool DUAL>
+__device__ __forceinline__ double cell_dt1(const SweepArgs& a, const Cell& o, double dx_sweep,
+                                           int64_t t1, int64_t t2, const Phys& P) {
+  double vel[3], dx[3];
+  vel[a.dim] = o.u;
+  vel[(a.dim + 1) % 3] = o.v;
+  vel[(a.dim + 2) % 3] = o.w;
+  const int ax1 = a.dim == 0 ? 1 : 0, ax2 = a.dim == 2 ? 1 : 2;
+  dx[a.dim] = dx_sweep;
+  dx[ax1] = a.cw1 ? a.cw1[t1] : 1.0;
+  dx[ax2] = a.cw2 ? a.cw2[t2] : 1.0;
+  const double velocity1 = vel[0];
+  const double velocity2 = a.rank > 1 ? vel[1] : 0.0;
+  const double velocity3 = a.rank > 2 ? vel[2] : 0.0;
+  double gas_energy;
+  if (DUAL) {
+    gas_energy = o.ge;
+  } else {
+    gas_energy = o.e - 0.5 * (velocity1 * velocity1 + velocity2 * velocity2 +
+                              velocity3 * velocity3);
+  }
+  double p = P.gm1 * o.d * gas_energy;
+  if (p < P.pmin) p = P.pmin;
+  const double min_pressure = a.min_support * P.gm1 * o.d * o.d;
+  if (p < min_pressure) p = min_pressure;
+  const double cs = dmax(sqrt(P.gamma * p / o.d), kTiny);
+  if (a.rank == 1) return dx[0] * a.aye / (cs + fabs(velocity1 - a.vg[0]));
+  if (a.rank == 2)
+    return a.aye / ((cs + fabs(velocity1 - a.vg[0])) / dx[0] +
+                    (cs + fabs(velocity2 - a.vg[1])) / dx[1]);
+  return a.aye / ((cs + fabs(velocity1 - a.vg[0])) / dx[0] +
+                  (cs + fabs(velocity2 - a.vg[1])) / dx[1] +
+                  (cs + fabs(velocity3 - a.vg[2])) / dx[2]);
+}
 
 // Output staging of the x sweep.  Its pencils run along the contiguous axis, so a warp
 // storing one cell per pencil writes 32 separate sectors; instead every thread stores
@@ -500,6 +540,10 @@ __device__ __forceinline__ bool update_pencil(const SweepArgs& a, int64_t pid, c
                                               double* stage = nullptr, int64_t pid0 = 0) {
   bool live = valid, flagged = false;
   const int64_t base = live ? (pid % a.n1) * a.s1 + (pid / a.n1) * a.s2 : 0;
+  const int64_t t1 = pid % a.n1, t2 = pid / a.n1;
+  // the pencil's cells are active across the sweep (calc_dt covers active cells only)
+  const bool cfl = a.cfl_min_bits && t1 >= a.ts1 && t1 <= a.te1 && t2 >= a.ts2 && t2 <= a.te2;
+  double dtmin = 1.0e20;
   const int64_t sa = a.sa, np = a.npencils;
   const int n = a.n, is = a.is, ie = a.ie;
 
@@ -606,6 +650,8 @@ __device__ __forceinline__ bool update_pencil(const SweepArgs& a, int64_t pid, c
           dep = o.d * o.e;
         }
         if (!isfinite(o.d) || !isfinite(o.e)) nonfin += 1;
+        if (cfl && c >= is && c <= ie)
+          dtmin = dmin(dtmin, cell_dt1<DUAL>(a, o, a.coef[c].dx, t1, t2, P));
         if (STAGED) {
           double* sp = stage + (c % kStageCells) * kStageLd + (threadIdx.x & 31);
           sp[0] = o.d;
@@ -671,6 +717,7 @@ __device__ __forceinline__ bool update_pencil(const SweepArgs& a, int64_t pid, c
     }
   }
   cnt.nonfinite += nonfin;
+  cnt.dtmin = dtmin;
   return flagged;
 }
 
@@ -691,10 +738,11 @@ __global__ void __launch_bounds__(kMarchThreads, PPM_UPDATE_MINBLOCKS)
   if (ONE) __syncthreads();
   const int64_t pid = lb * kMarchThreads + threadIdx.x;
   const int64_t wpid0 = pid - (threadIdx.x & 31);  // first pencil of this warp
+  double my_dt = 1.0e20;
   const bool valid = pid < a.npencils;
   if (STAGED || valid) {
     const Phys P = make_phys(a);
-    UpdateCounts cnt = {0, 0, 0};
+    UpdateCounts cnt = {0, 0, 0, 1.0e20};
     if (update_pencil<DUAL, GRAV, false, STAGED>(
             a, pid, P, cnt, valid, s_stage + (threadIdx.x >> 5) * kStageWarp, wpid0)) {
       const unsigned long long slot = atomicAdd(&B.counters[kCntFlagged], 1ull);
@@ -702,7 +750,14 @@ __global__ void __launch_bounds__(kMarchThreads, PPM_UPDATE_MINBLOCKS)
     } else {
       if (cnt.fatal) atomicAdd(&s_cnt[0], (unsigned long long)cnt.fatal);
       if (cnt.nonfinite) atomicAdd(&s_cnt[1], (unsigned long long)cnt.nonfinite);
+      my_dt = cnt.dtmin;  // a flagged pencil's time step comes from the fallback pass
     }
+  }
+  if (a.cfl_min_bits) {  // warp minimum, one atomic per warp (every lane reaches this)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) my_dt = dmin(my_dt, __shfl_xor_sync(0xffffffffu, my_dt, o));
+    if ((threadIdx.x & 31) == 0 && my_dt < 1.0e20)
+      atomicMin(a.cfl_min_bits, (unsigned long long)__double_as_longlong(my_dt));
   }
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -720,8 +775,10 @@ __global__ void __launch_bounds__(128) fallback_kernel(const __grid_constant__ B
     const int64_t code = B.flagged[k];
     const SweepArgs& a = ONE ? B.one : B.grids[(int)(code >> 40)];
     const Phys P = make_phys(a);
-    UpdateCounts cnt = {0, 0, 0};
+    UpdateCounts cnt = {0, 0, 0, 1.0e20};
     update_pencil<DUAL, GRAV, true>(a, code & ((int64_t(1) << 40) - 1), P, cnt);
+    if (a.cfl_min_bits && cnt.dtmin < 1.0e20)
+      atomicMin(a.cfl_min_bits, (unsigned long long)__double_as_longlong(cnt.dtmin));
     if (cnt.fallbacks) atomicAdd(&B.counters[kCntFallbacks], (unsigned long long)cnt.fallbacks);
     if (cnt.fatal) atomicAdd(&B.counters[kCntFatal], (unsigned long long)cnt.fatal);
     if (cnt.nonfinite) atomicAdd(&B.counters[kCntNonFinite], (unsigned long long)cnt.nonfinite);

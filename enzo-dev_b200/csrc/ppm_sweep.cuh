@@ -78,6 +78,15 @@ struct SweepArgs {
   unsigned long long* log_count;     // records claimed (may exceed log_cap)
   int64_t log_cap;
   int log_stride;                    // about one face in log_stride is logged; 0 = off
+  // Courant time step of the updated fields (calc_dt.F), computed in the update kernel of
+  // a solve's last sweep when cfl_min_bits is set: the minimum over the batch of dt1
+  // goes to *cfl_min_bits (positive doubles order as integers)
+  unsigned long long* cfl_min_bits;
+  const double* cw1;                 // cell widths along the t1 and t2 axes (device)
+  const double* cw2;
+  int dim, rank;                     // the sweep axis and GridRank
+  int ts1, te1, ts2, te2;            // active ranges along the t1 and t2 axes
+  double aye, vg[3], min_support;    // calc_dt's a, grid velocity, ComputePressure's floor
 };
 
 enum { kFaceVars = 12, kFluxVars = 7 };

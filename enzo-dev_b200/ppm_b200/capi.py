@@ -38,7 +38,7 @@ EXPORTS = (
     "ppm_b200_profile_stages", "ppm_b200_set_guess", "ppm_b200_riemann_log",
     "ppm_b200_riemann_log_count", "ppm_b200_guess_features", "ppm_b200_guess_grad",
     "ppm_b200_guess_adam", "ppm_b200_guess_eval", "ppm_b200_expansion_terms",
-    "ppm_b200_expansion_terms_level",
+    "ppm_b200_expansion_terms_level", "ppm_b200_set_cfl",
 )
 
 GUESS_WEIGHTS = 4673  # W1[6][64] b1[64] W2[64][64] b2[64] w3[64] b3
@@ -151,6 +151,7 @@ def lib(build_if_missing: bool = True):
     L.ppm_b200_set_graphs.argtypes = [vp, C.c_int]
     fp = C.POINTER(C.c_float)
     L.ppm_b200_set_guess.argtypes = [vp, vp]
+    L.ppm_b200_set_cfl.argtypes = [vp, vp, C.c_double, C.c_double, C.POINTER(C.c_double)]
     L.ppm_b200_expansion_terms.argtypes = [vp, C.POINTER(Params), C.POINTER(GridDesc),
                                            C.POINTER(GridDesc), C.c_double, C.c_double,
                                            C.c_double, C.c_int]
@@ -420,6 +421,15 @@ class Context:
         if rc != OK:
             raise PPMError(rc, "ppm_b200_profile_read")
         return ms.value, n.value
+
+    def set_cfl(self, dt_device, courant=1.0, aye=1.0, vgrid=(0.0, 0.0, 0.0)):
+        """Fold the next cycle's time step into later solves (dt_device: float64 device
+        tensor of one element, or None to stop)."""
+        vg = (C.c_double * 3)(*vgrid)
+        rc = self.L.ppm_b200_set_cfl(self.h, dt_device.data_ptr() if dt_device is not None
+                                     else None, float(courant), float(aye), vg)
+        if rc != OK:
+            raise PPMError(rc, "ppm_b200_set_cfl")
 
     # ---- comoving expansion terms
     def expansion_terms(self, grid, hp, fields, old, time, old_time, coefficient,

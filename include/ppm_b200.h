@@ -158,6 +158,16 @@ int ppm_b200_compute_timestep(ppm_b200_context *ctx, const ppm_b200_params *para
 int ppm_b200_set_boundary(ppm_b200_context *ctx, ppm_b200_grid *grid, int dual_energy,
                           const int bc_type[3]);
 
+/* The time step of the next cycle, folded into every later solve on this context:
+   the last sweep's update kernel evaluates calc_dt (ihydro = 0, calc_dt.F:136-153 with
+   the pressure of grid::ComputePressure, Grid_ComputePressure.C:96-164) on each active
+   cell as soon as its final state is known, and the solve writes courant * min dt1 over
+   its grid(s) to *dt_device (device memory) -- the value ppm_b200_compute_timestep (or
+   _level) would return after the solve, without its pass over the fields.
+   dt_device = NULL turns it off.  aye and vgrid as in ppm_b200_compute_timestep. */
+int ppm_b200_set_cfl(ppm_b200_context *ctx, double *dt_device, double courant, double aye,
+                     const double vgrid[3]);
+
 /* --- AMR level entry points: every grid of a level in one batch (DEVICE memory) ---
    The reference advances a level one grid at a time: the grid loop of
    EvolveLevel.C:569-585 calls grid::SolveHydroEquations -> SolvePPM_DE per grid,
