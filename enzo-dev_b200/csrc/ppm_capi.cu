@@ -1366,6 +1366,10 @@ int ppm_b200_euler_sweep(ppm_b200_context* ctx, int dim, const ppm_b200_params* 
 int ppm_b200_compute_pressure(ppm_b200_context* ctx, const ppm_b200_params* p, ppm_b200_grid* g,
                               double* pressure, int memory) {
   if (!ctx || !p || !g || !pressure) return PPM_B200_ERR_INVALID;
+  // this call does not read the acceleration: a gravity run's grids need none here
+  ppm_b200_params q = *p;
+  q.gravity = 0;
+  p = &q;
   int rc = check_grid(g, p);
   if (rc) return rc;
   CK(cudaSetDevice(ctx->device));
@@ -1422,6 +1426,10 @@ int ppm_b200_compute_timestep(ppm_b200_context* ctx, const ppm_b200_params* p, p
                               int memory, double courant, double aye, const double vgrid_in[3],
                               double* dt_device, double* dt_host) {
   if (!ctx || !p || !g) return PPM_B200_ERR_INVALID;
+  // this call does not read the acceleration: a gravity run's grids need none here
+  ppm_b200_params q = *p;
+  q.gravity = 0;
+  p = &q;
   int rc = check_grid(g, p);
   if (rc) return rc;
   CK(cudaSetDevice(ctx->device));
@@ -1436,6 +1444,10 @@ int ppm_b200_compute_timestep_level(ppm_b200_context* ctx, const ppm_b200_params
                                     ppm_b200_grid* grids, int ngrids, double courant, double aye,
                                     const double vgrid[3], double* dt_device, double* dt_host) {
   if (!ctx || !p || !grids || ngrids <= 0) return PPM_B200_ERR_INVALID;
+  // this call does not read the acceleration: a gravity run's grids need none here
+  ppm_b200_params q = *p;
+  q.gravity = 0;
+  p = &q;
   CK(cudaSetDevice(ctx->device));
   std::vector<GridIO> io(ngrids);
   for (int k = 0; k < ngrids; ++k) {
@@ -1537,6 +1549,10 @@ int ppm_b200_expansion_terms(ppm_b200_context* ctx, const ppm_b200_params* p, pp
                              const ppm_b200_grid* old, double time, double old_time,
                              double coefficient, int memory) {
   if (!ctx || !p || !g) return PPM_B200_ERR_INVALID;
+  // this call does not read the acceleration: a gravity run's grids need none here
+  ppm_b200_params q = *p;
+  q.gravity = 0;
+  p = &q;
   int rc = check_grid(g, p);
   if (rc) return rc;
   CK(cudaSetDevice(ctx->device));
@@ -1564,6 +1580,10 @@ int ppm_b200_expansion_terms_level(ppm_b200_context* ctx, const ppm_b200_params*
                                    int ngrids, double time, double old_time,
                                    double coefficient) {
   if (!ctx || !p || !grids || ngrids <= 0) return PPM_B200_ERR_INVALID;
+  // this call does not read the acceleration: a gravity run's grids need none here
+  ppm_b200_params q = *p;
+  q.gravity = 0;
+  p = &q;
   CK(cudaSetDevice(ctx->device));
   std::vector<GridIO> io(ngrids);
   std::vector<FieldSet> ofs(ngrids);
