@@ -373,18 +373,43 @@ __global__ void __launch_bounds__(kRiemannThreads) riemann_kernel(const __grid_c
     atomicAdd(&B.counters[kCntGuessRejected], (unsigned long long)s_rejected);
 }
 
+// The flux planes are read once, with whole lines per warp: streaming loads (evicted
+// first) keep them from displacing the cells the marching kernels reuse.
 __device__ __forceinline__ Flux load_flux(const SweepArgs& a, int64_t idx) {
   const double* s = a.fflux + idx;
   const int64_t pl = a.plane;
   Flux f;
-  f.df = s[XDF * pl];
-  f.ef = s[XEF * pl];
-  f.uf = s[XUF * pl];
-  f.vf = s[XVF * pl];
-  f.wf = s[XWF * pl];
-  f.gef = s[XGEF * pl];
-  f.ub = s[XUB * pl];
+  f.df = __ldcs(s + XDF * pl);
+  f.ef = __ldcs(s + XEF * pl);
+  f.uf = __ldcs(s + XUF * pl);
+  f.vf = __ldcs(s + XVF * pl);
+  f.wf = __ldcs(s + XWF * pl);
+  f.gef = __ldcs(s + XGEF * pl);
+  f.ub = __ldcs(s + XUB * pl);
   return f;
+}
+
+// The x sweep's cells: each lane reads its pencil's line over 16 consecutive steps, so
+// these lines are marked to be evicted last from L1.
+__device__ __forceinline__ double ldg_keep(const double* p) {
+  double v;
+  asm volatile("ld.global.nc.L1::evict_last.f64 %0, [%1];" : "=d"(v) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ double ldg_keep0(const double* p, int64_t off) {
+  return p ? ldg_keep(p + off) : 0.0;
+}
+
+template <bool DUAL>
+__device__ __forceinline__ Cell load_cell_keep(const SweepArgs& a, int64_t off) {
+  Cell c;
+  c.d = ldg_keep(a.in_d + off);
+  c.e = ldg_keep(a.in_e + off);
+  c.u = ldg_keep0(a.in_u, off);
+  c.v = ldg_keep0(a.in_v, off);
+  c.w = ldg_keep0(a.in_w, off);
+  c.ge = DUAL ? ldg_keep(a.in_ge + off) : 0.0;
+  return c;
 }
 
 template <bool DUAL>
@@ -572,7 +597,7 @@ __device__ __forceinline__ bool update_pencil(const SweepArgs& a, int64_t pid, c
   Cell Cpf = Cm;
   Flux Fpf = F0;
   if (live) {
-    Cpf = load_cell<DUAL>(a, base);
+    Cpf = STAGED ? load_cell_keep<DUAL>(a, base) : load_cell<DUAL>(a, base);
     if (0 >= is && 0 <= ie) Fpf = load_flux(a, (int64_t)(1 - is) * np + pid);
   }
 
@@ -588,7 +613,8 @@ __device__ __forceinline__ bool update_pencil(const SweepArgs& a, int64_t pid, c
       Cn = Cpf;
       if (t >= is && t <= ie) F1 = Fpf;
       if (t + 1 < n) {
-        Cpf = load_cell<DUAL>(a, base + (int64_t)(t + 1) * sa);
+        Cpf = STAGED ? load_cell_keep<DUAL>(a, base + (int64_t)(t + 1) * sa)
+                     : load_cell<DUAL>(a, base + (int64_t)(t + 1) * sa);
         if (t + 1 >= is && t + 1 <= ie) Fpf = load_flux(a, (int64_t)(t + 2 - is) * np + pid);
       }
       if (t >= is && t <= ie) {
