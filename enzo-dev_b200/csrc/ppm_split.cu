@@ -525,6 +525,9 @@ __device__ __forceinline__ double cell_dt1(const SweepArgs& a, const Cell& o, do
 // 32 pencils' cells with consecutive lanes on consecutive cells of a pencil (warp-local:
 // no block barrier).  Layout per warp [field][cell][lane], the cell row padded
 // (kStageLd) so that the flush reads hit distinct banks.
+#ifndef PPM_X_STAGE_STORES
+#define PPM_X_STAGE_STORES 1
+#endif
 enum { kStageCells = 4, kStageLd = 32 + 8 };
 constexpr int kStageField = kStageCells * kStageLd;
 constexpr int kStageWarp = 6 * kStageField;  // doubles per warp
@@ -678,7 +681,7 @@ __device__ __forceinline__ bool update_pencil(const SweepArgs& a, int64_t pid, c
         if (!isfinite(o.d) || !isfinite(o.e)) nonfin += 1;
         if (cfl && c >= is && c <= ie)
           dtmin = dmin(dtmin, cell_dt1<DUAL>(a, o, a.coef[c].dx, t1, t2, P));
-        if (STAGED) {
+        if (STAGED && PPM_X_STAGE_STORES) {
           double* sp = stage + (c % kStageCells) * kStageLd + (threadIdx.x & 31);
           sp[0] = o.d;
           sp[kStageField] = o.e;
@@ -697,7 +700,7 @@ __device__ __forceinline__ bool update_pencil(const SweepArgs& a, int64_t pid, c
         }
       }
       // warp-wide: the same steps on every lane
-      if (STAGED && c >= 0 && c % kStageCells == kStageCells - 1)
+      if (STAGED && PPM_X_STAGE_STORES && c >= 0 && c % kStageCells == kStageCells - 1)
         flush_stage<DUAL>(a, stage, pid0, c - (kStageCells - 1), kStageCells);
     }
     Fm = F0;
@@ -719,7 +722,7 @@ __device__ __forceinline__ bool update_pencil(const SweepArgs& a, int64_t pid, c
         pgas2d_dual(o, (c == 0) ? own : dep, own, P);
       }
       if (!isfinite(o.d) || !isfinite(o.e)) nonfin += 1;
-      if (STAGED) {
+      if (STAGED && PPM_X_STAGE_STORES) {
         double* sp = stage + (c % kStageCells) * kStageLd + (threadIdx.x & 31);
         sp[0] = o.d;
         sp[kStageField] = o.e;
@@ -737,7 +740,7 @@ __device__ __forceinline__ bool update_pencil(const SweepArgs& a, int64_t pid, c
         if (DUAL) a.out_ge[off] = o.ge;
       }
     }
-    if (STAGED) {  // the partial last chunk, cells c0 .. n-1
+    if (STAGED && PPM_X_STAGE_STORES) {  // the partial last chunk, cells c0 .. n-1
       const int c0 = c - c % kStageCells;
       flush_stage<DUAL>(a, stage, pid0, c0, c - c0 + 1);
     }
