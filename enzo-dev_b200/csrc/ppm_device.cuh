@@ -5,7 +5,7 @@
 // MAX/MIN as a compare-select).  The library is compiled with -fmad=false, so every
 // product and sum is rounded separately, and CUDA's FP64 '/' and sqrt are IEEE
 // correctly rounded: the results are bit-identical to a plain x86-64 build of the
-// same expressions.  The sweep kernels (ppm_sweep.cu) only schedule these points.
+// same expressions.  The sweep kernels (ppm_split.cu) only schedule these points.
 #pragma once
 
 #include <cstdint>
@@ -139,31 +139,37 @@ __device__ __forceinline__ CoreState face_core(const CoreL& L, const CoreR& R, d
   CoreState s;
   double cla = sqrt(dmax(P.gamma * L.pla * L.dla, 0.0));
   double cra = sqrt(dmax(P.gamma * R.pra * R.dra, 0.0));
+  // 0.5/c is computed as 0.5*(1/c): equal, since c is 0, inf, NaN or a square root of
+  // a double (|c| <= 2^512), so 1/c never reaches the subnormal range
   double f1 = 1.0 / cla;
+  const double hla = 0.5 * f1;
+  const double ydla = 1.0 / L.dla;
   double betalp = (L.ula - L.ulp) + (L.pla - L.plp) * f1;
   double betalm = (L.ula - L.ulm) - (L.pla - L.plm) * f1;
-  double betal0 = (L.pla - L.pl0) * (f1 * f1) + 1.0 / L.dla - 1.0 / L.dl0;
+  double betal0 = (L.pla - L.pl0) * (f1 * f1) + ydla - 1.0 / L.dl0;
   double gterm = 0.0;
   if (GRAV) {
     gterm = 0.25 * P.dt * gsum;
     betalp = betalp - gterm;
     betalm = betalm - gterm;
   }
-  f1 = 0.5 / cla;
+  f1 = hla;
   betalp = -(betalp * f1);
   betalm = +betalm * f1;
   if (L.cp <= 0.0) betalp = 0.0;
   if (L.cm <= 0.0) betalm = 0.0;
   if (L.c0 <= 0.0) betal0 = 0.0;
   f1 = 1.0 / cra;
+  const double hra = 0.5 * f1;
+  const double ydra = 1.0 / R.dra;
   double betarp = (R.ura - R.urp) + (R.pra - R.prp) * f1;
   double betarm = (R.ura - R.urm) - (R.pra - R.prm) * f1;
-  double betar0 = (R.pra - R.pr0) * (f1 * f1) + 1.0 / R.dra - 1.0 / R.dr0;
+  double betar0 = (R.pra - R.pr0) * (f1 * f1) + ydra - 1.0 / R.dr0;
   if (GRAV) {
     betarp = betarp - gterm;
     betarm = betarm - gterm;
   }
-  f1 = 0.5 / cra;
+  f1 = hra;
   betarp = -(betarp * f1);
   betarm = +betarm * f1;
   if (R.cp >= 0.0) betarp = 0.0;
@@ -173,15 +179,17 @@ __device__ __forceinline__ CoreState face_core(const CoreL& L, const CoreR& R, d
   s.pr = R.pra + (betarp + betarm) * (cra * cra);
   s.ul = L.ula + (betalp - betalm) * cla;
   s.ur = R.ura + (betarp - betarm) * cra;
-  s.dl = 1.0 / (1.0 / L.dla - (betal0 + betalp + betalm));
-  s.dr = 1.0 / (1.0 / R.dra - (betar0 + betarp + betarm));
+  s.dl = 1.0 / (ydla - (betal0 + betalp + betalm));
+  s.dr = 1.0 / (ydra - (betar0 + betarp + betarm));
   if (DUAL) {
     double ml = dmax(dmax(fabs(L.cm), fabs(L.c0)), fabs(L.cp));
-    if (P.gamma * L.pla / L.dla < P.eta2 * (L.ula * L.ula) || ml < 1.0e-3 || s.dl / L.dla > 5.0) {
+    if (P.gamma * L.pla / L.dla < P.eta2 * (L.ula * L.ula) || ml < 1.0e-3 ||
+        s.dl / L.dla > 5.0) {
       s.pl = L.pla; s.ul = L.ula; s.dl = L.dla;
     }
     double mr = dmax(dmax(fabs(R.cm), fabs(R.c0)), fabs(R.cp));
-    if (P.gamma * R.pra / R.dra < P.eta2 * (R.ura * R.ura) || mr < 1.0e-3 || s.dr / R.dra > 5.0) {
+    if (P.gamma * R.pra / R.dra < P.eta2 * (R.ura * R.ura) || mr < 1.0e-3 ||
+        s.dr / R.dra > 5.0) {
       s.pr = R.pra; s.ur = R.ura; s.dr = R.dra;
     }
   }

@@ -281,8 +281,15 @@ __device__ __forceinline__ FaceState load_face(const SweepArgs& a, int64_t idx) 
 // back to the acoustic start, i.e. the plain solver, when it does not converge.
 // Without LEARNED, a sample of the faces can be logged (states + converged p*) as
 // training data for that net.
+// 8 resident blocks of 128 faces per SM (64 registers, a few spilled): the Newton
+// iteration's dependent FP64 chains want warps more than registers (256^3 sweep:
+// 1.65 -> 1.53 ms against the unconstrained 80 registers; 7 blocks: 1.59 ms).  The
+// learned start holds the net's fragments as well and keeps 3 blocks (168 registers).
+#ifndef PPM_RIEMANN_MINBLOCKS
+#define PPM_RIEMANN_MINBLOCKS (8 * 128 / PPM_RIEMANN_THREADS)
+#endif
 template <bool DUAL, bool ONE, bool LEARNED>
-__global__ void __launch_bounds__(kRiemannThreads) riemann_kernel(const __grid_constant__ BatchArgs B) {
+__global__ void __launch_bounds__(kRiemannThreads, LEARNED ? 3 : PPM_RIEMANN_MINBLOCKS) riemann_kernel(const __grid_constant__ BatchArgs B) {
   __shared__ unsigned int s_hist[8];
   __shared__ unsigned int s_newton;
   __shared__ unsigned int s_rejected;
