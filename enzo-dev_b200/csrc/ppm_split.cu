@@ -17,6 +17,8 @@
 // warp's scratch accesses are contiguous.
 #include <cuda_runtime.h>
 
+#include <atomic>
+
 #include "ppm_device.cuh"
 #include "ppm_guess.cuh"
 #include "ppm_sweep.cuh"
@@ -431,6 +433,97 @@ __device__ __forceinline__ Cell load_cell(const SweepArgs& a, int64_t off) {
   return c;
 }
 
+// Input pipeline of the y and z sweeps' update kernel.  A step of a pencil consumes one
+// unit: cell s (6 fields) and, for is <= s <= ie, face s+1-is (7 flux planes).  Each
+// thread copies its own units PD steps ahead with cp.async (8 bytes a lane, so a warp's
+// 32 consecutive pencils fill whole sectors) into a private ring of PD+1 units in
+// shared memory, laid out [slot][value][thread]; the bytes in flight do not occupy
+// registers.  The ring has one slot more than the distance, so a slot is refilled one
+// step after it was read.  No barrier is involved: every thread reads only what it
+// copied itself, after its own cp.async.wait_group.
+// Measured (y/z update at 256^3, 0.76 ms with the one-step register prefetch at 3
+// blocks/SM): distance 1 at 4 blocks/SM (128 registers) 0.55 ms; distance 2 at 4
+// blocks 0.60; distance 1 or 2 at 3 blocks 0.74 / 0.70; 5 blocks spill.  On the
+// 600-patch level (many short pencils, records in shared memory) distance 2 at 3
+// blocks is the fastest.  The x sweep's update measured slower through the ring (1.64
+// -> 2.12 ms): its lanes read 32 different lines, which the evict-last loads keep in
+// L1 better.
+#ifndef PPM_UPDATE_PIPE_ONE
+#define PPM_UPDATE_PIPE_ONE 1
+#endif
+#ifndef PPM_UPDATE_PIPE_BATCH
+#define PPM_UPDATE_PIPE_BATCH 2
+#endif
+constexpr int kUnitVals = 6 + kFluxVars;
+template <int PD>
+__host__ __device__ constexpr int ring_doubles() {
+  return PD > 0 ? (PD + 1) * kUnitVals * kMarchThreads : 0;
+}
+
+__device__ __forceinline__ void cp_async8(double* dst, const double* src) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(s), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// ring: this thread's column of the block's ring (ring[v * kMarchThreads] is value v)
+template <bool DUAL, int PD>
+__device__ __forceinline__ void pipe_issue(const SweepArgs& a, double* ring, int64_t base,
+                                           int64_t pid, int s) {
+  if (s < a.n) {
+    double* r = ring + (s % (PD + 1)) * (kUnitVals * kMarchThreads);
+    const int64_t off = base + (int64_t)s * a.sa;
+    cp_async8(r, a.in_d + off);
+    cp_async8(r + kMarchThreads, a.in_e + off);
+    if (a.in_u) cp_async8(r + 2 * kMarchThreads, a.in_u + off);
+    if (a.in_v) cp_async8(r + 3 * kMarchThreads, a.in_v + off);
+    if (a.in_w) cp_async8(r + 4 * kMarchThreads, a.in_w + off);
+    if (DUAL) cp_async8(r + 5 * kMarchThreads, a.in_ge + off);
+    if (s >= a.is && s <= a.ie) {
+      const double* f = a.fflux + (int64_t)(s + 1 - a.is) * a.npencils + pid;
+      const int64_t pl = a.plane;
+      cp_async8(r + 6 * kMarchThreads, f + XDF * pl);
+      cp_async8(r + 7 * kMarchThreads, f + XEF * pl);
+      cp_async8(r + 8 * kMarchThreads, f + XUF * pl);
+      cp_async8(r + 9 * kMarchThreads, f + XVF * pl);
+      cp_async8(r + 10 * kMarchThreads, f + XWF * pl);
+      cp_async8(r + 11 * kMarchThreads, f + XGEF * pl);
+      cp_async8(r + 12 * kMarchThreads, f + XUB * pl);
+    }
+  }
+  cp_async_commit();  // one group per unit, empty past the pencil's end
+}
+
+template <bool DUAL>
+__device__ __forceinline__ Cell pipe_cell(const SweepArgs& a, const double* r) {
+  Cell c;
+  c.d = r[0];
+  c.e = r[kMarchThreads];
+  c.u = a.in_u ? r[2 * kMarchThreads] : 0.0;
+  c.v = a.in_v ? r[3 * kMarchThreads] : 0.0;
+  c.w = a.in_w ? r[4 * kMarchThreads] : 0.0;
+  c.ge = DUAL ? r[5 * kMarchThreads] : 0.0;
+  return c;
+}
+
+__device__ __forceinline__ Flux pipe_flux(const double* r) {
+  Flux f;
+  f.df = r[6 * kMarchThreads];
+  f.ef = r[7 * kMarchThreads];
+  f.uf = r[8 * kMarchThreads];
+  f.vf = r[9 * kMarchThreads];
+  f.wf = r[10 * kMarchThreads];
+  f.gef = r[11 * kMarchThreads];
+  f.ub = r[12 * kMarchThreads];
+  return f;
+}
+
 // flux_hll for cell c (flux_hll.F with i1 = i2 = c): replaces the fluxes of faces c and
 // c+1 and returns ges(c); ges(c+1), which the single-cell call leaves to its unset
 // locals at index c+2, is defined from the HLL state of face c+2 when that face exists.
@@ -569,10 +662,15 @@ __device__ __forceinline__ void flush_stage(const SweepArgs& a, const double* st
 // lanes without a pencil (valid = false) and lanes whose pencil was flagged, since the
 // warp flushes the staged outputs together; those lanes skip all loads and computation.  A flagged pencil's partial outputs are rewritten by the
 // fallback pass.
-template <bool DUAL, bool GRAV, bool FALLBACK, bool STAGED = false>
+//
+// PD > 0 (y and z sweeps, hot pass): the inputs arrive through the cp.async ring at
+// distance PD (ring: this thread's column of it) instead of a one-step register
+// prefetch.
+template <bool DUAL, bool GRAV, bool FALLBACK, bool STAGED = false, int PD = 0>
 __device__ __forceinline__ bool update_pencil(const SweepArgs& a, int64_t pid, const Phys& P,
                                               UpdateCounts& cnt, bool valid = true,
-                                              double* stage = nullptr, int64_t pid0 = 0) {
+                                              double* stage = nullptr, int64_t pid0 = 0,
+                                              double* ring = nullptr) {
   bool live = valid, flagged = false;
   const int64_t base = live ? (pid % a.n1) * a.s1 + (pid / a.n1) * a.s2 : 0;
   const int64_t t1 = pid % a.n1, t2 = pid / a.n1;
@@ -606,9 +704,15 @@ __device__ __forceinline__ bool update_pencil(const SweepArgs& a, int64_t pid, c
   // one-step prefetch of cell t and face t+1
   Cell Cpf = Cm;
   Flux Fpf = F0;
+  constexpr bool PIPE = PD > 0;
   if (live) {
-    Cpf = STAGED ? load_cell_keep<DUAL>(a, base) : load_cell<DUAL>(a, base);
-    if (0 >= is && 0 <= ie) Fpf = load_flux(a, (int64_t)(1 - is) * np + pid);
+    if (PIPE) {
+#pragma unroll
+      for (int u = 0; u < PD; ++u) pipe_issue<DUAL, PD>(a, ring, base, pid, u);
+    } else {
+      Cpf = STAGED ? load_cell_keep<DUAL>(a, base) : load_cell<DUAL>(a, base);
+      if (0 >= is && 0 <= ie) Fpf = load_flux(a, (int64_t)(1 - is) * np + pid);
+    }
   }
 
 #pragma unroll 1
@@ -620,12 +724,20 @@ __device__ __forceinline__ bool update_pencil(const SweepArgs& a, int64_t pid, c
     double govv_next = 0.0;
     // (1) check of cell t
     if (live && t < n) {
-      Cn = Cpf;
-      if (t >= is && t <= ie) F1 = Fpf;
-      if (t + 1 < n) {
-        Cpf = STAGED ? load_cell_keep<DUAL>(a, base + (int64_t)(t + 1) * sa)
-                     : load_cell<DUAL>(a, base + (int64_t)(t + 1) * sa);
-        if (t + 1 >= is && t + 1 <= ie) Fpf = load_flux(a, (int64_t)(t + 2 - is) * np + pid);
+      if (PIPE) {
+        cp_async_wait<(PD > 0 ? PD - 1 : 0)>();  // unit t has landed, t+1 .. t+PD-1 may not
+        const double* r = ring + (t % (PD + 1)) * (kUnitVals * kMarchThreads);
+        Cn = pipe_cell<DUAL>(a, r);
+        if (t >= is && t <= ie) F1 = pipe_flux(r);
+        pipe_issue<DUAL, PD>(a, ring, base, pid, t + PD);  // into the slot read at t-1
+      } else {
+        Cn = Cpf;
+        if (t >= is && t <= ie) F1 = Fpf;
+        if (t + 1 < n) {
+          Cpf = STAGED ? load_cell_keep<DUAL>(a, base + (int64_t)(t + 1) * sa)
+                       : load_cell<DUAL>(a, base + (int64_t)(t + 1) * sa);
+          if (t + 1 >= is && t + 1 <= ie) Fpf = load_flux(a, (int64_t)(t + 2 - is) * np + pid);
+        }
       }
       if (t >= is && t <= ie) {
         if (DUAL) {
@@ -633,7 +745,10 @@ __device__ __forceinline__ bool update_pencil(const SweepArgs& a, int64_t pid, c
           ges_n = gov ? govv : P.dt / a.coef[t].dx * pcent * (F0.ub - F1.ub);
         }
         if (Cn.d + (F0.df - F1.df) <= 0.0 || Cn.e < 0.0) {
-          if (!FALLBACK && !STAGED) return true;  // hand the pencil to the fallback pass
+          if (!FALLBACK && !STAGED) {  // hand the pencil to the fallback pass
+            if (PIPE) cp_async_wait<0>();
+            return true;
+          }
           if (!FALLBACK) {  // STAGED: stop computing, keep joining the block's flushes
             live = false;
             flagged = true;
@@ -752,6 +867,7 @@ __device__ __forceinline__ bool update_pencil(const SweepArgs& a, int64_t pid, c
       flush_stage<DUAL>(a, stage, pid0, c0, c - c0 + 1);
     }
   }
+  if (PIPE) cp_async_wait<0>();  // only empty groups remain
   cnt.nonfinite += nonfin;
   cnt.dtmin = dtmin;
   return flagged;
@@ -760,13 +876,39 @@ __device__ __forceinline__ bool update_pencil(const SweepArgs& a, int64_t pid, c
 #ifndef PPM_UPDATE_MINBLOCKS
 #define PPM_UPDATE_MINBLOCKS (3 * 128 / PPM_MARCH_THREADS)
 #endif
+// y and z sweeps: a single grid at 4 blocks/SM (the ring frees the prefetch registers),
+// a batch of grids at 3
+#ifndef PPM_UPDATE_YZ_MINBLOCKS
+#define PPM_UPDATE_YZ_MINBLOCKS (4 * 128 / PPM_MARCH_THREADS)
+#endif
+#ifndef PPM_UPDATE_YZ_BATCH_MINBLOCKS
+#define PPM_UPDATE_YZ_BATCH_MINBLOCKS PPM_UPDATE_MINBLOCKS
+#endif
+
+// the input ring's distance: none for the x sweep
+template <bool ONE, bool STAGED>
+__host__ __device__ constexpr int update_pipe() {
+  return STAGED ? 0 : (ONE ? PPM_UPDATE_PIPE_ONE : PPM_UPDATE_PIPE_BATCH);
+}
+constexpr int kStageBlock = (kMarchThreads / 32) * kStageWarp;
+// dynamic shared memory of the update kernel: the x sweep's output staging (one buffer
+// per warp) or the y and z sweeps' input ring
+template <bool ONE, bool STAGED>
+constexpr size_t update_smem_bytes() {
+  return sizeof(double) * ((STAGED ? kStageBlock : 0) + ring_doubles<update_pipe<ONE, STAGED>()>());
+}
 
 // STAGED: the x sweep (pencils along the contiguous axis) with staged outputs.
 template <bool DUAL, bool GRAV, bool ONE, bool STAGED>
-__global__ void __launch_bounds__(kMarchThreads, PPM_UPDATE_MINBLOCKS)
+__global__ void __launch_bounds__(kMarchThreads,
+                                  STAGED ? PPM_UPDATE_MINBLOCKS
+                                         : (ONE ? PPM_UPDATE_YZ_MINBLOCKS
+                                                : PPM_UPDATE_YZ_BATCH_MINBLOCKS))
     update_kernel(const __grid_constant__ BatchArgs B) {
   __shared__ unsigned long long s_cnt[2];
-  __shared__ double s_stage[STAGED ? (kMarchThreads / 32) * kStageWarp : 1];  // per warp
+  extern __shared__ double s_dyn[];
+  double* const s_stage = s_dyn;
+  double* const s_ring = s_dyn;
   if (threadIdx.x < 2) s_cnt[threadIdx.x] = 0ull;
   int64_t lb;
   const int g = locate<ONE>(B.march_prefix, B.ngrids, lb);
@@ -779,8 +921,9 @@ __global__ void __launch_bounds__(kMarchThreads, PPM_UPDATE_MINBLOCKS)
   if (STAGED || valid) {
     const Phys P = make_phys(a);
     UpdateCounts cnt = {0, 0, 0, 1.0e20};
-    if (update_pencil<DUAL, GRAV, false, STAGED>(
-            a, pid, P, cnt, valid, s_stage + (threadIdx.x >> 5) * kStageWarp, wpid0)) {
+    if (update_pencil<DUAL, GRAV, false, STAGED, update_pipe<ONE, STAGED>()>(
+            a, pid, P, cnt, valid, s_stage + (threadIdx.x >> 5) * kStageWarp, wpid0,
+            s_ring + threadIdx.x)) {
       const unsigned long long slot = atomicAdd(&B.counters[kCntFlagged], 1ull);
       B.flagged[slot] = ((int64_t)g << 40) | pid;
     } else {
@@ -821,6 +964,26 @@ __global__ void __launch_bounds__(128) fallback_kernel(const __grid_constant__ B
   }
 }
 
+// Above 48 KB of dynamic shared memory a kernel needs the opt-in attribute, set once
+// per device (a function attribute is not a stream operation, so this is also legal
+// while a stream is being captured).
+template <bool DUAL, bool GRAV, bool ONE, bool STAGED>
+void launch_update(const BatchArgs& B, int64_t march_blocks, cudaStream_t st) {
+  constexpr size_t bytes = update_smem_bytes<ONE, STAGED>();
+  if (bytes > 48 * 1024) {
+    static std::atomic<unsigned long long> done{0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const unsigned long long bit = 1ull << (dev & 63);
+    if (!(done.load(std::memory_order_acquire) & bit)) {
+      cudaFuncSetAttribute(update_kernel<DUAL, GRAV, ONE, STAGED>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+      done.fetch_or(bit, std::memory_order_release);
+    }
+  }
+  update_kernel<DUAL, GRAV, ONE, STAGED><<<(unsigned)march_blocks, kMarchThreads, bytes, st>>>(B);
+}
+
 template <bool DUAL, bool GRAV, bool ONE>
 void launch_stages(const BatchArgs& B, int64_t march_blocks, int64_t riemann_blocks,
                    cudaStream_t st, cudaEvent_t* ev, bool learned, bool staged) {
@@ -839,9 +1002,9 @@ void launch_stages(const BatchArgs& B, int64_t march_blocks, int64_t riemann_blo
     riemann_kernel<DUAL, ONE, false><<<(unsigned)riemann_blocks, kRiemannThreads, 0, st>>>(B);
   mark(3);
   if (staged)
-    update_kernel<DUAL, GRAV, ONE, true><<<(unsigned)march_blocks, kMarchThreads, 0, st>>>(B);
+    launch_update<DUAL, GRAV, ONE, true>(B, march_blocks, st);
   else
-    update_kernel<DUAL, GRAV, ONE, false><<<(unsigned)march_blocks, kMarchThreads, 0, st>>>(B);
+    launch_update<DUAL, GRAV, ONE, false>(B, march_blocks, st);
   mark(4);
   fallback_kernel<DUAL, GRAV, ONE><<<64, 128, 0, st>>>(B);
   mark(5);
