@@ -9,6 +9,7 @@
 // device-resident time loop issues no host-to-device copies after its first step and
 // can be replayed as a CUDA graph.
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>  // PFN_cuTensorMapEncodeTiled
 
 #include <algorithm>
 #include <array>
@@ -417,6 +418,50 @@ void build_coef_tables(int dim, const std::vector<GridIO>& io, CoefTables& ct) {
   }
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link against the
+// driver library); null when the driver does not offer it
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static const PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) !=
+            cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      f = nullptr;
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+  }();
+  return fn;
+}
+
+// The x sweep of a single grid: 2-D tensor maps (cells x pencils) of its six input
+// fields, for the update kernel's TMA tiles.  They need a pencil to be a whole row of
+// the array (the x sweep covers every row, ghosts included), a 16-byte aligned base and
+// rows of a multiple of 16 bytes (even GridDimension[0]); otherwise B.x_tma stays 0 and
+// the kernel uses plain loads.
+void set_x_tiles(BatchArgs& B, const SweepArgs& a) {
+  B.x_tma = 0;
+  if (a.sa != 1 || a.s1 != a.n || a.s2 != (int64_t)a.n * a.n1 ||
+      a.npencils != (int64_t)a.n1 * a.n2 || a.n % 2 != 0 || a.npencils >= (int64_t(1) << 31))
+    return;
+  const PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+  if (!enc) return;
+  const double* f[6] = {a.in_d, a.in_e, a.in_u, a.in_v, a.in_w, a.in_ge};
+  for (int k = 0; k < 6; ++k) {
+    std::memset(&B.xin[k], 0, sizeof(B.xin[k]));
+    if (!f[k]) continue;
+    if ((uintptr_t)f[k] % 16 != 0) return;
+    cuuint64_t dim[2] = {(cuuint64_t)a.n, (cuuint64_t)a.npencils};
+    cuuint64_t stride[1] = {(cuuint64_t)a.n * sizeof(double)};
+    cuuint32_t box[2] = {ppm::kXTileCells, ppm::kXTileRows};
+    cuuint32_t estride[2] = {1, 1};
+    if (enc(&B.xin[k], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<double*>(f[k]), dim,
+            stride, box, estride, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+            CU_TENSOR_MAP_L2_PROMOTION_L2_64B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+      return;
+  }
+  B.x_tma = 1;
+}
+
 // Everything one directional sweep of a batch needs on the device.
 struct SweepPlan {
   BatchArgs B;
@@ -669,6 +714,8 @@ int prepare_sweep(ppm_b200_context* ctx, int dim, int position, const ppm_b200_p
   unsigned char* base = (unsigned char*)ctx->mirror[slot].dev.p;
   std::memset(&plan.B.one, 0, sizeof(plan.B.one));
   if (ng == 1) plan.B.one = rec[0];
+  plan.B.x_tma = 0;
+  if (ng == 1 && dim == 0) set_x_tiles(plan.B, rec[0]);
   plan.B.grids = (const SweepArgs*)base;
   plan.B.ngrids = ng;
   plan.B.march_prefix = (const int64_t*)(base + off_m);
@@ -750,7 +797,8 @@ int read_counters(ppm_b200_context* ctx, ppm_b200_stats* st, int* status) {
     st->guess_rejected += (long long)c[ppm::kCntGuessRejected];
   }
   int s = PPM_B200_OK;
-  if (c[ppm::kCntFatal]) s = PPM_B200_ERR_NEGATIVE;
+  if (c[ppm::kCntTimeout]) s = PPM_B200_ERR_TIMEOUT;
+  else if (c[ppm::kCntFatal]) s = PPM_B200_ERR_NEGATIVE;
   else if (c[ppm::kCntNonFinite]) s = PPM_B200_ERR_NONFINITE;
   if (status) *status = s;
   return PPM_B200_OK;
@@ -1063,6 +1111,7 @@ std::string graph_key(ppm_b200_context* ctx, const ppm_b200_params* p, const Sol
     key_put(k, sp.sweep[s].march_blocks);
     key_put(k, sp.sweep[s].riemann_blocks);
     key_put(k, sp.sweep[s].contiguous);
+    key_put(k, b.x_tma);
     key_put(k, ctx->mirror[kSlotSweep0 + 3 * sp.order[s] + s].version);
   }
   return k;
@@ -1090,6 +1139,7 @@ const char* ppm_b200_error_string(int code) {
     case PPM_B200_ERR_NEGATIVE: return "negative density or energy the reference aborts on";
     case PPM_B200_ERR_NONFINITE: return "non-finite value in the output";
     case PPM_B200_ERR_TOO_LARGE: return "size exceeds the fixed limit of this entry point";
+    case PPM_B200_ERR_TIMEOUT: return "a bounded device wait on an asynchronous copy gave up";
     default: return "unknown error";
   }
 }

@@ -153,9 +153,18 @@ __global__ void __launch_bounds__(256) boundary_kernel(const __grid_constant__ E
   const ElemGrid& G = B.grids[batch_locate(B.size_prefix, B.ngrids, blockIdx.x, lb)];
   const int64_t g = lb * 256 + threadIdx.x;
   if (g >= G.size) return;
-  const int i = (int)(g % G.dims[0]);
-  const int j = (int)((g / G.dims[0]) % G.dims[1]);
-  const int k = (int)(g / ((int64_t)G.dims[0] * G.dims[1]));
+  int i, j, k;
+  if (G.size <= 0x7fffffff) {  // 32-bit divides: far cheaper than 64-bit ones
+    const unsigned gg = (unsigned)g, n0 = (unsigned)G.dims[0], n1 = (unsigned)G.dims[1];
+    const unsigned row = gg / n0;
+    i = (int)(gg - row * n0);
+    k = (int)(row / n1);
+    j = (int)(row - (unsigned)k * n1);
+  } else {
+    i = (int)(g % G.dims[0]);
+    j = (int)((g / G.dims[0]) % G.dims[1]);
+    k = (int)(g / ((int64_t)G.dims[0] * G.dims[1]));
+  }
   const int si = G.dims[0] > 1 ? bc_map(i, G.start[0], G.end[0], G.bc[0]) : i;
   const int sj = G.dims[1] > 1 ? bc_map(j, G.start[1], G.end[1], G.bc[1]) : j;
   const int sk = G.dims[2] > 1 ? bc_map(k, G.start[2], G.end[2], G.bc[2]) : k;

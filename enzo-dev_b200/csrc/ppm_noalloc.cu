@@ -258,6 +258,7 @@ extern "C" int ppm_b200_euler_sweep_static(int dim, const ppm_b200_params* p,
     stats->fallbacks += (long long)c[ppm::kCntFallbacks];
     stats->fatal_cells += (long long)c[ppm::kCntFatal];
   }
+  if (c[ppm::kCntTimeout]) return PPM_B200_ERR_TIMEOUT;
   if (c[ppm::kCntFatal]) return PPM_B200_ERR_NEGATIVE;
   if (c[ppm::kCntNonFinite]) return PPM_B200_ERR_NONFINITE;
   return PPM_B200_OK;

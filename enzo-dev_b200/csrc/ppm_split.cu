@@ -512,6 +512,120 @@ __device__ __forceinline__ Cell pipe_cell(const SweepArgs& a, const double* r) {
   return c;
 }
 
+// ------------------------------------------------ TMA tiles of the x sweep's update
+// The x sweep's pencils run along the contiguous axis: a warp's 32 pencils are 32 rows
+// of every field.  Plain loads fetch one sector per lane per cell; instead lane 0 of
+// each warp has the tensor-memory accelerator copy the warp's [32 pencils x 2 cells]
+// tile of every input field into shared memory, two chunks ahead, completing on an
+// mbarrier per buffer (no multicast; the tensor maps cover this GPU's own fields).
+// Every lane waits on the chunk's barrier (bounded: after ~1 s the warp records a
+// timeout, stops copying and drains what is in flight) and reads its own row.
+#ifndef PPM_X_TMA
+#define PPM_X_TMA 1
+#endif
+constexpr int kXTile = kXTileRows * kXTileCells;       // doubles per field and buffer
+constexpr int kXWarp = kXBuffers * 6 * kXTile;         // doubles per warp
+constexpr long long kXWaitCycles = 2000000000ll;       // ~1 s at the B200's clocks
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const long long t0 = clock64();
+  while (!mbar_try_wait(bar, parity))
+    if (clock64() - t0 > kXWaitCycles) return false;
+  return true;
+}
+__device__ __forceinline__ void tma_load_2d(double* dst, const CUtensorMap* map, int x, int y,
+                                            uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3}], [%4];" ::"r"(smem_u32(dst)),
+      "l"(map), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
+
+struct XTiles {
+  double* buf;                  // this warp's kXBuffers x 6 tiles [field][pencil][cell]
+  uint64_t* bar;                // this warp's kXBuffers mbarriers
+  const CUtensorMap* map;       // the six tensor maps (kernel parameter space)
+  unsigned long long* timeouts; // the batch's kCntTimeout counter
+  unsigned fields;              // bit f: input field f present
+  unsigned bytes;               // bytes of one chunk (all present fields)
+  int row0;                     // the warp's first pencil
+  int last;                     // last chunk issued, -1: none
+  bool broken;                  // a wait gave up: no further copies
+};
+
+__device__ __forceinline__ void x_issue(XTiles& x, int q) {
+  const int b = q % kXBuffers;
+  if ((threadIdx.x & 31) == 0) {
+    mbar_expect_tx(x.bar + b, x.bytes);
+#pragma unroll
+    for (int f = 0; f < 6; ++f)
+      if (x.fields & (1u << f))
+        tma_load_2d(x.buf + (b * 6 + f) * kXTile, x.map + f, q * kXTileCells, x.row0, x.bar + b);
+  }
+  x.last = q;
+}
+
+// warp-uniform: called by every lane at the first step of chunk q (t = q * kXTileCells)
+__device__ __forceinline__ void x_chunk(XTiles& x, int q, int n) {
+  __syncwarp();  // every lane has read chunk q-1, whose buffer the next copy reuses
+  if (x.broken) return;
+  const int next = q + kXBuffers - 1;
+  if (next * kXTileCells < n) x_issue(x, next);
+  const bool ok = mbar_wait_bounded(x.bar + q % kXBuffers, (unsigned)(q / kXBuffers) & 1u);
+  if (__any_sync(0xffffffffu, !ok)) {
+    x.broken = true;
+    if ((threadIdx.x & 31) == 0) atomicAdd(x.timeouts, 1ull);
+  }
+}
+
+// after a timeout: wait (bounded) for the last copy issued into every buffer
+__device__ __forceinline__ void x_drain(XTiles& x) {
+  if (!x.broken) return;
+  for (int b = 0; b < kXBuffers; ++b) {
+    int q = x.last - ((x.last - b) % kXBuffers + kXBuffers) % kXBuffers;
+    if (q >= 0) mbar_wait_bounded(x.bar + b, (unsigned)(q / kXBuffers) & 1u);
+  }
+}
+
+template <bool DUAL>
+__device__ __forceinline__ Cell x_cell(const XTiles& x, const SweepArgs& a, int t) {
+  const double* r = x.buf + ((t / kXTileCells) % kXBuffers) * (6 * kXTile) +
+                    (threadIdx.x & 31) * kXTileCells + t % kXTileCells;
+  Cell c;
+  c.d = r[0];
+  c.e = r[kXTile];
+  c.u = a.in_u ? r[2 * kXTile] : 0.0;
+  c.v = a.in_v ? r[3 * kXTile] : 0.0;
+  c.w = a.in_w ? r[4 * kXTile] : 0.0;
+  c.ge = DUAL ? r[5 * kXTile] : 0.0;
+  return c;
+}
+
 __device__ __forceinline__ Flux pipe_flux(const double* r) {
   Flux f;
   f.df = r[6 * kMarchThreads];
@@ -587,17 +701,18 @@ struct UpdateCounts {
 template <bool DUAL>
 __device__ __forceinline__ double cell_dt1(const SweepArgs& a, const Cell& o, double dx_sweep,
                                            int64_t t1, int64_t t2, const Phys& P) {
-  double vel[3], dx[3];
-  vel[a.dim] = o.u;
-  vel[(a.dim + 1) % 3] = o.v;
-  vel[(a.dim + 2) % 3] = o.w;
-  const int ax1 = a.dim == 0 ? 1 : 0, ax2 = a.dim == 2 ? 1 : 2;
-  dx[a.dim] = dx_sweep;
-  dx[ax1] = a.cw1 ? a.cw1[t1] : 1.0;
-  dx[ax2] = a.cw2 ? a.cw2[t2] : 1.0;
-  const double velocity1 = vel[0];
-  const double velocity2 = a.rank > 1 ? vel[1] : 0.0;
-  const double velocity3 = a.rank > 2 ? vel[2] : 0.0;
+  // axis x, y, z of the sweep's (u, v, w) and cell widths: (sweep, t1, t2) axes are
+  // (x, y, z), (y, x, z) and (z, x, y) -- as selects, not a dynamically indexed array
+  const int dim = a.dim;
+  const double w1 = a.cw1 ? a.cw1[t1] : 1.0, w2 = a.cw2 ? a.cw2[t2] : 1.0;
+  const double dx[3] = {dim == 0 ? dx_sweep : w1, dim == 1 ? dx_sweep : (dim == 0 ? w1 : w2),
+                        dim == 2 ? dx_sweep : w2};
+  const double vx = dim == 0 ? o.u : (dim == 1 ? o.w : o.v);
+  const double vy = dim == 0 ? o.v : (dim == 1 ? o.u : o.w);
+  const double vz = dim == 0 ? o.w : (dim == 1 ? o.v : o.u);
+  const double velocity1 = vx;
+  const double velocity2 = a.rank > 1 ? vy : 0.0;
+  const double velocity3 = a.rank > 2 ? vz : 0.0;
   double gas_energy;
   if (DUAL) {
     gas_energy = o.ge;
@@ -628,7 +743,10 @@ __device__ __forceinline__ double cell_dt1(const SweepArgs& a, const Cell& o, do
 #ifndef PPM_X_STAGE_STORES
 #define PPM_X_STAGE_STORES 1
 #endif
-enum { kStageCells = 4, kStageLd = 32 + 8 };
+#ifndef PPM_STAGE_LD
+#define PPM_STAGE_LD (32 + 8)
+#endif
+enum { kStageCells = 4, kStageLd = PPM_STAGE_LD };
 constexpr int kStageField = kStageCells * kStageLd;
 constexpr int kStageWarp = 6 * kStageField;  // doubles per warp
 
@@ -666,11 +784,13 @@ __device__ __forceinline__ void flush_stage(const SweepArgs& a, const double* st
 // PD > 0 (y and z sweeps, hot pass): the inputs arrive through the cp.async ring at
 // distance PD (ring: this thread's column of it) instead of a one-step register
 // prefetch.
-template <bool DUAL, bool GRAV, bool FALLBACK, bool STAGED = false, int PD = 0>
+//
+// XT (x sweep of a single grid, with STAGED): the input cells arrive as TMA tiles (xt).
+template <bool DUAL, bool GRAV, bool FALLBACK, bool STAGED = false, int PD = 0, bool XT = false>
 __device__ __forceinline__ bool update_pencil(const SweepArgs& a, int64_t pid, const Phys& P,
                                               UpdateCounts& cnt, bool valid = true,
                                               double* stage = nullptr, int64_t pid0 = 0,
-                                              double* ring = nullptr) {
+                                              double* ring = nullptr, XTiles* xt = nullptr) {
   bool live = valid, flagged = false;
   const int64_t base = live ? (pid % a.n1) * a.s1 + (pid / a.n1) * a.s2 : 0;
   const int64_t t1 = pid % a.n1, t2 = pid / a.n1;
@@ -710,13 +830,17 @@ __device__ __forceinline__ bool update_pencil(const SweepArgs& a, int64_t pid, c
 #pragma unroll
       for (int u = 0; u < PD; ++u) pipe_issue<DUAL, PD>(a, ring, base, pid, u);
     } else {
-      Cpf = STAGED ? load_cell_keep<DUAL>(a, base) : load_cell<DUAL>(a, base);
+      if (!XT) Cpf = STAGED ? load_cell_keep<DUAL>(a, base) : load_cell<DUAL>(a, base);
       if (0 >= is && 0 <= ie) Fpf = load_flux(a, (int64_t)(1 - is) * np + pid);
     }
+  }
+  if (XT) {  // warp-wide, live or not: the first chunks
+    for (int q = 0; q < kXBuffers - 1 && q * kXTileCells < n; ++q) x_issue(*xt, q);
   }
 
 #pragma unroll 1
   for (int t = 0; t <= n; ++t) {
+    if (XT && t < n && t % kXTileCells == 0) x_chunk(*xt, t / kXTileCells, n);
     Cell Cn = Cm;
     double ges_n = 0.0;
     Flux F1 = F0;
@@ -731,11 +855,12 @@ __device__ __forceinline__ bool update_pencil(const SweepArgs& a, int64_t pid, c
         if (t >= is && t <= ie) F1 = pipe_flux(r);
         pipe_issue<DUAL, PD>(a, ring, base, pid, t + PD);  // into the slot read at t-1
       } else {
-        Cn = Cpf;
+        Cn = XT ? x_cell<DUAL>(*xt, a, t) : Cpf;
         if (t >= is && t <= ie) F1 = Fpf;
         if (t + 1 < n) {
-          Cpf = STAGED ? load_cell_keep<DUAL>(a, base + (int64_t)(t + 1) * sa)
-                       : load_cell<DUAL>(a, base + (int64_t)(t + 1) * sa);
+          if (!XT)
+            Cpf = STAGED ? load_cell_keep<DUAL>(a, base + (int64_t)(t + 1) * sa)
+                         : load_cell<DUAL>(a, base + (int64_t)(t + 1) * sa);
           if (t + 1 >= is && t + 1 <= ie) Fpf = load_flux(a, (int64_t)(t + 2 - is) * np + pid);
         }
       }
@@ -868,6 +993,7 @@ __device__ __forceinline__ bool update_pencil(const SweepArgs& a, int64_t pid, c
     }
   }
   if (PIPE) cp_async_wait<0>();  // only empty groups remain
+  if (XT) x_drain(*xt);
   cnt.nonfinite += nonfin;
   cnt.dtmin = dtmin;
   return flagged;
@@ -881,6 +1007,11 @@ __device__ __forceinline__ bool update_pencil(const SweepArgs& a, int64_t pid, c
 #ifndef PPM_UPDATE_YZ_MINBLOCKS
 #define PPM_UPDATE_YZ_MINBLOCKS (4 * 128 / PPM_MARCH_THREADS)
 #endif
+// x sweep with TMA tiles: 2 blocks/SM (78 KB of shared memory a block; at 3 blocks the
+// shared memory leaves too little L1)
+#ifndef PPM_UPDATE_XT_MINBLOCKS
+#define PPM_UPDATE_XT_MINBLOCKS (2 * 128 / PPM_MARCH_THREADS)
+#endif
 #ifndef PPM_UPDATE_YZ_BATCH_MINBLOCKS
 #define PPM_UPDATE_YZ_BATCH_MINBLOCKS PPM_UPDATE_MINBLOCKS
 #endif
@@ -891,39 +1022,65 @@ __host__ __device__ constexpr int update_pipe() {
   return STAGED ? 0 : (ONE ? PPM_UPDATE_PIPE_ONE : PPM_UPDATE_PIPE_BATCH);
 }
 constexpr int kStageBlock = (kMarchThreads / 32) * kStageWarp;
-// dynamic shared memory of the update kernel: the x sweep's output staging (one buffer
-// per warp) or the y and z sweeps' input ring
-template <bool ONE, bool STAGED>
+constexpr int kXBlock = (kMarchThreads / 32) * kXWarp;
+// dynamic shared memory of the update kernel: the x sweep's TMA tiles (XT) and output
+// staging, one of each per warp, or the y and z sweeps' input ring
+template <bool ONE, bool STAGED, bool XT>
 constexpr size_t update_smem_bytes() {
-  return sizeof(double) * ((STAGED ? kStageBlock : 0) + ring_doubles<update_pipe<ONE, STAGED>()>());
+  return sizeof(double) * ((XT ? kXBlock : 0) + (STAGED ? kStageBlock : 0) +
+                           ring_doubles<update_pipe<ONE, STAGED>()>());
 }
 
-// STAGED: the x sweep (pencils along the contiguous axis) with staged outputs.
-template <bool DUAL, bool GRAV, bool ONE, bool STAGED>
+// STAGED: the x sweep (pencils along the contiguous axis) with staged outputs; XT: its
+// input cells as TMA tiles (a single grid with B.x_tma set).
+template <bool DUAL, bool GRAV, bool ONE, bool STAGED, bool XT>
 __global__ void __launch_bounds__(kMarchThreads,
-                                  STAGED ? PPM_UPDATE_MINBLOCKS
+                                  STAGED ? (XT ? PPM_UPDATE_XT_MINBLOCKS : PPM_UPDATE_MINBLOCKS)
                                          : (ONE ? PPM_UPDATE_YZ_MINBLOCKS
                                                 : PPM_UPDATE_YZ_BATCH_MINBLOCKS))
     update_kernel(const __grid_constant__ BatchArgs B) {
+  static_assert(!XT || (ONE && STAGED), "TMA tiles serve the x sweep of a single grid");
   __shared__ unsigned long long s_cnt[2];
-  extern __shared__ double s_dyn[];
-  double* const s_stage = s_dyn;
-  double* const s_ring = s_dyn;
+  __shared__ uint64_t s_xbar[XT ? (kMarchThreads / 32) * kXBuffers : 1];
+  extern __shared__ __align__(128) double s_dyn[];
+  double* const s_xtile = s_dyn;                                // XT: kXWarp per warp
+  double* const s_stage = s_dyn + (XT ? kXBlock : 0);           // STAGED: kStageWarp per warp
+  double* const s_ring = s_dyn;                                 // y, z: the input ring
   if (threadIdx.x < 2) s_cnt[threadIdx.x] = 0ull;
   int64_t lb;
   const int g = locate<ONE>(B.march_prefix, B.ngrids, lb);
   PPM_BIND_RECORD(a, g)
-  if (ONE) __syncthreads();
   const int64_t pid = lb * kMarchThreads + threadIdx.x;
   const int64_t wpid0 = pid - (threadIdx.x & 31);  // first pencil of this warp
+  const int warp = threadIdx.x >> 5;
+  XTiles xt;
+  if (XT) {
+    xt.buf = s_xtile + warp * kXWarp;
+    xt.bar = s_xbar + warp * kXBuffers;
+    xt.map = B.xin;
+    xt.timeouts = B.counters + kCntTimeout;
+    xt.fields = 3u | (a.in_u ? 4u : 0u) | (a.in_v ? 8u : 0u) | (a.in_w ? 16u : 0u) |
+                ((DUAL && a.in_ge) ? 32u : 0u);
+    xt.bytes = (unsigned)__popc(xt.fields) * kXTile * (unsigned)sizeof(double);
+    xt.row0 = (int)wpid0;
+    xt.last = -1;
+    xt.broken = false;
+    if ((threadIdx.x & 31) == 0) {
+      for (int b = 0; b < kXBuffers; ++b) mbar_init(xt.bar + b, 1);
+      // the barriers' initialisation is visible to the tensor-memory accelerator
+      asm volatile("fence.mbarrier_init.release.cluster;\n\tfence.proxy.async.shared::cta;" ::
+                       : "memory");
+    }
+  }
+  if (ONE) __syncthreads();
   double my_dt = 1.0e20;
   const bool valid = pid < a.npencils;
   if (STAGED || valid) {
     const Phys P = make_phys(a);
     UpdateCounts cnt = {0, 0, 0, 1.0e20};
-    if (update_pencil<DUAL, GRAV, false, STAGED, update_pipe<ONE, STAGED>()>(
-            a, pid, P, cnt, valid, s_stage + (threadIdx.x >> 5) * kStageWarp, wpid0,
-            s_ring + threadIdx.x)) {
+    if (update_pencil<DUAL, GRAV, false, STAGED, update_pipe<ONE, STAGED>(), XT>(
+            a, pid, P, cnt, valid, s_stage + warp * kStageWarp, wpid0, s_ring + threadIdx.x,
+            &xt)) {
       const unsigned long long slot = atomicAdd(&B.counters[kCntFlagged], 1ull);
       B.flagged[slot] = ((int64_t)g << 40) | pid;
     } else {
@@ -967,21 +1124,22 @@ __global__ void __launch_bounds__(128) fallback_kernel(const __grid_constant__ B
 // Above 48 KB of dynamic shared memory a kernel needs the opt-in attribute, set once
 // per device (a function attribute is not a stream operation, so this is also legal
 // while a stream is being captured).
-template <bool DUAL, bool GRAV, bool ONE, bool STAGED>
+template <bool DUAL, bool GRAV, bool ONE, bool STAGED, bool XT>
 void launch_update(const BatchArgs& B, int64_t march_blocks, cudaStream_t st) {
-  constexpr size_t bytes = update_smem_bytes<ONE, STAGED>();
+  constexpr size_t bytes = update_smem_bytes<ONE, STAGED, XT>();
   if (bytes > 48 * 1024) {
     static std::atomic<unsigned long long> done{0};
     int dev = 0;
     cudaGetDevice(&dev);
     const unsigned long long bit = 1ull << (dev & 63);
     if (!(done.load(std::memory_order_acquire) & bit)) {
-      cudaFuncSetAttribute(update_kernel<DUAL, GRAV, ONE, STAGED>,
+      cudaFuncSetAttribute(update_kernel<DUAL, GRAV, ONE, STAGED, XT>,
                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
       done.fetch_or(bit, std::memory_order_release);
     }
   }
-  update_kernel<DUAL, GRAV, ONE, STAGED><<<(unsigned)march_blocks, kMarchThreads, bytes, st>>>(B);
+  update_kernel<DUAL, GRAV, ONE, STAGED, XT>
+      <<<(unsigned)march_blocks, kMarchThreads, bytes, st>>>(B);
 }
 
 template <bool DUAL, bool GRAV, bool ONE>
@@ -1001,10 +1159,12 @@ void launch_stages(const BatchArgs& B, int64_t march_blocks, int64_t riemann_blo
   else
     riemann_kernel<DUAL, ONE, false><<<(unsigned)riemann_blocks, kRiemannThreads, 0, st>>>(B);
   mark(3);
-  if (staged)
-    launch_update<DUAL, GRAV, ONE, true>(B, march_blocks, st);
+  if (PPM_X_TMA && staged && ONE && B.x_tma)
+    launch_update<DUAL, GRAV, ONE, true, ONE>(B, march_blocks, st);
+  else if (staged)
+    launch_update<DUAL, GRAV, ONE, true, false>(B, march_blocks, st);
   else
-    launch_update<DUAL, GRAV, ONE, false>(B, march_blocks, st);
+    launch_update<DUAL, GRAV, ONE, false, false>(B, march_blocks, st);
   mark(4);
   fallback_kernel<DUAL, GRAV, ONE><<<64, 128, 0, st>>>(B);
   mark(5);

@@ -1,6 +1,8 @@
 // ppm_sweep.cuh -- launch arguments shared by the sweep kernels and the host driver.
 #pragma once
 
+#include <cuda.h>  // CUtensorMap
+
 #include <cstdint>
 
 namespace ppm {
@@ -31,6 +33,7 @@ enum {
   kCntGuessRejected = 12,
   kCntNonFinite = 13,
   kCntFlagged = 14,  // pencils handed to the fallback pass (index into BatchArgs::flagged)
+  kCntTimeout = 15,  // bounded waits on asynchronous copies that gave up
 };
 
 struct SweepArgs {
@@ -117,7 +120,22 @@ struct BatchArgs {
   const int64_t* riemann_prefix;     // ngrids + 1
   unsigned long long* counters;      // kMaxCounters, shared by the batch
   int64_t* flagged;                  // pencils needing the fallback pass: (grid << 40) | pencil
+  // x sweep of a single grid: the update kernel reads its input cells as TMA tiles of
+  // kXTileRows pencils x kXTileCells cells, through 2-D tensor maps (cells x pencils) of
+  // d, e, u, v, w, ge (absent fields: unused).  x_tma = 0: plain loads.
+  int x_tma = 0;
+  CUtensorMap xin[6];
 };
+
+// TMA tiles of the x sweep's update kernel: a warp's 32 pencils x 4 cells (32 bytes a
+// pencil), double-buffered per warp
+#ifndef PPM_X_BUFFERS
+#define PPM_X_BUFFERS 2
+#endif
+#ifndef PPM_X_TILE_CELLS
+#define PPM_X_TILE_CELLS 4
+#endif
+enum { kXTileRows = 32, kXTileCells = PPM_X_TILE_CELLS, kXBuffers = PPM_X_BUFFERS };
 
 // Grid that owns block b of a stage, and the block's index inside that grid.
 __device__ __forceinline__ int batch_locate(const int64_t* prefix, int ngrids, int64_t b,

@@ -23,6 +23,7 @@ ERR_CUDA = -3
 ERR_NEGATIVE = -4
 ERR_NONFINITE = -5
 ERR_TOO_LARGE = -6
+ERR_TIMEOUT = -7
 MEM_HOST = 0
 MEM_DEVICE = 1
 RIEMANN_TWOSHOCK = 5

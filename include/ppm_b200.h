@@ -36,6 +36,7 @@ extern "C" {
 #define PPM_B200_ERR_NEGATIVE (-4)     /* a state the reference aborts on (flux_twoshock.F:440-443, flux_hll.F:336-383, euler.F:203-215) */
 #define PPM_B200_ERR_NONFINITE (-5)    /* non-finite output detected */
 #define PPM_B200_ERR_TOO_LARGE (-6)    /* size beyond a fixed limit of the entry point */
+#define PPM_B200_ERR_TIMEOUT (-7)      /* a bounded device wait on an asynchronous copy gave up: outputs invalid */
 
 /* memory kinds of the field pointers */
 #define PPM_B200_MEM_HOST 0   /* fields in host memory: copied in and out inside the call (like cuPPMSetBaryon/GetBaryon) */
