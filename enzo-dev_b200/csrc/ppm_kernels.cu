@@ -144,35 +144,48 @@ __device__ __forceinline__ int bc_map(int i, int s, int e, int bc) {
   return i < s ? s : e;
 }
 
-// One thread per cell of the padded grid: every ghost cell copies the cell it maps to.
-// Sources are cells that map to themselves (active cells, or ghosts of a face left to a
-// halo exchange), which this kernel never writes, so the in-place fill has no
-// read-after-write hazard.
-__global__ void __launch_bounds__(256) boundary_kernel(const __grid_constant__ ElemBatch B) {
-  int64_t lb;
-  const ElemGrid& G = B.grids[batch_locate(B.size_prefix, B.ngrids, blockIdx.x, lb)];
-  const int64_t g = lb * 256 + threadIdx.x;
-  if (g >= G.size) return;
-  int i, j, k;
-  if (G.size <= 0x7fffffff) {  // 32-bit divides: far cheaper than 64-bit ones
-    const unsigned gg = (unsigned)g, n0 = (unsigned)G.dims[0], n1 = (unsigned)G.dims[1];
-    const unsigned row = gg / n0;
-    i = (int)(gg - row * n0);
-    k = (int)(row / n1);
-    j = (int)(row - (unsigned)k * n1);
-  } else {
-    i = (int)(g % G.dims[0]);
-    j = (int)((g / G.dims[0]) % G.dims[1]);
-    k = (int)(g / ((int64_t)G.dims[0] * G.dims[1]));
-  }
-  const int si = G.dims[0] > 1 ? bc_map(i, G.start[0], G.end[0], G.bc[0]) : i;
-  const int sj = G.dims[1] > 1 ? bc_map(j, G.start[1], G.end[1], G.bc[1]) : j;
-  const int sk = G.dims[2] > 1 ? bc_map(k, G.start[2], G.end[2], G.bc[2]) : k;
-  if (si == i && sj == j && sk == k) return;
-  const int64_t src = ((int64_t)sk * G.dims[1] + sj) * G.dims[0] + si;
+__device__ __forceinline__ void copy_cell(const ElemGrid& G, int64_t dst, int64_t src) {
 #pragma unroll
   for (int n = 0; n < 6; ++n)
-    if (G.f[n]) G.f[n][g] = G.f[n][src];
+    if (G.f[n]) G.f[n][dst] = G.f[n][src];
+}
+
+// One warp per row (j, k) of the padded grid: every ghost cell copies the cell it maps
+// to.  A row whose (j, k) maps to itself holds ghosts only at its x ends; any other row
+// is copied whole from its source row, with consecutive lanes on consecutive cells.
+// Sources are cells that map to themselves in all three dimensions (active cells, or
+// ghosts of a face left to a halo exchange), which this kernel never writes, so the
+// in-place fill has no read-after-write hazard.  A grid's blocks (ceil(size / 256), 8
+// warps each) stride over its rows.
+__global__ void __launch_bounds__(256) boundary_kernel(const __grid_constant__ ElemBatch B) {
+  int64_t lb;
+  const int gi = batch_locate(B.size_prefix, B.ngrids, blockIdx.x, lb);
+  const ElemGrid& G = B.grids[gi];
+  const int64_t warps = (B.size_prefix[gi + 1] - B.size_prefix[gi]) * 8;
+  const int n0 = G.dims[0], n1 = G.dims[1], n2 = G.dims[2];
+  const int s0 = G.start[0], e0 = G.end[0], bc0 = G.bc[0];
+  const int64_t rows = (int64_t)n1 * n2;
+  const int lane = threadIdx.x & 31;
+  for (int64_t row = lb * 8 + (threadIdx.x >> 5); row < rows; row += warps) {
+    const int k = (int)(row / n1), j = (int)(row - (int64_t)k * n1);
+    const int sj = n1 > 1 ? bc_map(j, G.start[1], G.end[1], G.bc[1]) : j;
+    const int sk = n2 > 1 ? bc_map(k, G.start[2], G.end[2], G.bc[2]) : k;
+    const int64_t dst = row * n0;
+    const int64_t src = ((int64_t)sk * n1 + sj) * n0;
+    if (sj == j && sk == k) {
+      if (n0 > 1) {  // the x ghosts: i in [0, s0) and (e0, n0)
+        const int lo = s0, nx = s0 + (n0 - 1 - e0);
+        for (int m = lane; m < nx; m += 32) {
+          const int i = m < lo ? m : e0 + 1 + (m - lo);
+          const int si = bc_map(i, s0, e0, bc0);
+          if (si != i) copy_cell(G, dst + i, src + si);
+        }
+      }
+    } else {
+      for (int i = lane; i < n0; i += 32)
+        copy_cell(G, dst + i, src + (n0 > 1 ? bc_map(i, s0, e0, bc0) : i));
+    }
+  }
 }
 
 // ------------------------------------------------------------------ comoving expansion
