@@ -158,7 +158,7 @@ def committed_fp64():
 
 def committed_traffic():
     """Per-zone-sweep DRAM bytes of the sweep kernel from the committed ncu summary."""
-    f = REPO / "profiles" / "sweep_traffic_turbulence128.json"
+    f = REPO / "profiles" / "sweep_traffic_turbulence256.json"
     if f.exists():
         try:
             d = json.loads(f.read_text())
