@@ -277,6 +277,21 @@ __device__ __forceinline__ FaceState load_face(const SweepArgs& a, int64_t idx) 
   return f;
 }
 
+// The advected states (v, w, ge) of a face, which only the flux needs: the Riemann
+// kernel loads them after the Newton iteration, so they hold no registers during it.
+template <bool DUAL>
+__device__ __forceinline__ void load_face_advected(const SweepArgs& a, int64_t idx,
+                                                   FaceState& f) {
+  const double* s = a.fstate + idx;
+  const int64_t pl = a.plane;
+  f.vl = s[SVL * pl];
+  f.vr = s[SVR * pl];
+  f.wl = s[SWL * pl];
+  f.wr = s[SWR * pl];
+  f.gel = DUAL ? s[SGEL * pl] : 0.0;
+  f.ger = DUAL ? s[SGER * pl] : 0.0;
+}
+
 // ------------------------------------------------------------------ stage 2
 // per grid, blocks over (face plane fi = face - is) x (chunks of pencils)
 // LEARNED: the Newton iteration starts from the MLP's pressure (ppm_guess.cuh) and falls
@@ -310,11 +325,16 @@ __global__ void __launch_bounds__(kRiemannThreads, LEARNED ? 3 : PPM_RIEMANN_MIN
   const bool valid = pid < a.npencils;
   const Phys P = make_phys(a);
   const int64_t idx = (int64_t)fi * a.npencils + pid;
-  FaceState s;
-  if (valid) {
-    s = load_face<DUAL>(a, idx);
-  } else {
-    s = FaceState{1.0, 1.0, 1.0, 1.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  FaceState s = FaceState{1.0, 1.0, 1.0, 1.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  if (valid) {  // d, p, u now; v, w, ge after the Newton iteration
+    const double* f = a.fstate + idx;
+    const int64_t pl = a.plane;
+    s.dl = f[SDL * pl];
+    s.dr = f[SDR * pl];
+    s.pl = f[SPL * pl];
+    s.pr = f[SPR * pl];
+    s.ul = f[SUL * pl];
+    s.ur = f[SUR * pl];
   }
   float y = 0.0f, d2 = 0.0f;
   if (LEARNED) {
@@ -356,6 +376,7 @@ __global__ void __launch_bounds__(kRiemannThreads, LEARNED ? 3 : PPM_RIEMANN_MIN
       }
     }
     const double qc = P.dt / a.coef[a.is + fi].dx;
+    load_face_advected<DUAL>(a, idx, s);
     const Flux F = flux_twoshock<DUAL>(s, rs.pbar, rs.ubar, qc, P);
     double* o = a.fflux + idx;
     const int64_t pl = a.plane;
