@@ -212,6 +212,8 @@ def make_params(hp, dt, learned_guess=False, dt_device=None) -> Params:
     P.riemann_solver = RIEMANN_TWOSHOCK
     P.riemann_fallback = int(hp.fallback)
     P.reconstruction = RECONSTRUCTION_PPM
+    P.steepening = int(getattr(hp, "steepen", 0))
+    P.flattening = int(getattr(hp, "flatten", 0))
     P.learned_guess = int(learned_guess)
     P.dt_device = _addr(dt_device) if dt_device is not None else None
     return P

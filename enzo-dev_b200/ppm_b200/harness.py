@@ -91,6 +91,8 @@ class HydroParams:
     gravity: bool = False             # GravityOn
     pressure_free: bool = False       # PressureFree (:195)
     fallback: bool = True             # RiemannSolverFallback (:809)
+    steepen: int = 0                  # PPMSteepeningParameter (:184): 0 or 1
+    flatten: int = 0                  # PPMFlatteningParameter (:182): 0, 1 or 3
 
 
 def new_fields(grid, dual):

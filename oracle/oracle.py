@@ -39,6 +39,8 @@ class OraParams(C.Structure):
         ("pressure_free", C.c_int),
         ("fallback", C.c_int),
         ("max_velocity_index", C.c_int),
+        ("steepen", C.c_int),
+        ("flatten", C.c_int),
     ]
 
 
@@ -138,6 +140,8 @@ def make_params(grid, hp, dt) -> OraParams:
     P.pressure_free = int(hp.pressure_free)
     P.fallback = int(hp.fallback)
     P.max_velocity_index = grid.rank
+    P.steepen = int(getattr(hp, "steepen", 0))
+    P.flatten = int(getattr(hp, "flatten", 0))
     return P
 
 

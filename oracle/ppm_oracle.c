@@ -74,6 +74,8 @@ typedef struct {
   double *h_sl, *h_sr, *h_gesl, *h_gesr, *h_el, *h_er, *h_bm0, *h_bp0, *h_pcent;
   /* euler locals */
   double *dnu, *dnuinv, *uold;
+  /* calcdiss / steepening locals */
+  double *flat, *steep, *wflag, *ftemp, *d2d, *dxb;
   double *block;
 } work_t;
 
@@ -107,7 +109,8 @@ static int work_alloc(work_t *W, int idim, int jdim) {
       &W->duvb, &W->duwb, &W->dueb, &W->dugeb, &W->pcent,
       &W->h_sl, &W->h_sr, &W->h_gesl, &W->h_gesr, &W->h_el, &W->h_er, &W->h_bm0, &W->h_bp0,
       &W->h_pcent,
-      &W->dnu, &W->dnuinv, &W->uold};
+      &W->dnu, &W->dnuinv, &W->uold,
+      &W->flat, &W->steep, &W->wflag, &W->ftemp, &W->d2d, &W->dxb};
   const size_t n_one = sizeof(one) / sizeof(one[0]);
   /* 29 slice arrays + the 1-D temporaries */
   W->block = (double *)calloc(29 * ns + n_one * n1, sizeof(double));
@@ -135,7 +138,8 @@ static void work_free(work_t *W) {
 /* ------------------------------------------------------------------------ */
 /* intvar.F:5-179 (one pencil)                                               */
 /* ------------------------------------------------------------------------ */
-static void intvar(const double *q, int idim, int i1, int i2,
+static void intvar(const double *q, int idim, int i1, int i2, int isteep,
+                   const double *steepen, int iflatten, const double *flatten,
                    const double *c1, const double *c2, const double *c3, const double *c4,
                    const double *c5, const double *c6, const double *char1, const double *char2,
                    const double *c0, double *dq, double *ql, double *qr, double *q6,
@@ -164,7 +168,16 @@ static void intvar(const double *q, int idim, int i1, int i2,
                V(c6, i) * V(dq, i);
     V(qr, i - 1) = V(ql, i);
   }
-  /* (steepening off) monotonise, intvar.F:117-131 */
+  /* steepening, intvar.F:106-113 */
+  if (isteep != 0) {
+    for (i = i1 - 1; i <= i2 + 1; i++) {
+      V(ql, i) = (1.0 - V(steepen, i)) * V(ql, i) +
+                 V(steepen, i) * (V(q, i - 1) + 0.5 * V(dq, i - 1));
+      V(qr, i) = (1.0 - V(steepen, i)) * V(qr, i) +
+                 V(steepen, i) * (V(q, i + 1) - 0.5 * V(dq, i + 1));
+    }
+  }
+  /* monotonise, intvar.F:117-131 */
   for (i = i1 - 1; i <= i2 + 1; i++) {
     double temp1 = (V(qr, i) - V(q, i)) * (V(q, i) - V(ql, i));
     double temp2 = V(qr, i) - V(ql, i);
@@ -178,7 +191,14 @@ static void intvar(const double *q, int idim, int i1, int i2,
     if (temp22 < temp23) V(ql, i) = 3.0 * V(q, i) - 2.0 * V(qr, i);
     if (temp22 < -temp23) V(qr, i) = 3.0 * V(q, i) - 2.0 * V(ql, i);
   }
-  /* (flattening off) CHECK_LR, intvar.F:145-153 */
+  /* flattening, intvar.F:135-140 */
+  if (iflatten != 0) {
+    for (i = i1 - 1; i <= i2 + 1; i++) {
+      V(ql, i) = V(q, i) * V(flatten, i) + V(ql, i) * (1.0 - V(flatten, i));
+      V(qr, i) = V(q, i) * V(flatten, i) + V(qr, i) * (1.0 - V(flatten, i));
+    }
+  }
+  /* CHECK_LR, intvar.F:145-153 */
   for (i = i1 - 1; i <= i2 + 2; i++) {
     V(ql, i) = fmax2(fmin2(V(q, i), V(q, i - 1)), V(ql, i));
     V(ql, i) = fmin2(fmax2(V(q, i), V(q, i - 1)), V(ql, i));
@@ -202,8 +222,98 @@ static void intvar(const double *q, int idim, int i1, int i2,
 }
 
 /* ------------------------------------------------------------------------ */
-/* inteuler.F:5-566 (steepening, flattening, conservative/positive           */
-/* reconstruction and colours off)                                           */
+/* calcdiss.F: the flattening coefficients of one pencil (iflatten 1 or 3;    */
+/* no diffusion).  wflag (eq. A1) :213-224, type 1 (A1-A2) :407-438, type 3  */
+/* (A7-A10) :486-559, both ending with the max of eq. A2.                     */
+/* ------------------------------------------------------------------------ */
+static void calcdiss_flatten(work_t *W, const ora_params *P, const double *dsl,
+                             const double *esl, const double *usl, const double *psl, int i1,
+                             int i2) {
+  const double epsilon = 0.33, kappa1 = 2.0, kappa2 = 0.01, omega1 = 0.75, omega2 = 10.0,
+               sigma1 = 0.5, sigma2 = 1.0;
+  const double gamma = P->gamma;
+  int i;
+  for (i = i1 - 2; i <= i2 + 2; i++) {
+    double qb = fabs(V(psl, i + 1) - V(psl, i - 1)) / fmin2(V(psl, i + 1), V(psl, i - 1));
+    V(W->wflag, i) = (qb > epsilon && V(usl, i - 1) > V(usl, i + 1)) ? 1.0 : 0.0;
+  }
+  if (P->flatten == 1) {
+    for (i = i1 - 1; i <= i2 + 1; i++) {
+      double qa;
+      if (fabs(V(psl, i + 2) - V(psl, i - 2)) / fmin2(V(psl, i + 2), V(psl, i - 2)) < epsilon)
+        qa = 1.0;
+      else
+        qa = (V(psl, i + 1) - V(psl, i - 1)) / (V(psl, i + 2) - V(psl, i - 2));
+      V(W->ftemp, i) = fmin2(1.0, (qa - omega1) * omega2 * V(W->wflag, i));
+      V(W->ftemp, i) = fmax2(0.0, V(W->ftemp, i));
+    }
+  } else {  /* P->flatten == 3 */
+    for (i = i1 - 1; i <= i2 + 1; i++) {
+      const double dp1 = V(psl, i + 1) - V(psl, i - 1);
+      const double dp2 = V(psl, i + 2) - V(psl, i - 2);
+      const double de1 = V(esl, i + 1) - V(esl, i - 1);
+      const double de2 = V(esl, i + 2) - V(esl, i - 2);
+      double dpp = 0.0, dee = 0.0;
+      if (dp2 != 0.0) dpp = dp1 / dp2;
+      if (de2 != 0.0) dee = de1 / de2;
+      const double omega_tilde = fmax2(dpp, dee);
+      const int ism = i + (int)copysign(2.0, dp1); /* post-shock */
+      const int isp = i - (int)copysign(2.0, dp1); /* upstream */
+      double s = -copysign(1.0, dp1);
+      if (dp1 == 0.0) s = 0.0;
+      const double sigma_tilde =
+          V(W->wflag, i) * fabs(dp2) / fmin2(V(psl, i + 2), V(psl, i - 2));
+      const double sigma = fmax2(0.0, (sigma_tilde - sigma1) / (sigma_tilde + sigma2));
+      const double omega = fmax2(0.0, omega2 * (omega_tilde - omega1));
+      const double di2p = 1.0 / V(dsl, i + 2), di2m = 1.0 / V(dsl, i - 2);
+      const double Z = sqrt((fmax2(V(psl, i + 2), V(psl, i - 2)) +
+                             0.5 * (V(psl, i + 2) + V(psl, i - 2)) * (gamma - 1.0)) /
+                            fmax2(di2p, di2m));
+      const double ZE = s * Z / V(dsl, ism) + V(usl, ism) + F_TINY;
+      const double cj2s = sqrt(gamma * V(psl, isp) / V(dsl, isp));
+      const double kappa_tilde = fabs((ZE - V(usl, isp) + s * cj2s) / ZE);
+      const double kappa = fmax2(0.0, (kappa_tilde - kappa1) / (kappa_tilde + kappa2));
+      V(W->ftemp, i) =
+          fmin2(fmin2(kappa, V(W->wflag, i) * omega), V(W->wflag, i) * sigma);
+    }
+  }
+  V(W->ftemp, i1 - 2) = V(W->ftemp, i1 - 1);
+  V(W->ftemp, i2 + 2) = V(W->ftemp, i2 + 1);
+  for (i = i1 - 1; i <= i2 + 1; i++) {
+    if (V(psl, i + 1) - V(psl, i - 1) < 0.0)
+      V(W->flat, i) = fmax2(V(W->ftemp, i), V(W->ftemp, i + 1));
+    else
+      V(W->flat, i) = fmax2(V(W->ftemp, i), V(W->ftemp, i - 1));
+  }
+}
+
+/* inteuler.F:166-193: the density steepening coefficients of one pencil */
+static void steepening(work_t *W, const ora_params *P, const double *dxi, const double *dsl,
+                       const double *psl, int i1, int i2) {
+  int i;
+  for (i = i1 - 2; i <= i2 + 2; i++) {
+    double qa = V(dxi, i - 1) + V(dxi, i) + V(dxi, i + 1);
+    V(W->d2d, i) = (V(dsl, i + 1) - V(dsl, i)) / (V(dxi, i + 1) + V(dxi, i));
+    V(W->d2d, i) = (V(W->d2d, i) - (V(dsl, i) - V(dsl, i - 1)) / (V(dxi, i) + V(dxi, i - 1))) / qa;
+    V(W->dxb, i) = 0.5 * (V(dxi, i) + V(dxi, i + 1));
+  }
+  for (i = i1 - 1; i <= i2 + 1; i++) {
+    double qc = fabs(V(dsl, i + 1) - V(dsl, i - 1)) -
+                0.01 * fmin2(fabs(V(dsl, i + 1)), fabs(V(dsl, i - 1)));
+    const double bm = V(W->dxb, i - 1), b0 = V(W->dxb, i);
+    double s1 = (V(W->d2d, i - 1) - V(W->d2d, i + 1)) * (bm * bm * bm + b0 * b0 * b0) /
+                ((b0 + bm) * (V(dsl, i + 1) - V(dsl, i - 1) + F_TINY));
+    if (V(W->d2d, i + 1) * V(W->d2d, i - 1) > 0.0) s1 = 0.0;
+    if (qc <= 0.0) s1 = 0.0;
+    const double s2 = fmax2(0.0, fmin2(20.0 * (s1 - 0.05), 1.0));
+    const double qa = fabs(V(dsl, i + 1) - V(dsl, i - 1)) / fmin2(V(dsl, i + 1), V(dsl, i - 1));
+    const double qb = fabs(V(psl, i + 1) - V(psl, i - 1)) / fmin2(V(psl, i + 1), V(psl, i - 1));
+    V(W->steep, i) = (P->gamma * 0.1 * qa >= qb) ? s2 : 0.0;
+  }
+}
+
+/* ------------------------------------------------------------------------ */
+/* inteuler.F:5-566 (conservative/positive reconstruction and colours off)   */
 /* ------------------------------------------------------------------------ */
 static void inteuler(work_t *W, const ora_params *P, const double *dxi, int i1, int i2,
                      int j1, int j2) {
@@ -247,20 +357,31 @@ static void inteuler(work_t *W, const ora_params *P, const double *dxi, int i1, 
       V(W->c0, i) = dt * (V(usl, i)) * V(W->dx2i, i);
       V(W->cp, i) = dt * (V(usl, i) + V(W->cs, i)) * V(W->dx2i, i);
     }
-    /* inteuler.F:235-274 */
-    intvar(dsl, idim, i1, i2, W->c1, W->c2, W->c3, W->c4, W->c5, W->c6, W->char1, W->char2,
-           W->c0, W->t1, W->t2, W->t3, W->t4, W->dla, W->dra, W->dl0, W->dr0);
-    intvar(psl, idim, i1, i2, W->c1, W->c2, W->c3, W->c4, W->c5, W->c6, W->char1, W->char2,
-           W->c0, W->dp, W->pl, W->pr, W->p6, W->pla, W->pra, W->pl0, W->pr0);
-    intvar(usl, idim, i1, i2, W->c1, W->c2, W->c3, W->c4, W->c5, W->c6, W->char1, W->char2,
-           W->c0, W->du, W->ul, W->ur, W->u6, W->ula, W->ura, W->ul0, W->ur0);
-    intvar(vsl, idim, i1, i2, W->c1, W->c2, W->c3, W->c4, W->c5, W->c6, W->char1, W->char2,
-           W->c0, W->dv, W->vl, W->vr, W->v6, W->vla, W->vra, W->vl0, W->vr0);
-    intvar(wsl, idim, i1, i2, W->c1, W->c2, W->c3, W->c4, W->c5, W->c6, W->char1, W->char2,
-           W->c0, W->dw, W->wl, W->wr, W->w6, W->wla, W->wra, W->wl0, W->wr0);
+    /* the pencil's flattening (calcdiss, called by the sweep before inteuler) and
+       steepening coefficients */
+    if (P->flatten != 0) calcdiss_flatten(W, P, dsl, &S(W->e, 1, j), usl, psl, i1, i2);
+    if (P->steepen != 0) steepening(W, P, dxi, dsl, psl, i1, i2);
+    const int ist = P->steepen, ifl = P->flatten;
+    /* inteuler.F:235-274 (steepening applies to the density only) */
+    intvar(dsl, idim, i1, i2, ist, W->steep, ifl, W->flat, W->c1, W->c2, W->c3, W->c4, W->c5,
+           W->c6, W->char1, W->char2, W->c0, W->t1, W->t2, W->t3, W->t4, W->dla, W->dra,
+           W->dl0, W->dr0);
+    intvar(psl, idim, i1, i2, 0, W->steep, ifl, W->flat, W->c1, W->c2, W->c3, W->c4, W->c5,
+           W->c6, W->char1, W->char2, W->c0, W->dp, W->pl, W->pr, W->p6, W->pla, W->pra,
+           W->pl0, W->pr0);
+    intvar(usl, idim, i1, i2, 0, W->steep, ifl, W->flat, W->c1, W->c2, W->c3, W->c4, W->c5,
+           W->c6, W->char1, W->char2, W->c0, W->du, W->ul, W->ur, W->u6, W->ula, W->ura,
+           W->ul0, W->ur0);
+    intvar(vsl, idim, i1, i2, 0, W->steep, ifl, W->flat, W->c1, W->c2, W->c3, W->c4, W->c5,
+           W->c6, W->char1, W->char2, W->c0, W->dv, W->vl, W->vr, W->v6, W->vla, W->vra,
+           W->vl0, W->vr0);
+    intvar(wsl, idim, i1, i2, 0, W->steep, ifl, W->flat, W->c1, W->c2, W->c3, W->c4, W->c5,
+           W->c6, W->char1, W->char2, W->c0, W->dw, W->wl, W->wr, W->w6, W->wla, W->wra,
+           W->wl0, W->wr0);
     if (P->dual == 1)
-      intvar(gesl, idim, i1, i2, W->c1, W->c2, W->c3, W->c4, W->c5, W->c6, W->char1, W->char2,
-             W->c0, W->dge, W->gel, W->ger, W->ge6, W->gela, W->gera, W->gel0, W->ger0);
+      intvar(gesl, idim, i1, i2, 0, W->steep, ifl, W->flat, W->c1, W->c2, W->c3, W->c4, W->c5,
+             W->c6, W->char1, W->char2, W->c0, W->dge, W->gel, W->ger, W->ge6, W->gela,
+             W->gera, W->gel0, W->ger0);
     /* characteristic domain-of-dependence averages, inteuler.F:304-316 */
     for (i = i1; i <= i2 + 1; i++) {
       V(W->plm, i) = V(W->pr, i - 1) - V(W->cm, i - 1) * (V(W->dp, i - 1) - (1.0 - ft * V(W->cm, i - 1)) * V(W->p6, i - 1));

@@ -18,6 +18,7 @@
  *   pgas2d_dual                src/enzo/pgas2d_dual.F:4-122
  *   grid::ComputePressure      src/enzo/Grid_ComputePressure.C:36-164
  *   calc_dt (PPM branch)       src/enzo/calc_dt.F:6-181
+ *   calcdiss (flattening 1, 3) src/enzo/calcdiss.F:213-224, 407-438, 486-559
  *
  * Parity anchors: the reference's analytic shock-tube answer tests
  * (run/Hydro/Hydro-1D/{SodShockTube,Toro-*}) at the reference's own
@@ -51,6 +52,8 @@ typedef struct {
   int pressure_free;   /* PressureFree */
   int fallback;        /* RiemannSolverFallback */
   int max_velocity_index; /* MaxVelocityIndex used by ComputePressure */
+  int steepen;         /* PPMSteepeningParameter (0 or 1: density steepening) */
+  int flatten;         /* PPMFlatteningParameter (0, 1 or 3) */
 } ora_params;
 
 /* struct fluxes (src/enzo/Fluxes.h:29-37), restricted to the six hydro slots */
