@@ -285,8 +285,12 @@ void build_coef(const double* dxi_in, int n, int is0, int ie0, std::vector<Coef>
 
 int check_supported(const ppm_b200_params* p) {
   if (!p) return PPM_B200_ERR_INVALID;
-  if (p->pressure_free || p->steepening || p->flattening || p->diffusion ||
-      p->conservative_rec || p->positive_rec || p->eos_type != 0 || p->number_of_colours != 0)
+  if (p->pressure_free || p->diffusion || p->conservative_rec || p->positive_rec ||
+      p->eos_type != 0 || p->number_of_colours != 0)
+    return PPM_B200_ERR_UNSUPPORTED;
+  // slope corrections: calcdiss's flattening types 1 and 3, inteuler's steepening
+  if ((p->flattening != 0 && p->flattening != 1 && p->flattening != 3) ||
+      (p->steepening != 0 && p->steepening != 1))
     return PPM_B200_ERR_UNSUPPORTED;
   if (p->riemann_solver != PPM_B200_RIEMANN_TWOSHOCK) return PPM_B200_ERR_UNSUPPORTED;
   if (p->reconstruction != PPM_B200_RECONSTRUCTION_PPM) return PPM_B200_ERR_UNSUPPORTED;
@@ -540,13 +544,19 @@ int reserve_captures(ppm_b200_context* ctx, SweepPlan* plans, int n) {
 // Face scratch of one directional sweep of a batch: 19 planes of (active cells along
 // the sweep + 1) x pencils per grid, then one flagged-pencil slot per pencil.  The
 // size differs between directions for non-cubic grids.
-size_t sweep_scratch_bytes(int dim, const std::vector<GridIO>& io) {
+// planes of slope-correction coefficients a grid's sweep needs (cells is-1 .. ie+1)
+size_t correction_planes(const ppm_b200_params* p) {
+  return (p->flattening ? 1 : 0) + (p->steepening ? 1 : 0);
+}
+
+size_t sweep_scratch_bytes(int dim, const std::vector<GridIO>& io, const ppm_b200_params* p) {
   size_t doubles = 0, pencils = 0;
   for (const auto& x : io) {
     const ppm_b200_grid* g = x.g;
     const size_t np = (size_t)grid_size(g) / (size_t)g->dims[dim];
     doubles += (size_t)(ppm::kFaceVars + ppm::kFluxVars) *
                (size_t)(g->end[dim] - g->start[dim] + 2) * np;
+    doubles += correction_planes(p) * (size_t)(g->end[dim] - g->start[dim] + 3) * np;
     pencils += np;
   }
   return doubles * sizeof(double) + pencils * sizeof(int64_t);
@@ -613,6 +623,7 @@ int prepare_sweep(ppm_b200_context* ctx, int dim, int position, const ppm_b200_p
     a.npencils = (int64_t)a.n1 * a.n2;
     a.plane = (int64_t)(a.ie - a.is + 2) * a.npencils;
     scratch_doubles += (size_t)(ppm::kFaceVars + ppm::kFluxVars) * (size_t)a.plane;
+    scratch_doubles += correction_planes(p) * (size_t)(a.ie - a.is + 3) * (size_t)a.npencils;
     total_pencils += a.npencils;
     const int64_t mb = (a.npencils + ppm::kMarchThreads - 1) / ppm::kMarchThreads;
     const int64_t rb = (int64_t)(a.ie - a.is + 2) *
@@ -668,6 +679,17 @@ int prepare_sweep(ppm_b200_context* ctx, int dim, int position, const ppm_b200_p
     a.fstate = scratch + at;
     a.fflux = a.fstate + (size_t)ppm::kFaceVars * (size_t)a.plane;
     at += (size_t)(ppm::kFaceVars + ppm::kFluxVars) * (size_t)a.plane;
+    a.flatten = p->flattening;
+    a.steepen = p->steepening;
+    const size_t cplane = (size_t)(a.ie - a.is + 3) * (size_t)a.npencils;
+    if (p->flattening) {
+      a.flat = scratch + at;
+      at += cplane;
+    }
+    if (p->steepening) {
+      a.steep = scratch + at;
+      at += cplane;
+    }
     a.dim = dim;
     a.rank = g->rank;
     if (cfl) {
@@ -716,6 +738,7 @@ int prepare_sweep(ppm_b200_context* ctx, int dim, int position, const ppm_b200_p
   if (ng == 1) plan.B.one = rec[0];
   plan.B.x_tma = 0;
   if (ng == 1 && dim == 0) set_x_tiles(plan.B, rec[0]);
+  plan.B.corrections = correction_planes(p) > 0 ? 1 : 0;
   plan.B.grids = (const SweepArgs*)base;
   plan.B.ngrids = ng;
   plan.B.march_prefix = (const int64_t*)(base + off_m);
@@ -1024,7 +1047,7 @@ int prepare_solve(ppm_b200_context* ctx, const ppm_b200_params* p, int cycle,
   // sweep records its pointers
   size_t scratch = 0;
   for (int s = 0; s < sp.nsweeps; ++s)
-    scratch = std::max(scratch, sweep_scratch_bytes(sp.order[s], io));
+    scratch = std::max(scratch, sweep_scratch_bytes(sp.order[s], io, p));
   rc = ensure(ctx, ctx->face_scratch, scratch);
   if (rc) return rc;
   const void* scratch_base = ctx->face_scratch.p;
@@ -1112,6 +1135,7 @@ std::string graph_key(ppm_b200_context* ctx, const ppm_b200_params* p, const Sol
     key_put(k, sp.sweep[s].riemann_blocks);
     key_put(k, sp.sweep[s].contiguous);
     key_put(k, b.x_tma);
+    key_put(k, b.corrections);
     key_put(k, ctx->mirror[kSlotSweep0 + 3 * sp.order[s] + s].version);
   }
   return k;

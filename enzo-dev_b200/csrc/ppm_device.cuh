@@ -61,12 +61,102 @@ __device__ __forceinline__ double pm_edge(double qm, double q0, double dqm, doub
   return c3 * qm + c4 * q0 + c5 * dqm + c6 * dq0;
 }
 
-// ------------------------------------------- intvar.F:117-160 (no steepening/flattening)
+// ------------------------------------------------ calcdiss.F: flattening coefficients
+// Per cell j of a pencil, from the cells j-2 .. j+2 (index 2 = cell j); the sweep's
+// pressure, velocity, density and total energy.
+constexpr double kCdEpsilon = 0.33, kCdKappa1 = 2.0, kCdKappa2 = 0.01, kCdOmega1 = 0.75,
+                 kCdOmega2 = 10.0, kCdSigma1 = 0.5, kCdSigma2 = 1.0;  // calcdiss.F:143-149
+
+// eq. A1, calcdiss.F:213-224: a shock at j (pressure jump above epsilon, compression)
+__device__ __forceinline__ double cd_wflag(double pm1, double pp1, double um1, double up1) {
+  const double qb = fabs(pp1 - pm1) / dmin(pp1, pm1);
+  return (qb > kCdEpsilon && um1 > up1) ? 1.0 : 0.0;
+}
+
+// type 1, calcdiss.F:409-424 (before the max of eq. A2)
+__device__ __forceinline__ double cd_ftemp1(const double p[5], double wflag) {
+  double qa;
+  if (fabs(p[4] - p[0]) / dmin(p[4], p[0]) < kCdEpsilon)
+    qa = 1.0;
+  else
+    qa = (p[3] - p[1]) / (p[4] - p[0]);
+  const double f = dmin(1.0, (qa - kCdOmega1) * kCdOmega2 * wflag);
+  return dmax(0.0, f);
+}
+
+// type 3, calcdiss.F:486-555 (before the max of eq. A2): d, e, u, p at j-2 .. j+2
+__device__ __forceinline__ double cd_ftemp3(const double d[5], const double e[5],
+                                            const double u[5], const double p[5], double wflag,
+                                            double gamma) {
+  const double dp1 = p[3] - p[1];
+  const double dp2 = p[4] - p[0];
+  const double de1 = e[3] - e[1];
+  const double de2 = e[4] - e[0];
+  double dpp = 0.0, dee = 0.0;
+  if (dp2 != 0.0) dpp = dp1 / dp2;
+  if (de2 != 0.0) dee = de1 / de2;
+  const double omega_tilde = dmax(dpp, dee);
+  // ism = j + sign(2, dp1) (post-shock), isp = j - sign(2, dp1) (upstream)
+  const bool neg = signbit(dp1);
+  const double d_ism = neg ? d[0] : d[4], u_ism = neg ? u[0] : u[4];
+  const double d_isp = neg ? d[4] : d[0], u_isp = neg ? u[4] : u[0], p_isp = neg ? p[4] : p[0];
+  double s = -copysign(1.0, dp1);
+  if (dp1 == 0.0) s = 0.0;
+  const double sigma_tilde = wflag * fabs(dp2) / dmin(p[4], p[0]);
+  const double sigma = dmax(0.0, (sigma_tilde - kCdSigma1) / (sigma_tilde + kCdSigma2));
+  const double omega = dmax(0.0, kCdOmega2 * (omega_tilde - kCdOmega1));
+  const double di2p = 1.0 / d[4], di2m = 1.0 / d[0];
+  const double Z = sqrt((dmax(p[4], p[0]) + 0.5 * (p[4] + p[0]) * (gamma - 1.0)) /
+                        dmax(di2p, di2m));
+  const double ZE = s * Z / d_ism + u_ism + kTiny;
+  const double cj2s = sqrt(gamma * p_isp / d_isp);
+  const double kappa_tilde = fabs((ZE - u_isp + s * cj2s) / ZE);
+  const double kappa = dmax(0.0, (kappa_tilde - kCdKappa1) / (kappa_tilde + kCdKappa2));
+  return dmin(dmin(kappa, wflag * omega), wflag * sigma);
+}
+
+// inteuler.F:166-193: the density steepening coefficient of cell j from d and the cell
+// widths at j-2 .. j+2 (index 2 = cell j) and p at j-1, j+1
+__device__ __forceinline__ double st_d2d(const double* d, const double* dx) {
+  // d2d of the middle one of three consecutive cells
+  const double qa = dx[0] + dx[1] + dx[2];
+  double r = (d[2] - d[1]) / (dx[2] + dx[1]);
+  r = (r - (d[1] - d[0]) / (dx[1] + dx[0])) / qa;
+  return r;
+}
+__device__ __forceinline__ double steepen_coef(const double d[5], const double dx[5], double pm1,
+                                               double pp1, double gamma) {
+  const double d2m = st_d2d(d, dx);          // d2d(j-1)
+  const double d2p = st_d2d(d + 2, dx + 2);  // d2d(j+1)
+  const double bm = 0.5 * (dx[1] + dx[2]);   // dxb(j-1)
+  const double b0 = 0.5 * (dx[2] + dx[3]);   // dxb(j)
+  const double qc = fabs(d[3] - d[1]) - 0.01 * dmin(fabs(d[3]), fabs(d[1]));
+  double s1 = (d2m - d2p) * (bm * bm * bm + b0 * b0 * b0) / ((b0 + bm) * (d[3] - d[1] + kTiny));
+  if (d2p * d2m > 0.0) s1 = 0.0;
+  if (qc <= 0.0) s1 = 0.0;
+  const double s2 = dmax(0.0, dmin(20.0 * (s1 - 0.05), 1.0));
+  const double qa = fabs(d[3] - d[1]) / dmin(d[3], d[1]);
+  const double qb = fabs(pp1 - pm1) / dmin(pp1, pm1);
+  return (gamma * 0.1 * qa >= qb) ? s2 : 0.0;
+}
+
+// ---------------------------------------------------------------- intvar.F:106-160
+// The parabola of one cell from its edge values.  STEEP (density only): steepening
+// toward the neighbours' linear profiles with coefficient st (intvar.F:106-113; dqm, dqp:
+// the neighbours' slopes); FLAT: flattening toward the cell value with coefficient fl
+// (intvar.F:135-140).  Without them this is the plain PPM parabola.
 struct Para {
   double ql, qr, q6, dq;
 };
 
-__device__ __forceinline__ Para pm_parabola(double qm, double q0, double qp, double ql, double qr) {
+template <bool STEEP = false, bool FLAT = false>
+__device__ __forceinline__ Para pm_parabola(double qm, double q0, double qp, double ql, double qr,
+                                            double st = 0.0, double dqm = 0.0,
+                                            double dqp = 0.0, double fl = 0.0) {
+  if (STEEP) {
+    ql = (1.0 - st) * ql + st * (qm + 0.5 * dqm);
+    qr = (1.0 - st) * qr + st * (qp - 0.5 * dqp);
+  }
   double temp1 = (qr - q0) * (q0 - ql);
   double temp2 = qr - ql;
   double temp3 = 6.0 * (q0 - 0.5 * (qr + ql));
@@ -78,6 +168,10 @@ __device__ __forceinline__ Para pm_parabola(double qm, double q0, double qp, dou
   double temp23 = temp2 * temp3;
   if (temp22 < temp23) ql = 3.0 * q0 - 2.0 * qr;
   if (temp22 < -temp23) qr = 3.0 * q0 - 2.0 * ql;
+  if (FLAT) {
+    ql = q0 * fl + ql * (1.0 - fl);
+    qr = q0 * fl + qr * (1.0 - fl);
+  }
   // CHECK_LR, intvar.F:145-153
   ql = dmax(dmin(q0, qm), ql);
   ql = dmin(dmax(q0, qm), ql);

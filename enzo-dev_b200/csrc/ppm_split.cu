@@ -77,6 +77,66 @@ __device__ __forceinline__ Phys make_phys(const SweepArgs& a) {
   return P;
 }
 
+// ------------------------------------------------------------------ stage 0 (optional)
+// Slope-correction coefficients of every cell is-1 .. ie+1 of a pencil: calcdiss's
+// flattening (calcdiss.F:213-224 with type 1 :407-438 or type 3 :486-564) from the
+// sweep's pressure, velocity, density and total energy, and inteuler's density
+// steepening (inteuler.F:166-193).  Thread per pencil, marching; the flattening's
+// flattemp values are computed once each and kept for the max of eq. A2.
+template <bool ONE>
+__global__ void __launch_bounds__(kMarchThreads) corrections_kernel(const __grid_constant__ BatchArgs B) {
+  int64_t lb;
+  const int g = locate<ONE>(B.march_prefix, B.ngrids, lb);
+  PPM_BIND_RECORD(a, g)
+  const int64_t pid = lb * kMarchThreads + threadIdx.x;
+  if (pid >= a.npencils) return;
+  const int64_t base = (pid % a.n1) * a.s1 + (pid / a.n1) * a.s2;
+  const int64_t sa = a.sa, np = a.npencils;
+  const int is = a.is, ie = a.ie;
+  const double gamma = a.gamma;
+  auto ld = [&](const double* f, int i) { return __ldg(f + base + (int64_t)i * sa); };
+  // flattemp of cell j, j clamped to is-1 .. ie+1 (calcdiss.F:427-428, 563-564)
+  auto ftemp = [&](int j) {
+    j = j < is - 1 ? is - 1 : (j > ie + 1 ? ie + 1 : j);
+    double p[5];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) p[k] = ld(a.pres, j - 2 + k);
+    const double wf = cd_wflag(p[1], p[3], ld(a.in_u, j - 1), ld(a.in_u, j + 1));
+    if (a.flatten == 1) return cd_ftemp1(p, wf);
+    double d[5], e[5], u[5];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+      d[k] = ld(a.in_d, j - 2 + k);
+      e[k] = ld(a.in_e, j - 2 + k);
+      u[k] = ld(a.in_u, j - 2 + k);
+    }
+    return cd_ftemp3(d, e, u, p, wf, gamma);
+  };
+  double fm = 0.0, f0 = 0.0;
+  if (a.flatten) {
+    fm = ftemp(is - 2);
+    f0 = ftemp(is - 1);
+  }
+  for (int c = is - 1; c <= ie + 1; ++c) {
+    const int64_t o = (int64_t)(c - (is - 1)) * np + pid;
+    if (a.flatten) {  // eq. A2: the max with the neighbour on the high-pressure side
+      const double fp = ftemp(c + 1);
+      a.flat[o] = (ld(a.pres, c + 1) - ld(a.pres, c - 1) < 0.0) ? dmax(f0, fp) : dmax(f0, fm);
+      fm = f0;
+      f0 = fp;
+    }
+    if (a.steepen) {
+      double d[5], dx[5];
+#pragma unroll
+      for (int k = 0; k < 5; ++k) {
+        d[k] = ld(a.in_d, c - 2 + k);
+        dx[k] = a.coef[c - 2 + k].dx;
+      }
+      a.steep[o] = steepen_coef(d, dx, ld(a.pres, c - 1), ld(a.pres, c + 1), gamma);
+    }
+  }
+}
+
 // ------------------------------------------------------------------ stage 1
 // Two roles march the same pencil independently: ROLE 0 reconstructs density,
 // pressure and normal velocity and applies inteuler's characteristic corrections,
@@ -91,7 +151,8 @@ __device__ __forceinline__ Phys make_phys(const SweepArgs& a) {
 #ifndef PPM_RECON0_MINBLOCKS
 #define PPM_RECON0_MINBLOCKS PPM_RECON_MINBLOCKS
 #endif
-template <bool DUAL, bool GRAV, int ROLE, bool ONE>
+// COR: the batch carries slope corrections (the coefficients of the corrections kernel).
+template <bool DUAL, bool GRAV, int ROLE, bool ONE, bool COR = false>
 __global__ void __launch_bounds__(kMarchThreads,
                                   ROLE == 0 ? PPM_RECON0_MINBLOCKS : PPM_RECON_MINBLOCKS)
     reconstruct_kernel(const __grid_constant__ BatchArgs B) {
@@ -113,6 +174,7 @@ __global__ void __launch_bounds__(kMarchThreads,
 
   double wq0[3], wq1[3], wq2[3];  // cells t-3, t-2, t-1
   double dqm1[3], qlm1[3];        // dq(t-2), ql(t-2)
+  double dqm2 = 0.0;              // dq(t-3) of the density (COR, steepening)
 #pragma unroll
   for (int v = 0; v < 3; ++v) wq0[v] = wq1[v] = wq2[v] = dqm1[v] = qlm1[v] = 0.0;
   double wu0 = 0.0, wu1 = 0.0, wu2 = 0.0;  // normal velocity of cells t-3, t-2, t-1
@@ -164,8 +226,29 @@ __global__ void __launch_bounds__(kMarchThreads,
         Para pa[3];
 #pragma unroll
         for (int v = 0; v < 3; ++v) pa[v] = Para{0.0, 0.0, 0.0, 0.0};
+        if (COR) {
+          const int64_t co = (int64_t)(c - (is - 1)) * np + pid;
+          const bool fl_on = a.flatten != 0, st_on = ROLE == 0 && a.steepen != 0;
+          const double fl = fl_on ? a.flat[co] : 0.0;
 #pragma unroll
-        for (int v = 0; v < NV; ++v) pa[v] = pm_parabola(wq0[v], wq1[v], wq2[v], qlm1[v], qlN[v]);
+          for (int v = 0; v < NV; ++v) {
+            if (v == 0 && st_on) {
+              const double st = a.steep[co];
+              pa[v] = fl_on ? pm_parabola<true, true>(wq0[v], wq1[v], wq2[v], qlm1[v], qlN[v],
+                                                      st, dqm2, dqN[v], fl)
+                            : pm_parabola<true, false>(wq0[v], wq1[v], wq2[v], qlm1[v],
+                                                       qlN[v], st, dqm2, dqN[v]);
+            } else if (fl_on) {
+              pa[v] = pm_parabola<false, true>(wq0[v], wq1[v], wq2[v], qlm1[v], qlN[v], 0.0,
+                                               0.0, 0.0, fl);
+            } else {
+              pa[v] = pm_parabola(wq0[v], wq1[v], wq2[v], qlm1[v], qlN[v]);
+            }
+          }
+        } else {
+#pragma unroll
+          for (int v = 0; v < NV; ++v) pa[v] = pm_parabola(wq0[v], wq1[v], wq2[v], qlm1[v], qlN[v]);
+        }
         double* o = a.fstate + (int64_t)(c - is) * np + pid;
         if (ROLE == 0) {
           if (c >= is) {
@@ -236,6 +319,7 @@ __global__ void __launch_bounds__(kMarchThreads,
         }
       }
     }
+    if (COR) dqm2 = dqm1[0];
 #pragma unroll
     for (int v = 0; v < 3; ++v) {
       wq0[v] = wq1[v];
@@ -1171,9 +1255,16 @@ void launch_stages(const BatchArgs& B, int64_t march_blocks, int64_t riemann_blo
   };
   mark(0);
   cudaMemsetAsync(B.counters + kCntFlagged, 0, sizeof(unsigned long long), st);
-  reconstruct_kernel<DUAL, GRAV, 0, ONE><<<(unsigned)march_blocks, kMarchThreads, 0, st>>>(B);
-  mark(1);
-  reconstruct_kernel<DUAL, GRAV, 1, ONE><<<(unsigned)march_blocks, kMarchThreads, 0, st>>>(B);
+  if (B.corrections) {
+    corrections_kernel<ONE><<<(unsigned)march_blocks, kMarchThreads, 0, st>>>(B);
+    reconstruct_kernel<DUAL, GRAV, 0, ONE, true><<<(unsigned)march_blocks, kMarchThreads, 0, st>>>(B);
+    mark(1);
+    reconstruct_kernel<DUAL, GRAV, 1, ONE, true><<<(unsigned)march_blocks, kMarchThreads, 0, st>>>(B);
+  } else {
+    reconstruct_kernel<DUAL, GRAV, 0, ONE><<<(unsigned)march_blocks, kMarchThreads, 0, st>>>(B);
+    mark(1);
+    reconstruct_kernel<DUAL, GRAV, 1, ONE><<<(unsigned)march_blocks, kMarchThreads, 0, st>>>(B);
+  }
   mark(2);
   if (learned)
     riemann_kernel<DUAL, ONE, true><<<(unsigned)riemann_blocks, kRiemannThreads, 0, st>>>(B);

@@ -90,6 +90,12 @@ struct SweepArgs {
   int dim, rank;                     // the sweep axis and GridRank
   int ts1, te1, ts2, te2;            // active ranges along the t1 and t2 axes
   double aye, vg[3], min_support;    // calc_dt's a, grid velocity, ComputePressure's floor
+  // slope corrections: calcdiss's flattening (type 1 or 3) of every variable and
+  // inteuler's steepening of the density, as per-cell coefficients of cells is-1 .. ie+1
+  // in planes [cell - (is-1)][pencil], written by the corrections kernel; null when off
+  double* flat;
+  double* steep;
+  int flatten, steepen;              // PPMFlatteningParameter, PPMSteepeningParameter
 };
 
 enum { kFaceVars = 12, kFluxVars = 7 };
@@ -120,6 +126,7 @@ struct BatchArgs {
   const int64_t* riemann_prefix;     // ngrids + 1
   unsigned long long* counters;      // kMaxCounters, shared by the batch
   int64_t* flagged;                  // pencils needing the fallback pass: (grid << 40) | pencil
+  int corrections = 0;               // the batch's grids carry flattening / steepening
   // x sweep of a single grid: the update kernel reads its input cells as TMA tiles of
   // kXTileRows pencils x kXTileCells cells, through 2-D tensor maps (cells x pencils) of
   // d, e, u, v, w, ge (absent fields: unused).  x_tma = 0: plain loads.

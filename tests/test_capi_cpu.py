@@ -39,15 +39,17 @@ def test_version_and_error_strings():
 
 
 def test_unsupported_configuration_is_rejected_before_any_device_work():
-    # PPMFlatteningParameter != 0 is outside this library: the caller keeps the Fortran path.
+    # Options outside this library (flattening type 2, diffusion, steepening other than
+    # 0/1): the caller keeps the Fortran path.  The context pointer is never touched.
     L = capi.lib()
     from ppm_b200 import harness as H
-    import numpy as np
     g = H.Grid.uniform((8, 8, 8))
     hp = H.HydroParams()
     f = H.new_fields(g, False)
-    P = capi.make_params(hp, 0.1)
-    P.flattening = 3
-    G, keep = capi.make_grid(g, f)
-    rc = L.ppm_b200_solve_ppm_de(C.c_void_p(1), C.byref(P), 0, C.byref(G), 0, 0, None, None, None)
-    assert rc == capi.ERR_UNSUPPORTED
+    for field, value in (("flattening", 2), ("diffusion", 1), ("steepening", 2)):
+        P = capi.make_params(hp, 0.1)
+        setattr(P, field, value)
+        G, keep = capi.make_grid(g, f)
+        rc = L.ppm_b200_solve_ppm_de(C.c_void_p(1), C.byref(P), 0, C.byref(G), 0, 0, None, None,
+                                     None)
+        assert rc == capi.ERR_UNSUPPORTED, field
