@@ -74,6 +74,13 @@ void launch_pressure_batch(const ElemBatch& B, int64_t blocks, cudaStream_t st);
 void launch_timestep_batch(const ElemBatch& B, int64_t blocks, double courant, double* dt_out,
                            cudaStream_t st);
 void launch_boundary_batch(const ElemBatch& B, int64_t blocks, cudaStream_t st);
+struct CopyBox {
+  int dst, src;
+  int d0[3], s0[3], ext[3];
+  int pad;
+};
+void launch_copy_zones(const ElemGrid* grids, const CopyBox* boxes, const int64_t* prefix,
+                       int nboxes, int64_t blocks, cudaStream_t st);
 }  // namespace ppm
 
 using ppm::BatchArgs;
@@ -115,7 +122,9 @@ enum {
   kSlotBoundary = 15,  // element records of the ghost-fill kernel
   kSlotExpansion = 16, // element records of the comoving-expansion kernel
   kSlotCflCw = 17,     // cell widths read by the time step folded into the last sweep
-  kSlotCount = 18
+  kSlotCopy = 18,      // element records of the sibling-zone copy
+  kSlotCopyBoxes = 19, // its boxes and block prefix
+  kSlotCount = 20
 };
 // captured level graphs kept at most (a changed grid list leaves the old ones unused)
 constexpr size_t kMaxGraphs = 16;
@@ -1563,6 +1572,101 @@ static int boundary_batch(ppm_b200_context* ctx, ppm_b200_grid* grids, int ngrid
   return PPM_B200_OK;
 }
 
+// The boxes of Grid_CopyZonesFromGrid.C:100-160 over a level, from integer positions:
+// grid a's whole region (ghosts included) against grid b's active region shifted by
+// every periodic image (shift 0 of a itself excluded).
+static void copy_boxes(const ppm_b200_grid* grids, int ngrids, const long long* left,
+                       const long long domain[3], const int periodic[3],
+                       std::vector<ppm::CopyBox>& boxes) {
+  const int rank = grids[0].rank;
+  int span[3];
+  for (int d = 0; d < 3; ++d) span[d] = (d < rank && periodic[d]) ? 1 : 0;
+  for (int a = 0; a < ngrids; ++a)
+    for (int b = 0; b < ngrids; ++b)
+      for (int sz = -span[2]; sz <= span[2]; ++sz)
+        for (int sy = -span[1]; sy <= span[1]; ++sy)
+          for (int sx = -span[0]; sx <= span[0]; ++sx) {
+            const int sh[3] = {sx, sy, sz};
+            if (a == b && sx == 0 && sy == 0 && sz == 0) continue;
+            ppm::CopyBox x{};
+            x.dst = a;
+            x.src = b;
+            bool empty = false;
+            for (int d = 0; d < 3 && !empty; ++d) {
+              if (d >= rank) {
+                x.d0[d] = x.s0[d] = 0;
+                x.ext[d] = 1;
+                continue;
+              }
+              const long long off = (long long)sh[d] * domain[d];
+              const long long la = left[3 * a + d], lb = left[3 * b + d];
+              const long long lo = std::max(la, lb + grids[b].start[d] + off);
+              const long long hi = std::min(la + grids[a].dims[d] - 1, lb + grids[b].end[d] + off);
+              if (hi < lo) {
+                empty = true;
+                break;
+              }
+              x.d0[d] = (int)(lo - la);
+              x.s0[d] = (int)(lo - off - lb);
+              x.ext[d] = (int)(hi - lo + 1);
+            }
+            if (!empty) boxes.push_back(x);
+          }
+}
+
+static int copy_zones_level(ppm_b200_context* ctx, ppm_b200_grid* grids, int ngrids,
+                            const long long* left, const long long domain[3],
+                            const int periodic[3], int dual_energy) {
+  if (!ctx || ngrids < 0 || (ngrids > 0 && (!grids || !left)) || !domain || !periodic)
+    return PPM_B200_ERR_INVALID;
+  if (ngrids == 0) return PPM_B200_OK;
+  const int rank = grids[0].rank;
+  for (int k = 0; k < ngrids; ++k) {
+    ppm_b200_grid* g = &grids[k];
+    if (g->rank != rank || !g->density || !g->total_energy || !g->velocity[0])
+      return PPM_B200_ERR_INVALID;
+    for (int d = 1; d < g->rank; ++d)
+      if (!g->velocity[d]) return PPM_B200_ERR_INVALID;
+    if (dual_energy && !g->gas_energy) return PPM_B200_ERR_INVALID;
+  }
+  for (int d = 0; d < rank; ++d)
+    if (domain[d] <= 0) return PPM_B200_ERR_INVALID;
+  std::vector<ppm::CopyBox> boxes;
+  copy_boxes(grids, ngrids, left, domain, periodic, boxes);
+  if (boxes.empty()) return PPM_B200_OK;
+  CK(cudaSetDevice(ctx->device));
+  ppm_b200_params p;
+  std::memset(&p, 0, sizeof(p));
+  p.dual_energy = dual_energy;
+  std::vector<GridIO> io(ngrids);
+  for (int k = 0; k < ngrids; ++k) {
+    io[k].g = &grids[k];
+    int rc = stage_in(ctx, &p, &grids[k], PPM_B200_MEM_DEVICE, io[k].user, io[k].acc);
+    if (rc) return rc;
+  }
+  ElemPlan ep;
+  int rc = prepare_elem(ctx, kSlotCopy, &p, io, false, nullptr, ep);
+  if (rc) return rc;
+  std::vector<int64_t> pre(boxes.size() + 1, 0);
+  for (size_t b = 0; b < boxes.size(); ++b) {
+    const int64_t cells = (int64_t)boxes[b].ext[0] * boxes[b].ext[1] * boxes[b].ext[2];
+    pre[b + 1] = pre[b] + (cells + 255) / 256;
+  }
+  std::vector<unsigned char> img;
+  append(img, boxes.data(), boxes.size());
+  const size_t off_p = align256(img.size());
+  img.resize(off_p);
+  append(img, pre.data(), pre.size());
+  rc = mirror_put(ctx, ctx->mirror[kSlotCopyBoxes], img);
+  if (rc) return rc;
+  const unsigned char* base = (const unsigned char*)ctx->mirror[kSlotCopyBoxes].dev.p;
+  ppm::launch_copy_zones(ep.B.grids, (const ppm::CopyBox*)base, (const int64_t*)(base + off_p),
+                         (int)boxes.size(), pre.back(), ctx->stream);
+  ctx->launches += 1;
+  CK(cudaGetLastError());
+  return PPM_B200_OK;
+}
+
 // Old fields of a grid on the device: device pointers as given, or copies of host arrays.
 static int stage_old(ppm_b200_context* ctx, const ppm_b200_params* p, const ppm_b200_grid* g,
                      const ppm_b200_grid* old, int memory, FieldSet& fs) {
@@ -1781,6 +1885,12 @@ int ppm_b200_set_boundary(ppm_b200_context* ctx, ppm_b200_grid* g, int dual_ener
 int ppm_b200_set_boundary_level(ppm_b200_context* ctx, ppm_b200_grid* grids, int ngrids,
                                 int dual_energy, const int bc_type[3]) {
   return boundary_batch(ctx, grids, ngrids, dual_energy, bc_type);
+}
+
+int ppm_b200_copy_zones_level(ppm_b200_context* ctx, ppm_b200_grid* grids, int ngrids,
+                              const long long* left, const long long domain[3],
+                              const int periodic[3], int dual_energy) {
+  return copy_zones_level(ctx, grids, ngrids, left, domain, periodic, dual_energy);
 }
 
 }  // extern "C"

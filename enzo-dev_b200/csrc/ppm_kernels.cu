@@ -188,6 +188,45 @@ __global__ void __launch_bounds__(256) boundary_kernel(const __grid_constant__ E
   }
 }
 
+// ------------------------------------------------------------------ sibling zones
+// Grid_CopyZonesFromGrid.C:100-300 (the copy3drel of every field) for a list of boxes: box
+// b copies ext[0] x ext[1] x ext[2] zones of grid src, starting at s0, into grid dst at
+// d0.  Blocks of 256 zones; box b owns blocks [prefix[b], prefix[b+1]).  The boxes read
+// active zones and write zones outside every active region, so they never race.
+struct CopyBox {
+  int dst, src;
+  int d0[3], s0[3], ext[3];
+  int pad;
+};
+
+__global__ void __launch_bounds__(256) copy_zones_kernel(const ElemGrid* __restrict__ grids,
+                                                         const CopyBox* __restrict__ boxes,
+                                                         const int64_t* __restrict__ prefix,
+                                                         int nboxes) {
+  int64_t lb;
+  const CopyBox& X = boxes[batch_locate(prefix, nboxes, blockIdx.x, lb)];
+  const int64_t c = lb * 256 + threadIdx.x;
+  const int64_t e0 = X.ext[0], e01 = (int64_t)X.ext[0] * X.ext[1];
+  if (c >= e01 * X.ext[2]) return;
+  const int k = (int)(c / e01);
+  const int j = (int)((c - (int64_t)k * e01) / e0);
+  const int i = (int)(c - (int64_t)k * e01 - (int64_t)j * e0);
+  const ElemGrid& D = grids[X.dst];
+  const ElemGrid& S = grids[X.src];
+  const int64_t di =
+      ((int64_t)(k + X.d0[2]) * D.dims[1] + (j + X.d0[1])) * D.dims[0] + (i + X.d0[0]);
+  const int64_t si =
+      ((int64_t)(k + X.s0[2]) * S.dims[1] + (j + X.s0[1])) * S.dims[0] + (i + X.s0[0]);
+#pragma unroll
+  for (int n = 0; n < 6; ++n)
+    if (D.f[n] && S.f[n]) D.f[n][di] = S.f[n][si];
+}
+
+void launch_copy_zones(const ElemGrid* grids, const CopyBox* boxes, const int64_t* prefix,
+                       int nboxes, int64_t blocks, cudaStream_t st) {
+  copy_zones_kernel<<<(unsigned)blocks, 256, 0, st>>>(grids, boxes, prefix, nboxes);
+}
+
 // ------------------------------------------------------------------ comoving expansion
 // grid::ComovingExpansionTerms for PPM (Grid_ComovingExpansionTerms.C:36-99 with
 // expand_terms.F, ENERGY_METHOD3 / VELOCITY_METHOD3) over every cell of every grid:

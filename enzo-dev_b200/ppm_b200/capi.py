@@ -36,6 +36,7 @@ EXPORTS = (
     "ppm_b200_version", "ppm_b200_profile", "ppm_b200_profile_read",
     "ppm_b200_euler_sweep_static", "ppm_b200_solve_level", "ppm_b200_set_graphs",
     "ppm_b200_compute_timestep_level", "ppm_b200_set_boundary_level",
+    "ppm_b200_copy_zones_level",
     "ppm_b200_profile_stages", "ppm_b200_set_guess", "ppm_b200_riemann_log",
     "ppm_b200_riemann_log_count", "ppm_b200_guess_features", "ppm_b200_guess_grad",
     "ppm_b200_guess_adam", "ppm_b200_guess_eval", "ppm_b200_expansion_terms",
@@ -170,6 +171,10 @@ def lib(build_if_missing: bool = True):
                                                   C.c_int, C.c_double, C.c_double,
                                                   C.POINTER(C.c_double), vp,
                                                   C.POINTER(C.c_double)]
+    L.ppm_b200_copy_zones_level.argtypes = [vp, C.POINTER(GridDesc), C.c_int,
+                                            C.POINTER(C.c_longlong), C.c_longlong * 3,
+                                            C.c_int * 3, C.c_int]
+    L.ppm_b200_copy_zones_level.restype = C.c_int
     L.ppm_b200_set_boundary_level.argtypes = [vp, C.POINTER(GridDesc), C.c_int, C.c_int,
                                               C.POINTER(C.c_int)]
     L.ppm_b200_profile_read.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]
@@ -413,6 +418,19 @@ class Context:
         rc = self.L.ppm_b200_set_boundary_level(self.h, arr, len(grids), int(bool(dual)), codes)
         if rc != OK:
             raise PPMError(rc, "ppm_b200_set_boundary_level")
+
+    def copy_zones_level(self, grids, fields_list, left, domain, periodic, dual):
+        """grid::CopyZonesFromGrid over a level (siblings and periodic images) on device
+        fields.  left[k]: level index of grid k's first zone (ghosts included) per axis;
+        domain: the level's extent in zones; periodic: per-axis flags."""
+        arr, keep = self._level(grids, fields_list)
+        lf = (C.c_longlong * (3 * len(grids)))(*[int(v) for l in left for v in list(l) + [0] * (3 - len(l))])
+        dom = (C.c_longlong * 3)(*[int(v) for v in list(domain) + [1] * (3 - len(domain))])
+        per = (C.c_int * 3)(*[int(bool(v)) for v in list(periodic) + [0] * (3 - len(periodic))])
+        rc = self.L.ppm_b200_copy_zones_level(self.h, arr, len(grids), lf, dom, per,
+                                              int(bool(dual)))
+        if rc != OK:
+            raise PPMError(rc, "ppm_b200_copy_zones_level")
 
     def profile(self, enable=True):
         self.L.ppm_b200_profile(self.h, int(bool(enable)))

@@ -200,6 +200,21 @@ int ppm_b200_compute_timestep_level(ppm_b200_context *ctx, const ppm_b200_params
 int ppm_b200_set_boundary_level(ppm_b200_context *ctx, ppm_b200_grid *grids, int ngrids,
                                 int dual_energy, const int bc_type[3]);
 
+/* grid::CopyZonesFromGrid (Grid_CopyZonesFromGrid.C:37-300, without the shearing box)
+   over a level, the sibling and periodic part of SetBoundaryConditions
+   (SetBoundaryConditions.C:113-201): every grid receives, into its whole region (ghost
+   zones included), the zones of every grid's active region that overlap it -- its
+   siblings', and the periodic images of all grids (itself included) shifted by
+   domain[d] along the axes with periodic[d] != 0.  Zones outside the domain on
+   non-periodic axes and zones covered only by the parent grid are left as they are
+   (ppm_b200_set_boundary_level fills the former).  left[3*k + d]: the index, at this
+   level's resolution, of grid k's first zone (ghosts included) along axis d; the grids
+   share their rank.  Active regions of a level are disjoint, so every zone receives at
+   most one copy; all copies run as one launch on device fields. */
+int ppm_b200_copy_zones_level(ppm_b200_context *ctx, ppm_b200_grid *grids, int ngrids,
+                              const long long *left, const long long domain[3],
+                              const int periodic[3], int dual_energy);
+
 /* Waits for all work queued on the context and returns the first error code
    recorded by device work since the last call; accumulates device counters
    into *stats (may be NULL). */
