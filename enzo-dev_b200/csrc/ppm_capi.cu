@@ -81,6 +81,22 @@ struct CopyBox {
 };
 void launch_copy_zones(const ElemGrid* grids, const CopyBox* boxes, const int64_t* prefix,
                        int nboxes, int64_t blocks, cudaStream_t st);
+struct FluxPhase {
+  int start[3], dim[3];
+  long long offset;
+  int correct_left, correct_right;
+  const double* il[6];
+  double* rl[6];
+  const double* ir[6];
+  double* rr[6];
+};
+struct FluxFix {
+  double* f[6];
+  int dims[3], rank, dual;
+  double tiny_number;
+  int nphases;
+};
+void launch_correct_fluxes(const FluxFix& X, const FluxPhase* phases, cudaStream_t st);
 }  // namespace ppm
 
 using ppm::BatchArgs;
@@ -149,6 +165,7 @@ struct ppm_b200_context {
   DevBuf misc;              // [0] min_bits, [1] dt, [2] min_bits of the folded time step
   DevBuf captures;
   DevBuf capture_buf;
+  DevBuf flux_fix;          // flux arrays and phases of ppm_b200_correct_fluxes
   std::vector<double> capture_host;
   Mirror mirror[kSlotCount];
   // event timing of sweep launches
@@ -1229,6 +1246,7 @@ int ppm_b200_destroy(ppm_b200_context* ctx) {
   fr(ctx->misc);
   fr(ctx->captures);
   fr(ctx->capture_buf);
+  fr(ctx->flux_fix);
   fr(ctx->guess);
   fr(ctx->log_count);
   for (auto& m : ctx->mirror) {
@@ -1667,6 +1685,136 @@ static int copy_zones_level(ppm_b200_context* ctx, ppm_b200_grid* grids, int ngr
   return PPM_B200_OK;
 }
 
+// grid::CorrectForRefinedFluxes for the proper subgrids of one grid (see the header):
+// the phases and their index arithmetic on the host (Grid_CorrectForRefinedFluxes.C:
+// 118-266), the flux arrays copied to the device, one kernel, the refined fluxes (which
+// an undone correction resets to the initial ones) copied back.
+static int correct_fluxes(ppm_b200_context* ctx, const ppm_b200_params* p, ppm_b200_grid* g,
+                          int memory, int nsub, const ppm_b200_fluxes* initial,
+                          ppm_b200_fluxes* refined, const long long gl[3]) {
+  if (!ctx || !p || !g || nsub < 0 || (nsub > 0 && (!initial || !refined)) || !gl)
+    return PPM_B200_ERR_INVALID;
+  if (nsub == 0) return PPM_B200_OK;
+  if (g->rank < 1 || g->rank > 3) return PPM_B200_ERR_INVALID;
+  CK(cudaSetDevice(ctx->device));
+  GridIO io;
+  io.g = g;
+  int rc = stage_in(ctx, p, g, memory, io.user, io.acc);
+  if (rc) return rc;
+  const int rank = g->rank;
+  const int* GD = g->dims;
+  // fields present: d, te, v1..v_rank, ge if dual (slots of ppm_b200_fluxes)
+  bool present[6];
+  for (int s = 0; s < 6; ++s) present[s] = io.user.f[s] != nullptr;
+  struct HostPhase {
+    ppm::FluxPhase ph;
+    int n, dim;
+    size_t count;
+  };
+  std::vector<HostPhase> phases;
+  for (int n = 0; n < nsub; ++n) {
+    const ppm_b200_fluxes& I = initial[n];
+    const ppm_b200_fluxes& R = refined[n];
+    for (int dim = 0; dim < rank; ++dim) {
+      if (GD[dim] <= 1) continue;
+      ppm::FluxPhase ph{};
+      int Start[3] = {0, 0, 0}, End[3] = {0, 0, 0};
+      for (int i = 0; i < rank; ++i) {
+        Start[i] = (int)(std::max(I.left_start[dim][i], R.left_start[dim][i]) - gl[i]);
+        End[i] = (int)(std::min(I.left_end[dim][i], R.left_end[dim][i]) - gl[i]);
+        if (Start[i] < 0 || End[i] > GD[i]) return PPM_B200_ERR_INVALID;
+      }
+      Start[dim] = std::max(Start[dim] - 1, 0);
+      End[dim] = Start[dim];
+      long long off = I.right_start[dim][dim] - I.left_start[dim][dim] + 2;
+      off = std::min<long long>(off, GD[dim] - 1);
+      ph.correct_left = Start[dim] == g->start[dim] - 1 ? 0 : 1;
+      ph.correct_right = Start[dim] + off == g->end[dim] + 1 ? 0 : 1;
+      for (int i = 0; i < dim; ++i) off *= GD[i];
+      ph.offset = off;
+      for (int i = 0; i < 3; ++i) {
+        ph.start[i] = Start[i];
+        ph.dim[i] = End[i] - Start[i] + 1;
+      }
+      // the layer's zones stay inside the grid
+      for (int i = 0; i < 3; ++i)
+        if (ph.start[i] < 0 || ph.start[i] + ph.dim[i] > GD[i]) return PPM_B200_ERR_INVALID;
+      if (ph.start[dim] + (off / (dim == 0 ? 1 : (dim == 1 ? GD[0] : (long long)GD[0] * GD[1]))) >=
+          GD[dim])
+        return PPM_B200_ERR_INVALID;
+      for (int s = 0; s < 6; ++s)
+        if (present[s] && (!I.left[s][dim] || !I.right[s][dim] || !R.left[s][dim] ||
+                           !R.right[s][dim]))
+          return PPM_B200_ERR_INVALID;
+      const size_t count = (size_t)ph.dim[0] * ph.dim[1] * ph.dim[2];
+      phases.push_back({ph, n, dim, count});
+    }
+  }
+  // flux arrays on the device: per phase and present field, il | rl | ir | rr
+  size_t total = 0;
+  for (const auto& h : phases)
+    for (int s = 0; s < 6; ++s)
+      if (present[s]) total += 4 * h.count;
+  rc = ensure(ctx, ctx->flux_fix, std::max<size_t>(total, 1) * sizeof(double) +
+                                      phases.size() * sizeof(ppm::FluxPhase) + 256);
+  if (rc) return rc;
+  double* dev = (double*)ctx->flux_fix.p;
+  size_t at = 0;
+  for (auto& h : phases) {
+    const ppm_b200_fluxes& I = initial[h.n];
+    const ppm_b200_fluxes& R = refined[h.n];
+    for (int s = 0; s < 6; ++s) {
+      if (!present[s]) continue;
+      const double* src[4] = {I.left[s][h.dim], R.left[s][h.dim], I.right[s][h.dim],
+                              R.right[s][h.dim]};
+      double* dst[4];
+      for (int q = 0; q < 4; ++q) {
+        dst[q] = dev + at;
+        at += h.count;
+        CK(cudaMemcpyAsync(dst[q], src[q], h.count * sizeof(double), cudaMemcpyHostToDevice,
+                           ctx->stream));
+      }
+      h.ph.il[s] = dst[0];
+      h.ph.rl[s] = dst[1];
+      h.ph.ir[s] = dst[2];
+      h.ph.rr[s] = dst[3];
+    }
+  }
+  std::vector<ppm::FluxPhase> host_ph(phases.size());
+  for (size_t q = 0; q < phases.size(); ++q) host_ph[q] = phases[q].ph;
+  ppm::FluxPhase* dph = (ppm::FluxPhase*)(dev + at);
+  if ((uintptr_t)dph % alignof(ppm::FluxPhase)) return PPM_B200_ERR_CUDA;
+  CK(cudaMemcpyAsync(dph, host_ph.data(), host_ph.size() * sizeof(ppm::FluxPhase),
+                     cudaMemcpyHostToDevice, ctx->stream));
+  ppm::FluxFix X{};
+  for (int s = 0; s < 6; ++s) X.f[s] = io.user.f[s];
+  for (int d = 0; d < 3; ++d) X.dims[d] = GD[d];
+  X.rank = rank;
+  X.dual = p->dual_energy ? 1 : 0;
+  X.tiny_number = p->tiny_number;
+  X.nphases = (int)phases.size();
+  ppm::launch_correct_fluxes(X, dph, ctx->stream);
+  ctx->launches += 1;
+  CK(cudaGetLastError());
+  // the refined fluxes back (an undone correction set them to the initial ones)
+  for (const auto& h : phases) {
+    ppm_b200_fluxes& R = refined[h.n];
+    for (int s = 0; s < 6; ++s) {
+      if (!present[s]) continue;
+      CK(cudaMemcpyAsync(R.left[s][h.dim], h.ph.rl[s], h.count * sizeof(double),
+                         cudaMemcpyDeviceToHost, ctx->stream));
+      CK(cudaMemcpyAsync(R.right[s][h.dim], h.ph.rr[s], h.count * sizeof(double),
+                         cudaMemcpyDeviceToHost, ctx->stream));
+    }
+  }
+  if (memory == PPM_B200_MEM_HOST) {
+    rc = stage_out(ctx, p, g, io.user);
+    if (rc) return rc;
+  }
+  CK(cudaStreamSynchronize(ctx->stream));
+  return PPM_B200_OK;
+}
+
 // Old fields of a grid on the device: device pointers as given, or copies of host arrays.
 static int stage_old(ppm_b200_context* ctx, const ppm_b200_params* p, const ppm_b200_grid* g,
                      const ppm_b200_grid* old, int memory, FieldSet& fs) {
@@ -1891,6 +2039,13 @@ int ppm_b200_copy_zones_level(ppm_b200_context* ctx, ppm_b200_grid* grids, int n
                               const long long* left, const long long domain[3],
                               const int periodic[3], int dual_energy) {
   return copy_zones_level(ctx, grids, ngrids, left, domain, periodic, dual_energy);
+}
+
+int ppm_b200_correct_fluxes(ppm_b200_context* ctx, const ppm_b200_params* params,
+                            ppm_b200_grid* grid, int memory, int nsub,
+                            const ppm_b200_fluxes* initial, ppm_b200_fluxes* refined,
+                            const long long grid_global_start[3]) {
+  return correct_fluxes(ctx, params, grid, memory, nsub, initial, refined, grid_global_start);
 }
 
 }  // extern "C"

@@ -227,6 +227,116 @@ void launch_copy_zones(const ElemGrid* grids, const CopyBox* boxes, const int64_
   copy_zones_kernel<<<(unsigned)blocks, 256, 0, st>>>(grids, boxes, prefix, nboxes);
 }
 
+// ------------------------------------------------------------------ flux correction
+// grid::CorrectForRefinedFluxes (Grid_CorrectForRefinedFluxes.C:38-760) for the proper
+// subgrids of one grid, Cartesian, the six hydro fields.  One phase per (subgrid, axis):
+// the layers of zones just outside the subgrid's left and right faces (Offset apart);
+// phases run in the reference's order, one block, a barrier between phases (two
+// subgrids may correct the same zone).  Within a phase every zone is independent: the
+// reference's loops over fields (outer) and zones (inner) give each zone the same
+// sequence as one thread running through the fields.
+struct FluxPhase {
+  int start[3], dim[3];      // the left layer in this grid's zones, and its extents
+  long long offset;          // from a left-layer zone to its right-layer zone
+  int correct_left, correct_right;
+  // per field slot (d, te, v1, v2, v3, ge): initial / refined left and right fluxes,
+  // indexed like the layer (null: field absent)
+  const double* il[6];
+  double* rl[6];
+  const double* ir[6];
+  double* rr[6];
+};
+
+struct FluxFix {
+  double* f[6];              // fields d, te, v1, v2, v3, ge (null: absent)
+  int dims[3], rank, dual;
+  double tiny_number;
+  int nphases;
+};
+
+__global__ void __launch_bounds__(256) correct_fluxes_kernel(const FluxFix X,
+                                                             const FluxPhase* __restrict__ ph) {
+  // correction order: density and the energies first, then the velocities
+  // (Grid_CorrectForRefinedFluxes.C:288-350): slots d, te, ge, v1, v2, v3
+  const int order[6] = {0, 1, 5, 2, 3, 4};
+  double* const* F = X.f;
+  for (int n = 0; n < X.nphases; ++n) {
+    const FluxPhase& P = ph[n];
+    const long long nz = (long long)P.dim[0] * P.dim[1] * P.dim[2];
+    for (long long z = threadIdx.x; z < nz; z += blockDim.x) {
+      const int i = (int)(z % P.dim[0]);
+      const int j = (int)((z / P.dim[0]) % P.dim[1]);
+      const int k = (int)(z / ((long long)P.dim[0] * P.dim[1]));
+      const long long c = ((long long)(k + P.start[2]) * X.dims[1] + (j + P.start[1])) * X.dims[0] +
+                          (i + P.start[0]);
+      const long long c2 = c + P.offset;
+      const long long x = z;  // the flux index ((k*Dim1 + j)*Dim0 + i)
+      // conserved quantities on both layers (:304-322): every field but density
+      for (int s = 1; s < 6; ++s)
+        if (F[s]) {
+          F[s][c] *= F[0][c];
+          F[s][c2] *= F[0][c2];
+        }
+      for (int q = 0; q < 6; ++q) {
+        const int f = order[q];
+        if (!F[f]) continue;
+        if (P.correct_left) {
+          const double amount = P.il[f][x] - P.rl[f][x];
+          F[f][c] += amount;
+        }
+        if (P.correct_right) {
+          const double amount = -(P.ir[f][x] - P.rr[f][x]);
+          F[f][c2] += amount;
+        }
+        if (f == 0 || f == 1 || f == 5) {  // density and the energies stay positive
+          if (P.correct_left && F[f][c] <= 0) {
+            for (int u = 0; u < 6; ++u) {
+              const int g = order[u];
+              if (!F[g]) continue;
+              if (u <= q) F[g][c] -= (P.il[g][x] - P.rl[g][x]);
+              P.rl[g][x] = P.il[g][x];
+            }
+          }
+          if (P.correct_right && F[f][c2] <= 0) {
+            for (int u = 0; u < 6; ++u) {
+              const int g = order[u];
+              if (!F[g]) continue;
+              if (u <= q) F[g][c2] -= -(P.ir[g][x] - P.rr[g][x]);
+              P.rr[g][x] = P.ir[g][x];
+            }
+          }
+        }
+      }
+      // back to specific quantities (:683-700)
+      for (int s = 1; s < 6; ++s)
+        if (F[s]) {
+          F[s][c] /= F[0][c];
+          F[s][c2] /= F[0][c2];
+        }
+      // gas and total energy consistent again (:704-742)
+      if (X.dual) {
+        F[5][c] = dmax(F[5][c], X.tiny_number);
+        F[5][c2] = dmax(F[5][c2], X.tiny_number);
+        F[1][c] = F[5][c] + 0.5 * F[2][c] * F[2][c];
+        F[1][c2] = F[5][c2] + 0.5 * F[2][c2] * F[2][c2];
+        if (X.rank > 1) {
+          F[1][c] += 0.5 * F[3][c] * F[3][c];
+          F[1][c2] += 0.5 * F[3][c2] * F[3][c2];
+        }
+        if (X.rank > 2) {
+          F[1][c] += 0.5 * F[4][c] * F[4][c];
+          F[1][c2] += 0.5 * F[4][c2] * F[4][c2];
+        }
+      }
+    }
+    __syncthreads();  // the next phase may touch the same zones
+  }
+}
+
+void launch_correct_fluxes(const FluxFix& X, const FluxPhase* phases, cudaStream_t st) {
+  correct_fluxes_kernel<<<1, 256, 0, st>>>(X, phases);
+}
+
 // ------------------------------------------------------------------ comoving expansion
 // grid::ComovingExpansionTerms for PPM (Grid_ComovingExpansionTerms.C:36-99 with
 // expand_terms.F, ENERGY_METHOD3 / VELOCITY_METHOD3) over every cell of every grid:

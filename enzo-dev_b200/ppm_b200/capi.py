@@ -36,7 +36,7 @@ EXPORTS = (
     "ppm_b200_version", "ppm_b200_profile", "ppm_b200_profile_read",
     "ppm_b200_euler_sweep_static", "ppm_b200_solve_level", "ppm_b200_set_graphs",
     "ppm_b200_compute_timestep_level", "ppm_b200_set_boundary_level",
-    "ppm_b200_copy_zones_level",
+    "ppm_b200_copy_zones_level", "ppm_b200_correct_fluxes",
     "ppm_b200_profile_stages", "ppm_b200_set_guess", "ppm_b200_riemann_log",
     "ppm_b200_riemann_log_count", "ppm_b200_guess_features", "ppm_b200_guess_grad",
     "ppm_b200_guess_adam", "ppm_b200_guess_eval", "ppm_b200_expansion_terms",
@@ -175,6 +175,10 @@ def lib(build_if_missing: bool = True):
                                             C.POINTER(C.c_longlong), C.c_longlong * 3,
                                             C.c_int * 3, C.c_int]
     L.ppm_b200_copy_zones_level.restype = C.c_int
+    L.ppm_b200_correct_fluxes.argtypes = [vp, C.POINTER(Params), C.POINTER(GridDesc), C.c_int,
+                                          C.c_int, C.POINTER(Fluxes), C.POINTER(Fluxes),
+                                          C.c_longlong * 3]
+    L.ppm_b200_correct_fluxes.restype = C.c_int
     L.ppm_b200_set_boundary_level.argtypes = [vp, C.POINTER(GridDesc), C.c_int, C.c_int,
                                               C.POINTER(C.c_int)]
     L.ppm_b200_profile_read.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]
@@ -418,6 +422,21 @@ class Context:
         rc = self.L.ppm_b200_set_boundary_level(self.h, arr, len(grids), int(bool(dual)), codes)
         if rc != OK:
             raise PPMError(rc, "ppm_b200_set_boundary_level")
+
+    def correct_fluxes(self, grid, hp, fields, initial, refined, ggs, memory=MEM_HOST):
+        """grid::CorrectForRefinedFluxes for the proper subgrids of one grid.  initial /
+        refined: lists of flux boxes (dicts as for make_fluxes, host numpy arrays); the
+        refined arrays are updated in place where a correction is undone."""
+        P = make_params(hp, 0.0)
+        G, keep = make_grid(grid, fields)
+        n = len(initial)
+        ini = (Fluxes * n)(*[make_fluxes(b) for b in initial])
+        ref = (Fluxes * n)(*[make_fluxes(b) for b in refined])
+        g = (C.c_longlong * 3)(*[int(x) for x in ggs])
+        rc = self.L.ppm_b200_correct_fluxes(self.h, C.byref(P), C.byref(G), int(memory), n, ini,
+                                            ref, g)
+        if rc != OK:
+            raise PPMError(rc, "ppm_b200_correct_fluxes")
 
     def copy_zones_level(self, grids, fields_list, left, domain, periodic, dual):
         """grid::CopyZonesFromGrid over a level (siblings and periodic images) on device

@@ -215,6 +215,21 @@ int ppm_b200_copy_zones_level(ppm_b200_context *ctx, ppm_b200_grid *grids, int n
                               const long long *left, const long long domain[3],
                               const int periodic[3], int dual_energy);
 
+/* grid::CorrectForRefinedFluxes (Grid_CorrectForRefinedFluxes.C:38-760) for the proper
+   subgrids of one grid: Cartesian coordinates, the six hydro fields (no species or
+   colours), RadiativeCooling == 0 and CorrectParentBoundaryFlux off (the defaults).  The
+   zones just outside each subgrid face get the difference of the coarse (initial, as
+   captured by the solve) and refined fluxes, in conserved form, with the reference's
+   undo when density or an energy would become non-positive -- which also resets those
+   refined fluxes to the initial ones, as the reference does -- and the dual-energy
+   consistency of the corrected zones.  initial[n] / refined[n]: the n-th subgrid's flux
+   structures (host arrays, the same index boxes); grid_global_start: the global index of
+   the grid's first zone (ghosts included).  memory: where the grid's fields live. */
+int ppm_b200_correct_fluxes(ppm_b200_context *ctx, const ppm_b200_params *params,
+                            ppm_b200_grid *grid, int memory, int nsub,
+                            const ppm_b200_fluxes *initial, ppm_b200_fluxes *refined,
+                            const long long grid_global_start[3]);
+
 /* Waits for all work queued on the context and returns the first error code
    recorded by device work since the last call; accumulates device counters
    into *stats (may be NULL). */

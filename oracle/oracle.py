@@ -109,6 +109,10 @@ def lib():
         L.ora_expansion_terms.argtypes = [C.POINTER(OraParams), dp * 6, C.c_void_p, C.c_double,
                                           C.c_double, C.c_double]
         L.ora_expansion_terms.restype = None
+        L.ora_correct_fluxes.argtypes = [C.POINTER(OraParams), dp * 6, C.c_int,
+                                         C.POINTER(OraFluxes), C.POINTER(OraFluxes),
+                                         C.c_longlong * 3]
+        L.ora_correct_fluxes.restype = C.c_int
         _lib = L
     return _lib
 
@@ -231,3 +235,19 @@ def expansion_terms(grid, hp, fields, old, time, old_time, coefficient):
     F = _fields6(fields)
     O = C.cast(_fields6(old), C.c_void_p) if old is not None else None
     L.ora_expansion_terms(C.byref(P), F, O, float(time), float(old_time), float(coefficient))
+
+
+def correct_fluxes(grid, hp, fields, initial, refined, ggs):
+    """grid::CorrectForRefinedFluxes (proper subgrids) on host fields, in place.  initial /
+    refined: lists of OraFluxes (the refined ones are updated where a correction is
+    undone).  ggs: global index of the grid's first zone.  Returns the C status."""
+    L = lib()
+    P = make_params(grid, hp, 0.0)
+    n = len(initial)
+    ini = (OraFluxes * n)(*initial)
+    ref = (OraFluxes * n)(*refined)
+    rc = L.ora_correct_fluxes(C.byref(P), _fields6(fields), n, ini, ref,
+                              (C.c_longlong * 3)(*[int(x) for x in ggs]))
+    for k in range(n):
+        refined[k] = ref[k]
+    return rc

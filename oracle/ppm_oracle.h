@@ -19,6 +19,7 @@
  *   grid::ComputePressure      src/enzo/Grid_ComputePressure.C:36-164
  *   calc_dt (PPM branch)       src/enzo/calc_dt.F:6-181
  *   calcdiss (flattening 1, 3) src/enzo/calcdiss.F:213-224, 407-438, 486-559
+ *   CorrectForRefinedFluxes    src/enzo/Grid_CorrectForRefinedFluxes.C:38-760
  *
  * Parity anchors: the reference's analytic shock-tube answer tests
  * (run/Hydro/Hydro-1D/{SodShockTube,Toro-*}) at the reference's own
@@ -115,6 +116,16 @@ void ora_set_riemann_log(ora_riemann_log_fn fn, void *ctx);
 void ora_expansion_terms(const ora_params *P, double *const fields[ORA_NFIELD],
                          double *const old[ORA_NFIELD], double time, double old_time,
                          double coefficient);
+
+/* grid::CorrectForRefinedFluxes (Grid_CorrectForRefinedFluxes.C:38-760) for the
+   proper subgrids of one grid (SUBlingGrid == FALSE), Cartesian coordinates, the six
+   hydro fields (no species or colours), RadiativeCooling == 0, CorrectParentBoundaryFlux
+   == FALSE.  initial[n] / refined[n]: the subgrid's coarse and refined boundary fluxes
+   (same index boxes); refined entries of undone corrections are set to the initial ones,
+   as the reference does.  gl: global index of the grid's first zone (ghosts included).
+   Returns 0, or -1 if a flux box does not fit the grid. */
+int ora_correct_fluxes(const ora_params *P, double *const fields[ORA_NFIELD], int nsub,
+                       const ora_fluxes *initial, ora_fluxes *refined, const long long gl[3]);
 
 #ifdef __cplusplus
 }
