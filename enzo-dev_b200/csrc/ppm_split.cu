@@ -385,12 +385,16 @@ __device__ __forceinline__ void load_face_advected(const SweepArgs& a, int64_t i
 // 8 resident blocks of 128 faces per SM (64 registers, a few spilled): the Newton
 // iteration's dependent FP64 chains want warps more than registers (256^3 sweep:
 // 1.65 -> 1.53 ms against the unconstrained 80 registers; 7 blocks: 1.59 ms).  The
-// learned start holds the net's fragments as well and keeps 3 blocks (168 registers).
+// learned start, with the net's fragments as well, gains the same way (3 blocks at 168
+// registers: 3.94 ms; 8 blocks at 64: 2.71 ms).
 #ifndef PPM_RIEMANN_MINBLOCKS
 #define PPM_RIEMANN_MINBLOCKS (8 * 128 / PPM_RIEMANN_THREADS)
 #endif
+#ifndef PPM_RIEMANN_LEARNED_MINBLOCKS
+#define PPM_RIEMANN_LEARNED_MINBLOCKS (8 * 128 / PPM_RIEMANN_THREADS)
+#endif
 template <bool DUAL, bool ONE, bool LEARNED>
-__global__ void __launch_bounds__(kRiemannThreads, LEARNED ? 3 : PPM_RIEMANN_MINBLOCKS) riemann_kernel(const __grid_constant__ BatchArgs B) {
+__global__ void __launch_bounds__(kRiemannThreads, LEARNED ? PPM_RIEMANN_LEARNED_MINBLOCKS : PPM_RIEMANN_MINBLOCKS) riemann_kernel(const __grid_constant__ BatchArgs B) {
   __shared__ unsigned int s_hist[8];
   __shared__ unsigned int s_newton;
   __shared__ unsigned int s_rejected;
