@@ -65,19 +65,24 @@ enum {
   kPackWords = kPackB3 + 4
 };
 
-// Interface-state features of one face (see the header comment); returns |x|^2.
+// Interface-state features of one face (see the header comment); returns |x|^2.  FP32
+// arithmetic on the FP32 pipe: the net sees its inputs rounded to BF16, so FP64 logs
+// and divides (which would load the FP64 pipe the Newton iteration is bound by) buy
+// nothing.  Training computes the features with this same function.
 __device__ __forceinline__ float guess_features(double dl, double dr, double pl, double pr,
                                                 double ul, double ur, double gamma, float f[6]) {
-  const double rho = 0.5 * (dl + dr);
-  const double p = 0.5 * (pl + pr);
-  const double u = 0.5 * (ul + ur);
-  const double c = sqrt(gamma * p / rho);
-  f[0] = (float)log(dl / rho);
-  f[1] = (float)log(dr / rho);
-  f[2] = (float)((ul - u) / c);
-  f[3] = (float)((ur - u) / c);
-  f[4] = (float)log(pl / p);
-  f[5] = (float)log(pr / p);
+  const float dlf = (float)dl, drf = (float)dr, plf = (float)pl, prf = (float)pr;
+  const float ulf = (float)ul, urf = (float)ur;
+  const float rho = 0.5f * (dlf + drf);
+  const float p = 0.5f * (plf + prf);
+  const float u = 0.5f * (ulf + urf);
+  const float ic = 1.0f / sqrtf((float)gamma * p / rho);
+  f[0] = logf(dlf / rho);
+  f[1] = logf(drf / rho);
+  f[2] = (ulf - u) * ic;
+  f[3] = (urf - u) * ic;
+  f[4] = logf(plf / p);
+  f[5] = logf(prf / p);
   float d2 = 0.0f;
   for (int k = 0; k < 6; ++k) d2 += f[k] * f[k];
   return d2;
@@ -183,12 +188,13 @@ __device__ __forceinline__ float guess_mlp_warp(const uint32_t* __restrict__ W, 
 }
 
 // The starting pressure from the net output r and |x|^2 (clamped so that a poor
-// prediction costs Newton iterations, never a non-finite start).
+// prediction costs Newton iterations, never a non-finite start).  The factor is an FP32
+// exponential: the start only has to be close, Newton refines it to the tolerance.
 __device__ __forceinline__ double guess_pressure(double p_acoustic, float r, float d2,
                                                  double pmin) {
   float yc = fminf(fmaxf(d2 * r, -8.0f), 8.0f);
   if (!(yc == yc)) yc = 0.0f;
-  double ps = p_acoustic * exp((double)yc);
+  double ps = p_acoustic * (double)expf(yc);
   if (!(ps >= pmin)) ps = pmin;
   return ps;
 }
