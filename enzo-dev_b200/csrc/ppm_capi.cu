@@ -47,6 +47,7 @@ struct ElemBatch {
   int ngrids;
   const int64_t* size_prefix;
   const int64_t* active_prefix;
+  const int64_t* row_prefix;
   double gamma, tiny_number, min_support;
   double aye, vg[3];
   unsigned long long* min_bits;
@@ -856,15 +857,16 @@ int read_counters(ppm_b200_context* ctx, ppm_b200_stats* st, int* status) {
 // Element descriptors of a batch (pressure, time step, ghost fill), one image slot.
 struct ElemPlan {
   ElemBatch B;
-  int64_t size_blocks = 0, active_blocks = 0;
+  int64_t size_blocks = 0, active_blocks = 0, row_blocks = 0;
 };
+constexpr int kFillRowsPerBlock = 32;  // rows of the padded grid per ghost-fill block
 
 int prepare_elem(ppm_b200_context* ctx, int slot, const ppm_b200_params* p,
                  const std::vector<GridIO>& io, bool with_cw, const int* bc, ElemPlan& plan,
                  const std::vector<FieldSet>* old = nullptr) {
   const int ng = (int)io.size();
   std::vector<ElemGrid> rec(ng);
-  std::vector<int64_t> spre(ng + 1, 0), apre(ng + 1, 0);
+  std::vector<int64_t> spre(ng + 1, 0), apre(ng + 1, 0), rpre(ng + 1, 0);
   // cell widths (time step only), deduplicated, in their own slot
   std::vector<std::array<int64_t, 3>> cwoff(ng, std::array<int64_t, 3>{{-1, -1, -1}});
   if (with_cw) {
@@ -916,6 +918,8 @@ int prepare_elem(ppm_b200_context* ctx, int slot, const ppm_b200_params* p,
     e.active = grid_active(g);
     spre[k + 1] = spre[k] + (e.size + 255) / 256;
     apre[k + 1] = apre[k] + (e.active + 255) / 256;
+    const int64_t rows = (int64_t)g->dims[1] * g->dims[2];
+    rpre[k + 1] = rpre[k] + (rows + kFillRowsPerBlock - 1) / kFillRowsPerBlock;
   }
   std::vector<unsigned char> img;
   append(img, rec.data(), rec.size());
@@ -925,6 +929,9 @@ int prepare_elem(ppm_b200_context* ctx, int slot, const ppm_b200_params* p,
   const size_t off_a = align256(img.size());
   img.resize(off_a);
   append(img, apre.data(), apre.size());
+  const size_t off_r = align256(img.size());
+  img.resize(off_r);
+  append(img, rpre.data(), rpre.size());
   int rc = mirror_put(ctx, ctx->mirror[slot], img);
   if (rc) return rc;
   unsigned char* base = (unsigned char*)ctx->mirror[slot].dev.p;
@@ -932,6 +939,7 @@ int prepare_elem(ppm_b200_context* ctx, int slot, const ppm_b200_params* p,
   plan.B.ngrids = ng;
   plan.B.size_prefix = (const int64_t*)(base + off_s);
   plan.B.active_prefix = (const int64_t*)(base + off_a);
+  plan.B.row_prefix = (const int64_t*)(base + off_r);
   plan.B.gamma = p->gamma;
   plan.B.tiny_number = p->tiny_number;
   plan.B.min_support = p->min_support;
@@ -942,6 +950,7 @@ int prepare_elem(ppm_b200_context* ctx, int slot, const ppm_b200_params* p,
   plan.B.interpolate = 0;
   plan.size_blocks = spre[ng];
   plan.active_blocks = apre[ng];
+  plan.row_blocks = rpre[ng];
   return PPM_B200_OK;
 }
 
@@ -1143,6 +1152,7 @@ std::string graph_key(ppm_b200_context* ctx, const ppm_b200_params* p, const Sol
   key_put(k, e.ngrids);
   key_put(k, e.size_prefix);
   key_put(k, e.active_prefix);
+  key_put(k, e.row_prefix);
   key_put(k, e.gamma);
   key_put(k, e.tiny_number);
   key_put(k, e.min_support);
@@ -1584,7 +1594,7 @@ static int boundary_batch(ppm_b200_context* ctx, ppm_b200_grid* grids, int ngrid
   ElemPlan ep;
   int rc = prepare_elem(ctx, kSlotBoundary, &p, io, false, bc_type, ep);
   if (rc) return rc;
-  ppm::launch_boundary_batch(ep.B, ep.size_blocks, ctx->stream);
+  ppm::launch_boundary_batch(ep.B, ep.row_blocks, ctx->stream);
   ctx->launches += 1;
   CK(cudaGetLastError());
   return PPM_B200_OK;

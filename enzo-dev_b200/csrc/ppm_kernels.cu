@@ -38,6 +38,7 @@ struct ElemBatch {
   int ngrids;
   const int64_t* size_prefix;    // ceil(size / 256) blocks per grid
   const int64_t* active_prefix;  // ceil(active / 256) blocks per grid
+  const int64_t* row_prefix;     // ceil(rows / 32) blocks per grid (ghost fill: 8 warps x 4 rows)
   double gamma, tiny_number, min_support;
   double aye, vg[3];
   unsigned long long* min_bits;  // running minimum of dt1 (positive doubles order as integers)
@@ -144,10 +145,12 @@ __device__ __forceinline__ int bc_map(int i, int s, int e, int bc) {
   return i < s ? s : e;
 }
 
-__device__ __forceinline__ void copy_cell(const ElemGrid& G, int64_t dst, int64_t src) {
+// f: the grid's field pointers held in registers (a store through one of them could
+// otherwise alias the record in global memory and force the pointers to be reloaded)
+__device__ __forceinline__ void copy_cell(double* const (&f)[6], int64_t dst, int64_t src) {
 #pragma unroll
   for (int n = 0; n < 6; ++n)
-    if (G.f[n]) G.f[n][dst] = G.f[n][src];
+    if (f[n]) f[n][dst] = f[n][src];
 }
 
 // One warp per row (j, k) of the padded grid: every ghost cell copies the cell it maps
@@ -155,21 +158,25 @@ __device__ __forceinline__ void copy_cell(const ElemGrid& G, int64_t dst, int64_
 // is copied whole from its source row, with consecutive lanes on consecutive cells.
 // Sources are cells that map to themselves in all three dimensions (active cells, or
 // ghosts of a face left to a halo exchange), which this kernel never writes, so the
-// in-place fill has no read-after-write hazard.  A grid's blocks (ceil(size / 256), 8
-// warps each) stride over its rows.
+// in-place fill has no read-after-write hazard.  A grid's blocks (ceil(rows / 32), 8
+// warps each) stride over its rows, about four per warp, so that the block-to-grid search
+// and the record's fields are amortised over several rows.
 __global__ void __launch_bounds__(256) boundary_kernel(const __grid_constant__ ElemBatch B) {
   int64_t lb;
-  const int gi = batch_locate(B.size_prefix, B.ngrids, blockIdx.x, lb);
+  const int gi = batch_locate(B.row_prefix, B.ngrids, blockIdx.x, lb);
   const ElemGrid& G = B.grids[gi];
-  const int64_t warps = (B.size_prefix[gi + 1] - B.size_prefix[gi]) * 8;
+  const int64_t warps = (B.row_prefix[gi + 1] - B.row_prefix[gi]) * 8;
   const int n0 = G.dims[0], n1 = G.dims[1], n2 = G.dims[2];
   const int s0 = G.start[0], e0 = G.end[0], bc0 = G.bc[0];
+  const int s1 = G.start[1], e1 = G.end[1], bc1 = G.bc[1];
+  const int s2 = G.start[2], e2 = G.end[2], bc2 = G.bc[2];
+  double* const f[6] = {G.f[0], G.f[1], G.f[2], G.f[3], G.f[4], G.f[5]};
   const int64_t rows = (int64_t)n1 * n2;
   const int lane = threadIdx.x & 31;
   for (int64_t row = lb * 8 + (threadIdx.x >> 5); row < rows; row += warps) {
     const int k = (int)(row / n1), j = (int)(row - (int64_t)k * n1);
-    const int sj = n1 > 1 ? bc_map(j, G.start[1], G.end[1], G.bc[1]) : j;
-    const int sk = n2 > 1 ? bc_map(k, G.start[2], G.end[2], G.bc[2]) : k;
+    const int sj = n1 > 1 ? bc_map(j, s1, e1, bc1) : j;
+    const int sk = n2 > 1 ? bc_map(k, s2, e2, bc2) : k;
     const int64_t dst = row * n0;
     const int64_t src = ((int64_t)sk * n1 + sj) * n0;
     if (sj == j && sk == k) {
@@ -178,12 +185,12 @@ __global__ void __launch_bounds__(256) boundary_kernel(const __grid_constant__ E
         for (int m = lane; m < nx; m += 32) {
           const int i = m < lo ? m : e0 + 1 + (m - lo);
           const int si = bc_map(i, s0, e0, bc0);
-          if (si != i) copy_cell(G, dst + i, src + si);
+          if (si != i) copy_cell(f, dst + i, src + si);
         }
       }
     } else {
       for (int i = lane; i < n0; i += 32)
-        copy_cell(G, dst + i, src + (n0 > 1 ? bc_map(i, s0, e0, bc0) : i));
+        copy_cell(f, dst + i, src + (n0 > 1 ? bc_map(i, s0, e0, bc0) : i));
     }
   }
 }
@@ -217,9 +224,16 @@ __global__ void __launch_bounds__(256) copy_zones_kernel(const ElemGrid* __restr
       ((int64_t)(k + X.d0[2]) * D.dims[1] + (j + X.d0[1])) * D.dims[0] + (i + X.d0[0]);
   const int64_t si =
       ((int64_t)(k + X.s0[2]) * S.dims[1] + (j + X.s0[1])) * S.dims[0] + (i + X.s0[0]);
+  double* dp[6];
+  const double* sp[6];
+#pragma unroll
+  for (int n = 0; n < 6; ++n) {  // pointers first: the stores below may not reload them
+    dp[n] = D.f[n];
+    sp[n] = S.f[n];
+  }
 #pragma unroll
   for (int n = 0; n < 6; ++n)
-    if (D.f[n] && S.f[n]) D.f[n][di] = S.f[n][si];
+    if (dp[n] && sp[n]) dp[n][di] = sp[n][si];
 }
 
 void launch_copy_zones(const ElemGrid* grids, const CopyBox* boxes, const int64_t* prefix,
