@@ -177,6 +177,7 @@ struct ppm_b200_context {
   // time step of the next cycle, folded into each solve's last sweep (ppm_b200_set_cfl)
   double* cfl_dt = nullptr;
   double cfl_courant = 1.0, cfl_aye = 1.0, cfl_vg[3] = {0.0, 0.0, 0.0};
+  unsigned debug_tma_extra = 0;  // ppm_b200_debug_tma_stall
   // learned Newton start: packed inference weights (ppm_b200_set_guess)
   DevBuf guess;
   bool has_guess = false;
@@ -765,6 +766,7 @@ int prepare_sweep(ppm_b200_context* ctx, int dim, int position, const ppm_b200_p
   if (ng == 1) plan.B.one = rec[0];
   plan.B.x_tma = 0;
   if (ng == 1 && dim == 0) set_x_tiles(plan.B, rec[0]);
+  plan.B.x_tma_extra_tx = plan.B.x_tma ? ctx->debug_tma_extra : 0u;
   plan.B.corrections = correction_planes(p) > 0 ? 1 : 0;
   plan.B.grids = (const SweepArgs*)base;
   plan.B.ngrids = ng;
@@ -1171,6 +1173,7 @@ std::string graph_key(ppm_b200_context* ctx, const ppm_b200_params* p, const Sol
     key_put(k, sp.sweep[s].riemann_blocks);
     key_put(k, sp.sweep[s].contiguous);
     key_put(k, b.x_tma);
+    key_put(k, b.x_tma_extra_tx);
     key_put(k, b.corrections);
     key_put(k, ctx->mirror[kSlotSweep0 + 3 * sp.order[s] + s].version);
   }
@@ -2049,6 +2052,13 @@ int ppm_b200_copy_zones_level(ppm_b200_context* ctx, ppm_b200_grid* grids, int n
                               const long long* left, const long long domain[3],
                               const int periodic[3], int dual_energy) {
   return copy_zones_level(ctx, grids, ngrids, left, domain, periodic, dual_energy);
+}
+
+int ppm_b200_debug_tma_stall(ppm_b200_context* ctx, int extra_bytes) {
+  if (!ctx || extra_bytes < 0 || extra_bytes > 4096 || extra_bytes % 16 != 0)
+    return PPM_B200_ERR_INVALID;
+  ctx->debug_tma_extra = (unsigned)extra_bytes;
+  return PPM_B200_OK;
 }
 
 int ppm_b200_correct_fluxes(ppm_b200_context* ctx, const ppm_b200_params* params,

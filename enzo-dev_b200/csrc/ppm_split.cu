@@ -1170,7 +1170,8 @@ __global__ void __launch_bounds__(kMarchThreads,
     xt.timeouts = B.counters + kCntTimeout;
     xt.fields = 3u | (a.in_u ? 4u : 0u) | (a.in_v ? 8u : 0u) | (a.in_w ? 16u : 0u) |
                 ((DUAL && a.in_ge) ? 32u : 0u);
-    xt.bytes = (unsigned)__popc(xt.fields) * kXTile * (unsigned)sizeof(double);
+    xt.bytes = (unsigned)__popc(xt.fields) * kXTile * (unsigned)sizeof(double) +
+               B.x_tma_extra_tx;
     xt.row0 = (int)wpid0;
     xt.last = -1;
     xt.broken = false;

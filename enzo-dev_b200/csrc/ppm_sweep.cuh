@@ -131,6 +131,9 @@ struct BatchArgs {
   // kXTileRows pencils x kXTileCells cells, through 2-D tensor maps (cells x pencils) of
   // d, e, u, v, w, ge (absent fields: unused).  x_tma = 0: plain loads.
   int x_tma = 0;
+  // test hook (ppm_b200_debug_tma_stall): bytes every TMA chunk expects beyond its
+  // copies, so that its barrier never completes and the bounded waits run out; 0
+  unsigned x_tma_extra_tx = 0;
   CUtensorMap xin[6];
 };
 

@@ -36,7 +36,7 @@ EXPORTS = (
     "ppm_b200_version", "ppm_b200_profile", "ppm_b200_profile_read",
     "ppm_b200_euler_sweep_static", "ppm_b200_solve_level", "ppm_b200_set_graphs",
     "ppm_b200_compute_timestep_level", "ppm_b200_set_boundary_level",
-    "ppm_b200_copy_zones_level", "ppm_b200_correct_fluxes",
+    "ppm_b200_copy_zones_level", "ppm_b200_correct_fluxes", "ppm_b200_debug_tma_stall",
     "ppm_b200_profile_stages", "ppm_b200_set_guess", "ppm_b200_riemann_log",
     "ppm_b200_riemann_log_count", "ppm_b200_guess_features", "ppm_b200_guess_grad",
     "ppm_b200_guess_adam", "ppm_b200_guess_eval", "ppm_b200_expansion_terms",
@@ -179,6 +179,8 @@ def lib(build_if_missing: bool = True):
                                           C.c_int, C.POINTER(Fluxes), C.POINTER(Fluxes),
                                           C.c_longlong * 3]
     L.ppm_b200_correct_fluxes.restype = C.c_int
+    L.ppm_b200_debug_tma_stall.argtypes = [vp, C.c_int]
+    L.ppm_b200_debug_tma_stall.restype = C.c_int
     L.ppm_b200_set_boundary_level.argtypes = [vp, C.POINTER(GridDesc), C.c_int, C.c_int,
                                               C.POINTER(C.c_int)]
     L.ppm_b200_profile_read.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]
@@ -422,6 +424,12 @@ class Context:
         rc = self.L.ppm_b200_set_boundary_level(self.h, arr, len(grids), int(bool(dual)), codes)
         if rc != OK:
             raise PPMError(rc, "ppm_b200_set_boundary_level")
+
+    def debug_tma_stall(self, extra_bytes):
+        """Test hook: make the x sweep's TMA chunk waits run out (0 restores)."""
+        rc = self.L.ppm_b200_debug_tma_stall(self.h, int(extra_bytes))
+        if rc != OK:
+            raise PPMError(rc, "ppm_b200_debug_tma_stall")
 
     def correct_fluxes(self, grid, hp, fields, initial, refined, ggs, memory=MEM_HOST):
         """grid::CorrectForRefinedFluxes for the proper subgrids of one grid.  initial /

@@ -225,6 +225,14 @@ int ppm_b200_copy_zones_level(ppm_b200_context *ctx, ppm_b200_grid *grids, int n
    consistency of the corrected zones.  initial[n] / refined[n]: the n-th subgrid's flux
    structures (host arrays, the same index boxes); grid_global_start: the global index of
    the grid's first zone (ghosts included).  memory: where the grid's fields live. */
+/* Test hook for the bounded device waits (not for production use): with extra_bytes > 0
+   (a multiple of 16, at most 4096) every TMA chunk of the x sweep's update kernel
+   expects that many bytes more than its copies deliver, so its barrier never completes;
+   each wait gives up after about a second, the kernel drains its copies and returns,
+   and the call reports PPM_B200_ERR_TIMEOUT with the context still usable.  0 restores
+   normal operation.  Nothing faults or hangs. */
+int ppm_b200_debug_tma_stall(ppm_b200_context *ctx, int extra_bytes);
+
 int ppm_b200_correct_fluxes(ppm_b200_context *ctx, const ppm_b200_params *params,
                             ppm_b200_grid *grid, int memory, int nsub,
                             const ppm_b200_fluxes *initial, ppm_b200_fluxes *refined,
