@@ -141,7 +141,8 @@ enum {
   kSlotCflCw = 17,     // cell widths read by the time step folded into the last sweep
   kSlotCopy = 18,      // element records of the sibling-zone copy
   kSlotCopyBoxes = 19, // its boxes and block prefix
-  kSlotCount = 20
+  kSlotColours = 20,   // colour field pointers of every grid of a sweep batch
+  kSlotCount = 21
 };
 // captured level graphs kept at most (a changed grid list leaves the old ones unused)
 constexpr size_t kMaxGraphs = 16;
@@ -159,6 +160,7 @@ struct ppm_b200_context {
   DevBuf host_set[6];       // device copies of host-memory fields (single grid)
   DevBuf host_acc[3];       // device copies of host-memory accelerations
   DevBuf host_old[6];       // device copies of host-memory fields at OldTime
+  DevBuf host_col;          // device copies of host-memory colour fields (single grid)
   DevBuf ring;              // two ring sets of the six updated fields, every grid of the batch
   DevBuf pressure;          // pressure of every grid of the batch
   DevBuf face_scratch;      // interface states, fluxes and the flagged-pencil list
@@ -166,8 +168,10 @@ struct ppm_b200_context {
   DevBuf misc;              // [0] min_bits, [1] dt, [2] min_bits of the folded time step
   DevBuf captures;
   DevBuf capture_buf;
+  DevBuf col_capture;       // colour fluxes of the capture requests (ncolour per request)
   DevBuf flux_fix;          // flux arrays and phases of ppm_b200_correct_fluxes
   std::vector<double> capture_host;
+  std::vector<double> col_capture_host;
   Mirror mirror[kSlotCount];
   // event timing of sweep launches
   bool profiling = false;
@@ -314,7 +318,9 @@ void build_coef(const double* dxi_in, int n, int is0, int ie0, std::vector<Coef>
 int check_supported(const ppm_b200_params* p) {
   if (!p) return PPM_B200_ERR_INVALID;
   if (p->pressure_free || p->diffusion || p->conservative_rec || p->positive_rec ||
-      p->eos_type != 0 || p->number_of_colours != 0)
+      p->eos_type != 0)
+    return PPM_B200_ERR_UNSUPPORTED;
+  if (p->number_of_colours < 0 || p->number_of_colours > PPM_B200_MAX_COLOURS)
     return PPM_B200_ERR_UNSUPPORTED;
   // slope corrections: calcdiss's flattening types 1 and 3, inteuler's steepening
   if ((p->flattening != 0 && p->flattening != 1 && p->flattening != 3) ||
@@ -329,6 +335,11 @@ int check_grid(const ppm_b200_grid* g, const ppm_b200_params* p) {
   if (!g || g->rank < 1 || g->rank > 3) return PPM_B200_ERR_INVALID;
   if (!g->density || !g->total_energy || !g->velocity[0]) return PPM_B200_ERR_INVALID;
   if (p->dual_energy && !g->gas_energy) return PPM_B200_ERR_INVALID;
+  if (p->number_of_colours > 0) {
+    if (!g->colours) return PPM_B200_ERR_INVALID;
+    for (int n = 0; n < p->number_of_colours; ++n)
+      if (!g->colours[n]) return PPM_B200_ERR_INVALID;
+  }
   for (int d = 0; d < 3; ++d) {
     if (d < g->rank) {
       if (g->end[d] - g->start[d] + 1 > 1) {
@@ -403,6 +414,8 @@ void pack_guess(const float* w, std::vector<uint32_t>& out) {
 
 struct FieldSet {
   double* f[6];  // d, e, v1, v2, v3, ge
+  int ncol = 0;  // colour fields (the grid's own set only: colours are updated in place)
+  double* col[ppm::kMaxColours];
 };
 
 // Device pointers of one grid for one call.
@@ -557,7 +570,7 @@ int build_captures(const ppm_b200_grid* g, int dim, int nsub, const ppm_b200_flu
 
 // Places the capture requests of several sweeps one after another in the capture
 // buffers (sized before any sweep is queued, so no buffer moves under queued work).
-int reserve_captures(ppm_b200_context* ctx, SweepPlan* plans, int n) {
+int reserve_captures(ppm_b200_context* ctx, SweepPlan* plans, int n, int ncolour) {
   int64_t total = 0;
   for (int s = 0; s < n; ++s) {
     plans[s].cap_offset = total;
@@ -566,6 +579,10 @@ int reserve_captures(ppm_b200_context* ctx, SweepPlan* plans, int n) {
   if (total == 0) return PPM_B200_OK;
   int rc = ensure(ctx, ctx->captures, (size_t)total * sizeof(FluxCapture));
   if (rc) return rc;
+  if (ncolour > 0) {
+    rc = ensure(ctx, ctx->col_capture, (size_t)total * (size_t)ncolour * sizeof(double));
+    if (rc) return rc;
+  }
   return ensure(ctx, ctx->capture_buf, (size_t)total * 6 * sizeof(double));
 }
 
@@ -577,17 +594,30 @@ size_t correction_planes(const ppm_b200_params* p) {
   return (p->flattening ? 1 : 0) + (p->steepening ? 1 : 0);
 }
 
+// colour face planes of a sweep (planes of the face scratch) and its fallback-face flags
+// (bytes, one plane per grid after the flagged-pencil list)
+size_t colour_planes(const ppm_b200_params* p) {
+  return p->number_of_colours > 0 ? (size_t)ppm::kColVars : 0;
+}
+
+// kernels one sweep launches: reconstruct x2, Riemann, update, fallback, and the
+// corrections and colour kernels when present
+int sweep_kernels(const ppm_b200_params* p) {
+  return 5 + (correction_planes(p) > 0 ? 1 : 0) + (p->number_of_colours > 0 ? 1 : 0);
+}
+
 size_t sweep_scratch_bytes(int dim, const std::vector<GridIO>& io, const ppm_b200_params* p) {
-  size_t doubles = 0, pencils = 0;
+  size_t doubles = 0, pencils = 0, flags = 0;
   for (const auto& x : io) {
     const ppm_b200_grid* g = x.g;
     const size_t np = (size_t)grid_size(g) / (size_t)g->dims[dim];
-    doubles += (size_t)(ppm::kFaceVars + ppm::kFluxVars) *
+    doubles += (size_t)(ppm::kFaceVars + ppm::kFluxVars + colour_planes(p)) *
                (size_t)(g->end[dim] - g->start[dim] + 2) * np;
     doubles += correction_planes(p) * (size_t)(g->end[dim] - g->start[dim] + 3) * np;
     pencils += np;
+    if (p->number_of_colours > 0) flags += (size_t)(g->end[dim] - g->start[dim] + 2) * np;
   }
-  return doubles * sizeof(double) + pencils * sizeof(int64_t);
+  return doubles * sizeof(double) + pencils * sizeof(int64_t) + flags;
 }
 
 int prepare_sweep(ppm_b200_context* ctx, int dim, int position, const ppm_b200_params* p,
@@ -631,8 +661,23 @@ int prepare_sweep(ppm_b200_context* ctx, int dim, int position, const ppm_b200_p
   // face scratch: planes of every grid, then the flagged-pencil list
   std::vector<SweepArgs> rec(ng);
   std::vector<int64_t> mpre(ng + 1, 0), rpre(ng + 1, 0);
-  size_t scratch_doubles = 0;
+  size_t scratch_doubles = 0, flag_bytes = 0;
   int64_t total_pencils = 0;
+  // colour field pointers of every grid, ncolour per grid
+  const int nc = p->number_of_colours;
+  double* const* col_dev = nullptr;
+  if (nc > 0) {
+    std::vector<double*> cptr;
+    for (int k = 0; k < ng; ++k) {
+      if (io[k].user.ncol != nc) return PPM_B200_ERR_INVALID;
+      cptr.insert(cptr.end(), io[k].user.col, io[k].user.col + nc);
+    }
+    std::vector<unsigned char> cimg;
+    append(cimg, cptr.data(), cptr.size());
+    int rc0 = mirror_put(ctx, ctx->mirror[kSlotColours], cimg);
+    if (rc0) return rc0;
+    col_dev = (double* const*)ctx->mirror[kSlotColours].dev.p;
+  }
   for (int k = 0; k < ng; ++k) {
     const ppm_b200_grid* g = io[k].g;
     const int GD0 = g->dims[0], GD1 = g->dims[1], GD2 = g->dims[2];
@@ -650,9 +695,11 @@ int prepare_sweep(ppm_b200_context* ctx, int dim, int position, const ppm_b200_p
     }
     a.npencils = (int64_t)a.n1 * a.n2;
     a.plane = (int64_t)(a.ie - a.is + 2) * a.npencils;
-    scratch_doubles += (size_t)(ppm::kFaceVars + ppm::kFluxVars) * (size_t)a.plane;
+    scratch_doubles += (size_t)(ppm::kFaceVars + ppm::kFluxVars + colour_planes(p)) *
+                       (size_t)a.plane;
     scratch_doubles += correction_planes(p) * (size_t)(a.ie - a.is + 3) * (size_t)a.npencils;
     total_pencils += a.npencils;
+    if (nc > 0) flag_bytes += (size_t)a.plane;
     const int64_t mb = (a.npencils + ppm::kMarchThreads - 1) / ppm::kMarchThreads;
     const int64_t rb = (int64_t)(a.ie - a.is + 2) *
                        ((a.npencils + ppm::kRiemannThreads - 1) / ppm::kRiemannThreads);
@@ -662,10 +709,13 @@ int prepare_sweep(ppm_b200_context* ctx, int dim, int position, const ppm_b200_p
   // callers that queue several sweeps size the scratch for all of them first, so this
   // never moves the buffer under a sweep prepared earlier
   rc = ensure(ctx, ctx->face_scratch,
-              scratch_doubles * sizeof(double) + (size_t)total_pencils * sizeof(int64_t));
+              scratch_doubles * sizeof(double) + (size_t)total_pencils * sizeof(int64_t) +
+                  flag_bytes);
   if (rc) return rc;
   double* scratch = (double*)ctx->face_scratch.p;
-  size_t at = 0;
+  unsigned char* flags = (unsigned char*)(scratch + scratch_doubles) +
+                         (size_t)total_pencils * sizeof(int64_t);
+  size_t at = 0, flag_at = 0;
   const int vu = dim, vv = (dim + 1) % 3, vw = (dim + 2) % 3;
   for (int k = 0; k < ng; ++k) {
     const ppm_b200_grid* g = io[k].g;
@@ -718,6 +768,14 @@ int prepare_sweep(ppm_b200_context* ctx, int dim, int position, const ppm_b200_p
       a.steep = scratch + at;
       at += cplane;
     }
+    if (nc > 0) {
+      a.ncolour = nc;
+      a.col = col_dev + (size_t)k * (size_t)nc;
+      a.fcol = scratch + at;
+      at += (size_t)ppm::kColVars * (size_t)a.plane;
+      a.fhll = flags + flag_at;
+      flag_at += (size_t)a.plane;
+    }
     a.dim = dim;
     a.rank = g->rank;
     if (cfl) {
@@ -747,6 +805,7 @@ int prepare_sweep(ppm_b200_context* ctx, int dim, int position, const ppm_b200_p
     a.captures = dev_reqs;
     a.ncaptures = (int64_t)plan.reqs.size();
     a.capture_buf = (double*)ctx->capture_buf.p;
+    if (nc > 0) a.col_capture = (double*)ctx->col_capture.p;
   }
 
   // descriptor image: records | march prefix | riemann prefix
@@ -768,6 +827,9 @@ int prepare_sweep(ppm_b200_context* ctx, int dim, int position, const ppm_b200_p
   if (ng == 1 && dim == 0) set_x_tiles(plan.B, rec[0]);
   plan.B.x_tma_extra_tx = plan.B.x_tma ? ctx->debug_tma_extra : 0u;
   plan.B.corrections = correction_planes(p) > 0 ? 1 : 0;
+  plan.B.ncolour = nc;
+  plan.B.hll_flags = nc > 0 ? flags : nullptr;
+  plan.B.hll_bytes = (int64_t)flag_bytes;
   plan.B.grids = (const SweepArgs*)base;
   plan.B.ngrids = ng;
   plan.B.march_prefix = (const int64_t*)(base + off_m);
@@ -795,7 +857,7 @@ int enqueue_sweep(ppm_b200_context* ctx, const SweepPlan& plan, const ppm_b200_p
   ppm::launch_sweep_batch(plan.B, plan.march_blocks, plan.riemann_blocks, p->dual_energy != 0,
                           p->gravity != 0, ctx->stream, ev, p->learned_guess != 0,
                           plan.contiguous);
-  ctx->launches += 5;
+  ctx->launches += sweep_kernels(p);
   CK(cudaGetLastError());
   return PPM_B200_OK;
 }
@@ -806,6 +868,14 @@ int scatter_captures(ppm_b200_context* ctx, int dim, const ppm_b200_params* p,
   ctx->capture_host.resize(plan.reqs.size() * 6);
   CK(cudaMemcpyAsync(ctx->capture_host.data(), (double*)ctx->capture_buf.p + plan.cap_offset * 6,
                      plan.reqs.size() * 6 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  const int nc = p->number_of_colours;
+  if (nc > 0) {
+    ctx->col_capture_host.resize(plan.reqs.size() * (size_t)nc);
+    CK(cudaMemcpyAsync(ctx->col_capture_host.data(),
+                       (double*)ctx->col_capture.p + plan.cap_offset * nc,
+                       plan.reqs.size() * (size_t)nc * sizeof(double), cudaMemcpyDeviceToHost,
+                       ctx->stream));
+  }
   CK(cudaStreamSynchronize(ctx->stream));
   // active extents for the transverse-velocity rule (nxz/nyz/nzz > 1)
   long long nact[3];
@@ -831,6 +901,11 @@ int scatter_captures(ppm_b200_context* ctx, int dim, const ppm_b200_params* p,
       put(slot_of_role[r], v[2 + r]);
     }
     if (p->dual_energy) put(5, v[5]);
+    // colours (Grid_xEulerSweep.C:361-371): entry n*3 + dim of the colour arrays
+    double* const* cdst = h.side == 0 ? fx.colour_left : fx.colour_right;
+    if (nc > 0 && cdst)
+      for (int n = 0; n < nc; ++n)
+        if (cdst[n * 3 + dim]) cdst[n * 3 + dim][h.offset] = ctx->col_capture_host[k * nc + n];
   }
   return PPM_B200_OK;
 }
@@ -958,20 +1033,32 @@ int prepare_elem(ppm_b200_context* ctx, int slot, const ppm_b200_params* p,
 
 // Resolve the device field set of a grid: device pointers as given, or the context's
 // device copies of host fields (copied in here; single grid only).
+// colours: also the colour fields (the sweeps; the other entry points do not read them).
 int stage_in(ppm_b200_context* ctx, const ppm_b200_params* p, ppm_b200_grid* g, int memory,
-             FieldSet& fs, const double* acc[3]) {
+             FieldSet& fs, const double* acc[3], bool colours = false) {
   double* src[6] = {g->density, g->total_energy, g->velocity[0],
                     g->rank > 1 ? g->velocity[1] : nullptr,
                     g->rank > 2 ? g->velocity[2] : nullptr,
                     p->dual_energy ? g->gas_energy : nullptr};
   const size_t bytes = (size_t)grid_size(g) * sizeof(double);
   for (int k = 0; k < 3; ++k) acc[k] = nullptr;
+  fs.ncol = colours ? p->number_of_colours : 0;
   if (memory == PPM_B200_MEM_DEVICE) {
     for (int k = 0; k < 6; ++k) fs.f[k] = src[k];
     for (int k = 0; k < g->rank; ++k) acc[k] = p->gravity ? g->acceleration[k] : nullptr;
+    for (int n = 0; n < fs.ncol; ++n) fs.col[n] = g->colours[n];
     return PPM_B200_OK;
   }
   if (memory != PPM_B200_MEM_HOST) return PPM_B200_ERR_INVALID;
+  if (fs.ncol > 0) {
+    int rc = ensure(ctx, ctx->host_col, bytes * (size_t)fs.ncol);
+    if (rc) return rc;
+    for (int n = 0; n < fs.ncol; ++n) {
+      fs.col[n] = (double*)ctx->host_col.p + (size_t)n * (size_t)grid_size(g);
+      CK(cudaMemcpyAsync(fs.col[n], g->colours[n], bytes, cudaMemcpyHostToDevice,
+                         ctx->stream));
+    }
+  }
   for (int k = 0; k < 6; ++k) {
     fs.f[k] = nullptr;
     if (!src[k]) continue;
@@ -1002,6 +1089,8 @@ int stage_out(ppm_b200_context* ctx, const ppm_b200_params* p, ppm_b200_grid* g,
   for (int k = 0; k < 6; ++k)
     if (dst[k] && fs.f[k])
       CK(cudaMemcpyAsync(dst[k], fs.f[k], bytes, cudaMemcpyDeviceToHost, ctx->stream));
+  for (int n = 0; n < fs.ncol; ++n)
+    CK(cudaMemcpyAsync(g->colours[n], fs.col[n], bytes, cudaMemcpyDeviceToHost, ctx->stream));
   return PPM_B200_OK;
 }
 
@@ -1078,7 +1167,7 @@ int prepare_solve(ppm_b200_context* ctx, const ppm_b200_params* p, int cycle,
     rc = build_captures(io[0].g, sp.order[s], ng == 1 ? nsub : 0, sub, ggs, sp.sweep[s]);
     if (rc) return rc;
   }
-  rc = reserve_captures(ctx, sp.sweep, sp.nsweeps);
+  rc = reserve_captures(ctx, sp.sweep, sp.nsweeps, p->number_of_colours);
   if (rc) return rc;
   // one face scratch serves the sweeps in turn: size it for the largest before any
   // sweep records its pointers
@@ -1175,6 +1264,9 @@ std::string graph_key(ppm_b200_context* ctx, const ppm_b200_params* p, const Sol
     key_put(k, b.x_tma);
     key_put(k, b.x_tma_extra_tx);
     key_put(k, b.corrections);
+    key_put(k, b.ncolour);
+    key_put(k, b.hll_flags);
+    key_put(k, b.hll_bytes);
     key_put(k, ctx->mirror[kSlotSweep0 + 3 * sp.order[s] + s].version);
   }
   return k;
@@ -1252,6 +1344,7 @@ int ppm_b200_destroy(ppm_b200_context* ctx) {
   for (auto& b : ctx->host_set) fr(b);
   for (auto& b : ctx->host_acc) fr(b);
   for (auto& b : ctx->host_old) fr(b);
+  fr(ctx->host_col);
   fr(ctx->ring);
   fr(ctx->pressure);
   fr(ctx->face_scratch);
@@ -1259,6 +1352,7 @@ int ppm_b200_destroy(ppm_b200_context* ctx) {
   fr(ctx->misc);
   fr(ctx->captures);
   fr(ctx->capture_buf);
+  fr(ctx->col_capture);
   fr(ctx->flux_fix);
   fr(ctx->guess);
   fr(ctx->log_count);
@@ -1346,7 +1440,7 @@ int ppm_b200_solve_ppm_de(ppm_b200_context* ctx, const ppm_b200_params* p, int c
   const long long* ggs = ggs_in ? ggs_in : zero3;
   std::vector<GridIO> io(1);
   io[0].g = g;
-  rc = stage_in(ctx, p, g, memory, io[0].user, io[0].acc);
+  rc = stage_in(ctx, p, g, memory, io[0].user, io[0].acc, true);
   if (rc) return rc;
   SolvePlan sp;
   rc = prepare_solve(ctx, p, cycle_number, io, nsub, sub, ggs, sp);
@@ -1386,7 +1480,7 @@ int ppm_b200_solve_level(ppm_b200_context* ctx, const ppm_b200_params* p, int cy
   std::vector<GridIO> io(ngrids);
   for (int k = 0; k < ngrids; ++k) {
     io[k].g = &grids[idx[k]];
-    rc = stage_in(ctx, p, &grids[idx[k]], PPM_B200_MEM_DEVICE, io[k].user, io[k].acc);
+    rc = stage_in(ctx, p, &grids[idx[k]], PPM_B200_MEM_DEVICE, io[k].user, io[k].acc, true);
     if (rc) return rc;
   }
   SolvePlan sp;
@@ -1417,7 +1511,7 @@ int ppm_b200_solve_level(ppm_b200_context* ctx, const ppm_b200_params* p, int cy
       it = ctx->graphs.emplace(key, ex).first;
     }
     CK(cudaGraphLaunch(it->second, ctx->stream));
-    ctx->launches += 1 + 5 * sp.nsweeps;
+    ctx->launches += 1 + sweep_kernels(p) * sp.nsweeps;
   } else {
     rc = enqueue_solve(ctx, p, io, sp, false);
     if (rc) return rc;
@@ -1442,7 +1536,7 @@ int ppm_b200_euler_sweep(ppm_b200_context* ctx, int dim, const ppm_b200_params* 
   const long long* ggs = ggs_in ? ggs_in : zero3;
   std::vector<GridIO> io(1);
   io[0].g = g;
-  rc = stage_in(ctx, p, g, memory, io[0].user, io[0].acc);
+  rc = stage_in(ctx, p, g, memory, io[0].user, io[0].acc, true);
   if (rc) return rc;
   rc = assign_scratch(ctx, io);
   if (rc) return rc;
@@ -1455,7 +1549,7 @@ int ppm_b200_euler_sweep(ppm_b200_context* ctx, int dim, const ppm_b200_params* 
   SweepPlan plan;
   rc = build_captures(g, dim, nsub, sub, ggs, plan);
   if (rc) return rc;
-  rc = reserve_captures(ctx, &plan, 1);
+  rc = reserve_captures(ctx, &plan, 1, p->number_of_colours);
   if (rc) return rc;
   std::vector<int> src(1, -1), dst(1, 0);
   rc = prepare_sweep(ctx, dim, 0, p, io, src, dst, plan);

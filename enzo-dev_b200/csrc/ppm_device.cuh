@@ -226,10 +226,19 @@ struct AdvState {
   double vl, vr, wl, wr, gel, ger;
 };
 
-// inteuler.F:320-410, 493-551 (d, p, u); gsum = grslice(i-1) + grslice(i) (GRAV only)
-template <bool DUAL, bool GRAV>
+// What the colour states of a face need from its density states (inteuler.F:436-450,
+// :500-515): the corrected densities before the dual-energy override and whether the
+// override replaced each side.
+struct ColFace {
+  double dlc, drc;
+  bool ovl, ovr;
+};
+
+// inteuler.F:320-410, 493-551 (d, p, u); gsum = grslice(i-1) + grslice(i) (GRAV only).
+// CX: also report the colour data of the face in *cx.
+template <bool DUAL, bool GRAV, bool CX = false>
 __device__ __forceinline__ CoreState face_core(const CoreL& L, const CoreR& R, double gsum,
-                                               const Phys& P) {
+                                               const Phys& P, ColFace* cx = nullptr) {
   CoreState s;
   double cla = sqrt(dmax(P.gamma * L.pla * L.dla, 0.0));
   double cra = sqrt(dmax(P.gamma * R.pra * R.dra, 0.0));
@@ -275,16 +284,23 @@ __device__ __forceinline__ CoreState face_core(const CoreL& L, const CoreR& R, d
   s.ur = R.ura + (betarp - betarm) * cra;
   s.dl = 1.0 / (ydla - (betal0 + betalp + betalm));
   s.dr = 1.0 / (ydra - (betar0 + betarp + betarm));
+  if (CX) {
+    cx->dlc = s.dl;
+    cx->drc = s.dr;
+    cx->ovl = cx->ovr = false;
+  }
   if (DUAL) {
     double ml = dmax(dmax(fabs(L.cm), fabs(L.c0)), fabs(L.cp));
     if (P.gamma * L.pla / L.dla < P.eta2 * (L.ula * L.ula) || ml < 1.0e-3 ||
         s.dl / L.dla > 5.0) {
       s.pl = L.pla; s.ul = L.ula; s.dl = L.dla;
+      if (CX) cx->ovl = true;
     }
     double mr = dmax(dmax(fabs(R.cm), fabs(R.c0)), fabs(R.cp));
     if (P.gamma * R.pra / R.dra < P.eta2 * (R.ura * R.ura) || mr < 1.0e-3 ||
         s.dr / R.dra > 5.0) {
       s.pr = R.pra; s.ur = R.ura; s.dr = R.dra;
+      if (CX) cx->ovr = true;
     }
   }
   s.pl = dmax(s.pl, kTiny);
@@ -362,9 +378,12 @@ struct Flux {
   double df, ef, uf, vf, wf, gef, ub;
 };
 
+// db_out (optional): the Godunov density db, which the colour fluxes scale by
+// (flux_twoshock.F:251-259)
 template <bool DUAL>
 __device__ __forceinline__ Flux flux_twoshock(const FaceState& s, double pbar, double ubar,
-                                              double qc, const Phys& P) {
+                                              double qc, const Phys& P,
+                                              double* db_out = nullptr) {
   const double gamma = P.gamma;
   double sn = copysign(1.0, -ubar);
   double u0, p0, d0;
@@ -398,6 +417,7 @@ __device__ __forceinline__ Flux flux_twoshock(const FaceState& s, double pbar, d
   if (l0 < 0.0) {
     pb = p0; db = d0; ub = u0;
   }
+  if (db_out) *db_out = db;
   double vb, wb, geb;
   if (ub > 0.0) {
     vb = s.vl; wb = s.wl; geb = s.gel;

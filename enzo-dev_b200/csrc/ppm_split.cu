@@ -266,7 +266,21 @@ __global__ void __launch_bounds__(kMarchThreads,
             R.cm = prA.cm;
             R.c0 = prA.c0;
             R.cp = prA.cp;
-            const CoreState s = face_core<DUAL, GRAV>(cLp, R, GRAV ? (wg0 + wg1) : 0.0, P);
+            CoreState s;
+            if (COR && a.fcol) {  // colours: what their face states need (kColVars planes)
+              ColFace cx;
+              s = face_core<DUAL, GRAV, true>(cLp, R, GRAV ? (wg0 + wg1) : 0.0, P, &cx);
+              double* oc = a.fcol + (int64_t)(c - is) * np + pid;
+              oc[CDLA * plane] = cLp.dla;
+              oc[CDL0 * plane] = cLp.dl0;
+              oc[CDRA * plane] = R.dra;
+              oc[CDR0 * plane] = R.dr0;
+              oc[CDLC * plane] = cx.dlc;
+              oc[CDRC * plane] = cx.drc;
+              oc[COVR * plane] = (cx.ovl ? 1.0 : 0.0) + (cx.ovr ? 2.0 : 0.0);
+            } else {
+              s = face_core<DUAL, GRAV>(cLp, R, GRAV ? (wg0 + wg1) : 0.0, P);
+            }
             o[SDL * plane] = s.dl;
             o[SDR * plane] = s.dr;
             o[SPL * plane] = s.pl;
@@ -393,7 +407,8 @@ __device__ __forceinline__ void load_face_advected(const SweepArgs& a, int64_t i
 #ifndef PPM_RIEMANN_LEARNED_MINBLOCKS
 #define PPM_RIEMANN_LEARNED_MINBLOCKS (8 * 128 / PPM_RIEMANN_THREADS)
 #endif
-template <bool DUAL, bool ONE, bool LEARNED>
+// COL: also store the Godunov density of every face for the colour kernel
+template <bool DUAL, bool ONE, bool LEARNED, bool COL = false>
 __global__ void __launch_bounds__(kRiemannThreads, LEARNED ? PPM_RIEMANN_LEARNED_MINBLOCKS : PPM_RIEMANN_MINBLOCKS) riemann_kernel(const __grid_constant__ BatchArgs B) {
   __shared__ unsigned int s_hist[8];
   __shared__ unsigned int s_newton;
@@ -465,9 +480,11 @@ __global__ void __launch_bounds__(kRiemannThreads, LEARNED ? PPM_RIEMANN_LEARNED
     }
     const double qc = P.dt / a.coef[a.is + fi].dx;
     load_face_advected<DUAL>(a, idx, s);
-    const Flux F = flux_twoshock<DUAL>(s, rs.pbar, rs.ubar, qc, P);
+    double db;
+    const Flux F = flux_twoshock<DUAL>(s, rs.pbar, rs.ubar, qc, P, COL ? &db : nullptr);
     double* o = a.fflux + idx;
     const int64_t pl = a.plane;
+    if (COL) a.fcol[CDB * pl + idx] = db;
     o[XDF * pl] = F.df;
     o[XEF * pl] = F.ef;
     o[XUF * pl] = F.uf;
@@ -995,6 +1012,10 @@ __device__ __forceinline__ bool update_pencil(const SweepArgs& a, int64_t pid, c
             bool fatal = false;
             cnt.fallbacks += 1;
             hll_fallback<DUAL>(a, pid, base, t, Cn, P, F0, F1, ges_n, govv_next, fatal);
+            if (a.fhll) {  // the colour kernel recomputes these faces' colour fluxes
+              a.fhll[(int64_t)(t - is) * np + pid] = 1;
+              a.fhll[(int64_t)(t + 1 - is) * np + pid] = 1;
+            }
             gov_next = DUAL;
             if (fatal) cnt.fatal += 1;
           }
@@ -1231,6 +1252,141 @@ __global__ void __launch_bounds__(128) fallback_kernel(const __grid_constant__ B
   }
 }
 
+// ------------------------------------------------------------------ stage 5 (colours)
+// The colour fields of the sweep (NumberOfColours > 0), one thread per (pencil, colour),
+// marching like the reconstruction: each colour's PPM parabola (intvar with the
+// slice's flattening and no steepening, inteuler.F:276-282), its face states scaled by
+// the corrected density and undone with the dual-energy override (inteuler.F:436-450,
+// :500-515) and floored (:546-551), the flux at the Godunov state
+// (flux_twoshock.F:251-259, :375-380) or, on faces the HLL fallback replaced, HLL's
+// (flux_hll.F:236-262, :328-332), divided by dx (euler.F:173-176), the subgrid-flux
+// capture of that quotient (Grid_xEulerSweep.C:361-371), and the update with its floor
+// (euler.F:178-186), written in place: a cell is read three steps before it is written
+// and never read again.
+// Blocks: (march block, colour) with the colour fastest, so that the blocks of one
+// pencil block run together and share their density, pressure, velocity and face reads
+// through L2.
+constexpr double kColourFloor = 1.0e-35;        // color_floor, fortran.def:8
+constexpr double kMinColour = 1.0e-5 * kTiny;   // min_color, euler.F:104-105
+
+template <bool DUAL, bool ONE>
+__global__ void __launch_bounds__(kMarchThreads) colour_kernel(const __grid_constant__ BatchArgs B) {
+  const int nc = B.ncolour;
+  const int64_t mb = blockIdx.x / nc;
+  const int colour = (int)(blockIdx.x - mb * nc);
+  int64_t lb = mb;
+  const int g = ONE ? 0 : batch_locate(B.march_prefix, B.ngrids, mb, lb);
+  PPM_BIND_RECORD(a, g)
+  const int64_t pid = lb * kMarchThreads + threadIdx.x;
+  if (pid >= a.npencils) return;
+  const Phys P = make_phys(a);
+  const int64_t base = (pid % a.n1) * a.s1 + (pid / a.n1) * a.s2;
+  const int64_t sa = a.sa;
+  const int is = a.is, ie = a.ie;
+  const int64_t np = a.npencils, plane = a.plane;
+  double* const q = a.col[colour];
+
+  int64_t cap = 0, cap_end = 0;
+  if (a.ncaptures > 0) {
+    int64_t lo = 0, hi = a.ncaptures;
+    while (lo < hi) {
+      int64_t mid = (lo + hi) >> 1;
+      if (a.captures[mid].pencil < pid) lo = mid + 1; else hi = mid;
+    }
+    cap = cap_end = lo;
+    while (cap_end < a.ncaptures && a.captures[cap_end].pencil == pid) ++cap_end;
+  }
+
+  double wq0 = 0.0, wq1 = 0.0, wq2 = 0.0;  // colour of cells t-3, t-2, t-1
+  double dqm1 = 0.0, qlm1 = 0.0;           // dq(t-2), ql(t-2)
+  double wu0 = 0.0, wu1 = 0.0, wu2 = 0.0;  // normal velocity of cells t-3, t-2, t-1
+  Prep prA = {0, 0, 0, 0, 0}, prB = {0, 0, 0, 0, 0};  // cells t-2, t-1
+  double colla = 0.0, coll0 = 0.0;         // left data of face t-2
+  double fm = 0.0;                         // colf / dx of face t-3
+  const int tend = ie + 3;
+#pragma unroll 1
+  for (int t = 0; t <= tend; ++t) {
+    const int64_t off = base + (int64_t)t * sa;
+    const double nq = q[off];
+    const double nu = ldg0(a.in_u, off);
+    Prep prC = prB;
+    if (t >= is - 1 && t <= ie + 1)
+      prC = cell_prep(__ldg(a.in_d + off), __ldg(a.pres + off), nu, a.coef[t].dx2i, P);
+    double dqN = 0.0, qlN = 0.0;  // slope and left edge of cell t-1
+    {
+      const int c = t - 1;
+      if (c >= is - 2 && c <= ie + 2) {
+        const Coef cf = a.coef[c];
+        dqN = pm_slope(wq1, wq2, nq, cf.c1, cf.c2);
+        if (c >= is - 1) qlN = pm_edge(wq1, wq2, dqm1, dqN, cf.c3, cf.c4, cf.c5, cf.c6);
+      }
+    }
+    {
+      const int c = t - 2;  // parabola of cell c; face c
+      if (c >= is - 1 && c <= ie + 1) {
+        Para pa;
+        if (a.flatten != 0) {
+          const double fl = a.flat[(int64_t)(c - (is - 1)) * np + pid];
+          pa = pm_parabola<false, true>(wq0, wq1, wq2, qlm1, qlN, 0.0, 0.0, 0.0, fl);
+        } else {
+          pa = pm_parabola(wq0, wq1, wq2, qlm1, qlN);
+        }
+        if (c >= is) {
+          const int64_t fidx = (int64_t)(c - is) * np + pid;
+          const double* fc = a.fcol + fidx;
+          const double colra = pm_C(pa, prA.char2), colr0 = pm_B(pa, prA.c0);
+          const double dla = fc[CDLA * plane], dra = fc[CDRA * plane];
+          const double dlc = fc[CDLC * plane], drc = fc[CDRC * plane];
+          double cls = (wu0 <= 0.0) ? colla * dlc / dla : coll0 * dlc / fc[CDL0 * plane];
+          double crs = (wu1 >= 0.0) ? colra * drc / dra : colr0 * drc / fc[CDR0 * plane];
+          const double ov = fc[COVR * plane];
+          if (ov == 1.0 || ov == 3.0) cls = cls * dla / dlc;
+          if (ov >= 2.0) crs = crs * dra / drc;
+          cls = dmax(cls, kColourFloor);
+          crs = dmax(crs, kColourFloor);
+          double cf;
+          if (a.fhll[fidx]) {
+            const HllFace h = hll_face<DUAL>(load_face<DUAL>(a, fidx), P);
+            cf = h.sl * (h.gesl * cls) + h.sr * (h.gesr * crs);
+            cf = P.dt * cf;
+          } else {
+            const double ub = a.fflux[XUB * plane + fidx];
+            const double db = fc[CDB * plane];
+            const double colb = ub > 0.0 ? cls * db / a.fstate[SDL * plane + fidx]
+                                         : crs * db / a.fstate[SDR * plane + fidx];
+            cf = P.dt * ub * colb;
+          }
+          cf = cf / a.coef[c].dx;
+          while (cap < cap_end && a.captures[cap].face <= c) {
+            const FluxCapture& rq = a.captures[cap];
+            if (rq.face == c) a.col_capture[(rq.dst / 6) * nc + colour] = cf;
+            ++cap;
+          }
+          if (c - 1 >= is && c - 1 <= ie) {
+            const double v = wq0 + (fm - cf);
+            q[base + (int64_t)(c - 1) * sa] = dmax(v, kMinColour);
+          }
+          fm = cf;
+        }
+        if (c <= ie) {
+          colla = pm_A(pa, prA.char1);
+          coll0 = pm_A(pa, prA.c0);
+        }
+      }
+    }
+    wq0 = wq1;
+    wq1 = wq2;
+    wq2 = nq;
+    dqm1 = dqN;
+    qlm1 = qlN;
+    wu0 = wu1;
+    wu1 = wu2;
+    wu2 = nu;
+    prA = prB;
+    prB = prC;
+  }
+}
+
 // Above 48 KB of dynamic shared memory a kernel needs the opt-in attribute, set once
 // per device (a function attribute is not a stream operation, so this is also legal
 // while a stream is being captured).
@@ -1260,8 +1416,10 @@ void launch_stages(const BatchArgs& B, int64_t march_blocks, int64_t riemann_blo
   };
   mark(0);
   cudaMemsetAsync(B.counters + kCntFlagged, 0, sizeof(unsigned long long), st);
-  if (B.corrections) {
-    corrections_kernel<ONE><<<(unsigned)march_blocks, kMarchThreads, 0, st>>>(B);
+  if (B.ncolour > 0) cudaMemsetAsync(B.hll_flags, 0, (size_t)B.hll_bytes, st);
+  if (B.corrections || B.ncolour > 0) {  // the colour data come from the COR variant
+    if (B.corrections)
+      corrections_kernel<ONE><<<(unsigned)march_blocks, kMarchThreads, 0, st>>>(B);
     reconstruct_kernel<DUAL, GRAV, 0, ONE, true><<<(unsigned)march_blocks, kMarchThreads, 0, st>>>(B);
     mark(1);
     reconstruct_kernel<DUAL, GRAV, 1, ONE, true><<<(unsigned)march_blocks, kMarchThreads, 0, st>>>(B);
@@ -1271,10 +1429,15 @@ void launch_stages(const BatchArgs& B, int64_t march_blocks, int64_t riemann_blo
     reconstruct_kernel<DUAL, GRAV, 1, ONE><<<(unsigned)march_blocks, kMarchThreads, 0, st>>>(B);
   }
   mark(2);
-  if (learned)
-    riemann_kernel<DUAL, ONE, true><<<(unsigned)riemann_blocks, kRiemannThreads, 0, st>>>(B);
+  const unsigned rb = (unsigned)riemann_blocks;
+  if (learned && B.ncolour > 0)
+    riemann_kernel<DUAL, ONE, true, true><<<rb, kRiemannThreads, 0, st>>>(B);
+  else if (learned)
+    riemann_kernel<DUAL, ONE, true><<<rb, kRiemannThreads, 0, st>>>(B);
+  else if (B.ncolour > 0)
+    riemann_kernel<DUAL, ONE, false, true><<<rb, kRiemannThreads, 0, st>>>(B);
   else
-    riemann_kernel<DUAL, ONE, false><<<(unsigned)riemann_blocks, kRiemannThreads, 0, st>>>(B);
+    riemann_kernel<DUAL, ONE, false><<<rb, kRiemannThreads, 0, st>>>(B);
   mark(3);
   if (PPM_X_TMA && staged && ONE && B.x_tma)
     launch_update<DUAL, GRAV, ONE, true, ONE>(B, march_blocks, st);
@@ -1284,6 +1447,9 @@ void launch_stages(const BatchArgs& B, int64_t march_blocks, int64_t riemann_blo
     launch_update<DUAL, GRAV, ONE, false, false>(B, march_blocks, st);
   mark(4);
   fallback_kernel<DUAL, GRAV, ONE><<<64, 128, 0, st>>>(B);
+  if (B.ncolour > 0)
+    colour_kernel<DUAL, ONE>
+        <<<(unsigned)(march_blocks * B.ncolour), kMarchThreads, 0, st>>>(B);
   mark(5);
 }
 

@@ -96,9 +96,24 @@ struct SweepArgs {
   double* flat;
   double* steep;
   int flatten, steepen;              // PPMFlatteningParameter, PPMSteepeningParameter
+  // colour fields (NumberOfColours > 0): advected in place by the colour kernel after the
+  // sweep's update.  col: device array of ncolour field pointers; fcol: kColVars face
+  // planes that the density reconstruction and the Riemann stage leave for it; fhll: one
+  // byte per face, set where the HLL fallback replaced the face's fluxes;
+  // col_capture: ncolour doubles per subgrid-flux capture request (request r = dst / 6)
+  int ncolour;
+  double* const* col;
+  double* fcol;
+  unsigned char* fhll;
+  double* col_capture;
 };
 
 enum { kFaceVars = 12, kFluxVars = 7 };
+// colour face planes: dla dl0 dra dr0 (the density's characteristic averages), the
+// corrected densities before the dual-energy override, the override flags (1 left,
+// 2 right) and the Godunov density db
+enum { CDLA = 0, CDL0, CDRA, CDR0, CDLC, CDRC, COVR, CDB, kColVars };
+enum { kMaxColours = 45 };  // MAX_COLOR (fortran.def:2)
 
 // Threads per block of the marching stages and of the face-parallel Riemann stage.
 // (Riemann blocks of 128 faces leave fewer idle lanes at the end of each face plane of
@@ -134,6 +149,11 @@ struct BatchArgs {
   // test hook (ppm_b200_debug_tma_stall): bytes every TMA chunk expects beyond its
   // copies, so that its barrier never completes and the bounded waits run out; 0
   unsigned x_tma_extra_tx = 0;
+  // colours: the batch's NumberOfColours (every grid the same) and the fallback-face
+  // flags of all its grids (one region, cleared at the start of each sweep)
+  int ncolour = 0;
+  unsigned char* hll_flags = nullptr;
+  int64_t hll_bytes = 0;
   CUtensorMap xin[6];
 };
 

@@ -70,7 +70,7 @@ class GridDesc(C.Structure):
         ("rank", C.c_int), ("dims", C.c_int * 3), ("start", C.c_int * 3), ("end", C.c_int * 3),
         ("density", C.c_void_p), ("total_energy", C.c_void_p), ("velocity", C.c_void_p * 3),
         ("gas_energy", C.c_void_p), ("acceleration", C.c_void_p * 3),
-        ("cell_width", C.c_void_p * 3),
+        ("cell_width", C.c_void_p * 3), ("colours", C.c_void_p),
     ]
 
 
@@ -79,6 +79,7 @@ class Fluxes(C.Structure):
         ("left_start", (C.c_longlong * 3) * 3), ("left_end", (C.c_longlong * 3) * 3),
         ("right_start", (C.c_longlong * 3) * 3), ("right_end", (C.c_longlong * 3) * 3),
         ("left", (C.c_void_p * 3) * 6), ("right", (C.c_void_p * 3) * 6),
+        ("colour_left", C.c_void_p), ("colour_right", C.c_void_p),
     ]
 
 
@@ -230,8 +231,16 @@ def make_params(hp, dt, learned_guess=False, dt_device=None) -> Params:
     return P
 
 
+def colour_names(fields):
+    """Colour fields of a field dict: keys col0, col1, ... in colnum[] order."""
+    n = 0
+    while f"col{n}" in fields:
+        n += 1
+    return [f"col{k}" for k in range(n)]
+
+
 def make_grid(grid, fields, accel=None):
-    """Returns (GridDesc, keepalive list)."""
+    """Returns (GridDesc, keepalive list).  Colour fields: keys col0, col1, ..."""
     G = GridDesc()
     G.rank = grid.rank
     for d in range(3):
@@ -250,12 +259,19 @@ def make_grid(grid, fields, accel=None):
         cw = np.ascontiguousarray(grid.cellwidth[d], dtype=np.float64)
         keep.append(cw)
         G.cell_width[d] = cw.ctypes.data
+    cols = colour_names(fields)
+    if cols:
+        arr = (C.c_void_p * len(cols))(*[_addr(fields[n]) for n in cols])
+        keep.append(arr)
+        G.colours = C.cast(arr, C.c_void_p)
     return G, keep
 
 
-def make_fluxes(box):
+def make_fluxes(box, keep=None):
     """box: dict with left_start/left_end/right_start/right_end (3x3) and arrays
-    left[slot][dim], right[slot][dim] (numpy, may be None). Returns Fluxes."""
+    left[slot][dim], right[slot][dim] (numpy, may be None), and optionally
+    colour_left[n][dim] / colour_right[n][dim].  Returns Fluxes; keep (a list) holds the
+    colour pointer arrays alive."""
     F = Fluxes()
     for key in ("left_start", "left_end", "right_start", "right_end"):
         arr = getattr(F, key)
@@ -268,6 +284,18 @@ def make_fluxes(box):
             for d in range(3):
                 a = box[side][s][d]
                 arr[s][d] = _addr(a) if a is not None else None
+    for side in ("colour_left", "colour_right"):
+        rows = box.get(side)
+        if not rows:
+            continue
+        ptrs = (C.c_void_p * (3 * len(rows)))()
+        for n, row in enumerate(rows):
+            for d in range(3):
+                a = row[d]
+                ptrs[3 * n + d] = _addr(a) if a is not None else None
+        if keep is not None:
+            keep.append(ptrs)
+        setattr(F, side, C.cast(ptrs, C.c_void_p))
     return F
 
 
@@ -319,12 +347,13 @@ class Context:
                      subgrids=None, ggs=(0, 0, 0), want_stats=True, learned_guess=False,
                      dt_device=None, check=True):
         P = make_params(hp, dt, learned_guess, dt_device)
+        P.number_of_colours = len(colour_names(fields))
         G, keep = make_grid(grid, fields, accel)
         st = Stats()
         nsub = 0 if not subgrids else len(subgrids)
         sub = None
         if nsub:
-            sub = (Fluxes * nsub)(*[make_fluxes(b) for b in subgrids])
+            sub = (Fluxes * nsub)(*[make_fluxes(b, keep) for b in subgrids])
         g = (C.c_longlong * 3)(*[int(x) for x in ggs])
         rc = self.L.ppm_b200_solve_ppm_de(self.h, C.byref(P), int(cycle), C.byref(G), int(memory),
                                           nsub, sub, g, C.byref(st) if want_stats else None)
@@ -335,6 +364,7 @@ class Context:
     def euler_sweep(self, dim, grid, hp, dt, fields, pressure, memory=MEM_HOST, accel=None,
                     check=True, learned_guess=False):
         P = make_params(hp, dt, learned_guess)
+        P.number_of_colours = len(colour_names(fields))
         G, keep = make_grid(grid, fields, accel)
         st = Stats()
         g = (C.c_longlong * 3)(0, 0, 0)
@@ -390,6 +420,7 @@ class Context:
                     dt_device=None, check=True, learned_guess=False):
         """SolvePPM_DE of every grid of a level in one batch (device tensors)."""
         P = make_params(hp, dt, learned_guess, dt_device)
+        P.number_of_colours = len(colour_names(fields_list[0]))
         arr, keep = self._level(grids, fields_list, accels)
         st = Stats()
         rc = self.L.ppm_b200_solve_level(self.h, C.byref(P), int(cycle), arr, len(grids),

@@ -42,6 +42,9 @@ extern "C" {
 #define PPM_B200_MEM_HOST 0   /* fields in host memory: copied in and out inside the call (like cuPPMSetBaryon/GetBaryon) */
 #define PPM_B200_MEM_DEVICE 1 /* fields already resident in device memory */
 
+/* MAX_COLOR (fortran.def:2): the most colour fields a sweep advects */
+#define PPM_B200_MAX_COLOURS 45
+
 /* Riemann solver / reconstruction enums, values as in Enzo's typedefs.h */
 #define PPM_B200_RIEMANN_TWOSHOCK 5
 #define PPM_B200_RECONSTRUCTION_PPM 1
@@ -68,7 +71,9 @@ typedef struct ppm_b200_params {
   int conservative_rec;     /* ConservativeReconstruction: must be 0 */
   int positive_rec;         /* PositiveReconstruction: must be 0 */
   int eos_type;             /* EOSType: must be 0 */
-  int number_of_colours;    /* NumberOfColours: must be 0 */
+  int number_of_colours;    /* NumberOfColours: 0 .. PPM_B200_MAX_COLOURS advected colour fields
+                               (Grid_SolveHydroEquations.C:90-285); their fields are
+                               ppm_b200_grid.colours[] */
   int learned_guess;        /* 1: start twoshock's Newton iteration from the learned p* guess
                                (weights from ppm_b200_set_guess) */
   const double *dt_device;  /* optional: device pointer holding dtFixed (overrides dt) */
@@ -89,6 +94,9 @@ typedef struct ppm_b200_grid {
   double *gas_energy;       /* BaryonField[GENum] */
   const double *acceleration[3]; /* AccelerationField[dim] */
   const double *cell_width[3];   /* CellWidthTemp[dim]: HOST arrays of dims[dim] values */
+  double *const *colours;        /* HOST array of params->number_of_colours field pointers,
+                                    BaryonField[colnum[n]] in colnum[] order; the fields
+                                    are updated in place (NULL when there are none) */
 } ppm_b200_grid;
 
 /* struct fluxes (Fluxes.h:29-37) restricted to the six hydro slots.
@@ -100,6 +108,12 @@ typedef struct ppm_b200_fluxes {
   long long right_start[3][3], right_end[3][3];
   double *left[6][3];
   double *right[6][3];
+  /* colours: HOST arrays of number_of_colours * 3 pointers, entry n*3 + dim =
+     LeftFluxes/RightFluxes[colnum[n]][dim] (NULL arrays or entries are skipped).  Like
+     the reference these hold colf / dx: dt * ub * colour, divided by the cell width
+     (Grid_xEulerSweep.C:361-371 after euler.F:173-176). */
+  double *const *colour_left;
+  double *const *colour_right;
 } ppm_b200_fluxes;
 
 typedef struct ppm_b200_stats {

@@ -19,6 +19,15 @@ HERE = Path(__file__).resolve().parent
 LIB_PATH = HERE / "_build" / "libppm_oracle.so"
 
 FIELD_NAMES = ("d", "te", "v1", "v2", "v3", "ge")
+MAX_COLOUR = 45  # MAX_COLOR, fortran.def:2
+
+
+def colour_names(fields):
+    """Colour fields of a field dict: keys col0, col1, ... (the colnum[] order)."""
+    n = 0
+    while f"col{n}" in fields:
+        n += 1
+    return [f"col{k}" for k in range(n)]
 
 
 class OraParams(C.Structure):
@@ -41,6 +50,7 @@ class OraParams(C.Structure):
         ("max_velocity_index", C.c_int),
         ("steepen", C.c_int),
         ("flatten", C.c_int),
+        ("ncolour", C.c_int),
     ]
 
 
@@ -52,6 +62,8 @@ class OraFluxes(C.Structure):
         ("right_end", (C.c_longlong * 3) * 3),
         ("left", (C.POINTER(C.c_double) * 3) * 6),
         ("right", (C.POINTER(C.c_double) * 3) * 6),
+        ("colour_left", (C.POINTER(C.c_double) * 3) * MAX_COLOUR),
+        ("colour_right", (C.POINTER(C.c_double) * 3) * MAX_COLOUR),
     ]
 
 
@@ -90,11 +102,11 @@ def lib():
             build()
         L = C.CDLL(str(LIB_PATH))
         dp = C.POINTER(C.c_double)
-        L.ora_solve_ppm_de.argtypes = [C.POINTER(OraParams), C.c_int, dp * 6, dp * 3, dp * 3,
+        L.ora_solve_ppm_de.argtypes = [C.POINTER(OraParams), C.c_int, C.c_void_p, dp * 3, dp * 3,
                                        C.c_int, C.POINTER(OraFluxes), C.c_longlong * 3,
                                        C.POINTER(OraStats), C.c_int]
         L.ora_solve_ppm_de.restype = C.c_int
-        L.ora_sweep.argtypes = [C.c_int, C.POINTER(OraParams), dp * 6, dp, dp * 3, dp * 3,
+        L.ora_sweep.argtypes = [C.c_int, C.POINTER(OraParams), C.c_void_p, dp, dp * 3, dp * 3,
                                 C.c_int, C.POINTER(OraFluxes), C.c_longlong * 3,
                                 C.POINTER(OraStats), C.c_int]
         L.ora_sweep.restype = C.c_int
@@ -124,7 +136,7 @@ def _ptr(a):
     return a.ctypes.data_as(C.POINTER(C.c_double))
 
 
-def make_params(grid, hp, dt) -> OraParams:
+def make_params(grid, hp, dt, ncolour=0) -> OraParams:
     """grid: object with rank, dims(3), start(3), end(3); hp: HydroParams-like."""
     P = OraParams()
     P.rank = grid.rank
@@ -146,6 +158,7 @@ def make_params(grid, hp, dt) -> OraParams:
     P.max_velocity_index = grid.rank
     P.steepen = int(getattr(hp, "steepen", 0))
     P.flatten = int(getattr(hp, "flatten", 0))
+    P.ncolour = int(ncolour)
     return P
 
 
@@ -154,6 +167,15 @@ def _fields6(fields):
     for i, n in enumerate(FIELD_NAMES):
         arr[i] = _ptr(fields.get(n))
     return arr
+
+
+def _fields_all(fields):
+    """The six hydro fields, then the colour fields (kept alive by the returned array)."""
+    cols = colour_names(fields)
+    arr = (C.POINTER(C.c_double) * (6 + len(cols)))()
+    for i, n in enumerate(FIELD_NAMES + tuple(cols)):
+        arr[i] = _ptr(fields.get(n))
+    return arr, len(cols)
 
 
 def _cw3(cellwidth):
@@ -169,7 +191,8 @@ def solve_ppm_de(grid, hp, dt, cycle, fields, cellwidth, accel=None, subgrids=No
 
     Returns (rc, stats dict).  subgrids: list of OraFluxes (filled in place)."""
     L = lib()
-    P = make_params(grid, hp, dt)
+    F, ncol = _fields_all(fields)
+    P = make_params(grid, hp, dt, ncol)
     acc = (C.POINTER(C.c_double) * 3)()
     if accel is not None:
         for d in range(3):
@@ -180,7 +203,7 @@ def solve_ppm_de(grid, hp, dt, cycle, fields, cellwidth, accel=None, subgrids=No
     if nsub:
         subarr = (OraFluxes * nsub)(*subgrids)
     g = (C.c_longlong * 3)(*ggs)
-    rc = L.ora_solve_ppm_de(C.byref(P), int(cycle), _fields6(fields), acc, _cw3(cellwidth), nsub,
+    rc = L.ora_solve_ppm_de(C.byref(P), int(cycle), F, acc, _cw3(cellwidth), nsub,
                             subarr, g, C.byref(st), int(nthreads))
     if nsub:
         for i in range(nsub):
@@ -190,14 +213,15 @@ def solve_ppm_de(grid, hp, dt, cycle, fields, cellwidth, accel=None, subgrids=No
 
 def sweep(dim, grid, hp, dt, fields, pressure, cellwidth, accel=None, nthreads=1):
     L = lib()
-    P = make_params(grid, hp, dt)
+    F, ncol = _fields_all(fields)
+    P = make_params(grid, hp, dt, ncol)
     acc = (C.POINTER(C.c_double) * 3)()
     if accel is not None:
         for d in range(3):
             acc[d] = _ptr(accel[d])
     st = OraStats()
     g = (C.c_longlong * 3)(0, 0, 0)
-    rc = L.ora_sweep(int(dim), C.byref(P), _fields6(fields), _ptr(pressure), acc,
+    rc = L.ora_sweep(int(dim), C.byref(P), F, _ptr(pressure), acc,
                      _cw3(cellwidth), 0, None, g, C.byref(st), int(nthreads))
     return rc, st.as_dict()
 

@@ -22,6 +22,9 @@
 /* fortran_types.def (CONFIG_PFLOAT_8): tiny = 1e-20, huge = 1e20 */
 #define F_TINY 1.0e-20
 #define F_HUGE 1.0e+20
+/* fortran.def:8 and euler.F:104-105 (a Fortran parameter, folded in FP64) */
+#define F_COLOR_FLOOR 1.0e-35
+static const double F_MIN_COLOR = 1.0e-5 * F_TINY;
 /* twoshock.F:97-106 (CONFIG_BFLOAT_8) */
 #define TS_TOLERANCE 1.0e-14
 #define TS_NUMITER 8
@@ -77,9 +80,16 @@ typedef struct {
   /* calcdiss / steepening locals */
   double *flat, *steep, *wflag, *ftemp, *d2d, *dxb;
   double *block;
+  /* colours (ncolour > 0): slices colslice/colls/colrs/colf of (idim, jdim, ncolor), and
+     the (ijkn, MAX_COLOR) locals of inteuler (dcol coll colr col6 colla colra coll0
+     colr0) and flux_twoshock (colb), ncolor columns each */
+  int ncol;
+  double *col, *colls, *colrs, *colf;
+  double *dcol, *coll, *colr, *col6, *colla, *colra, *coll0, *colr0, *colb;
+  double *cblock;
 } work_t;
 
-static int work_alloc(work_t *W, int idim, int jdim) {
+static int work_alloc(work_t *W, int idim, int jdim, int ncol) {
   memset(W, 0, sizeof(*W));
   W->idim = idim;
   W->jdim = jdim;
@@ -127,13 +137,30 @@ static int work_alloc(work_t *W, int idim, int jdim) {
   for (size_t k = 0; k < n_one; ++k) TAKE(*one[k], n1);
 #undef TAKE
   W->niter = W->mask + n1;
+  W->ncol = ncol;
+  if (ncol > 0) {
+    const size_t nc = (size_t)ncol;
+    W->cblock = (double *)calloc(4 * nc * ns + 9 * nc * n1, sizeof(double));
+    if (!W->cblock) return -1;
+    double *c = W->cblock;
+    double **sl[] = {&W->col, &W->colls, &W->colrs, &W->colf};
+    for (int k = 0; k < 4; k++) { *sl[k] = c; c += nc * ns; }
+    double **on[] = {&W->dcol, &W->coll, &W->colr, &W->col6, &W->colla, &W->colra,
+                     &W->coll0, &W->colr0, &W->colb};
+    for (int k = 0; k < 9; k++) { *on[k] = c; c += nc * n1; }
+  }
   return 0;
 }
 
 static void work_free(work_t *W) {
   free(W->block);
   free(W->mask);
+  free(W->cblock);
 }
+
+/* colour n's slice and (ijkn) locals */
+#define CS(a, i, j, n) (a)[(size_t)(n) * (size_t)idim * (size_t)W->jdim + ((size_t)(j)-1) * (size_t)idim + ((size_t)(i)-1)]
+#define CV(a, i, n) (a)[(size_t)(n) * ((size_t)idim + 4) + ((size_t)(i)-1)]
 
 /* ------------------------------------------------------------------------ */
 /* intvar.F:5-179 (one pencil)                                               */
@@ -382,6 +409,12 @@ static void inteuler(work_t *W, const ora_params *P, const double *dxi, int i1, 
       intvar(gesl, idim, i1, i2, 0, W->steep, ifl, W->flat, W->c1, W->c2, W->c3, W->c4, W->c5,
              W->c6, W->char1, W->char2, W->c0, W->dge, W->gel, W->ger, W->ge6, W->gela,
              W->gera, W->gel0, W->ger0);
+    /* colours, inteuler.F:276-282 (no steepening, the slice's flattening) */
+    for (int n = 0; n < W->ncol; n++)
+      intvar(&CS(W->col, 1, j, n), idim, i1, i2, 0, W->steep, ifl, W->flat, W->c1, W->c2,
+             W->c3, W->c4, W->c5, W->c6, W->char1, W->char2, W->c0, &CV(W->dcol, 1, n),
+             &CV(W->coll, 1, n), &CV(W->colr, 1, n), &CV(W->col6, 1, n), &CV(W->colla, 1, n),
+             &CV(W->colra, 1, n), &CV(W->coll0, 1, n), &CV(W->colr0, 1, n));
     /* characteristic domain-of-dependence averages, inteuler.F:304-316 */
     for (i = i1; i <= i2 + 1; i++) {
       V(W->plm, i) = V(W->pr, i - 1) - V(W->cm, i - 1) * (V(W->dp, i - 1) - (1.0 - ft * V(W->cm, i - 1)) * V(W->p6, i - 1));
@@ -474,12 +507,27 @@ static void inteuler(work_t *W, const ora_params *P, const double *dxi, int i1, 
         S(W->gers, i, j) = V(W->ger0, i);
       }
     }
+    /* colour states scaled by the corrected density, inteuler.F:436-450 */
+    for (int n = 0; n < W->ncol; n++) {
+      for (i = i1; i <= i2 + 1; i++) {
+        if (V(usl, i - 1) <= 0.0)
+          CS(W->colls, i, j, n) = CV(W->colla, i, n) * S(W->dls, i, j) / V(W->dla, i);
+        else
+          CS(W->colls, i, j, n) = CV(W->coll0, i, n) * S(W->dls, i, j) / V(W->dl0, i);
+        if (V(usl, i) >= 0.0)
+          CS(W->colrs, i, j, n) = CV(W->colra, i, n) * S(W->drs, i, j) / V(W->dra, i);
+        else
+          CS(W->colrs, i, j, n) = CV(W->colr0, i, n) * S(W->drs, i, j) / V(W->dr0, i);
+      }
+    }
     /* dual-energy hypersonic override, inteuler.F:493-521 */
     if (P->dual == 1) {
       for (i = i1; i <= i2 + 1; i++) {
         double ml = fmax2(fmax2(fabs(V(W->cm, i - 1)), fabs(V(W->c0, i - 1))), fabs(V(W->cp, i - 1)));
         if (gamma * V(W->pla, i) / V(W->dla, i) < eta2 * (V(W->ula, i) * V(W->ula, i)) ||
             ml < 1.0e-3 || S(W->dls, i, j) / V(W->dla, i) > 5.0) {
+          for (int n = 0; n < W->ncol; n++)
+            CS(W->colls, i, j, n) = CS(W->colls, i, j, n) * V(W->dla, i) / S(W->dls, i, j);
           S(W->pls, i, j) = V(W->pla, i);
           S(W->uls, i, j) = V(W->ula, i);
           S(W->dls, i, j) = V(W->dla, i);
@@ -487,6 +535,8 @@ static void inteuler(work_t *W, const ora_params *P, const double *dxi, int i1, 
         double mr = fmax2(fmax2(fabs(V(W->cm, i)), fabs(V(W->c0, i))), fabs(V(W->cp, i)));
         if (gamma * V(W->pra, i) / V(W->dra, i) < eta2 * (V(W->ura, i) * V(W->ura, i)) ||
             mr < 1.0e-3 || S(W->drs, i, j) / V(W->dra, i) > 5.0) {
+          for (int n = 0; n < W->ncol; n++)
+            CS(W->colrs, i, j, n) = CS(W->colrs, i, j, n) * V(W->dra, i) / S(W->drs, i, j);
           S(W->prs, i, j) = V(W->pra, i);
           S(W->urs, i, j) = V(W->ura, i);
           S(W->drs, i, j) = V(W->dra, i);
@@ -499,6 +549,12 @@ static void inteuler(work_t *W, const ora_params *P, const double *dxi, int i1, 
       S(W->prs, i, j) = fmax2(S(W->prs, i, j), F_TINY);
       S(W->dls, i, j) = fmax2(S(W->dls, i, j), F_TINY);
       S(W->drs, i, j) = fmax2(S(W->drs, i, j), F_TINY);
+    }
+    for (int n = 0; n < W->ncol; n++) {  /* inteuler.F:546-551 */
+      for (i = i1; i <= i2 + 1; i++) {
+        CS(W->colls, i, j, n) = fmax2(CS(W->colls, i, j, n), F_COLOR_FLOOR);
+        CS(W->colrs, i, j, n) = fmax2(CS(W->colrs, i, j, n), F_COLOR_FLOOR);
+      }
     }
     if (P->pressure_free == 1) {
       for (i = i1; i <= i2 + 1; i++) {
@@ -715,12 +771,22 @@ static int flux_hll_cell(work_t *W, const ora_params *P, const double *dx, int i
     S(W->ef, ii, j) = qc * fl[f][4];
     if (P->dual == 1) S(W->gef, ii, j) = dt / V(dx, ii) * fl[f][5];
   }
+  /* colours: bm0 = gesl, bp0 = gesr (flux_hll.F:236-262, :328-332) */
+  for (int n = 0; n < W->ncol; n++) {
+    for (f = 0; f < 2; f++) {
+      const int ii = i + f;
+      const double colfl = gl[f] * CS(W->colls, ii, j, n);
+      const double colfr = gr[f] * CS(W->colrs, ii, j, n);
+      CS(W->colf, ii, j, n) = sl[f] * colfl + sr[f] * colfr;
+      CS(W->colf, ii, j, n) = dt * CS(W->colf, ii, j, n);
+    }
+  }
   if (S(W->d, i, j) + S(W->df, i, j) - S(W->df, i + 1, j) <= 0.0) return -1;
   return 0;
 }
 
 /* ------------------------------------------------------------------------ */
-/* flux_twoshock.F:6-490 (RAREFACTION2, no diffusion, no colours)            */
+/* flux_twoshock.F:6-490 (RAREFACTION2, no diffusion)                        */
 /* ------------------------------------------------------------------------ */
 static int flux_twoshock(work_t *W, const ora_params *P, const double *dx, int i1, int i2,
                          int j1, int j2, ora_stats *st) {
@@ -788,6 +854,15 @@ static int flux_twoshock(work_t *W, const ora_params *P, const double *dx, int i
         V(W->geb, i) = S(W->gers, i, j);
       }
     }
+    /* colours at the Godunov state, flux_twoshock.F:251-259 */
+    for (int n = 0; n < W->ncol; n++) {
+      for (i = i1; i <= i2 + 1; i++) {
+        if (V(W->ub, i) > 0.0)
+          CV(W->colb, i, n) = CS(W->colls, i, j, n) * V(W->db, i) / S(W->dls, i, j);
+        else
+          CV(W->colb, i, n) = CS(W->colrs, i, j, n) * V(W->db, i) / S(W->drs, i, j);
+      }
+    }
     for (i = i1; i <= i2 + 1; i++) {
       V(W->eb, i) = V(W->pb, i) / ((gamma - 1.0) * V(W->db, i)) +
                     0.5 * (V(W->ub, i) * V(W->ub, i) + V(W->vb, i) * V(W->vb, i) + V(W->wb, i) * V(W->wb, i));
@@ -810,6 +885,10 @@ static int flux_twoshock(work_t *W, const ora_params *P, const double *dx, int i
       S(W->vf, i, j) = qc * V(W->duvb, i);
       S(W->wf, i, j) = qc * V(W->duwb, i);
     }
+    /* colour fluxes times dt only, flux_twoshock.F:375-380 */
+    for (int n = 0; n < W->ncol; n++)
+      for (i = i1; i <= i2 + 1; i++)
+        CS(W->colf, i, j, n) = dt * V(W->ub, i) * CV(W->colb, i, n);
     if (P->dual == 1) {
       for (i = i1; i <= i2 + 1; i++)
         V(W->pcent, i) = fmax2((gamma - 1.0) * S(W->ge, i, j) * S(W->d, i, j), F_TINY);
@@ -842,9 +921,10 @@ static int flux_twoshock(work_t *W, const ora_params *P, const double *dx, int i
 
 /* ------------------------------------------------------------------------ */
 /* euler.F:7-285 (GRAVITY_METHOD1, no second-order gravity correction,       */
-/* no diffusion, no colours)                                                 */
+/* no diffusion)                                                             */
 /* ------------------------------------------------------------------------ */
-static int euler(work_t *W, const ora_params *P, int i1, int i2, int j1, int j2, ora_stats *st) {
+static int euler(work_t *W, const ora_params *P, const double *dx, int i1, int i2, int j1, int j2,
+                 ora_stats *st) {
   const int idim = W->idim;
   const double dt = P->dt, dfloor = P->small_rho;
   int i, j, rc = 0;
@@ -882,6 +962,15 @@ static int euler(work_t *W, const ora_params *P, int i1, int i2, int j1, int j2,
         S(W->e, i, j) = fmax2(S(W->e, i, j), F_TINY);
       }
     }
+    /* colours, euler.F:171-186: colf divided by dx in place (the subgrid flux capture
+       reads it afterwards), then the advective update with its floor */
+    for (int n = 0; n < W->ncol; n++)
+      for (i = i1; i <= i2 + 1; i++) CS(W->colf, i, j, n) = CS(W->colf, i, j, n) / V(dx, i);
+    for (int n = 0; n < W->ncol; n++)
+      for (i = i1; i <= i2; i++) {
+        CS(W->col, i, j, n) = CS(W->col, i, j, n) + (CS(W->colf, i, j, n) - CS(W->colf, i + 1, j, n));
+        CS(W->col, i, j, n) = fmax2(CS(W->col, i, j, n), F_MIN_COLOR);
+      }
     for (i = i1; i <= i2; i++) S(W->d, i, j) = V(W->dnu, i);
   }
   return rc;
@@ -966,7 +1055,7 @@ static inline size_t gidx(const int *GD, int dim, int a, int b, int s) {
   return ((size_t)ijk[2] * (size_t)GD[1] + (size_t)ijk[1]) * (size_t)GD[0] + (size_t)ijk[0];
 }
 
-static int sweep_slice(work_t *W, int dim, int s, const ora_params *P, double *const F[ORA_NFIELD],
+static int sweep_slice(work_t *W, int dim, int s, const ora_params *P, double *const F[],
                        const double *pressure, double *const accel[3], double *const cw[3],
                        int nsub, ora_fluxes *sub, const long long ggs[3], ora_stats *st) {
   const int *GD = P->dims;
@@ -993,6 +1082,8 @@ static int sweep_slice(work_t *W, int dim, int s, const ora_params *P, double *c
       W->w[l] = hw ? F[vw][g] : 0.0;
       if (P->gravity) W->gr[l] = accel[dim][g];
       if (P->dual) W->ge[l] = F[ORA_GE][g];
+      for (int n = 0; n < W->ncol; n++)  /* Grid_xEulerSweep.C:124-132 */
+        W->col[(size_t)n * (size_t)idim * (size_t)jdim + l] = F[ORA_NFIELD + n][g];
     }
   }
   const int is = P->start[dim] + 1, ie = P->end[dim] + 1, js = 1, je = jdim;
@@ -1001,7 +1092,7 @@ static int sweep_slice(work_t *W, int dim, int s, const ora_params *P, double *c
   inteuler(W, P, dx, is, ie, js, je);
   twoshock(W, P, is, ie + 1, js, je, st);
   if (flux_twoshock(W, P, dx, is, ie, js, je, st) != 0) rc = -1;
-  if (euler(W, P, is, ie, js, je, st) != 0) rc = -1;
+  if (euler(W, P, dx, is, ie, js, je, st) != 0) rc = -1;
   if (P->dual) pgas2d_dual(W, P, is - 3, ie + 3, js, je);
 
   /* subgrid flux capture, Grid_xEulerSweep.C:313-377 */
@@ -1049,6 +1140,11 @@ static int sweep_slice(work_t *W, int dim, int s, const ora_params *P, double *c
         fx->left[ORA_GE][dim][offset] = W->gef[li];
         fx->right[ORA_GE][dim][offset] = W->gef[ri];
       }
+      for (int n = 0; n < W->ncol; n++) {  /* Grid_xEulerSweep.C:361-371 */
+        const size_t cn = (size_t)n * (size_t)idim * (size_t)jdim;
+        if (fx->colour_left[n][dim]) fx->colour_left[n][dim][offset] = W->colf[cn + li];
+        if (fx->colour_right[n][dim]) fx->colour_right[n][dim][offset] = W->colf[cn + ri];
+      }
     }
   }
 
@@ -1063,12 +1159,14 @@ static int sweep_slice(work_t *W, int dim, int s, const ora_params *P, double *c
       if (hv) F[vv][g] = W->v[l];
       if (hw) F[vw][g] = W->w[l];
       if (P->dual) F[ORA_GE][g] = W->ge[l];
+      for (int n = 0; n < W->ncol; n++)
+        F[ORA_NFIELD + n][g] = W->col[(size_t)n * (size_t)idim * (size_t)jdim + l];
     }
   }
   return rc;
 }
 
-int ora_sweep(int dim, const ora_params *P, double *const F[ORA_NFIELD], const double *pressure,
+int ora_sweep(int dim, const ora_params *P, double *const F[], const double *pressure,
               double *const accel[3], double *const cw[3], int nsub, ora_fluxes *sub,
               const long long ggs[3], ora_stats *st, int nthreads) {
   int nd, sd;
@@ -1086,7 +1184,7 @@ int ora_sweep(int dim, const ora_params *P, double *const F[ORA_NFIELD], const d
       work_t W;
       ora_stats lst;
       memset(&lst, 0, sizeof(lst));
-      if (work_alloc(&W, P->dims[dim], P->dims[nd]) != 0) {
+      if (work_alloc(&W, P->dims[dim], P->dims[nd], P->ncolour) != 0) {
         err |= 1;
       } else {
 #pragma omp for schedule(dynamic, 1)
@@ -1112,14 +1210,14 @@ int ora_sweep(int dim, const ora_params *P, double *const F[ORA_NFIELD], const d
   }
 #endif
   work_t W;
-  if (work_alloc(&W, P->dims[dim], P->dims[nd]) != 0) return -2;
+  if (work_alloc(&W, P->dims[dim], P->dims[nd], P->ncolour) != 0) return -2;
   for (int s = 0; s < nslices; s++)
     if (sweep_slice(&W, dim, s, P, F, pressure, accel, cw, nsub, sub, ggs, st) != 0) rc = -1;
   work_free(&W);
   return rc;
 }
 
-int ora_solve_ppm_de(const ora_params *P, int cycle, double *const F[ORA_NFIELD],
+int ora_solve_ppm_de(const ora_params *P, int cycle, double *const F[],
                      double *const accel[3], double *const cw[3], int nsub, ora_fluxes *sub,
                      const long long ggs[3], ora_stats *st, int nthreads) {
   ora_params Q = *P;

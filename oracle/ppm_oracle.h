@@ -12,6 +12,9 @@
  *   grid::SolvePPM_DE          src/enzo/Grid_SolvePPM_DE.C:36-164
  *   grid::{x,y,z}EulerSweep    src/enzo/Grid_{x,y,z}EulerSweep.C
  *   inteuler / intvar          src/enzo/inteuler.F:5-566, intvar.F:5-179
+ *   (colour fields: inteuler.F:276-282, :436-450, :500-515, :546-551,
+ *    flux_twoshock.F:251-259, :375-380, flux_hll.F:236-262, euler.F:171-186,
+ *    Grid_xEulerSweep.C:124-132, :361-371, :409-416)
  *   twoshock                   src/enzo/twoshock.F:5-276
  *   flux_twoshock / flux_hll   src/enzo/flux_twoshock.F:6-490, flux_hll.F:6-415
  *   euler                      src/enzo/euler.F:7-285
@@ -36,6 +39,10 @@ extern "C" {
 
 /* field slots, in BaryonField roles */
 enum { ORA_D = 0, ORA_TE = 1, ORA_V1 = 2, ORA_V2 = 3, ORA_V3 = 4, ORA_GE = 5, ORA_NFIELD = 6 };
+/* MAX_COLOR (fortran.def:2): colour fields follow the six hydro fields in the field
+   array, fields[ORA_NFIELD + n] for n < ncolour (the colnum[] list of
+   Grid_SolveHydroEquations.C:90-285, in that order) */
+#define ORA_MAX_COLOUR 45
 
 typedef struct {
   int rank;            /* GridRank (1..3) */
@@ -55,6 +62,7 @@ typedef struct {
   int max_velocity_index; /* MaxVelocityIndex used by ComputePressure */
   int steepen;         /* PPMSteepeningParameter (0 or 1: density steepening) */
   int flatten;         /* PPMFlatteningParameter (0, 1 or 3) */
+  int ncolour;         /* NumberOfColours: advected colour fields after the hydro fields */
 } ora_params;
 
 /* struct fluxes (src/enzo/Fluxes.h:29-37), restricted to the six hydro slots */
@@ -63,6 +71,9 @@ typedef struct {
   long long right_start[3][3], right_end[3][3];
   double *left[ORA_NFIELD][3];
   double *right[ORA_NFIELD][3];
+  /* LeftFluxes/RightFluxes[colnum[n]][dim] of the colour fields (NULL: not captured) */
+  double *colour_left[ORA_MAX_COLOUR][3];
+  double *colour_right[ORA_MAX_COLOUR][3];
 } ora_fluxes;
 
 typedef struct {
@@ -82,14 +93,15 @@ void ora_compute_pressure(const ora_params *P, double *const fields[ORA_NFIELD],
 
 /* One directional sweep over all slices of the grid (dim 0,1,2), i.e. the
    `for k ... xEulerSweep(k)` loop of Grid_SolvePPM_DE.C:91-97 and its y/z
-   siblings.  accel may be NULL when gravity is off. */
-int ora_sweep(int dim, const ora_params *P, double *const fields[ORA_NFIELD],
+   siblings.  accel may be NULL when gravity is off.  fields: the six hydro fields,
+   then P->ncolour colour fields. */
+int ora_sweep(int dim, const ora_params *P, double *const fields[],
               const double *pressure, double *const accel[3],
               double *const cellwidth[3], int nsub, ora_fluxes *sub,
               const long long ggs[3], ora_stats *st, int nthreads);
 
 /* grid::SolvePPM_DE (Grid_SolvePPM_DE.C:36-164), EOSType = 0. */
-int ora_solve_ppm_de(const ora_params *P, int cycle, double *const fields[ORA_NFIELD],
+int ora_solve_ppm_de(const ora_params *P, int cycle, double *const fields[],
                      double *const accel[3], double *const cellwidth[3],
                      int nsub, ora_fluxes *sub, const long long ggs[3],
                      ora_stats *st, int nthreads);

@@ -40,16 +40,38 @@ def test_version_and_error_strings():
 
 def test_unsupported_configuration_is_rejected_before_any_device_work():
     # Options outside this library (flattening type 2, diffusion, steepening other than
-    # 0/1): the caller keeps the Fortran path.  The context pointer is never touched.
+    # 0/1, more colours than MAX_COLOR): the caller keeps the Fortran path.  The context
+    # pointer is never touched.
     L = capi.lib()
     from ppm_b200 import harness as H
     g = H.Grid.uniform((8, 8, 8))
     hp = H.HydroParams()
     f = H.new_fields(g, False)
-    for field, value in (("flattening", 2), ("diffusion", 1), ("steepening", 2)):
+    for field, value in (("flattening", 2), ("diffusion", 1), ("steepening", 2),
+                         ("number_of_colours", 46), ("number_of_colours", -1)):
         P = capi.make_params(hp, 0.1)
         setattr(P, field, value)
         G, keep = capi.make_grid(g, f)
         rc = L.ppm_b200_solve_ppm_de(C.c_void_p(1), C.byref(P), 0, C.byref(G), 0, 0, None, None,
                                      None)
         assert rc == capi.ERR_UNSUPPORTED, field
+
+
+def test_colours_without_field_pointers_are_invalid():
+    # number_of_colours > 0 needs grid.colours with that many non-NULL fields; the check
+    # precedes any use of the context
+    L = capi.lib()
+    from ppm_b200 import harness as H
+    g = H.Grid.uniform((8, 8, 8))
+    f = H.new_fields(g, False)
+    P = capi.make_params(H.HydroParams(), 0.1)
+    P.number_of_colours = 2
+    G, keep = capi.make_grid(g, f)
+    rc = L.ppm_b200_solve_ppm_de(C.c_void_p(1), C.byref(P), 0, C.byref(G), 0, 0, None, None,
+                                 None)
+    assert rc == capi.ERR_INVALID
+    arr = (C.c_void_p * 2)(f["d"].ctypes.data, None)
+    G.colours = C.cast(arr, C.c_void_p)
+    rc = L.ppm_b200_solve_ppm_de(C.c_void_p(1), C.byref(P), 0, C.byref(G), 0, 0, None, None,
+                                 None)
+    assert rc == capi.ERR_INVALID
