@@ -59,7 +59,15 @@ def parse():
     ap.add_argument("--level-patches", type=int, default=600)
     ap.add_argument("--no-learned", action="store_true",
                     help="skip the learned-Newton-start comparison")
+    ap.add_argument("--colours", type=int, default=0,
+                    help="advect this many colour fields (NumberOfColours; mass fractions "
+                         "of the density) with the workload; 0 = the headline workload")
     return ap.parse_args()
+
+
+def colour_fractions(n):
+    """Positive mass fractions of the density for the workload's colour fields."""
+    return [1.0 / (k + 2) for k in range(n)]
 
 
 def workload_config(args):
@@ -71,7 +79,8 @@ def workload_config(args):
         "step": "SolvePPM_DE (pressure, 3 sweeps, calc_dt of the next cycle folded into the "
                 "last sweep) + periodic ghost fill",
         "l2": "inputs larger than L2 (13 fields x 144 MB resident per GPU)",
-        "bytes_per_zone_update": BYTES_PER_ZONE_UPDATE,
+        "bytes_per_zone_update": BYTES_PER_ZONE_UPDATE + 3 * 16 * args.colours,
+        **({"colours": args.colours} if args.colours else {}),
     }
 
 
@@ -169,7 +178,7 @@ def committed_traffic():
 
 
 # ---------------------------------------------------------------- CPU reference (oracle port)
-def cpu_reference_rate(size, seed, nthreads, min_seconds=10.0, max_steps=12):
+def cpu_reference_rate(size, seed, nthreads, min_seconds=10.0, max_steps=12, colours=0):
     """Times the C restatement of the Fortran path (the oracle) on the host cores: steps
     of the same workload until min_seconds of SolvePPM_DE time (at least 2 steps).
     Returns (zone-updates/s, seconds, steps)."""
@@ -178,6 +187,8 @@ def cpu_reference_rate(size, seed, nthreads, min_seconds=10.0, max_steps=12):
     hp = H.HydroParams(gamma=5.0 / 3.0, cfl=0.4, dual=True)
     g = H.Grid.uniform((size, size, size))
     f = H.turbulence(g, hp, mach=3.0, seed=seed)
+    for k, frac in enumerate(colour_fractions(colours)):
+        f[f"col{k}"] = frac * f["d"]
     times = []
     for cyc in range(max_steps):
         if cyc >= 2 and sum(times) >= min_seconds:
@@ -205,6 +216,8 @@ def run_reference(args):
     import oracle as O
     g = H.Grid.uniform((sample,) * 3)
     f = H.turbulence(g, hp, mach=3.0, seed=args.seed)
+    for k, frac in enumerate(colour_fractions(args.colours)):
+        f[f"col{k}"] = frac * f["d"]
     total = 0.0
     for cyc in range(args.warmup + args.steps):
         p = O.compute_pressure(g, hp, f)
@@ -411,6 +424,8 @@ def run_ours(args):
     hp = H.HydroParams(gamma=5.0 / 3.0, cfl=0.4, dual=True)
     g = H.Grid.uniform((args.size,) * 3)
     f_host = H.turbulence(g, hp, mach=3.0, seed=args.seed + rank)
+    for k, frac in enumerate(colour_fractions(args.colours)):  # +16 B per colour and sweep
+        f_host[f"col{k}"] = frac * f_host["d"]
     fields = {k: torch.from_numpy(v).to(dev) for k, v in f_host.items()}
     dt_dev = torch.zeros(1, dtype=torch.float64, device=dev)
     periodic = ("periodic",) * 3
@@ -477,7 +492,7 @@ def run_ours(args):
     # cell (every field read once and written once), over its average duration
     peak, peak_src = measured_peak_hbm()
     avg_sweep_s = sweep_ms * 1e-3 / max(nsweep, 1)
-    achieved = BYTES_PER_SWEEP_CELL * cells / avg_sweep_s / 1e9
+    achieved = (BYTES_PER_SWEEP_CELL + 16 * args.colours) * cells / avg_sweep_s / 1e9
     tr, tr_src = committed_traffic()
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": (tr * cells if tr else None),
@@ -533,7 +548,8 @@ def run_ours(args):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         nthreads = os.cpu_count() or 1
-        rate, secs, nst = cpu_reference_rate(args.size, args.seed, nthreads)
+        rate, secs, nst = cpu_reference_rate(args.size, args.seed, nthreads,
+                                             colours=args.colours)
         cpu = {"value": rate, "unit": UNIT, "cores": nthreads, "kind": "port",
                "sample": f"the same {args.size}^3 turbulence workload, {nst} SolvePPM_DE "
                          f"steps, {nthreads} threads ({secs:.1f} s); C restatement of the "

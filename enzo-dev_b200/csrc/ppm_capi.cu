@@ -1668,26 +1668,63 @@ int ppm_b200_compute_timestep_level(ppm_b200_context* ctx, const ppm_b200_params
   return timestep_batch(ctx, p, io, courant, aye, vgrid, dt_device, dt_host);
 }
 
+// Colour fields of a level as extra element records of six fields each, with their
+// grid's geometry, so that the ghost-fill and zone-copy kernels treat them like the
+// hydro fields.  Record order: the ng grids, then grid k's colour chunks at
+// ng + k * colour_chunks(nc) + c.
+int colour_chunks(int nc) { return (nc + 5) / 6; }
+
+void append_colour_records(std::vector<GridIO>& io, int ng, int nc) {
+  const int nch = colour_chunks(nc);
+  for (int k = 0; k < ng; ++k)
+    for (int c = 0; c < nch; ++c) {
+      GridIO x{};
+      x.g = io[k].g;
+      for (int j = 0; j < 6; ++j) {
+        const int n = 6 * c + j;
+        x.user.f[j] = n < nc ? io[k].user.col[n] : nullptr;
+      }
+      io.push_back(x);
+    }
+}
+
+// the fields a ghost fill or zone copy moves: hydro fields, and colours when nc > 0
+int check_fill_grid(const ppm_b200_grid* g, int dual_energy, int nc) {
+  if (!g->density || !g->total_energy || !g->velocity[0]) return PPM_B200_ERR_INVALID;
+  for (int d = 1; d < g->rank; ++d)
+    if (!g->velocity[d]) return PPM_B200_ERR_INVALID;
+  if (dual_energy && !g->gas_energy) return PPM_B200_ERR_INVALID;
+  if (nc < 0 || nc > PPM_B200_MAX_COLOURS) return PPM_B200_ERR_INVALID;
+  if (nc > 0) {
+    if (!g->colours) return PPM_B200_ERR_INVALID;
+    for (int n = 0; n < nc; ++n)
+      if (!g->colours[n]) return PPM_B200_ERR_INVALID;
+  }
+  return PPM_B200_OK;
+}
+
 static int boundary_batch(ppm_b200_context* ctx, ppm_b200_grid* grids, int ngrids,
-                          int dual_energy, const int bc_type[3]) {
+                          int dual_energy, int ncolour, const int bc_type[3]) {
   if (!ctx || !grids || ngrids <= 0 || !bc_type) return PPM_B200_ERR_INVALID;
   for (int d = 0; d < 3; ++d)
     if (bc_type[d] < 0 || bc_type[d] > 2) return PPM_B200_ERR_INVALID;
+  for (int k = 0; k < ngrids; ++k) {
+    int rc = check_fill_grid(&grids[k], dual_energy, ncolour);
+    if (rc) return rc;
+  }
   CK(cudaSetDevice(ctx->device));
   ppm_b200_params p;
   std::memset(&p, 0, sizeof(p));
   p.dual_energy = dual_energy;
+  p.number_of_colours = ncolour;
   std::vector<GridIO> io(ngrids);
   for (int k = 0; k < ngrids; ++k) {
-    ppm_b200_grid* g = &grids[k];
-    if (!g->density || !g->total_energy || !g->velocity[0]) return PPM_B200_ERR_INVALID;
-    for (int d = 1; d < g->rank; ++d)
-      if (!g->velocity[d]) return PPM_B200_ERR_INVALID;
-    if (dual_energy && !g->gas_energy) return PPM_B200_ERR_INVALID;
-    io[k].g = g;
-    int rc = stage_in(ctx, &p, g, PPM_B200_MEM_DEVICE, io[k].user, io[k].acc);
+    io[k].g = &grids[k];
+    int rc = stage_in(ctx, &p, &grids[k], PPM_B200_MEM_DEVICE, io[k].user, io[k].acc, true);
     if (rc) return rc;
   }
+  append_colour_records(io, ngrids, ncolour);
+  p.dual_energy = 1;  // keep every record's sixth field (a grid's is null unless dual)
   ElemPlan ep;
   int rc = prepare_elem(ctx, kSlotBoundary, &p, io, false, bc_type, ep);
   if (rc) return rc;
@@ -1741,18 +1778,15 @@ static void copy_boxes(const ppm_b200_grid* grids, int ngrids, const long long* 
 
 static int copy_zones_level(ppm_b200_context* ctx, ppm_b200_grid* grids, int ngrids,
                             const long long* left, const long long domain[3],
-                            const int periodic[3], int dual_energy) {
+                            const int periodic[3], int dual_energy, int ncolour) {
   if (!ctx || ngrids < 0 || (ngrids > 0 && (!grids || !left)) || !domain || !periodic)
     return PPM_B200_ERR_INVALID;
   if (ngrids == 0) return PPM_B200_OK;
   const int rank = grids[0].rank;
   for (int k = 0; k < ngrids; ++k) {
-    ppm_b200_grid* g = &grids[k];
-    if (g->rank != rank || !g->density || !g->total_energy || !g->velocity[0])
-      return PPM_B200_ERR_INVALID;
-    for (int d = 1; d < g->rank; ++d)
-      if (!g->velocity[d]) return PPM_B200_ERR_INVALID;
-    if (dual_energy && !g->gas_energy) return PPM_B200_ERR_INVALID;
+    if (grids[k].rank != rank) return PPM_B200_ERR_INVALID;
+    int rc = check_fill_grid(&grids[k], dual_energy, ncolour);
+    if (rc) return rc;
   }
   for (int d = 0; d < rank; ++d)
     if (domain[d] <= 0) return PPM_B200_ERR_INVALID;
@@ -1763,12 +1797,26 @@ static int copy_zones_level(ppm_b200_context* ctx, ppm_b200_grid* grids, int ngr
   ppm_b200_params p;
   std::memset(&p, 0, sizeof(p));
   p.dual_energy = dual_energy;
+  p.number_of_colours = ncolour;
   std::vector<GridIO> io(ngrids);
   for (int k = 0; k < ngrids; ++k) {
     io[k].g = &grids[k];
-    int rc = stage_in(ctx, &p, &grids[k], PPM_B200_MEM_DEVICE, io[k].user, io[k].acc);
+    int rc = stage_in(ctx, &p, &grids[k], PPM_B200_MEM_DEVICE, io[k].user, io[k].acc, true);
     if (rc) return rc;
   }
+  if (ncolour > 0) {  // every box again for each colour chunk of its two grids
+    append_colour_records(io, ngrids, ncolour);
+    const int nch = colour_chunks(ncolour);
+    const size_t nb = boxes.size();
+    for (int c = 0; c < nch; ++c)
+      for (size_t b = 0; b < nb; ++b) {
+        ppm::CopyBox x = boxes[b];
+        x.dst = ngrids + x.dst * nch + c;
+        x.src = ngrids + x.src * nch + c;
+        boxes.push_back(x);
+      }
+  }
+  p.dual_energy = 1;  // keep every record's sixth field (a grid's is null unless dual)
   ElemPlan ep;
   int rc = prepare_elem(ctx, kSlotCopy, &p, io, false, nullptr, ep);
   if (rc) return rc;
@@ -2133,19 +2181,20 @@ int ppm_b200_guess_eval(ppm_b200_context* ctx, const float* features, long long 
 }
 
 int ppm_b200_set_boundary(ppm_b200_context* ctx, ppm_b200_grid* g, int dual_energy,
-                          const int bc_type[3]) {
-  return boundary_batch(ctx, g, 1, dual_energy, bc_type);
+                          int number_of_colours, const int bc_type[3]) {
+  return boundary_batch(ctx, g, 1, dual_energy, number_of_colours, bc_type);
 }
 
 int ppm_b200_set_boundary_level(ppm_b200_context* ctx, ppm_b200_grid* grids, int ngrids,
-                                int dual_energy, const int bc_type[3]) {
-  return boundary_batch(ctx, grids, ngrids, dual_energy, bc_type);
+                                int dual_energy, int number_of_colours, const int bc_type[3]) {
+  return boundary_batch(ctx, grids, ngrids, dual_energy, number_of_colours, bc_type);
 }
 
 int ppm_b200_copy_zones_level(ppm_b200_context* ctx, ppm_b200_grid* grids, int ngrids,
                               const long long* left, const long long domain[3],
-                              const int periodic[3], int dual_energy) {
-  return copy_zones_level(ctx, grids, ngrids, left, domain, periodic, dual_energy);
+                              const int periodic[3], int dual_energy, int number_of_colours) {
+  return copy_zones_level(ctx, grids, ngrids, left, domain, periodic, dual_energy,
+                          number_of_colours);
 }
 
 int ppm_b200_debug_tma_stall(ppm_b200_context* ctx, int extra_bytes) {

@@ -777,6 +777,15 @@ __device__ __noinline__ void hll_fallback(const SweepArgs& a, int64_t pid, int64
   const FaceState s1 = load_face<DUAL>(a, (int64_t)(c + 1 - is) * np + pid);
   const HllFace h0 = hll_face<DUAL>(s0, P);
   const HllFace h1 = hll_face<DUAL>(s1, P);
+  if (a.fcol) {  // the colour kernel's HLL weights of faces c and c+1 (flux_hll.F:236-262)
+    const int64_t plane = a.plane;
+    double* w0 = a.fcol + (int64_t)(c - is) * np + pid;
+    double* w1 = w0 + np;
+    w0[CHSL * plane] = h0.sl; w0[CHBM * plane] = h0.gesl;
+    w0[CHSR * plane] = h0.sr; w0[CHBP * plane] = h0.gesr;
+    w1[CHSL * plane] = h1.sl; w1[CHBM * plane] = h1.gesl;
+    w1[CHSR * plane] = h1.sr; w1[CHBP * plane] = h1.gesr;
+  }
   HllFace h2 = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
   if (c + 2 <= ie + 1) h2 = hll_face<DUAL>(load_face<DUAL>(a, (int64_t)(c + 2 - is) * np + pid), P);
   const double qcc = P.dt / a.coef[c].dx;
@@ -1012,7 +1021,7 @@ __device__ __forceinline__ bool update_pencil(const SweepArgs& a, int64_t pid, c
             bool fatal = false;
             cnt.fallbacks += 1;
             hll_fallback<DUAL>(a, pid, base, t, Cn, P, F0, F1, ges_n, govv_next, fatal);
-            if (a.fhll) {  // the colour kernel recomputes these faces' colour fluxes
+            if (a.fhll) {  // these faces' colour fluxes are HLL's (weights in fcol)
               a.fhll[(int64_t)(t - is) * np + pid] = 1;
               a.fhll[(int64_t)(t + 1 - is) * np + pid] = 1;
             }
@@ -1253,8 +1262,8 @@ __global__ void __launch_bounds__(128) fallback_kernel(const __grid_constant__ B
 }
 
 // ------------------------------------------------------------------ stage 5 (colours)
-// The colour fields of the sweep (NumberOfColours > 0), one thread per (pencil, colour),
-// marching like the reconstruction: each colour's PPM parabola (intvar with the
+// The colour fields of the sweep (NumberOfColours > 0), one thread per (pencil, chunk of
+// colours), marching like the reconstruction: each colour's PPM parabola (intvar with the
 // slice's flattening and no steepening, inteuler.F:276-282), its face states scaled by
 // the corrected density and undone with the dual-energy override (inteuler.F:436-450,
 // :500-515) and floored (:546-551), the flux at the Godunov state
@@ -1263,17 +1272,27 @@ __global__ void __launch_bounds__(128) fallback_kernel(const __grid_constant__ B
 // capture of that quotient (Grid_xEulerSweep.C:361-371), and the update with its floor
 // (euler.F:178-186), written in place: a cell is read three steps before it is written
 // and never read again.
-// Blocks: (march block, colour) with the colour fastest, so that the blocks of one
+// Blocks: (march block, colour chunk) with the chunk fastest, so that the blocks of one
 // pencil block run together and share their density, pressure, velocity and face reads
-// through L2.
+// through L2; within a thread the colours of a chunk share them outright.
+#ifndef PPM_COLOUR_MINBLOCKS
+#define PPM_COLOUR_MINBLOCKS 4
+#endif
+#ifndef PPM_COLOURS_PER_THREAD
+#define PPM_COLOURS_PER_THREAD 2
+#endif
 constexpr double kColourFloor = 1.0e-35;        // color_floor, fortran.def:8
 constexpr double kMinColour = 1.0e-5 * kTiny;   // min_color, euler.F:104-105
 
-template <bool DUAL, bool ONE>
-__global__ void __launch_bounds__(kMarchThreads) colour_kernel(const __grid_constant__ BatchArgs B) {
+// CPT colours per thread: each thread marches one pencil for colours c0 .. c0+CPT-1 of
+// its block's chunk, sharing the cell and face data between them.
+template <bool DUAL, bool ONE, int CPT>
+__global__ void __launch_bounds__(kMarchThreads, PPM_COLOUR_MINBLOCKS)
+    colour_kernel(const __grid_constant__ BatchArgs B) {
   const int nc = B.ncolour;
-  const int64_t mb = blockIdx.x / nc;
-  const int colour = (int)(blockIdx.x - mb * nc);
+  const int nchunk = (nc + CPT - 1) / CPT;
+  const int64_t mb = blockIdx.x / nchunk;
+  const int chunk = (int)(blockIdx.x - mb * nchunk);
   int64_t lb = mb;
   const int g = ONE ? 0 : batch_locate(B.march_prefix, B.ngrids, mb, lb);
   PPM_BIND_RECORD(a, g)
@@ -1284,7 +1303,11 @@ __global__ void __launch_bounds__(kMarchThreads) colour_kernel(const __grid_cons
   const int64_t sa = a.sa;
   const int is = a.is, ie = a.ie;
   const int64_t np = a.npencils, plane = a.plane;
-  double* const q = a.col[colour];
+  const int c0 = chunk * CPT;
+  const int ncol = nc - c0 < CPT ? nc - c0 : CPT;  // colours of this chunk
+  double* q[CPT];
+#pragma unroll
+  for (int u = 0; u < CPT; ++u) q[u] = u < ncol ? a.col[c0 + u] : nullptr;
 
   int64_t cap = 0, cap_end = 0;
   if (a.ncaptures > 0) {
@@ -1297,88 +1320,123 @@ __global__ void __launch_bounds__(kMarchThreads) colour_kernel(const __grid_cons
     while (cap_end < a.ncaptures && a.captures[cap_end].pencil == pid) ++cap_end;
   }
 
-  double wq0 = 0.0, wq1 = 0.0, wq2 = 0.0;  // colour of cells t-3, t-2, t-1
-  double dqm1 = 0.0, qlm1 = 0.0;           // dq(t-2), ql(t-2)
+  double wq0[CPT], wq1[CPT], wq2[CPT];  // colour of cells t-3, t-2, t-1
+  double dqm1[CPT], qlm1[CPT];          // dq(t-2), ql(t-2)
+  double colla[CPT], coll0[CPT];        // left data of face t-2
+  double fm[CPT];                       // colf / dx of face t-3
+#pragma unroll
+  for (int u = 0; u < CPT; ++u)
+    wq0[u] = wq1[u] = wq2[u] = dqm1[u] = qlm1[u] = colla[u] = coll0[u] = fm[u] = 0.0;
   double wu0 = 0.0, wu1 = 0.0, wu2 = 0.0;  // normal velocity of cells t-3, t-2, t-1
   Prep prA = {0, 0, 0, 0, 0}, prB = {0, 0, 0, 0, 0};  // cells t-2, t-1
-  double colla = 0.0, coll0 = 0.0;         // left data of face t-2
-  double fm = 0.0;                         // colf / dx of face t-3
   const int tend = ie + 3;
 #pragma unroll 1
   for (int t = 0; t <= tend; ++t) {
     const int64_t off = base + (int64_t)t * sa;
-    const double nq = q[off];
+    double nq[CPT];
+#pragma unroll
+    for (int u = 0; u < CPT; ++u) nq[u] = u < ncol ? q[u][off] : 0.0;
     const double nu = ldg0(a.in_u, off);
     Prep prC = prB;
     if (t >= is - 1 && t <= ie + 1)
       prC = cell_prep(__ldg(a.in_d + off), __ldg(a.pres + off), nu, a.coef[t].dx2i, P);
-    double dqN = 0.0, qlN = 0.0;  // slope and left edge of cell t-1
+    double dqN[CPT], qlN[CPT];  // slope and left edge of cell t-1
+#pragma unroll
+    for (int u = 0; u < CPT; ++u) dqN[u] = qlN[u] = 0.0;
     {
       const int c = t - 1;
       if (c >= is - 2 && c <= ie + 2) {
         const Coef cf = a.coef[c];
-        dqN = pm_slope(wq1, wq2, nq, cf.c1, cf.c2);
-        if (c >= is - 1) qlN = pm_edge(wq1, wq2, dqm1, dqN, cf.c3, cf.c4, cf.c5, cf.c6);
+#pragma unroll
+        for (int u = 0; u < CPT; ++u) {
+          dqN[u] = pm_slope(wq1[u], wq2[u], nq[u], cf.c1, cf.c2);
+          if (c >= is - 1) qlN[u] = pm_edge(wq1[u], wq2[u], dqm1[u], dqN[u], cf.c3, cf.c4, cf.c5, cf.c6);
+        }
       }
     }
     {
       const int c = t - 2;  // parabola of cell c; face c
       if (c >= is - 1 && c <= ie + 1) {
-        Para pa;
-        if (a.flatten != 0) {
-          const double fl = a.flat[(int64_t)(c - (is - 1)) * np + pid];
-          pa = pm_parabola<false, true>(wq0, wq1, wq2, qlm1, qlN, 0.0, 0.0, 0.0, fl);
-        } else {
-          pa = pm_parabola(wq0, wq1, wq2, qlm1, qlN);
-        }
+        const double fl = a.flatten != 0 ? a.flat[(int64_t)(c - (is - 1)) * np + pid] : 0.0;
+        Para pa[CPT];
+#pragma unroll
+        for (int u = 0; u < CPT; ++u)
+          pa[u] = a.flatten != 0
+                      ? pm_parabola<false, true>(wq0[u], wq1[u], wq2[u], qlm1[u], qlN[u], 0.0,
+                                                 0.0, 0.0, fl)
+                      : pm_parabola(wq0[u], wq1[u], wq2[u], qlm1[u], qlN[u]);
         if (c >= is) {
           const int64_t fidx = (int64_t)(c - is) * np + pid;
           const double* fc = a.fcol + fidx;
-          const double colra = pm_C(pa, prA.char2), colr0 = pm_B(pa, prA.c0);
-          const double dla = fc[CDLA * plane], dra = fc[CDRA * plane];
+          const double dla = fc[CDLA * plane], dl0 = fc[CDL0 * plane];
+          const double dra = fc[CDRA * plane], dr0 = fc[CDR0 * plane];
           const double dlc = fc[CDLC * plane], drc = fc[CDRC * plane];
-          double cls = (wu0 <= 0.0) ? colla * dlc / dla : coll0 * dlc / fc[CDL0 * plane];
-          double crs = (wu1 >= 0.0) ? colra * drc / dra : colr0 * drc / fc[CDR0 * plane];
           const double ov = fc[COVR * plane];
-          if (ov == 1.0 || ov == 3.0) cls = cls * dla / dlc;
-          if (ov >= 2.0) crs = crs * dra / drc;
-          cls = dmax(cls, kColourFloor);
-          crs = dmax(crs, kColourFloor);
-          double cf;
-          if (a.fhll[fidx]) {
-            const HllFace h = hll_face<DUAL>(load_face<DUAL>(a, fidx), P);
-            cf = h.sl * (h.gesl * cls) + h.sr * (h.gesr * crs);
-            cf = P.dt * cf;
+          const bool ovl = ov == 1.0 || ov == 3.0, ovr = ov >= 2.0;
+          const bool hll = a.fhll[fidx] != 0;
+          double w[4] = {0.0, 0.0, 0.0, 0.0};
+          double ub = 0.0, db = 0.0, dsl = 1.0, dsr = 1.0;
+          if (hll) {  // the HLL weights the fallback pass left (sl, bm0, sr, bp0)
+            w[0] = fc[CHSL * plane];
+            w[1] = fc[CHBM * plane];
+            w[2] = fc[CHSR * plane];
+            w[3] = fc[CHBP * plane];
           } else {
-            const double ub = a.fflux[XUB * plane + fidx];
-            const double db = fc[CDB * plane];
-            const double colb = ub > 0.0 ? cls * db / a.fstate[SDL * plane + fidx]
-                                         : crs * db / a.fstate[SDR * plane + fidx];
-            cf = P.dt * ub * colb;
+            ub = a.fflux[XUB * plane + fidx];
+            db = fc[CDB * plane];
+            if (ub > 0.0) dsl = a.fstate[SDL * plane + fidx];
+            else dsr = a.fstate[SDR * plane + fidx];
           }
-          cf = cf / a.coef[c].dx;
-          while (cap < cap_end && a.captures[cap].face <= c) {
-            const FluxCapture& rq = a.captures[cap];
-            if (rq.face == c) a.col_capture[(rq.dst / 6) * nc + colour] = cf;
-            ++cap;
+          const double dx = a.coef[c].dx;
+          int64_t cq = cap;  // this face's capture requests (the same for every colour)
+#pragma unroll
+          for (int u = 0; u < CPT; ++u) {
+            if (u >= ncol) break;
+            const double colra = pm_C(pa[u], prA.char2), colr0 = pm_B(pa[u], prA.c0);
+            double cls = (wu0 <= 0.0) ? colla[u] * dlc / dla : coll0[u] * dlc / dl0;
+            double crs = (wu1 >= 0.0) ? colra * drc / dra : colr0 * drc / dr0;
+            if (ovl) cls = cls * dla / dlc;
+            if (ovr) crs = crs * dra / drc;
+            cls = dmax(cls, kColourFloor);
+            crs = dmax(crs, kColourFloor);
+            double cf;
+            if (hll) {
+              cf = w[0] * (w[1] * cls) + w[2] * (w[3] * crs);
+              cf = P.dt * cf;
+            } else {
+              const double colb = ub > 0.0 ? cls * db / dsl : crs * db / dsr;
+              cf = P.dt * ub * colb;
+            }
+            cf = cf / dx;
+            for (cq = cap; cq < cap_end && a.captures[cq].face <= c; ++cq) {
+              const FluxCapture& rq = a.captures[cq];
+              if (rq.face == c) a.col_capture[(rq.dst / 6) * nc + c0 + u] = cf;
+            }
+            if (c - 1 >= is && c - 1 <= ie) {
+              const double v = wq0[u] + (fm[u] - cf);
+              q[u][base + (int64_t)(c - 1) * sa] = dmax(v, kMinColour);
+            }
+            fm[u] = cf;
           }
-          if (c - 1 >= is && c - 1 <= ie) {
-            const double v = wq0 + (fm - cf);
-            q[base + (int64_t)(c - 1) * sa] = dmax(v, kMinColour);
-          }
-          fm = cf;
+          cap = cq;
         }
         if (c <= ie) {
-          colla = pm_A(pa, prA.char1);
-          coll0 = pm_A(pa, prA.c0);
+#pragma unroll
+          for (int u = 0; u < CPT; ++u) {
+            colla[u] = pm_A(pa[u], prA.char1);
+            coll0[u] = pm_A(pa[u], prA.c0);
+          }
         }
       }
     }
-    wq0 = wq1;
-    wq1 = wq2;
-    wq2 = nq;
-    dqm1 = dqN;
-    qlm1 = qlN;
+#pragma unroll
+    for (int u = 0; u < CPT; ++u) {
+      wq0[u] = wq1[u];
+      wq1[u] = wq2[u];
+      wq2[u] = nq[u];
+      dqm1[u] = dqN[u];
+      qlm1[u] = qlN[u];
+    }
     wu0 = wu1;
     wu1 = wu2;
     wu2 = nu;
@@ -1447,9 +1505,11 @@ void launch_stages(const BatchArgs& B, int64_t march_blocks, int64_t riemann_blo
     launch_update<DUAL, GRAV, ONE, false, false>(B, march_blocks, st);
   mark(4);
   fallback_kernel<DUAL, GRAV, ONE><<<64, 128, 0, st>>>(B);
-  if (B.ncolour > 0)
-    colour_kernel<DUAL, ONE>
-        <<<(unsigned)(march_blocks * B.ncolour), kMarchThreads, 0, st>>>(B);
+  if (B.ncolour > 0) {
+    constexpr int cpt = PPM_COLOURS_PER_THREAD;
+    const int64_t chunks = (B.ncolour + cpt - 1) / cpt;
+    colour_kernel<DUAL, ONE, cpt><<<(unsigned)(march_blocks * chunks), kMarchThreads, 0, st>>>(B);
+  }
   mark(5);
 }
 

@@ -111,8 +111,9 @@ struct SweepArgs {
 enum { kFaceVars = 12, kFluxVars = 7 };
 // colour face planes: dla dl0 dra dr0 (the density's characteristic averages), the
 // corrected densities before the dual-energy override, the override flags (1 left,
-// 2 right) and the Godunov density db
-enum { CDLA = 0, CDL0, CDRA, CDR0, CDLC, CDRC, COVR, CDB, kColVars };
+// 2 right), the Godunov density db, and on faces the HLL fallback replaced its weights
+// sl, bm0, sr, bp0 (written by the fallback pass only there)
+enum { CDLA = 0, CDL0, CDRA, CDR0, CDLC, CDRC, COVR, CDB, CHSL, CHBM, CHSR, CHBP, kColVars };
 enum { kMaxColours = 45 };  // MAX_COLOR (fortran.def:2)
 
 // Threads per block of the marching stages and of the face-parallel Riemann stage.

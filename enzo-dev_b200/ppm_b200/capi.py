@@ -138,7 +138,8 @@ def lib(build_if_missing: bool = True):
     L.ppm_b200_compute_timestep.argtypes = [vp, C.POINTER(Params), C.POINTER(GridDesc), C.c_int,
                                             C.c_double, C.c_double, C.POINTER(C.c_double),
                                             vp, C.POINTER(C.c_double)]
-    L.ppm_b200_set_boundary.argtypes = [vp, C.POINTER(GridDesc), C.c_int, C.POINTER(C.c_int)]
+    L.ppm_b200_set_boundary.argtypes = [vp, C.POINTER(GridDesc), C.c_int, C.c_int,
+                                        C.POINTER(C.c_int)]
     L.ppm_b200_synchronize.argtypes = [vp, C.POINTER(Stats)]
     L.ppm_b200_launch_count.argtypes = [vp]
     L.ppm_b200_launch_count.restype = C.c_longlong
@@ -174,7 +175,7 @@ def lib(build_if_missing: bool = True):
                                                   C.POINTER(C.c_double)]
     L.ppm_b200_copy_zones_level.argtypes = [vp, C.POINTER(GridDesc), C.c_int,
                                             C.POINTER(C.c_longlong), C.c_longlong * 3,
-                                            C.c_int * 3, C.c_int]
+                                            C.c_int * 3, C.c_int, C.c_int]
     L.ppm_b200_copy_zones_level.restype = C.c_int
     L.ppm_b200_correct_fluxes.argtypes = [vp, C.POINTER(Params), C.POINTER(GridDesc), C.c_int,
                                           C.c_int, C.POINTER(Fluxes), C.POINTER(Fluxes),
@@ -183,7 +184,7 @@ def lib(build_if_missing: bool = True):
     L.ppm_b200_debug_tma_stall.argtypes = [vp, C.c_int]
     L.ppm_b200_debug_tma_stall.restype = C.c_int
     L.ppm_b200_set_boundary_level.argtypes = [vp, C.POINTER(GridDesc), C.c_int, C.c_int,
-                                              C.POINTER(C.c_int)]
+                                              C.c_int, C.POINTER(C.c_int)]
     L.ppm_b200_profile_read.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]
     for name in EXPORTS:
         fn = getattr(L, name)
@@ -398,9 +399,11 @@ class Context:
         return out.value
 
     def set_boundary(self, grid, fields, dual, bc=("periodic",) * 3):
+        """Ghost fill of the hydro fields and of the colours (keys col0, col1, ...)."""
         G, keep = make_grid(grid, fields)
         codes = (C.c_int * 3)(*[BC_CODES[b] for b in bc])
-        rc = self.L.ppm_b200_set_boundary(self.h, C.byref(G), int(bool(dual)), codes)
+        rc = self.L.ppm_b200_set_boundary(self.h, C.byref(G), int(bool(dual)),
+                                          len(colour_names(fields)), codes)
         if rc != OK:
             raise PPMError(rc, "ppm_b200_set_boundary")
 
@@ -420,7 +423,7 @@ class Context:
                     dt_device=None, check=True, learned_guess=False):
         """SolvePPM_DE of every grid of a level in one batch (device tensors)."""
         P = make_params(hp, dt, learned_guess, dt_device)
-        P.number_of_colours = len(colour_names(fields_list[0]))
+        P.number_of_colours = len(colour_names(fields_list[0])) if fields_list else 0
         arr, keep = self._level(grids, fields_list, accels)
         st = Stats()
         rc = self.L.ppm_b200_solve_level(self.h, C.byref(P), int(cycle), arr, len(grids),
@@ -452,7 +455,9 @@ class Context:
     def set_boundary_level(self, grids, fields_list, dual, bc=("periodic",) * 3):
         arr, keep = self._level(grids, fields_list)
         codes = (C.c_int * 3)(*[BC_CODES[b] for b in bc])
-        rc = self.L.ppm_b200_set_boundary_level(self.h, arr, len(grids), int(bool(dual)), codes)
+        nc = len(colour_names(fields_list[0])) if fields_list else 0
+        rc = self.L.ppm_b200_set_boundary_level(self.h, arr, len(grids), int(bool(dual)), nc,
+                                                codes)
         if rc != OK:
             raise PPMError(rc, "ppm_b200_set_boundary_level")
 
@@ -485,8 +490,9 @@ class Context:
         lf = (C.c_longlong * (3 * len(grids)))(*[int(v) for l in left for v in list(l) + [0] * (3 - len(l))])
         dom = (C.c_longlong * 3)(*[int(v) for v in list(domain) + [1] * (3 - len(domain))])
         per = (C.c_int * 3)(*[int(bool(v)) for v in list(periodic) + [0] * (3 - len(periodic))])
+        nc = len(colour_names(fields_list[0])) if fields_list else 0
         rc = self.L.ppm_b200_copy_zones_level(self.h, arr, len(grids), lf, dom, per,
-                                              int(bool(dual)))
+                                              int(bool(dual)), nc)
         if rc != OK:
             raise PPMError(rc, "ppm_b200_copy_zones_level")
 

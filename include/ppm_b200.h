@@ -171,7 +171,7 @@ int ppm_b200_compute_timestep(ppm_b200_context *ctx, const ppm_b200_params *para
    external-boundary part of SetBoundaryConditions for a single grid
    (ExternalBoundary_SetExternalBoundaryIO.C:201-209, :378-386). */
 int ppm_b200_set_boundary(ppm_b200_context *ctx, ppm_b200_grid *grid, int dual_energy,
-                          const int bc_type[3]);
+                          int number_of_colours, const int bc_type[3]);
 
 /* The time step of the next cycle, folded into every later solve on this context:
    the last sweep's update kernel evaluates calc_dt (ihydro = 0, calc_dt.F:136-153 with
@@ -212,7 +212,7 @@ int ppm_b200_compute_timestep_level(ppm_b200_context *ctx, const ppm_b200_params
 
 /* ppm_b200_set_boundary on every grid of a list, one launch. */
 int ppm_b200_set_boundary_level(ppm_b200_context *ctx, ppm_b200_grid *grids, int ngrids,
-                                int dual_energy, const int bc_type[3]);
+                                int dual_energy, int number_of_colours, const int bc_type[3]);
 
 /* grid::CopyZonesFromGrid (Grid_CopyZonesFromGrid.C:37-300, without the shearing box)
    over a level, the sibling and periodic part of SetBoundaryConditions
@@ -227,7 +227,7 @@ int ppm_b200_set_boundary_level(ppm_b200_context *ctx, ppm_b200_grid *grids, int
    most one copy; all copies run as one launch on device fields. */
 int ppm_b200_copy_zones_level(ppm_b200_context *ctx, ppm_b200_grid *grids, int ngrids,
                               const long long *left, const long long domain[3],
-                              const int periodic[3], int dual_energy);
+                              const int periodic[3], int dual_energy, int number_of_colours);
 
 /* grid::CorrectForRefinedFluxes (Grid_CorrectForRefinedFluxes.C:38-760) for the proper
    subgrids of one grid: Cartesian coordinates, the six hydro fields (no species or

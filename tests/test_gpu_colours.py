@@ -236,3 +236,52 @@ def test_colour_subgrid_fluxes_match_oracle(ctx):
                 a, b = bg["colour_" + side][n][dim], bo["colour_" + side][n][dim]
                 assert np.any(a != 0.0)
                 assert np.array_equal(a, b), ("colour", side, n, dim)
+
+
+@pytest.mark.parametrize("bc", ["periodic", "outflow"])
+def test_ghost_fill_moves_colours(ctx, bc):
+    # SetBoundaryConditions fills every baryon field, colours included
+    torch = pytest.importorskip("torch")
+    rng = np.random.default_rng(3)
+    grids, host = [], []
+    for shape in ((12, 10, 8), (9, 7, 11), (16, 6, 5)):
+        g = H.Grid.uniform(shape)
+        f = H.new_fields(g, True)
+        for k in f:
+            f[k][...] = rng.standard_normal(f[k].shape)
+        add_colours(g, f, seed=int(rng.integers(1000)), extra=9)  # 12 colours: two chunks
+        grids.append(g)
+        host.append(f)
+    dev = [{k: torch.from_numpy(v.copy()).cuda() for k, v in f.items()} for f in host]
+    ctx.set_boundary(grids[0], dev[0], True, (bc,) * 3)
+    ctx.set_boundary_level(grids[1:], dev[1:], True, (bc,) * 3)
+    torch.cuda.synchronize()
+    for g, f, d in zip(grids, host, dev):
+        ref = copy_fields(f)
+        H.fill_ghosts(g, ref, bc)
+        for k in ref:
+            assert np.array_equal(d[k].cpu().numpy(), ref[k]), k
+
+
+def test_zone_copies_move_colours(ctx):
+    torch = pytest.importorskip("torch")
+    from test_gpu_copy_zones import TILED, copy_zones_host
+    domain = (24, 20, 16)
+    rng = np.random.default_rng(8)
+    grids, left, host = [], [], []
+    for box in TILED:
+        g = H.Grid.uniform(tuple(hi - lo for lo, hi in box))
+        f = H.new_fields(g, True)
+        for k in f:
+            f[k][...] = rng.standard_normal(f[k].shape)
+        add_colours(g, f, seed=int(rng.integers(1000)), extra=5)  # 8 colours
+        grids.append(g)
+        left.append([box[d][0] - H.NGHOST for d in range(3)])
+        host.append(f)
+    dev = [{k: torch.from_numpy(v.copy()).cuda() for k, v in f.items()} for f in host]
+    ctx.copy_zones_level(grids, dev, left, domain, (1, 1, 1), True)
+    torch.cuda.synchronize()
+    ref = copy_zones_host(grids, host, left, domain, (1, 1, 1))
+    for k in range(len(grids)):
+        for name in ref[k]:
+            assert np.array_equal(dev[k][name].cpu().numpy(), ref[k][name]), (k, name)
