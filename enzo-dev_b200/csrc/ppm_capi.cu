@@ -326,7 +326,10 @@ int check_supported(const ppm_b200_params* p) {
   if ((p->flattening != 0 && p->flattening != 1 && p->flattening != 3) ||
       (p->steepening != 0 && p->steepening != 1))
     return PPM_B200_ERR_UNSUPPORTED;
-  if (p->riemann_solver != PPM_B200_RIEMANN_TWOSHOCK) return PPM_B200_ERR_UNSUPPORTED;
+  // the solver switch of Grid_xEulerSweep.C:223-283 (two-shock, HLL, HLLC)
+  if (p->riemann_solver != PPM_B200_RIEMANN_TWOSHOCK && p->riemann_solver != PPM_B200_RIEMANN_HLL &&
+      p->riemann_solver != PPM_B200_RIEMANN_HLLC)
+    return PPM_B200_ERR_UNSUPPORTED;
   if (p->reconstruction != PPM_B200_RECONSTRUCTION_PPM) return PPM_B200_ERR_UNSUPPORTED;
   return PPM_B200_OK;
 }
@@ -600,6 +603,12 @@ size_t colour_planes(const ppm_b200_params* p) {
   return p->number_of_colours > 0 ? (size_t)ppm::kColVars : 0;
 }
 
+// SweepArgs::solver of a RiemannSolver value: 0 two-shock, 1 HLL, 2 HLLC
+int solver_code(const ppm_b200_params* p) {
+  return p->riemann_solver == PPM_B200_RIEMANN_HLL ? 1
+         : p->riemann_solver == PPM_B200_RIEMANN_HLLC ? 2 : 0;
+}
+
 // kernels one sweep launches: reconstruct x2, Riemann, update, fallback, and the
 // corrections and colour kernels when present
 int sweep_kernels(const ppm_b200_params* p) {
@@ -746,7 +755,9 @@ int prepare_sweep(ppm_b200_context* ctx, int dim, int position, const ppm_b200_p
     a.eta2 = p->eta2;
     a.small_rho = p->small_rho;
     a.pmin = p->tiny_number;
-    a.fallback = p->riemann_fallback;
+    // HLL has no fallback: a negative density stops the reference (flux_hll.F:378-380)
+    a.solver = solver_code(p);
+    a.fallback = p->riemann_solver == PPM_B200_RIEMANN_HLL ? 0 : p->riemann_fallback;
     a.guess = p->learned_guess ? (const uint32_t*)ctx->guess.p : nullptr;
     if (ctx->log && !p->learned_guess) {
       a.log = ctx->log;
@@ -828,6 +839,7 @@ int prepare_sweep(ppm_b200_context* ctx, int dim, int position, const ppm_b200_p
   plan.B.x_tma_extra_tx = plan.B.x_tma ? ctx->debug_tma_extra : 0u;
   plan.B.corrections = correction_planes(p) > 0 ? 1 : 0;
   plan.B.ncolour = nc;
+  plan.B.solver = solver_code(p);
   plan.B.hll_flags = nc > 0 ? flags : nullptr;
   plan.B.hll_bytes = (int64_t)flag_bytes;
   plan.B.grids = (const SweepArgs*)base;
@@ -1265,6 +1277,7 @@ std::string graph_key(ppm_b200_context* ctx, const ppm_b200_params* p, const Sol
     key_put(k, b.x_tma_extra_tx);
     key_put(k, b.corrections);
     key_put(k, b.ncolour);
+    key_put(k, b.solver);
     key_put(k, b.hll_flags);
     key_put(k, b.hll_bytes);
     key_put(k, ctx->mirror[kSlotSweep0 + 3 * sp.order[s] + s].version);

@@ -502,6 +502,83 @@ __device__ __forceinline__ HllFace hll_face(const FaceState& s, const Phys& P) {
   return h;
 }
 
+// ------------------------------- flux_hllc.F:105-300 for one face (no diffusion, HLLC)
+// The HLLC weights sl, sr (the star region's side by the contact speed cw), the advective
+// speeds gesl = ul - bm, gesr = ur - bp, and the fluxes before the dt/dx factor with the
+// contact's momentum and energy terms (:282-286) included.
+template <bool DUAL>
+__device__ __forceinline__ HllFace hllc_face(const FaceState& s, const Phys& P) {
+  const double gamma = P.gamma;
+  const double gamma1 = gamma - 1.0;
+  const double gamma1i = 1.0 / gamma1;
+  double sqrtdl = sqrt(s.dl);
+  double sqrtdr = sqrt(s.dr);
+  double isdlpdr = 1.0 / (sqrtdl + sqrtdr);
+  double vroe1 = (sqrtdl * s.ul + sqrtdr * s.ur) * isdlpdr;
+  double vroe2 = (sqrtdl * s.vl + sqrtdr * s.vr) * isdlpdr;
+  double vroe3 = (sqrtdl * s.wl + sqrtdr * s.wr) * isdlpdr;
+  double v2 = vroe1 * vroe1 + vroe2 * vroe2 + vroe3 * vroe3;
+  double el = gamma1i * s.pl + 0.5 * s.dl * (s.ul * s.ul + s.vl * s.vl + s.wl * s.wl);
+  double er = gamma1i * s.pr + 0.5 * s.dr * (s.ur * s.ur + s.vr * s.vr + s.wr * s.wr);
+  double hroe = ((el + s.pl) / sqrtdl + (er + s.pr) / sqrtdr) * isdlpdr;
+  double cs = sqrt(gamma1 * dmax((hroe - 0.5 * v2), kTiny));
+  double char1 = vroe1 - cs;
+  double char2 = vroe1 + cs;
+  double csl0 = sqrt(gamma * s.pl / s.dl);
+  double csr0 = sqrt(gamma * s.pr / s.dr);
+  double csl = dmin(s.ul - csl0, char1);
+  double csr = dmax(s.ur + csr0, char2);
+  double bm = dmin(csl, 0.0);
+  double bp = dmax(csr, 0.0);
+  // contact speed cw and pressure cp (flux_hllc.F:160-183)
+  double tl = s.pl - (csl - s.ul) * s.dl * s.ul;
+  double tr = s.pr - (csr - s.ur) * s.dr * s.ur;
+  double dl = s.dl * (csl - s.ul);
+  double dr = -(s.dr * (csr - s.ur));
+  double q1 = 1.0 / (dl + dr);
+  double cw = (tr - tl) * q1;
+  double cp = (dl * tr + dr * tl) * q1;
+  double sl, sr, sm;
+  if (cw >= 0.0) {
+    sl = cw / (cw - bm);
+    sr = 0.0;
+    sm = -(bm / (cw - bm));
+  } else {
+    sl = 0.0;
+    sr = -(cw / (bp - cw));
+    sm = bp / (bp - cw);
+  }
+  cp = dmax(cp, 0.0);
+  const double bm0 = s.ul - bm, bp0 = s.ur - bp;
+  double dubl = s.dl * s.ul;
+  double dubr = s.dr * s.ur;
+  double dfl = dubl - bm * s.dl, dfr = dubr - bp * s.dr;
+  double ufl = dubl * bm0 + s.pl, ufr = dubr * bp0 + s.pr;
+  double vfl = s.dl * s.vl * bm0, vfr = s.dr * s.vr * bp0;
+  double wfl = s.dl * s.wl * bm0, wfr = s.dr * s.wr * bp0;
+  double efl = el * bm0 + s.pl * s.ul, efr = er * bp0 + s.pr * s.ur;
+  HllFace h;
+  h.sl = sl;
+  h.sr = sr;
+  h.gesl = bm0;
+  h.gesr = bp0;
+  h.df = sl * dfl + sr * dfr + 0.0;
+  h.uf = sl * ufl + sr * ufr + 0.0;
+  h.vf = sl * vfl + sr * vfr + 0.0;
+  h.wf = sl * wfl + sr * wfr + 0.0;
+  h.ef = sl * efl + sr * efr + 0.0;
+  if (DUAL) {
+    double gefl = bm0 * s.gel * s.dl;
+    double gefr = bp0 * s.ger * s.dr;
+    h.gef = sl * gefl + sr * gefr + 0.0;
+  } else {
+    h.gef = 0.0;
+  }
+  h.uf = h.uf + sm * cp;
+  h.ef = h.ef + sm * cp * cw;
+  return h;
+}
+
 // -------------------------------------------------------------- euler.F:126-279 (one cell)
 struct Cell {
   double d, e, u, v, w, ge;

@@ -508,6 +508,56 @@ __global__ void __launch_bounds__(kRiemannThreads, LEARNED ? PPM_RIEMANN_LEARNED
     atomicAdd(&B.counters[kCntGuessRejected], (unsigned long long)s_rejected);
 }
 
+// RiemannSolver = HLL (flux_hll.F:6-415) or HLLC (flux_hllc.F:6-421) at every face, one
+// thread per face: the fluxes times dt/dx, and in the XUB plane the gas-energy source of
+// the face's right cell c, ges(c) = dt/dx * pcent(c) * (sl*gesl + sr*gesr of face c,
+// minus those of face c+1, in the reference's order), which needs face c+1's weights:
+// recomputed here from its states (bit-identical to its own thread's).  COL: the weights
+// (sl, gesl, sr, gesr) of every face for the colour kernel.
+template <bool DUAL, bool HLLC>
+__device__ __forceinline__ HllFace hll_any(const FaceState& s, const Phys& P) {
+  return HLLC ? hllc_face<DUAL>(s, P) : hll_face<DUAL>(s, P);
+}
+
+template <bool DUAL, bool ONE, bool HLLC, bool COL>
+__global__ void __launch_bounds__(kRiemannThreads) hll_riemann_kernel(const __grid_constant__ BatchArgs B) {
+  int64_t lb;
+  const int g = locate<ONE>(B.riemann_prefix, B.ngrids, lb);
+  PPM_BIND_RECORD(a, g)
+  const int64_t chunks = (a.npencils + kRiemannThreads - 1) / kRiemannThreads;
+  const int fi = (int)(lb / chunks);
+  const int64_t pid = (lb - (int64_t)fi * chunks) * kRiemannThreads + threadIdx.x;
+  if (pid >= a.npencils) return;
+  const Phys P = make_phys(a);
+  const int64_t np = a.npencils, pl = a.plane;
+  const int64_t idx = (int64_t)fi * np + pid;
+  const int c = a.is + fi;  // the face's right cell
+  const HllFace h = hll_any<DUAL, HLLC>(load_face<DUAL>(a, idx), P);
+  const double qc = P.dt / a.coef[c].dx;
+  double* o = a.fflux + idx;
+  o[XDF * pl] = qc * h.df;
+  o[XEF * pl] = qc * h.ef;
+  o[XUF * pl] = qc * h.uf;
+  o[XVF * pl] = qc * h.vf;
+  o[XWF * pl] = qc * h.wf;
+  if (DUAL) o[XGEF * pl] = P.dt / a.coef[c].dx * h.gef;
+  double ges = 0.0;  // ges(ie+1) is not consumed
+  if (DUAL && c <= a.ie) {
+    const HllFace h1 = hll_any<DUAL, HLLC>(load_face<DUAL>(a, idx + np), P);
+    const int64_t off = (pid % a.n1) * a.s1 + (pid / a.n1) * a.s2 + (int64_t)c * a.sa;
+    const double pcent = dmax(P.gm1 * __ldg(a.in_ge + off) * __ldg(a.in_d + off), kTiny);
+    ges = qc * pcent * (h.sl * h.gesl + h.sr * h.gesr - h1.sl * h1.gesl - h1.sr * h1.gesr);
+  }
+  o[XUB * pl] = ges;
+  if (COL) {
+    double* w = a.fcol + idx;
+    w[CHSL * pl] = h.sl;
+    w[CHBM * pl] = h.gesl;
+    w[CHSR * pl] = h.sr;
+    w[CHBP * pl] = h.gesr;
+  }
+}
+
 // The flux planes are read once, with whole lines per warp: streaming loads (evicted
 // first) keep them from displacing the cells the marching kernels reuse.
 __device__ __forceinline__ Flux load_flux(const SweepArgs& a, int64_t idx) {
@@ -921,7 +971,8 @@ __device__ __forceinline__ void flush_stage(const SweepArgs& a, const double* st
 // prefetch.
 //
 // XT (x sweep of a single grid, with STAGED): the input cells arrive as TMA tiles (xt).
-template <bool DUAL, bool GRAV, bool FALLBACK, bool STAGED = false, int PD = 0, bool XT = false>
+template <bool DUAL, bool GRAV, bool FALLBACK, bool STAGED = false, int PD = 0, bool XT = false,
+          bool RS = false>
 __device__ __forceinline__ bool update_pencil(const SweepArgs& a, int64_t pid, const Phys& P,
                                               UpdateCounts& cnt, bool valid = true,
                                               double* stage = nullptr, int64_t pid0 = 0,
@@ -1002,9 +1053,12 @@ __device__ __forceinline__ bool update_pencil(const SweepArgs& a, int64_t pid, c
       if (t >= is && t <= ie) {
         if (DUAL) {
           const double pcent = dmax(P.gm1 * Cn.ge * Cn.d, kTiny);
-          ges_n = gov ? govv : P.dt / a.coef[t].dx * pcent * (F0.ub - F1.ub);
+          ges_n = gov ? govv : (RS ? F0.ub : P.dt / a.coef[t].dx * pcent * (F0.ub - F1.ub));
         }
-        if (Cn.d + (F0.df - F1.df) <= 0.0 || Cn.e < 0.0) {
+        // RS (HLL, HLLC): flux_hll.F:336 / flux_hllc.F:332 test the density alone
+        const bool bad = RS ? (Cn.d + F0.df - F1.df <= 0.0)
+                            : (Cn.d + (F0.df - F1.df) <= 0.0 || Cn.e < 0.0);
+        if (bad) {
           if (!FALLBACK && !STAGED) {  // hand the pencil to the fallback pass
             if (PIPE) cp_async_wait<0>();
             return true;
@@ -1014,7 +1068,7 @@ __device__ __forceinline__ bool update_pencil(const SweepArgs& a, int64_t pid, c
             flagged = true;
           }
         }
-        if (live && (Cn.d + (F0.df - F1.df) <= 0.0 || Cn.e < 0.0)) {
+        if (live && bad) {
           if (a.fallback == 0) {
             cnt.fatal += 1;
           } else {
@@ -1172,7 +1226,8 @@ constexpr size_t update_smem_bytes() {
 
 // STAGED: the x sweep (pencils along the contiguous axis) with staged outputs; XT: its
 // input cells as TMA tiles (a single grid with B.x_tma set).
-template <bool DUAL, bool GRAV, bool ONE, bool STAGED, bool XT>
+// RS: HLL or HLLC fluxes (ges precomputed in the XUB plane, the density-only check)
+template <bool DUAL, bool GRAV, bool ONE, bool STAGED, bool XT, bool RS = false>
 __global__ void __launch_bounds__(kMarchThreads,
                                   STAGED ? (XT ? PPM_UPDATE_XT_MINBLOCKS : PPM_UPDATE_MINBLOCKS)
                                          : (ONE ? PPM_UPDATE_YZ_MINBLOCKS
@@ -1218,7 +1273,7 @@ __global__ void __launch_bounds__(kMarchThreads,
   if (STAGED || valid) {
     const Phys P = make_phys(a);
     UpdateCounts cnt = {0, 0, 0, 1.0e20};
-    if (update_pencil<DUAL, GRAV, false, STAGED, update_pipe<ONE, STAGED>(), XT>(
+    if (update_pencil<DUAL, GRAV, false, STAGED, update_pipe<ONE, STAGED>(), XT, RS>(
             a, pid, P, cnt, valid, s_stage + warp * kStageWarp, wpid0, s_ring + threadIdx.x,
             &xt)) {
       const unsigned long long slot = atomicAdd(&B.counters[kCntFlagged], 1ull);
@@ -1243,7 +1298,7 @@ __global__ void __launch_bounds__(kMarchThreads,
 }
 
 // The fallback pass: a fixed grid that walks the list of flagged pencils.
-template <bool DUAL, bool GRAV, bool ONE>
+template <bool DUAL, bool GRAV, bool ONE, bool RS = false>
 __global__ void __launch_bounds__(128) fallback_kernel(const __grid_constant__ BatchArgs B) {
   const unsigned long long nflag = *(volatile unsigned long long*)&B.counters[kCntFlagged];
   for (unsigned long long k = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1252,7 +1307,8 @@ __global__ void __launch_bounds__(128) fallback_kernel(const __grid_constant__ B
     const SweepArgs& a = ONE ? B.one : B.grids[(int)(code >> 40)];
     const Phys P = make_phys(a);
     UpdateCounts cnt = {0, 0, 0, 1.0e20};
-    update_pencil<DUAL, GRAV, true>(a, code & ((int64_t(1) << 40) - 1), P, cnt);
+    update_pencil<DUAL, GRAV, true, false, 0, false, RS>(a, code & ((int64_t(1) << 40) - 1), P,
+                                                        cnt);
     if (a.cfl_min_bits && cnt.dtmin < 1.0e20)
       atomicMin(a.cfl_min_bits, (unsigned long long)__double_as_longlong(cnt.dtmin));
     if (cnt.fallbacks) atomicAdd(&B.counters[kCntFallbacks], (unsigned long long)cnt.fallbacks);
@@ -1373,7 +1429,7 @@ __global__ void __launch_bounds__(kMarchThreads, PPM_COLOUR_MINBLOCKS)
           const double dlc = fc[CDLC * plane], drc = fc[CDRC * plane];
           const double ov = fc[COVR * plane];
           const bool ovl = ov == 1.0 || ov == 3.0, ovr = ov >= 2.0;
-          const bool hll = a.fhll[fidx] != 0;
+          const bool hll = a.solver != 0 || a.fhll[fidx] != 0;
           double w[4] = {0.0, 0.0, 0.0, 0.0};
           double ub = 0.0, db = 0.0, dsl = 1.0, dsr = 1.0;
           if (hll) {  // the HLL weights the fallback pass left (sl, bm0, sr, bp0)
@@ -1448,7 +1504,7 @@ __global__ void __launch_bounds__(kMarchThreads, PPM_COLOUR_MINBLOCKS)
 // Above 48 KB of dynamic shared memory a kernel needs the opt-in attribute, set once
 // per device (a function attribute is not a stream operation, so this is also legal
 // while a stream is being captured).
-template <bool DUAL, bool GRAV, bool ONE, bool STAGED, bool XT>
+template <bool DUAL, bool GRAV, bool ONE, bool STAGED, bool XT, bool RS = false>
 void launch_update(const BatchArgs& B, int64_t march_blocks, cudaStream_t st) {
   constexpr size_t bytes = update_smem_bytes<ONE, STAGED, XT>();
   if (bytes > 48 * 1024) {
@@ -1457,12 +1513,12 @@ void launch_update(const BatchArgs& B, int64_t march_blocks, cudaStream_t st) {
     cudaGetDevice(&dev);
     const unsigned long long bit = 1ull << (dev & 63);
     if (!(done.load(std::memory_order_acquire) & bit)) {
-      cudaFuncSetAttribute(update_kernel<DUAL, GRAV, ONE, STAGED, XT>,
+      cudaFuncSetAttribute(update_kernel<DUAL, GRAV, ONE, STAGED, XT, RS>,
                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
       done.fetch_or(bit, std::memory_order_release);
     }
   }
-  update_kernel<DUAL, GRAV, ONE, STAGED, XT>
+  update_kernel<DUAL, GRAV, ONE, STAGED, XT, RS>
       <<<(unsigned)march_blocks, kMarchThreads, bytes, st>>>(B);
 }
 
@@ -1488,7 +1544,16 @@ void launch_stages(const BatchArgs& B, int64_t march_blocks, int64_t riemann_blo
   }
   mark(2);
   const unsigned rb = (unsigned)riemann_blocks;
-  if (learned && B.ncolour > 0)
+  const bool col = B.ncolour > 0;
+  if (B.solver == 1 && col)
+    hll_riemann_kernel<DUAL, ONE, false, true><<<rb, kRiemannThreads, 0, st>>>(B);
+  else if (B.solver == 1)
+    hll_riemann_kernel<DUAL, ONE, false, false><<<rb, kRiemannThreads, 0, st>>>(B);
+  else if (B.solver == 2 && col)
+    hll_riemann_kernel<DUAL, ONE, true, true><<<rb, kRiemannThreads, 0, st>>>(B);
+  else if (B.solver == 2)
+    hll_riemann_kernel<DUAL, ONE, true, false><<<rb, kRiemannThreads, 0, st>>>(B);
+  else if (learned && B.ncolour > 0)
     riemann_kernel<DUAL, ONE, true, true><<<rb, kRiemannThreads, 0, st>>>(B);
   else if (learned)
     riemann_kernel<DUAL, ONE, true><<<rb, kRiemannThreads, 0, st>>>(B);
@@ -1497,14 +1562,25 @@ void launch_stages(const BatchArgs& B, int64_t march_blocks, int64_t riemann_blo
   else
     riemann_kernel<DUAL, ONE, false><<<rb, kRiemannThreads, 0, st>>>(B);
   mark(3);
-  if (PPM_X_TMA && staged && ONE && B.x_tma)
-    launch_update<DUAL, GRAV, ONE, true, ONE>(B, march_blocks, st);
-  else if (staged)
-    launch_update<DUAL, GRAV, ONE, true, false>(B, march_blocks, st);
-  else
-    launch_update<DUAL, GRAV, ONE, false, false>(B, march_blocks, st);
-  mark(4);
-  fallback_kernel<DUAL, GRAV, ONE><<<64, 128, 0, st>>>(B);
+  if (B.solver != 0) {  // HLL / HLLC
+    if (PPM_X_TMA && staged && ONE && B.x_tma)
+      launch_update<DUAL, GRAV, ONE, true, ONE, true>(B, march_blocks, st);
+    else if (staged)
+      launch_update<DUAL, GRAV, ONE, true, false, true>(B, march_blocks, st);
+    else
+      launch_update<DUAL, GRAV, ONE, false, false, true>(B, march_blocks, st);
+    mark(4);
+    fallback_kernel<DUAL, GRAV, ONE, true><<<64, 128, 0, st>>>(B);
+  } else {
+    if (PPM_X_TMA && staged && ONE && B.x_tma)
+      launch_update<DUAL, GRAV, ONE, true, ONE>(B, march_blocks, st);
+    else if (staged)
+      launch_update<DUAL, GRAV, ONE, true, false>(B, march_blocks, st);
+    else
+      launch_update<DUAL, GRAV, ONE, false, false>(B, march_blocks, st);
+    mark(4);
+    fallback_kernel<DUAL, GRAV, ONE><<<64, 128, 0, st>>>(B);
+  }
   if (B.ncolour > 0) {
     constexpr int cpt = PPM_COLOURS_PER_THREAD;
     const int64_t chunks = (B.ncolour + cpt - 1) / cpt;

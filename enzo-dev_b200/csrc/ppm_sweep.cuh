@@ -106,6 +106,10 @@ struct SweepArgs {
   double* fcol;
   unsigned char* fhll;
   double* col_capture;
+  // Riemann solver (Grid_xEulerSweep.C:223-283): 0 two-shock, 1 HLL, 2 HLLC.  For HLL and
+  // HLLC the flux plane XUB holds the gas-energy source ges of the face's right cell
+  // instead of the Godunov velocity.
+  int solver;
 };
 
 enum { kFaceVars = 12, kFluxVars = 7 };
@@ -155,6 +159,7 @@ struct BatchArgs {
   int ncolour = 0;
   unsigned char* hll_flags = nullptr;
   int64_t hll_bytes = 0;
+  int solver = 0;                    // the batch's Riemann solver (SweepArgs::solver)
   CUtensorMap xin[6];
 };
 

@@ -27,6 +27,8 @@ ERR_TIMEOUT = -7
 MEM_HOST = 0
 MEM_DEVICE = 1
 RIEMANN_TWOSHOCK = 5
+RIEMANN_HLL = 1
+RIEMANN_HLLC = 4
 RECONSTRUCTION_PPM = 1
 
 EXPORTS = (
@@ -222,7 +224,7 @@ def make_params(hp, dt, learned_guess=False, dt_device=None) -> Params:
     P.dual_energy = int(hp.dual)
     P.gravity = int(hp.gravity)
     P.pressure_free = int(hp.pressure_free)
-    P.riemann_solver = RIEMANN_TWOSHOCK
+    P.riemann_solver = int(getattr(hp, "riemann", RIEMANN_TWOSHOCK))
     P.riemann_fallback = int(hp.fallback)
     P.reconstruction = RECONSTRUCTION_PPM
     P.steepening = int(getattr(hp, "steepen", 0))

@@ -93,6 +93,8 @@ class HydroParams:
     fallback: bool = True             # RiemannSolverFallback (:809)
     steepen: int = 0                  # PPMSteepeningParameter (:184): 0 or 1
     flatten: int = 0                  # PPMFlatteningParameter (:182): 0, 1 or 3
+    riemann: int = 5                  # RiemannSolver: 5 TwoShock (the PPM default,
+                                      # ReadParameterFile.C:1575-1576), 1 HLL, 4 HLLC
 
 
 def new_fields(grid, dual):

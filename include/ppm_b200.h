@@ -46,7 +46,9 @@ extern "C" {
 #define PPM_B200_MAX_COLOURS 45
 
 /* Riemann solver / reconstruction enums, values as in Enzo's typedefs.h */
-#define PPM_B200_RIEMANN_TWOSHOCK 5
+#define PPM_B200_RIEMANN_TWOSHOCK 5   /* twoshock + flux_twoshock (the PPM default) */
+#define PPM_B200_RIEMANN_HLL 1        /* flux_hll.F */
+#define PPM_B200_RIEMANN_HLLC 4       /* flux_hllc.F */
 #define PPM_B200_RECONSTRUCTION_PPM 1
 
 /* Hydro globals consumed by the sweeps (global_data.h, defaults in
@@ -62,7 +64,8 @@ typedef struct ppm_b200_params {
   int dual_energy;          /* DualEnergyFormalism */
   int gravity;              /* GravityOn (AccelerationField used) */
   int pressure_free;        /* PressureFree: unsupported, must be 0 */
-  int riemann_solver;       /* RiemannSolver: PPM_B200_RIEMANN_TWOSHOCK */
+  int riemann_solver;       /* RiemannSolver: PPM_B200_RIEMANN_TWOSHOCK, _HLL or _HLLC
+                               (learned_guess applies to the two-shock solver only) */
   int riemann_fallback;     /* RiemannSolverFallback */
   int reconstruction;       /* ReconstructionMethod: PPM_B200_RECONSTRUCTION_PPM */
   int steepening;           /* PPMSteepeningParameter: 0 or 1 (density steepening, inteuler.F:166-193) */

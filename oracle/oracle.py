@@ -51,6 +51,7 @@ class OraParams(C.Structure):
         ("steepen", C.c_int),
         ("flatten", C.c_int),
         ("ncolour", C.c_int),
+        ("riemann", C.c_int),
     ]
 
 
@@ -159,6 +160,7 @@ def make_params(grid, hp, dt, ncolour=0) -> OraParams:
     P.steepen = int(getattr(hp, "steepen", 0))
     P.flatten = int(getattr(hp, "flatten", 0))
     P.ncolour = int(ncolour)
+    P.riemann = int(getattr(hp, "riemann", 5))
     return P
 
 

@@ -786,6 +786,162 @@ static int flux_hll_cell(work_t *W, const ora_params *P, const double *dx, int i
 }
 
 /* ------------------------------------------------------------------------ */
+/* HLLC face (flux_hllc.F:105-300 for one interface, no diffusion): the      */
+/* weights sl, sr, the advective speeds gesl = ul - bm, gesr = ur - bp and   */
+/* the five (six) fluxes before the dt/dx factor, the contact's momentum and  */
+/* energy terms included (:282-286).                                         */
+/* ------------------------------------------------------------------------ */
+static void hllc_face(work_t *W, const ora_params *P, int i, int j, double *sl_o, double *sr_o,
+                      double *gesl_o, double *gesr_o, double *fl) {
+  const int idim = W->idim;
+  const double gamma = P->gamma;
+  const double gamma1 = gamma - 1.0;
+  const double gamma1i = 1.0 / gamma1;
+  double dls = S(W->dls, i, j), drs = S(W->drs, i, j), pls = S(W->pls, i, j), prs = S(W->prs, i, j);
+  double uls = S(W->uls, i, j), urs = S(W->urs, i, j), vls = S(W->vls, i, j), vrs = S(W->vrs, i, j);
+  double wls = S(W->wls, i, j), wrs = S(W->wrs, i, j);
+  double sqrtdl = sqrt(dls);
+  double sqrtdr = sqrt(drs);
+  double isdlpdr = 1.0 / (sqrtdl + sqrtdr);
+  double vroe1 = (sqrtdl * uls + sqrtdr * urs) * isdlpdr;
+  double vroe2 = (sqrtdl * vls + sqrtdr * vrs) * isdlpdr;
+  double vroe3 = (sqrtdl * wls + sqrtdr * wrs) * isdlpdr;
+  double v2 = vroe1 * vroe1 + vroe2 * vroe2 + vroe3 * vroe3;
+  double el = gamma1i * pls + 0.5 * dls * (uls * uls + vls * vls + wls * wls);
+  double er = gamma1i * prs + 0.5 * drs * (urs * urs + vrs * vrs + wrs * wrs);
+  double hroe = ((el + pls) / sqrtdl + (er + prs) / sqrtdr) * isdlpdr;
+  double cs = sqrt(gamma1 * fmax2((hroe - 0.5 * v2), F_TINY));
+  double char1 = vroe1 - cs;
+  double char2 = vroe1 + cs;
+  double csl0 = sqrt(gamma * pls / dls);
+  double csr0 = sqrt(gamma * prs / drs);
+  double csl = fmin2(uls - csl0, char1);
+  double csr = fmax2(urs + csr0, char2);
+  double bm = fmin2(csl, 0.0);
+  double bp = fmax2(csr, 0.0);
+  /* contact speed cw and pressure cp, flux_hllc.F:160-183 */
+  double tl = pls - (csl - uls) * dls * uls;
+  double tr = prs - (csr - urs) * drs * urs;
+  double dl = dls * (csl - uls);
+  double dr = -(drs * (csr - urs));
+  double q1 = 1.0 / (dl + dr);
+  double cw = (tr - tl) * q1;
+  double cp = (dl * tr + dr * tl) * q1;
+  double sl, sr, sm;
+  if (cw >= 0.0) {
+    sl = cw / (cw - bm);
+    sr = 0.0;
+    sm = -(bm / (cw - bm));
+  } else {
+    sl = 0.0;
+    sr = -(cw / (bp - cw));
+    sm = bp / (bp - cw);
+  }
+  cp = fmax2(cp, 0.0);
+  double dubl = dls * uls;
+  double dubr = drs * urs;
+  double dfl = dubl - bm * dls, dfr = dubr - bp * drs;
+  double ufl = dubl * (uls - bm) + pls, ufr = dubr * (urs - bp) + prs;
+  double vfl = dls * vls * (uls - bm), vfr = drs * vrs * (urs - bp);
+  double wfl = dls * wls * (uls - bm), wfr = drs * wrs * (urs - bp);
+  double efl = el * (uls - bm) + pls * uls, efr = er * (urs - bp) + prs * urs;
+  *sl_o = sl;
+  *sr_o = sr;
+  *gesl_o = uls - bm;
+  *gesr_o = urs - bp;
+  fl[0] = sl * dfl + sr * dfr + 0.0;
+  fl[1] = sl * ufl + sr * ufr + 0.0;
+  fl[2] = sl * vfl + sr * vfr + 0.0;
+  fl[3] = sl * wfl + sr * wfr + 0.0;
+  fl[4] = sl * efl + sr * efr + 0.0;
+  if (P->dual == 1) {
+    double gefl = (uls - bm) * S(W->gels, i, j) * dls;
+    double gefr = (urs - bp) * S(W->gers, i, j) * drs;
+    fl[5] = sl * gefl + sr * gefr + 0.0;
+  }
+  fl[1] = fl[1] + sm * cp;
+  fl[4] = fl[4] + sm * cp * cw;
+}
+
+/* ------------------------------------------------------------------------ */
+/* RiemannSolver = HLL (flux_hll.F:6-415) or HLLC (flux_hllc.F:6-421) over   */
+/* the pencils: fluxes of faces i1..i2+1, the gas-energy source, colours,    */
+/* dt/dx; then the negative-density check, fatal for HLL, the per-cell HLL  */
+/* fallback for HLLC (flux_hllc.F:331-389).  ges(i2+1) reads locals at i2+2 */
+/* that the reference never sets; it is not consumed and is zero here.      */
+/* ------------------------------------------------------------------------ */
+static int flux_hll_family(work_t *W, const ora_params *P, const double *dx, int i1, int i2,
+                           int j1, int j2, int hllc, ora_stats *st) {
+  const int idim = W->idim;
+  const double gamma = P->gamma, dt = P->dt;
+  int i, j, rc = 0;
+  for (j = j1; j <= j2; j++) {
+    /* per-face weights in the flux_hll locals (index i2+2 zero) */
+    for (i = i1; i <= i2 + 2; i++) {
+      V(W->h_sl, i) = V(W->h_sr, i) = V(W->h_gesl, i) = V(W->h_gesr, i) = 0.0;
+    }
+    for (i = i1; i <= i2 + 1; i++) {
+      double fl[6] = {0, 0, 0, 0, 0, 0};
+      if (hllc)
+        hllc_face(W, P, i, j, &V(W->h_sl, i), &V(W->h_sr, i), &V(W->h_gesl, i), &V(W->h_gesr, i), fl);
+      else
+        hll_face(W, P, i, j, 1, &V(W->h_sl, i), &V(W->h_sr, i), &V(W->h_gesl, i), &V(W->h_gesr, i), fl);
+      S(W->df, i, j) = fl[0];
+      S(W->uf, i, j) = fl[1];
+      S(W->vf, i, j) = fl[2];
+      S(W->wf, i, j) = fl[3];
+      S(W->ef, i, j) = fl[4];
+      if (P->dual == 1) S(W->gef, i, j) = fl[5];
+    }
+    for (int n = 0; n < W->ncol; n++)
+      for (i = i1; i <= i2 + 1; i++) {
+        const double colfl = V(W->h_gesl, i) * CS(W->colls, i, j, n);
+        const double colfr = V(W->h_gesr, i) * CS(W->colrs, i, j, n);
+        CS(W->colf, i, j, n) = V(W->h_sl, i) * colfl + V(W->h_sr, i) * colfr;
+      }
+    if (P->dual == 1) {
+      for (i = i1; i <= i2 + 1; i++)
+        V(W->h_pcent, i) = fmax2((gamma - 1.0) * S(W->ge, i, j) * S(W->d, i, j), F_TINY);
+      for (i = i1; i <= i2 + 1; i++) {
+        double qc = dt / V(dx, i);
+        S(W->ges, i, j) = qc * V(W->h_pcent, i) *
+                          (V(W->h_sl, i) * V(W->h_gesl, i) + V(W->h_sr, i) * V(W->h_gesr, i) -
+                           V(W->h_sl, i + 1) * V(W->h_gesl, i + 1) -
+                           V(W->h_sr, i + 1) * V(W->h_gesr, i + 1));
+      }
+    }
+    for (i = i1; i <= i2 + 1; i++) {
+      double qc = dt / V(dx, i);
+      S(W->df, i, j) = qc * S(W->df, i, j);
+      S(W->uf, i, j) = qc * S(W->uf, i, j);
+      S(W->vf, i, j) = qc * S(W->vf, i, j);
+      S(W->wf, i, j) = qc * S(W->wf, i, j);
+      S(W->ef, i, j) = qc * S(W->ef, i, j);
+    }
+    if (P->dual == 1)
+      for (i = i1; i <= i2 + 1; i++) S(W->gef, i, j) = dt / V(dx, i) * S(W->gef, i, j);
+    for (int n = 0; n < W->ncol; n++)
+      for (i = i1; i <= i2 + 1; i++) CS(W->colf, i, j, n) = dt * CS(W->colf, i, j, n);
+    /* flux_hll.F:336-383 / flux_hllc.F:331-389 */
+    for (i = i1; i <= i2; i++) {
+      if (S(W->d, i, j) + S(W->df, i, j) - S(W->df, i + 1, j) <= 0.0) {
+        if (!hllc || P->fallback == 0) {
+          rc = -1;
+          if (st) st->fatal = 1;
+        } else {
+          if (st) st->fallbacks += 1;
+          if (flux_hll_cell(W, P, dx, i, j, i2) != 0) {
+            rc = -1;
+            if (st) st->fatal = 1;
+          }
+        }
+      }
+    }
+  }
+  return rc;
+}
+
+/* ------------------------------------------------------------------------ */
 /* flux_twoshock.F:6-490 (RAREFACTION2, no diffusion)                        */
 /* ------------------------------------------------------------------------ */
 static int flux_twoshock(work_t *W, const ora_params *P, const double *dx, int i1, int i2,
@@ -1090,8 +1246,14 @@ static int sweep_slice(work_t *W, int dim, int s, const ora_params *P, double *c
   const double *dx = cw[dim];
   int rc = 0;
   inteuler(W, P, dx, is, ie, js, je);
-  twoshock(W, P, is, ie + 1, js, je, st);
-  if (flux_twoshock(W, P, dx, is, ie, js, je, st) != 0) rc = -1;
+  /* the solver switch of Grid_xEulerSweep.C:223-283 */
+  if (P->riemann == ORA_RIEMANN_HLL || P->riemann == ORA_RIEMANN_HLLC) {
+    if (flux_hll_family(W, P, dx, is, ie, js, je, P->riemann == ORA_RIEMANN_HLLC, st) != 0)
+      rc = -1;
+  } else {
+    twoshock(W, P, is, ie + 1, js, je, st);
+    if (flux_twoshock(W, P, dx, is, ie, js, je, st) != 0) rc = -1;
+  }
   if (euler(W, P, dx, is, ie, js, je, st) != 0) rc = -1;
   if (P->dual) pgas2d_dual(W, P, is - 3, ie + 3, js, je);
 

@@ -17,6 +17,7 @@
  *    Grid_xEulerSweep.C:124-132, :361-371, :409-416)
  *   twoshock                   src/enzo/twoshock.F:5-276
  *   flux_twoshock / flux_hll   src/enzo/flux_twoshock.F:6-490, flux_hll.F:6-415
+ *   flux_hllc                  src/enzo/flux_hllc.F:6-421 (RiemannSolver = HLLC)
  *   euler                      src/enzo/euler.F:7-285
  *   pgas2d_dual                src/enzo/pgas2d_dual.F:4-122
  *   grid::ComputePressure      src/enzo/Grid_ComputePressure.C:36-164
@@ -63,7 +64,11 @@ typedef struct {
   int steepen;         /* PPMSteepeningParameter (0 or 1: density steepening) */
   int flatten;         /* PPMFlatteningParameter (0, 1 or 3) */
   int ncolour;         /* NumberOfColours: advected colour fields after the hydro fields */
+  int riemann;         /* RiemannSolver (typedefs.h:279-280): 5 TwoShock (0 taken as 5),
+                          1 HLL, 4 HLLC */
 } ora_params;
+
+enum { ORA_RIEMANN_HLL = 1, ORA_RIEMANN_HLLC = 4, ORA_RIEMANN_TWOSHOCK = 5 };
 
 /* struct fluxes (src/enzo/Fluxes.h:29-37), restricted to the six hydro slots */
 typedef struct {
