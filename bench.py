@@ -41,6 +41,8 @@ UNIT = "zone-updates/s"
 # ComputePressure reads rho, ge and writes p (24 B); each sweep reads rho, E, u, v, w,
 # ge, p (56 B) and writes rho, E, u, v, w, ge (48 B).
 BYTES_PER_SWEEP_CELL = 104
+# RiemannSolver values (typedefs.h:279-280)
+RIEMANN = {"twoshock": 5, "hll": 1, "hllc": 4}
 BYTES_PER_ZONE_UPDATE = 24 + 3 * BYTES_PER_SWEEP_CELL
 
 
@@ -59,6 +61,9 @@ def parse():
     ap.add_argument("--level-patches", type=int, default=600)
     ap.add_argument("--no-learned", action="store_true",
                     help="skip the learned-Newton-start comparison")
+    ap.add_argument("--riemann", choices=list(RIEMANN), default="twoshock",
+                    help="RiemannSolver of the workload (two-shock is the PPM default and "
+                         "the headline)")
     ap.add_argument("--colours", type=int, default=0,
                     help="advect this many colour fields (NumberOfColours; mass fractions "
                          "of the density) with the workload; 0 = the headline workload")
@@ -73,7 +78,9 @@ def colour_fractions(n):
 def workload_config(args):
     return {
         "workload": f"decaying supersonic turbulence {args.size}^3 periodic (+3 ghosts), "
-                    "Mach 3, gamma 5/3, dual energy, FP64 PPM-DE (plain two-shock guess)",
+                    "Mach 3, gamma 5/3, dual energy, FP64 PPM-DE "
+                    + ("(plain two-shock guess)" if args.riemann == "twoshock"
+                       else f"({args.riemann.upper()} Riemann solver)"),
         "grid": [args.size + 6] * 3,
         "active_cells_per_gpu": args.size ** 3,
         "step": "SolvePPM_DE (pressure, 3 sweeps, calc_dt of the next cycle folded into the "
@@ -178,13 +185,14 @@ def committed_traffic():
 
 
 # ---------------------------------------------------------------- CPU reference (oracle port)
-def cpu_reference_rate(size, seed, nthreads, min_seconds=10.0, max_steps=12, colours=0):
+def cpu_reference_rate(size, seed, nthreads, min_seconds=10.0, max_steps=12, colours=0,
+                       riemann=5):
     """Times the C restatement of the Fortran path (the oracle) on the host cores: steps
     of the same workload until min_seconds of SolvePPM_DE time (at least 2 steps).
     Returns (zone-updates/s, seconds, steps)."""
     sys.path.insert(0, str(REPO / "oracle"))
     import oracle as O  # the CPU baseline leg is the one place bench.py runs the oracle
-    hp = H.HydroParams(gamma=5.0 / 3.0, cfl=0.4, dual=True)
+    hp = H.HydroParams(gamma=5.0 / 3.0, cfl=0.4, dual=True, riemann=riemann)
     g = H.Grid.uniform((size, size, size))
     f = H.turbulence(g, hp, mach=3.0, seed=seed)
     for k, frac in enumerate(colour_fractions(colours)):
@@ -211,7 +219,7 @@ def run_reference(args):
     nthreads = os.cpu_count() or 1
     # the same workload (grid size and generator); each step about 1.5 s on 16 threads
     sample = args.size
-    hp = H.HydroParams(gamma=5.0 / 3.0, cfl=0.4, dual=True)
+    hp = H.HydroParams(gamma=5.0 / 3.0, cfl=0.4, dual=True, riemann=RIEMANN[args.riemann])
     sys.path.insert(0, str(REPO / "oracle"))
     import oracle as O
     g = H.Grid.uniform((sample,) * 3)
@@ -421,7 +429,7 @@ def run_ours(args):
     torch.cuda.set_stream(stream)
     ctx = capi.Context(local, stream=stream.cuda_stream)
 
-    hp = H.HydroParams(gamma=5.0 / 3.0, cfl=0.4, dual=True)
+    hp = H.HydroParams(gamma=5.0 / 3.0, cfl=0.4, dual=True, riemann=RIEMANN[args.riemann])
     g = H.Grid.uniform((args.size,) * 3)
     f_host = H.turbulence(g, hp, mach=3.0, seed=args.seed + rank)
     for k, frac in enumerate(colour_fractions(args.colours)):  # +16 B per colour and sweep
@@ -538,7 +546,7 @@ def run_ours(args):
 
     # the learned Newton start on the same workload (same state, a few steps each way)
     learned = None
-    if world == 1 and not args.no_learned:
+    if world == 1 and not args.no_learned and args.riemann == "twoshock":
         learned = run_learned(ctx, g, hp, f_host, args, stream)
 
     level = None
@@ -549,7 +557,8 @@ def run_ours(args):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         nthreads = os.cpu_count() or 1
         rate, secs, nst = cpu_reference_rate(args.size, args.seed, nthreads,
-                                             colours=args.colours)
+                                             colours=args.colours,
+                                             riemann=RIEMANN[args.riemann])
         cpu = {"value": rate, "unit": UNIT, "cores": nthreads, "kind": "port",
                "sample": f"the same {args.size}^3 turbulence workload, {nst} SolvePPM_DE "
                          f"steps, {nthreads} threads ({secs:.1f} s); C restatement of the "

@@ -322,8 +322,8 @@ int check_supported(const ppm_b200_params* p) {
     return PPM_B200_ERR_UNSUPPORTED;
   if (p->number_of_colours < 0 || p->number_of_colours > PPM_B200_MAX_COLOURS)
     return PPM_B200_ERR_UNSUPPORTED;
-  // slope corrections: calcdiss's flattening types 1 and 3, inteuler's steepening
-  if ((p->flattening != 0 && p->flattening != 1 && p->flattening != 3) ||
+  // slope corrections: calcdiss's flattening types 1-3, inteuler's steepening
+  if ((p->flattening < 0 || p->flattening > 3) ||
       (p->steepening != 0 && p->steepening != 1))
     return PPM_B200_ERR_UNSUPPORTED;
   // the solver switch of Grid_xEulerSweep.C:223-283 (two-shock, HLL, HLLC)

@@ -19,6 +19,12 @@ constexpr int kNumIter = 8;              // twoshock.F:105-106
 
 __device__ __forceinline__ double dmax(double a, double b) { return a > b ? a : b; }
 __device__ __forceinline__ double dmin(double a, double b) { return a < b ? a : b; }
+// Fortran MAX/MIN as gfortran lowers them without -ffinite-math-only: the first argument
+// unless a later one compares greater (smaller) or the first is NaN, so a NaN argument
+// after the first is ignored.  Used where a NaN is routine: calcdiss type 2's
+// (p(i+1)-p(i-1))/(p(i+2)-p(i-2)) is 0/0 wherever the pressure is uniform.
+__device__ __forceinline__ double dmax_g(double a, double b) { return (b > a || isnan(a)) ? b : a; }
+__device__ __forceinline__ double dmin_g(double a, double b) { return (b < a || isnan(a)) ? b : a; }
 
 struct Phys {
   double gamma, dt, eta1, eta2, small_rho, pmin;
@@ -82,6 +88,22 @@ __device__ __forceinline__ double cd_ftemp1(const double p[5], double wflag) {
     qa = (p[3] - p[1]) / (p[4] - p[0]);
   const double f = dmin(1.0, (qa - kCdOmega1) * kCdOmega2 * wflag);
   return dmax(0.0, f);
+}
+
+// type 2, calcdiss.F:447-478 (before the max of eq. A6): d, p at j-2 .. j+2
+__device__ __forceinline__ double cd_ftemp2(const double d[5], const double p[5], double wflag,
+                                            double gamma) {
+  const double dp1 = p[3] - p[1];
+  // is = j + sign(2, dp1)
+  const bool neg = signbit(dp1);
+  const double p_is = neg ? p[0] : p[4], d_is = neg ? d[0] : d[4];
+  const double omega = dmax_g(0.0, kCdOmega1 * (kCdOmega2 - dp1 / (p[4] - p[0])));
+  const double di2p = 1.0 / d[4], di2m = 1.0 / d[0];
+  const double Z = sqrt((dmax_g(p[4], p[0]) + 0.5 * (p[4] + p[0]) * (gamma - 1.0)) /
+                        dmax_g(di2p, di2m));
+  const double kappa_tilde = (Z + sqrt(gamma * p_is * d_is)) / Z;
+  const double kappa = dmax_g(0.0, (kappa_tilde - kCdKappa1) / (kappa_tilde + kCdKappa2));
+  return dmin_g(wflag * omega, kappa);
 }
 
 // type 3, calcdiss.F:486-555 (before the max of eq. A2): d, e, u, p at j-2 .. j+2

@@ -104,6 +104,11 @@ __global__ void __launch_bounds__(kMarchThreads) corrections_kernel(const __grid
     const double wf = cd_wflag(p[1], p[3], ld(a.in_u, j - 1), ld(a.in_u, j + 1));
     if (a.flatten == 1) return cd_ftemp1(p, wf);
     double d[5], e[5], u[5];
+    if (a.flatten == 2) {
+#pragma unroll
+      for (int k = 0; k < 5; ++k) d[k] = ld(a.in_d, j - 2 + k);
+      return cd_ftemp2(d, p, wf, gamma);
+    }
 #pragma unroll
     for (int k = 0; k < 5; ++k) {
       d[k] = ld(a.in_d, j - 2 + k);
@@ -121,7 +126,10 @@ __global__ void __launch_bounds__(kMarchThreads) corrections_kernel(const __grid
     const int64_t o = (int64_t)(c - (is - 1)) * np + pid;
     if (a.flatten) {  // eq. A2: the max with the neighbour on the high-pressure side
       const double fp = ftemp(c + 1);
-      a.flat[o] = (ld(a.pres, c + 1) - ld(a.pres, c - 1) < 0.0) ? dmax(f0, fp) : dmax(f0, fm);
+      if (a.flatten == 2)  // eq. A6: the max over both neighbours (calcdiss.F:480-483)
+        a.flat[o] = dmax_g(dmax_g(fm, f0), fp);
+      else
+        a.flat[o] = (ld(a.pres, c + 1) - ld(a.pres, c - 1) < 0.0) ? dmax(f0, fp) : dmax(f0, fm);
       fm = f0;
       f0 = fp;
     }

@@ -69,7 +69,7 @@ typedef struct ppm_b200_params {
   int riemann_fallback;     /* RiemannSolverFallback */
   int reconstruction;       /* ReconstructionMethod: PPM_B200_RECONSTRUCTION_PPM */
   int steepening;           /* PPMSteepeningParameter: 0 or 1 (density steepening, inteuler.F:166-193) */
-  int flattening;           /* PPMFlatteningParameter: 0, 1 or 3 (calcdiss.F eq. A1-A2 / A7-A10) */
+  int flattening;           /* PPMFlatteningParameter: 0, 1, 2 or 3 (calcdiss.F eq. A1-A2 / A4-A6 / A7-A10) */
   int diffusion;            /* PPMDiffusionParameter: must be 0 */
   int conservative_rec;     /* ConservativeReconstruction: must be 0 */
   int positive_rec;         /* PositiveReconstruction: must be 0 */

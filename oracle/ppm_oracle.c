@@ -41,6 +41,12 @@ static inline double fmax2(double a, double b) { return a > b ? a : b; }
 static inline double fmin2(double a, double b) { return a < b ? a : b; }
 /* Fortran SIGN(1, x): gfortran honours the sign of a signed zero. */
 static inline double fsign1(double x) { return copysign(1.0, x); }
+/* Fortran MAX/MIN as gfortran lowers them without -ffinite-math-only: the first argument
+   unless a later one compares greater (smaller) or the first is NaN, so a NaN argument
+   after the first is ignored.  Used where a NaN is routine: calcdiss type 2's
+   (p(i+1)-p(i-1))/(p(i+2)-p(i-2)) is 0/0 wherever the pressure is uniform. */
+static inline double fmax_g(double a, double b) { return (b > a || isnan(a)) ? b : a; }
+static inline double fmin_g(double a, double b) { return (b < a || isnan(a)) ? b : a; }
 
 #define V(a, i) (a)[(i)-1]
 #define S(a, i, j) (a)[((size_t)(j)-1) * (size_t)idim + ((size_t)(i)-1)]
@@ -274,6 +280,20 @@ static void calcdiss_flatten(work_t *W, const ora_params *P, const double *dsl,
       V(W->ftemp, i) = fmin2(1.0, (qa - omega1) * omega2 * V(W->wflag, i));
       V(W->ftemp, i) = fmax2(0.0, V(W->ftemp, i));
     }
+  } else if (P->flatten == 2) {  /* calcdiss.F:445-478, eq. A4-A5 */
+    for (i = i1 - 1; i <= i2 + 1; i++) {
+      const double dp1 = V(psl, i + 1) - V(psl, i - 1);
+      const int is2 = i + (int)copysign(2.0, dp1);
+      const double omega =
+          fmax_g(0.0, omega1 * (omega2 - dp1 / (V(psl, i + 2) - V(psl, i - 2))));
+      const double di2p = 1.0 / V(dsl, i + 2), di2m = 1.0 / V(dsl, i - 2);
+      const double Z = sqrt((fmax_g(V(psl, i + 2), V(psl, i - 2)) +
+                             0.5 * (V(psl, i + 2) + V(psl, i - 2)) * (gamma - 1.0)) /
+                            fmax_g(di2p, di2m));
+      const double kappa_tilde = (Z + sqrt(gamma * V(psl, is2) * V(dsl, is2))) / Z;
+      const double kappa = fmax_g(0.0, (kappa_tilde - kappa1) / (kappa_tilde + kappa2));
+      V(W->ftemp, i) = fmin_g(V(W->wflag, i) * omega, kappa);
+    }
   } else {  /* P->flatten == 3 */
     for (i = i1 - 1; i <= i2 + 1; i++) {
       const double dp1 = V(psl, i + 1) - V(psl, i - 1);
@@ -307,7 +327,9 @@ static void calcdiss_flatten(work_t *W, const ora_params *P, const double *dsl,
   V(W->ftemp, i1 - 2) = V(W->ftemp, i1 - 1);
   V(W->ftemp, i2 + 2) = V(W->ftemp, i2 + 1);
   for (i = i1 - 1; i <= i2 + 1; i++) {
-    if (V(psl, i + 1) - V(psl, i - 1) < 0.0)
+    if (P->flatten == 2) /* eq. A6, calcdiss.F:480-483 */
+      V(W->flat, i) = fmax_g(fmax_g(V(W->ftemp, i - 1), V(W->ftemp, i)), V(W->ftemp, i + 1));
+    else if (V(psl, i + 1) - V(psl, i - 1) < 0.0)
       V(W->flat, i) = fmax2(V(W->ftemp, i), V(W->ftemp, i + 1));
     else
       V(W->flat, i) = fmax2(V(W->ftemp, i), V(W->ftemp, i - 1));

@@ -22,7 +22,7 @@
  *   pgas2d_dual                src/enzo/pgas2d_dual.F:4-122
  *   grid::ComputePressure      src/enzo/Grid_ComputePressure.C:36-164
  *   calc_dt (PPM branch)       src/enzo/calc_dt.F:6-181
- *   calcdiss (flattening 1, 3) src/enzo/calcdiss.F:213-224, 407-438, 486-559
+ *   calcdiss (flattening 1-3) src/enzo/calcdiss.F:213-224, 407-483, 486-559
  *   CorrectForRefinedFluxes    src/enzo/Grid_CorrectForRefinedFluxes.C:38-760
  *
  * Parity anchors: the reference's analytic shock-tube answer tests
@@ -62,7 +62,7 @@ typedef struct {
   int fallback;        /* RiemannSolverFallback */
   int max_velocity_index; /* MaxVelocityIndex used by ComputePressure */
   int steepen;         /* PPMSteepeningParameter (0 or 1: density steepening) */
-  int flatten;         /* PPMFlatteningParameter (0, 1 or 3) */
+  int flatten;         /* PPMFlatteningParameter (0, 1, 2 or 3) */
   int ncolour;         /* NumberOfColours: advected colour fields after the hydro fields */
   int riemann;         /* RiemannSolver (typedefs.h:279-280): 5 TwoShock (0 taken as 5),
                           1 HLL, 4 HLLC */

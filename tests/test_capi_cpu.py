@@ -39,7 +39,7 @@ def test_version_and_error_strings():
 
 
 def test_unsupported_configuration_is_rejected_before_any_device_work():
-    # Options outside this library (flattening type 2, diffusion, steepening other than
+    # Options outside this library (flattening types above 3, diffusion, steepening other than
     # 0/1, more colours than MAX_COLOR, Riemann solvers other than two-shock, HLL and
     # HLLC): the caller keeps the Fortran path.  The context pointer is never touched.
     L = capi.lib()
@@ -47,7 +47,7 @@ def test_unsupported_configuration_is_rejected_before_any_device_work():
     g = H.Grid.uniform((8, 8, 8))
     hp = H.HydroParams()
     f = H.new_fields(g, False)
-    for field, value in (("flattening", 2), ("diffusion", 1), ("steepening", 2),
+    for field, value in (("flattening", 4), ("diffusion", 1), ("steepening", 2),
                          ("number_of_colours", 46), ("number_of_colours", -1),
                          ("riemann_solver", 2), ("riemann_solver", 6)):
         P = capi.make_params(hp, 0.1)

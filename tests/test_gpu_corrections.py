@@ -1,4 +1,4 @@
-"""Slope flattening (PPMFlatteningParameter 1 and 3, calcdiss.F) and density steepening
+"""Slope flattening (PPMFlatteningParameter 1, 2 and 3, calcdiss.F) and density steepening
 (PPMSteepeningParameter 1, inteuler.F:166-193) on the GPU against the CPU oracle:
 bit-identical fields after every step on shock-dominated problems (a Sedov blast, a
 random supersonic state, the Sod tube), for single grids and a batched level."""
@@ -15,7 +15,7 @@ from shocktube_driver import GOLDEN, check_against_exact
 
 pytestmark = pytest.mark.gpu
 
-CORRECTIONS = [(1, 0), (3, 0), (0, 1), (3, 1), (1, 1)]
+CORRECTIONS = [(1, 0), (2, 0), (3, 0), (0, 1), (3, 1), (1, 1), (2, 1)]
 
 
 @pytest.fixture(scope="module")
@@ -111,7 +111,7 @@ def test_level_with_corrections_matches_per_grid_and_oracle(ctx):
 
 def test_unsupported_flattening_types_are_rejected(ctx):
     g = H.Grid.uniform((8, 8, 8))
-    for flatten in (2, 4):
+    for flatten in (4, 5):
         hp = H.HydroParams(dual=True, flatten=flatten)
         f = random_state(g, hp, seed=1)
         with pytest.raises(capi.PPMError) as e:

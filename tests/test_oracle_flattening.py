@@ -1,4 +1,4 @@
-"""The oracle's slope flattening (calcdiss.F types 1 and 3) and density steepening
+"""The oracle's slope flattening (calcdiss.F types 1, 2 and 3) and density steepening
 (inteuler.F:166-193, intvar.F:106-113), against the reference's own answer tests: every
 shock tube (Sod, Toro 1-7) still passes at the reference's tolerances with the
 corrections on, the corrections change the shocked solutions, and on smooth data
@@ -34,7 +34,7 @@ def _run(name, dual, flatten, steepen, monkeypatch):
     return SD.run_problem(name, _step, _dt, dual=dual)
 
 
-@pytest.mark.parametrize("flatten,steepen", [(1, 0), (3, 0), (0, 1), (3, 1)])
+@pytest.mark.parametrize("flatten,steepen", [(1, 0), (2, 0), (3, 0), (0, 1), (3, 1), (2, 1)])
 @pytest.mark.parametrize("name", sorted(SD.GOLDEN["problems"]))
 def test_shock_tubes_pass_with_corrections(name, flatten, steepen, monkeypatch):
     g, hp, f, cycles = _run(name, True, flatten, steepen, monkeypatch)
@@ -42,14 +42,14 @@ def test_shock_tubes_pass_with_corrections(name, flatten, steepen, monkeypatch):
     assert SD.check_against_exact(name, g, hp, f) == []
 
 
-@pytest.mark.parametrize("flatten,steepen", [(1, 0), (3, 0), (0, 1)])
+@pytest.mark.parametrize("flatten,steepen", [(1, 0), (2, 0), (3, 0), (0, 1)])
 def test_corrections_act_on_sod(flatten, steepen, monkeypatch):
     _, _, plain, _ = _run("SodShockTube", True, 0, 0, monkeypatch)
     _, _, corr, _ = _run("SodShockTube", True, flatten, steepen, monkeypatch)
     assert not np.array_equal(plain["d"], corr["d"])
 
 
-@pytest.mark.parametrize("flatten", [1, 3])
+@pytest.mark.parametrize("flatten", [1, 2, 3])
 def test_flattening_leaves_smooth_flow_unchanged(flatten):
     g = H.Grid.uniform((24, 6, 5))
     hp = H.HydroParams(gamma=1.4, cfl=0.4, dual=True)
