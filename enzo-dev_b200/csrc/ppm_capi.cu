@@ -86,6 +86,8 @@ struct FluxPhase {
   int start[3], dim[3];
   long long offset;
   int correct_left, correct_right;
+  int id[3], io[3], rd[3], ro[3];
+  int subling;
   const double* il[6];
   double* rl[6];
   const double* ir[6];
@@ -1857,11 +1859,15 @@ static int copy_zones_level(ppm_b200_context* ctx, ppm_b200_grid* grids, int ngr
 // the phases and their index arithmetic on the host (Grid_CorrectForRefinedFluxes.C:
 // 118-266), the flux arrays copied to the device, one kernel, the refined fluxes (which
 // an undone correction resets to the initial ones) copied back.
+// subling: the SUBling calls (initial = the grid's own boundary fluxes, the same for every
+// refined entry), with the level's extent gdims and periodic faces (:147-221, :284-305)
 static int correct_fluxes(ppm_b200_context* ctx, const ppm_b200_params* p, ppm_b200_grid* g,
                           int memory, int nsub, const ppm_b200_fluxes* initial,
-                          ppm_b200_fluxes* refined, const long long gl[3]) {
+                          ppm_b200_fluxes* refined, const long long gl[3], bool subling = false,
+                          const long long* gdims = nullptr, const int* periodic = nullptr) {
   if (!ctx || !p || !g || nsub < 0 || (nsub > 0 && (!initial || !refined)) || !gl)
     return PPM_B200_ERR_INVALID;
+  if (subling && (!gdims || !periodic)) return PPM_B200_ERR_INVALID;
   if (nsub == 0) return PPM_B200_OK;
   if (g->rank < 1 || g->rank > 3) return PPM_B200_ERR_INVALID;
   CK(cudaSetDevice(ctx->device));
@@ -1877,69 +1883,125 @@ static int correct_fluxes(ppm_b200_context* ctx, const ppm_b200_params* p, ppm_b
   struct HostPhase {
     ppm::FluxPhase ph;
     int n, dim;
-    size_t count;
+    size_t icount, rcount;  // initial / refined flux values per array
   };
   std::vector<HostPhase> phases;
   for (int n = 0; n < nsub; ++n) {
-    const ppm_b200_fluxes& I = initial[n];
+    const ppm_b200_fluxes& I = subling ? initial[0] : initial[n];
     const ppm_b200_fluxes& R = refined[n];
     for (int dim = 0; dim < rank; ++dim) {
       if (GD[dim] <= 1) continue;
       ppm::FluxPhase ph{};
-      int Start[3] = {0, 0, 0}, End[3] = {0, 0, 0};
+      ph.subling = subling ? 1 : 0;
+      ph.correct_left = ph.correct_right = 1;
+      long long rls[3], rle[3];
+      int RefinedDim[3] = {0, 0, 0}, RefinedOffset[3] = {0, 0, 0}, InitialOffset[3] = {0, 0, 0};
+      for (int i = 0; i < 3; ++i) {
+        rls[i] = R.left_start[dim][i];
+        rle[i] = R.left_end[dim][i];
+      }
+      if (subling) {
+        const long long GlobalDim = gdims[dim];
+        for (int i = 0; i < 3; ++i)
+          RefinedDim[i] = (int)(R.left_end[dim][i] - R.left_start[dim][i] + 1);
+        long long rrs = R.right_start[dim][dim];
+        if (rls[dim] == 0 && periodic[dim]) {
+          rls[dim] = rle[dim] = GlobalDim - 1;
+        } else {
+          rls[dim]--;
+          rle[dim]--;
+        }
+        if (rrs == GlobalDim - 1 && periodic[dim]) rrs = 0; else rrs++;
+        ph.correct_right = I.right_start[dim][dim] == rls[dim] ? 1 : 0;
+        ph.correct_left = I.left_start[dim][dim] == rrs ? 1 : 0;
+        for (int i = 0; i < 3; ++i)
+          RefinedOffset[i] = (int)std::max<long long>(I.left_start[dim][i] - rls[i], 0);
+        rls[dim] = 0;
+        RefinedOffset[dim] = 0;
+      }
+      if (!ph.correct_left && !ph.correct_right) continue;
+      int Start[3] = {0, 0, 0}, End[3] = {0, 0, 0}, Dim[3];
       for (int i = 0; i < rank; ++i) {
-        Start[i] = (int)(std::max(I.left_start[dim][i], R.left_start[dim][i]) - gl[i]);
-        End[i] = (int)(std::min(I.left_end[dim][i], R.left_end[dim][i]) - gl[i]);
+        Start[i] = (int)(std::max(I.left_start[dim][i], rls[i]) - gl[i]);
+        End[i] = (int)(std::min(I.left_end[dim][i], rle[i]) - gl[i]);
         if (Start[i] < 0 || End[i] > GD[i]) return PPM_B200_ERR_INVALID;
       }
       Start[dim] = std::max(Start[dim] - 1, 0);
       End[dim] = Start[dim];
+      for (int i = 0; i < 3; ++i) Dim[i] = End[i] - Start[i] + 1;
       long long off = I.right_start[dim][dim] - I.left_start[dim][dim] + 2;
       off = std::min<long long>(off, GD[dim] - 1);
-      ph.correct_left = Start[dim] == g->start[dim] - 1 ? 0 : 1;
-      ph.correct_right = Start[dim] + off == g->end[dim] + 1 ? 0 : 1;
+      if (subling) {
+        off -= 2;
+        Start[dim]++;
+        End[dim]++;
+        for (int i = 0; i < rank; ++i) {
+          if (i != dim) {
+            Dim[i] = g->end[i] - g->start[i] + 1;
+            InitialOffset[i] = (int)std::max<long long>(rls[i] - I.left_start[dim][i], 0);
+          } else {
+            Dim[i] = 1;
+            InitialOffset[i] = 0;
+          }
+        }
+      }
+      if (Start[dim] == g->start[dim] - 1) ph.correct_left = 0;
+      if (Start[dim] + off == g->end[dim] + 1) ph.correct_right = 0;
+      const long long off_dim = off;
       for (int i = 0; i < dim; ++i) off *= GD[i];
       ph.offset = off;
       for (int i = 0; i < 3; ++i) {
         ph.start[i] = Start[i];
         ph.dim[i] = End[i] - Start[i] + 1;
+        ph.id[i] = Dim[i];
+        ph.io[i] = InitialOffset[i];
+        ph.rd[i] = subling ? RefinedDim[i] : Dim[i];
+        ph.ro[i] = subling ? RefinedOffset[i] : 0;
       }
-      // the layer's zones stay inside the grid
-      for (int i = 0; i < 3; ++i)
+      // the layers' zones and flux indexes stay inside the grid and the flux arrays
+      for (int i = 0; i < 3; ++i) {
         if (ph.start[i] < 0 || ph.start[i] + ph.dim[i] > GD[i]) return PPM_B200_ERR_INVALID;
-      if (ph.start[dim] + (off / (dim == 0 ? 1 : (dim == 1 ? GD[0] : (long long)GD[0] * GD[1]))) >=
-          GD[dim])
+        if (ph.io[i] + ph.dim[i] > ph.id[i] || (subling && ph.ro[i] + ph.dim[i] > ph.rd[i]))
+          return PPM_B200_ERR_INVALID;
+      }
+      if (ph.start[dim] + off_dim >= GD[dim] || ph.start[dim] + off_dim < 0)
         return PPM_B200_ERR_INVALID;
       for (int s = 0; s < 6; ++s)
         if (present[s] && (!I.left[s][dim] || !I.right[s][dim] || !R.left[s][dim] ||
                            !R.right[s][dim]))
           return PPM_B200_ERR_INVALID;
-      const size_t count = (size_t)ph.dim[0] * ph.dim[1] * ph.dim[2];
-      phases.push_back({ph, n, dim, count});
+      const size_t icount = (size_t)ph.id[0] * ph.id[1] * ph.id[2];
+      const size_t rcount = (size_t)ph.rd[0] * ph.rd[1] * ph.rd[2];
+      phases.push_back({ph, n, dim, icount, rcount});
     }
+  }
+  if (phases.empty()) {
+    if (memory == PPM_B200_MEM_HOST) CK(cudaStreamSynchronize(ctx->stream));
+    return PPM_B200_OK;
   }
   // flux arrays on the device: per phase and present field, il | rl | ir | rr
   size_t total = 0;
   for (const auto& h : phases)
     for (int s = 0; s < 6; ++s)
-      if (present[s]) total += 4 * h.count;
+      if (present[s]) total += 2 * h.icount + 2 * h.rcount;
   rc = ensure(ctx, ctx->flux_fix, std::max<size_t>(total, 1) * sizeof(double) +
                                       phases.size() * sizeof(ppm::FluxPhase) + 256);
   if (rc) return rc;
   double* dev = (double*)ctx->flux_fix.p;
   size_t at = 0;
   for (auto& h : phases) {
-    const ppm_b200_fluxes& I = initial[h.n];
+    const ppm_b200_fluxes& I = subling ? initial[0] : initial[h.n];
     const ppm_b200_fluxes& R = refined[h.n];
     for (int s = 0; s < 6; ++s) {
       if (!present[s]) continue;
       const double* src[4] = {I.left[s][h.dim], R.left[s][h.dim], I.right[s][h.dim],
                               R.right[s][h.dim]};
+      const size_t cnt[4] = {h.icount, h.rcount, h.icount, h.rcount};
       double* dst[4];
       for (int q = 0; q < 4; ++q) {
         dst[q] = dev + at;
-        at += h.count;
-        CK(cudaMemcpyAsync(dst[q], src[q], h.count * sizeof(double), cudaMemcpyHostToDevice,
+        at += cnt[q];
+        CK(cudaMemcpyAsync(dst[q], src[q], cnt[q] * sizeof(double), cudaMemcpyHostToDevice,
                            ctx->stream));
       }
       h.ph.il[s] = dst[0];
@@ -1969,9 +2031,9 @@ static int correct_fluxes(ppm_b200_context* ctx, const ppm_b200_params* p, ppm_b
     ppm_b200_fluxes& R = refined[h.n];
     for (int s = 0; s < 6; ++s) {
       if (!present[s]) continue;
-      CK(cudaMemcpyAsync(R.left[s][h.dim], h.ph.rl[s], h.count * sizeof(double),
+      CK(cudaMemcpyAsync(R.left[s][h.dim], h.ph.rl[s], h.rcount * sizeof(double),
                          cudaMemcpyDeviceToHost, ctx->stream));
-      CK(cudaMemcpyAsync(R.right[s][h.dim], h.ph.rr[s], h.count * sizeof(double),
+      CK(cudaMemcpyAsync(R.right[s][h.dim], h.ph.rr[s], h.rcount * sizeof(double),
                          cudaMemcpyDeviceToHost, ctx->stream));
     }
   }
@@ -2222,6 +2284,15 @@ int ppm_b200_correct_fluxes(ppm_b200_context* ctx, const ppm_b200_params* params
                             const ppm_b200_fluxes* initial, ppm_b200_fluxes* refined,
                             const long long grid_global_start[3]) {
   return correct_fluxes(ctx, params, grid, memory, nsub, initial, refined, grid_global_start);
+}
+
+int ppm_b200_correct_fluxes_sublings(ppm_b200_context* ctx, const ppm_b200_params* params,
+                                     ppm_b200_grid* grid, int memory, int nsib,
+                                     const ppm_b200_fluxes* own, ppm_b200_fluxes* refined,
+                                     const long long grid_global_start[3],
+                                     const long long level_dims[3], const int periodic[3]) {
+  return correct_fluxes(ctx, params, grid, memory, nsib, own, refined, grid_global_start, true,
+                        level_dims, periodic);
 }
 
 }  // extern "C"

@@ -253,6 +253,10 @@ struct FluxPhase {
   int start[3], dim[3];      // the left layer in this grid's zones, and its extents
   long long offset;          // from a left-layer zone to its right-layer zone
   int correct_left, correct_right;
+  // flux indexes of a layer zone (i, j, k): initial ((k+io2)*id1 + (j+io1))*id0 + i+io0,
+  // refined likewise with rd / ro (Grid_CorrectForRefinedFluxes.C:458-468)
+  int id[3], io[3], rd[3], ro[3];
+  int subling;               // SUBlingGrid: refined fluxes of a sibling's subgrid
   // per field slot (d, te, v1, v2, v3, ge): initial / refined left and right fluxes,
   // indexed like the layer (null: field absent)
   const double* il[6];
@@ -284,7 +288,11 @@ __global__ void __launch_bounds__(256) correct_fluxes_kernel(const FluxFix X,
       const long long c = ((long long)(k + P.start[2]) * X.dims[1] + (j + P.start[1])) * X.dims[0] +
                           (i + P.start[0]);
       const long long c2 = c + P.offset;
-      const long long x = z;  // the flux index ((k*Dim1 + j)*Dim0 + i)
+      const long long x = ((long long)(k + P.io[2]) * P.id[1] + (j + P.io[1])) * P.id[0] +
+                          (i + P.io[0]);
+      const long long xr = ((long long)(k + P.ro[2]) * P.rd[1] + (j + P.ro[1])) * P.rd[0] +
+                           (i + P.ro[0]);
+      const bool sub = P.subling != 0;
       // conserved quantities on both layers (:304-322): every field but density
       for (int s = 1; s < 6; ++s)
         if (F[s]) {
@@ -294,12 +302,13 @@ __global__ void __launch_bounds__(256) correct_fluxes_kernel(const FluxFix X,
       for (int q = 0; q < 6; ++q) {
         const int f = order[q];
         if (!F[f]) continue;
+        // a SUBling's correction uses its opposite face (:495-542)
         if (P.correct_left) {
-          const double amount = P.il[f][x] - P.rl[f][x];
+          const double amount = sub ? -(P.il[f][x] - P.rr[f][xr]) : P.il[f][x] - P.rl[f][x];
           F[f][c] += amount;
         }
         if (P.correct_right) {
-          const double amount = -(P.ir[f][x] - P.rr[f][x]);
+          const double amount = sub ? P.ir[f][x] - P.rl[f][xr] : -(P.ir[f][x] - P.rr[f][x]);
           F[f][c2] += amount;
         }
         if (f == 0 || f == 1 || f == 5) {  // density and the energies stay positive
@@ -307,16 +316,27 @@ __global__ void __launch_bounds__(256) correct_fluxes_kernel(const FluxFix X,
             for (int u = 0; u < 6; ++u) {
               const int g = order[u];
               if (!F[g]) continue;
-              if (u <= q) F[g][c] -= (P.il[g][x] - P.rl[g][x]);
-              P.rl[g][x] = P.il[g][x];
+              if (sub) {
+                if (u <= q) F[g][c] -= -(P.il[g][x] - P.rr[g][xr]);
+                P.rr[g][xr] = P.il[g][x];
+              } else {
+                if (u <= q) F[g][c] -= (P.il[g][x] - P.rl[g][x]);
+                P.rl[g][x] = P.il[g][x];
+              }
             }
           }
           if (P.correct_right && F[f][c2] <= 0) {
             for (int u = 0; u < 6; ++u) {
               const int g = order[u];
               if (!F[g]) continue;
-              if (u <= q) F[g][c2] -= -(P.ir[g][x] - P.rr[g][x]);
-              P.rr[g][x] = P.ir[g][x];
+              if (sub) {
+                // the reference subtracts the triggering field's amount here (:643-645)
+                if (u <= q) F[g][c2] -= (P.ir[f][x] - P.rl[f][xr]);
+                P.rl[g][xr] = P.ir[g][x];
+              } else {
+                if (u <= q) F[g][c2] -= -(P.ir[g][x] - P.rr[g][x]);
+                P.rr[g][x] = P.ir[g][x];
+              }
             }
           }
         }

@@ -1345,6 +1345,12 @@ __global__ void __launch_bounds__(128) fallback_kernel(const __grid_constant__ B
 #ifndef PPM_COLOURS_PER_THREAD
 #define PPM_COLOURS_PER_THREAD 2
 #endif
+// below this many (pencil block, colour) pairs a sweep runs one colour per thread: two
+// would leave too few warps to hide the march's load latency (128^3 with 4 colours: 7.5
+// of 16 warps active per SM)
+#ifndef PPM_COLOUR_WIDE_BLOCKS
+#define PPM_COLOUR_WIDE_BLOCKS (148 * 8)
+#endif
 constexpr double kColourFloor = 1.0e-35;        // color_floor, fortran.def:8
 constexpr double kMinColour = 1.0e-5 * kTiny;   // min_color, euler.F:104-105
 
@@ -1592,7 +1598,11 @@ void launch_stages(const BatchArgs& B, int64_t march_blocks, int64_t riemann_blo
   if (B.ncolour > 0) {
     constexpr int cpt = PPM_COLOURS_PER_THREAD;
     const int64_t chunks = (B.ncolour + cpt - 1) / cpt;
-    colour_kernel<DUAL, ONE, cpt><<<(unsigned)(march_blocks * chunks), kMarchThreads, 0, st>>>(B);
+    if (march_blocks * B.ncolour < PPM_COLOUR_WIDE_BLOCKS)
+      colour_kernel<DUAL, ONE, 1>
+          <<<(unsigned)(march_blocks * B.ncolour), kMarchThreads, 0, st>>>(B);
+    else
+      colour_kernel<DUAL, ONE, cpt><<<(unsigned)(march_blocks * chunks), kMarchThreads, 0, st>>>(B);
   }
   mark(5);
 }

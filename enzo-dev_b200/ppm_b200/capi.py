@@ -39,6 +39,7 @@ EXPORTS = (
     "ppm_b200_euler_sweep_static", "ppm_b200_solve_level", "ppm_b200_set_graphs",
     "ppm_b200_compute_timestep_level", "ppm_b200_set_boundary_level",
     "ppm_b200_copy_zones_level", "ppm_b200_correct_fluxes", "ppm_b200_debug_tma_stall",
+    "ppm_b200_correct_fluxes_sublings",
     "ppm_b200_profile_stages", "ppm_b200_set_guess", "ppm_b200_riemann_log",
     "ppm_b200_riemann_log_count", "ppm_b200_guess_features", "ppm_b200_guess_grad",
     "ppm_b200_guess_adam", "ppm_b200_guess_eval", "ppm_b200_expansion_terms",
@@ -183,6 +184,11 @@ def lib(build_if_missing: bool = True):
                                           C.c_int, C.POINTER(Fluxes), C.POINTER(Fluxes),
                                           C.c_longlong * 3]
     L.ppm_b200_correct_fluxes.restype = C.c_int
+    L.ppm_b200_correct_fluxes_sublings.argtypes = [vp, C.POINTER(Params), C.POINTER(GridDesc),
+                                                   C.c_int, C.c_int, C.POINTER(Fluxes),
+                                                   C.POINTER(Fluxes), C.c_longlong * 3,
+                                                   C.c_longlong * 3, C.c_int * 3]
+    L.ppm_b200_correct_fluxes_sublings.restype = C.c_int
     L.ppm_b200_debug_tma_stall.argtypes = [vp, C.c_int]
     L.ppm_b200_debug_tma_stall.restype = C.c_int
     L.ppm_b200_set_boundary_level.argtypes = [vp, C.POINTER(GridDesc), C.c_int, C.c_int,
@@ -483,6 +489,24 @@ class Context:
                                             ref, g)
         if rc != OK:
             raise PPMError(rc, "ppm_b200_correct_fluxes")
+
+    def correct_fluxes_sublings(self, grid, hp, fields, own, refined, ggs, level_dims, periodic,
+                                memory=MEM_HOST):
+        """The SUBling calls of grid::CorrectForRefinedFluxes for one grid: own = its own
+        boundary flux box, refined = the sibling subgrids' projected flux boxes (dicts as
+        for make_fluxes; refined arrays updated where a correction is undone)."""
+        P = make_params(hp, 0.0)
+        G, keep = make_grid(grid, fields)
+        n = len(refined)
+        ow = make_fluxes(own)
+        ref = (Fluxes * n)(*[make_fluxes(b) for b in refined])
+        g = (C.c_longlong * 3)(*[int(x) for x in ggs])
+        ld = (C.c_longlong * 3)(*[int(x) for x in level_dims])
+        per = (C.c_int * 3)(*[int(bool(x)) for x in periodic])
+        rc = self.L.ppm_b200_correct_fluxes_sublings(self.h, C.byref(P), C.byref(G), int(memory),
+                                                     n, C.byref(ow), ref, g, ld, per)
+        if rc != OK:
+            raise PPMError(rc, "ppm_b200_correct_fluxes_sublings")
 
     def copy_zones_level(self, grids, fields_list, left, domain, periodic, dual):
         """grid::CopyZonesFromGrid over a level (siblings and periodic images) on device

@@ -255,6 +255,23 @@ int ppm_b200_correct_fluxes(ppm_b200_context *ctx, const ppm_b200_params *params
                             const ppm_b200_fluxes *initial, ppm_b200_fluxes *refined,
                             const long long grid_global_start[3]);
 
+/* The SUBling calls of grid::CorrectForRefinedFluxes (SUBlingGrid == TRUE,
+   UpdateFromFinerGrids.C:176-206, Grid_CorrectForRefinedFluxes.C:147-305, :455-656), in
+   order, for the nsib sibling subgrids of a grid: refined[n] holds sibling subgrid n's
+   refined boundary fluxes projected to this level (GetProjectedBoundaryFluxes), own
+   this grid's own boundary fluxes (SubgridFluxesEstimate[grid][NumberOfSubgrids - 1]).
+   The grid's edge layer that touches a sibling's projected face is corrected by the
+   difference; a periodic level boundary wraps.  level_dims: the level's extent in zones
+   (nint((DomainRightEdge - DomainLeftEdge)/CellWidth)) per axis; periodic: periodic
+   faces per axis.  The refined index boxes are read only; refined flux values are
+   updated where a correction is undone.  Cartesian, hydro fields, as
+   ppm_b200_correct_fluxes. */
+int ppm_b200_correct_fluxes_sublings(ppm_b200_context *ctx, const ppm_b200_params *params,
+                                     ppm_b200_grid *grid, int memory, int nsib,
+                                     const ppm_b200_fluxes *own, ppm_b200_fluxes *refined,
+                                     const long long grid_global_start[3],
+                                     const long long level_dims[3], const int periodic[3]);
+
 /* Waits for all work queued on the context and returns the first error code
    recorded by device work since the last call; accumulates device counters
    into *stats (may be NULL). */

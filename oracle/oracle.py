@@ -126,6 +126,11 @@ def lib():
                                          C.POINTER(OraFluxes), C.POINTER(OraFluxes),
                                          C.c_longlong * 3]
         L.ora_correct_fluxes.restype = C.c_int
+        L.ora_correct_fluxes_sublings.argtypes = [C.POINTER(OraParams), dp * 6, C.c_int,
+                                                  C.POINTER(OraFluxes), C.POINTER(OraFluxes),
+                                                  C.c_longlong * 3, C.c_longlong * 3,
+                                                  C.c_int * 3]
+        L.ora_correct_fluxes_sublings.restype = C.c_int
         _lib = L
     return _lib
 
@@ -274,6 +279,23 @@ def correct_fluxes(grid, hp, fields, initial, refined, ggs):
     ref = (OraFluxes * n)(*refined)
     rc = L.ora_correct_fluxes(C.byref(P), _fields6(fields), n, ini, ref,
                               (C.c_longlong * 3)(*[int(x) for x in ggs]))
+    for k in range(n):
+        refined[k] = ref[k]
+    return rc
+
+
+def correct_fluxes_sublings(grid, hp, fields, own, refined, ggs, level_dims, periodic):
+    """The SUBling calls of grid::CorrectForRefinedFluxes on host fields, in place.  own:
+    OraFluxes of the grid's own boundary; refined: list of OraFluxes (updated where a
+    correction is undone).  Returns the C status."""
+    L = lib()
+    P = make_params(grid, hp, 0.0)
+    n = len(refined)
+    ref = (OraFluxes * n)(*refined)
+    rc = L.ora_correct_fluxes_sublings(C.byref(P), _fields6(fields), n, C.byref(own), ref,
+                                       (C.c_longlong * 3)(*[int(x) for x in ggs]),
+                                       (C.c_longlong * 3)(*[int(x) for x in level_dims]),
+                                       (C.c_int * 3)(*[int(bool(x)) for x in periodic]))
     for k in range(n):
         refined[k] = ref[k]
     return rc

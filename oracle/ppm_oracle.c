@@ -1548,131 +1548,220 @@ void ora_expansion_terms(const ora_params *P, double *const F[ORA_NFIELD],
 /* ------------------------------------------------------------------------ */
 /* Grid_CorrectForRefinedFluxes.C:38-760, proper subgrids, Cartesian         */
 /* ------------------------------------------------------------------------ */
-int ora_correct_fluxes(const ora_params *P, double *const F[ORA_NFIELD], int nsub,
-                       const ora_fluxes *IN, ora_fluxes *RF, const long long gl[3]) {
+/* One call of grid::CorrectForRefinedFluxes (Grid_CorrectForRefinedFluxes.C:38-760) for
+   one (initial, refined) pair.  subling: SUBlingGrid == TRUE, the refined fluxes of a
+   sibling's subgrid projected to this level, I the grid's own boundary fluxes; gdims and
+   periodic: the level's extent in zones and the periodic faces (:147-221). */
+static int correct_one(const ora_params *P, double *const F[ORA_NFIELD], const int *order,
+                       int nf, const ora_fluxes *I, ora_fluxes *R, const long long gl[3],
+                       int subling, const long long gdims[3], const int periodic[3]) {
   const int rank = P->rank;
   const int *GD = P->dims;
-  /* fields in the reference's BaryonField order (Density, TotalEnergy, InternalEnergy,
-     Velocity1..3); the correction list puts density and the energies first
-     (:288-303), then the remaining fields in that order (:337-350) */
-  int order[ORA_NFIELD], nf = 0;
-  const int base_order[ORA_NFIELD] = {ORA_D, ORA_TE, ORA_GE, ORA_V1, ORA_V2, ORA_V3};
-  for (int q = 0; q < ORA_NFIELD; q++) {
-    const int f = base_order[q];
-    if (!F[f]) continue;
-    if (f == ORA_GE && !P->dual) continue;
-    if (f >= ORA_V1 && f <= ORA_V3 && f - ORA_V1 >= rank) continue;
-    order[nf++] = f;
-  }
-  for (int n = 0; n < nsub; n++) {
-    const ora_fluxes *I = &IN[n];
-    ora_fluxes *R = &RF[n];
-    for (int dim = 0; dim < rank; dim++) {
-      if (GD[dim] <= 1) continue;
-      int Start[3] = {0, 0, 0}, End[3] = {0, 0, 0}, Dim[3];
+  for (int dim = 0; dim < rank; dim++) {
+    if (GD[dim] <= 1) continue;
+    int correct_left = 1, correct_right = 1;
+    long long rls[3], rle[3];  /* the refined box as the routine sees it along dim */
+    int RefinedDim[3] = {0, 0, 0}, RefinedOffset[3] = {0, 0, 0}, InitialOffset[3] = {0, 0, 0};
+    for (int i = 0; i < 3; i++) {
+      rls[i] = R->left_start[dim][i];
+      rle[i] = R->left_end[dim][i];
+    }
+    if (subling) {
+      const long long GlobalDim = gdims[dim];
+      for (int i = 0; i < 3; i++)
+        RefinedDim[i] = (int)(R->left_end[dim][i] - R->left_start[dim][i] + 1);
+      long long rrs = R->right_start[dim][dim];
+      /* a face on a periodic domain boundary wraps; otherwise step outward (:163-179) */
+      if (rls[dim] == 0 && periodic[dim]) {
+        rls[dim] = rle[dim] = GlobalDim - 1;
+      } else {
+        rls[dim]--;
+        rle[dim]--;
+      }
+      if (rrs == GlobalDim - 1 && periodic[dim])
+        rrs = 0;
+      else
+        rrs++;
+      correct_right = I->right_start[dim][dim] == rls[dim];
+      correct_left = I->left_start[dim][dim] == rrs;
+      for (int i = 0; i < 3; i++) {
+        const long long d = I->left_start[dim][i] - rls[i];
+        RefinedOffset[i] = (int)(d > 0 ? d : 0);
+      }
+      rls[dim] = 0;
+      RefinedOffset[dim] = 0;
+    }
+    if (!correct_left && !correct_right) continue;
+    int Start[3] = {0, 0, 0}, End[3] = {0, 0, 0}, Dim[3];
+    for (int i = 0; i < rank; i++) {
+      const long long s0 = I->left_start[dim][i] > rls[i] ? I->left_start[dim][i] : rls[i];
+      const long long e0 = I->left_end[dim][i] < rle[i] ? I->left_end[dim][i] : rle[i];
+      Start[i] = (int)(s0 - gl[i]);
+      End[i] = (int)(e0 - gl[i]);
+      if (Start[i] < 0 || End[i] > GD[i]) return -1;
+    }
+    /* the layer just outside the left face (:225-230) */
+    Start[dim] = Start[dim] - 1 > 0 ? Start[dim] - 1 : 0;
+    End[dim] = Start[dim];
+    for (int i = 0; i < 3; i++) Dim[i] = End[i] - Start[i] + 1;
+    /* :234-237 */
+    long long Offset = I->right_start[dim][dim] - I->left_start[dim][dim] + 2;
+    if (Offset > GD[dim] - 1) Offset = GD[dim] - 1;
+    if (subling) {  /* the grid's own edge layers (:284-305) */
+      Offset -= 2;
+      Start[dim]++;
+      End[dim]++;
       for (int i = 0; i < rank; i++) {
-        const long long s0 = I->left_start[dim][i] > R->left_start[dim][i] ? I->left_start[dim][i]
-                                                                           : R->left_start[dim][i];
-        const long long e0 = I->left_end[dim][i] < R->left_end[dim][i] ? I->left_end[dim][i]
-                                                                       : R->left_end[dim][i];
-        Start[i] = (int)(s0 - gl[i]);
-        End[i] = (int)(e0 - gl[i]);
-        if (Start[i] < 0 || End[i] > GD[i]) return -1;
+        if (i != dim) {
+          Dim[i] = P->end[i] - P->start[i] + 1;
+          const long long d = rls[i] - I->left_start[dim][i];
+          InitialOffset[i] = (int)(d > 0 ? d : 0);
+        } else {
+          Dim[i] = 1;
+          InitialOffset[i] = 0;
+        }
       }
-      /* the layer just outside the left face (:225-230) */
-      Start[dim] = Start[dim] - 1 > 0 ? Start[dim] - 1 : 0;
-      End[dim] = Start[dim];
-      for (int i = 0; i < 3; i++) Dim[i] = End[i] - Start[i] + 1;
-      /* :234-237 */
-      long long Offset = I->right_start[dim][dim] - I->left_start[dim][dim] + 2;
-      if (Offset > GD[dim] - 1) Offset = GD[dim] - 1;
-      /* a layer that is this grid's ghost zone is not corrected (:258-266) */
-      int correct_left = 1, correct_right = 1;
-      if (Start[dim] == P->start[dim] - 1) correct_left = 0;
-      if (Start[dim] + Offset == P->end[dim] + 1) correct_right = 0;
-      for (int i = 0; i < dim; i++) Offset *= GD[i];
+    }
+    /* a layer that is this grid's ghost zone is not corrected (:311-320) */
+    if (Start[dim] == P->start[dim] - 1) correct_left = 0;
+    if (Start[dim] + Offset == P->end[dim] + 1) correct_right = 0;
+    for (int i = 0; i < dim; i++) Offset *= GD[i];
 #define CELL(k, j, i) (((size_t)(k) * GD[1] + (j)) * GD[0] + (i))
-#define FLUX(k, j, i) (((size_t)((k) - Start[2]) * Dim[1] + ((j) - Start[1])) * Dim[0] + ((i) - Start[0]))
-      /* conserved quantities on both layers (:304-322): all but density */
-      for (int q = 0; q < nf; q++) {
-        const int f = order[q];
-        if (f == ORA_D) continue;
-        for (int k = Start[2]; k <= End[2]; k++)
-          for (int j = Start[1]; j <= End[1]; j++)
-            for (int i = Start[0]; i <= End[0]; i++) {
-              const size_t c = CELL(k, j, i);
-              F[f][c] *= F[ORA_D][c];
-              F[f][c + Offset] *= F[ORA_D][c + Offset];
+#define FLUX(k, j, i)                                                                  \
+  (((size_t)((k) - Start[2] + InitialOffset[2]) * Dim[1] + ((j) - Start[1] + InitialOffset[1])) * \
+       Dim[0] + ((i) - Start[0] + InitialOffset[0]))
+#define RFLUX(k, j, i)                                                                 \
+  (((size_t)((k) - Start[2] + RefinedOffset[2]) * RefinedDim[1] +                      \
+    ((j) - Start[1] + RefinedOffset[1])) * RefinedDim[0] + ((i) - Start[0] + RefinedOffset[0]))
+    /* conserved quantities on both layers (:370-394): all but density */
+    for (int q = 0; q < nf; q++) {
+      const int f = order[q];
+      if (f == ORA_D) continue;
+      for (int k = Start[2]; k <= End[2]; k++)
+        for (int j = Start[1]; j <= End[1]; j++)
+          for (int i = Start[0]; i <= End[0]; i++) {
+            const size_t c = CELL(k, j, i);
+            F[f][c] *= F[ORA_D][c];
+            F[f][c + Offset] *= F[ORA_D][c + Offset];
+          }
+    }
+    /* the corrections with the undo for density and energies (:455-656) */
+    for (int q = 0; q < nf; q++) {
+      const int f = order[q];
+      for (int k = Start[2]; k <= End[2]; k++)
+        for (int j = Start[1]; j <= End[1]; j++)
+          for (int i = Start[0]; i <= End[0]; i++) {
+            const size_t c = CELL(k, j, i), x = FLUX(k, j, i);
+            const size_t xr = subling ? RFLUX(k, j, i) : x;
+            if (correct_left) {
+              const double amount = subling ? -(I->left[f][dim][x] - R->right[f][dim][xr])
+                                            : I->left[f][dim][x] - R->left[f][dim][x];
+              F[f][c] += amount;
             }
-      }
-      /* the corrections with the undo for density and energies (:422-640) */
-      for (int q = 0; q < nf; q++) {
-        const int f = order[q];
-        for (int k = Start[2]; k <= End[2]; k++)
-          for (int j = Start[1]; j <= End[1]; j++)
-            for (int i = Start[0]; i <= End[0]; i++) {
-              const size_t c = CELL(k, j, i), x = FLUX(k, j, i);
-              if (correct_left) {
-                const double amount = I->left[f][dim][x] - R->left[f][dim][x];
-                F[f][c] += amount;
-              }
-              if (correct_right) {
-                const double amount = -(I->right[f][dim][x] - R->right[f][dim][x]);
-                F[f][c + Offset] += amount;
-              }
-              if (f == ORA_D || f == ORA_TE || f == ORA_GE) {
-                if (correct_left && F[f][c] <= 0) {
-                  for (int u = 0; u < nf; u++) {
-                    const int g = order[u];
+            if (correct_right) {
+              const double amount = subling ? I->right[f][dim][x] - R->left[f][dim][xr]
+                                            : -(I->right[f][dim][x] - R->right[f][dim][x]);
+              F[f][c + Offset] += amount;
+            }
+            if (f == ORA_D || f == ORA_TE || f == ORA_GE) {
+              if (correct_left && F[f][c] <= 0) {
+                for (int u = 0; u < nf; u++) {
+                  const int g = order[u];
+                  if (subling) {
+                    if (u <= q) F[g][c] -= -(I->left[g][dim][x] - R->right[g][dim][xr]);
+                    R->right[g][dim][xr] = I->left[g][dim][x];
+                  } else {
                     if (u <= q) F[g][c] -= (I->left[g][dim][x] - R->left[g][dim][x]);
                     R->left[g][dim][x] = I->left[g][dim][x];
                   }
                 }
-                if (correct_right && F[f][c + Offset] <= 0) {
-                  for (int u = 0; u < nf; u++) {
-                    const int g = order[u];
+              }
+              if (correct_right && F[f][c + Offset] <= 0) {
+                for (int u = 0; u < nf; u++) {
+                  const int g = order[u];
+                  if (subling) {
+                    /* the reference subtracts the triggering field's amount from every
+                       undone field here (:643-645) */
+                    if (u <= q) F[g][c + Offset] -= (I->right[f][dim][x] - R->left[f][dim][xr]);
+                    R->left[g][dim][xr] = I->right[g][dim][x];
+                  } else {
                     if (u <= q) F[g][c + Offset] -= -(I->right[g][dim][x] - R->right[g][dim][x]);
                     R->right[g][dim][x] = I->right[g][dim][x];
                   }
                 }
               }
             }
-      }
-      /* back to specific quantities with the new density (:683-700) */
-      for (int q = 0; q < nf; q++) {
-        const int f = order[q];
-        if (f == ORA_D) continue;
-        for (int k = Start[2]; k <= End[2]; k++)
-          for (int j = Start[1]; j <= End[1]; j++)
-            for (int i = Start[0]; i <= End[0]; i++) {
-              const size_t c = CELL(k, j, i);
-              F[f][c] /= F[ORA_D][c];
-              F[f][c + Offset] /= F[ORA_D][c + Offset];
+          }
+    }
+    /* back to specific quantities with the new density (:683-700) */
+    for (int q = 0; q < nf; q++) {
+      const int f = order[q];
+      if (f == ORA_D) continue;
+      for (int k = Start[2]; k <= End[2]; k++)
+        for (int j = Start[1]; j <= End[1]; j++)
+          for (int i = Start[0]; i <= End[0]; i++) {
+            const size_t c = CELL(k, j, i);
+            F[f][c] /= F[ORA_D][c];
+            F[f][c + Offset] /= F[ORA_D][c + Offset];
+          }
+    }
+    /* total and gas energy made consistent again (:704-742) */
+    if (P->dual) {
+      for (int k = Start[2]; k <= End[2]; k++)
+        for (int j = Start[1]; j <= End[1]; j++)
+          for (int i = Start[0]; i <= End[0]; i++) {
+            const size_t c1 = CELL(k, j, i), c2 = c1 + Offset;
+            F[ORA_GE][c1] = fmax2(F[ORA_GE][c1], P->tiny_number);
+            F[ORA_GE][c2] = fmax2(F[ORA_GE][c2], P->tiny_number);
+            F[ORA_TE][c1] = F[ORA_GE][c1] + 0.5 * F[ORA_V1][c1] * F[ORA_V1][c1];
+            F[ORA_TE][c2] = F[ORA_GE][c2] + 0.5 * F[ORA_V1][c2] * F[ORA_V1][c2];
+            if (rank > 1) {
+              F[ORA_TE][c1] += 0.5 * F[ORA_V2][c1] * F[ORA_V2][c1];
+              F[ORA_TE][c2] += 0.5 * F[ORA_V2][c2] * F[ORA_V2][c2];
             }
-      }
-      /* total and gas energy made consistent again (:704-742) */
-      if (P->dual) {
-        for (int k = Start[2]; k <= End[2]; k++)
-          for (int j = Start[1]; j <= End[1]; j++)
-            for (int i = Start[0]; i <= End[0]; i++) {
-              const size_t c1 = CELL(k, j, i), c2 = c1 + Offset;
-              F[ORA_GE][c1] = fmax2(F[ORA_GE][c1], P->tiny_number);
-              F[ORA_GE][c2] = fmax2(F[ORA_GE][c2], P->tiny_number);
-              F[ORA_TE][c1] = F[ORA_GE][c1] + 0.5 * F[ORA_V1][c1] * F[ORA_V1][c1];
-              F[ORA_TE][c2] = F[ORA_GE][c2] + 0.5 * F[ORA_V1][c2] * F[ORA_V1][c2];
-              if (rank > 1) {
-                F[ORA_TE][c1] += 0.5 * F[ORA_V2][c1] * F[ORA_V2][c1];
-                F[ORA_TE][c2] += 0.5 * F[ORA_V2][c2] * F[ORA_V2][c2];
-              }
-              if (rank > 2) {
-                F[ORA_TE][c1] += 0.5 * F[ORA_V3][c1] * F[ORA_V3][c1];
-                F[ORA_TE][c2] += 0.5 * F[ORA_V3][c2] * F[ORA_V3][c2];
-              }
+            if (rank > 2) {
+              F[ORA_TE][c1] += 0.5 * F[ORA_V3][c1] * F[ORA_V3][c1];
+              F[ORA_TE][c2] += 0.5 * F[ORA_V3][c2] * F[ORA_V3][c2];
             }
-      }
+          }
+    }
 #undef CELL
 #undef FLUX
-    }
+#undef RFLUX
   }
+  return 0;
+}
+
+/* the fields in the order the routine corrects them: density and the energies first
+   (:341-360), then the remaining fields in BaryonField order (:396-452) */
+static int correction_order(const ora_params *P, double *const F[ORA_NFIELD], int *order) {
+  int nf = 0;
+  const int base_order[ORA_NFIELD] = {ORA_D, ORA_TE, ORA_GE, ORA_V1, ORA_V2, ORA_V3};
+  for (int q = 0; q < ORA_NFIELD; q++) {
+    const int f = base_order[q];
+    if (!F[f]) continue;
+    if (f == ORA_GE && !P->dual) continue;
+    if (f >= ORA_V1 && f <= ORA_V3 && f - ORA_V1 >= P->rank) continue;
+    order[nf++] = f;
+  }
+  return nf;
+}
+
+int ora_correct_fluxes(const ora_params *P, double *const F[ORA_NFIELD], int nsub,
+                       const ora_fluxes *IN, ora_fluxes *RF, const long long gl[3]) {
+  int order[ORA_NFIELD];
+  const int nf = correction_order(P, F, order);
+  for (int n = 0; n < nsub; n++)
+    if (correct_one(P, F, order, nf, &IN[n], &RF[n], gl, 0, 0, 0) != 0) return -1;
+  return 0;
+}
+
+int ora_correct_fluxes_sublings(const ora_params *P, double *const F[ORA_NFIELD], int nsib,
+                                const ora_fluxes *own, ora_fluxes *RF, const long long gl[3],
+                                const long long gdims[3], const int periodic[3]) {
+  int order[ORA_NFIELD];
+  const int nf = correction_order(P, F, order);
+  for (int n = 0; n < nsib; n++)
+    if (correct_one(P, F, order, nf, own, &RF[n], gl, 1, gdims, periodic) != 0) return -1;
   return 0;
 }

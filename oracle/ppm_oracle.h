@@ -144,6 +144,19 @@ void ora_expansion_terms(const ora_params *P, double *const fields[ORA_NFIELD],
 int ora_correct_fluxes(const ora_params *P, double *const fields[ORA_NFIELD], int nsub,
                        const ora_fluxes *initial, ora_fluxes *refined, const long long gl[3]);
 
+/* The SUBling calls of grid::CorrectForRefinedFluxes (SUBlingGrid == TRUE,
+   UpdateFromFinerGrids.C:176-206): for each sibling subgrid n, refined[n] holds its
+   refined boundary fluxes projected to this level and `own` this grid's own boundary
+   fluxes (SubgridFluxesEstimate[grid][NumberOfSubgrids - 1]); the grid's edge layers that
+   touch the sibling's projected faces are corrected (Grid_CorrectForRefinedFluxes.C:147-
+   305, :464-656).  gdims: the level's extent in zones per axis; periodic: periodic
+   faces per axis.  refined[n]'s index boxes are not modified; its flux values are where a
+   correction is undone.  Returns 0, or -1 if a flux box does not fit the grid. */
+int ora_correct_fluxes_sublings(const ora_params *P, double *const fields[ORA_NFIELD], int nsib,
+                                const ora_fluxes *own, ora_fluxes *refined,
+                                const long long gl[3], const long long gdims[3],
+                                const int periodic[3]);
+
 #ifdef __cplusplus
 }
 #endif
