@@ -98,6 +98,8 @@ struct FluxFix {
   int dims[3], rank, dual;
   double tiny_number;
   int nphases;
+  double* const* species;
+  int nspecies;
 };
 void launch_correct_fluxes(const FluxFix& X, const FluxPhase* phases, cudaStream_t st);
 }  // namespace ppm
@@ -1870,11 +1872,22 @@ static int correct_fluxes(ppm_b200_context* ctx, const ppm_b200_params* p, ppm_b
   if (subling && (!gdims || !periodic)) return PPM_B200_ERR_INVALID;
   if (nsub == 0) return PPM_B200_OK;
   if (g->rank < 1 || g->rank > 3) return PPM_B200_ERR_INVALID;
+  // species colours: the colours the caller marks as keeping their density fraction
+  const bool species = p->number_of_colours > 0 && p->colour_species != nullptr;
+  if (species) {
+    if (p->number_of_colours > PPM_B200_MAX_COLOURS || !g->colours) return PPM_B200_ERR_INVALID;
+    for (int n = 0; n < p->number_of_colours; ++n)
+      if (!g->colours[n]) return PPM_B200_ERR_INVALID;
+  }
   CK(cudaSetDevice(ctx->device));
   GridIO io;
   io.g = g;
-  int rc = stage_in(ctx, p, g, memory, io.user, io.acc);
+  int rc = stage_in(ctx, p, g, memory, io.user, io.acc, species);
   if (rc) return rc;
+  std::vector<double*> species_ptr;
+  if (species)
+    for (int n = 0; n < p->number_of_colours; ++n)
+      if (p->colour_species[n]) species_ptr.push_back(io.user.col[n]);
   const int rank = g->rank;
   const int* GD = g->dims;
   // fields present: d, te, v1..v_rank, ge if dual (slots of ppm_b200_fluxes)
@@ -1985,7 +1998,8 @@ static int correct_fluxes(ppm_b200_context* ctx, const ppm_b200_params* p, ppm_b
     for (int s = 0; s < 6; ++s)
       if (present[s]) total += 2 * h.icount + 2 * h.rcount;
   rc = ensure(ctx, ctx->flux_fix, std::max<size_t>(total, 1) * sizeof(double) +
-                                      phases.size() * sizeof(ppm::FluxPhase) + 256);
+                                      phases.size() * sizeof(ppm::FluxPhase) + 256 +
+                                      species_ptr.size() * sizeof(double*));
   if (rc) return rc;
   double* dev = (double*)ctx->flux_fix.p;
   size_t at = 0;
@@ -2016,7 +2030,13 @@ static int correct_fluxes(ppm_b200_context* ctx, const ppm_b200_params* p, ppm_b
   if ((uintptr_t)dph % alignof(ppm::FluxPhase)) return PPM_B200_ERR_CUDA;
   CK(cudaMemcpyAsync(dph, host_ph.data(), host_ph.size() * sizeof(ppm::FluxPhase),
                      cudaMemcpyHostToDevice, ctx->stream));
+  double** dsp = reinterpret_cast<double**>(dph + host_ph.size());
+  if (!species_ptr.empty())
+    CK(cudaMemcpyAsync(dsp, species_ptr.data(), species_ptr.size() * sizeof(double*),
+                       cudaMemcpyHostToDevice, ctx->stream));
   ppm::FluxFix X{};
+  X.species = dsp;
+  X.nspecies = (int)species_ptr.size();
   for (int s = 0; s < 6; ++s) X.f[s] = io.user.f[s];
   for (int d = 0; d < 3; ++d) X.dims[d] = GD[d];
   X.rank = rank;

@@ -270,6 +270,11 @@ struct FluxFix {
   int dims[3], rank, dual;
   double tiny_number;
   int nphases;
+  // colours that keep their fraction of the density (species): device array of nspecies
+  // field pointers, divided by the density before the corrections and multiplied by the
+  // corrected density after them (Grid_CorrectForRefinedFluxes.C:397-421, :849-866)
+  double* const* species;
+  int nspecies;
 };
 
 __global__ void __launch_bounds__(256) correct_fluxes_kernel(const FluxFix X,
@@ -293,12 +298,18 @@ __global__ void __launch_bounds__(256) correct_fluxes_kernel(const FluxFix X,
       const long long xr = ((long long)(k + P.ro[2]) * P.rd[1] + (j + P.ro[1])) * P.rd[0] +
                            (i + P.ro[0]);
       const bool sub = P.subling != 0;
-      // conserved quantities on both layers (:304-322): every field but density
+      // conserved quantities on both layers (:370-394): every field but density; species
+      // as fractions of the density (:397-421)
       for (int s = 1; s < 6; ++s)
         if (F[s]) {
           F[s][c] *= F[0][c];
           F[s][c2] *= F[0][c2];
         }
+      for (int s = 0; s < X.nspecies; ++s) {
+        double* q = X.species[s];
+        q[c] /= F[0][c];
+        q[c2] /= F[0][c2];
+      }
       for (int q = 0; q < 6; ++q) {
         const int f = order[q];
         if (!F[f]) continue;
@@ -361,6 +372,12 @@ __global__ void __launch_bounds__(256) correct_fluxes_kernel(const FluxFix X,
           F[1][c] += 0.5 * F[4][c] * F[4][c];
           F[1][c2] += 0.5 * F[4][c2] * F[4][c2];
         }
+      }
+      // species back to densities with the corrected density (:849-866)
+      for (int s = 0; s < X.nspecies; ++s) {
+        double* q = X.species[s];
+        q[c] *= F[0][c];
+        q[c2] *= F[0][c2];
       }
     }
     __syncthreads();  // the next phase may touch the same zones

@@ -64,7 +64,7 @@ class Params(C.Structure):
         ("steepening", C.c_int), ("flattening", C.c_int), ("diffusion", C.c_int),
         ("conservative_rec", C.c_int), ("positive_rec", C.c_int), ("eos_type", C.c_int),
         ("number_of_colours", C.c_int), ("learned_guess", C.c_int),
-        ("dt_device", C.c_void_p), ("reserved", C.c_int * 6),
+        ("dt_device", C.c_void_p), ("colour_species", C.c_void_p), ("reserved", C.c_int * 4),
     ]
 
 
@@ -475,12 +475,25 @@ class Context:
         if rc != OK:
             raise PPMError(rc, "ppm_b200_debug_tma_stall")
 
-    def correct_fluxes(self, grid, hp, fields, initial, refined, ggs, memory=MEM_HOST):
+    @staticmethod
+    def _species(P, fields, species, keep):
+        """Colours (keys col0, ...) and the flags of those that keep their density
+        fraction under flux correction (params.colour_species)."""
+        P.number_of_colours = len(colour_names(fields)) if species else 0
+        if species:
+            arr = (C.c_int * len(species))(*[int(bool(x)) for x in species])
+            keep.append(arr)
+            P.colour_species = C.cast(arr, C.c_void_p)
+
+    def correct_fluxes(self, grid, hp, fields, initial, refined, ggs, memory=MEM_HOST,
+                       species=None):
         """grid::CorrectForRefinedFluxes for the proper subgrids of one grid.  initial /
         refined: lists of flux boxes (dicts as for make_fluxes, host numpy arrays); the
-        refined arrays are updated in place where a correction is undone."""
+        refined arrays are updated in place where a correction is undone.  species: one
+        flag per colour field (keys col0, ...): nonzero keeps its density fraction."""
         P = make_params(hp, 0.0)
         G, keep = make_grid(grid, fields)
+        self._species(P, fields, species, keep)
         n = len(initial)
         ini = (Fluxes * n)(*[make_fluxes(b) for b in initial])
         ref = (Fluxes * n)(*[make_fluxes(b) for b in refined])
@@ -491,12 +504,13 @@ class Context:
             raise PPMError(rc, "ppm_b200_correct_fluxes")
 
     def correct_fluxes_sublings(self, grid, hp, fields, own, refined, ggs, level_dims, periodic,
-                                memory=MEM_HOST):
+                                memory=MEM_HOST, species=None):
         """The SUBling calls of grid::CorrectForRefinedFluxes for one grid: own = its own
         boundary flux box, refined = the sibling subgrids' projected flux boxes (dicts as
         for make_fluxes; refined arrays updated where a correction is undone)."""
         P = make_params(hp, 0.0)
         G, keep = make_grid(grid, fields)
+        self._species(P, fields, species, keep)
         n = len(refined)
         ow = make_fluxes(own)
         ref = (Fluxes * n)(*[make_fluxes(b) for b in refined])

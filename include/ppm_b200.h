@@ -80,7 +80,14 @@ typedef struct ppm_b200_params {
   int learned_guess;        /* 1: start twoshock's Newton iteration from the learned p* guess
                                (weights from ppm_b200_set_guess) */
   const double *dt_device;  /* optional: device pointer holding dtFixed (overrides dt) */
-  int reserved[6];
+  const int *colour_species; /* optional HOST array of number_of_colours flags for
+                               ppm_b200_correct_fluxes[_sublings]: nonzero for a colour
+                               that keeps its fraction of the corrected density there
+                               (FluxCorrection = 1: fields ElectronDensity .. ExtraType1
+                               and the SN Ia / II metal densities,
+                               Grid_CorrectForRefinedFluxes.C:397-421, :849-866); other
+                               colours are left alone.  NULL: none */
+  int reserved[4];
 } ppm_b200_params;
 
 /* One grid.  Field pointers are host or device memory as the call says.

@@ -52,6 +52,7 @@ class OraParams(C.Structure):
         ("flatten", C.c_int),
         ("ncolour", C.c_int),
         ("riemann", C.c_int),
+        ("colour_species", C.c_void_p),
     ]
 
 
@@ -122,11 +123,11 @@ def lib():
         L.ora_expansion_terms.argtypes = [C.POINTER(OraParams), dp * 6, C.c_void_p, C.c_double,
                                           C.c_double, C.c_double]
         L.ora_expansion_terms.restype = None
-        L.ora_correct_fluxes.argtypes = [C.POINTER(OraParams), dp * 6, C.c_int,
+        L.ora_correct_fluxes.argtypes = [C.POINTER(OraParams), C.c_void_p, C.c_int,
                                          C.POINTER(OraFluxes), C.POINTER(OraFluxes),
                                          C.c_longlong * 3]
         L.ora_correct_fluxes.restype = C.c_int
-        L.ora_correct_fluxes_sublings.argtypes = [C.POINTER(OraParams), dp * 6, C.c_int,
+        L.ora_correct_fluxes_sublings.argtypes = [C.POINTER(OraParams), C.c_void_p, C.c_int,
                                                   C.POINTER(OraFluxes), C.POINTER(OraFluxes),
                                                   C.c_longlong * 3, C.c_longlong * 3,
                                                   C.c_int * 3]
@@ -268,31 +269,45 @@ def expansion_terms(grid, hp, fields, old, time, old_time, coefficient):
     L.ora_expansion_terms(C.byref(P), F, O, float(time), float(old_time), float(coefficient))
 
 
-def correct_fluxes(grid, hp, fields, initial, refined, ggs):
+def _species(P, ncol, species):
+    """Species flags (one per colour) into P; returns the array to keep alive."""
+    if not species:
+        return None
+    arr = (C.c_int * max(ncol, 1))(*[int(bool(x)) for x in species])
+    P.colour_species = C.cast(arr, C.c_void_p)
+    return arr
+
+
+def correct_fluxes(grid, hp, fields, initial, refined, ggs, species=None):
     """grid::CorrectForRefinedFluxes (proper subgrids) on host fields, in place.  initial /
     refined: lists of OraFluxes (the refined ones are updated where a correction is
     undone).  ggs: global index of the grid's first zone.  Returns the C status."""
     L = lib()
-    P = make_params(grid, hp, 0.0)
+    F, ncol = _fields_all(fields)
+    P = make_params(grid, hp, 0.0, ncol)
+    keep = _species(P, ncol, species)
     n = len(initial)
     ini = (OraFluxes * n)(*initial)
     ref = (OraFluxes * n)(*refined)
-    rc = L.ora_correct_fluxes(C.byref(P), _fields6(fields), n, ini, ref,
+    rc = L.ora_correct_fluxes(C.byref(P), F, n, ini, ref,
                               (C.c_longlong * 3)(*[int(x) for x in ggs]))
     for k in range(n):
         refined[k] = ref[k]
     return rc
 
 
-def correct_fluxes_sublings(grid, hp, fields, own, refined, ggs, level_dims, periodic):
+def correct_fluxes_sublings(grid, hp, fields, own, refined, ggs, level_dims, periodic,
+                            species=None):
     """The SUBling calls of grid::CorrectForRefinedFluxes on host fields, in place.  own:
     OraFluxes of the grid's own boundary; refined: list of OraFluxes (updated where a
     correction is undone).  Returns the C status."""
     L = lib()
-    P = make_params(grid, hp, 0.0)
+    F, ncol = _fields_all(fields)
+    P = make_params(grid, hp, 0.0, ncol)
+    keep = _species(P, ncol, species)
     n = len(refined)
     ref = (OraFluxes * n)(*refined)
-    rc = L.ora_correct_fluxes_sublings(C.byref(P), _fields6(fields), n, C.byref(own), ref,
+    rc = L.ora_correct_fluxes_sublings(C.byref(P), F, n, C.byref(own), ref,
                                        (C.c_longlong * 3)(*[int(x) for x in ggs]),
                                        (C.c_longlong * 3)(*[int(x) for x in level_dims]),
                                        (C.c_int * 3)(*[int(bool(x)) for x in periodic]))

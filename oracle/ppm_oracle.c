@@ -1552,7 +1552,7 @@ void ora_expansion_terms(const ora_params *P, double *const F[ORA_NFIELD],
    one (initial, refined) pair.  subling: SUBlingGrid == TRUE, the refined fluxes of a
    sibling's subgrid projected to this level, I the grid's own boundary fluxes; gdims and
    periodic: the level's extent in zones and the periodic faces (:147-221). */
-static int correct_one(const ora_params *P, double *const F[ORA_NFIELD], const int *order,
+static int correct_one(const ora_params *P, double *const F[], const int *order,
                        int nf, const ora_fluxes *I, ora_fluxes *R, const long long gl[3],
                        int subling, const long long gdims[3], const int periodic[3]) {
   const int rank = P->rank;
@@ -1645,6 +1645,18 @@ static int correct_one(const ora_params *P, double *const F[ORA_NFIELD], const i
             F[f][c + Offset] *= F[ORA_D][c + Offset];
           }
     }
+    /* species as fractions of the density (:397-421) */
+    for (int n = 0; n < P->ncolour && P->colour_species; n++) {
+      if (!P->colour_species[n]) continue;
+      double *q = F[ORA_NFIELD + n];
+      for (int k = Start[2]; k <= End[2]; k++)
+        for (int j = Start[1]; j <= End[1]; j++)
+          for (int i = Start[0]; i <= End[0]; i++) {
+            const size_t c = CELL(k, j, i);
+            q[c] /= F[ORA_D][c];
+            q[c + Offset] /= F[ORA_D][c + Offset];
+          }
+    }
     /* the corrections with the undo for density and energies (:455-656) */
     for (int q = 0; q < nf; q++) {
       const int f = order[q];
@@ -1725,6 +1737,18 @@ static int correct_one(const ora_params *P, double *const F[ORA_NFIELD], const i
             }
           }
     }
+    /* species back to densities with the corrected density (:849-866) */
+    for (int n = 0; n < P->ncolour && P->colour_species; n++) {
+      if (!P->colour_species[n]) continue;
+      double *q = F[ORA_NFIELD + n];
+      for (int k = Start[2]; k <= End[2]; k++)
+        for (int j = Start[1]; j <= End[1]; j++)
+          for (int i = Start[0]; i <= End[0]; i++) {
+            const size_t c = CELL(k, j, i);
+            q[c] *= F[ORA_D][c];
+            q[c + Offset] *= F[ORA_D][c + Offset];
+          }
+    }
 #undef CELL
 #undef FLUX
 #undef RFLUX
@@ -1734,7 +1758,7 @@ static int correct_one(const ora_params *P, double *const F[ORA_NFIELD], const i
 
 /* the fields in the order the routine corrects them: density and the energies first
    (:341-360), then the remaining fields in BaryonField order (:396-452) */
-static int correction_order(const ora_params *P, double *const F[ORA_NFIELD], int *order) {
+static int correction_order(const ora_params *P, double *const F[], int *order) {
   int nf = 0;
   const int base_order[ORA_NFIELD] = {ORA_D, ORA_TE, ORA_GE, ORA_V1, ORA_V2, ORA_V3};
   for (int q = 0; q < ORA_NFIELD; q++) {
@@ -1747,7 +1771,7 @@ static int correction_order(const ora_params *P, double *const F[ORA_NFIELD], in
   return nf;
 }
 
-int ora_correct_fluxes(const ora_params *P, double *const F[ORA_NFIELD], int nsub,
+int ora_correct_fluxes(const ora_params *P, double *const F[], int nsub,
                        const ora_fluxes *IN, ora_fluxes *RF, const long long gl[3]) {
   int order[ORA_NFIELD];
   const int nf = correction_order(P, F, order);
@@ -1756,7 +1780,7 @@ int ora_correct_fluxes(const ora_params *P, double *const F[ORA_NFIELD], int nsu
   return 0;
 }
 
-int ora_correct_fluxes_sublings(const ora_params *P, double *const F[ORA_NFIELD], int nsib,
+int ora_correct_fluxes_sublings(const ora_params *P, double *const F[], int nsib,
                                 const ora_fluxes *own, ora_fluxes *RF, const long long gl[3],
                                 const long long gdims[3], const int periodic[3]) {
   int order[ORA_NFIELD];

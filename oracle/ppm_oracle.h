@@ -66,6 +66,8 @@ typedef struct {
   int ncolour;         /* NumberOfColours: advected colour fields after the hydro fields */
   int riemann;         /* RiemannSolver (typedefs.h:279-280): 5 TwoShock (0 taken as 5),
                           1 HLL, 4 HLLC */
+  const int *colour_species; /* flux correction: ncolour flags, nonzero for a colour that
+                                keeps its fraction of the corrected density; NULL: none */
 } ora_params;
 
 enum { ORA_RIEMANN_HLL = 1, ORA_RIEMANN_HLLC = 4, ORA_RIEMANN_TWOSHOCK = 5 };
@@ -141,7 +143,7 @@ void ora_expansion_terms(const ora_params *P, double *const fields[ORA_NFIELD],
    (same index boxes); refined entries of undone corrections are set to the initial ones,
    as the reference does.  gl: global index of the grid's first zone (ghosts included).
    Returns 0, or -1 if a flux box does not fit the grid. */
-int ora_correct_fluxes(const ora_params *P, double *const fields[ORA_NFIELD], int nsub,
+int ora_correct_fluxes(const ora_params *P, double *const fields[], int nsub,
                        const ora_fluxes *initial, ora_fluxes *refined, const long long gl[3]);
 
 /* The SUBling calls of grid::CorrectForRefinedFluxes (SUBlingGrid == TRUE,
@@ -152,7 +154,7 @@ int ora_correct_fluxes(const ora_params *P, double *const fields[ORA_NFIELD], in
    305, :464-656).  gdims: the level's extent in zones per axis; periodic: periodic
    faces per axis.  refined[n]'s index boxes are not modified; its flux values are where a
    correction is undone.  Returns 0, or -1 if a flux box does not fit the grid. */
-int ora_correct_fluxes_sublings(const ora_params *P, double *const fields[ORA_NFIELD], int nsib,
+int ora_correct_fluxes_sublings(const ora_params *P, double *const fields[], int nsib,
                                 const ora_fluxes *own, ora_fluxes *refined,
                                 const long long gl[3], const long long gdims[3],
                                 const int periodic[3]);

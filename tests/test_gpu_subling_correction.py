@@ -97,3 +97,24 @@ def test_undo_matches_oracle(ctx, slot, side):
     arr = ref["left" if side.endswith("right") else "right"][slot][dim]
     arr += 50.0 * (1.0 if side.endswith("right") else -1.0)
     _compare(ctx, g, hp, f, own, [ref], GGS, (64, 64, 64), (0, 0, 0))
+
+
+def test_species_colours_match_oracle(ctx):
+    hp = H.HydroParams(gamma=5.0 / 3.0, dual=True)
+    g = H.Grid.uniform((8, 6, 4))
+    f = random_state(g, hp, seed=19)
+    rng = np.random.default_rng(20)
+    for n in range(3):
+        f[f"col{n}"] = (0.2 + 0.3 * n) * f["d"]
+    species = [1, 0, 1]
+    own = own_box(g, GGS, rng)
+    refs = [gbox(*CONTACTS["x_right"], rng), gbox(*CONTACTS["y_left"], rng)]
+    f_ora, f_gpu = copy_fields(f), copy_fields(f)
+    r_ora, r_gpu = [copy_box(r) for r in refs], [copy_box(r) for r in refs]
+    assert O.correct_fluxes_sublings(g, hp, f_ora, ora_fluxes(own),
+                                     [ora_fluxes(r) for r in r_ora], GGS, (64, 64, 64),
+                                     (0, 0, 0), species=species) == 0
+    ctx.correct_fluxes_sublings(g, hp, f_gpu, own, r_gpu, GGS, (64, 64, 64), (0, 0, 0),
+                                species=species)
+    for k in f:
+        assert np.array_equal(f_gpu[k], f_ora[k]), k

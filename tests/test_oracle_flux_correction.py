@@ -78,3 +78,24 @@ def test_undo_keeps_states_positive_and_resets_refined_fluxes():
             undone += changed.sum()
             assert np.array_equal(now[changed], init[changed])
     assert undone > 0
+
+
+def test_species_keep_their_density_fraction():
+    # FluxCorrection = 1: species colours are divided by the density before the
+    # corrections and multiplied by the corrected density after them
+    # (Grid_CorrectForRefinedFluxes.C:397-421, :849-866); other colours are untouched
+    hp, g, f, ini, ref = _setup(kick=0.0, seed=5)
+    rng = np.random.default_rng(6)
+    f["col0"] = 0.25 * f["d"] * (1.0 + 0.1 * rng.random(f["d"].shape))
+    f["col1"] = rng.random(f["d"].shape)
+    before = {k: v.copy() for k, v in f.items()}
+    rc = O.correct_fluxes(g, hp, f, [ora_fluxes(ini)], [ora_fluxes(ref)], GGS,
+                          species=[1, 0])
+    assert rc == 0
+    changed = f["d"] != before["d"]
+    assert changed.any()
+    frac0, frac1 = before["col0"] / before["d"], f["col0"] / f["d"]
+    assert np.allclose(frac1, frac0, rtol=1e-15, atol=0)
+    assert not np.array_equal(f["col0"][changed], before["col0"][changed])
+    assert np.array_equal(f["col0"][~changed], before["col0"][~changed])
+    assert np.array_equal(f["col1"], before["col1"])
