@@ -85,7 +85,8 @@ def workload_config(args):
         "active_cells_per_gpu": args.size ** 3,
         "step": "SolvePPM_DE (pressure, 3 sweeps, calc_dt of the next cycle folded into the "
                 "last sweep) + periodic ghost fill",
-        "l2": "inputs larger than L2 (13 fields x 144 MB resident per GPU)",
+        "l2": f"inputs larger than L2 ({6 + args.colours} fields of "
+              f"{(args.size + 6) ** 3 * 8 / 1e6:.0f} MB each, 126 MB L2)",
         "bytes_per_zone_update": BYTES_PER_ZONE_UPDATE + 3 * 16 * args.colours,
         **({"colours": args.colours} if args.colours else {}),
     }

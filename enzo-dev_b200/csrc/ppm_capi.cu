@@ -53,6 +53,7 @@ struct ElemBatch {
   unsigned long long* min_bits;
   double expansion, coef_new, coef_old;
   int interpolate;
+  int presfree;
 };
 void launch_expansion_batch(const ElemBatch& B, int64_t blocks, cudaStream_t st);
 void launch_cfl_reset(unsigned long long* min_bits, cudaStream_t st);
@@ -321,9 +322,9 @@ void build_coef(const double* dxi_in, int n, int is0, int ie0, std::vector<Coef>
 
 int check_supported(const ppm_b200_params* p) {
   if (!p) return PPM_B200_ERR_INVALID;
-  if (p->pressure_free || p->diffusion || p->conservative_rec || p->positive_rec ||
-      p->eos_type != 0)
+  if (p->diffusion || p->conservative_rec || p->positive_rec || p->eos_type != 0)
     return PPM_B200_ERR_UNSUPPORTED;
+  if (p->pressure_free != 0 && p->pressure_free != 1) return PPM_B200_ERR_UNSUPPORTED;
   if (p->number_of_colours < 0 || p->number_of_colours > PPM_B200_MAX_COLOURS)
     return PPM_B200_ERR_UNSUPPORTED;
   // slope corrections: calcdiss's flattening types 1-3, inteuler's steepening
@@ -761,6 +762,7 @@ int prepare_sweep(ppm_b200_context* ctx, int dim, int position, const ppm_b200_p
     a.pmin = p->tiny_number;
     // HLL has no fallback: a negative density stops the reference (flux_hll.F:378-380)
     a.solver = solver_code(p);
+    a.presfree = p->pressure_free == 1 ? 1 : 0;
     a.fallback = p->riemann_solver == PPM_B200_RIEMANN_HLL ? 0 : p->riemann_fallback;
     a.guess = p->learned_guess ? (const uint32_t*)ctx->guess.p : nullptr;
     if (ctx->log && !p->learned_guess) {
@@ -844,6 +846,7 @@ int prepare_sweep(ppm_b200_context* ctx, int dim, int position, const ppm_b200_p
   plan.B.corrections = correction_planes(p) > 0 ? 1 : 0;
   plan.B.ncolour = nc;
   plan.B.solver = solver_code(p);
+  plan.B.presfree = p->pressure_free == 1 ? 1 : 0;
   plan.B.hll_flags = nc > 0 ? flags : nullptr;
   plan.B.hll_bytes = (int64_t)flag_bytes;
   plan.B.grids = (const SweepArgs*)base;
@@ -1041,6 +1044,7 @@ int prepare_elem(ppm_b200_context* ctx, int slot, const ppm_b200_params* p,
   plan.B.min_bits = (unsigned long long*)ctx->misc.p;
   plan.B.expansion = plan.B.coef_new = plan.B.coef_old = 0.0;
   plan.B.interpolate = 0;
+  plan.B.presfree = p->pressure_free == 1 ? 1 : 0;
   plan.size_blocks = spre[ng];
   plan.active_blocks = apre[ng];
   plan.row_blocks = rpre[ng];
@@ -1282,6 +1286,7 @@ std::string graph_key(ppm_b200_context* ctx, const ppm_b200_params* p, const Sol
     key_put(k, b.corrections);
     key_put(k, b.ncolour);
     key_put(k, b.solver);
+    key_put(k, b.presfree);
     key_put(k, b.hll_flags);
     key_put(k, b.hll_bytes);
     key_put(k, ctx->mirror[kSlotSweep0 + 3 * sp.order[s] + s].version);

@@ -38,10 +38,13 @@ struct Prep {
   double char1, char2, cm, c0, cp;
 };
 
+// PF: PressureFree, the sound speed set to tiny (inteuler.F:199)
+template <bool PF = false>
 __device__ __forceinline__ Prep cell_prep(double d, double p, double u, double dx2i,
                                           const Phys& P) {
   Prep r;
   double cs = sqrt(P.gamma * p / d);
+  if (PF) cs = kTiny;
   r.char1 = dmax(0.0, P.dt * (u + cs)) * dx2i;
   r.char2 = dmax(0.0, -(P.dt * (u - cs))) * dx2i;
   r.cm = P.dt * (u - cs) * dx2i;

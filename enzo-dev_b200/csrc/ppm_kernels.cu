@@ -45,6 +45,7 @@ struct ElemBatch {
   // expansion kernel: dt * adot / a, and the pressure's interpolation weights
   double expansion, coef_new, coef_old;
   int interpolate;
+  int presfree;                  // PressureFree: calc_dt's sound speed tiny (calc_dt.F:78-137)
 };
 
 // grid::ComputePressure at time == Time (Grid_ComputePressure.C:96-164)
@@ -95,7 +96,7 @@ __global__ void __launch_bounds__(256) timestep_kernel(const __grid_constant__ E
     const double w = G.v[2] ? __ldg(G.v[2] + g) : 0.0;
     const double p = cell_pressure(G, g, B.gamma, B.tiny_number, B.min_support);
     // calc_dt.F:136-153
-    const double cs = dmax(sqrt(B.gamma * p / density), kTiny);
+    const double cs = B.presfree ? kTiny : dmax(sqrt(B.gamma * p / density), kTiny);
     double dt1;
     if (G.rank == 1) {
       dt1 = G.cw[0][i] * B.aye / (cs + fabs(u - B.vg[0]));

@@ -206,7 +206,8 @@ __global__ void __launch_bounds__(kMarchThreads,
     if (t >= is - 1 && t <= ie + 1) {
       const double nd = ROLE == 0 ? nq[0] : __ldg(a.in_d + off);
       const double npr = ROLE == 0 ? nq[1] : __ldg(a.pres + off);
-      prC = cell_prep(nd, npr, nu, a.coef[t].dx2i, P);
+      prC = (COR && a.presfree) ? cell_prep<true>(nd, npr, nu, a.coef[t].dx2i, P)
+                                : cell_prep(nd, npr, nu, a.coef[t].dx2i, P);
     }
     // slope and left edge of cell t-1 (intvar.F:82-102)
     double dqN[3], qlN[3];
@@ -288,6 +289,10 @@ __global__ void __launch_bounds__(kMarchThreads,
               oc[COVR * plane] = (cx.ovl ? 1.0 : 0.0) + (cx.ovr ? 2.0 : 0.0);
             } else {
               s = face_core<DUAL, GRAV>(cLp, R, GRAV ? (wg0 + wg1) : 0.0, P);
+            }
+            if (COR && a.presfree) {  // the uncorrected densities (inteuler.F:556-561)
+              s.dl = cLp.dla;
+              s.dr = R.dra;
             }
             o[SDL * plane] = s.dl;
             o[SDR * plane] = s.dr;
@@ -514,6 +519,42 @@ __global__ void __launch_bounds__(kRiemannThreads, LEARNED ? PPM_RIEMANN_LEARNED
   }
   if (LEARNED && threadIdx.x == 9 && s_rejected)
     atomicAdd(&B.counters[kCntGuessRejected], (unsigned long long)s_rejected);
+}
+
+// PressureFree with the two-shock solver: no Riemann problem, p* = pmin, u* the mean of
+// the face velocities, and the face pressures set to pmin before flux_twoshock
+// (twoshock.F:124-130).  COL: the Godunov density for the colour kernel.
+template <bool DUAL, bool ONE, bool COL>
+__global__ void __launch_bounds__(kRiemannThreads) presfree_riemann_kernel(const __grid_constant__ BatchArgs B) {
+  int64_t lb;
+  const int g = locate<ONE>(B.riemann_prefix, B.ngrids, lb);
+  PPM_BIND_RECORD(a, g)
+  const int64_t chunks = (a.npencils + kRiemannThreads - 1) / kRiemannThreads;
+  const int fi = (int)(lb / chunks);
+  const int64_t pid = (lb - (int64_t)fi * chunks) * kRiemannThreads + threadIdx.x;
+  if (pid >= a.npencils) return;
+  const Phys P = make_phys(a);
+  const int64_t pl = a.plane, idx = (int64_t)fi * a.npencils + pid;
+  FaceState s = load_face<DUAL>(a, idx);
+  const double pbar = P.pmin;
+  const double ubar = 0.5 * (s.ul + s.ur);
+  s.pl = P.pmin;
+  s.pr = P.pmin;
+  // the reference overwrites pls/prs in place: an HLL fallback reads these too
+  a.fstate[SPL * pl + idx] = P.pmin;
+  a.fstate[SPR * pl + idx] = P.pmin;
+  const double qc = P.dt / a.coef[a.is + fi].dx;
+  double db;
+  const Flux F = flux_twoshock<DUAL>(s, pbar, ubar, qc, P, COL ? &db : nullptr);
+  double* o = a.fflux + idx;
+  o[XDF * pl] = F.df;
+  o[XEF * pl] = F.ef;
+  o[XUF * pl] = F.uf;
+  o[XVF * pl] = F.vf;
+  o[XWF * pl] = F.wf;
+  if (DUAL) o[XGEF * pl] = F.gef;
+  o[XUB * pl] = F.ub;
+  if (COL) a.fcol[CDB * pl + idx] = db;
 }
 
 // RiemannSolver = HLL (flux_hll.F:6-415) or HLLC (flux_hllc.F:6-421) at every face, one
@@ -917,7 +958,7 @@ __device__ __forceinline__ double cell_dt1(const SweepArgs& a, const Cell& o, do
   if (p < P.pmin) p = P.pmin;
   const double min_pressure = a.min_support * P.gm1 * o.d * o.d;
   if (p < min_pressure) p = min_pressure;
-  const double cs = dmax(sqrt(P.gamma * p / o.d), kTiny);
+  const double cs = a.presfree ? kTiny : dmax(sqrt(P.gamma * p / o.d), kTiny);
   if (a.rank == 1) return dx[0] * a.aye / (cs + fabs(velocity1 - a.vg[0]));
   if (a.rank == 2)
     return a.aye / ((cs + fabs(velocity1 - a.vg[0])) / dx[0] +
@@ -1409,7 +1450,10 @@ __global__ void __launch_bounds__(kMarchThreads, PPM_COLOUR_MINBLOCKS)
     const double nu = ldg0(a.in_u, off);
     Prep prC = prB;
     if (t >= is - 1 && t <= ie + 1)
-      prC = cell_prep(__ldg(a.in_d + off), __ldg(a.pres + off), nu, a.coef[t].dx2i, P);
+      prC = a.presfree ? cell_prep<true>(__ldg(a.in_d + off), __ldg(a.pres + off), nu,
+                                         a.coef[t].dx2i, P)
+                       : cell_prep(__ldg(a.in_d + off), __ldg(a.pres + off), nu,
+                                   a.coef[t].dx2i, P);
     double dqN[CPT], qlN[CPT];  // slope and left edge of cell t-1
 #pragma unroll
     for (int u = 0; u < CPT; ++u) dqN[u] = qlN[u] = 0.0;
@@ -1545,7 +1589,7 @@ void launch_stages(const BatchArgs& B, int64_t march_blocks, int64_t riemann_blo
   mark(0);
   cudaMemsetAsync(B.counters + kCntFlagged, 0, sizeof(unsigned long long), st);
   if (B.ncolour > 0) cudaMemsetAsync(B.hll_flags, 0, (size_t)B.hll_bytes, st);
-  if (B.corrections || B.ncolour > 0) {  // the colour data come from the COR variant
+  if (B.corrections || B.ncolour > 0 || B.presfree) {  // colours, PressureFree: COR too
     if (B.corrections)
       corrections_kernel<ONE><<<(unsigned)march_blocks, kMarchThreads, 0, st>>>(B);
     reconstruct_kernel<DUAL, GRAV, 0, ONE, true><<<(unsigned)march_blocks, kMarchThreads, 0, st>>>(B);
@@ -1559,7 +1603,11 @@ void launch_stages(const BatchArgs& B, int64_t march_blocks, int64_t riemann_blo
   mark(2);
   const unsigned rb = (unsigned)riemann_blocks;
   const bool col = B.ncolour > 0;
-  if (B.solver == 1 && col)
+  if (B.solver == 0 && B.presfree && col)
+    presfree_riemann_kernel<DUAL, ONE, true><<<rb, kRiemannThreads, 0, st>>>(B);
+  else if (B.solver == 0 && B.presfree)
+    presfree_riemann_kernel<DUAL, ONE, false><<<rb, kRiemannThreads, 0, st>>>(B);
+  else if (B.solver == 1 && col)
     hll_riemann_kernel<DUAL, ONE, false, true><<<rb, kRiemannThreads, 0, st>>>(B);
   else if (B.solver == 1)
     hll_riemann_kernel<DUAL, ONE, false, false><<<rb, kRiemannThreads, 0, st>>>(B);

@@ -110,6 +110,10 @@ struct SweepArgs {
   // HLLC the flux plane XUB holds the gas-energy source ges of the face's right cell
   // instead of the Godunov velocity.
   int solver;
+  // PressureFree: sound speed tiny in the characteristics (inteuler.F:199) and the time
+  // step (calc_dt.F:78-137), the face densities the uncorrected ones (inteuler.F:556-561),
+  // the two-shock solve replaced by p* = pmin, u* = (ul + ur)/2 (twoshock.F:124-130)
+  int presfree;
 };
 
 enum { kFaceVars = 12, kFluxVars = 7 };
@@ -160,6 +164,7 @@ struct BatchArgs {
   unsigned char* hll_flags = nullptr;
   int64_t hll_bytes = 0;
   int solver = 0;                    // the batch's Riemann solver (SweepArgs::solver)
+  int presfree = 0;                  // PressureFree (SweepArgs::presfree)
   CUtensorMap xin[6];
 };
 
