@@ -63,7 +63,7 @@ typedef struct ppm_b200_params {
   double min_support;       /* MinimumSupportEnergyCoefficient (ComputePressure) */
   int dual_energy;          /* DualEnergyFormalism */
   int gravity;              /* GravityOn (AccelerationField used) */
-  int pressure_free;        /* PressureFree: unsupported, must be 0 */
+  int pressure_free;        /* PressureFree: 0 or 1 (inteuler.F:199, :556-561, twoshock.F:124-130) */
   int riemann_solver;       /* RiemannSolver: PPM_B200_RIEMANN_TWOSHOCK, _HLL or _HLLC
                                (learned_guess applies to the two-shock solver only) */
   int riemann_fallback;     /* RiemannSolverFallback */
