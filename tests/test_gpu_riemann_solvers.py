@@ -144,3 +144,25 @@ def test_unknown_solver_is_unsupported(ctx):
     g = H.Grid.uniform((8, 8, 8))
     rc, _ = ctx.solve_ppm_de(g, hp, 1e-3, 0, random_state(g, hp, seed=1), check=False)
     assert rc == capi.ERR_UNSUPPORTED
+
+
+@pytest.mark.parametrize("riemann", [5, HLL, HLLC])
+def test_gravity_colours_and_options_together(ctx, riemann):
+    # the options at once: gravity, colours, flattening + steepening, with each solver
+    hp = H.HydroParams(gamma=5.0 / 3.0, cfl=0.4, dual=True, gravity=True, riemann=riemann,
+                       flatten=2, steepen=1)
+    g = H.Grid.uniform((15, 13, 11))
+    f = random_state(g, hp, seed=91, mach=2.0)
+    add_colours(g, f, seed=92)
+    rng = np.random.default_rng(93)
+    accel = [0.1 * rng.standard_normal(g.shape) for _ in range(3)]
+    f_gpu, f_ora = copy_fields(f), copy_fields(f)
+    for cyc in range(3):
+        dt = hp.cfl * _dt(g, hp, f_ora)
+        rc, _ = O.solve_ppm_de(g, hp, dt, cyc, f_ora, g.cellwidth, accel=accel)
+        assert rc == 0
+        rc, _ = ctx.solve_ppm_de(g, hp, dt, cyc, f_gpu, accel=accel)
+        assert rc == capi.OK
+        _bitexact(f_gpu, f_ora, g, cyc)
+        H.fill_ghosts(g, f_ora, "periodic")
+        H.fill_ghosts(g, f_gpu, "periodic")
