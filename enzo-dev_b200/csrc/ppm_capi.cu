@@ -54,6 +54,8 @@ struct ElemBatch {
   double expansion, coef_new, coef_old;
   int interpolate;
   int presfree;
+  int eos_type;
+  double eos_cs;
 };
 void launch_expansion_batch(const ElemBatch& B, int64_t blocks, cudaStream_t st);
 void launch_cfl_reset(unsigned long long* min_bits, cudaStream_t st);
@@ -322,7 +324,9 @@ void build_coef(const double* dxi_in, int n, int is0, int ie0, std::vector<Coef>
 
 int check_supported(const ppm_b200_params* p) {
   if (!p) return PPM_B200_ERR_INVALID;
-  if (p->diffusion || p->conservative_rec || p->positive_rec || p->eos_type != 0)
+  // EOSType: ideal gas, or 3 (isothermal; the other polytropes need the unit system)
+  if (p->diffusion || p->conservative_rec || p->positive_rec ||
+      (p->eos_type != 0 && p->eos_type != 3))
     return PPM_B200_ERR_UNSUPPORTED;
   if (p->pressure_free != 0 && p->pressure_free != 1) return PPM_B200_ERR_UNSUPPORTED;
   if (p->number_of_colours < 0 || p->number_of_colours > PPM_B200_MAX_COLOURS)
@@ -763,6 +767,8 @@ int prepare_sweep(ppm_b200_context* ctx, int dim, int position, const ppm_b200_p
     // HLL has no fallback: a negative density stops the reference (flux_hll.F:378-380)
     a.solver = solver_code(p);
     a.presfree = p->pressure_free == 1 ? 1 : 0;
+    a.eos_type = p->eos_type;
+    a.eos_cs = p->eos_sound_speed;
     a.fallback = p->riemann_solver == PPM_B200_RIEMANN_HLL ? 0 : p->riemann_fallback;
     a.guess = p->learned_guess ? (const uint32_t*)ctx->guess.p : nullptr;
     if (ctx->log && !p->learned_guess) {
@@ -1045,6 +1051,8 @@ int prepare_elem(ppm_b200_context* ctx, int slot, const ppm_b200_params* p,
   plan.B.expansion = plan.B.coef_new = plan.B.coef_old = 0.0;
   plan.B.interpolate = 0;
   plan.B.presfree = p->pressure_free == 1 ? 1 : 0;
+  plan.B.eos_type = p->eos_type;
+  plan.B.eos_cs = p->eos_sound_speed;
   plan.size_blocks = spre[ng];
   plan.active_blocks = apre[ng];
   plan.row_blocks = rpre[ng];
@@ -1238,6 +1246,11 @@ int enqueue_solve(ppm_b200_context* ctx, const ppm_b200_params* p, const std::ve
                              ctx->stream));
     }
   }
+  if (p->eos_type > 0) {  // energies consistent with the EOS again (Grid_SolvePPM_DE.C:155-157)
+    ppm::launch_pressure_batch(sp.pressure.B, sp.pressure.size_blocks, ctx->stream);
+    ctx->launches += 1;
+    CK(cudaGetLastError());
+  }
   return PPM_B200_OK;
 }
 
@@ -1267,6 +1280,8 @@ std::string graph_key(ppm_b200_context* ctx, const ppm_b200_params* p, const Sol
   key_put(k, e.gamma);
   key_put(k, e.tiny_number);
   key_put(k, e.min_support);
+  key_put(k, e.eos_type);
+  key_put(k, e.eos_cs);
   key_put(k, e.min_bits);
   key_put(k, sp.pressure.size_blocks);
   for (int s = 0; s < sp.nsweeps; ++s) {
@@ -1533,7 +1548,7 @@ int ppm_b200_solve_level(ppm_b200_context* ctx, const ppm_b200_params* p, int cy
       it = ctx->graphs.emplace(key, ex).first;
     }
     CK(cudaGraphLaunch(it->second, ctx->stream));
-    ctx->launches += 1 + sweep_kernels(p) * sp.nsweeps;
+    ctx->launches += 1 + sweep_kernels(p) * sp.nsweeps + (p->eos_type > 0 ? 1 : 0);
   } else {
     rc = enqueue_solve(ctx, p, io, sp, false);
     if (rc) return rc;
@@ -1600,6 +1615,7 @@ int ppm_b200_compute_pressure(ppm_b200_context* ctx, const ppm_b200_params* p, p
   ppm_b200_params q = *p;
   q.gravity = 0;
   p = &q;
+  if (p->eos_type != 0 && p->eos_type != 3) return PPM_B200_ERR_UNSUPPORTED;
   int rc = check_grid(g, p);
   if (rc) return rc;
   CK(cudaSetDevice(ctx->device));
@@ -1623,6 +1639,10 @@ int ppm_b200_compute_pressure(ppm_b200_context* ctx, const ppm_b200_params* p, p
   if (memory == PPM_B200_MEM_HOST) {
     CK(cudaMemcpyAsync(pressure, io[0].pres, (size_t)grid_size(g) * sizeof(double),
                        cudaMemcpyDeviceToHost, ctx->stream));
+    if (p->eos_type > 0) {  // the total energy was reset with the pressure
+      rc = stage_out(ctx, p, g, io[0].user);
+      if (rc) return rc;
+    }
     CK(cudaStreamSynchronize(ctx->stream));
   }
   return PPM_B200_OK;

@@ -46,6 +46,10 @@ struct ElemBatch {
   double expansion, coef_new, coef_old;
   int interpolate;
   int presfree;                  // PressureFree: calc_dt's sound speed tiny (calc_dt.F:78-137)
+  // EOSType 3 (isothermal, EOS.h): p = rho cs^2 and the total energy reset to
+  // p/((gamma-1) rho) + v^2/2 wherever the pressure is computed (Grid_ComputePressure.C:112-124)
+  int eos_type;
+  double eos_cs;
 };
 
 // grid::ComputePressure at time == Time (Grid_ComputePressure.C:96-164)
@@ -70,11 +74,30 @@ __device__ __forceinline__ double cell_pressure(const ElemGrid& G, int64_t i, do
   return p;
 }
 
+// EOSType 3: the pressure of cell i, and (RESET) its total energy reset (G.f[1] is the
+// field).  The time step does not reset: after a solve the energies are already
+// consistent, and the reset is idempotent.
+template <bool RESET>
+__device__ __forceinline__ double eos_pressure(const ElemGrid& G, int64_t i, const ElemBatch& B) {
+  const double density = G.d[i];
+  const double velocity1 = G.v[0][i];
+  const double velocity2 = G.v[1] ? G.v[1][i] : 0.0;
+  const double velocity3 = G.v[2] ? G.v[2][i] : 0.0;
+  const double cs = B.eos_cs;
+  const double p = density * cs * cs;
+  const double e = p / ((B.gamma - 1.0) * density);
+  if (RESET)
+    G.f[1][i] = e + 0.5 * (velocity1 * velocity1 + velocity2 * velocity2 + velocity3 * velocity3);
+  return p;
+}
+
 __global__ void __launch_bounds__(256) pressure_kernel(const __grid_constant__ ElemBatch B) {
   int64_t lb;
   const ElemGrid& G = B.grids[batch_locate(B.size_prefix, B.ngrids, blockIdx.x, lb)];
   const int64_t i = lb * 256 + threadIdx.x;
-  if (i < G.size) G.p[i] = cell_pressure(G, i, B.gamma, B.tiny_number, B.min_support);
+  if (i < G.size)
+    G.p[i] = B.eos_type == 3 ? eos_pressure<true>(G, i, B)
+                             : cell_pressure(G, i, B.gamma, B.tiny_number, B.min_support);
 }
 
 // calc_dt (ihydro = 0) over the active cells of every grid; min over the batch
@@ -94,7 +117,8 @@ __global__ void __launch_bounds__(256) timestep_kernel(const __grid_constant__ E
     const double u = __ldg(G.v[0] + g);
     const double v = G.v[1] ? __ldg(G.v[1] + g) : 0.0;
     const double w = G.v[2] ? __ldg(G.v[2] + g) : 0.0;
-    const double p = cell_pressure(G, g, B.gamma, B.tiny_number, B.min_support);
+    const double p = B.eos_type == 3 ? eos_pressure<false>(G, g, B)
+                                     : cell_pressure(G, g, B.gamma, B.tiny_number, B.min_support);
     // calc_dt.F:136-153
     const double cs = B.presfree ? kTiny : dmax(sqrt(B.gamma * p / density), kTiny);
     double dt1;

@@ -958,6 +958,7 @@ __device__ __forceinline__ double cell_dt1(const SweepArgs& a, const Cell& o, do
   if (p < P.pmin) p = P.pmin;
   const double min_pressure = a.min_support * P.gm1 * o.d * o.d;
   if (p < min_pressure) p = min_pressure;
+  if (a.eos_type == 3) p = o.d * a.eos_cs * a.eos_cs;  // EOS.h type 3
   const double cs = a.presfree ? kTiny : dmax(sqrt(P.gamma * p / o.d), kTiny);
   if (a.rank == 1) return dx[0] * a.aye / (cs + fabs(velocity1 - a.vg[0]));
   if (a.rank == 2)

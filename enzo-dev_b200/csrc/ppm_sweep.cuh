@@ -114,6 +114,9 @@ struct SweepArgs {
   // step (calc_dt.F:78-137), the face densities the uncorrected ones (inteuler.F:556-561),
   // the two-shock solve replaced by p* = pmin, u* = (ul + ur)/2 (twoshock.F:124-130)
   int presfree;
+  // EOSType 3 (isothermal): the folded time step's pressure is rho * eos_cs^2
+  int eos_type;
+  double eos_cs;
 };
 
 enum { kFaceVars = 12, kFluxVars = 7 };

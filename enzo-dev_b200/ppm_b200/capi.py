@@ -64,7 +64,8 @@ class Params(C.Structure):
         ("steepening", C.c_int), ("flattening", C.c_int), ("diffusion", C.c_int),
         ("conservative_rec", C.c_int), ("positive_rec", C.c_int), ("eos_type", C.c_int),
         ("number_of_colours", C.c_int), ("learned_guess", C.c_int),
-        ("dt_device", C.c_void_p), ("colour_species", C.c_void_p), ("reserved", C.c_int * 4),
+        ("dt_device", C.c_void_p), ("colour_species", C.c_void_p),
+        ("eos_sound_speed", C.c_double), ("reserved", C.c_int * 2),
     ]
 
 
@@ -236,6 +237,8 @@ def make_params(hp, dt, learned_guess=False, dt_device=None) -> Params:
     P.steepening = int(getattr(hp, "steepen", 0))
     P.flattening = int(getattr(hp, "flatten", 0))
     P.learned_guess = int(learned_guess)
+    P.eos_type = int(getattr(hp, "eos_type", 0))
+    P.eos_sound_speed = float(getattr(hp, "eos_sound_speed", 2.65e4))
     P.dt_device = _addr(dt_device) if dt_device is not None else None
     return P
 

@@ -93,6 +93,8 @@ class HydroParams:
     fallback: bool = True             # RiemannSolverFallback (:809)
     steepen: int = 0                  # PPMSteepeningParameter (:184): 0 or 1
     flatten: int = 0                  # PPMFlatteningParameter (:182): 0, 1 or 3
+    eos_type: int = 0                 # EOSType: 0 ideal gas, 3 isothermal
+    eos_sound_speed: float = 2.65e4   # EOSSoundSpeed (:814)
     riemann: int = 5                  # RiemannSolver: 5 TwoShock (the PPM default,
                                       # ReadParameterFile.C:1575-1576), 1 HLL, 4 HLLC
 

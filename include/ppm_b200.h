@@ -73,7 +73,9 @@ typedef struct ppm_b200_params {
   int diffusion;            /* PPMDiffusionParameter: must be 0 */
   int conservative_rec;     /* ConservativeReconstruction: must be 0 */
   int positive_rec;         /* PositiveReconstruction: must be 0 */
-  int eos_type;             /* EOSType: must be 0 */
+  int eos_type;             /* EOSType: 0, or 3 (isothermal, hydro_rk/EOS.h): p = rho cs^2 and the
+                               total energy reset where the pressure is computed (the solve's
+                               start and end, Grid_SolvePPM_DE.C:60, :155-157) */
   int number_of_colours;    /* NumberOfColours: 0 .. PPM_B200_MAX_COLOURS advected colour fields
                                (Grid_SolveHydroEquations.C:90-285); their fields are
                                ppm_b200_grid.colours[] */
@@ -87,7 +89,8 @@ typedef struct ppm_b200_params {
                                and the SN Ia / II metal densities,
                                Grid_CorrectForRefinedFluxes.C:397-421, :849-866); other
                                colours are left alone.  NULL: none */
-  int reserved[4];
+  double eos_sound_speed;   /* EOSSoundSpeed (EOSType 3) */
+  int reserved[2];
 } ppm_b200_params;
 
 /* One grid.  Field pointers are host or device memory as the call says.

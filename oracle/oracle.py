@@ -53,6 +53,8 @@ class OraParams(C.Structure):
         ("ncolour", C.c_int),
         ("riemann", C.c_int),
         ("colour_species", C.c_void_p),
+        ("eos_type", C.c_int),
+        ("eos_sound_speed", C.c_double),
     ]
 
 
@@ -167,6 +169,8 @@ def make_params(grid, hp, dt, ncolour=0) -> OraParams:
     P.flatten = int(getattr(hp, "flatten", 0))
     P.ncolour = int(ncolour)
     P.riemann = int(getattr(hp, "riemann", 5))
+    P.eos_type = int(getattr(hp, "eos_type", 0))
+    P.eos_sound_speed = float(getattr(hp, "eos_sound_speed", 2.65e4))
     return P
 
 

@@ -1193,6 +1193,20 @@ void ora_compute_pressure(const ora_params *P, double *const F[ORA_NFIELD], doub
   for (size_t i = 0; i < size; i++) {
     double density = F[ORA_D][i];
     double gas_energy;
+    if (P->eos_type == 3) {
+      /* Grid_ComputePressure.C:112-124 with hydro_rk/EOS.h type 3: the pressure from the
+         density and the total energy reset to the EOS energy plus the kinetic one */
+      double velocity1 = F[ORA_V1][i], velocity2 = 0.0, velocity3 = 0.0;
+      if (P->max_velocity_index > 1) velocity2 = F[ORA_V2][i];
+      if (P->max_velocity_index > 2) velocity3 = F[ORA_V3][i];
+      const double cs = P->eos_sound_speed;
+      const double p = density * cs * cs;
+      const double e = p / ((Gamma - 1.0) * density);
+      pressure[i] = p;
+      F[ORA_TE][i] = e + 0.5 * (velocity1 * velocity1 + velocity2 * velocity2 +
+                                velocity3 * velocity3);
+      continue;
+    }
     if (P->dual == 0) {
       double velocity1 = F[ORA_V1][i], velocity2 = 0.0, velocity3 = 0.0;
       if (P->max_velocity_index > 1) velocity2 = F[ORA_V2][i];
@@ -1428,6 +1442,8 @@ int ora_solve_ppm_de(const ora_params *P, int cycle, double *const F[],
     if ((n % Q.rank == 2) && nzz > 1)
       if (ora_sweep(2, &Q, F, pressure, accel, cw, nsub, sub, ggs, st, nthreads) != 0) rc = -1;
   }
+  /* energies consistent with the EOS again, Grid_SolvePPM_DE.C:155-157 */
+  if (Q.eos_type > 0) ora_compute_pressure(&Q, F, pressure);
   free(pressure);
   return rc;
 }

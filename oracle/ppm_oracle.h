@@ -68,6 +68,8 @@ typedef struct {
                           1 HLL, 4 HLLC */
   const int *colour_species; /* flux correction: ncolour flags, nonzero for a colour that
                                 keeps its fraction of the corrected density; NULL: none */
+  int eos_type;        /* EOSType: 0 ideal gas, 3 isothermal (hydro_rk/EOS.h) */
+  double eos_sound_speed; /* EOSSoundSpeed */
 } ora_params;
 
 enum { ORA_RIEMANN_HLL = 1, ORA_RIEMANN_HLLC = 4, ORA_RIEMANN_TWOSHOCK = 5 };

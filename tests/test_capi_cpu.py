@@ -50,7 +50,7 @@ def test_unsupported_configuration_is_rejected_before_any_device_work():
     for field, value in (("flattening", 4), ("diffusion", 1), ("steepening", 2),
                          ("number_of_colours", 46), ("number_of_colours", -1),
                          ("riemann_solver", 2), ("riemann_solver", 6),
-                         ("pressure_free", 2)):
+                         ("pressure_free", 2), ("eos_type", 1), ("eos_type", 2)):
         P = capi.make_params(hp, 0.1)
         setattr(P, field, value)
         G, keep = capi.make_grid(g, f)
