@@ -1651,6 +1651,7 @@ int ppm_b200_compute_pressure(ppm_b200_context* ctx, const ppm_b200_params* p, p
 static int timestep_batch(ppm_b200_context* ctx, const ppm_b200_params* p,
                           std::vector<GridIO>& io, double courant, double aye,
                           const double vgrid_in[3], double* dt_device, double* dt_host) {
+  if (p->eos_type != 0 && p->eos_type != 3) return PPM_B200_ERR_UNSUPPORTED;
   for (auto& x : io)
     for (int d = 0; d < x.g->rank; ++d)
       if (!x.g->cell_width[d]) return PPM_B200_ERR_INVALID;
