@@ -1667,7 +1667,10 @@ void launch_any(const BatchArgs& B, int64_t march_blocks, int64_t riemann_blocks
 
 }  // namespace split
 
-// One directional sweep of every grid of a batch: five launches.  The caller provides
+// One directional sweep of every grid of a batch: five launches (six with slope
+// corrections, one more with colours; the Riemann stage by B.solver and B.presfree,
+// the reconstruction's corrections variant whenever corrections, colours or
+// PressureFree need it).  The caller provides
 // each grid's fstate / fflux / plane, the prefix tables and the flagged list, and for a
 // batch of one grid also B.one (a copy of that grid's record).  ev (optional): six
 // events recorded before each kernel and after the last.  learned: start the Newton
