@@ -3,13 +3,12 @@ order of Grid_SolveHydroEquations.C:90-285).  Colours in Enzo are densities (spe
 metal density, SN colour) advected with the flow."""
 import numpy as np
 
-from ppm_b200 import harness as H
-
 
 def add_colours(g, f, seed=0, fractions=(0.25, 0.3), extra=1, marker=True):
     """Colours that are fixed mass fractions of the density (one per entry of fractions),
     `extra` smooth positive random fields, and (marker) a density-weighted step along x
-    that is zero on one side.  Ghost zones periodic, like random_state's."""
+    that is zero on one side.  The fractions inherit the density's ghost zones; the other
+    colours' ghost zones are whatever the generator gives (both solvers see the same)."""
     rng = np.random.default_rng(seed)
     n = 0
     for frac in fractions:
@@ -46,5 +45,3 @@ def hydro_only(f):
 def active(g, a):
     return a[g.active_slices()]
 
-
-__all__ = ["add_colours", "colour_keys", "hydro_only", "active", "H"]

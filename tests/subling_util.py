@@ -1,7 +1,6 @@
 """Flux boxes for the SUBling flux-correction tests, in global (level) zone indices: a
 grid's own boundary fluxes and the projected refined fluxes of a sibling's subgrid
 (struct fluxes, Fluxes.h:29-37; GetProjectedBoundaryFluxes fills the latter)."""
-import numpy as np
 
 
 def gbox(glo, ghi, rng, rank=3, scale=0.05):

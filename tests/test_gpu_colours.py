@@ -7,7 +7,7 @@ import numpy as np
 import pytest
 
 import oracle as O
-from colour_util import add_colours, colour_keys
+from colour_util import add_colours
 from parity_util import compare, copy_fields, random_state
 from ppm_b200 import capi
 from ppm_b200 import harness as H

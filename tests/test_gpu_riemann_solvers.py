@@ -3,8 +3,6 @@ plane, the density-only check) against the CPU oracle: bit-identical fields afte
 step, single grids of rank 1-3, dual energy on and off, colours, slope corrections, the
 batched level with and without graphs, HLLC's per-cell HLL fallback, and HLL's stop on
 a negative density (ERR_NEGATIVE)."""
-import dataclasses
-
 import numpy as np
 import pytest
 

@@ -8,7 +8,6 @@ import dataclasses
 import numpy as np
 
 import oracle as O
-from parity_util import copy_fields
 from ppm_b200 import harness as H
 
 

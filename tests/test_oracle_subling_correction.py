@@ -7,8 +7,6 @@ arithmetic: the corrected density of each edge zone is its old density plus
 (own right flux - refined left flux) on a right contact, minus (own left flux - refined
 right flux) on a left contact; zones outside the contact are untouched; a contact across
 a periodic level boundary wraps."""
-import ctypes as C
-
 import numpy as np
 import pytest
 
