@@ -118,3 +118,16 @@ def test_species_colours_match_oracle(ctx):
                                 species=species)
     for k in f:
         assert np.array_equal(f_gpu[k], f_ora[k]), k
+
+
+@pytest.mark.parametrize("lo,hi", [((21, 22, 0), (24, 30, 0)), ((12, 15, 0), (18, 22, 0))])
+def test_rank2_contacts_match_oracle(ctx, lo, hi):
+    hp = H.HydroParams(gamma=5.0 / 3.0, dual=True)
+    g = H.Grid.uniform((8, 6))  # active global x 13..20, y 23..28 at GGS
+    f = random_state(g, hp, seed=21)
+    rng = np.random.default_rng(22)
+    ggs = (GGS[0], GGS[1], 0)
+    own = own_box(g, ggs, rng, rank=2)
+    out = _compare(ctx, g, hp, f, own, [gbox(lo, hi, rng, rank=2)], ggs, (64, 64, 1),
+                   (0, 0, 0))
+    assert not np.array_equal(out["d"], f["d"])
