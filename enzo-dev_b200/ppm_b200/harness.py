@@ -301,6 +301,39 @@ def turbulence_device(grid, hp, mach=3.0, sigma_lnrho=0.5, seed=1234, device="cu
     return f
 
 
+def zeldovich_pancake(grid, hp, z_init=100.0, z_collapse=1.0, e_init=1e-6, offset=0.0):
+    """A Zel'dovich pancake along x in code units (the published one-dimensional
+    solution that Grid_ZeldovichPancakeInitializeGrid.C:132-189 sets up): zone q of the
+    N active zones has the Lagrangian position q + 1/2 - offset - N/2 (in zones), mapped
+    to its Eulerian x by Newton's method on x - A sin(kx)/k = x_L with A = (1+z_c)/(1+z_i)
+    and k = 2 pi / N; the density is 1/(1 - A cos kx), the x velocity
+    -sqrt(2/3) (1+z_c)/((1+z_i) 2 pi) sin kx, the specific internal energy e_init times
+    rho^(gamma-1) (adiabatic from a uniform start).  Ghost zones periodic."""
+    f = new_fields(grid, hp.dual)
+    n = grid.end[0] - grid.start[0] + 1
+    amp = (1.0 + z_collapse) / (1.0 + z_init)
+    amp_v = -np.sqrt(2.0 / 3.0) * (1.0 + z_collapse) / ((1.0 + z_init) * 2.0 * np.pi)
+    k = 2.0 * np.pi / n
+    x_l = np.arange(n) + (0.5 - offset) - 0.5 * n
+    x_e = x_l.copy()
+    for _ in range(100):  # Newton iteration, converged well before the bound
+        step = (x_l - x_e + amp * np.sin(k * x_e) / k) / (1.0 - amp * np.cos(k * x_e))
+        x_e = x_e + step
+        if np.all(np.abs(step) <= 1e-14 * np.maximum(np.abs(x_e), 1.0)):
+            break
+    rho = 1.0 / (1.0 - amp * np.cos(k * x_e))
+    u = amp_v * np.sin(k * x_e)
+    e_int = e_init * rho ** (hp.gamma - 1.0) / (hp.gamma - 1.0)
+    act = grid.active_slices()
+    f["d"][act] = rho[None, None, :]
+    f["v1"][act] = u[None, None, :]
+    if hp.dual:
+        f["ge"][act] = e_int[None, None, :]
+    f["te"][act] = (e_int + 0.5 * u * u)[None, None, :]
+    fill_ghosts(grid, f, "periodic")
+    return f
+
+
 def sedov(grid, hp, e_blast=1.0, rho0=1.0, p0=1e-5):
     """Point blast: E deposited as thermal energy in the central 2^3 active cells."""
     assert grid.rank == 3
