@@ -41,7 +41,7 @@ def test_comoving_pancake_cycles_match_oracle(ctx, shape):
     for cyc in range(4):
         p = O.compute_pressure(g, hp, f_ora)
         dt = hp.cfl * O.calc_dt(g, hp, f_ora, p, g.cellwidth)
-        coef = dt * 0.5 / t  # dt * adot / a of an Einstein-de Sitter expansion
+        coef = 0.004  # dt * adot / a: the expansion limits a cosmological step to a few 1e-3
         O.expansion_terms(g, hp, f_ora, None, t + dt, t, coef)
         ctx.expansion_terms(g, hp, f_gpu, None, t + dt, t, coef)
         rc, _ = O.solve_ppm_de(g, hp, dt, cyc, f_ora, g.cellwidth, accel=acc)
