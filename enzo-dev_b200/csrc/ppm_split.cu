@@ -568,8 +568,14 @@ __device__ __forceinline__ HllFace hll_any(const FaceState& s, const Phys& P) {
   return HLLC ? hllc_face<DUAL>(s, P) : hll_face<DUAL>(s, P);
 }
 
+// 8 blocks of 128 threads per SM (64 registers): the Riemann stage 12 % faster than at the
+// 6 blocks its 74 registers allowed (HLLC 0.95 -> 0.83 ms per 256^3 sweep)
+#ifndef PPM_HLL_MINBLOCKS
+#define PPM_HLL_MINBLOCKS (8 * 128 / PPM_RIEMANN_THREADS)
+#endif
 template <bool DUAL, bool ONE, bool HLLC, bool COL>
-__global__ void __launch_bounds__(kRiemannThreads) hll_riemann_kernel(const __grid_constant__ BatchArgs B) {
+__global__ void __launch_bounds__(kRiemannThreads, PPM_HLL_MINBLOCKS)
+    hll_riemann_kernel(const __grid_constant__ BatchArgs B) {
   int64_t lb;
   const int g = locate<ONE>(B.riemann_prefix, B.ngrids, lb);
   PPM_BIND_RECORD(a, g)
