@@ -1322,6 +1322,15 @@ extern "C" {
 
 int ppm_b200_version(void) { return PPM_B200_VERSION; }
 
+int ppm_b200_abi_check(const long long* layout, int n) {
+  static const long long mine[] = {PPM_B200_ABI_LAYOUT(PPM_B200_ABI_ITEM)};
+  const int count = (int)(sizeof(mine) / sizeof(mine[0]));
+  if (!layout || n != count) return PPM_B200_ERR_INVALID;
+  for (int i = 0; i < count; ++i)
+    if (layout[i] != mine[i]) return PPM_B200_ERR_INVALID;
+  return PPM_B200_OK;
+}
+
 const char* ppm_b200_error_string(int code) {
   switch (code) {
     case PPM_B200_OK: return "ok";

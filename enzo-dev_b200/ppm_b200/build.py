@@ -45,14 +45,19 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     if not force and not needs_build():
         return LIB
     OUT_DIR.mkdir(parents=True, exist_ok=True)
+    headers = list(CSRC.glob("*.cuh")) + list(INCLUDE.glob("*.h"))
+    newest_header = max(p.stat().st_mtime for p in headers)
     objs = []
     for src in SOURCES:
         obj = OUT_DIR / (Path(src).stem + ".o")
-        cmd = [nvcc(), *ARCH, *NVCC_FLAGS, "-I", str(INCLUDE), "-I", str(CSRC),
-               "-c", str(CSRC / src), "-o", str(obj)]
-        if verbose:
-            cmd += ["-Xptxas", "-v"]
-        subprocess.run(cmd, check=True)
+        stale = (force or not obj.exists() or obj.stat().st_mtime < newest_header
+                 or obj.stat().st_mtime < (CSRC / src).stat().st_mtime)
+        if stale:
+            cmd = [nvcc(), *ARCH, *NVCC_FLAGS, "-I", str(INCLUDE), "-I", str(CSRC),
+                   "-c", str(CSRC / src), "-o", str(obj)]
+            if verbose:
+                cmd += ["-Xptxas", "-v"]
+            subprocess.run(cmd, check=True)
         objs.append(str(obj))
     tmp = LIB.with_suffix(".so.tmp")
     subprocess.run([nvcc(), *ARCH, "-shared", "-o", str(tmp), *objs, "-lcudart"], check=True)

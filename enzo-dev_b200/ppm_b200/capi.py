@@ -43,7 +43,7 @@ EXPORTS = (
     "ppm_b200_profile_stages", "ppm_b200_set_guess", "ppm_b200_riemann_log",
     "ppm_b200_riemann_log_count", "ppm_b200_guess_features", "ppm_b200_guess_grad",
     "ppm_b200_guess_adam", "ppm_b200_guess_eval", "ppm_b200_expansion_terms",
-    "ppm_b200_expansion_terms_level", "ppm_b200_set_cfl",
+    "ppm_b200_expansion_terms_level", "ppm_b200_set_cfl", "ppm_b200_abi_check",
 )
 
 GUESS_WEIGHTS = 4673  # W1[6][64] b1[64] W2[64][64] b2[64] w3[64] b3

@@ -22,6 +22,22 @@
 #ifndef PPM_B200_H
 #define PPM_B200_H
 
+/* Enzo includes its headers with `#define int long_int` (LARGE_INTS, which the
+   default CONFIG_INTEGERS = 64 selects: macros_and_parameters.h:217) and
+   `#define float double` (CONFIG_BFLOAT_8: macros_and_parameters.h:257) in force.
+   Under those macros every `int` below would become a 64-bit integer and every
+   `float` a double, so the caller's view of the structs, the return values and the
+   weight arrays would no longer be the library's.  Both macros are suspended for
+   the length of this header and restored at its end; the declarations always mean
+   the C types written here.  ppm_b200_abi_check lets a caller confirm at start-up
+   that its compiled view of the structs matches the library's. */
+#pragma push_macro("int")
+#pragma push_macro("float")
+#undef int
+#undef float
+
+#include <stddef.h>
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -378,7 +394,34 @@ int ppm_b200_euler_sweep_static(int dim, const ppm_b200_params *params,
 const char *ppm_b200_error_string(int code);
 int ppm_b200_version(void);
 
+/* --- ABI self-check (no counterpart in the reference) ---
+   PPM_B200_ABI_LAYOUT(X) lists the sizes and member offsets of the structs above as
+   the including translation unit sees them.  A caller builds the list once,
+     static const long long layout[] = { PPM_B200_ABI_LAYOUT(PPM_B200_ABI_ITEM) };
+     if (ppm_b200_abi_check(layout, (int)(sizeof layout / sizeof layout[0])) != 0) ...
+   and the library compares it with its own: PPM_B200_OK when they agree,
+   PPM_B200_ERR_INVALID otherwise (different build flags, packing or a stale header). */
+#define PPM_B200_ABI_ITEM(e) (long long)(e),
+#define PPM_B200_ABI_LAYOUT(X)                                                        \
+  X(sizeof(ppm_b200_params)) X(offsetof(ppm_b200_params, min_support))              \
+  X(offsetof(ppm_b200_params, dual_energy)) X(offsetof(ppm_b200_params, learned_guess)) \
+  X(offsetof(ppm_b200_params, dt_device)) X(offsetof(ppm_b200_params, colour_species)) \
+  X(offsetof(ppm_b200_params, eos_sound_speed)) X(offsetof(ppm_b200_params, reserved)) \
+  X(sizeof(ppm_b200_grid)) X(offsetof(ppm_b200_grid, dims))                          \
+  X(offsetof(ppm_b200_grid, end)) X(offsetof(ppm_b200_grid, density))                \
+  X(offsetof(ppm_b200_grid, velocity)) X(offsetof(ppm_b200_grid, acceleration))      \
+  X(offsetof(ppm_b200_grid, cell_width)) X(offsetof(ppm_b200_grid, colours))         \
+  X(sizeof(ppm_b200_fluxes)) X(offsetof(ppm_b200_fluxes, right_end))                 \
+  X(offsetof(ppm_b200_fluxes, left)) X(offsetof(ppm_b200_fluxes, right))             \
+  X(offsetof(ppm_b200_fluxes, colour_left)) X(offsetof(ppm_b200_fluxes, colour_right)) \
+  X(sizeof(ppm_b200_stats)) X(offsetof(ppm_b200_stats, newton_hist))                 \
+  X(offsetof(ppm_b200_stats, guess_rejected))
+int ppm_b200_abi_check(const long long *layout, int n);
+
 #ifdef __cplusplus
 }
 #endif
+
+#pragma pop_macro("float")
+#pragma pop_macro("int")
 #endif /* PPM_B200_H */
