@@ -108,6 +108,7 @@ void launch_correct_fluxes(const FluxFix& X, const FluxPhase* phases, cudaStream
 }  // namespace ppm
 
 using ppm::BatchArgs;
+using ppm::build_coef;
 using ppm::Coef;
 using ppm::ElemBatch;
 using ppm::ElemGrid;
@@ -295,31 +296,6 @@ int64_t grid_active(const ppm_b200_grid* g) {
   int64_t n = 1;
   for (int d = 0; d < g->rank; ++d) n *= g->end[d] - g->start[d] + 1;
   return n;
-}
-
-// inteuler.F:140-158 on the host, same expressions, 1-based i mapped to entry i-1.
-void build_coef(const double* dxi_in, int n, int is0, int ie0, std::vector<Coef>& out) {
-  out.assign(n, Coef{0, 0, 0, 0, 0, 0, 0, 0});
-  auto dxi = [&](int i) { return dxi_in[i - 1]; };
-  const int i1 = is0 + 1, i2 = ie0 + 1;
-  for (int i = 1; i <= n; ++i) out[i - 1].dx = dxi(i);
-  for (int i = i1 - 2; i <= i2 + 2; i++) {
-    double qa = dxi(i) / (dxi(i - 1) + dxi(i) + dxi(i + 1));
-    out[i - 1].c1 = qa * (2.0 * dxi(i - 1) + dxi(i)) / (dxi(i + 1) + dxi(i));
-    out[i - 1].c2 = qa * (2.0 * dxi(i + 1) + dxi(i)) / (dxi(i - 1) + dxi(i));
-  }
-  for (int i = i1 - 1; i <= i2 + 2; i++) {
-    double qa = dxi(i - 2) + dxi(i - 1) + dxi(i) + dxi(i + 1);
-    double qb = dxi(i - 1) / (dxi(i - 1) + dxi(i));
-    double qc = (dxi(i - 2) + dxi(i - 1)) / (2.0 * dxi(i - 1) + dxi(i));
-    double qd = (dxi(i + 1) + dxi(i)) / (2.0 * dxi(i) + dxi(i - 1));
-    qb = qb + 2.0 * dxi(i) * qb / qa * (qc - qd);
-    out[i - 1].c3 = 1.0 - qb;
-    out[i - 1].c4 = qb;
-    out[i - 1].c5 = dxi(i) / qa * qd;
-    out[i - 1].c6 = -(dxi(i - 1) / qa * qc);
-    out[i - 1].dx2i = 0.5 / dxi(i);
-  }
 }
 
 int check_supported(const ppm_b200_params* p) {

@@ -18,9 +18,16 @@
 //    any device work.
 //  * Every GPU that loads the library holds the array (about 48.1 MiB) until the
 //    process exits.
-//  * Set-up: the first call on a device, with that device current, looks up the
-//    array's device address (cudaGetSymbolAddress).  Make that first call before any
-//    stream capture.
+//  * Set-up: the first call in a CUDA context (a device's primary context, current on
+//    the calling thread) looks up the array's device address with cudaGetSymbolAddress
+//    and keeps it for that context; a new context (after cudaDeviceReset, or another
+//    device) looks it up again.
+//  * Never call it while its stream is being captured into a CUDA graph: it copies from
+//    pageable host memory and waits for its stream, which a capture cannot contain.  It
+//    checks this first and returns PPM_B200_ERR_INVALID without touching the stream.
+//  * Outputs must not overlap the inputs or the pressure (the kernels read their
+//    inputs as read-only, non-aliased data); an overlapping call, such as an in-place
+//    sweep, returns PPM_B200_ERR_INVALID.
 //  * The array is shared by every call on a device and keeps the last call's
 //    contents.  Calls that overlap on the GPU (different streams, or different host
 //    threads) race on it; serialise them.
@@ -57,11 +64,25 @@ static_assert(sizeof(ppm::SweepArgs) <= 512, "descriptor area");
 constexpr int kMaxDevices = 64;
 
 struct DeviceSlot {
-  bool ready = false;
+  void* context = nullptr;       // the CUDA context the address belongs to
   unsigned char* base = nullptr;
 };
 DeviceSlot g_slots[kMaxDevices];
 std::mutex g_setup_mutex;
+
+// cuCtxGetCurrent through the runtime's driver entry point (no link against libcuda)
+typedef int (*CtxGetCurrentFn)(void**);
+CtxGetCurrentFn ctx_get_current() {
+  static const CtxGetCurrentFn fn = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      f = nullptr;
+    return reinterpret_cast<CtxGetCurrentFn>(f);
+  }();
+  return fn;
+}
 
 }  // namespace
 
@@ -72,12 +93,17 @@ static __device__ __align__(256) unsigned char g_sweep_scratch[kStaticBytes];
 
 namespace {
 
-// Once per device, with that device current: look up the array's device address.
+// Once per device and CUDA context, with that device current: look up the array's
+// device address.  The address is kept with the context it belongs to; when the
+// device's context changes (cudaDeviceReset unloads the module), it is looked up again.
 int static_setup(int device, unsigned char** base) {
   if (device < 0 || device >= kMaxDevices) return PPM_B200_ERR_INVALID;
   std::lock_guard<std::mutex> lock(g_setup_mutex);
   DeviceSlot& s = g_slots[device];
-  if (!s.ready) {
+  void* current = nullptr;
+  const CtxGetCurrentFn get = ctx_get_current();
+  if (get) get(&current);  // no context yet: looked up below, which creates it
+  if (!s.base || !current || current != s.context) {
     void* p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_sweep_scratch);
     if (e != cudaSuccess || p == nullptr) {
@@ -85,35 +111,17 @@ int static_setup(int device, unsigned char** base) {
       return PPM_B200_ERR_CUDA;
     }
     s.base = static_cast<unsigned char*>(p);
-    s.ready = true;
+    s.context = nullptr;
+    if (get) get(&s.context);
   }
   *base = s.base;
   return PPM_B200_OK;
 }
 
-// inteuler.F:140-158 on the host (same expressions as the context path).
-void coef_table(const double* dxi_in, int n, int is0, int ie0, std::vector<ppm::Coef>& out) {
-  out.assign(n, ppm::Coef{0, 0, 0, 0, 0, 0, 0, 0});
-  auto dxi = [&](int i) { return dxi_in[i - 1]; };
-  const int i1 = is0 + 1, i2 = ie0 + 1;
-  for (int i = 1; i <= n; ++i) out[i - 1].dx = dxi(i);
-  for (int i = i1 - 2; i <= i2 + 2; i++) {
-    double qa = dxi(i) / (dxi(i - 1) + dxi(i) + dxi(i + 1));
-    out[i - 1].c1 = qa * (2.0 * dxi(i - 1) + dxi(i)) / (dxi(i + 1) + dxi(i));
-    out[i - 1].c2 = qa * (2.0 * dxi(i + 1) + dxi(i)) / (dxi(i - 1) + dxi(i));
-  }
-  for (int i = i1 - 1; i <= i2 + 2; i++) {
-    double qa = dxi(i - 2) + dxi(i - 1) + dxi(i) + dxi(i + 1);
-    double qb = dxi(i - 1) / (dxi(i - 1) + dxi(i));
-    double qc = (dxi(i - 2) + dxi(i - 1)) / (2.0 * dxi(i - 1) + dxi(i));
-    double qd = (dxi(i + 1) + dxi(i)) / (2.0 * dxi(i) + dxi(i - 1));
-    qb = qb + 2.0 * dxi(i) * qb / qa * (qc - qd);
-    out[i - 1].c3 = 1.0 - qb;
-    out[i - 1].c4 = qb;
-    out[i - 1].c5 = dxi(i) / qa * qd;
-    out[i - 1].c6 = -(dxi(i - 1) / qa * qc);
-    out[i - 1].dx2i = 0.5 / dxi(i);
-  }
+// true when [a, a + n) and [b, b + n) overlap (n doubles each)
+bool overlaps(const double* a, const double* b, int64_t n) {
+  if (!a || !b) return false;
+  return a < b + n && b < a + n;
 }
 
 int fail_cuda(cudaError_t e, const char* what) {
@@ -147,6 +155,18 @@ extern "C" int ppm_b200_euler_sweep_static(int dim, const ppm_b200_params* p,
     if (!in->velocity[d] || !out->velocity[d]) return PPM_B200_ERR_INVALID;
   if (p->dual_energy && (!in->gas_energy || !out->gas_energy)) return PPM_B200_ERR_INVALID;
   if (p->gravity && !in->acceleration[dim]) return PPM_B200_ERR_INVALID;
+  {  // outputs must not overlap any input (the kernels read inputs as non-aliased)
+    const int64_t cells = (int64_t)in->dims[0] * in->dims[1] * in->dims[2];
+    const double* ins[7] = {in->density, in->total_energy, in->velocity[0], in->velocity[1],
+                            in->velocity[2], in->gas_energy, pressure};
+    const double* outs[6] = {out->density, out->total_energy,
+                             out->velocity[0], in->rank > 1 ? out->velocity[1] : nullptr,
+                             in->rank > 2 ? out->velocity[2] : nullptr,
+                             p->dual_energy ? out->gas_energy : nullptr};
+    for (const double* o : outs)
+      for (const double* i : ins)
+        if (overlaps(o, i, cells)) return PPM_B200_ERR_INVALID;
+  }
 
   const int GD0 = in->dims[0], GD1 = in->dims[1], GD2 = in->dims[2];
   ppm::SweepArgs a;
@@ -168,7 +188,16 @@ extern "C" int ppm_b200_euler_sweep_static(int dim, const ppm_b200_params* p,
       (size_t)a.npencils * sizeof(int64_t);
   if (a.n > kStaticCoefEntries || plane_bytes > kStaticPlaneBytes) return PPM_B200_ERR_TOO_LARGE;
 
-  // ---- set-up of this device (first call only), with the caller's device current
+  // ---- never under stream capture: checked before anything touches the stream
+  cudaStream_t st = static_cast<cudaStream_t>(cuda_stream);
+  {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone)
+      return PPM_B200_ERR_INVALID;
+  }
+
+  // ---- set-up of this device and context (first call only), with the caller's device
+  // current
   int device = 0;
   cudaError_t e = cudaGetDevice(&device);
   if (e != cudaSuccess) return fail_cuda(e, "cudaGetDevice");
@@ -179,13 +208,12 @@ extern "C" int ppm_b200_euler_sweep_static(int dim, const ppm_b200_params* p,
   ppm::Coef* coef = reinterpret_cast<ppm::Coef*>(base + kStaticCounterBytes);
   unsigned char* desc = base + kStaticCounterBytes + kStaticCoefBytes;
   double* planes = reinterpret_cast<double*>(desc + kStaticDescBytes);
-  cudaStream_t st = static_cast<cudaStream_t>(cuda_stream);
 
   // ---- per-call contents: counters start at zero, the coefficient table is rewritten
   e = cudaMemsetAsync(counters, 0, kStaticCounterBytes, st);
   if (e != cudaSuccess) return fail_cuda(e, "cudaMemsetAsync");
   std::vector<ppm::Coef> table;
-  coef_table(in->cell_width[dim], a.n, a.is, a.ie, table);
+  ppm::build_coef(in->cell_width[dim], a.n, a.is, a.ie, table);
   e = cudaMemcpyAsync(coef, table.data(), table.size() * sizeof(ppm::Coef),
                       cudaMemcpyHostToDevice, st);
   if (e != cudaSuccess) return fail_cuda(e, "cudaMemcpyAsync");

@@ -4,6 +4,7 @@
 #include <cuda.h>  // CUtensorMap
 
 #include <cstdint>
+#include <vector>
 
 namespace ppm {
 
@@ -180,6 +181,33 @@ struct BatchArgs {
 #define PPM_X_TILE_CELLS 4
 #endif
 enum { kXTileRows = 32, kXTileCells = PPM_X_TILE_CELLS, kXBuffers = PPM_X_BUFFERS };
+
+// inteuler.F:140-158 on the host (same expressions; 1-based i mapped to entry i-1): the
+// coefficient table of one sweep axis.  Every entry point builds its table here, so the
+// library's paths cannot drift apart; host code is compiled with -ffp-contract=off.
+inline void build_coef(const double* dxi_in, int n, int is0, int ie0, std::vector<Coef>& out) {
+  out.assign(n, Coef{0, 0, 0, 0, 0, 0, 0, 0});
+  auto dxi = [&](int i) { return dxi_in[i - 1]; };
+  const int i1 = is0 + 1, i2 = ie0 + 1;
+  for (int i = 1; i <= n; ++i) out[i - 1].dx = dxi(i);
+  for (int i = i1 - 2; i <= i2 + 2; i++) {
+    double qa = dxi(i) / (dxi(i - 1) + dxi(i) + dxi(i + 1));
+    out[i - 1].c1 = qa * (2.0 * dxi(i - 1) + dxi(i)) / (dxi(i + 1) + dxi(i));
+    out[i - 1].c2 = qa * (2.0 * dxi(i + 1) + dxi(i)) / (dxi(i - 1) + dxi(i));
+  }
+  for (int i = i1 - 1; i <= i2 + 2; i++) {
+    double qa = dxi(i - 2) + dxi(i - 1) + dxi(i) + dxi(i + 1);
+    double qb = dxi(i - 1) / (dxi(i - 1) + dxi(i));
+    double qc = (dxi(i - 2) + dxi(i - 1)) / (2.0 * dxi(i - 1) + dxi(i));
+    double qd = (dxi(i + 1) + dxi(i)) / (2.0 * dxi(i) + dxi(i - 1));
+    qb = qb + 2.0 * dxi(i) * qb / qa * (qc - qd);
+    out[i - 1].c3 = 1.0 - qb;
+    out[i - 1].c4 = qb;
+    out[i - 1].c5 = dxi(i) / qa * qd;
+    out[i - 1].c6 = -(dxi(i - 1) / qa * qc);
+    out[i - 1].dx2i = 0.5 / dxi(i);
+  }
+}
 
 // Grid that owns block b of a stage, and the block's index inside that grid.
 __device__ __forceinline__ int batch_locate(const int64_t* prefix, int ngrids, int64_t b,

@@ -379,14 +379,18 @@ int ppm_b200_guess_eval(ppm_b200_context *ctx, const float *features, long long 
    For callers that cannot call cudaMalloc when they advance a grid -- code running
    under a memory arena that owns all device memory, or inside a callback where an
    allocation could synchronise or deadlock.  `in` and `out` are caller-owned DEVICE
-   arrays (out must not alias in; cell widths stay host arrays), `pressure` a device
-   array; the sweep's scratch comes from a fixed array compiled into the library.
+   arrays (cell widths stay host arrays), `pressure` a device array; no output may
+   overlap an input or the pressure (an in-place call returns PPM_B200_ERR_INVALID).
+   The sweep's scratch comes from a fixed array compiled into the library.
    Limit: 19 * 8 * (active cells along dim + 1) * pencils bytes <= 48 MiB (grids up
    to 64^3 active cells) and pencils of at most 1031 cells; larger sizes return
-   PPM_B200_ERR_TOO_LARGE.  The first call on a device (which must be current) looks
-   up the array's address; make it before any stream capture.  The array is shared
-   by all calls on a device: calls that overlap on the GPU race.  Synchronous on
-   cuda_stream (NULL = default stream); no subgrid flux capture. */
+   PPM_B200_ERR_TOO_LARGE.  The first call in a CUDA context (the device current)
+   looks up the array's address and keeps it for that context.  The call copies from
+   host memory and waits for its stream, so it must never run while cuda_stream is
+   being captured into a graph: it then returns PPM_B200_ERR_INVALID without touching
+   the stream.  The array is shared by all calls on a device: calls that overlap on the
+   GPU race.  Synchronous on cuda_stream (NULL = default stream); no subgrid flux
+   capture. */
 int ppm_b200_euler_sweep_static(int dim, const ppm_b200_params *params,
                                 const ppm_b200_grid *in, const double *pressure,
                                 ppm_b200_grid *out, void *cuda_stream, ppm_b200_stats *stats);

@@ -8,11 +8,11 @@ exact Riemann solution inside given x-windows at a given rtol/atol
 the exact solution computed by ``exact_riemann.py`` at the same 1000 sample
 positions the reference's ``*_exact.txt`` files use.
 
-When the reference tree is present (the build container), it also checks the
-exact solutions against the reference's own ``*_exact.txt`` files and records
-the largest deviation per column in the fixture.
+Given the root of an enzo-dev checkout, it also checks the exact solutions
+against the reference's own ``*_exact.txt`` files and records the largest
+deviation per column in the fixture.
 
-    python tests/golden/make_golden.py [--reference /root/reference]
+    python tests/golden/make_golden.py --reference <enzo-dev checkout>
 """
 from __future__ import annotations
 
@@ -74,7 +74,8 @@ COLS = ["density", "velocity_x", "pressure", "specific_thermal_energy"]
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", required=True,
+                    help="root of the enzo-dev tree holding run/Hydro/Hydro-1D")
     args = ap.parse_args()
     ref = Path(args.reference) / "run" / "Hydro" / "Hydro-1D"
     pos = (np.arange(1000) + 0.5) / 1000.0

@@ -2,8 +2,8 @@
 of a uniform grid with its halo exchange and global time step reproduces the undivided
 grid bit for bit; the AMR-level partition covers every patch once and balances cells.
 
-The ranks advance their slabs with the CPU oracle (the GPU path is the same host code
-with device tensors and NCCL; this machine has no GPU)."""
+The ranks advance their slabs with the CPU oracle, so the test runs without a GPU; the
+GPU path is the same host code with device tensors and NCCL."""
 import os
 import socket
 
