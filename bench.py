@@ -55,6 +55,9 @@ def parse():
     ap.add_argument("--size", type=int, default=256, help="active cells per dimension")
     ap.add_argument("--seed", type=int, default=20240611)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-table", action="store_true",
+                    help="time the CPU baseline table (configurations 1-3, one core and all "
+                         "cores, with and without contraction) and exit")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-level", action="store_true",
                     help="skip the batched AMR-level measurement")
@@ -186,13 +189,26 @@ def committed_traffic():
 
 
 # ---------------------------------------------------------------- CPU reference (oracle port)
+def cpu_build(kind="native"):
+    """The oracle module with the timing build `kind` selected: "native" (-O3
+    -march=native, no contraction: bit-identical to the checker) or "native_fma"
+    (contraction allowed).  Both are rebuilt here (make -B), on the machine that runs
+    them, so that -march=native matches this host's CPU."""
+    sys.path.insert(0, str(REPO / "oracle"))
+    import oracle as O  # the CPU baseline legs are the one place bench.py runs the oracle
+    if kind != "parity" and not getattr(cpu_build, "built", False):
+        subprocess.run(["make", "-s", "-B", "-C", str(REPO / "oracle"), "native"], check=True)
+        cpu_build.built = True
+    O.select(kind)
+    return O
+
+
 def cpu_reference_rate(size, seed, nthreads, min_seconds=10.0, max_steps=12, colours=0,
-                       riemann=5):
+                       riemann=5, kind="native"):
     """Times the C restatement of the Fortran path (the oracle) on the host cores: steps
     of the same workload until min_seconds of SolvePPM_DE time (at least 2 steps).
     Returns (zone-updates/s, seconds, steps)."""
-    sys.path.insert(0, str(REPO / "oracle"))
-    import oracle as O  # the CPU baseline leg is the one place bench.py runs the oracle
+    O = cpu_build(kind)
     hp = H.HydroParams(gamma=5.0 / 3.0, cfl=0.4, dual=True, riemann=riemann)
     g = H.Grid.uniform((size, size, size))
     f = H.turbulence(g, hp, mach=3.0, seed=seed)
@@ -213,6 +229,92 @@ def cpu_reference_rate(size, seed, nthreads, min_seconds=10.0, max_steps=12, col
     return g.active_cells * len(times) / sum(times), sum(times), len(times)
 
 
+def cpu_model():
+    try:
+        for ln in Path("/proc/cpuinfo").read_text().splitlines():
+            if ln.startswith("model name"):
+                return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def run_cpu_table(args):
+    """The CPU baseline table: configurations 1-3 on one core and on all host cores,
+    with the -O3 -march=native oracle build without and with contraction.  Each entry
+    times a bounded sample of its workload (steps, or patches of the level, until about
+    `budget` seconds); zone-updates/s counts active cells advanced one full step."""
+    budget = 8.0
+    ncores = os.cpu_count() or 1
+    # the workloads, generated once
+    hp1 = H.HydroParams(gamma=1.4, cfl=0.4, dual=True)
+    g1 = H.Grid.uniform((64, 64, 64))
+    f1 = H.shock_tube(g1, hp1, 0.5, (1.0, 0.0, 1.0), (0.125, 0.0, 0.1))
+    H.fill_ghosts(g1, f1, "outflow")
+    hp2 = H.HydroParams(gamma=5.0 / 3.0, cfl=0.4, dual=True)
+    g2 = H.Grid.uniform((args.size,) * 3)
+    f2 = H.turbulence(g2, hp2, mach=3.0, seed=args.seed)
+    grids3, f3 = H.amr_level(hp2, npatch=args.level_patches, seed=args.seed)
+    rows = []
+    for kind in ("native", "native_fma"):
+        O = cpu_build(kind)
+        for nt in (1, ncores):
+            row = {"build": "gcc -O3 -march=native " +
+                   ("-ffp-contract=off" if kind == "native" else "-ffp-contract=fast"),
+                   "threads": nt}
+            f = {k: v.copy() for k, v in f1.items()}
+            rate, n, t = _time_steps(O, g1, hp1, f, nt, "outflow", budget, 100)
+            row["sod64"] = {"zone_updates_per_s": rate, "steps": n, "seconds": t}
+            f = {k: v.copy() for k, v in f2.items()}
+            rate, n, t = _time_steps(O, g2, hp2, f, nt, "periodic", budget, 50)
+            row[f"turbulence{args.size}"] = {"zone_updates_per_s": rate, "steps": n,
+                                             "seconds": t}
+            # one level step, patch by patch (the reference's grid loop), with the level's
+            # time step; a bounded sample of the patches in order
+            dt = min(hp2.cfl * O.calc_dt(g, hp2, fh, O.compute_pressure(g, hp2, fh),
+                                         g.cellwidth) for g, fh in zip(grids3, f3))
+            total, cells, npat = 0.0, 0, 0
+            for g, fh in zip(grids3, f3):
+                f = {k: v.copy() for k, v in fh.items()}
+                t0 = time.perf_counter()
+                rc, _ = O.solve_ppm_de(g, hp2, dt, 0, f, g.cellwidth, nthreads=nt)
+                total += time.perf_counter() - t0
+                cells += g.active_cells
+                npat += 1
+                if rc != 0:
+                    raise RuntimeError("oracle level step failed")
+                if total >= budget:
+                    break
+            row["amr_level"] = {"zone_updates_per_s": cells / total, "patches": npat,
+                                "of": len(grids3), "seconds": total}
+            rows.append(row)
+            print(json.dumps(row), flush=True)
+    line = {"cpu_table": rows, "cpu_model": cpu_model(), "cores": ncores, "mpi_ranks": 1,
+            "kind": "port (C restatement of the Fortran path; no Fortran compiler)",
+            "sample": f"each entry about {budget:.0f} s: steps of Sod 64^3 (of 100), of the "
+                      f"{args.size}^3 turbulence, and patches of one {args.level_patches}-patch "
+                      "level step, in order"}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def _time_steps(O, g, hp, f, nthreads, bc, budget, max_steps):
+    total, steps = 0.0, 0
+    for cyc in range(max_steps):
+        p = O.compute_pressure(g, hp, f)
+        dt = hp.cfl * O.calc_dt(g, hp, f, p, g.cellwidth)
+        t0 = time.perf_counter()
+        rc, _ = O.solve_ppm_de(g, hp, dt, cyc, f, g.cellwidth, nthreads=nthreads)
+        total += time.perf_counter() - t0
+        steps += 1
+        if rc != 0:
+            raise RuntimeError("oracle step failed")
+        H.fill_ghosts(g, f, bc)
+        if total >= budget:
+            break
+    return g.active_cells * steps / total, steps, total
+
+
 def run_reference(args):
     rank, world, local = dist_env()
     if rank != 0:
@@ -221,8 +323,7 @@ def run_reference(args):
     # the same workload (grid size and generator); each step about 1.5 s on 16 threads
     sample = args.size
     hp = H.HydroParams(gamma=5.0 / 3.0, cfl=0.4, dual=True, riemann=RIEMANN[args.riemann])
-    sys.path.insert(0, str(REPO / "oracle"))
-    import oracle as O
+    O = cpu_build("native")
     g = H.Grid.uniform((sample,) * 3)
     f = H.turbulence(g, hp, mach=3.0, seed=args.seed)
     for k, frac in enumerate(colour_fractions(args.colours)):
@@ -248,7 +349,8 @@ def run_reference(args):
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": nthreads, "kind": "port",
                          "sample": f"{sample}^3 turbulence, {args.steps} SolvePPM_DE steps, "
                                    f"OpenMP over slices, {nthreads} threads; C restatement of "
-                                   "the Fortran (no Fortran compiler on the box)"},
+                                   "the Fortran (no Fortran compiler on the box), gcc -O3 "
+                                   "-march=native -ffp-contract=off"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -560,10 +662,16 @@ def run_ours(args):
         rate, secs, nst = cpu_reference_rate(args.size, args.seed, nthreads,
                                              colours=args.colours,
                                              riemann=RIEMANN[args.riemann])
+        rate_fma, secs_fma, nst_fma = cpu_reference_rate(
+            args.size, args.seed, nthreads, min_seconds=4.0, max_steps=4,
+            colours=args.colours, riemann=RIEMANN[args.riemann], kind="native_fma")
         cpu = {"value": rate, "unit": UNIT, "cores": nthreads, "kind": "port",
                "sample": f"the same {args.size}^3 turbulence workload, {nst} SolvePPM_DE "
                          f"steps, {nthreads} threads ({secs:.1f} s); C restatement of the "
-                         f"Fortran path"}
+                         f"Fortran path, gcc -O3 -march=native -ffp-contract=off",
+               "contraction_allowed": {"value": rate_fma, "steps": nst_fma,
+                                       "build": "gcc -O3 -march=native -ffp-contract=fast"},
+               "cpu_model": cpu_model()}
 
     if rank == 0:
         line = {
@@ -589,6 +697,8 @@ def run_ours(args):
 
 def main():
     args = parse()
+    if args.cpu_table:
+        return run_cpu_table(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

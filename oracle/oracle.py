@@ -91,20 +91,40 @@ class OraStats(C.Structure):
 
 
 _lib = None
+_kind = "parity"
+_loaded = {}
+# builds of the same source: "parity" is the checker (-O2, no contraction); "native"
+# (-O3 -march=native, no contraction: the same bits) and "native_fma" (-O3
+# -march=native, contraction allowed) are the timed CPU baselines, built by `make
+# native` on the machine that runs them
+BUILDS = {"parity": LIB_PATH, "native": HERE / "_build" / "libppm_oracle_native.so",
+          "native_fma": HERE / "_build" / "libppm_oracle_native_fma.so"}
 
 
-def build() -> Path:
+def build(kind: str = "parity") -> Path:
     """Compile the oracle (make in oracle/)."""
-    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
-    return LIB_PATH
+    target = [] if kind == "parity" else ["native"]
+    subprocess.run(["make", "-s", "-C", str(HERE), *target], check=True)
+    return BUILDS[kind]
+
+
+def select(kind: str) -> None:
+    """Make later calls use the given build ("parity", "native" or "native_fma")."""
+    global _lib, _kind
+    if kind not in BUILDS:
+        raise ValueError(kind)
+    if kind != _kind:
+        _kind = kind
+        _lib = _loaded.get(kind)
 
 
 def lib():
     global _lib
     if _lib is None:
-        if not LIB_PATH.exists():
-            build()
-        L = C.CDLL(str(LIB_PATH))
+        path = BUILDS[_kind]
+        if not path.exists():
+            build(_kind)
+        L = C.CDLL(str(path))
         dp = C.POINTER(C.c_double)
         L.ora_solve_ppm_de.argtypes = [C.POINTER(OraParams), C.c_int, C.c_void_p, dp * 3, dp * 3,
                                        C.c_int, C.POINTER(OraFluxes), C.c_longlong * 3,
@@ -135,6 +155,7 @@ def lib():
                                                   C.c_int * 3]
         L.ora_correct_fluxes_sublings.restype = C.c_int
         _lib = L
+        _loaded[_kind] = L
     return _lib
 
 
