@@ -2,13 +2,22 @@
 //
 // Each function is one stencil point of a reference Fortran loop, written with the
 // reference's operand order (left-to-right association, x**2 = x*x, x**3 = (x*x)*x,
-// MAX/MIN as a compare-select).  The library is compiled with -fmad=false, so every
-// product and sum is rounded separately, and CUDA's FP64 '/' and sqrt are IEEE
-// correctly rounded: the results are bit-identical to a plain x86-64 build of the
-// same expressions.  The sweep kernels (ppm_split.cu) only schedule these points.
+// MAX/MIN as a compare-select).  The exact build of the library is compiled with
+// -fmad=false, so every product and sum is rounded separately, and CUDA's FP64 '/' and
+// sqrt are IEEE correctly rounded: the results are bit-identical to a plain x86-64
+// build of the same expressions.  The tolerance-mode build (-fmad=true,
+// PPM_FAST_ALGEBRA) fuses multiply-adds and shares a few divisions; its results are
+// held to the oracle within a stated tolerance instead.  The sweep kernels
+// (ppm_split.cu) only schedule these points.
 #pragma once
 
 #include <cstdint>
+
+// PPM_FAST_ALGEBRA (the tolerance-mode build): a few quotients with a shared divisor
+// are formed from one reciprocal; everything else is the reference's expression.
+#ifndef PPM_FAST_ALGEBRA
+#define PPM_FAST_ALGEBRA 0
+#endif
 
 namespace ppm {
 
@@ -316,14 +325,26 @@ __device__ __forceinline__ CoreState face_core(const CoreL& L, const CoreR& R, d
   }
   if (DUAL) {
     double ml = dmax(dmax(fabs(L.cm), fabs(L.c0)), fabs(L.cp));
-    if (P.gamma * L.pla / L.dla < P.eta2 * (L.ula * L.ula) || ml < 1.0e-3 ||
-        s.dl / L.dla > 5.0) {
+#if PPM_FAST_ALGEBRA  // tolerance mode: the quotients by dla, dra from their reciprocals
+    const bool ovl = P.gamma * L.pla * ydla < P.eta2 * (L.ula * L.ula) || ml < 1.0e-3 ||
+                     s.dl * ydla > 5.0;
+#else
+    const bool ovl = P.gamma * L.pla / L.dla < P.eta2 * (L.ula * L.ula) || ml < 1.0e-3 ||
+                     s.dl / L.dla > 5.0;
+#endif
+    if (ovl) {
       s.pl = L.pla; s.ul = L.ula; s.dl = L.dla;
       if (CX) cx->ovl = true;
     }
     double mr = dmax(dmax(fabs(R.cm), fabs(R.c0)), fabs(R.cp));
-    if (P.gamma * R.pra / R.dra < P.eta2 * (R.ura * R.ura) || mr < 1.0e-3 ||
-        s.dr / R.dra > 5.0) {
+#if PPM_FAST_ALGEBRA
+    const bool ovr = P.gamma * R.pra * ydra < P.eta2 * (R.ura * R.ura) || mr < 1.0e-3 ||
+                     s.dr * ydra > 5.0;
+#else
+    const bool ovr = P.gamma * R.pra / R.dra < P.eta2 * (R.ura * R.ura) || mr < 1.0e-3 ||
+                     s.dr / R.dra > 5.0;
+#endif
+    if (ovr) {
       s.pr = R.pra; s.ur = R.ura; s.dr = R.dra;
       if (CX) cx->ovr = true;
     }
@@ -372,6 +393,34 @@ __device__ __forceinline__ Riemann twoshock_newton(const FaceState& s, double cl
   double old_ps = ps, ubl = 0.0, ubr = 0.0, dpdul = 0.0, dpdur = 0.0;
   int it = 0;
   bool active = true;
+#if PPM_FAST_ALGEBRA
+  // Tolerance-mode build: the same Newton update with the face's reciprocals 1/pl, 1/pr,
+  // 1/dl, 1/dr formed once, each pair of quotients with different divisors sharing one
+  // division (a/x, b/y = a*y*q, b*x*q with q = 1/(x*y)), and the convergence test as
+  // |dp| < tolerance * ps: three divisions per update instead of twelve.
+  const double ipl = 1.0 / s.pl, ipr = 1.0 / s.pr, idl = 1.0 / s.dl, idr = 1.0 / s.dr;
+#pragma unroll 1
+  for (int n = 2; n <= kNumIter; n++) {
+    if (active) {
+      const double zl = cl * sqrt((1.0 + P.qa * (ps * ipl - 1.0)));
+      const double zr = cr * sqrt((1.0 + P.qa * (ps * ipr - 1.0)));
+      const double qz = 1.0 / (zl * zr);
+      ubl = s.ul - (ps - s.pl) * (zr * qz);
+      ubr = s.ur + (ps - s.pr) * (zl * qz);
+      const double al = 4.0 * (zl * zl) * idl, ar = 4.0 * (zr * zr) * idr;
+      const double dl = al - P.gp1 * (ps - s.pl), dr = ar - P.gp1 * (ps - s.pr);
+      const double qd = 1.0 / (dl * dr);
+      dpdul = -(zl * al * (dr * qd));
+      dpdur = zr * ar * (dl * qd);
+      ps = ps + (ubr - ubl) * dpdur * dpdul / (dpdur - dpdul);
+      if (ps < P.pmin) ps = P.pmin;
+      const double delta_ps = ps - old_ps;
+      old_ps = ps;
+      it++;
+      if (fabs(delta_ps) < kTolerance * ps) active = false;
+    }
+  }
+#else
 #pragma unroll 1
   for (int n = 2; n <= kNumIter; n++) {
     if (active) {
@@ -389,6 +438,7 @@ __device__ __forceinline__ Riemann twoshock_newton(const FaceState& s, double cl
       if (fabs(delta_ps / ps) < kTolerance) active = false;
     }
   }
+#endif
   Riemann r;
   if (ps < P.pmin) ps = dmin(s.pl, s.pr);
   r.pbar = ps;
@@ -417,6 +467,23 @@ __device__ __forceinline__ Flux flux_twoshock(const FaceState& s, double pbar, d
   } else {
     u0 = s.ur; p0 = s.pr; d0 = s.dr;
   }
+#if PPM_FAST_ALGEBRA
+  // tolerance mode: 1/d0 once, and gamma*pbar/dbar as gamma*pbar*(1/dbar)
+  const double id0 = 1.0 / d0;
+  double c0 = sqrt(dmax(gamma * p0 * id0, kTiny));
+  double z0 = c0 * d0 * sqrt(dmax(1.0 + P.qa * (pbar / p0 - 1.0), kTiny));
+  const double idbar = id0 - (pbar - p0) / dmax(z0 * z0, kTiny);
+  double dbar = 1.0 / idbar;
+  double cbar = sqrt(dmax(gamma * pbar * idbar, kTiny));
+  double l0, lbar;
+  if (pbar < p0) {
+    l0 = u0 * sn + c0;
+    lbar = sn * ubar + cbar;
+  } else {
+    l0 = u0 * sn + z0 * id0;
+    lbar = l0;
+  }
+#else
   double c0 = sqrt(dmax(gamma * p0 / d0, kTiny));
   double z0 = c0 * d0 * sqrt(dmax(1.0 + P.qa * (pbar / p0 - 1.0), kTiny));
   double dbar = 1.0 / (1.0 / d0 - (pbar - p0) / dmax(z0 * z0, kTiny));
@@ -429,6 +496,7 @@ __device__ __forceinline__ Flux flux_twoshock(const FaceState& s, double pbar, d
     l0 = u0 * sn + z0 / d0;
     lbar = l0;
   }
+#endif
   double frac = l0 - lbar;
   if (frac < kTiny) frac = kTiny;
   frac = (0.0 - lbar) / frac;

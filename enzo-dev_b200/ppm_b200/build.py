@@ -1,10 +1,15 @@
-"""Builds libppm_b200.so (sm_100a) in-tree with nvcc.
+"""Builds the library (sm_100a) in-tree with nvcc, in two variants of the same sources.
 
-    python -m ppm_b200.build        (from enzo-dev_b200/)
+    python -m ppm_b200.build [--force] [-v]        (from enzo-dev_b200/)
 
-FP64 parity with the reference's arithmetic needs every multiply and add rounded
-separately: -fmad=false for device code and -ffp-contract=off for host code
-(the host builds the inteuler coefficient tables).
+- "exact": _build/libppm_b200.so.  Bit-identical to the FP64 oracle: every multiply
+  and add rounded separately (-fmad=false for device code, -ffp-contract=off for host
+  code, which builds the inteuler coefficient tables) and the reference's divisions
+  as written.
+- "fast": _build/libppm_b200_fast.so.  Fused multiply-adds (-fmad=true) and, where one
+  divisor serves several quotients, one reciprocal and multiplications
+  (PPM_FAST_ALGEBRA): the same algorithm, not the same bits, held to the tolerance
+  bar of 1e-12 relative after one step and 1e-10 after 100 steps against the oracle.
 """
 from __future__ import annotations
 
@@ -24,8 +29,19 @@ INCLUDE = REPO / "include"
 
 SOURCES = ["ppm_kernels.cu", "ppm_split.cu", "ppm_capi.cu", "ppm_noalloc.cu", "ppm_mlp.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-fmad=false",
-              "-Xcompiler", "-fPIC,-ffp-contract=off", "--expt-relaxed-constexpr"]
+# -fno-gnu-unique and the version script keep every symbol but the C ABI local to its
+# library: both variants can be loaded in one process without one's template statics
+# (gnu_unique objects, which the dynamic linker otherwise unifies process-wide) or
+# functions standing in for the other's.
+NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17",
+              "-Xcompiler", "-fPIC,-ffp-contract=off,-fno-gnu-unique",
+              "--expt-relaxed-constexpr"]
+EXPORTS_MAP = CSRC / "exports.map"
+VARIANTS = {
+    "exact": {"lib": LIB, "obj": OUT_DIR, "flags": ["-fmad=false"]},
+    "fast": {"lib": OUT_DIR / "libppm_b200_fast.so", "obj": OUT_DIR / "fast",
+             "flags": ["-fmad=true", "-DPPM_FAST_ALGEBRA=1"]},
+}
 
 
 def nvcc() -> str:
@@ -33,38 +49,47 @@ def nvcc() -> str:
     return cand
 
 
-def needs_build() -> bool:
-    if not LIB.exists():
+def needs_build(variant: str = "exact") -> bool:
+    lib = VARIANTS[variant]["lib"]
+    if not lib.exists():
         return True
-    t = LIB.stat().st_mtime
-    deps = list(CSRC.glob("*.cu")) + list(CSRC.glob("*.cuh")) + list(INCLUDE.glob("*.h"))
+    t = lib.stat().st_mtime
+    deps = (list(CSRC.glob("*.cu")) + list(CSRC.glob("*.cuh")) + list(INCLUDE.glob("*.h"))
+            + [Path(__file__)])
     return any(p.stat().st_mtime > t for p in deps)
 
 
-def build(force: bool = False, verbose: bool = False) -> Path:
-    if not force and not needs_build():
-        return LIB
-    OUT_DIR.mkdir(parents=True, exist_ok=True)
+def build(force: bool = False, verbose: bool = False, variant: str = "exact") -> Path:
+    v = VARIANTS[variant]
+    lib, obj_dir = v["lib"], v["obj"]
+    if not force and not needs_build(variant):
+        return lib
+    obj_dir.mkdir(parents=True, exist_ok=True)
     headers = list(CSRC.glob("*.cuh")) + list(INCLUDE.glob("*.h"))
     newest_header = max(p.stat().st_mtime for p in headers)
     objs = []
     for src in SOURCES:
-        obj = OUT_DIR / (Path(src).stem + ".o")
+        obj = obj_dir / (Path(src).stem + ".o")
         stale = (force or not obj.exists() or obj.stat().st_mtime < newest_header
                  or obj.stat().st_mtime < (CSRC / src).stat().st_mtime)
         if stale:
-            cmd = [nvcc(), *ARCH, *NVCC_FLAGS, "-I", str(INCLUDE), "-I", str(CSRC),
+            cmd = [nvcc(), *ARCH, *NVCC_FLAGS, *v["flags"], "-I", str(INCLUDE), "-I", str(CSRC),
                    "-c", str(CSRC / src), "-o", str(obj)]
             if verbose:
                 cmd += ["-Xptxas", "-v"]
             subprocess.run(cmd, check=True)
         objs.append(str(obj))
-    tmp = LIB.with_suffix(".so.tmp")
-    subprocess.run([nvcc(), *ARCH, "-shared", "-o", str(tmp), *objs, "-lcudart"], check=True)
-    os.replace(tmp, LIB)
-    return LIB
+    tmp = lib.with_suffix(".so.tmp")
+    subprocess.run([nvcc(), *ARCH, "-shared", "-o", str(tmp), *objs, "-lcudart",
+                    "-Xlinker", f"--version-script={EXPORTS_MAP}"], check=True)
+    os.replace(tmp, lib)
+    return lib
+
+
+def build_all(force: bool = False, verbose: bool = False) -> list:
+    return [build(force, verbose, name) for name in VARIANTS]
 
 
 if __name__ == "__main__":
-    build(force="--force" in sys.argv, verbose="-v" in sys.argv)
-    print(LIB)
+    for path in build_all(force="--force" in sys.argv, verbose="-v" in sys.argv):
+        print(path)

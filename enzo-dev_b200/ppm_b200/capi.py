@@ -108,25 +108,39 @@ class PPMError(RuntimeError):
         super().__init__(f"{what}: ppm_b200 error {code} ({error_string(code)})")
 
 
-_lib = None
+_libs = {}
 
 
-def library_path() -> Path:
-    """libppm_b200.so to load: $PPM_B200_LIB when set, else the in-tree build."""
+def default_variant() -> str:
+    """The build variant loaded when none is named: $PPM_B200_VARIANT, else "exact"
+    (bit-identical to the oracle); "fast" is the tolerance-mode build."""
+    v = os.environ.get("PPM_B200_VARIANT", "exact")
+    if v not in _build.VARIANTS:
+        raise ValueError(f"PPM_B200_VARIANT={v!r}: expected one of {sorted(_build.VARIANTS)}")
+    return v
+
+
+def library_path(variant: str | None = None) -> Path:
+    """The shared library of a build variant: $PPM_B200_LIB overrides the exact build's
+    path, otherwise the in-tree build."""
+    variant = variant or default_variant()
     env = os.environ.get("PPM_B200_LIB")
-    return Path(env) if env else _build.LIB
+    if env and variant == "exact":
+        return Path(env)
+    return _build.VARIANTS[variant]["lib"]
 
 
-def lib(build_if_missing: bool = True):
-    """Load libppm_b200.so (building it when missing and nvcc is available)."""
-    global _lib
-    if _lib is not None:
-        return _lib
-    path = library_path()
+def lib(build_if_missing: bool = True, variant: str | None = None):
+    """Load the library of a build variant (building it when missing and nvcc is
+    available).  Each variant is its own handle; both can be loaded at once."""
+    variant = variant or default_variant()
+    if variant in _libs:
+        return _libs[variant]
+    path = library_path(variant)
     if not path.exists():
-        if not build_if_missing or path != _build.LIB:
+        if not build_if_missing or path != _build.VARIANTS[variant]["lib"]:
             raise RuntimeError(f"{path} is missing; run python -m ppm_b200.build")
-        _build.build()
+        _build.build(variant=variant)
     L = C.CDLL(str(path))
     vp = C.c_void_p
     L.ppm_b200_create.argtypes = [C.c_int, vp, C.POINTER(vp)]
@@ -199,7 +213,7 @@ def lib(build_if_missing: bool = True):
         fn = getattr(L, name)
         if name not in ("ppm_b200_launch_count", "ppm_b200_error_string"):
             fn.restype = C.c_int
-    _lib = L
+    _libs[variant] = L
     return L
 
 
@@ -333,8 +347,9 @@ def euler_sweep_static(dim, grid, hp, dt, fields_in, pressure, fields_out, strea
 class Context:
     """One ppm_b200_context (one per rank / device)."""
 
-    def __init__(self, device: int = 0, stream=None):
-        self.L = lib()
+    def __init__(self, device: int = 0, stream=None, variant: str | None = None):
+        self.variant = variant or default_variant()
+        self.L = lib(variant=self.variant)
         h = C.c_void_p()
         rc = self.L.ppm_b200_create(int(device), stream, C.byref(h))
         if rc != OK:

@@ -251,7 +251,7 @@ def sweep(dim, grid, hp, dt, fields, pressure, cellwidth, accel=None, nthreads=1
     acc = (C.POINTER(C.c_double) * 3)()
     if accel is not None:
         for d in range(3):
-            acc[d] = _ptr(accel[d])
+            acc[d] = _ptr(accel[d] if d < len(accel) else None)
     st = OraStats()
     g = (C.c_longlong * 3)(0, 0, 0)
     rc = L.ora_sweep(int(dim), C.byref(P), F, _ptr(pressure), acc,

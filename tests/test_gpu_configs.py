@@ -14,10 +14,12 @@ their generators at a size the oracle finishes in seconds:
 - the 600-patch AMR level of the benchmark (edges log-uniform in 16-128, Sedov blasts
   and turbulence crops), one batched level step against the oracle patch by patch.
 
-The library is built so that both sides evaluate the same expressions in the same
-order (-fmad=false, IEEE division and square root), so every comparison is also
-required to be bit-identical.  With PPM_B200_REPORT_DIR set, the per-field errors at
-step 1 and step 100 and the conservation figures are written there as JSON.
+Every case runs with both builds of the library.  The exact build evaluates the same
+expressions in the same order as the oracle (-fmad=false, IEEE division and square
+root), so its comparisons are also required to be bit-identical; the tolerance-mode
+build (fused multiply-adds, shared reciprocals) is held to the bar alone.  With
+PPM_B200_REPORT_DIR set, the per-field errors at step 1 and step 100 and the
+conservation figures are written there as JSON.
 """
 import json
 import math
@@ -56,9 +58,9 @@ def torch():
     return t
 
 
-@pytest.fixture(scope="module")
-def ctx(torch):
-    c = capi.Context(0)
+@pytest.fixture(scope="module", params=["exact", "fast"])
+def ctx(torch, request):
+    c = capi.Context(0, variant=request.param)
     yield c
     c.close()
 
@@ -71,11 +73,12 @@ def _host(f):
     return {k: v.cpu().numpy() for k, v in f.items()}
 
 
-def _check(a, b, g, tol, what):
+def _check(a, b, g, tol, what, bitexact):
     cmp = compare(a, b, g)
     for k, r in cmp.items():
         assert r["maxrel"] <= tol, (what, k, r)
-        assert r["bitexact"], (what, k, r)
+        if bitexact:
+            assert r["bitexact"], (what, k, r)
     return {k: r["maxrel"] for k, r in cmp.items()}
 
 
@@ -108,7 +111,7 @@ def _run_steps(ctx, torch, g, hp, f0, nsteps, bc, name):
         rc, _ = ctx.synchronize()
         assert rc == capi.OK, (name, cyc, capi.error_string(rc))
         tol = TOL_1STEP if cyc == 0 else TOL_100STEP
-        e = _check(_host(f_gpu), f_ora, g, tol, (name, cyc + 1))
+        e = _check(_host(f_gpu), f_ora, g, tol, (name, cyc + 1), ctx.variant == "exact")
         if cyc == 0 or cyc == nsteps - 1:
             errs[f"step {cyc + 1}"] = e
     return f_ora, _host(f_gpu), errs
@@ -125,7 +128,7 @@ def test_sod_64cubed_100_steps(ctx, torch):
     for k in ("d", "te", "v1"):
         a = f_gpu[k][act]
         assert np.array_equal(a, np.broadcast_to(a[:1, :1, :], a.shape)), k
-    _report("sod 64^3 gamma 1.4 CFL 0.4 outflow dual, 100 steps: max rel error", errs)
+    _report(f"{ctx.variant} build: sod 64^3 gamma 1.4 CFL 0.4 outflow dual, 100 steps: max rel error", errs)
 
 
 def test_turbulence_256cubed_one_step(ctx, torch):
@@ -133,7 +136,7 @@ def test_turbulence_256cubed_one_step(ctx, torch):
     g = H.Grid.uniform((256, 256, 256))
     f0 = H.turbulence(g, hp, mach=3.0, seed=20240611)  # the benchmark's state
     _, _, errs = _run_steps(ctx, torch, g, hp, f0, 1, "periodic", "turb256")
-    _report("turbulence 256^3 Mach 3 dual, 1 step: max rel error", errs)
+    _report(f"{ctx.variant} build: turbulence 256^3 Mach 3 dual, 1 step: max rel error", errs)
 
 
 @pytest.mark.parametrize("dual", [True, False])
@@ -156,8 +159,8 @@ def test_turbulence_64cubed_100_steps_conserves(ctx, torch, dual):
             # momentum scale, sum |rho v|
             scale = math.fsum(np.abs(f0["d"] * f0[k.split("_")[1]])[g.active_slices()].ravel())
             assert abs(t1[k] - t0[k]) <= TOL_CONSERVED * scale, (k, t0[k], t1[k])
-    _report(f"turbulence 64^3 Mach 3 dual={dual}, 100 steps: max rel error", errs)
-    _report(f"turbulence 64^3 Mach 3 dual={dual}, 100 steps: relative drift of totals", drift)
+    _report(f"{ctx.variant} build: turbulence 64^3 Mach 3 dual={dual}, 100 steps: max rel error", errs)
+    _report(f"{ctx.variant} build: turbulence 64^3 Mach 3 dual={dual}, 100 steps: relative drift of totals", drift)
 
 
 def test_amr_level_600_patches_one_step(ctx, torch):
@@ -172,8 +175,47 @@ def test_amr_level_600_patches_one_step(ctx, torch):
     for k, (g, f) in enumerate(zip(grids, host)):
         rc, _ = O.solve_ppm_de(g, hp, dt, 0, f, g.cellwidth, nthreads=NTHREADS)
         assert rc == 0, k
-        e = _check(_host(dev[k]), f, g, TOL_1STEP, ("level patch", k))
+        e = _check(_host(dev[k]), f, g, TOL_1STEP, ("level patch", k), ctx.variant == "exact")
         for name, v in e.items():
             worst[name] = max(worst.get(name, 0.0), v)
         dev[k] = None
-    _report("600-patch level, 1 batched step: max rel error over patches", worst)
+    _report(f"{ctx.variant} build: 600-patch level, 1 batched step: max rel error over patches", worst)
+
+
+@pytest.mark.parametrize("shape,dual,grav,seed", [
+    ((16, 16, 16), True, True, 1),
+    ((20, 12, 9), False, False, 2),
+    ((24, 20), True, True, 4),
+    ((60,), True, False, 6),
+])
+def test_random_grids_with_gravity_100_steps(ctx, torch, shape, dual, grav, seed):
+    # ranks 1-3 with the gravity source terms: 100 steps of a smooth-plus-noise state,
+    # each compared with the oracle
+    from parity_util import random_state
+    hp = H.HydroParams(gamma=5.0 / 3.0, cfl=0.5, dual=dual, gravity=grav)
+    g = H.Grid.uniform(shape)
+    f_ora = random_state(g, hp, seed=seed)
+    f_gpu = _dev(f_ora, torch)
+    accel = None
+    if grav:
+        rng = np.random.default_rng(seed + 100)
+        accel = [0.1 * rng.standard_normal(g.shape) for _ in range(g.rank)]
+    acc_d = [torch.from_numpy(a).cuda() for a in accel] if accel else None
+    errs = {}
+    for cyc in range(100):
+        p = O.compute_pressure(g, hp, f_ora)
+        dt = hp.cfl * O.calc_dt(g, hp, f_ora, p, g.cellwidth)
+        rc, _ = O.solve_ppm_de(g, hp, dt, cyc, f_ora, g.cellwidth, accel=accel)
+        assert rc == 0
+        ctx.solve_ppm_de(g, hp, dt, cyc, f_gpu, memory=capi.MEM_DEVICE, accel=acc_d,
+                         want_stats=False)
+        H.fill_ghosts(g, f_ora, "periodic")
+        ctx.set_boundary(g, f_gpu, hp.dual, ("periodic",) * 3)
+        rc, _ = ctx.synchronize()  # the context's stream has finished before reading
+        assert rc == capi.OK, (shape, cyc, capi.error_string(rc))
+        tol = TOL_1STEP if cyc == 0 else TOL_100STEP
+        e = _check(_host(f_gpu), f_ora, g, tol, (shape, cyc + 1), ctx.variant == "exact")
+        if cyc in (0, 99):
+            errs[f"step {cyc + 1}"] = e
+    _report(f"{ctx.variant} build: random grid {shape} dual={dual} gravity={grav}, "
+            "100 steps: max rel error", errs)
