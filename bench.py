@@ -67,7 +67,9 @@ def parse():
                     help="skip the batched AMR-level measurement")
     ap.add_argument("--level-patches", type=int, default=600)
     ap.add_argument("--no-learned", action="store_true",
-                    help="skip the learned-Newton-start comparison")
+                    help="skip the learned-Newton-start comparisons")
+    ap.add_argument("--config4-size", type=int, default=512,
+                    help="grid of the learned-start configuration (Mach-10 turbulence)")
     ap.add_argument("--riemann", choices=list(RIEMANN), default="twoshock",
                     help="RiemannSolver of the workload (two-shock is the PPM default and "
                          "the headline)")
@@ -362,9 +364,11 @@ def run_reference(args):
 
 
 # ---------------------------------------------------------------- learned Newton start
-def run_learned(ctx, g, hp, f_host, args, stream):
-    """Plain vs learned starting pressure of the Newton iteration on the bench workload:
-    zone-updates/s (event-timed), Newton iterations per interface, the Riemann kernel's
+def run_learned(ctx, g, hp, f_host, args, stream, f_dev=None, steps=None):
+    """Plain vs learned starting pressure of the Newton iteration on one workload (host
+    fields f_host, or device fields f_dev): zone-updates/s (event-timed), Newton updates
+    per interface and per warp (the most any lane of a Riemann warp took, which is what
+    the divergent loop costs), faces that took 5 or more updates, the Riemann kernel's
     time per sweep, and the largest relative field difference after the steps."""
     import torch
     from ppm_b200 import capi
@@ -372,11 +376,14 @@ def run_learned(ctx, g, hp, f_host, args, stream):
 
     ctx.set_guess(LRN.default_weights())
     dev = torch.device("cuda", torch.cuda.current_device())
-    steps = max(1, min(args.steps, 5))
+    steps = steps or max(1, min(args.steps, 5))
     out = {"steps": steps, "warmup": 2}
     finals = {}
     for mode in ("plain", "learned"):
-        f = {k: torch.from_numpy(v).to(dev) for k, v in f_host.items()}
+        if f_dev is not None:
+            f = {k: v.clone() for k, v in f_dev.items()}
+        else:
+            f = {k: torch.from_numpy(v).to(dev) for k, v in f_host.items()}
         dtd = torch.zeros(1, dtype=torch.float64, device=dev)
         torch.cuda.synchronize()
 
@@ -407,6 +414,8 @@ def run_learned(ctx, g, hp, f_host, args, stream):
         ms = ev0.elapsed_time(ev1) / steps
         out[mode] = {"ms_per_step": ms, "zone_updates_per_s": g.active_cells / (ms * 1e-3),
                      "newton_per_interface": st["newton_iters"] / max(st["interfaces"], 1),
+                     "newton_per_warp": st["warp_newton_iters"] / max(st["warps"], 1),
+                     "faces_5plus_updates": int(sum(st["newton_hist"][5:])),
                      "riemann_ms_per_sweep": stages["riemann"] / max(nsweep, 1),
                      "guess_rejected": st["guess_rejected"]}
         finals[mode] = f
@@ -420,6 +429,23 @@ def run_learned(ctx, g, hp, f_host, args, stream):
     out["speedup_learned_vs_plain"] = (out["learned"]["zone_updates_per_s"] /
                                        out["plain"]["zone_updates_per_s"])
     del finals
+    torch.cuda.empty_cache()
+    return out
+
+
+def run_config4(ctx, args, stream):
+    """The learned-guess configuration: 512^3 periodic Mach-10 decaying turbulence (the
+    benchmark's generator at rms Mach 10, produced on the device), FP64 hydro with dual
+    energy, plain vs learned Newton start."""
+    import torch
+    n = args.config4_size
+    hp = H.HydroParams(gamma=5.0 / 3.0, cfl=0.4, dual=True)
+    g = H.Grid.uniform((n, n, n))
+    f_dev = H.turbulence_device(g, hp, mach=10.0, seed=args.seed + 4)
+    out = run_learned(ctx, g, hp, None, args, stream, f_dev=f_dev, steps=3)
+    out["workload"] = (f"decaying turbulence {n}^3 periodic (+3 ghosts), rms Mach 10, gamma 5/3, "
+                       "dual energy, FP64, seeded device-side generator")
+    del f_dev
     torch.cuda.empty_cache()
     return out
 
@@ -761,8 +787,10 @@ def run_ours(args):
 
     # the learned Newton start on the same workload (same state, a few steps each way)
     learned = None
+    config4 = None
     if world == 1 and not args.no_learned and args.riemann == "twoshock":
         learned = run_learned(ctx, g, hp, f_host, args, stream)
+        config4 = run_config4(ctx, args, stream)
 
     level = None
     if world == 1 and not args.no_level:
@@ -818,6 +846,7 @@ def run_ours(args):
             "hll_fallbacks": st["fallbacks"],
             "amr_level": level,
             "learned_start": learned,
+            "learned_start_mach10": config4,
         }
         print(json.dumps(line), flush=True)
     ctx.close()

@@ -923,6 +923,8 @@ int read_counters(ppm_b200_context* ctx, ppm_b200_stats* st, int* status) {
     st->fallbacks += (long long)c[ppm::kCntFallbacks];
     st->fatal_cells += (long long)c[ppm::kCntFatal];
     st->guess_rejected += (long long)c[ppm::kCntGuessRejected];
+    st->warp_newton_iters += (long long)c[ppm::kCntWarpNewton];
+    st->warps += (long long)c[ppm::kCntWarps];
   }
   int s = PPM_B200_OK;
   if (c[ppm::kCntTimeout]) s = PPM_B200_ERR_TIMEOUT;

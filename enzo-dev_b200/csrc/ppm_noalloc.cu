@@ -60,6 +60,7 @@ constexpr size_t kStaticBytes =
     kStaticCounterBytes + kStaticCoefBytes + kStaticDescBytes + kStaticPlaneBytes;
 static_assert(kStaticCoefEntries * sizeof(ppm::Coef) <= kStaticCoefBytes, "coef area");
 static_assert(sizeof(ppm::SweepArgs) <= 512, "descriptor area");
+static_assert(ppm::kMaxCounters * sizeof(unsigned long long) <= kStaticCounterBytes, "counters");
 
 constexpr int kMaxDevices = 64;
 
@@ -285,6 +286,8 @@ extern "C" int ppm_b200_euler_sweep_static(int dim, const ppm_b200_params* p,
     for (int h = 0; h < 8; ++h) stats->newton_hist[h] += (long long)c[ppm::kCntHist0 + h];
     stats->fallbacks += (long long)c[ppm::kCntFallbacks];
     stats->fatal_cells += (long long)c[ppm::kCntFatal];
+    stats->warp_newton_iters += (long long)c[ppm::kCntWarpNewton];
+    stats->warps += (long long)c[ppm::kCntWarps];
   }
   if (c[ppm::kCntTimeout]) return PPM_B200_ERR_TIMEOUT;
   if (c[ppm::kCntFatal]) return PPM_B200_ERR_NEGATIVE;

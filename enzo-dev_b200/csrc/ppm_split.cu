@@ -426,10 +426,13 @@ __global__ void __launch_bounds__(kRiemannThreads, LEARNED ? PPM_RIEMANN_LEARNED
   __shared__ unsigned int s_hist[8];
   __shared__ unsigned int s_newton;
   __shared__ unsigned int s_rejected;
+  __shared__ unsigned int s_wtrips, s_warps;
   if (threadIdx.x < 8) s_hist[threadIdx.x] = 0u;
   if (threadIdx.x == 0) {
     s_newton = 0u;
     s_rejected = 0u;
+    s_wtrips = 0u;
+    s_warps = 0u;
   }
   int64_t lb;
   const int g = locate<ONE>(B.riemann_prefix, B.ngrids, lb);
@@ -461,6 +464,7 @@ __global__ void __launch_bounds__(kRiemannThreads, LEARNED ? PPM_RIEMANN_LEARNED
     // jumps are all weak keeps the acoustic start, which is then within ~|x|^2 of p*
     if (__any_sync(0xffffffffu, d2 > kGuessMinJump)) y = guess_mlp_warp(a.guess, f);
   }
+  unsigned trips = 0;  // Newton updates of this lane's face (both starts when rejected)
   if (valid) {
     const double cl = sqrt(P.gamma * s.pl * s.dl);
     const double cr = sqrt(P.gamma * s.pr * s.dr);
@@ -507,6 +511,15 @@ __global__ void __launch_bounds__(kRiemannThreads, LEARNED ? PPM_RIEMANN_LEARNED
     o[XUB * pl] = F.ub;
     atomicAdd(&s_hist[rs.iters & 7], 1u);
     atomicAdd(&s_newton, (unsigned)rs.iters + spent);
+    trips = (unsigned)rs.iters + spent;
+  }
+  {  // what the warp pays for its divergent Newton loop: the most updates of any lane
+    const unsigned wmax = __reduce_max_sync(0xffffffffu, trips);
+    const unsigned any = __ballot_sync(0xffffffffu, valid);
+    if ((threadIdx.x & 31) == 0 && any) {
+      atomicAdd(&s_wtrips, wmax);
+      atomicAdd(&s_warps, 1u);
+    }
   }
   __syncthreads();
   if (threadIdx.x < 8 && s_hist[threadIdx.x])
@@ -519,6 +532,10 @@ __global__ void __launch_bounds__(kRiemannThreads, LEARNED ? PPM_RIEMANN_LEARNED
   }
   if (LEARNED && threadIdx.x == 9 && s_rejected)
     atomicAdd(&B.counters[kCntGuessRejected], (unsigned long long)s_rejected);
+  if (threadIdx.x == 10 && s_warps) {
+    atomicAdd(&B.counters[kCntWarpNewton], (unsigned long long)s_wtrips);
+    atomicAdd(&B.counters[kCntWarps], (unsigned long long)s_warps);
+  }
 }
 
 // PressureFree with the two-shock solver: no Riemann problem, p* = pmin, u* the mean of

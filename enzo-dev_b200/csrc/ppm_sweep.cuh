@@ -23,7 +23,7 @@ struct FluxCapture {
   int64_t dst;        // base offset (in doubles) of this request in the capture buffer
 };
 
-enum { kMaxCounters = 16 };
+enum { kMaxCounters = 32 };
 // device counters (unsigned long long), see ppm_b200_stats
 enum {
   kCntInterfaces = 0,
@@ -35,6 +35,8 @@ enum {
   kCntNonFinite = 13,
   kCntFlagged = 14,  // pencils handed to the fallback pass (index into BatchArgs::flagged)
   kCntTimeout = 15,  // bounded waits on asynchronous copies that gave up
+  kCntWarpNewton = 16,  // sum over Riemann warps of the most Newton updates any lane took
+  kCntWarps = 17,       // Riemann warps with at least one face
 };
 
 struct SweepArgs {

@@ -92,6 +92,7 @@ class Stats(C.Structure):
         ("interfaces", C.c_longlong), ("newton_iters", C.c_longlong),
         ("newton_hist", C.c_longlong * 8), ("fallbacks", C.c_longlong),
         ("fatal_cells", C.c_longlong), ("guess_rejected", C.c_longlong),
+        ("warp_newton_iters", C.c_longlong), ("warps", C.c_longlong),
     ]
 
     def as_dict(self):
@@ -99,6 +100,7 @@ class Stats(C.Structure):
             "interfaces": int(self.interfaces), "newton_iters": int(self.newton_iters),
             "newton_hist": [int(x) for x in self.newton_hist], "fallbacks": int(self.fallbacks),
             "fatal_cells": int(self.fatal_cells), "guess_rejected": int(self.guess_rejected),
+            "warp_newton_iters": int(self.warp_newton_iters), "warps": int(self.warps),
         }
 
 

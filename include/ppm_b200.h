@@ -152,6 +152,9 @@ typedef struct ppm_b200_stats {
   long long fallbacks;      /* cells recomputed with the HLL fallback */
   long long fatal_cells;    /* cells in a state the reference aborts on */
   long long guess_rejected; /* learned guesses that did not converge (plain guess reused) */
+  long long warp_newton_iters; /* sum over the Riemann kernel's warps of the most Newton
+                               updates any of its lanes took: what the divergent loop costs */
+  long long warps;          /* Riemann warps with at least one interface */
 } ppm_b200_stats;
 
 typedef struct ppm_b200_context ppm_b200_context;
@@ -419,7 +422,7 @@ int ppm_b200_version(void);
   X(offsetof(ppm_b200_fluxes, left)) X(offsetof(ppm_b200_fluxes, right))             \
   X(offsetof(ppm_b200_fluxes, colour_left)) X(offsetof(ppm_b200_fluxes, colour_right)) \
   X(sizeof(ppm_b200_stats)) X(offsetof(ppm_b200_stats, newton_hist))                 \
-  X(offsetof(ppm_b200_stats, guess_rejected))
+  X(offsetof(ppm_b200_stats, guess_rejected)) X(offsetof(ppm_b200_stats, warps))
 int ppm_b200_abi_check(const long long *layout, int n);
 
 #ifdef __cplusplus
