@@ -10,9 +10,11 @@ pressure; seeded synthetic data generated here (no external dataset).
 One step = what Enzo's level-0 cycle does around the hydro call for one grid:
 Courant time step (ComputeTimeStep/calc_dt, on device), grid::SolvePPM_DE
 (pressure + x/y/z sweeps in the cycle-rotated order), ghost-zone fill
-(periodic).  With N GPUs every rank advances its own grid (weak scaling) and the
-time step is the minimum over ranks (one 8-byte NCCL all-reduce, as
-SetLevelTimeStep.C does with MPI).  A zone-update is one active cell advanced
+(periodic).  With N GPUs the grid is N times longer in z and cut into N slabs of
+256^3 active cells (weak scaling): every step the slabs exchange their 3 z ghost
+layers over NCCL and the time step is the minimum over ranks (one 8-byte NCCL
+all-reduce, as SetLevelTimeStep.C does with MPI); the 600-patch AMR level is then
+also spread over the ranks by patch.  A zone-update is one active cell advanced
 through one full split step.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
@@ -475,12 +477,28 @@ def run_level(ctx, args, stream):
     digests = {}
     from ppm_b200 import learned as LRN
     ctx.set_guess(LRN.default_weights())
-    for mode in ("batched_graph", "per_patch_loop", "batched_graph_learned"):
+    default_cfg = ctx.level_config().as_dict()
+    tuning = None
+    bound = 4 << 30  # the bounded-scratch arm: at most 4 GiB of level scratch
+    for mode in ("batched_graph", "per_patch_loop", "per_patch_graph",
+                 "batched_graph_autotuned", "batched_graph_bounded", "batched_graph_learned"):
         f = [{k: torch.from_numpy(v).to(dev) for k, v in fh.items()} for fh in host]
         arr, keep = ctx._level(grids, f)
         P = capi.make_params(hp, 0.0, mode == "batched_graph_learned", dtd)
         ggs = (C.c_longlong * 3)(0, 0, 0)
         ctx.set_graphs(mode != "per_patch_loop")
+        # a fresh context-wide schedule per arm (each arm's own settings below)
+        ctx.set_level_config(schedule="batched", riemann_threads=128, persistent=0,
+                             max_scratch_bytes=0)
+        if mode == "per_patch_graph":
+            ctx.set_level_config(schedule="per_grid")
+        if mode == "batched_graph_bounded":
+            ctx.set_level_config(max_scratch_bytes=bound)
+        if mode == "batched_graph_autotuned":
+            dt0 = ctx.compute_timestep_level(grids, hp, f)
+            t0 = time.perf_counter()
+            tuning = ctx.autotune_level(grids, hp, f, dt0)
+            tuning["seconds"] = time.perf_counter() - t0
         torch.cuda.synchronize()
         L = ctx.L
 
@@ -531,17 +549,86 @@ def run_level(ctx, args, stream):
         if fold:
             ctx.set_cfl(None)
         out[mode] = {"ms_per_step": ms, "zone_updates_per_s": active / (ms * 1e-3),
-                     "newton_per_interface": newton}
+                     "newton_per_interface": newton,
+                     "context_device_bytes": ctx.device_bytes(),
+                     "schedule": ctx.level_config().as_dict()}
         del f, arr, keep
         torch.cuda.empty_cache()
     ctx.set_graphs(False)
-    out["speedup_batched_vs_loop"] = (out["batched_graph"]["zone_updates_per_s"] /
-                                      out["per_patch_loop"]["zone_updates_per_s"])
+    ctx.set_level_config(**{k: v for k, v in default_cfg.items()})
+    fields_bytes = sum(sum(v.nbytes for v in fh.values()) for fh in host)
+    out["fields_bytes"] = fields_bytes
+    out["bounded_scratch_limit_bytes"] = bound
+    out["autotuner"] = tuning
+    base = out["per_patch_loop"]["zone_updates_per_s"]
+    out["speedup_batched_vs_loop"] = out["batched_graph"]["zone_updates_per_s"] / base
+    out["speedup_per_patch_graph_vs_loop"] = out["per_patch_graph"]["zone_updates_per_s"] / base
+    out["speedup_batched_vs_per_patch_graph"] = (out["batched_graph"]["zone_updates_per_s"] /
+                                                 out["per_patch_graph"]["zone_updates_per_s"])
+    out["speedup_autotuned_vs_loop"] = (out["batched_graph_autotuned"]["zone_updates_per_s"] /
+                                        base)
     out["speedup_batched_learned_vs_loop"] = (
-        out["batched_graph_learned"]["zone_updates_per_s"] /
-        out["per_patch_loop"]["zone_updates_per_s"])
-    out["bit_identical"] = digests["batched_graph"] == digests["per_patch_loop"]
+        out["batched_graph_learned"]["zone_updates_per_s"] / base)
+    out["bit_identical"] = all(digests[m] == digests["per_patch_loop"] for m in
+                               ("batched_graph", "per_patch_graph", "batched_graph_autotuned",
+                                "batched_graph_bounded"))
     return out
+
+
+def run_level_partition(ctx, args, stream, rank, world, dist):
+    """The 600-patch level spread over the ranks (N > 1): whole patches to ranks by cell
+    count (parallel.partition_level, the reference's ProcessorNumber), each rank one
+    batched solve of its patches per step, the level time step the minimum over ranks
+    (an 8-byte NCCL all-reduce, SetLevelTimeStep.C:66-69).  Strong scaling: the level is
+    the same for every N.  Time: CUDA events, the maximum over ranks."""
+    import torch
+    from ppm_b200 import capi
+    from ppm_b200 import parallel as PAR
+    dev = torch.device("cuda", torch.cuda.current_device())
+    hp = H.HydroParams(gamma=5.0 / 3.0, cfl=0.4, dual=True)
+    grids, host = H.amr_level(hp, npatch=args.level_patches, seed=args.seed)
+    parts = PAR.partition_level(grids, world)
+    mine = parts[rank]
+    g_mine = [grids[k] for k in mine]
+    f = [{k: torch.from_numpy(v).to(dev) for k, v in host[i].items()} for i in mine]
+    del host
+    dtd = torch.zeros(1, dtype=torch.float64, device=dev)
+    ctx.set_graphs(True)
+
+    def step(cyc):
+        ctx.compute_timestep_level(g_mine, hp, f, dt_device=dtd, want_host=False)
+        dist.all_reduce(dtd, op=dist.ReduceOp.MIN)
+        ctx.solve_level(g_mine, hp, 0.0, cyc, f, dt_device=dtd)
+        ctx.set_boundary_level(g_mine, f, hp.dual)
+
+    for c in range(3):
+        step(c)
+    torch.cuda.synchronize()
+    dist.barrier()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    steps = 3
+    ev0.record(stream)
+    for c in range(3, 3 + steps):
+        step(c)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    dist.barrier()
+    rc, _ = ctx.synchronize()
+    if rc != 0:
+        raise RuntimeError(f"level partition steps failed: {capi.error_string(rc)}")
+    t = torch.tensor([ev0.elapsed_time(ev1) / steps], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ctx.set_graphs(False)
+    active = sum(g.active_cells for g in grids)
+    my_cells = sum(g.active_cells for g in g_mine)
+    cells = torch.tensor([float(my_cells)], dtype=torch.float64, device=dev)
+    dist.all_reduce(cells, op=dist.ReduceOp.MAX)
+    del f
+    torch.cuda.empty_cache()
+    return {"patches": len(grids), "active_cells": active, "ranks": world, "steps": steps,
+            "ms_per_step": float(t.item()), "zone_updates_per_s": active / (t.item() * 1e-3),
+            "scaling": "strong", "largest_rank_share": float(cells.item()) / active}
 
 
 # ---------------------------------------------------------------- tolerance check
@@ -671,13 +758,28 @@ def run_ours(args):
     ctx = capi.Context(local, stream=stream.cuda_stream, variant=variant)
 
     hp = H.HydroParams(gamma=5.0 / 3.0, cfl=0.4, dual=True, riemann=RIEMANN[args.riemann])
-    g = H.Grid.uniform((args.size,) * 3)
-    f_host = H.turbulence(g, hp, mach=3.0, seed=args.seed + rank)
+    # One GPU: a periodic size^3 grid.  N GPUs: a size x size x (N size) periodic grid cut
+    # into N z slabs of size^3 active cells (weak scaling), each slab with its own 3-cell
+    # ghost shell; every step the slabs exchange their z ghost layers over NCCL
+    # (parallel.Slabs.exchange) and fill their x/y ghosts locally.  Each slab starts from
+    # its own seeded turbulence realisation of the same generator.
+    from ppm_b200 import parallel as PAR
+    slabs = None
+    bc = ("periodic",) * 3
+    if world > 1:
+        slabs = PAR.Slabs((args.size, args.size, args.size * world), world,
+                          width=(1.0, 1.0, float(world)))
+        g = slabs.slab(rank)
+        bc = slabs.local_bc()
+    else:
+        g = H.Grid.uniform((args.size,) * 3)
+    f_host = H.turbulence(H.Grid.uniform((args.size,) * 3), hp, mach=3.0, seed=args.seed + rank)
     for k, frac in enumerate(colour_fractions(args.colours)):  # +16 B per colour and sweep
         f_host[f"col{k}"] = frac * f_host["d"]
     fields = {k: torch.from_numpy(v).to(dev) for k, v in f_host.items()}
     dt_dev = torch.zeros(1, dtype=torch.float64, device=dev)
-    periodic = ("periodic",) * 3
+    if slabs is not None:  # the initial z ghosts come from the neighbouring slabs
+        slabs.exchange(fields, rank, dist)
 
     # calc_dt: an explicit pass for the first cycle, then folded into the last sweep of
     # each solve (ppm_b200_set_cfl), which leaves the next cycle's dt in dt_dev
@@ -690,7 +792,9 @@ def run_ours(args):
             dist.all_reduce(dt_dev, op=dist.ReduceOp.MIN)
         ctx.solve_ppm_de(g, hp, 0.0, cyc, fields, memory=capi.MEM_DEVICE, want_stats=False,
                          dt_device=dt_dev)
-        ctx.set_boundary(g, fields, hp.dual, periodic)
+        if slabs is not None:
+            slabs.exchange(fields, rank, dist)
+        ctx.set_boundary(g, fields, hp.dual, bc)
 
     cyc = 0
     for _ in range(args.warmup):
@@ -795,6 +899,8 @@ def run_ours(args):
     level = None
     if world == 1 and not args.no_level:
         level = run_level(ctx, args, stream)
+    elif world > 1 and not args.no_level:
+        level = run_level_partition(ctx, args, stream, rank, world, dist)
 
     # both builds on the same initial state, a few steps each
     variants = None
@@ -832,7 +938,9 @@ def run_ours(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded turbulence generator)",
-            "config": dict(workload_config(args), parallelism=f"grid per GPU x{world}",
+            "config": dict(workload_config(args),
+                           parallelism=("one grid" if world == 1 else
+                                        f"z slabs x{world}, NCCL halo exchange + dt MIN"),
                            build=variant),
             "build": {"variant": variant,
                       "flags": ("nvcc -fmad=false (bit-identical to the FP64 oracle)"

@@ -18,6 +18,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -64,6 +65,7 @@ void launch_cfl_finalize(const unsigned long long* min_bits, double courant, dou
 void launch_sweep_batch(const BatchArgs& B, int64_t march_blocks, int64_t riemann_blocks,
                         bool dual, bool grav, cudaStream_t st, cudaEvent_t* ev, bool learned,
                         bool contiguous);
+int riemann_resident_blocks(bool dual, bool one, int threads);
 // learned-start training and evaluation (ppm_mlp.cu)
 cudaError_t launch_guess_features(const double* rec, int64_t n, double gamma, double pmin,
                                   float* out, cudaStream_t st);
@@ -180,7 +182,16 @@ struct ppm_b200_context {
   DevBuf flux_fix;          // flux arrays and phases of ppm_b200_correct_fluxes
   std::vector<double> capture_host;
   std::vector<double> col_capture_host;
-  Mirror mirror[kSlotCount];
+  // descriptor slots, in banks: bank 0 serves every entry point; a level solved in
+  // waves takes one bank per wave, so a graph holding all the waves finds each wave's
+  // descriptors where that wave left them.  `mirror` is the current bank.
+  std::vector<std::unique_ptr<std::array<Mirror, kSlotCount>>> banks;
+  Mirror* mirror = nullptr;
+  // level schedule (ppm_b200_set_level_config / the autotuner) and the Riemann settings
+  // of the batch being prepared (prepare_sweep reads them)
+  ppm_b200_level_config level{};
+  int wave_rt = ppm::kRiemannThreads;
+  int wave_persist = 0;
   // event timing of sweep launches
   bool profiling = false;
   std::vector<cudaEvent_t> ev_pool;  // kSweepEvents per timed sweep
@@ -238,6 +249,12 @@ int ensure(ppm_b200_context* ctx, DevBuf& b, size_t bytes) {
 }
 
 // Upload `img` into mirror slot m unless the device copy already holds it.
+// Make bank w the current descriptor bank (allocated on first use).
+void select_bank(ppm_b200_context* ctx, size_t w) {
+  while (ctx->banks.size() <= w) ctx->banks.emplace_back(new std::array<Mirror, kSlotCount>());
+  ctx->mirror = ctx->banks[w]->data();
+}
+
 int mirror_put(ppm_b200_context* ctx, Mirror& m, const std::vector<unsigned char>& img) {
   if (m.host.size() == img.size() && m.dev.p &&
       std::memcmp(m.host.data(), img.data(), img.size()) == 0)
@@ -652,6 +669,12 @@ int prepare_sweep(ppm_b200_context* ctx, int dim, int position, const ppm_b200_p
   if (rc) return rc;
   const Coef* coef_dev = (const Coef*)ctx->mirror[kSlotCoef0 + dim].dev.p;
 
+  // the two-shock stage with the plain start takes the batch's block size and
+  // persistence; every other Riemann stage runs kRiemannThreads faces per block
+  const bool plain_riemann = !p->learned_guess && p->number_of_colours == 0 &&
+                             solver_code(p) == 0 && p->pressure_free != 1;
+  const int rt = plain_riemann ? ctx->wave_rt : ppm::kRiemannThreads;
+  const bool persist = plain_riemann && ctx->wave_persist != 0;
   // face scratch: planes of every grid, then the flagged-pencil list
   std::vector<SweepArgs> rec(ng);
   std::vector<int64_t> mpre(ng + 1, 0), rpre(ng + 1, 0);
@@ -695,8 +718,7 @@ int prepare_sweep(ppm_b200_context* ctx, int dim, int position, const ppm_b200_p
     total_pencils += a.npencils;
     if (nc > 0) flag_bytes += (size_t)a.plane;
     const int64_t mb = (a.npencils + ppm::kMarchThreads - 1) / ppm::kMarchThreads;
-    const int64_t rb = (int64_t)(a.ie - a.is + 2) *
-                       ((a.npencils + ppm::kRiemannThreads - 1) / ppm::kRiemannThreads);
+    const int64_t rb = (int64_t)(a.ie - a.is + 2) * ((a.npencils + rt - 1) / rt);
     mpre[k + 1] = mpre[k] + mb;
     rpre[k + 1] = rpre[k] + rb;
   }
@@ -839,6 +861,13 @@ int prepare_sweep(ppm_b200_context* ctx, int dim, int position, const ppm_b200_p
   plan.B.flagged = (int64_t*)(scratch + scratch_doubles);
   plan.march_blocks = mpre[ng];
   plan.riemann_blocks = rpre[ng];
+  plan.B.riemann_threads = rt;
+  plan.B.persistent = persist ? 1 : 0;
+  plan.B.riemann_total = rpre[ng];
+  if (persist)
+    plan.riemann_blocks = std::min<int64_t>(
+        rpre[ng], (int64_t)ctx->sms *
+                      ppm::riemann_resident_blocks(p->dual_energy != 0, ng == 1, rt));
   plan.contiguous = dim == 0;
   return PPM_B200_OK;
 }
@@ -1198,18 +1227,22 @@ int prepare_solve(ppm_b200_context* ctx, const ppm_b200_params* p, int cycle,
   return PPM_B200_OK;
 }
 
+// cfl_first / cfl_last: this solve is the first / last of a level's waves, which share
+// one folded time step: the minimum is reset before the first wave's last sweep and the
+// time step written after the last wave's (every wave reads the old one until then).
 int enqueue_solve(ppm_b200_context* ctx, const ppm_b200_params* p, const std::vector<GridIO>& io,
-                  const SolvePlan& sp, bool capturing) {
+                  const SolvePlan& sp, bool capturing, bool cfl_first = true,
+                  bool cfl_last = true) {
   ppm::launch_pressure_batch(sp.pressure.B, sp.pressure.size_blocks, ctx->stream);
   ctx->launches += 1;
   CK(cudaGetLastError());
   unsigned long long* cfl_bits = ((unsigned long long*)ctx->misc.p) + 2;
   for (int s = 0; s < sp.nsweeps; ++s) {
     const bool cfl = ctx->cfl_dt != nullptr && s == sp.nsweeps - 1;
-    if (cfl) ppm::launch_cfl_reset(cfl_bits, ctx->stream);
+    if (cfl && cfl_first) ppm::launch_cfl_reset(cfl_bits, ctx->stream);
     int rc = enqueue_sweep(ctx, sp.sweep[s], p, capturing);
     if (rc) return rc;
-    if (cfl) {
+    if (cfl && cfl_last) {
       ppm::launch_cfl_finalize(cfl_bits, ctx->cfl_courant, ctx->cfl_dt, ctx->stream);
       ctx->launches += 1;
       CK(cudaGetLastError());
@@ -1230,6 +1263,124 @@ int enqueue_solve(ppm_b200_context* ctx, const ppm_b200_params* p, const std::ve
     CK(cudaGetLastError());
   }
   return PPM_B200_OK;
+}
+
+// ------------------------------------------------------------ level schedules (waves)
+// A wave: grids of a level solved as one batch (indices into the level's io list, which
+// is sorted largest first), with the Riemann settings of that batch.
+struct Wave {
+  std::vector<int> grids;
+  int riemann_threads = ppm::kRiemannThreads;
+  int persistent = 0;
+};
+
+int size_class(const ppm_b200_context* ctx, const ppm_b200_grid* g) {
+  const long long a = grid_active(g);
+  if (a < ctx->level.class_cells[0]) return 0;
+  if (a < ctx->level.class_cells[1]) return 1;
+  return 2;
+}
+
+// Device bytes a batch of grids takes beyond its fields: two ring sets and the pressure
+// per grid, and the face scratch of its largest sweep direction.
+size_t batch_scratch_bytes(const ppm_b200_params* p, const std::vector<GridIO>& io,
+                           const std::vector<int>& idx) {
+  size_t fields = 0;
+  std::vector<GridIO> sub;
+  for (int k : idx) {
+    const GridIO& x = io[k];
+    int nf = 0;
+    for (int f = 0; f < 6; ++f) nf += x.user.f[f] ? 1 : 0;
+    fields += (2 * (size_t)nf + 1) * (size_t)grid_size(x.g) * sizeof(double);
+    sub.push_back(x);
+  }
+  size_t faces = 0;
+  if (!sub.empty())
+    for (int d = 0; d < sub[0].g->rank; ++d) faces = std::max(faces, sweep_scratch_bytes(d, sub, p));
+  return fields + faces;
+}
+
+// The waves of a level solve under the context's level configuration.
+void plan_waves(const ppm_b200_context* ctx, const ppm_b200_params* p,
+                const std::vector<GridIO>& io, std::vector<Wave>& waves) {
+  const ppm_b200_level_config& c = ctx->level;
+  const int ng = (int)io.size();
+  waves.clear();
+  auto rt_of = [](int v) { return (v == 64 || v == 256) ? v : (int)ppm::kRiemannThreads; };
+  if (c.schedule == PPM_B200_LEVEL_PER_GRID) {
+    for (int k = 0; k < ng; ++k) {
+      Wave w;
+      w.grids.push_back(k);
+      w.riemann_threads = rt_of(c.riemann_threads[3]);
+      w.persistent = c.persistent[3] != 0;
+      waves.push_back(w);
+    }
+    return;
+  }
+  // groups: all grids, or the size classes in order (largest first, as io is sorted)
+  std::vector<std::vector<int>> groups;
+  std::vector<int> group_cfg;
+  if (c.schedule == PPM_B200_LEVEL_CLASSES) {
+    for (int cls = 2; cls >= 0; --cls) {
+      std::vector<int> gcls;
+      for (int k = 0; k < ng; ++k)
+        if (size_class(ctx, io[k].g) == cls) gcls.push_back(k);
+      if (!gcls.empty()) {
+        groups.push_back(gcls);
+        group_cfg.push_back(cls);
+      }
+    }
+  } else {
+    std::vector<int> all(ng);
+    for (int k = 0; k < ng; ++k) all[k] = k;
+    groups.push_back(all);
+    group_cfg.push_back(3);
+  }
+  // each group cut into waves that fit the scratch bound (a grid alone always fits)
+  for (size_t gi = 0; gi < groups.size(); ++gi) {
+    Wave w;
+    w.riemann_threads = rt_of(c.riemann_threads[group_cfg[gi]]);
+    w.persistent = c.persistent[group_cfg[gi]] != 0;
+    for (int k : groups[gi]) {
+      if (c.max_scratch_bytes > 0 && !w.grids.empty()) {
+        std::vector<int> trial = w.grids;
+        trial.push_back(k);
+        if (batch_scratch_bytes(p, io, trial) > (size_t)c.max_scratch_bytes) {
+          waves.push_back(w);
+          w.grids.clear();
+        }
+      }
+      w.grids.push_back(k);
+    }
+    if (!w.grids.empty()) waves.push_back(w);
+  }
+}
+
+// Sizes the ring sets, pressure and face scratch for the largest wave before any wave is
+// prepared, so no later wave moves a buffer an earlier one recorded.
+int reserve_level_scratch(ppm_b200_context* ctx, const ppm_b200_params* p,
+                          const std::vector<GridIO>& io, const std::vector<Wave>& waves) {
+  size_t ring = 0, pres = 0, faces = 0;
+  for (const Wave& w : waves) {
+    size_t r = 0, q = 0;
+    std::vector<GridIO> sub;
+    for (int k : w.grids) {
+      const GridIO& x = io[k];
+      int nf = 0;
+      for (int f = 0; f < 6; ++f) nf += x.user.f[f] ? 1 : 0;
+      r += 2 * (size_t)nf * (size_t)grid_size(x.g);
+      q += (size_t)grid_size(x.g);
+      sub.push_back(x);
+    }
+    ring = std::max(ring, r);
+    pres = std::max(pres, q);
+    for (int d = 0; d < sub[0].g->rank; ++d) faces = std::max(faces, sweep_scratch_bytes(d, sub, p));
+  }
+  int rc = ensure(ctx, ctx->ring, std::max<size_t>(ring, 1) * sizeof(double));
+  if (rc) return rc;
+  rc = ensure(ctx, ctx->pressure, std::max<size_t>(pres, 1) * sizeof(double));
+  if (rc) return rc;
+  return ensure(ctx, ctx->face_scratch, faces);
 }
 
 // Graph key: the by-value launch arguments of a level solve (kernel parameter structs,
@@ -1282,6 +1433,9 @@ std::string graph_key(ppm_b200_context* ctx, const ppm_b200_params* p, const Sol
     key_put(k, b.presfree);
     key_put(k, b.hll_flags);
     key_put(k, b.hll_bytes);
+    key_put(k, b.riemann_threads);
+    key_put(k, b.persistent);
+    key_put(k, b.riemann_total);
     key_put(k, ctx->mirror[kSlotSweep0 + 3 * sp.order[s] + s].version);
   }
   return k;
@@ -1328,6 +1482,15 @@ int ppm_b200_create(int device, void* cuda_stream, ppm_b200_context** out) {
   *out = nullptr;
   ppm_b200_context* ctx = new ppm_b200_context();
   ctx->device = device;
+  select_bank(ctx, 0);
+  ctx->level.schedule = PPM_B200_LEVEL_BATCHED;
+  for (int k = 0; k < 4; ++k) {
+    ctx->level.riemann_threads[k] = ppm::kRiemannThreads;
+    ctx->level.persistent[k] = 0;
+  }
+  ctx->level.class_cells[0] = 48LL * 48 * 48;
+  ctx->level.class_cells[1] = 96LL * 96 * 96;
+  ctx->level.max_scratch_bytes = 0;
   cudaError_t e = cudaSetDevice(device);
   if (e != cudaSuccess) {
     delete ctx;
@@ -1380,10 +1543,11 @@ int ppm_b200_destroy(ppm_b200_context* ctx) {
   fr(ctx->flux_fix);
   fr(ctx->guess);
   fr(ctx->log_count);
-  for (auto& m : ctx->mirror) {
-    fr(m.dev);
-    mirror_free(m);
-  }
+  for (auto& bank : ctx->banks)
+    for (auto& m : *bank) {
+      fr(m.dev);
+      mirror_free(m);
+    }
   for (auto e : ctx->ev_pool) cudaEventDestroy(e);
   if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
@@ -1423,6 +1587,173 @@ int ppm_b200_profile_stages(ppm_b200_context* ctx, double stage_ms[5]) {
   if (!ctx || !stage_ms) return PPM_B200_ERR_INVALID;
   for (int j = 0; j < 5; ++j) stage_ms[j] = ctx->stage_ms[j];
   return PPM_B200_OK;
+}
+
+int ppm_b200_device_bytes(ppm_b200_context* ctx, long long* bytes) {
+  if (!ctx || !bytes) return PPM_B200_ERR_INVALID;
+  size_t n = 0;
+  for (const DevBuf* b : {&ctx->host_set[0], &ctx->host_set[1], &ctx->host_set[2],
+                          &ctx->host_set[3], &ctx->host_set[4], &ctx->host_set[5],
+                          &ctx->host_acc[0], &ctx->host_acc[1], &ctx->host_acc[2],
+                          &ctx->host_col, &ctx->ring, &ctx->pressure, &ctx->face_scratch,
+                          &ctx->counters, &ctx->misc, &ctx->captures, &ctx->capture_buf,
+                          &ctx->col_capture, &ctx->flux_fix, &ctx->guess, &ctx->log_count})
+    n += b->bytes;
+  for (const auto& bank : ctx->banks)
+    for (const auto& m : *bank) n += m.dev.bytes;
+  *bytes = (long long)n;
+  return PPM_B200_OK;
+}
+
+int ppm_b200_set_level_config(ppm_b200_context* ctx, const ppm_b200_level_config* cfg) {
+  if (!ctx || !cfg) return PPM_B200_ERR_INVALID;
+  if (cfg->schedule < PPM_B200_LEVEL_BATCHED || cfg->schedule > PPM_B200_LEVEL_PER_GRID)
+    return PPM_B200_ERR_INVALID;
+  for (int k = 0; k < 4; ++k)
+    if (cfg->riemann_threads[k] != 64 && cfg->riemann_threads[k] != 128 &&
+        cfg->riemann_threads[k] != 256)
+      return PPM_B200_ERR_INVALID;
+  if (cfg->class_cells[0] < 0 || cfg->class_cells[1] < cfg->class_cells[0] ||
+      cfg->max_scratch_bytes < 0)
+    return PPM_B200_ERR_INVALID;
+  ctx->level = *cfg;
+  return PPM_B200_OK;
+}
+
+int ppm_b200_get_level_config(ppm_b200_context* ctx, ppm_b200_level_config* cfg) {
+  if (!ctx || !cfg) return PPM_B200_ERR_INVALID;
+  *cfg = ctx->level;
+  return PPM_B200_OK;
+}
+
+int ppm_b200_autotune_level(ppm_b200_context* ctx, const ppm_b200_params* p, int cycle_number,
+                            ppm_b200_grid* grids, int ngrids, ppm_b200_level_tuning* rep) {
+  if (!ctx || !p || !grids || ngrids <= 0) return PPM_B200_ERR_INVALID;
+  int rc = check_supported(p);
+  if (rc) return rc;
+  // the tuned settings apply to the two-shock stage with the plain start
+  if (p->number_of_colours > 0 || p->learned_guess || solver_code(p) != 0 ||
+      p->pressure_free == 1)
+    return PPM_B200_ERR_UNSUPPORTED;
+  for (int k = 0; k < ngrids; ++k) {
+    rc = check_grid(&grids[k], p);
+    if (rc) return rc;
+  }
+  CK(cudaSetDevice(ctx->device));
+  // copies of every grid's fields: the tuning solves advance these, not the caller's
+  std::vector<ppm_b200_grid> cg(grids, grids + ngrids);
+  size_t doubles = 0;
+  for (int k = 0; k < ngrids; ++k) {
+    const ppm_b200_grid& g = grids[k];
+    const size_t n = (size_t)grid_size(&g);
+    doubles += n * (2 + (size_t)g.rank + (p->dual_energy ? 1 : 0));
+  }
+  DevBuf copies;
+  rc = ensure(ctx, copies, doubles * sizeof(double));
+  if (rc) return rc;
+  double* at = (double*)copies.p;
+  for (int k = 0; k < ngrids; ++k) {
+    ppm_b200_grid& g = cg[k];
+    const size_t n = (size_t)grid_size(&g);
+    auto take = [&](double*& f) -> int {
+      if (!f) return PPM_B200_OK;
+      CK(cudaMemcpyAsync(at, f, n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+      f = at;
+      at += n;
+      return PPM_B200_OK;
+    };
+    int r = take(g.density);
+    if (!r) r = take(g.total_energy);
+    for (int d = 0; d < 3 && !r; ++d) r = d < g.rank ? take(g.velocity[d]) : PPM_B200_OK;
+    if (!r && p->dual_energy) r = take(g.gas_energy);
+    if (r) {
+      cudaFree(copies.p);
+      return r;
+    }
+  }
+  // the tuning solves neither fold a time step nor replay graphs; the caller's settings
+  // come back afterwards
+  const ppm_b200_level_config saved = ctx->level;
+  double* const saved_cfl = ctx->cfl_dt;
+  const bool saved_graphs = ctx->use_graphs;
+  ctx->cfl_dt = nullptr;
+  ctx->use_graphs = false;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  int err = PPM_B200_OK;
+  auto time_level = [&](const ppm_b200_level_config& cfg, std::vector<ppm_b200_grid>& list) {
+    ctx->level = cfg;
+    if (err || list.empty()) return 0.0;
+    int r = ppm_b200_solve_level(ctx, p, cycle_number, list.data(), (int)list.size(), nullptr);
+    if (!r && cudaEventRecord(e0, ctx->stream) != cudaSuccess) r = PPM_B200_ERR_CUDA;
+    if (!r) r = ppm_b200_solve_level(ctx, p, cycle_number, list.data(), (int)list.size(), nullptr);
+    if (!r && cudaEventRecord(e1, ctx->stream) != cudaSuccess) r = PPM_B200_ERR_CUDA;
+    float ms = 0.0f;
+    if (!r && (cudaEventSynchronize(e1) != cudaSuccess ||
+               cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess))
+      r = PPM_B200_ERR_CUDA;
+    if (r) err = r;
+    return (double)ms;
+  };
+  const int threads[3] = {64, 128, 256};
+  auto candidate = [&](int sched, int slot, int k) {
+    ppm_b200_level_config c = saved;
+    c.schedule = sched;
+    c.max_scratch_bytes = saved.max_scratch_bytes;
+    c.riemann_threads[slot] = threads[k / 2];
+    c.persistent[slot] = k % 2;
+    return c;
+  };
+  ppm_b200_level_tuning t;
+  std::memset(&t, 0, sizeof(t));
+  int best_class[3] = {2, 2, 2};  // candidate index: 128 faces, not persistent
+  for (int cls = 0; cls < 3; ++cls) {
+    std::vector<ppm_b200_grid> list;
+    for (const auto& g : cg)
+      if (size_class(ctx, &g) == cls) {
+        list.push_back(g);
+        t.class_active[cls] += grid_active(&g);
+      }
+    t.class_grids[cls] = (int)list.size();
+    double best = 0.0;
+    for (int k = 0; k < 6 && !list.empty(); ++k) {
+      t.class_ms[cls][k] = time_level(candidate(PPM_B200_LEVEL_BATCHED, 3, k), list);
+      if (k == 0 || t.class_ms[cls][k] < best) {
+        best = t.class_ms[cls][k];
+        best_class[cls] = k;
+      }
+    }
+  }
+  int best_all = 2;
+  for (int k = 0; k < 6; ++k) {
+    t.batched_ms[k] = time_level(candidate(PPM_B200_LEVEL_BATCHED, 3, k), cg);
+    if (t.batched_ms[k] < t.batched_ms[best_all]) best_all = k;
+  }
+  ppm_b200_level_config by_class = saved;
+  by_class.schedule = PPM_B200_LEVEL_CLASSES;
+  for (int cls = 0; cls < 3; ++cls) {
+    by_class.riemann_threads[cls] = threads[best_class[cls] / 2];
+    by_class.persistent[cls] = best_class[cls] % 2;
+  }
+  t.classes_ms = time_level(by_class, cg);
+  ppm_b200_level_config chosen = candidate(PPM_B200_LEVEL_BATCHED, 3, best_all);
+  if (t.classes_ms < t.batched_ms[best_all]) chosen = by_class;
+  t.chosen = chosen;
+  // restore, drop the counters of the tuning solves, free the copies
+  ctx->level = err ? saved : chosen;
+  ctx->cfl_dt = saved_cfl;
+  ctx->use_graphs = saved_graphs;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  int status = PPM_B200_OK;
+  int r2 = read_counters(ctx, nullptr, &status);
+  cudaStreamSynchronize(ctx->stream);
+  cudaFree(copies.p);
+  if (err) return err;
+  if (r2) return r2;
+  if (rep) *rep = t;
+  return status;
 }
 
 int ppm_b200_set_graphs(ppm_b200_context* ctx, int enable) {
@@ -1507,13 +1838,39 @@ int ppm_b200_solve_level(ppm_b200_context* ctx, const ppm_b200_params* p, int cy
     rc = stage_in(ctx, p, &grids[idx[k]], PPM_B200_MEM_DEVICE, io[k].user, io[k].acc, true);
     if (rc) return rc;
   }
-  SolvePlan sp;
-  rc = prepare_solve(ctx, p, cycle_number, io, 0, nullptr, nullptr, sp);
+  // the level's waves (one for the batched schedule without a scratch bound), each
+  // prepared into its own descriptor bank with its Riemann settings
+  std::vector<Wave> waves;
+  plan_waves(ctx, p, io, waves);
+  rc = reserve_level_scratch(ctx, p, io, waves);
   if (rc) return rc;
+  std::vector<SolvePlan> plans(waves.size());
+  std::vector<std::vector<GridIO>> wio(waves.size());
+  std::string key;
+  for (size_t w = 0; w < waves.size(); ++w) {
+    for (int k : waves[w].grids) wio[w].push_back(io[k]);
+    select_bank(ctx, w);
+    ctx->wave_rt = waves[w].riemann_threads;
+    ctx->wave_persist = waves[w].persistent;
+    rc = prepare_solve(ctx, p, cycle_number, wio[w], 0, nullptr, nullptr, plans[w]);
+    if (rc == PPM_B200_OK) key += graph_key(ctx, p, plans[w]);
+    if (rc) break;
+  }
+  select_bank(ctx, 0);
+  ctx->wave_rt = ppm::kRiemannThreads;
+  ctx->wave_persist = 0;
+  if (rc) return rc;
+  auto enqueue_all = [&](bool capturing) {
+    for (size_t w = 0; w < waves.size(); ++w) {
+      int r = enqueue_solve(ctx, p, wio[w], plans[w], capturing, w == 0,
+                            w + 1 == waves.size());
+      if (r) return r;
+    }
+    return (int)PPM_B200_OK;
+  };
   // graph replay needs every per-step value on the device (dt included)
   const bool graph = ctx->use_graphs && p->dt_device != nullptr && !ctx->profiling;
   if (graph) {
-    const std::string key = graph_key(ctx, p, sp);
     auto it = ctx->graphs.find(key);
     if (it == ctx->graphs.end()) {
       if (ctx->graphs.size() >= kMaxGraphs) {
@@ -1523,7 +1880,7 @@ int ppm_b200_solve_level(ppm_b200_context* ctx, const ppm_b200_params* p, int cy
       cudaGraph_t gr;
       CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
       const long long before = ctx->launches;
-      rc = enqueue_solve(ctx, p, io, sp, true);
+      rc = enqueue_all(true);
       cudaError_t e = cudaStreamEndCapture(ctx->stream, &gr);
       if (rc) return rc;
       if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaStreamEndCapture");
@@ -1535,9 +1892,11 @@ int ppm_b200_solve_level(ppm_b200_context* ctx, const ppm_b200_params* p, int cy
       it = ctx->graphs.emplace(key, ex).first;
     }
     CK(cudaGraphLaunch(it->second, ctx->stream));
-    ctx->launches += 1 + sweep_kernels(p) * sp.nsweeps + (p->eos_type > 0 ? 1 : 0);
+    for (const auto& sp : plans)
+      ctx->launches += 1 + sweep_kernels(p) * sp.nsweeps + (p->eos_type > 0 ? 1 : 0);
+    if (ctx->cfl_dt) ctx->launches += 1;  // the folded time step's finalize kernel
   } else {
-    rc = enqueue_solve(ctx, p, io, sp, false);
+    rc = enqueue_all(false);
     if (rc) return rc;
   }
   if (stats) return finish_status(ctx, stats);

@@ -420,13 +420,22 @@ __device__ __forceinline__ void load_face_advected(const SweepArgs& a, int64_t i
 #ifndef PPM_RIEMANN_LEARNED_MINBLOCKS
 #define PPM_RIEMANN_LEARNED_MINBLOCKS (8 * 128 / PPM_RIEMANN_THREADS)
 #endif
-// COL: also store the Godunov density of every face for the colour kernel
-template <bool DUAL, bool ONE, bool LEARNED, bool COL = false>
-__global__ void __launch_bounds__(kRiemannThreads, LEARNED ? PPM_RIEMANN_LEARNED_MINBLOCKS : PPM_RIEMANN_MINBLOCKS) riemann_kernel(const __grid_constant__ BatchArgs B) {
+// COL: also store the Godunov density of every face for the colour kernel.
+// RT: threads (faces) per block; the batch's Riemann prefix table is built for it.
+// PERSIST: a persistent launch -- a grid sized to the resident blocks walks the batch's
+// block list (B.riemann_total entries) with a stride of the grid, keeping each grid's
+// record in shared memory while consecutive blocks belong to it.  RT and PERSIST are the
+// level autotuner's choices per size class (ppm_b200_autotune_level).
+template <bool DUAL, bool ONE, bool LEARNED, bool COL = false, int RT = kRiemannThreads,
+          bool PERSIST = false>
+__global__ void __launch_bounds__(RT, (LEARNED ? PPM_RIEMANN_LEARNED_MINBLOCKS
+                                               : PPM_RIEMANN_MINBLOCKS) * kRiemannThreads / RT)
+    riemann_kernel(const __grid_constant__ BatchArgs B) {
   __shared__ unsigned int s_hist[8];
   __shared__ unsigned int s_newton;
   __shared__ unsigned int s_rejected;
   __shared__ unsigned int s_wtrips, s_warps;
+  __shared__ SweepArgs s_rec;
   if (threadIdx.x < 8) s_hist[threadIdx.x] = 0u;
   if (threadIdx.x == 0) {
     s_newton = 0u;
@@ -434,13 +443,20 @@ __global__ void __launch_bounds__(kRiemannThreads, LEARNED ? PPM_RIEMANN_LEARNED
     s_wtrips = 0u;
     s_warps = 0u;
   }
-  int64_t lb;
-  const int g = locate<ONE>(B.riemann_prefix, B.ngrids, lb);
-  PPM_BIND_RECORD(a, g)
-  if (ONE) __syncthreads();
-  const int64_t chunks = (a.npencils + kRiemannThreads - 1) / kRiemannThreads;
+  int cur = -1;
+  for (int64_t blk = blockIdx.x; !PERSIST || blk < B.riemann_total; blk += gridDim.x) {
+  int64_t lb = blk;
+  const int g = ONE ? 0 : batch_locate(B.riemann_prefix, B.ngrids, blk, lb);
+  if (!ONE && g != cur) {  // block-uniform: every thread takes this branch together
+    __syncthreads();       // the previous grid's record is no longer read
+    load_record(s_rec, B.grids + g);
+    cur = g;
+  }
+  __syncthreads();
+  const SweepArgs& a = ONE ? B.one : s_rec;
+  const int64_t chunks = (a.npencils + RT - 1) / RT;
   const int fi = (int)(lb / chunks);
-  const int64_t pid = (lb - (int64_t)fi * chunks) * kRiemannThreads + threadIdx.x;
+  const int64_t pid = (lb - (int64_t)fi * chunks) * RT + threadIdx.x;
   const bool valid = pid < a.npencils;
   const Phys P = make_phys(a);
   const int64_t idx = (int64_t)fi * a.npencils + pid;
@@ -520,6 +536,8 @@ __global__ void __launch_bounds__(kRiemannThreads, LEARNED ? PPM_RIEMANN_LEARNED
       atomicAdd(&s_wtrips, wmax);
       atomicAdd(&s_warps, 1u);
     }
+  }
+  if (!PERSIST) break;
   }
   __syncthreads();
   if (threadIdx.x < 8 && s_hist[threadIdx.x])
@@ -1604,6 +1622,26 @@ void launch_update(const BatchArgs& B, int64_t march_blocks, cudaStream_t st) {
       <<<(unsigned)march_blocks, kMarchThreads, bytes, st>>>(B);
 }
 
+// The two-shock stage with the plain start: the block size and persistence the batch
+// asks for.  riemann_blocks: the launch's grid (the resident blocks when persistent).
+template <bool DUAL, bool ONE, int RT>
+void launch_riemann_rt(const BatchArgs& B, unsigned rb, cudaStream_t st) {
+  if (B.persistent)
+    riemann_kernel<DUAL, ONE, false, false, RT, true><<<rb, RT, 0, st>>>(B);
+  else
+    riemann_kernel<DUAL, ONE, false, false, RT, false><<<rb, RT, 0, st>>>(B);
+}
+
+template <bool DUAL, bool ONE>
+void launch_riemann_plain(const BatchArgs& B, unsigned rb, cudaStream_t st) {
+  if (B.riemann_threads == 64)
+    launch_riemann_rt<DUAL, ONE, 64>(B, rb, st);
+  else if (B.riemann_threads == 256)
+    launch_riemann_rt<DUAL, ONE, 256>(B, rb, st);
+  else
+    launch_riemann_rt<DUAL, ONE, kRiemannThreads>(B, rb, st);
+}
+
 template <bool DUAL, bool GRAV, bool ONE>
 void launch_stages(const BatchArgs& B, int64_t march_blocks, int64_t riemann_blocks,
                    cudaStream_t st, cudaEvent_t* ev, bool learned, bool staged) {
@@ -1646,7 +1684,7 @@ void launch_stages(const BatchArgs& B, int64_t march_blocks, int64_t riemann_blo
   else if (B.ncolour > 0)
     riemann_kernel<DUAL, ONE, false, true><<<rb, kRiemannThreads, 0, st>>>(B);
   else
-    riemann_kernel<DUAL, ONE, false><<<rb, kRiemannThreads, 0, st>>>(B);
+    launch_riemann_plain<DUAL, ONE>(B, rb, st);
   mark(3);
   if (B.solver != 0) {  // HLL / HLLC
     if (PPM_X_TMA && staged && ONE && B.x_tma)
@@ -1700,6 +1738,33 @@ void launch_any(const BatchArgs& B, int64_t march_blocks, int64_t riemann_blocks
 // iteration from the MLP guess (every record's `guess` must point at packed weights).
 // contiguous: every grid's pencils run along the contiguous axis (sa == 1, the x
 // sweep); the update kernel then stages its stores.
+// Resident blocks per SM of the persistent two-shock stage for a block size (the grid of
+// a persistent launch is this times the SM count).
+int riemann_resident_blocks(bool dual, bool one, int threads) {
+  int n = 0;
+  auto occ = [&](auto kern, int rt) {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, rt, 0);
+  };
+  if (threads == 64) {
+    if (dual) one ? occ(split::riemann_kernel<true, true, false, false, 64, true>, 64)
+              : occ(split::riemann_kernel<true, false, false, false, 64, true>, 64);
+    else one ? occ(split::riemann_kernel<false, true, false, false, 64, true>, 64)
+             : occ(split::riemann_kernel<false, false, false, false, 64, true>, 64);
+  } else if (threads == 256) {
+    if (dual) one ? occ(split::riemann_kernel<true, true, false, false, 256, true>, 256)
+              : occ(split::riemann_kernel<true, false, false, false, 256, true>, 256);
+    else one ? occ(split::riemann_kernel<false, true, false, false, 256, true>, 256)
+             : occ(split::riemann_kernel<false, false, false, false, 256, true>, 256);
+  } else {
+    constexpr int rt = kRiemannThreads;
+    if (dual) one ? occ(split::riemann_kernel<true, true, false, false, rt, true>, rt)
+              : occ(split::riemann_kernel<true, false, false, false, rt, true>, rt);
+    else one ? occ(split::riemann_kernel<false, true, false, false, rt, true>, rt)
+             : occ(split::riemann_kernel<false, false, false, false, rt, true>, rt);
+  }
+  return n > 0 ? n : 1;
+}
+
 void launch_sweep_batch(const BatchArgs& B, int64_t march_blocks, int64_t riemann_blocks,
                         bool dual, bool grav, cudaStream_t st, cudaEvent_t* ev, bool learned,
                         bool contiguous) {

@@ -171,6 +171,12 @@ struct BatchArgs {
   int64_t hll_bytes = 0;
   int solver = 0;                    // the batch's Riemann solver (SweepArgs::solver)
   int presfree = 0;                  // PressureFree (SweepArgs::presfree)
+  // two-shock Riemann stage (plain start, no colours): faces per block (64, 128 or 256;
+  // the Riemann prefix table counts blocks of this size) and a persistent launch that
+  // walks riemann_total blocks with a grid of the resident blocks
+  int riemann_threads = kRiemannThreads;
+  int persistent = 0;
+  int64_t riemann_total = 0;
   CUtensorMap xin[6];
 };
 

@@ -44,6 +44,8 @@ EXPORTS = (
     "ppm_b200_riemann_log_count", "ppm_b200_guess_features", "ppm_b200_guess_grad",
     "ppm_b200_guess_adam", "ppm_b200_guess_eval", "ppm_b200_expansion_terms",
     "ppm_b200_expansion_terms_level", "ppm_b200_set_cfl", "ppm_b200_abi_check",
+    "ppm_b200_set_level_config", "ppm_b200_get_level_config", "ppm_b200_autotune_level",
+    "ppm_b200_device_bytes",
 )
 
 GUESS_WEIGHTS = 4673  # W1[6][64] b1[64] W2[64][64] b2[64] w3[64] b3
@@ -102,6 +104,39 @@ class Stats(C.Structure):
             "fatal_cells": int(self.fatal_cells), "guess_rejected": int(self.guess_rejected),
             "warp_newton_iters": int(self.warp_newton_iters), "warps": int(self.warps),
         }
+
+
+class LevelConfig(C.Structure):
+    _fields_ = [("schedule", C.c_int), ("riemann_threads", C.c_int * 4),
+                ("persistent", C.c_int * 4), ("class_cells", C.c_longlong * 2),
+                ("max_scratch_bytes", C.c_longlong)]
+
+    def as_dict(self):
+        return {"schedule": LEVEL_SCHEDULES[self.schedule],
+                "riemann_threads": list(self.riemann_threads),
+                "persistent": list(self.persistent),
+                "class_cells": list(self.class_cells),
+                "max_scratch_bytes": int(self.max_scratch_bytes)}
+
+
+class LevelTuning(C.Structure):
+    _fields_ = [("class_grids", C.c_int * 3), ("class_active", C.c_longlong * 3),
+                ("class_ms", (C.c_double * 6) * 3), ("batched_ms", C.c_double * 6),
+                ("classes_ms", C.c_double), ("chosen", LevelConfig)]
+
+    def as_dict(self):
+        cand = [f"{t} faces/block{' persistent' if pers else ''}" for t in (64, 128, 256)
+                for pers in (0, 1)]
+        return {"candidates": cand,
+                "class_grids": list(self.class_grids),
+                "class_active_cells": list(self.class_active),
+                "class_ms": [list(r) for r in self.class_ms],
+                "batched_ms": list(self.batched_ms), "classes_ms": self.classes_ms,
+                "chosen": self.chosen.as_dict()}
+
+
+# ppm_b200_level_config.schedule
+LEVEL_SCHEDULES = {0: "batched", 1: "classes", 2: "per_grid"}
 
 
 class PPMError(RuntimeError):
@@ -173,6 +208,11 @@ def lib(build_if_missing: bool = True, variant: str | None = None):
     L.ppm_b200_solve_level.argtypes = [vp, C.POINTER(Params), C.c_int, C.POINTER(GridDesc),
                                        C.c_int, C.POINTER(Stats)]
     L.ppm_b200_set_graphs.argtypes = [vp, C.c_int]
+    L.ppm_b200_set_level_config.argtypes = [vp, C.POINTER(LevelConfig)]
+    L.ppm_b200_device_bytes.argtypes = [vp, C.POINTER(C.c_longlong)]
+    L.ppm_b200_get_level_config.argtypes = [vp, C.POINTER(LevelConfig)]
+    L.ppm_b200_autotune_level.argtypes = [vp, C.POINTER(Params), C.c_int, C.POINTER(GridDesc),
+                                          C.c_int, C.POINTER(LevelTuning)]
     fp = C.POINTER(C.c_float)
     L.ppm_b200_set_guess.argtypes = [vp, vp]
     L.ppm_b200_set_cfl.argtypes = [vp, vp, C.c_double, C.c_double, C.POINTER(C.c_double)]
@@ -459,6 +499,56 @@ class Context:
         if check and rc != OK:
             raise PPMError(rc, "ppm_b200_solve_level")
         return rc, st.as_dict()
+
+    def device_bytes(self):
+        n = C.c_longlong(0)
+        rc = self.L.ppm_b200_device_bytes(self.h, C.byref(n))
+        if rc != OK:
+            raise PPMError(rc, "ppm_b200_device_bytes")
+        return int(n.value)
+
+    def level_config(self):
+        c = LevelConfig()
+        rc = self.L.ppm_b200_get_level_config(self.h, C.byref(c))
+        if rc != OK:
+            raise PPMError(rc, "ppm_b200_get_level_config")
+        return c
+
+    def set_level_config(self, schedule=None, riemann_threads=None, persistent=None,
+                         class_cells=None, max_scratch_bytes=None):
+        """Change the level schedule; arguments left at None keep their current value.
+        schedule: "batched", "classes" or "per_grid"; riemann_threads / persistent: four
+        entries (size classes 0-2, then the batched schedule) or one for all."""
+        c = self.level_config()
+        if schedule is not None:
+            c.schedule = {v: k for k, v in LEVEL_SCHEDULES.items()}[schedule]
+        for name, val in (("riemann_threads", riemann_threads), ("persistent", persistent)):
+            if val is not None:
+                vals = [val] * 4 if isinstance(val, int) else list(val)
+                arr = getattr(c, name)
+                for k in range(4):
+                    arr[k] = int(vals[k])
+        if class_cells is not None:
+            c.class_cells[0], c.class_cells[1] = (int(x) for x in class_cells)
+        if max_scratch_bytes is not None:
+            c.max_scratch_bytes = int(max_scratch_bytes)
+        rc = self.L.ppm_b200_set_level_config(self.h, C.byref(c))
+        if rc != OK:
+            raise PPMError(rc, "ppm_b200_set_level_config")
+        return c.as_dict()
+
+    def autotune_level(self, grids, hp, fields_list, dt, cycle=0, accels=None,
+                       dt_device=None):
+        """Runs the per-size-class autotuner on copies of the level's fields (time step dt,
+        or *dt_device) and keeps its choice; returns its report."""
+        P = make_params(hp, dt, False, dt_device)
+        arr, keep = self._level(grids, fields_list, accels)
+        t = LevelTuning()
+        rc = self.L.ppm_b200_autotune_level(self.h, C.byref(P), int(cycle), arr, len(grids),
+                                            C.byref(t))
+        if rc != OK:
+            raise PPMError(rc, "ppm_b200_autotune_level")
+        return t.as_dict()
 
     def set_graphs(self, enable=True):
         rc = self.L.ppm_b200_set_graphs(self.h, int(bool(enable)))

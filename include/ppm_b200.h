@@ -235,6 +235,53 @@ int ppm_b200_solve_level(ppm_b200_context *ctx, const ppm_b200_params *params,
 /* enable != 0: replay level solves from CUDA graphs (see ppm_b200_solve_level). */
 int ppm_b200_set_graphs(ppm_b200_context *ctx, int enable);
 
+/* How ppm_b200_solve_level schedules a level (no reference counterpart: the reference
+   runs its grid loop, EvolveLevel.C:569-585, one grid at a time).
+   schedule: PPM_B200_LEVEL_BATCHED -- every grid in one launch per kernel stage;
+             PPM_B200_LEVEL_CLASSES -- one such batch per size class, one after another,
+             each with its class's Riemann settings;
+             PPM_B200_LEVEL_PER_GRID -- one launch per kernel stage per grid, largest
+             first: the reference's loop, kept for comparison (graph-replayable).
+   Size classes by active cells: class 0 below class_cells[0], class 1 below
+   class_cells[1], class 2 the rest.  The two-shock Riemann stage (plain start, no
+   colours) of a batch runs riemann_threads faces per block (64, 128 or 256) and, with
+   persistent != 0, as a persistent launch of the resident blocks that walks the batch's
+   block list; index 3 is the setting of the BATCHED schedule, 0-2 those of the classes.
+   max_scratch_bytes > 0 bounds the level's device scratch (ring sets, pressure and face
+   planes): grids are then solved in waves that each fit it (a single grid larger than
+   the bound still runs, alone).  Results are bit-identical whatever the schedule. */
+#define PPM_B200_LEVEL_BATCHED 0
+#define PPM_B200_LEVEL_CLASSES 1
+#define PPM_B200_LEVEL_PER_GRID 2
+typedef struct ppm_b200_level_config {
+  int schedule;
+  int riemann_threads[4];
+  int persistent[4];
+  long long class_cells[2];
+  long long max_scratch_bytes;
+} ppm_b200_level_config;
+int ppm_b200_set_level_config(ppm_b200_context *ctx, const ppm_b200_level_config *cfg);
+int ppm_b200_get_level_config(ppm_b200_context *ctx, ppm_b200_level_config *cfg);
+
+/* The per-size-class autotuner (no reference counterpart).  Times, on copies of the
+   grids' fields made in the context (DEVICE memory; the grids themselves are not
+   changed), one solve of every size class for each Riemann setting -- candidate
+   k = 2 * t + persistent with t = 0, 1, 2 for 64, 128, 256 faces per block -- then the
+   whole level as one batch for each candidate and as one batch per class with each
+   class's best, and keeps the fastest schedule as the context's level configuration
+   (max_scratch_bytes is kept).  Synchronises; about 40 level solves. */
+typedef struct ppm_b200_level_tuning {
+  int class_grids[3];          /* grids per size class */
+  long long class_active[3];   /* active cells per size class */
+  double class_ms[3][6];       /* ms of one solve of the class, per candidate (0: no grids) */
+  double batched_ms[6];        /* ms of one solve of the whole level as one batch */
+  double classes_ms;           /* ms with one batch per class, each with its best candidate */
+  ppm_b200_level_config chosen;
+} ppm_b200_level_tuning;
+int ppm_b200_autotune_level(ppm_b200_context *ctx, const ppm_b200_params *params,
+                            int cycle_number, ppm_b200_grid *grids, int ngrids,
+                            ppm_b200_level_tuning *report);
+
 /* min over the grids of the hydro Courant time step (SetLevelTimeStep.C:66 over
    grid::ComputeTimeStep), one reduction for the whole level. */
 int ppm_b200_compute_timestep_level(ppm_b200_context *ctx, const ppm_b200_params *params,
@@ -305,6 +352,10 @@ int ppm_b200_correct_fluxes_sublings(ppm_b200_context *ctx, const ppm_b200_param
    recorded by device work since the last call; accumulates device counters
    into *stats (may be NULL). */
 int ppm_b200_synchronize(ppm_b200_context *ctx, ppm_b200_stats *stats);
+
+/* Device memory the context holds (scratch, staging of host-memory calls, descriptor
+   images), in bytes (no reference counterpart). */
+int ppm_b200_device_bytes(ppm_b200_context *ctx, long long *bytes);
 
 /* Number of kernels this library has launched on the context since creation. */
 long long ppm_b200_launch_count(ppm_b200_context *ctx);
@@ -422,7 +473,9 @@ int ppm_b200_version(void);
   X(offsetof(ppm_b200_fluxes, left)) X(offsetof(ppm_b200_fluxes, right))             \
   X(offsetof(ppm_b200_fluxes, colour_left)) X(offsetof(ppm_b200_fluxes, colour_right)) \
   X(sizeof(ppm_b200_stats)) X(offsetof(ppm_b200_stats, newton_hist))                 \
-  X(offsetof(ppm_b200_stats, guess_rejected)) X(offsetof(ppm_b200_stats, warps))
+  X(offsetof(ppm_b200_stats, guess_rejected)) X(offsetof(ppm_b200_stats, warps))             \
+  X(sizeof(ppm_b200_level_config)) X(offsetof(ppm_b200_level_config, max_scratch_bytes))     \
+  X(sizeof(ppm_b200_level_tuning)) X(offsetof(ppm_b200_level_tuning, chosen))
 int ppm_b200_abi_check(const long long *layout, int n);
 
 #ifdef __cplusplus

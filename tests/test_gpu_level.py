@@ -185,3 +185,77 @@ def test_level_rejects_mixed_rank(torch):
     rc, _ = ctx.solve_level(grids, hp, 1e-3, 0, [_dev(f, torch) for f in host], check=False)
     assert rc == capi.ERR_INVALID
     ctx.close()
+
+
+@pytest.mark.parametrize("schedule,threads,persistent,scratch", [
+    ("per_grid", 128, 0, 0),
+    ("classes", (64, 256, 128, 128), (1, 0, 1, 0), 0),
+    ("batched", 64, 1, 0),
+    ("batched", 256, 0, 0),
+    ("batched", 128, 1, 4_000_000),  # waves: a few grids at a time
+    ("classes", 128, 0, 1),          # every grid its own wave
+])
+def test_level_schedules_are_bit_identical(torch, schedule, threads, persistent, scratch):
+    # the level schedules (one batch, one batch per size class, one grid at a time), the
+    # Riemann stage's block size and persistent launch, and waves under a scratch bound
+    # change how the level is launched, never its results: the same fields and the same
+    # folded time step as the default batch, direct and replayed from graphs
+    hp = H.HydroParams(gamma=5.0 / 3.0, cfl=0.5, dual=True)
+    grids, host = _level(hp, 600)
+    ref = [_dev(f, torch) for f in host]
+    a = capi.Context(0)
+    dt_a = torch.zeros(1, dtype=torch.float64, device="cuda")
+    a.compute_timestep_level(grids, hp, ref, dt_device=dt_a, want_host=False)
+    a.set_cfl(dt_a, courant=hp.cfl)
+    for graphs in (False, True):
+        b = capi.Context(0)
+        b.set_graphs(graphs)
+        # class bounds inside the test level's range of sizes, so every class has grids
+        b.set_level_config(schedule=schedule, riemann_threads=threads, persistent=persistent,
+                           class_cells=(700, 2500), max_scratch_bytes=scratch)
+        cur = [_dev(f, torch) for f in host]
+        dt_b = torch.zeros(1, dtype=torch.float64, device="cuda")
+        b.compute_timestep_level(grids, hp, cur, dt_device=dt_b, want_host=False)
+        b.set_cfl(dt_b, courant=hp.cfl)
+        for cyc in range(4):
+            b.solve_level(grids, hp, 0.0, cyc, cur, dt_device=dt_b)
+            b.set_boundary_level(grids, cur, True)
+            if not graphs:
+                a.solve_level(grids, hp, 0.0, cyc, ref, dt_device=dt_a)
+                a.set_boundary_level(grids, ref, True)
+        assert b.synchronize()[0] == capi.OK
+        assert a.synchronize()[0] == capi.OK
+        # ref advanced the same 4 cycles in the first pass
+        assert dt_b.item() == dt_a.item(), (graphs, dt_b.item(), dt_a.item())
+        for k, g in enumerate(grids):
+            _assert_same(_host(cur[k]), _host(ref[k]), g, (schedule, graphs, k))
+        b.set_cfl(None)
+        b.close()
+    a.set_cfl(None)
+    a.close()
+
+
+def test_level_autotuner_keeps_a_choice_and_leaves_fields_alone(torch):
+    hp = H.HydroParams(gamma=5.0 / 3.0, cfl=0.5, dual=True)
+    grids, host = _level(hp, 700)
+    dev = [_dev(f, torch) for f in host]
+    before = [_host(f) for f in dev]
+    ctx = capi.Context(0)
+    ctx.set_level_config(class_cells=(700, 2500), max_scratch_bytes=0)
+    dt = ctx.compute_timestep_level(grids, hp, dev)
+    rep = ctx.autotune_level(grids, hp, dev, dt)
+    assert sum(rep["class_grids"]) == len(grids)
+    assert all(ms > 0.0 for ms in rep["batched_ms"]) and rep["classes_ms"] > 0.0
+    assert rep["chosen"] == ctx.level_config().as_dict()
+    for k, g in enumerate(grids):  # the tuning ran on copies
+        for name in before[k]:
+            assert np.array_equal(before[k][name], dev[k][name].cpu().numpy()), (k, name)
+    # and a solve under the chosen schedule is the oracle's
+    ora = [copy_fields(f) for f in host]
+    rc, _ = ctx.solve_level(grids, hp, dt, 0, dev, want_stats=True)
+    assert rc == capi.OK
+    for k, g in enumerate(grids):
+        rc, _ = O.solve_ppm_de(g, hp, dt, 0, ora[k], g.cellwidth)
+        assert rc == 0
+        _assert_same(_host(dev[k]), ora[k], g, ("tuned", k))
+    ctx.close()
