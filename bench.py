@@ -70,6 +70,10 @@ def parse():
     ap.add_argument("--level-patches", type=int, default=600)
     ap.add_argument("--no-learned", action="store_true",
                     help="skip the learned-Newton-start comparisons")
+    ap.add_argument("--pancake-size", type=int, default=256,
+                    help="root grid of the nested Zel'dovich-pancake configuration")
+    ap.add_argument("--pancake-steps", type=int, default=6,
+                    help="root steps of the pancake timed (0 skips it)")
     ap.add_argument("--config4-size", type=int, default=512,
                     help="grid of the learned-start configuration (Mach-10 turbulence)")
     ap.add_argument("--riemann", choices=list(RIEMANN), default="twoshock",
@@ -452,6 +456,61 @@ def run_config4(ctx, args, stream):
     return out
 
 
+def run_pancake(ctx, args, stream):
+    """The cosmological configuration: a Zel'dovich pancake (z_init = 100, caustic at
+    z = 1, dual energy, self-gravity, comoving expansion terms) on a root of n^3 zones with
+    two nested static levels (refinement 2, each the middle half of its parent, centred on
+    the caustic), advanced through Enzo's W cycle by the hierarchy stand-in of
+    ppm_b200.hierarchy with the fields on the device.  A bounded sample of root steps
+    from z = 100 is timed; the run to z = 1 takes the number of root steps the expansion
+    limit (da/a <= 0.01) allows, which the line states with the projected time."""
+    import torch
+    from ppm_b200 import hierarchy as N
+    n = args.pancake_size
+    hp = H.HydroParams(gamma=5.0 / 3.0, cfl=0.5, dual=True, gravity=True)
+    cosmo = N.EdS(100.0)
+    levels = N.nested_pancake(n, 3, hp, z_init=100.0, z_collapse=1.0)
+    run = N.NestedRun(levels, hp, N.DeviceBackend(ctx, hp), cosmo)
+    for _ in range(2):
+        run.step()
+    torch.cuda.synchronize()
+    steps0 = list(run.level_steps)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.pancake_steps):
+        run.step()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    rc, _ = ctx.synchronize()
+    if rc != 0:
+        raise RuntimeError("pancake steps failed")
+    zone_updates = sum((run.level_steps[l] - steps0[l]) * levels[l].grid.active_cells
+                       for l in range(len(levels)))
+    # root steps from z = 100 to z = 1 under the expansion limit alone
+    t, steps_to_z1 = cosmo.t_init, 0
+    t1 = cosmo.time_of(1.0)
+    while t < t1 * (1.0 - 1e-14):
+        t = min(t + 0.01 / cosmo.adot_over_a(t), t1)
+        steps_to_z1 += 1
+    ms_root = ms / args.pancake_steps
+    out = {"workload": f"Zel'dovich pancake, {n}^3 root + 2 nested levels of {n}^3 (refinement "
+                       "2, centred on the caustic), z_init 100, caustic z 1, dual energy, "
+                       "self-gravity (1-D spectral stand-in), comoving expansion, FP64",
+           "root_steps_timed": args.pancake_steps, "level_steps_timed":
+           [run.level_steps[l] - steps0[l] for l in range(len(levels))],
+           "ms_per_root_step": ms_root, "zone_updates_per_s": zone_updates / (ms * 1e-3),
+           "redshift_reached": cosmo.redshift(levels[0].t),
+           "root_steps_to_z1": steps_to_z1,
+           "projected_seconds_to_z1": steps_to_z1 * ms_root * 1e-3,
+           "note": "the finer levels take one step per parent step while the expansion limit "
+                   "sets the time step; device-resident fields, flux boxes on the host"}
+    del run, levels
+    torch.cuda.empty_cache()
+    return out
+
+
 # ---------------------------------------------------------------- AMR level (batched)
 def run_level(ctx, args, stream):
     """One AMR level of 600 patches (edges log-uniform in 16-128 per axis, 3 ghost zones,
@@ -482,6 +541,12 @@ def run_level(ctx, args, stream):
     bound = 4 << 30  # the bounded-scratch arm: at most 4 GiB of level scratch
     for mode in ("batched_graph", "per_patch_loop", "per_patch_graph",
                  "batched_graph_autotuned", "batched_graph_bounded", "batched_graph_learned"):
+        # the bounded-scratch arm runs in a context of its own, so its device footprint is
+        # its own (a context's scratch only grows)
+        if mode == "batched_graph_bounded":
+            main_ctx = ctx
+            ctx = capi.Context(torch.cuda.current_device(), stream=stream.cuda_stream,
+                               variant=main_ctx.variant)
         f = [{k: torch.from_numpy(v).to(dev) for k, v in fh.items()} for fh in host]
         arr, keep = ctx._level(grids, f)
         P = capi.make_params(hp, 0.0, mode == "batched_graph_learned", dtd)
@@ -553,6 +618,9 @@ def run_level(ctx, args, stream):
                      "context_device_bytes": ctx.device_bytes(),
                      "schedule": ctx.level_config().as_dict()}
         del f, arr, keep
+        if mode == "batched_graph_bounded":
+            ctx.close()
+            ctx = main_ctx
         torch.cuda.empty_cache()
     ctx.set_graphs(False)
     ctx.set_level_config(**{k: v for k, v in default_cfg.items()})
@@ -896,6 +964,10 @@ def run_ours(args):
         learned = run_learned(ctx, g, hp, f_host, args, stream)
         config4 = run_config4(ctx, args, stream)
 
+    pancake = None
+    if world == 1 and args.pancake_steps > 0:
+        pancake = run_pancake(ctx, args, stream)
+
     level = None
     if world == 1 and not args.no_level:
         level = run_level(ctx, args, stream)
@@ -955,6 +1027,7 @@ def run_ours(args):
             "amr_level": level,
             "learned_start": learned,
             "learned_start_mach10": config4,
+            "nested_pancake": pancake,
         }
         print(json.dumps(line), flush=True)
     ctx.close()
