@@ -61,6 +61,13 @@ def parse():
                     help="time the CPU baseline table (configurations 1-3, one core and all "
                          "cores, with and without contraction) and exit")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--sweep", choices=["split", "fused"], default="split",
+                    help="sweep kernels of the headline: split (reconstruction + Riemann over "
+                         "an interface-state scratch) or fused (one face kernel)")
+    ap.add_argument("--no-tolerance-check", action="store_true",
+                    help="with --variant fast: skip the check against the oracle (profiling)")
+    ap.add_argument("--no-variants", action="store_true",
+                    help="skip timing the other build (profiling)")
     ap.add_argument("--variant", choices=["auto", "exact", "fast"], default="auto",
                     help="library build of the headline: exact (bit-identical to the oracle), "
                          "fast (tolerance mode), or auto: fast when it passes the tolerance "
@@ -751,11 +758,17 @@ def tolerance_check(ctx, nsteps=100, size=64, seed=11):
             "seconds": time.perf_counter() - t0}
 
 
-def time_variant(ctx, g, hp, f_host, dev, stream, steps=5, warmup=3):
-    """ms per step (event-timed) and the per-sweep stage split of one build on the
-    benchmark workload, from the same initial state."""
+def args_sweep_mode():
+    """The headline's sweep mode (set once the arguments are parsed)."""
+    return getattr(args_sweep_mode, "mode", "split")
+
+
+def time_variant(ctx, g, hp, f_host, dev, stream, steps=5, warmup=3, sweep="split"):
+    """ms per step (event-timed) and the per-sweep stage split of one build and sweep
+    mode on the benchmark workload, from the same initial state."""
     import torch
     from ppm_b200 import capi
+    ctx.set_sweep_mode(sweep)
     fields = {k: torch.from_numpy(v).to(dev) for k, v in f_host.items()}
     dt_dev = torch.zeros(1, dtype=torch.float64, device=dev)
     ctx.compute_timestep(g, hp, fields, memory=capi.MEM_DEVICE, dt_device=dt_dev,
@@ -787,6 +800,7 @@ def time_variant(ctx, g, hp, f_host, dev, stream, steps=5, warmup=3):
         raise RuntimeError(f"{ctx.variant} steps failed: {capi.error_string(rc)}")
     ms = ev0.elapsed_time(ev1) / steps
     del fields
+    ctx.set_sweep_mode(args_sweep_mode())
     return {"ms_per_step": ms, "zone_updates_per_s": g.active_cells / (ms * 1e-3),
             "sweep_ms": sweep_ms / max(nsweep, 1),
             "stage_ms_per_sweep": {k: v / max(nsweep, 1) for k, v in stages.items()},
@@ -814,7 +828,7 @@ def run_ours(args):
     # oracle (checked here, every rank), else the bit-exact build
     tol = None
     variant = args.variant
-    if variant in ("auto", "fast"):
+    if variant == "auto" or (variant == "fast" and not args.no_tolerance_check):
         ctx_fast = capi.Context(local, stream=stream.cuda_stream, variant="fast")
         tol = tolerance_check(ctx_fast)
         ctx_fast.close()
@@ -824,6 +838,8 @@ def run_ours(args):
         if variant == "auto":
             variant = "fast" if ok.item() > 0 else "exact"
     ctx = capi.Context(local, stream=stream.cuda_stream, variant=variant)
+    ctx.set_sweep_mode(args.sweep)
+    args_sweep_mode.mode = args.sweep
 
     hp = H.HydroParams(gamma=5.0 / 3.0, cfl=0.4, dual=True, riemann=RIEMANN[args.riemann])
     # One GPU: a periodic size^3 grid.  N GPUs: a size x size x (N size) periodic grid cut
@@ -976,16 +992,20 @@ def run_ours(args):
 
     # both builds on the same initial state, a few steps each
     variants = None
-    if world == 1 and args.colours == 0:
+    if world == 1 and args.colours == 0 and not args.no_variants:
         variants = {}
         for name in ("exact", "fast"):
             c = ctx if name == variant else capi.Context(local, stream=stream.cuda_stream,
                                                          variant=name)
-            variants[name] = time_variant(c, g, hp, f_host, dev, stream)
+            for sweep in ("split", "fused"):
+                key = name if sweep == "split" else f"{name}_fused"
+                variants[key] = time_variant(c, g, hp, f_host, dev, stream, sweep=sweep)
             if c is not ctx:
                 c.close()
         variants["fast_vs_exact"] = (variants["fast"]["zone_updates_per_s"] /
                                      variants["exact"]["zone_updates_per_s"])
+        variants["fused_vs_split"] = (variants[f"{variant}_fused"]["zone_updates_per_s"] /
+                                      variants[variant]["zone_updates_per_s"])
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -1013,7 +1033,7 @@ def run_ours(args):
             "config": dict(workload_config(args),
                            parallelism=("one grid" if world == 1 else
                                         f"z slabs x{world}, NCCL halo exchange + dt MIN"),
-                           build=variant),
+                           build=variant, sweep=args.sweep),
             "build": {"variant": variant,
                       "flags": ("nvcc -fmad=false (bit-identical to the FP64 oracle)"
                                 if variant == "exact" else

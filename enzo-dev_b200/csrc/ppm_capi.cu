@@ -190,6 +190,7 @@ struct ppm_b200_context {
   // level schedule (ppm_b200_set_level_config / the autotuner) and the Riemann settings
   // of the batch being prepared (prepare_sweep reads them)
   ppm_b200_level_config level{};
+  int sweep_mode = PPM_B200_SWEEP_SPLIT;  // ppm_b200_set_sweep_mode
   int wave_rt = ppm::kRiemannThreads;
   int wave_persist = 0;
   // event timing of sweep launches
@@ -677,7 +678,10 @@ int prepare_sweep(ppm_b200_context* ctx, int dim, int position, const ppm_b200_p
   const bool persist = plain_riemann && ctx->wave_persist != 0;
   // face scratch: planes of every grid, then the flagged-pencil list
   std::vector<SweepArgs> rec(ng);
-  std::vector<int64_t> mpre(ng + 1, 0), rpre(ng + 1, 0);
+  std::vector<int64_t> mpre(ng + 1, 0), rpre(ng + 1, 0), fpre(ng + 1, 0);
+  // the fused face kernel serves the same plain two-shock path, without slope corrections
+  const bool fused = plain_riemann && ctx->sweep_mode == PPM_B200_SWEEP_FUSED &&
+                     correction_planes(p) == 0;
   size_t scratch_doubles = 0, flag_bytes = 0;
   int64_t total_pencils = 0;
   // colour field pointers of every grid, ncolour per grid
@@ -721,6 +725,7 @@ int prepare_sweep(ppm_b200_context* ctx, int dim, int position, const ppm_b200_p
     const int64_t rb = (int64_t)(a.ie - a.is + 2) * ((a.npencils + rt - 1) / rt);
     mpre[k + 1] = mpre[k] + mb;
     rpre[k + 1] = rpre[k] + rb;
+    fpre[k + 1] = fpre[k] + ppm::face_blocks(a.npencils, a.is, a.ie);
   }
   // callers that queue several sweeps size the scratch for all of them first, so this
   // never moves the buffer under a sweep prepared earlier
@@ -838,6 +843,9 @@ int prepare_sweep(ppm_b200_context* ctx, int dim, int position, const ppm_b200_p
   const size_t off_r = align256(img.size());
   img.resize(off_r);
   append(img, rpre.data(), rpre.size());
+  const size_t off_f = align256(img.size());
+  img.resize(off_f);
+  append(img, fpre.data(), fpre.size());
   const int slot = kSlotSweep0 + 3 * dim + position;
   rc = mirror_put(ctx, ctx->mirror[slot], img);
   if (rc) return rc;
@@ -864,6 +872,9 @@ int prepare_sweep(ppm_b200_context* ctx, int dim, int position, const ppm_b200_p
   plan.B.riemann_threads = rt;
   plan.B.persistent = persist ? 1 : 0;
   plan.B.riemann_total = rpre[ng];
+  plan.B.fused = fused ? 1 : 0;
+  plan.B.face_prefix = (const int64_t*)(base + off_f);
+  plan.B.face_blocks = fpre[ng];
   if (persist)
     plan.riemann_blocks = std::min<int64_t>(
         rpre[ng], (int64_t)ctx->sms *
@@ -1070,7 +1081,12 @@ int prepare_elem(ppm_b200_context* ctx, int slot, const ppm_b200_params* p,
 // device copies of host fields (copied in here; single grid only).
 // colours: also the colour fields (the sweeps; the other entry points do not read them).
 int stage_in(ppm_b200_context* ctx, const ppm_b200_params* p, ppm_b200_grid* g, int memory,
-             FieldSet& fs, const double* acc[3], bool colours = false) {
+             FieldSet& fs, const double* acc[3], bool colours = false, bool need_acc = false) {
+  // the accelerations: read by the sweeps alone, which need one per axis under gravity
+  const bool with_acc = need_acc && p->gravity;
+  if (with_acc)
+    for (int k = 0; k < g->rank; ++k)
+      if (!g->acceleration[k]) return PPM_B200_ERR_INVALID;
   double* src[6] = {g->density, g->total_energy, g->velocity[0],
                     g->rank > 1 ? g->velocity[1] : nullptr,
                     g->rank > 2 ? g->velocity[2] : nullptr,
@@ -1080,7 +1096,7 @@ int stage_in(ppm_b200_context* ctx, const ppm_b200_params* p, ppm_b200_grid* g, 
   fs.ncol = colours ? p->number_of_colours : 0;
   if (memory == PPM_B200_MEM_DEVICE) {
     for (int k = 0; k < 6; ++k) fs.f[k] = src[k];
-    for (int k = 0; k < g->rank; ++k) acc[k] = p->gravity ? g->acceleration[k] : nullptr;
+    for (int k = 0; k < g->rank; ++k) acc[k] = with_acc ? g->acceleration[k] : nullptr;
     for (int n = 0; n < fs.ncol; ++n) fs.col[n] = g->colours[n];
     return PPM_B200_OK;
   }
@@ -1102,7 +1118,7 @@ int stage_in(ppm_b200_context* ctx, const ppm_b200_params* p, ppm_b200_grid* g, 
     CK(cudaMemcpyAsync(ctx->host_set[k].p, src[k], bytes, cudaMemcpyHostToDevice, ctx->stream));
     fs.f[k] = (double*)ctx->host_set[k].p;
   }
-  if (p->gravity) {
+  if (with_acc) {
     for (int k = 0; k < g->rank; ++k) {
       int rc = ensure(ctx, ctx->host_acc[k], bytes);
       if (rc) return rc;
@@ -1436,6 +1452,9 @@ std::string graph_key(ppm_b200_context* ctx, const ppm_b200_params* p, const Sol
     key_put(k, b.riemann_threads);
     key_put(k, b.persistent);
     key_put(k, b.riemann_total);
+    key_put(k, b.fused);
+    key_put(k, b.face_prefix);
+    key_put(k, b.face_blocks);
     key_put(k, ctx->mirror[kSlotSweep0 + 3 * sp.order[s] + s].version);
   }
   return k;
@@ -1602,6 +1621,13 @@ int ppm_b200_device_bytes(ppm_b200_context* ctx, long long* bytes) {
   for (const auto& bank : ctx->banks)
     for (const auto& m : *bank) n += m.dev.bytes;
   *bytes = (long long)n;
+  return PPM_B200_OK;
+}
+
+int ppm_b200_set_sweep_mode(ppm_b200_context* ctx, int mode) {
+  if (!ctx || (mode != PPM_B200_SWEEP_SPLIT && mode != PPM_B200_SWEEP_FUSED))
+    return PPM_B200_ERR_INVALID;
+  ctx->sweep_mode = mode;
   return PPM_B200_OK;
 }
 
@@ -1795,7 +1821,7 @@ int ppm_b200_solve_ppm_de(ppm_b200_context* ctx, const ppm_b200_params* p, int c
   const long long* ggs = ggs_in ? ggs_in : zero3;
   std::vector<GridIO> io(1);
   io[0].g = g;
-  rc = stage_in(ctx, p, g, memory, io[0].user, io[0].acc, true);
+  rc = stage_in(ctx, p, g, memory, io[0].user, io[0].acc, true, true);
   if (rc) return rc;
   SolvePlan sp;
   rc = prepare_solve(ctx, p, cycle_number, io, nsub, sub, ggs, sp);
@@ -1835,7 +1861,8 @@ int ppm_b200_solve_level(ppm_b200_context* ctx, const ppm_b200_params* p, int cy
   std::vector<GridIO> io(ngrids);
   for (int k = 0; k < ngrids; ++k) {
     io[k].g = &grids[idx[k]];
-    rc = stage_in(ctx, p, &grids[idx[k]], PPM_B200_MEM_DEVICE, io[k].user, io[k].acc, true);
+    rc = stage_in(ctx, p, &grids[idx[k]], PPM_B200_MEM_DEVICE, io[k].user, io[k].acc, true,
+                  true);
     if (rc) return rc;
   }
   // the level's waves (one for the batched schedule without a scratch bound), each
@@ -1919,7 +1946,7 @@ int ppm_b200_euler_sweep(ppm_b200_context* ctx, int dim, const ppm_b200_params* 
   const long long* ggs = ggs_in ? ggs_in : zero3;
   std::vector<GridIO> io(1);
   io[0].g = g;
-  rc = stage_in(ctx, p, g, memory, io[0].user, io[0].acc, true);
+  rc = stage_in(ctx, p, g, memory, io[0].user, io[0].acc, true, true);
   if (rc) return rc;
   rc = assign_scratch(ctx, io);
   if (rc) return rc;

@@ -160,16 +160,10 @@ __global__ void __launch_bounds__(kMarchThreads) corrections_kernel(const __grid
 #define PPM_RECON0_MINBLOCKS PPM_RECON_MINBLOCKS
 #endif
 // COR: the batch carries slope corrections (the coefficients of the corrections kernel).
-template <bool DUAL, bool GRAV, int ROLE, bool ONE, bool COR = false>
-__global__ void __launch_bounds__(kMarchThreads,
-                                  ROLE == 0 ? PPM_RECON0_MINBLOCKS : PPM_RECON_MINBLOCKS)
-    reconstruct_kernel(const __grid_constant__ BatchArgs B) {
+// One pencil's march (the body of the reconstruct kernels).
+template <bool DUAL, bool GRAV, int ROLE, bool COR>
+__device__ __forceinline__ void reconstruct_pencil(const SweepArgs& a, int64_t pid) {
   constexpr int NV = (ROLE == 0) ? 3 : (DUAL ? 3 : 2);
-  int64_t lb;
-  const int g = locate<ONE>(B.march_prefix, B.ngrids, lb);
-  PPM_BIND_RECORD(a, g)
-  const int64_t pid = lb * kMarchThreads + threadIdx.x;
-  if (pid >= a.npencils) return;
   const Phys P = make_phys(a);
   const int64_t base = (pid % a.n1) * a.s1 + (pid / a.n1) * a.s2;
   const int64_t sa = a.sa;
@@ -368,6 +362,30 @@ __global__ void __launch_bounds__(kMarchThreads,
   }
 }
 
+// FLAG: only the pencils of the batch's flagged list (the fused sweep's fallback pass,
+// which needs the interface states of those pencils): a fixed grid walks the list.
+template <bool DUAL, bool GRAV, int ROLE, bool ONE, bool COR = false, bool FLAG = false>
+__global__ void __launch_bounds__(kMarchThreads,
+                                  ROLE == 0 ? PPM_RECON0_MINBLOCKS : PPM_RECON_MINBLOCKS)
+    reconstruct_kernel(const __grid_constant__ BatchArgs B) {
+  if (FLAG) {
+    const unsigned long long nflag = *(volatile unsigned long long*)&B.counters[kCntFlagged];
+    for (unsigned long long k = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+         k < nflag; k += (unsigned long long)gridDim.x * blockDim.x) {
+      const int64_t code = B.flagged[k];
+      const SweepArgs& a = ONE ? B.one : B.grids[(int)(code >> 40)];
+      reconstruct_pencil<DUAL, GRAV, ROLE, COR>(a, code & ((int64_t(1) << 40) - 1));
+    }
+    return;
+  }
+  int64_t lb;
+  const int g = locate<ONE>(B.march_prefix, B.ngrids, lb);
+  PPM_BIND_RECORD(a, g)
+  const int64_t pid = lb * kMarchThreads + threadIdx.x;
+  if (pid >= a.npencils) return;
+  reconstruct_pencil<DUAL, GRAV, ROLE, COR>(a, pid);
+}
+
 template <bool DUAL>
 __device__ __forceinline__ FaceState load_face(const SweepArgs& a, int64_t idx) {
   const double* s = a.fstate + idx;
@@ -550,6 +568,250 @@ __global__ void __launch_bounds__(RT, (LEARNED ? PPM_RIEMANN_LEARNED_MINBLOCKS
   }
   if (LEARNED && threadIdx.x == 9 && s_rejected)
     atomicAdd(&B.counters[kCntGuessRejected], (unsigned long long)s_rejected);
+  if (threadIdx.x == 10 && s_warps) {
+    atomicAdd(&B.counters[kCntWarpNewton], (unsigned long long)s_wtrips);
+    atomicAdd(&B.counters[kCntWarps], (unsigned long long)s_warps);
+  }
+}
+
+// ------------------------------------------------------------------ stages 1+2 fused
+// The interface states and the two-shock solution of every face in one kernel (the plain
+// path: two-shock solver, acoustic start, no colours or slope corrections), so the
+// twelve state planes never leave the chip; only the seven flux planes are written.
+// A warp takes one pencil and kFaceSeg consecutive faces f0 .. f0+30: lane l holds cell
+// c = f0 - 1 + l, reconstructs its parabolas (the neighbours' cells, slopes and edges
+// arrive by warp shuffles; lane 0 computes the slope left of its cell and lane 31 the
+// slope and edge right of its cell itself) and the contributions of that cell to its two
+// faces; lane l >= 1 then assembles face c from lane l-1's left-side data and its own,
+// solves its Riemann problem and writes its fluxes.  Each cell's work is done once, plus
+// one extra cell per 31 faces.  The per-point arithmetic is the split kernels', so the
+// fluxes are the same bits.
+#ifndef PPM_FACE_MINBLOCKS
+#define PPM_FACE_MINBLOCKS 2
+#endif
+
+__device__ __forceinline__ double shfl_up1(double v) { return __shfl_up_sync(0xffffffffu, v, 1); }
+__device__ __forceinline__ double shfl_dn1(double v) { return __shfl_down_sync(0xffffffffu, v, 1); }
+
+// Parabolas of one cell for three variables from the cell values of every lane's cell
+// (q), the slope left of lane 0's cell and right of lane 31's cell, and the coefficients.
+// Returns the parabolas; qm: the left neighbour's value (for the caller).
+template <int NV>
+__device__ __forceinline__ void face_parabolas(const double q[3], const double qm[3],
+                                               const double qp[3], const double qmm[3],
+                                               const double qpp[3], const Coef& cf,
+                                               const Coef& cfm, const Coef& cfp, int lane,
+                                               Para pa[3]) {
+#pragma unroll
+  for (int v = 0; v < 3; ++v) pa[v] = Para{0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    const double dq = pm_slope(qm[v], q[v], qp[v], cf.c1, cf.c2);
+    double dqm = shfl_up1(dq);
+    double dqp = shfl_dn1(dq);
+    if (lane == 0) dqm = pm_slope(qmm[v], qm[v], q[v], cfm.c1, cfm.c2);
+    if (lane == 31) dqp = pm_slope(q[v], qp[v], qpp[v], cfp.c1, cfp.c2);
+    const double ql = pm_edge(qm[v], q[v], dqm, dq, cf.c3, cf.c4, cf.c5, cf.c6);
+    double qr = shfl_dn1(ql);
+    if (lane == 31) qr = pm_edge(q[v], qp[v], dq, dqp, cfp.c3, cfp.c4, cfp.c5, cfp.c6);
+    pa[v] = pm_parabola(qm[v], q[v], qp[v], ql, qr);
+  }
+}
+
+template <bool DUAL, bool GRAV, bool ONE>
+__global__ void __launch_bounds__(kFaceThreads, PPM_FACE_MINBLOCKS)
+    face_kernel(const __grid_constant__ BatchArgs B) {
+  __shared__ unsigned int s_hist[8];
+  __shared__ unsigned int s_newton, s_wtrips, s_warps;
+  if (threadIdx.x < 8) s_hist[threadIdx.x] = 0u;
+  if (threadIdx.x == 0) {
+    s_newton = 0u;
+    s_wtrips = 0u;
+    s_warps = 0u;
+  }
+  int64_t lb;
+  const int g = locate<ONE>(B.face_prefix, B.ngrids, lb);
+  PPM_BIND_RECORD(a, g)
+  if (ONE) __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int is = a.is, ie = a.ie, n = a.n;
+  const int64_t nseg = face_segments(is, ie);
+  const int64_t grp = lb / nseg;
+  const int f0 = is + (int)(lb - grp * nseg) * kFaceSeg;
+  const int64_t pid = grp * kFaceWarps + (threadIdx.x >> 5);
+  const bool pencil_ok = pid < a.npencils;  // warp-uniform
+  const Phys P = make_phys(a);
+  const int64_t base = pencil_ok ? (pid % a.n1) * a.s1 + (pid / a.n1) * a.s2 : 0;
+  const int c = f0 - 1 + lane;  // this lane's cell; lanes >= 1: also the face of that index
+  // cells beyond the pencil (past the last face's neighbours) are clamped: their results
+  // are never used
+  auto cl = [&](int i) { return i < 0 ? 0 : (i > n - 1 ? n - 1 : i); };
+  auto ld = [&](const double* f, int i) -> double {
+    return (f && pencil_ok) ? __ldg(f + base + (int64_t)cl(i) * a.sa) : 0.0;
+  };
+  const Coef cf = a.coef[cl(c)];
+  const Coef cfm = a.coef[cl(c - 1)];
+  const Coef cfp = a.coef[cl(c + 1)];
+
+  // ---- density, pressure, normal velocity: parabolas, characteristic corrections
+  const double* vA[3] = {a.in_d, a.pres, a.in_u};
+  double q[3], qm[3], qp[3], qmm[3], qpp[3];
+#pragma unroll
+  for (int v = 0; v < 3; ++v) {
+    q[v] = ld(vA[v], c);
+    qm[v] = shfl_up1(q[v]);
+    qp[v] = shfl_dn1(q[v]);
+    qmm[v] = qpp[v] = 0.0;
+    if (lane == 0) {
+      qm[v] = ld(vA[v], c - 1);
+      qmm[v] = ld(vA[v], c - 2);
+    }
+    if (lane == 31) {
+      qp[v] = ld(vA[v], c + 1);
+      qpp[v] = ld(vA[v], c + 2);
+    }
+  }
+  const double u_c = q[2], u_m = qm[2];  // uslice(c), uslice(c-1) for the upwinding
+  Para pa[3];
+  face_parabolas<3>(q, qm, qp, qmm, qpp, cf, cfm, cfp, lane, pa);
+  const Prep pr = cell_prep(q[0], q[1], q[2], cf.dx2i, P);
+  // right-side data of face c, left-side data of face c+1 (inteuler.F:304-316)
+  CoreR R;
+  R.dra = pm_C(pa[0], pr.char2);
+  R.dr0 = pm_B(pa[0], pr.c0);
+  R.pra = pm_C(pa[1], pr.char2);
+  R.pr0 = pm_B(pa[1], pr.c0);
+  R.prm = pm_B(pa[1], pr.cm);
+  R.prp = pm_B(pa[1], pr.cp);
+  R.ura = pm_C(pa[2], pr.char2);
+  R.ur0 = pm_B(pa[2], pr.c0);
+  R.urm = pm_B(pa[2], pr.cm);
+  R.urp = pm_B(pa[2], pr.cp);
+  R.cm = pr.cm;
+  R.c0 = pr.c0;
+  R.cp = pr.cp;
+  CoreL L;  // of this cell, then moved to the right neighbour lane
+  L.dla = shfl_up1(pm_A(pa[0], pr.char1));
+  L.dl0 = shfl_up1(pm_A(pa[0], pr.c0));
+  L.pla = shfl_up1(pm_A(pa[1], pr.char1));
+  L.pl0 = shfl_up1(pm_A(pa[1], pr.c0));
+  L.plm = shfl_up1(pm_A(pa[1], pr.cm));
+  L.plp = shfl_up1(pm_A(pa[1], pr.cp));
+  L.ula = shfl_up1(pm_A(pa[2], pr.char1));
+  L.ul0 = shfl_up1(pm_A(pa[2], pr.c0));
+  L.ulm = shfl_up1(pm_A(pa[2], pr.cm));
+  L.ulp = shfl_up1(pm_A(pa[2], pr.cp));
+  L.cm = shfl_up1(pr.cm);
+  L.c0 = shfl_up1(pr.c0);
+  L.cp = shfl_up1(pr.cp);
+  double gsum = 0.0;
+  if (GRAV) {
+    const double gc = ld(a.grav, c);
+    gsum = shfl_up1(gc) + gc;  // grslice(c-1) + grslice(c)
+  }
+  const bool face_ok = pencil_ok && lane >= 1 && c <= ie + 1;
+  const CoreState cs = face_core<DUAL, GRAV>(L, R, gsum, P);
+
+  // ---- the two-shock solution (twoshock.F:156-254)
+  FaceState st = FaceState{1.0, 1.0, 1.0, 1.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  if (face_ok) {
+    st.dl = cs.dl; st.dr = cs.dr; st.pl = cs.pl; st.pr = cs.pr; st.ul = cs.ul; st.ur = cs.ur;
+  }
+  Riemann rs = {0.0, 0.0, 0, true};
+  const int64_t np = a.npencils, plane = a.plane;
+  const int64_t idx = (int64_t)(c - is) * np + pid;
+  unsigned trips = 0;
+  if (face_ok) {
+    const double clr = sqrt(P.gamma * st.pl * st.dl);
+    const double crr = sqrt(P.gamma * st.pr * st.dr);
+    rs = twoshock_newton(st, clr, crr, acoustic_guess(st, clr, crr, P), P);
+    trips = (unsigned)rs.iters;
+    if (a.log && a.log_stride > 0) {
+      const unsigned long long h =
+          ((unsigned long long)idx + 0x9E3779B97F4A7C15ull * (unsigned long long)(g + 1)) *
+          0xD1B54A32D192ED03ull;
+      if ((h >> 40) % (unsigned long long)a.log_stride == 0) {
+        const unsigned long long slot = atomicAdd(a.log_count, 1ull);
+        if (slot < (unsigned long long)a.log_cap) {
+          double* r = a.log + slot * 8;
+          r[0] = st.dl; r[1] = st.dr; r[2] = st.pl; r[3] = st.pr;
+          r[4] = st.ul; r[5] = st.ur; r[6] = rs.pbar;
+          r[7] = rs.converged ? (double)rs.iters : -(double)rs.iters;
+        }
+      }
+    }
+    atomicAdd(&s_hist[rs.iters & 7], 1u);
+    atomicAdd(&s_newton, (unsigned)rs.iters);
+  }
+  {
+    const unsigned wmax = __reduce_max_sync(0xffffffffu, trips);
+    const unsigned any = __ballot_sync(0xffffffffu, face_ok);
+    if (lane == 0 && any != 0u) {
+      atomicAdd(&s_wtrips, wmax);
+      atomicAdd(&s_warps, 1u);
+    }
+  }
+
+  // ---- transverse velocities and gas energy: parabolas and upwinded states
+  constexpr int NB = DUAL ? 3 : 2;
+  const double* vB[3] = {a.in_v, a.in_w, DUAL ? a.in_ge : nullptr};
+#pragma unroll
+  for (int v = 0; v < 3; ++v) {
+    q[v] = ld(vB[v], c);
+    qm[v] = shfl_up1(q[v]);
+    qp[v] = shfl_dn1(q[v]);
+    qmm[v] = qpp[v] = 0.0;
+    if (lane == 0) {
+      qm[v] = ld(vB[v], c - 1);
+      qmm[v] = ld(vB[v], c - 2);
+    }
+    if (lane == 31) {
+      qp[v] = ld(vB[v], c + 1);
+      qpp[v] = ld(vB[v], c + 2);
+    }
+  }
+  face_parabolas<NB>(q, qm, qp, qmm, qpp, cf, cfm, cfp, lane, pa);
+  AdvR AR;
+  AR.vra = pm_C(pa[0], pr.char2);
+  AR.vr0 = pm_B(pa[0], pr.c0);
+  AR.wra = pm_C(pa[1], pr.char2);
+  AR.wr0 = pm_B(pa[1], pr.c0);
+  AR.gera = DUAL ? pm_C(pa[2], pr.char2) : 0.0;
+  AR.ger0 = DUAL ? pm_B(pa[2], pr.c0) : 0.0;
+  AdvL AL;
+  AL.vla = shfl_up1(pm_A(pa[0], pr.char1));
+  AL.vl0 = shfl_up1(pm_A(pa[0], pr.c0));
+  AL.wla = shfl_up1(pm_A(pa[1], pr.char1));
+  AL.wl0 = shfl_up1(pm_A(pa[1], pr.c0));
+  AL.gela = shfl_up1(DUAL ? pm_A(pa[2], pr.char1) : 0.0);
+  AL.gel0 = shfl_up1(DUAL ? pm_A(pa[2], pr.c0) : 0.0);
+  const AdvState as = face_advected(AL, AR, u_m, u_c);
+
+  // ---- the Godunov flux (flux_twoshock.F:84-396)
+  if (face_ok) {
+    st.vl = as.vl; st.vr = as.vr; st.wl = as.wl; st.wr = as.wr;
+    st.gel = DUAL ? as.gel : 0.0;
+    st.ger = DUAL ? as.ger : 0.0;
+    const double qc = P.dt / cf.dx;
+    const Flux F = flux_twoshock<DUAL>(st, rs.pbar, rs.ubar, qc, P);
+    double* o = a.fflux + idx;
+    o[XDF * plane] = F.df;
+    o[XEF * plane] = F.ef;
+    o[XUF * plane] = F.uf;
+    o[XVF * plane] = F.vf;
+    o[XWF * plane] = F.wf;
+    if (DUAL) o[XGEF * plane] = F.gef;
+    o[XUB * plane] = F.ub;
+  }
+  __syncthreads();
+  if (threadIdx.x < 8 && s_hist[threadIdx.x])
+    atomicAdd(&B.counters[kCntHist0 + threadIdx.x], (unsigned long long)s_hist[threadIdx.x]);
+  if (threadIdx.x == 8 && s_newton) {
+    unsigned long long nif = 0;
+    for (int h = 0; h < 8; ++h) nif += s_hist[h];
+    atomicAdd(&B.counters[kCntInterfaces], nif);
+    atomicAdd(&B.counters[kCntNewton], (unsigned long long)s_newton);
+  }
   if (threadIdx.x == 10 && s_warps) {
     atomicAdd(&B.counters[kCntWarpNewton], (unsigned long long)s_wtrips);
     atomicAdd(&B.counters[kCntWarps], (unsigned long long)s_warps);
@@ -1650,6 +1912,25 @@ void launch_stages(const BatchArgs& B, int64_t march_blocks, int64_t riemann_blo
   };
   mark(0);
   cudaMemsetAsync(B.counters + kCntFlagged, 0, sizeof(unsigned long long), st);
+  if (B.fused) {  // the plain path with the fused face kernel
+    face_kernel<DUAL, GRAV, ONE><<<(unsigned)B.face_blocks, kFaceThreads, 0, st>>>(B);
+    mark(1);
+    mark(2);
+    mark(3);
+    if (PPM_X_TMA && staged && ONE && B.x_tma)
+      launch_update<DUAL, GRAV, ONE, true, ONE>(B, march_blocks, st);
+    else if (staged)
+      launch_update<DUAL, GRAV, ONE, true, false>(B, march_blocks, st);
+    else
+      launch_update<DUAL, GRAV, ONE, false, false>(B, march_blocks, st);
+    mark(4);
+    // the flagged pencils' interface states, then their per-cell HLL fallback
+    reconstruct_kernel<DUAL, GRAV, 0, ONE, false, true><<<64, kMarchThreads, 0, st>>>(B);
+    reconstruct_kernel<DUAL, GRAV, 1, ONE, false, true><<<64, kMarchThreads, 0, st>>>(B);
+    fallback_kernel<DUAL, GRAV, ONE><<<64, 128, 0, st>>>(B);
+    mark(5);
+    return;
+  }
   if (B.ncolour > 0) cudaMemsetAsync(B.hll_flags, 0, (size_t)B.hll_bytes, st);
   if (B.corrections || B.ncolour > 0 || B.presfree) {  // colours, PressureFree: COR too
     if (B.corrections)

@@ -177,8 +177,29 @@ struct BatchArgs {
   int riemann_threads = kRiemannThreads;
   int persistent = 0;
   int64_t riemann_total = 0;
+  // fused sweep (two-shock with the plain start, no colours or slope corrections): one
+  // kernel reconstructs the interface states and solves the Riemann problems of a
+  // (group of kFaceWarps pencils, segment of kFaceSeg faces) per block; face_prefix is
+  // its block prefix table
+  int fused = 0;
+  const int64_t* face_prefix = nullptr;
+  int64_t face_blocks = 0;
   CUtensorMap xin[6];
 };
+
+// The fused face kernel: a warp takes one pencil and kFaceSeg consecutive faces, lane
+// l >= 1 the face of cell f0 - 1 + l (lane 0 the cell left of the first face); a block
+// takes kFaceWarps consecutive pencils.
+#ifndef PPM_FACE_WARPS
+#define PPM_FACE_WARPS 8
+#endif
+enum { kFaceWarps = PPM_FACE_WARPS, kFaceThreads = 32 * PPM_FACE_WARPS, kFaceSeg = 31 };
+__host__ __device__ inline int64_t face_segments(int is, int ie) {
+  return (ie - is + 2 + kFaceSeg - 1) / kFaceSeg;
+}
+__host__ __device__ inline int64_t face_blocks(int64_t npencils, int is, int ie) {
+  return ((npencils + kFaceWarps - 1) / kFaceWarps) * face_segments(is, ie);
+}
 
 // TMA tiles of the x sweep's update kernel: a warp's 32 pencils x 4 cells (32 bytes a
 // pencil), double-buffered per warp

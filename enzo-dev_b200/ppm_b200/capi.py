@@ -45,7 +45,7 @@ EXPORTS = (
     "ppm_b200_guess_adam", "ppm_b200_guess_eval", "ppm_b200_expansion_terms",
     "ppm_b200_expansion_terms_level", "ppm_b200_set_cfl", "ppm_b200_abi_check",
     "ppm_b200_set_level_config", "ppm_b200_get_level_config", "ppm_b200_autotune_level",
-    "ppm_b200_device_bytes",
+    "ppm_b200_device_bytes", "ppm_b200_set_sweep_mode",
 )
 
 GUESS_WEIGHTS = 4673  # W1[6][64] b1[64] W2[64][64] b2[64] w3[64] b3
@@ -210,6 +210,7 @@ def lib(build_if_missing: bool = True, variant: str | None = None):
     L.ppm_b200_set_graphs.argtypes = [vp, C.c_int]
     L.ppm_b200_set_level_config.argtypes = [vp, C.POINTER(LevelConfig)]
     L.ppm_b200_device_bytes.argtypes = [vp, C.POINTER(C.c_longlong)]
+    L.ppm_b200_set_sweep_mode.argtypes = [vp, C.c_int]
     L.ppm_b200_get_level_config.argtypes = [vp, C.POINTER(LevelConfig)]
     L.ppm_b200_autotune_level.argtypes = [vp, C.POINTER(Params), C.c_int, C.POINTER(GridDesc),
                                           C.c_int, C.POINTER(LevelTuning)]
@@ -499,6 +500,13 @@ class Context:
         if check and rc != OK:
             raise PPMError(rc, "ppm_b200_solve_level")
         return rc, st.as_dict()
+
+    def set_sweep_mode(self, mode):
+        """"split" (reconstruction and Riemann kernels over an interface-state scratch) or
+        "fused" (one face kernel); the same results."""
+        rc = self.L.ppm_b200_set_sweep_mode(self.h, {"split": 0, "fused": 1}[mode])
+        if rc != OK:
+            raise PPMError(rc, "ppm_b200_set_sweep_mode")
 
     def device_bytes(self):
         n = C.c_longlong(0)

@@ -214,18 +214,29 @@ def project_solution(parent, child, xp):
     parent.fields["d"][sl] = dsum * 0.125
 
 
+def ghost_map(parent, child):
+    """Flat indices of the child's ghost zones and of the parent zone each one takes its
+    value from (x fastest, as the fields are laid out)."""
+    idx = parent_index(child, parent)
+    m = ghost_mask(child)
+    kz, jy, ix = np.nonzero(m)
+    pd = parent.grid.dims
+    cd = child.grid.dims
+    child_flat = (kz * cd[1] + jy) * cd[0] + ix
+    parent_flat = (idx[kz] * pd[1] + idx[jy]) * pd[0] + idx[ix]
+    return child_flat.astype(np.int64), parent_flat.astype(np.int64)
+
+
 def fill_child_ghosts(parent, child, t, be):
     """SetBoundaryConditions for a subgrid: each ghost zone takes its parent zone's value,
     linear in time between the parent's old (t_old) and new (t) fields."""
-    idx = be.index(parent_index(child, parent))
-    mask = child.ghost_mask
+    gi, pi = child.ghosts
     span = parent.t - parent.t_old
     w = 0.0 if span <= 0.0 else (t - parent.t_old) / span
     for k, v in child.fields.items():
-        new = be.gather3(parent.fields[k], idx)
-        old = be.gather3(parent.old[k], idx)
-        val = old + w * (new - old)
-        v[mask] = val[mask]
+        new = parent.fields[k].reshape(-1)[pi]
+        old = parent.old[k].reshape(-1)[pi]
+        v.reshape(-1)[gi] = old + w * (new - old)
 
 
 def gravity_profile(root, cosmo, t):
@@ -246,15 +257,12 @@ def gravity_profile(root, cosmo, t):
 
 def level_accel(level, root, acc_root):
     """The root's acceleration profile, linearly interpolated (periodic) to a level's zone
-    centres, as the three acceleration arrays of the grid (x only)."""
+    centres (ghosts included): the x acceleration along the x axis."""
     xr = (np.arange(root.n) + 0.5) / root.n
     x = level.centres()
     xe = np.concatenate([xr - 1.0, xr, xr + 1.0])
     ae = np.concatenate([acc_root, acc_root, acc_root])
-    prof = np.interp(x, xe, ae)
-    shape = level.grid.shape
-    ax = np.ascontiguousarray(np.broadcast_to(prof[None, None, :], shape))
-    return [ax, np.zeros(shape), np.zeros(shape)]
+    return np.interp(x, xe, ae)
 
 
 # ---------------------------------------------------------------- the W cycle
@@ -268,9 +276,10 @@ class NestedRun:
         self.cosmo = cosmo
         self.max_expansion = max_expansion
         t0 = cosmo.t_init
-        for lev in levels:
+        for l, lev in enumerate(levels):
             lev.t = lev.t_old = t0
-            lev.ghost_mask = backend.mask(ghost_mask(lev))
+            if l > 0:
+                lev.ghosts = tuple(backend.index(a) for a in ghost_map(levels[l - 1], lev))
         self.root_steps = 0
         self.level_steps = [0] * len(levels)
         # a consistent start: the zones a subgrid covers are its projection (finest first)
@@ -343,7 +352,7 @@ class NestedRun:
         acc = gravity_profile(root, self.cosmo, root.t)
         for lev in self.levels:
             lev.own_fluxes = None
-            lev.accel = self.be.accel(level_accel(lev, root, acc))
+            lev.accel = self.be.accel(lev, level_accel(lev, root, acc))
         t_end = min(root.t + self._dt(root, math.inf), t_final)
         self._evolve(0, t_end, acc)
         self.root_steps += 1
@@ -370,9 +379,6 @@ class LibraryBackend:
     def adopt(self, levels):
         pass
 
-    def mask(self, m):
-        return m
-
     def copy(self, f):
         return {k: v.copy() for k, v in f.items()}
 
@@ -382,11 +388,13 @@ class LibraryBackend:
     def index(self, idx):
         return idx
 
-    def gather3(self, a, idx):
-        return a[np.ix_(idx, idx, idx)]
-
-    def accel(self, arrays):
-        return arrays
+    def accel(self, lev, prof):
+        """The grid's three acceleration arrays from the x profile (kept per level)."""
+        shape = lev.grid.shape
+        if getattr(lev, "accel_arrays", None) is None:
+            lev.accel_arrays = [np.zeros(shape), np.zeros(shape), np.zeros(shape)]
+        lev.accel_arrays[0][...] = prof[None, None, :]
+        return lev.accel_arrays
 
     def fill_periodic(self, lev):
         H.fill_ghosts(lev.grid, lev.fields, "periodic")
@@ -424,20 +432,20 @@ class DeviceBackend(LibraryBackend):
         for lev in levels:
             lev.fields = {k: t.from_numpy(v).to(self.device) for k, v in lev.fields.items()}
 
-    def mask(self, m):
-        return self.torch.from_numpy(m).to(self.device)
-
     def copy(self, f):
         return {k: v.clone() for k, v in f.items()}
 
     def index(self, idx):
         return self.torch.as_tensor(idx, dtype=self.torch.int64, device=self.device)
 
-    def gather3(self, a, idx):
-        return a[idx[:, None, None], idx[None, :, None], idx[None, None, :]]
-
-    def accel(self, arrays):
-        return [self.torch.from_numpy(a).to(self.device) for a in arrays]
+    def accel(self, lev, prof):
+        t = self.torch
+        shape = lev.grid.shape
+        if getattr(lev, "accel_arrays", None) is None:
+            lev.accel_arrays = [t.zeros(shape, dtype=t.float64, device=self.device)
+                                for _ in range(3)]
+        lev.accel_arrays[0].copy_(t.from_numpy(prof).to(self.device).view(1, 1, -1).expand(shape))
+        return lev.accel_arrays
 
     def fill_periodic(self, lev):
         self.ctx.set_boundary(lev.grid, lev.fields, self.hp.dual, ("periodic",) * 3)

@@ -235,6 +235,19 @@ int ppm_b200_solve_level(ppm_b200_context *ctx, const ppm_b200_params *params,
 /* enable != 0: replay level solves from CUDA graphs (see ppm_b200_solve_level). */
 int ppm_b200_set_graphs(ppm_b200_context *ctx, int enable);
 
+/* Which kernels run a directional sweep of the plain path (two-shock solver with the
+   acoustic start, no colours, no flattening or steepening; other paths always split).
+   PPM_B200_SWEEP_SPLIT: two marching reconstruction kernels write the interface states
+   of every face, a face-parallel Riemann kernel reads them and writes the fluxes.
+   PPM_B200_SWEEP_FUSED: one kernel reconstructs and solves every face (a warp per
+   pencil segment of 31 faces, neighbours by warp shuffles), so the interface states never
+   reach device memory.  Both give the same bits; the update and fallback kernels are
+   shared.  No reference counterpart (the reference runs one slice at a time,
+   Grid_xEulerSweep.C:196-305). */
+#define PPM_B200_SWEEP_SPLIT 0
+#define PPM_B200_SWEEP_FUSED 1
+int ppm_b200_set_sweep_mode(ppm_b200_context *ctx, int mode);
+
 /* How ppm_b200_solve_level schedules a level (no reference counterpart: the reference
    runs its grid loop, EvolveLevel.C:569-585, one grid at a time).
    schedule: PPM_B200_LEVEL_BATCHED -- every grid in one launch per kernel stage;
