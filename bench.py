@@ -183,9 +183,18 @@ def measured_peak_hbm():
     return 6650.0, "fallback 6.65 TB/s"
 
 
-def committed_fp64():
+def profile_file(variant, kind):
+    """The committed ncu summary of a build: the exact build's at 256^3, the tolerance
+    build's at 192^3 (per active cell, so the sizes compare)."""
+    if variant == "fast":
+        return REPO / "profiles" / "sweep_fast_turbulence192.json"
+    return REPO / "profiles" / ("sweep_fp64_turbulence256.json" if kind == "fp64"
+                                else "sweep_traffic_turbulence256.json")
+
+
+def committed_fp64(variant="exact"):
     """FP64 warp-instructions per active cell and sweep from the committed ncu summary."""
-    f = REPO / "profiles" / "sweep_fp64_turbulence256.json"
+    f = profile_file(variant, "fp64")
     if f.exists():
         try:
             d = json.loads(f.read_text())
@@ -195,9 +204,9 @@ def committed_fp64():
     return None, ""
 
 
-def committed_traffic():
+def committed_traffic(variant="exact"):
     """Per-zone-sweep DRAM bytes of the sweep kernel from the committed ncu summary."""
-    f = REPO / "profiles" / "sweep_traffic_turbulence256.json"
+    f = profile_file(variant, "traffic")
     if f.exists():
         try:
             d = json.loads(f.read_text())
@@ -392,7 +401,7 @@ def run_learned(ctx, g, hp, f_host, args, stream, f_dev=None, steps=None):
     steps = steps or max(1, min(args.steps, 5))
     out = {"steps": steps, "warmup": 2}
     finals = {}
-    for mode in ("plain", "learned"):
+    for mode in ("plain", "learned", "learned_tc"):
         if f_dev is not None:
             f = {k: v.clone() for k, v in f_dev.items()}
         else:
@@ -404,7 +413,8 @@ def run_learned(ctx, g, hp, f_host, args, stream, f_dev=None, steps=None):
             ctx.compute_timestep(g, hp, f, memory=capi.MEM_DEVICE, dt_device=dtd,
                                  want_host=False)
             ctx.solve_ppm_de(g, hp, 0.0, cyc, f, memory=capi.MEM_DEVICE, want_stats=False,
-                             dt_device=dtd, learned_guess=(mode == "learned"))
+                             dt_device=dtd,
+                             learned_guess={"plain": 0, "learned": 1, "learned_tc": 2}[mode])
             ctx.set_boundary(g, f, hp.dual, ("periodic",) * 3)
 
         for c in range(2):
@@ -441,6 +451,11 @@ def run_learned(ctx, g, hp, f_host, args, stream, f_dev=None, steps=None):
     out["max_rel_field_difference"] = worst
     out["speedup_learned_vs_plain"] = (out["learned"]["zone_updates_per_s"] /
                                        out["plain"]["zone_updates_per_s"])
+    out["speedup_learned_tc_vs_plain"] = (out["learned_tc"]["zone_updates_per_s"] /
+                                          out["plain"]["zone_updates_per_s"])
+    out["modes"] = {"learned": "the net inside the Riemann kernel (mma.sync m16n8k16)",
+                    "learned_tc": "a guess pass on the tcgen05 tensor cores (TMEM "
+                                  "accumulators) before the Riemann kernel"}
     del finals
     torch.cuda.empty_cache()
     return out
@@ -930,7 +945,7 @@ def run_ours(args):
     peak, peak_src = measured_peak_hbm()
     avg_sweep_s = sweep_ms * 1e-3 / max(nsweep, 1)
     achieved = (BYTES_PER_SWEEP_CELL + 16 * args.colours) * cells / avg_sweep_s / 1e9
-    tr, tr_src = committed_traffic()
+    tr, tr_src = committed_traffic(variant)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": (tr * cells if tr else None),
                 "kernel": "directional sweep (reconstruct x2, riemann, update, fallback)",
@@ -940,7 +955,7 @@ def run_ours(args):
                 "traffic_source": tr_src or None}
     # the bound that is active: FP64 issue (64 FP64 lanes = 2 warp-instructions per SM
     # and clock), from the committed per-cell instruction count and the sampled clock
-    fp, fp_src = committed_fp64()
+    fp, fp_src = committed_fp64(variant)
     if fp:
         sms = torch.cuda.get_device_properties(dev).multi_processor_count
         mhz = clocks.get("sm_mhz") or clocks.get("sm_max_mhz") or 1965.0

@@ -76,6 +76,8 @@ cudaError_t launch_guess_adam(float* W, float* grad, float* m, float* v, int ste
                               float beta1, float beta2, float eps, cudaStream_t st);
 cudaError_t launch_guess_eval(const uint32_t* packed, const float* feats, int64_t n, float* y,
                               cudaStream_t st);
+cudaError_t launch_guess_eval_tc(const uint32_t* words, const float* feats, int64_t n, float* y,
+                                 unsigned long long* timeouts, int sms, cudaStream_t st);
 void launch_pressure_batch(const ElemBatch& B, int64_t blocks, cudaStream_t st);
 void launch_timestep_batch(const ElemBatch& B, int64_t blocks, double courant, double* dt_out,
                            cudaStream_t st);
@@ -330,6 +332,7 @@ int check_supported(const ppm_b200_params* p) {
       (p->steepening != 0 && p->steepening != 1))
     return PPM_B200_ERR_UNSUPPORTED;
   // the solver switch of Grid_xEulerSweep.C:223-283 (two-shock, HLL, HLLC)
+  if (p->learned_guess < 0 || p->learned_guess > 2) return PPM_B200_ERR_UNSUPPORTED;
   if (p->riemann_solver != PPM_B200_RIEMANN_TWOSHOCK && p->riemann_solver != PPM_B200_RIEMANN_HLL &&
       p->riemann_solver != PPM_B200_RIEMANN_HLLC)
     return PPM_B200_ERR_UNSUPPORTED;
@@ -380,6 +383,35 @@ uint16_t bf16_bits(float x) {
 
 uint32_t bf16_pair(float lo, float hi) {
   return (uint32_t)bf16_bits(lo) | ((uint32_t)bf16_bits(hi) << 16);
+}
+
+// The tcgen05 image (ppm_guess.cuh kTc*) appended at word kTcWordOffset.
+void pack_guess_tc(const float* w, std::vector<uint32_t>& out) {
+  using namespace ppm;
+  out.resize(kGuessBufferWords, 0u);
+  unsigned char* img = reinterpret_cast<unsigned char*>(out.data() + kTcWordOffset);
+  auto put_b = [&](int base, int N, int n, int k, float v) {
+    const uint16_t h = bf16_bits(v);
+    const size_t off = (size_t)base + (size_t)((k / 8) * (N / 8) + n / 8) * 128 +
+                       (size_t)(n % 8) * 16 + (size_t)(k % 8) * 2;
+    std::memcpy(img + off, &h, 2);
+  };
+  for (int n = 0; n < kGuessHidden; ++n)
+    for (int k = 0; k < 16; ++k)
+      put_b(kTcW1, kGuessHidden, n, k, k < kGuessIn ? w[kOffW1 + k * kGuessHidden + n] : 0.0f);
+  for (int n = 0; n < kGuessHidden; ++n)
+    for (int k = 0; k < kGuessHidden; ++k)
+      put_b(kTcW2, kGuessHidden, n, k, w[kOffW2 + k * kGuessHidden + n]);
+  auto put_f = [&](int off, float v) { std::memcpy(img + off, &v, 4); };
+  for (int j = 0; j < kGuessHidden; ++j) {
+    put_f(kTcB1 + 4 * j, w[kOffB1 + j]);
+    put_f(kTcB2 + 4 * j, w[kOffB2 + j]);
+    uint32_t u = (uint32_t)bf16_bits(w[kOffW3 + j]) << 16;  // w3 as the bf16 value it holds
+    float f;
+    std::memcpy(&f, &u, 4);
+    put_f(kTcW3 + 4 * j, f);
+  }
+  put_f(kTcB3, w[kOffB3]);
 }
 
 void pack_guess(const float* w, std::vector<uint32_t>& out) {
@@ -875,6 +907,9 @@ int prepare_sweep(ppm_b200_context* ctx, int dim, int position, const ppm_b200_p
   plan.B.fused = fused ? 1 : 0;
   plan.B.face_prefix = (const int64_t*)(base + off_f);
   plan.B.face_blocks = fpre[ng];
+  // the tensor-core guess pass takes 128 faces per tile, as the Riemann kernel's blocks
+  plan.B.learned_pass = (p->learned_guess == 2 && nc == 0) ? 1 : 0;
+  plan.B.sms = ctx->sms;
   if (persist)
     plan.riemann_blocks = std::min<int64_t>(
         rpre[ng], (int64_t)ctx->sms *
@@ -2595,6 +2630,7 @@ int ppm_b200_set_guess(ppm_b200_context* ctx, const float* weights) {
   }
   std::vector<uint32_t> packed;
   pack_guess(weights, packed);
+  pack_guess_tc(weights, packed);
   int rc = ensure(ctx, ctx->guess, packed.size() * sizeof(uint32_t));
   if (rc) return rc;
   CK(cudaStreamSynchronize(ctx->stream));  // a queued solve may still read the old weights
@@ -2669,7 +2705,9 @@ int ppm_b200_guess_eval(ppm_b200_context* ctx, const float* features, long long 
   if (!ctx || n < 0 || (n > 0 && (!features || !y))) return PPM_B200_ERR_INVALID;
   if (!ctx->has_guess) return PPM_B200_ERR_INVALID;
   CK(cudaSetDevice(ctx->device));
-  CK(ppm::launch_guess_eval((const uint32_t*)ctx->guess.p, features, n, y, ctx->stream));
+  CK(ppm::launch_guess_eval_tc((const uint32_t*)ctx->guess.p, features, n, y,
+                               (unsigned long long*)ctx->counters.p + ppm::kCntTimeout,
+                               ctx->sms, ctx->stream));
   ctx->launches += 1;
   return PPM_B200_OK;
 }

@@ -65,6 +65,23 @@ enum {
   kPackWords = kPackB3 + 4
 };
 
+// The same weights for the tcgen05 kernels (ppm_guess_tc.cu), after the packed words in
+// the same device buffer (word offset kTcWordOffset), bytes: W1 and W2 as the MMA's B
+// operands (N x K, K-major, bf16, the canonical layout without swizzle: element (n, k) at
+// ((k/8) * (N/8) + n/8) * 128 + (n%8) * 16 + (k%8) * 2), then b1, b2, w3 (its bf16 value)
+// and b3 as FP32.
+enum {
+  kTcW1 = 0,                    // 64 x 16 (the 6 inputs, zero padded)
+  kTcW2 = kTcW1 + 64 * 16 * 2,  // 64 x 64
+  kTcB1 = kTcW2 + 64 * 64 * 2,
+  kTcB2 = kTcB1 + 64 * 4,
+  kTcW3 = kTcB2 + 64 * 4,
+  kTcB3 = kTcW3 + 64 * 4,
+  kTcBytes = kTcB3 + 16,
+  kTcWordOffset = ((kPackWords + 255) / 256) * 256,
+  kGuessBufferWords = kTcWordOffset + kTcBytes / 4
+};
+
 // Interface-state features of one face (see the header comment); returns |x|^2.  FP32
 // arithmetic on the FP32 pipe: the net sees its inputs rounded to BF16, so FP64 logs
 // and divides (which would load the FP64 pipe the Newton iteration is bound by) buy

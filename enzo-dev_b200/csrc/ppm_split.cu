@@ -24,6 +24,7 @@
 #include "ppm_sweep.cuh"
 
 namespace ppm {
+void launch_guess_pass(const BatchArgs& B, int sms, cudaStream_t st);
 namespace split {
 
 enum { VD = 0, VP = 1, VU = 2, VV = 3, VW = 4, VGE = 5 };
@@ -444,8 +445,10 @@ __device__ __forceinline__ void load_face_advected(const SweepArgs& a, int64_t i
 // block list (B.riemann_total entries) with a stride of the grid, keeping each grid's
 // record in shared memory while consecutive blocks belong to it.  RT and PERSIST are the
 // level autotuner's choices per size class (ppm_b200_autotune_level).
+// PLANE (with LEARNED): the net's output and |x|^2 of each face come from the guess
+// pass, in the face's slot of the XUB plane.
 template <bool DUAL, bool ONE, bool LEARNED, bool COL = false, int RT = kRiemannThreads,
-          bool PERSIST = false>
+          bool PERSIST = false, bool PLANE = false>
 __global__ void __launch_bounds__(RT, (LEARNED ? PPM_RIEMANN_LEARNED_MINBLOCKS
                                                : PPM_RIEMANN_MINBLOCKS) * kRiemannThreads / RT)
     riemann_kernel(const __grid_constant__ BatchArgs B) {
@@ -490,7 +493,13 @@ __global__ void __launch_bounds__(RT, (LEARNED ? PPM_RIEMANN_LEARNED_MINBLOCKS
     s.ur = f[SUR * pl];
   }
   float y = 0.0f, d2 = 0.0f;
-  if (LEARNED) {
+  if (LEARNED && PLANE) {
+    if (valid) {
+      const float2 v = *reinterpret_cast<const float2*>(a.fflux + XUB * a.plane + idx);
+      y = v.x;
+      d2 = v.y;
+    }
+  } else if (LEARNED) {
     float f[6];
     d2 = guess_features(s.dl, s.dr, s.pl, s.pr, s.ul, s.ur, P.gamma, f);
     if (!valid) d2 = 0.0f;
@@ -1960,7 +1969,11 @@ void launch_stages(const BatchArgs& B, int64_t march_blocks, int64_t riemann_blo
     hll_riemann_kernel<DUAL, ONE, true, false><<<rb, kRiemannThreads, 0, st>>>(B);
   else if (learned && B.ncolour > 0)
     riemann_kernel<DUAL, ONE, true, true><<<rb, kRiemannThreads, 0, st>>>(B);
-  else if (learned)
+  else if (learned && B.learned_pass) {
+    launch_guess_pass(B, B.sms, st);
+    riemann_kernel<DUAL, ONE, true, false, kRiemannThreads, false, true>
+        <<<rb, kRiemannThreads, 0, st>>>(B);
+  } else if (learned)
     riemann_kernel<DUAL, ONE, true><<<rb, kRiemannThreads, 0, st>>>(B);
   else if (B.ncolour > 0)
     riemann_kernel<DUAL, ONE, false, true><<<rb, kRiemannThreads, 0, st>>>(B);

@@ -184,6 +184,10 @@ struct BatchArgs {
   int fused = 0;
   const int64_t* face_prefix = nullptr;
   int64_t face_blocks = 0;
+  // learned start from a tensor-core guess pass (tcgen05, ppm_guess_tc.cu) over the
+  // interface states before the Riemann kernel, instead of inside it
+  int learned_pass = 0;
+  int sms = 148;
   CUtensorMap xin[6];
 };
 

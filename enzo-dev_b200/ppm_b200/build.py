@@ -27,7 +27,8 @@ OUT_DIR = ROOT / "_build"
 LIB = OUT_DIR / "libppm_b200.so"
 INCLUDE = REPO / "include"
 
-SOURCES = ["ppm_kernels.cu", "ppm_split.cu", "ppm_capi.cu", "ppm_noalloc.cu", "ppm_mlp.cu"]
+SOURCES = ["ppm_kernels.cu", "ppm_split.cu", "ppm_capi.cu", "ppm_noalloc.cu", "ppm_mlp.cu",
+           "ppm_guess_tc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # -fno-gnu-unique and the version script keep every symbol but the C ABI local to its
 # library: both variants can be loaded in one process without one's template statics

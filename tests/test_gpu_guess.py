@@ -155,9 +155,12 @@ def _totals(g, f):
     return float(np.sum(f["d"][act])), float(np.sum((f["d"] * f["te"])[act]))
 
 
-@pytest.mark.parametrize("mach,steps", [(3.0, 40), (10.0, 25)])
+# learned_guess 1: the net inside the Riemann kernel (mma.sync); 2: a tensor-core guess
+# pass (tcgen05, TMEM accumulators) over the interface states before it
+@pytest.mark.parametrize("mach,steps,mode", [(3.0, 40, 1), (10.0, 25, 1), (3.0, 40, 2),
+                                             (10.0, 25, 2)])
 def test_learned_start_stays_within_the_parity_bar_and_saves_iterations(ctx, torch, mach,
-                                                                          steps):
+                                                                          steps, mode):
     w = LRN.default_weights()
     ctx.set_guess(w)
     hp = H.HydroParams(gamma=5.0 / 3.0, cfl=0.4, dual=True)
@@ -170,7 +173,7 @@ def test_learned_start_stays_within_the_parity_bar_and_saves_iterations(ctx, tor
         dt = hp.cfl * O.calc_dt(g, hp, f_ora, p, g.cellwidth)
         rc, st_o = O.solve_ppm_de(g, hp, dt, cyc, f_ora, g.cellwidth)
         assert rc == 0
-        rc, st_g = ctx.solve_ppm_de(g, hp, dt, cyc, f_gpu, learned_guess=True)
+        rc, st_g = ctx.solve_ppm_de(g, hp, dt, cyc, f_gpu, learned_guess=mode)
         assert rc == capi.OK
         it_plain += st_o["newton_iters"]
         it_learn += st_g["newton_iters"]
@@ -206,7 +209,8 @@ def test_mass_and_energy_conserved_without_dual_energy(ctx, torch, learned):
     assert abs(e1 - e0) <= 1e-12 * e0
 
 
-def test_learned_start_in_level_batches_matches_per_grid(ctx, torch):
+@pytest.mark.parametrize("mode", [1, 2])
+def test_learned_start_in_level_batches_matches_per_grid(ctx, torch, mode):
     ctx.set_guess(LRN.default_weights())
     hp = H.HydroParams(gamma=5.0 / 3.0, cfl=0.5, dual=True)
     shapes = [(16, 16, 16), (12, 20, 8), (9, 9, 30)]
@@ -216,10 +220,10 @@ def test_learned_start_in_level_batches_matches_per_grid(ctx, torch):
     b = [{k: torch.from_numpy(v.copy()).cuda() for k, v in f.items()} for f in host]
     torch.cuda.synchronize()
     dt = 1e-3
-    rc, st = ctx.solve_level(grids, hp, dt, 0, a, want_stats=True, learned_guess=True)
+    rc, st = ctx.solve_level(grids, hp, dt, 0, a, want_stats=True, learned_guess=mode)
     assert rc == capi.OK
     for k, gr in enumerate(grids):
-        ctx.solve_ppm_de(gr, hp, dt, 0, b[k], memory=capi.MEM_DEVICE, learned_guess=True)
+        ctx.solve_ppm_de(gr, hp, dt, 0, b[k], memory=capi.MEM_DEVICE, learned_guess=mode)
     torch.cuda.synchronize()
     for k, gr in enumerate(grids):
         for name in a[k]:
