@@ -95,8 +95,10 @@ typedef struct ppm_b200_params {
   int number_of_colours;    /* NumberOfColours: 0 .. PPM_B200_MAX_COLOURS advected colour fields
                                (Grid_SolveHydroEquations.C:90-285); their fields are
                                ppm_b200_grid.colours[] */
-  int learned_guess;        /* 1: start twoshock's Newton iteration from the learned p* guess
-                               (weights from ppm_b200_set_guess) */
+  int learned_guess;        /* start twoshock's Newton iteration from the learned p* guess
+                               (weights from ppm_b200_set_guess): 0 off; 1 the net evaluated
+                               inside the Riemann kernel (mma.sync); 2 a guess pass on the
+                               tcgen05 tensor cores before the Riemann kernel */
   const double *dt_device;  /* optional: device pointer holding dtFixed (overrides dt) */
   const int *colour_species; /* optional HOST array of number_of_colours flags for
                                ppm_b200_correct_fluxes[_sublings]: nonzero for a colour
@@ -403,8 +405,10 @@ int ppm_b200_expansion_terms_level(ppm_b200_context *ctx, const ppm_b200_params 
 
 /* --- learned starting pressure of twoshock's Newton iteration (twoshock.F:156-170) ---
    A 6 -> 64 -> 64 -> 1 MLP predicts ln(p* / p_acoustic) from the two interface states;
-   with params->learned_guess = 1 the Riemann kernel evaluates it on the tensor cores
-   (BF16 operands, FP32 accumulation), starts Newton from that pressure, iterates to the
+   with params->learned_guess = 1 the Riemann kernel evaluates it with warp-level MMAs,
+   with 2 a separate pass evaluates it with tcgen05.mma (accumulators in tensor memory)
+   into the face's flux-plane slot (BF16 operands, FP32 accumulation either way); the
+   Riemann kernel starts Newton from that pressure, iterates to the
    reference tolerance, and re-solves from the acoustic start (the plain solver) any
    face that does not converge (counted in stats->guess_rejected).  The fields then
    agree with the plain solver to round-off, not bit for bit.
@@ -438,8 +442,12 @@ int ppm_b200_guess_grad(ppm_b200_context *ctx, const float *weights, const float
 int ppm_b200_guess_adam(ppm_b200_context *ctx, float *weights, float *grad, float *m,
                         float *v, int step, float lr, float beta1, float beta2, float eps);
 
-/* The tensor-core inference of the Riemann kernel on given inputs (6 floats each),
-   with the weights of ppm_b200_set_guess: y[i] = predicted ln(p* / p_acoustic). */
+/* The net on given inputs (6 floats each), with the weights of ppm_b200_set_guess, on
+   the tcgen05 tensor cores (the kernel of learned_guess = 2): y[i] = the net's output
+   (the predicted ln(p* / p_acoustic) / |x|^2).  Queues and returns.  Waits on the MMAs
+   are bounded: a CTA whose MMA does not complete within about a second stops, leaves its
+   remaining outputs unwritten and counts a timeout, which the context's next status
+   read (ppm_b200_synchronize, a synchronous solve) reports as PPM_B200_ERR_TIMEOUT. */
 int ppm_b200_guess_eval(ppm_b200_context *ctx, const float *features, long long n, float *y);
 
 /* One directional sweep that allocates nothing (no counterpart in the reference).
