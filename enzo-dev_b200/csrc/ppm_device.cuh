@@ -268,91 +268,99 @@ struct ColFace {
   bool ovl, ovr;
 };
 
-// inteuler.F:320-410, 493-551 (d, p, u); gsum = grslice(i-1) + grslice(i) (GRAV only).
-// CX: also report the colour data of the face in *cx.
+// One side of a face's d, p, u states (inteuler.F:320-410 for the left side, :493-551
+// for the right; the two sides share nothing but gsum = grslice(i-1) + grslice(i)).
+// qa, q0, qm, qp: the parabola averages over the domains of dependence (char, the
+// zero, minus and plus characteristics) of density (a, 0 only), pressure and velocity
+// of the cell on this side; cm, c0, cp: the characteristic speeds.  LEFT: a wave enters
+// the face from the left where its speed is positive.
+struct SideIn {
+  double da, d0, pa, p0, pm, pp, ua, u0, um, up, cm, c0, cp;
+};
+struct SideOut {
+  double p, u, d;  // the face state on this side
+  double dc;       // the corrected density before the dual-energy override (colours)
+  bool ov;         // the override replaced this side
+};
+
+template <bool DUAL, bool GRAV, bool LEFT>
+__device__ __forceinline__ SideOut face_side(const SideIn& S, double gsum, const Phys& P) {
+  SideOut o;
+  const double c = sqrt(dmax(P.gamma * S.pa * S.da, 0.0));
+  // 0.5/c is computed as 0.5*(1/c): equal, since c is 0, inf, NaN or a square root of
+  // a double (|c| <= 2^512), so 1/c never reaches the subnormal range
+  double f1 = 1.0 / c;
+  const double hc = 0.5 * f1;
+  const double yd = 1.0 / S.da;
+  double bp = (S.ua - S.up) + (S.pa - S.pp) * f1;
+  double bm = (S.ua - S.um) - (S.pa - S.pm) * f1;
+  double b0 = (S.pa - S.p0) * (f1 * f1) + yd - 1.0 / S.d0;
+  if (GRAV) {
+    const double gterm = 0.25 * P.dt * gsum;
+    bp = bp - gterm;
+    bm = bm - gterm;
+  }
+  f1 = hc;
+  bp = -(bp * f1);
+  bm = +bm * f1;
+  if (LEFT ? S.cp <= 0.0 : S.cp >= 0.0) bp = 0.0;
+  if (LEFT ? S.cm <= 0.0 : S.cm >= 0.0) bm = 0.0;
+  if (LEFT ? S.c0 <= 0.0 : S.c0 >= 0.0) b0 = 0.0;
+  o.p = S.pa + (bp + bm) * (c * c);
+  o.u = S.ua + (bp - bm) * c;
+  o.d = 1.0 / (yd - (b0 + bp + bm));
+  o.dc = o.d;
+  o.ov = false;
+  if (DUAL) {
+    const double m = dmax(dmax(fabs(S.cm), fabs(S.c0)), fabs(S.cp));
+#if PPM_FAST_ALGEBRA  // tolerance mode: the quotient by da from its reciprocal
+    const bool ov = P.gamma * S.pa * yd < P.eta2 * (S.ua * S.ua) || m < 1.0e-3 ||
+                    o.d * yd > 5.0;
+#else
+    const bool ov = P.gamma * S.pa / S.da < P.eta2 * (S.ua * S.ua) || m < 1.0e-3 ||
+                    o.d / S.da > 5.0;
+#endif
+    if (ov) {
+      o.p = S.pa;
+      o.u = S.ua;
+      o.d = S.da;
+      o.ov = true;
+    }
+  }
+  o.p = dmax(o.p, kTiny);
+  o.d = dmax(o.d, kTiny);
+  return o;
+}
+
+__device__ __forceinline__ SideIn side_in(const CoreL& L) {
+  return SideIn{L.dla, L.dl0, L.pla, L.pl0, L.plm, L.plp, L.ula, L.ul0, L.ulm, L.ulp,
+                L.cm, L.c0, L.cp};
+}
+__device__ __forceinline__ SideIn side_in(const CoreR& R) {
+  return SideIn{R.dra, R.dr0, R.pra, R.pr0, R.prm, R.prp, R.ura, R.ur0, R.urm, R.urp,
+                R.cm, R.c0, R.cp};
+}
+
+// inteuler.F:320-410, 493-551 (d, p, u) for both sides of a face; gsum = grslice(i-1) +
+// grslice(i) (GRAV only).  CX: also report the colour data of the face in *cx.
 template <bool DUAL, bool GRAV, bool CX = false>
 __device__ __forceinline__ CoreState face_core(const CoreL& L, const CoreR& R, double gsum,
                                                const Phys& P, ColFace* cx = nullptr) {
-  CoreState s;
-  double cla = sqrt(dmax(P.gamma * L.pla * L.dla, 0.0));
-  double cra = sqrt(dmax(P.gamma * R.pra * R.dra, 0.0));
-  // 0.5/c is computed as 0.5*(1/c): equal, since c is 0, inf, NaN or a square root of
-  // a double (|c| <= 2^512), so 1/c never reaches the subnormal range
-  double f1 = 1.0 / cla;
-  const double hla = 0.5 * f1;
-  const double ydla = 1.0 / L.dla;
-  double betalp = (L.ula - L.ulp) + (L.pla - L.plp) * f1;
-  double betalm = (L.ula - L.ulm) - (L.pla - L.plm) * f1;
-  double betal0 = (L.pla - L.pl0) * (f1 * f1) + ydla - 1.0 / L.dl0;
-  double gterm = 0.0;
-  if (GRAV) {
-    gterm = 0.25 * P.dt * gsum;
-    betalp = betalp - gterm;
-    betalm = betalm - gterm;
-  }
-  f1 = hla;
-  betalp = -(betalp * f1);
-  betalm = +betalm * f1;
-  if (L.cp <= 0.0) betalp = 0.0;
-  if (L.cm <= 0.0) betalm = 0.0;
-  if (L.c0 <= 0.0) betal0 = 0.0;
-  f1 = 1.0 / cra;
-  const double hra = 0.5 * f1;
-  const double ydra = 1.0 / R.dra;
-  double betarp = (R.ura - R.urp) + (R.pra - R.prp) * f1;
-  double betarm = (R.ura - R.urm) - (R.pra - R.prm) * f1;
-  double betar0 = (R.pra - R.pr0) * (f1 * f1) + ydra - 1.0 / R.dr0;
-  if (GRAV) {
-    betarp = betarp - gterm;
-    betarm = betarm - gterm;
-  }
-  f1 = hra;
-  betarp = -(betarp * f1);
-  betarm = +betarm * f1;
-  if (R.cp >= 0.0) betarp = 0.0;
-  if (R.cm >= 0.0) betarm = 0.0;
-  if (R.c0 >= 0.0) betar0 = 0.0;
-  s.pl = L.pla + (betalp + betalm) * (cla * cla);
-  s.pr = R.pra + (betarp + betarm) * (cra * cra);
-  s.ul = L.ula + (betalp - betalm) * cla;
-  s.ur = R.ura + (betarp - betarm) * cra;
-  s.dl = 1.0 / (ydla - (betal0 + betalp + betalm));
-  s.dr = 1.0 / (ydra - (betar0 + betarp + betarm));
+  const SideOut l = face_side<DUAL, GRAV, true>(side_in(L), gsum, P);
+  const SideOut r = face_side<DUAL, GRAV, false>(side_in(R), gsum, P);
   if (CX) {
-    cx->dlc = s.dl;
-    cx->drc = s.dr;
-    cx->ovl = cx->ovr = false;
+    cx->dlc = l.dc;
+    cx->drc = r.dc;
+    cx->ovl = l.ov;
+    cx->ovr = r.ov;
   }
-  if (DUAL) {
-    double ml = dmax(dmax(fabs(L.cm), fabs(L.c0)), fabs(L.cp));
-#if PPM_FAST_ALGEBRA  // tolerance mode: the quotients by dla, dra from their reciprocals
-    const bool ovl = P.gamma * L.pla * ydla < P.eta2 * (L.ula * L.ula) || ml < 1.0e-3 ||
-                     s.dl * ydla > 5.0;
-#else
-    const bool ovl = P.gamma * L.pla / L.dla < P.eta2 * (L.ula * L.ula) || ml < 1.0e-3 ||
-                     s.dl / L.dla > 5.0;
-#endif
-    if (ovl) {
-      s.pl = L.pla; s.ul = L.ula; s.dl = L.dla;
-      if (CX) cx->ovl = true;
-    }
-    double mr = dmax(dmax(fabs(R.cm), fabs(R.c0)), fabs(R.cp));
-#if PPM_FAST_ALGEBRA
-    const bool ovr = P.gamma * R.pra * ydra < P.eta2 * (R.ura * R.ura) || mr < 1.0e-3 ||
-                     s.dr * ydra > 5.0;
-#else
-    const bool ovr = P.gamma * R.pra / R.dra < P.eta2 * (R.ura * R.ura) || mr < 1.0e-3 ||
-                     s.dr / R.dra > 5.0;
-#endif
-    if (ovr) {
-      s.pr = R.pra; s.ur = R.ura; s.dr = R.dra;
-      if (CX) cx->ovr = true;
-    }
-  }
-  s.pl = dmax(s.pl, kTiny);
-  s.pr = dmax(s.pr, kTiny);
-  s.dl = dmax(s.dl, kTiny);
-  s.dr = dmax(s.dr, kTiny);
+  CoreState s;
+  s.pl = l.p;
+  s.pr = r.p;
+  s.ul = l.u;
+  s.ur = r.u;
+  s.dl = l.d;
+  s.dr = r.d;
   return s;
 }
 

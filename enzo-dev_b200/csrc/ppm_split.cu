@@ -160,6 +160,17 @@ __global__ void __launch_bounds__(kMarchThreads) corrections_kernel(const __grid
 #ifndef PPM_RECON0_MINBLOCKS
 #define PPM_RECON0_MINBLOCKS PPM_RECON_MINBLOCKS
 #endif
+// PPM_RECON_PREFETCH: the march loads cell t+1 while it computes with cell t.
+// PPM_RECON_UNROLL: unroll factor of the march.
+#ifndef PPM_RECON_PREFETCH
+#define PPM_RECON_PREFETCH 0
+#endif
+#ifndef PPM_RECON_UNROLL
+#define PPM_RECON_UNROLL 1
+#endif
+#define PPM_STR_(x) #x
+#define PPM_UNROLL_(n) _Pragma(PPM_STR_(unroll n))
+
 // COR: the batch carries slope corrections (the coefficients of the corrections kernel).
 // One pencil's march (the body of the reconstruct kernels).
 template <bool DUAL, bool GRAV, int ROLE, bool COR>
@@ -183,24 +194,65 @@ __device__ __forceinline__ void reconstruct_pencil(const SweepArgs& a, int64_t p
   double wu0 = 0.0, wu1 = 0.0, wu2 = 0.0;  // normal velocity of cells t-3, t-2, t-1
   double wg0 = 0.0, wg1 = 0.0, wg2 = 0.0;  // acceleration (ROLE 0, GRAV)
   Prep prA = {0, 0, 0, 0, 0}, prB = {0, 0, 0, 0, 0};  // cells t-2, t-1
-  CoreL cLp = {};  // left data of face t-2 (ROLE 0)
+  // ROLE 0: the left side of face t-2 (cell t-3's right edge), solved when that cell's
+  // parabola was formed, with its raw density averages (colours, PressureFree)
+  SideOut sLp = {0.0, 0.0, 0.0, 0.0, false};
+  double lda = 0.0, ld0 = 0.0;
   AdvL aLp = {};   // left data of face t-2 (ROLE 1)
 
   const int tend = ie + 3;  // the last face, ie+1, is assembled at t = ie+3
-#pragma unroll 1
+#if PPM_RECON_PREFETCH
+  // cell t's loads, issued one iteration ahead
+  double xq0, xq1, xq2, xu, xg, xd, xp;
+  {
+    const int64_t off = base;
+    xq0 = ldg0(q0p, off);
+    xq1 = ldg0(q1p, off);
+    xq2 = ldg0(q2p, off);
+    xu = ROLE == 0 ? 0.0 : ldg0(a.in_u, off);
+    xg = (GRAV && ROLE == 0) ? __ldg(a.grav + off) : 0.0;
+    xd = ROLE == 0 ? 0.0 : __ldg(a.in_d + off);
+    xp = ROLE == 0 ? 0.0 : __ldg(a.pres + off);
+  }
+#endif
+  PPM_UNROLL_(PPM_RECON_UNROLL)
   for (int t = 0; t <= tend; ++t) {
     const int64_t off = base + (int64_t)t * sa;
     double nq[3];
+#if PPM_RECON_PREFETCH
+    nq[0] = xq0;
+    nq[1] = xq1;
+    nq[2] = xq2;
+    const double nu = ROLE == 0 ? nq[2] : xu;
+    const double ng = xg;
+    const double nd = ROLE == 0 ? nq[0] : xd;
+    const double npr = ROLE == 0 ? nq[1] : xp;
+    if (t < tend) {
+      const int64_t o1 = off + sa;
+      xq0 = ldg0(q0p, o1);
+      xq1 = ldg0(q1p, o1);
+      xq2 = ldg0(q2p, o1);
+      if (ROLE != 0) xu = ldg0(a.in_u, o1);
+      if (GRAV && ROLE == 0) xg = __ldg(a.grav + o1);
+      if (ROLE != 0) {
+        xd = __ldg(a.in_d + o1);
+        xp = __ldg(a.pres + o1);
+      }
+    }
+#else
     nq[0] = ldg0(q0p, off);
     nq[1] = ldg0(q1p, off);
     nq[2] = ldg0(q2p, off);
     const double nu = ROLE == 0 ? nq[2] : ldg0(a.in_u, off);
     const double ng = (GRAV && ROLE == 0) ? __ldg(a.grav + off) : 0.0;
+#endif
     // characteristic distances of cell t (inteuler.F:197-208)
     Prep prC = prB;
     if (t >= is - 1 && t <= ie + 1) {
+#if !PPM_RECON_PREFETCH
       const double nd = ROLE == 0 ? nq[0] : __ldg(a.in_d + off);
       const double npr = ROLE == 0 ? nq[1] : __ldg(a.pres + off);
+#endif
       prC = (COR && a.presfree) ? cell_prep<true>(nd, npr, nu, a.coef[t].dx2i, P)
                                 : cell_prep(nd, npr, nu, a.coef[t].dx2i, P);
     }
@@ -222,7 +274,8 @@ __device__ __forceinline__ void reconstruct_pencil(const SweepArgs& a, int64_t p
       }
     }
     // parabola of cell t-2, its face contributions, and face t-2 (inteuler.F:304-551)
-    CoreL cLn = cLp;
+    SideOut sLn = sLp;
+    double ldn = lda, ld0n = ld0;
     AdvL aLn = aLp;
     {
       const int c = t - 2;
@@ -255,61 +308,51 @@ __device__ __forceinline__ void reconstruct_pencil(const SweepArgs& a, int64_t p
         }
         double* o = a.fstate + (int64_t)(c - is) * np + pid;
         if (ROLE == 0) {
+          // cell c's left edge gives the right side of face c, its right edge the left
+          // side of face c+1; each side is solved on its own (face_side), the left one
+          // carried to the next step
           if (c >= is) {
-            CoreR R;
-            R.dra = pm_C(pa[0], prA.char2);
-            R.dr0 = pm_B(pa[0], prA.c0);
-            R.pra = pm_C(pa[1], prA.char2);
-            R.pr0 = pm_B(pa[1], prA.c0);
-            R.prm = pm_B(pa[1], prA.cm);
-            R.prp = pm_B(pa[1], prA.cp);
-            R.ura = pm_C(pa[2], prA.char2);
-            R.ur0 = pm_B(pa[2], prA.c0);
-            R.urm = pm_B(pa[2], prA.cm);
-            R.urp = pm_B(pa[2], prA.cp);
-            R.cm = prA.cm;
-            R.c0 = prA.c0;
-            R.cp = prA.cp;
-            CoreState s;
+            const SideIn Rin{pm_C(pa[0], prA.char2), pm_B(pa[0], prA.c0),
+                             pm_C(pa[1], prA.char2), pm_B(pa[1], prA.c0),
+                             pm_B(pa[1], prA.cm),    pm_B(pa[1], prA.cp),
+                             pm_C(pa[2], prA.char2), pm_B(pa[2], prA.c0),
+                             pm_B(pa[2], prA.cm),    pm_B(pa[2], prA.cp),
+                             prA.cm,                 prA.c0,
+                             prA.cp};
+            const SideOut r = face_side<DUAL, GRAV, false>(Rin, GRAV ? (wg0 + wg1) : 0.0, P);
+            double dl = sLp.d, dr = r.d;
             if (COR && a.fcol) {  // colours: what their face states need (kColVars planes)
-              ColFace cx;
-              s = face_core<DUAL, GRAV, true>(cLp, R, GRAV ? (wg0 + wg1) : 0.0, P, &cx);
               double* oc = a.fcol + (int64_t)(c - is) * np + pid;
-              oc[CDLA * plane] = cLp.dla;
-              oc[CDL0 * plane] = cLp.dl0;
-              oc[CDRA * plane] = R.dra;
-              oc[CDR0 * plane] = R.dr0;
-              oc[CDLC * plane] = cx.dlc;
-              oc[CDRC * plane] = cx.drc;
-              oc[COVR * plane] = (cx.ovl ? 1.0 : 0.0) + (cx.ovr ? 2.0 : 0.0);
-            } else {
-              s = face_core<DUAL, GRAV>(cLp, R, GRAV ? (wg0 + wg1) : 0.0, P);
+              oc[CDLA * plane] = lda;
+              oc[CDL0 * plane] = ld0;
+              oc[CDRA * plane] = Rin.da;
+              oc[CDR0 * plane] = Rin.d0;
+              oc[CDLC * plane] = sLp.dc;
+              oc[CDRC * plane] = r.dc;
+              oc[COVR * plane] = (sLp.ov ? 1.0 : 0.0) + (r.ov ? 2.0 : 0.0);
             }
             if (COR && a.presfree) {  // the uncorrected densities (inteuler.F:556-561)
-              s.dl = cLp.dla;
-              s.dr = R.dra;
+              dl = lda;
+              dr = Rin.da;
             }
-            o[SDL * plane] = s.dl;
-            o[SDR * plane] = s.dr;
-            o[SPL * plane] = s.pl;
-            o[SPR * plane] = s.pr;
-            o[SUL * plane] = s.ul;
-            o[SUR * plane] = s.ur;
+            o[SDL * plane] = dl;
+            o[SDR * plane] = dr;
+            o[SPL * plane] = sLp.p;
+            o[SPR * plane] = r.p;
+            o[SUL * plane] = sLp.u;
+            o[SUR * plane] = r.u;
           }
           if (c <= ie) {
-            cLn.dla = pm_A(pa[0], prA.char1);
-            cLn.dl0 = pm_A(pa[0], prA.c0);
-            cLn.pla = pm_A(pa[1], prA.char1);
-            cLn.pl0 = pm_A(pa[1], prA.c0);
-            cLn.plm = pm_A(pa[1], prA.cm);
-            cLn.plp = pm_A(pa[1], prA.cp);
-            cLn.ula = pm_A(pa[2], prA.char1);
-            cLn.ul0 = pm_A(pa[2], prA.c0);
-            cLn.ulm = pm_A(pa[2], prA.cm);
-            cLn.ulp = pm_A(pa[2], prA.cp);
-            cLn.cm = prA.cm;
-            cLn.c0 = prA.c0;
-            cLn.cp = prA.cp;
+            const SideIn Lin{pm_A(pa[0], prA.char1), pm_A(pa[0], prA.c0),
+                             pm_A(pa[1], prA.char1), pm_A(pa[1], prA.c0),
+                             pm_A(pa[1], prA.cm),    pm_A(pa[1], prA.cp),
+                             pm_A(pa[2], prA.char1), pm_A(pa[2], prA.c0),
+                             pm_A(pa[2], prA.cm),    pm_A(pa[2], prA.cp),
+                             prA.cm,                 prA.c0,
+                             prA.cp};
+            sLn = face_side<DUAL, GRAV, true>(Lin, GRAV ? (wg1 + wg2) : 0.0, P);
+            ldn = Lin.da;
+            ld0n = Lin.d0;
           }
         } else {
           if (c >= is) {
@@ -358,7 +401,9 @@ __device__ __forceinline__ void reconstruct_pencil(const SweepArgs& a, int64_t p
     wg2 = ng;
     prA = prB;
     prB = prC;
-    cLp = cLn;
+    sLp = sLn;
+    lda = ldn;
+    ld0 = ld0n;
     aLp = aLn;
   }
 }
