@@ -13,11 +13,12 @@
 
 #include <cstdint>
 
+#include "ppm_fastmath.cuh"
+
 // PPM_FAST_ALGEBRA (the tolerance-mode build): a few quotients with a shared divisor
-// are formed from one reciprocal; everything else is the reference's expression.
-#ifndef PPM_FAST_ALGEBRA
-#define PPM_FAST_ALGEBRA 0
-#endif
+// are formed from one reciprocal, and the reconstruction's and the Riemann solvers'
+// divisions and square roots go through qrcp / qdiv / qsqrt (ppm_fastmath.cuh; the
+// IEEE operations in the exact build); everything else is the reference's expression.
 
 namespace ppm {
 
@@ -52,7 +53,7 @@ template <bool PF = false>
 __device__ __forceinline__ Prep cell_prep(double d, double p, double u, double dx2i,
                                           const Phys& P) {
   Prep r;
-  double cs = sqrt(P.gamma * p / d);
+  double cs = qsqrt(qdiv(P.gamma * p, d));
   if (PF) cs = kTiny;
   r.char1 = dmax(0.0, P.dt * (u + cs)) * dx2i;
   r.char2 = dmax(0.0, -(P.dt * (u - cs))) * dx2i;
@@ -67,7 +68,7 @@ __device__ __forceinline__ double pm_slope(double qm, double q0, double qp, doub
   double qplus = qp - q0;
   double qmnus = q0 - qm;
   double qcent = c1 * qplus + c2 * qmnus;
-  double qvanl = 2.0 * qplus * qmnus / (qmnus + qplus);
+  double qvanl = qdiv(2.0 * qplus * qmnus, qmnus + qplus);
   double temp1 = dmin(dmin(dmin(fabs(qcent), fabs(qvanl)), 2.0 * fabs(qmnus)), 2.0 * fabs(qplus));
   double r = temp1 * copysign(1.0, qcent);
   return (qplus * qmnus > 0.0) ? r : 0.0;
@@ -286,15 +287,15 @@ struct SideOut {
 template <bool DUAL, bool GRAV, bool LEFT>
 __device__ __forceinline__ SideOut face_side(const SideIn& S, double gsum, const Phys& P) {
   SideOut o;
-  const double c = sqrt(dmax(P.gamma * S.pa * S.da, 0.0));
+  const double c = qsqrt(dmax(P.gamma * S.pa * S.da, 0.0));
   // 0.5/c is computed as 0.5*(1/c): equal, since c is 0, inf, NaN or a square root of
   // a double (|c| <= 2^512), so 1/c never reaches the subnormal range
-  double f1 = 1.0 / c;
+  double f1 = qrcp(c);
   const double hc = 0.5 * f1;
-  const double yd = 1.0 / S.da;
+  const double yd = qrcp(S.da);
   double bp = (S.ua - S.up) + (S.pa - S.pp) * f1;
   double bm = (S.ua - S.um) - (S.pa - S.pm) * f1;
-  double b0 = (S.pa - S.p0) * (f1 * f1) + yd - 1.0 / S.d0;
+  double b0 = (S.pa - S.p0) * (f1 * f1) + yd - qrcp(S.d0);
   if (GRAV) {
     const double gterm = 0.25 * P.dt * gsum;
     bp = bp - gterm;
@@ -308,7 +309,7 @@ __device__ __forceinline__ SideOut face_side(const SideIn& S, double gsum, const
   if (LEFT ? S.c0 <= 0.0 : S.c0 >= 0.0) b0 = 0.0;
   o.p = S.pa + (bp + bm) * (c * c);
   o.u = S.ua + (bp - bm) * c;
-  o.d = 1.0 / (yd - (b0 + bp + bm));
+  o.d = qrcp(yd - (b0 + bp + bm));
   o.dc = o.d;
   o.ov = false;
   if (DUAL) {
@@ -391,7 +392,7 @@ struct Riemann {
 
 __device__ __forceinline__ double acoustic_guess(const FaceState& s, double cl, double cr,
                                                  const Phys& P) {
-  double ps = (cr * s.pl + cl * s.pr + cr * cl * (s.ul - s.ur)) / (cr + cl);
+  double ps = qdiv(cr * s.pl + cl * s.pr + cr * cl * (s.ul - s.ur), cr + cl);
   if (ps < P.pmin) ps = P.pmin;
   return ps;
 }
@@ -406,21 +407,21 @@ __device__ __forceinline__ Riemann twoshock_newton(const FaceState& s, double cl
   // 1/dl, 1/dr formed once, each pair of quotients with different divisors sharing one
   // division (a/x, b/y = a*y*q, b*x*q with q = 1/(x*y)), and the convergence test as
   // |dp| < tolerance * ps: three divisions per update instead of twelve.
-  const double ipl = 1.0 / s.pl, ipr = 1.0 / s.pr, idl = 1.0 / s.dl, idr = 1.0 / s.dr;
+  const double ipl = qrcp(s.pl), ipr = qrcp(s.pr), idl = qrcp(s.dl), idr = qrcp(s.dr);
 #pragma unroll 1
   for (int n = 2; n <= kNumIter; n++) {
     if (active) {
-      const double zl = cl * sqrt((1.0 + P.qa * (ps * ipl - 1.0)));
-      const double zr = cr * sqrt((1.0 + P.qa * (ps * ipr - 1.0)));
-      const double qz = 1.0 / (zl * zr);
+      const double zl = cl * qsqrt((1.0 + P.qa * (ps * ipl - 1.0)));
+      const double zr = cr * qsqrt((1.0 + P.qa * (ps * ipr - 1.0)));
+      const double qz = qrcp(zl * zr);
       ubl = s.ul - (ps - s.pl) * (zr * qz);
       ubr = s.ur + (ps - s.pr) * (zl * qz);
       const double al = 4.0 * (zl * zl) * idl, ar = 4.0 * (zr * zr) * idr;
       const double dl = al - P.gp1 * (ps - s.pl), dr = ar - P.gp1 * (ps - s.pr);
-      const double qd = 1.0 / (dl * dr);
+      const double qd = qrcp(dl * dr);
       dpdul = -(zl * al * (dr * qd));
       dpdur = zr * ar * (dl * qd);
-      ps = ps + (ubr - ubl) * dpdur * dpdul / (dpdur - dpdul);
+      ps = ps + qdiv((ubr - ubl) * dpdur * dpdul, dpdur - dpdul);
       if (ps < P.pmin) ps = P.pmin;
       const double delta_ps = ps - old_ps;
       old_ps = ps;
@@ -450,7 +451,7 @@ __device__ __forceinline__ Riemann twoshock_newton(const FaceState& s, double cl
   Riemann r;
   if (ps < P.pmin) ps = dmin(s.pl, s.pr);
   r.pbar = ps;
-  r.ubar = ubl + (ubr - ubl) * dpdur / (dpdur - dpdul);
+  r.ubar = ubl + qdiv((ubr - ubl) * dpdur, dpdur - dpdul);
   r.iters = it;
   r.converged = !active;
   return r;
@@ -477,12 +478,12 @@ __device__ __forceinline__ Flux flux_twoshock(const FaceState& s, double pbar, d
   }
 #if PPM_FAST_ALGEBRA
   // tolerance mode: 1/d0 once, and gamma*pbar/dbar as gamma*pbar*(1/dbar)
-  const double id0 = 1.0 / d0;
-  double c0 = sqrt(dmax(gamma * p0 * id0, kTiny));
-  double z0 = c0 * d0 * sqrt(dmax(1.0 + P.qa * (pbar / p0 - 1.0), kTiny));
-  const double idbar = id0 - (pbar - p0) / dmax(z0 * z0, kTiny);
-  double dbar = 1.0 / idbar;
-  double cbar = sqrt(dmax(gamma * pbar * idbar, kTiny));
+  const double id0 = qrcp(d0);
+  double c0 = qsqrt(dmax(gamma * p0 * id0, kTiny));
+  double z0 = c0 * d0 * qsqrt(dmax(1.0 + P.qa * (qdiv(pbar, p0) - 1.0), kTiny));
+  const double idbar = id0 - qdiv(pbar - p0, dmax(z0 * z0, kTiny));
+  double dbar = qrcp(idbar);
+  double cbar = qsqrt(dmax(gamma * pbar * idbar, kTiny));
   double l0, lbar;
   if (pbar < p0) {
     l0 = u0 * sn + c0;
@@ -507,7 +508,7 @@ __device__ __forceinline__ Flux flux_twoshock(const FaceState& s, double pbar, d
 #endif
   double frac = l0 - lbar;
   if (frac < kTiny) frac = kTiny;
-  frac = (0.0 - lbar) / frac;
+  frac = qdiv(0.0 - lbar, frac);
   frac = dmin(dmax(frac, 0.0), 1.0);
   double pb = p0 * frac + pbar * (1.0 - frac);
   double db = d0 * frac + dbar * (1.0 - frac);
@@ -525,7 +526,7 @@ __device__ __forceinline__ Flux flux_twoshock(const FaceState& s, double pbar, d
   } else {
     vb = s.vr; wb = s.wr; geb = s.ger;
   }
-  double eb = pb / (P.gm1 * db) + 0.5 * (ub * ub + vb * vb + wb * wb);
+  double eb = qdiv(pb, P.gm1 * db) + 0.5 * (ub * ub + vb * vb + wb * wb);
   double upb = pb * ub;
   double dub = ub * db;
   double duub = dub * ub;
@@ -553,29 +554,29 @@ template <bool DUAL>
 __device__ __forceinline__ HllFace hll_face(const FaceState& s, const Phys& P) {
   const double gamma = P.gamma;
   const double gamma1 = gamma - 1.0;
-  const double gamma1i = 1.0 / gamma1;
-  double sqrtdl = sqrt(s.dl);
-  double sqrtdr = sqrt(s.dr);
-  double isdlpdr = 1.0 / (sqrtdl + sqrtdr);
+  const double gamma1i = qrcp(gamma1);
+  double sqrtdl = qsqrt(s.dl);
+  double sqrtdr = qsqrt(s.dr);
+  double isdlpdr = qrcp(sqrtdl + sqrtdr);
   double vroe1 = (sqrtdl * s.ul + sqrtdr * s.ur) * isdlpdr;
   double vroe2 = (sqrtdl * s.vl + sqrtdr * s.vr) * isdlpdr;
   double vroe3 = (sqrtdl * s.wl + sqrtdr * s.wr) * isdlpdr;
   double v2 = vroe1 * vroe1 + vroe2 * vroe2 + vroe3 * vroe3;
   double el = gamma1i * s.pl + 0.5 * s.dl * (s.ul * s.ul + s.vl * s.vl + s.wl * s.wl);
   double er = gamma1i * s.pr + 0.5 * s.dr * (s.ur * s.ur + s.vr * s.vr + s.wr * s.wr);
-  double hroe = ((el + s.pl) / sqrtdl + (er + s.pr) / sqrtdr) * isdlpdr;
-  double cs = sqrt(gamma1 * dmax((hroe - 0.5 * v2), kTiny));
+  double hroe = (qdiv(el + s.pl, sqrtdl) + qdiv(er + s.pr, sqrtdr)) * isdlpdr;
+  double cs = qsqrt(gamma1 * dmax((hroe - 0.5 * v2), kTiny));
   double char1 = vroe1 - cs;
   double char2 = vroe1 + cs;
-  double csl0 = sqrt(gamma * s.pl / s.dl);
-  double csr0 = sqrt(gamma * s.pr / s.dr);
+  double csl0 = qsqrt(qdiv(gamma * s.pl, s.dl));
+  double csr0 = qsqrt(qdiv(gamma * s.pr, s.dr));
   double csl = dmin(s.ul - csl0, char1);
   double csr = dmax(s.ur + csr0, char2);
   double bm = dmin(csl, 0.0);
   double bp = dmax(csr, 0.0);
   double bm0 = s.ul - bm;
   double bp0 = s.ur - bp;
-  double q1 = (bp + bm) / (bp - bm);
+  double q1 = qdiv(bp + bm, bp - bm);
   HllFace h;
   h.sl = 0.5 * (1.0 + q1);
   h.sr = 0.5 * (1.0 - q1);
@@ -611,22 +612,22 @@ template <bool DUAL>
 __device__ __forceinline__ HllFace hllc_face(const FaceState& s, const Phys& P) {
   const double gamma = P.gamma;
   const double gamma1 = gamma - 1.0;
-  const double gamma1i = 1.0 / gamma1;
-  double sqrtdl = sqrt(s.dl);
-  double sqrtdr = sqrt(s.dr);
-  double isdlpdr = 1.0 / (sqrtdl + sqrtdr);
+  const double gamma1i = qrcp(gamma1);
+  double sqrtdl = qsqrt(s.dl);
+  double sqrtdr = qsqrt(s.dr);
+  double isdlpdr = qrcp(sqrtdl + sqrtdr);
   double vroe1 = (sqrtdl * s.ul + sqrtdr * s.ur) * isdlpdr;
   double vroe2 = (sqrtdl * s.vl + sqrtdr * s.vr) * isdlpdr;
   double vroe3 = (sqrtdl * s.wl + sqrtdr * s.wr) * isdlpdr;
   double v2 = vroe1 * vroe1 + vroe2 * vroe2 + vroe3 * vroe3;
   double el = gamma1i * s.pl + 0.5 * s.dl * (s.ul * s.ul + s.vl * s.vl + s.wl * s.wl);
   double er = gamma1i * s.pr + 0.5 * s.dr * (s.ur * s.ur + s.vr * s.vr + s.wr * s.wr);
-  double hroe = ((el + s.pl) / sqrtdl + (er + s.pr) / sqrtdr) * isdlpdr;
-  double cs = sqrt(gamma1 * dmax((hroe - 0.5 * v2), kTiny));
+  double hroe = (qdiv(el + s.pl, sqrtdl) + qdiv(er + s.pr, sqrtdr)) * isdlpdr;
+  double cs = qsqrt(gamma1 * dmax((hroe - 0.5 * v2), kTiny));
   double char1 = vroe1 - cs;
   double char2 = vroe1 + cs;
-  double csl0 = sqrt(gamma * s.pl / s.dl);
-  double csr0 = sqrt(gamma * s.pr / s.dr);
+  double csl0 = qsqrt(qdiv(gamma * s.pl, s.dl));
+  double csr0 = qsqrt(qdiv(gamma * s.pr, s.dr));
   double csl = dmin(s.ul - csl0, char1);
   double csr = dmax(s.ur + csr0, char2);
   double bm = dmin(csl, 0.0);
@@ -636,18 +637,18 @@ __device__ __forceinline__ HllFace hllc_face(const FaceState& s, const Phys& P) 
   double tr = s.pr - (csr - s.ur) * s.dr * s.ur;
   double dl = s.dl * (csl - s.ul);
   double dr = -(s.dr * (csr - s.ur));
-  double q1 = 1.0 / (dl + dr);
+  double q1 = qrcp(dl + dr);
   double cw = (tr - tl) * q1;
   double cp = (dl * tr + dr * tl) * q1;
   double sl, sr, sm;
   if (cw >= 0.0) {
-    sl = cw / (cw - bm);
+    sl = qdiv(cw, cw - bm);
     sr = 0.0;
-    sm = -(bm / (cw - bm));
+    sm = -qdiv(bm, cw - bm);
   } else {
     sl = 0.0;
-    sr = -(cw / (bp - cw));
-    sm = bp / (bp - cw);
+    sr = -qdiv(cw, bp - cw);
+    sm = qdiv(bp, bp - cw);
   }
   cp = dmax(cp, 0.0);
   const double bm0 = s.ul - bm, bp0 = s.ur - bp;

@@ -160,17 +160,6 @@ __global__ void __launch_bounds__(kMarchThreads) corrections_kernel(const __grid
 #ifndef PPM_RECON0_MINBLOCKS
 #define PPM_RECON0_MINBLOCKS PPM_RECON_MINBLOCKS
 #endif
-// PPM_RECON_PREFETCH: the march loads cell t+1 while it computes with cell t.
-// PPM_RECON_UNROLL: unroll factor of the march.
-#ifndef PPM_RECON_PREFETCH
-#define PPM_RECON_PREFETCH 0
-#endif
-#ifndef PPM_RECON_UNROLL
-#define PPM_RECON_UNROLL 1
-#endif
-#define PPM_STR_(x) #x
-#define PPM_UNROLL_(n) _Pragma(PPM_STR_(unroll n))
-
 // COR: the batch carries slope corrections (the coefficients of the corrections kernel).
 // One pencil's march (the body of the reconstruct kernels).
 template <bool DUAL, bool GRAV, int ROLE, bool COR>
@@ -201,58 +190,20 @@ __device__ __forceinline__ void reconstruct_pencil(const SweepArgs& a, int64_t p
   AdvL aLp = {};   // left data of face t-2 (ROLE 1)
 
   const int tend = ie + 3;  // the last face, ie+1, is assembled at t = ie+3
-#if PPM_RECON_PREFETCH
-  // cell t's loads, issued one iteration ahead
-  double xq0, xq1, xq2, xu, xg, xd, xp;
-  {
-    const int64_t off = base;
-    xq0 = ldg0(q0p, off);
-    xq1 = ldg0(q1p, off);
-    xq2 = ldg0(q2p, off);
-    xu = ROLE == 0 ? 0.0 : ldg0(a.in_u, off);
-    xg = (GRAV && ROLE == 0) ? __ldg(a.grav + off) : 0.0;
-    xd = ROLE == 0 ? 0.0 : __ldg(a.in_d + off);
-    xp = ROLE == 0 ? 0.0 : __ldg(a.pres + off);
-  }
-#endif
-  PPM_UNROLL_(PPM_RECON_UNROLL)
+#pragma unroll 1
   for (int t = 0; t <= tend; ++t) {
     const int64_t off = base + (int64_t)t * sa;
     double nq[3];
-#if PPM_RECON_PREFETCH
-    nq[0] = xq0;
-    nq[1] = xq1;
-    nq[2] = xq2;
-    const double nu = ROLE == 0 ? nq[2] : xu;
-    const double ng = xg;
-    const double nd = ROLE == 0 ? nq[0] : xd;
-    const double npr = ROLE == 0 ? nq[1] : xp;
-    if (t < tend) {
-      const int64_t o1 = off + sa;
-      xq0 = ldg0(q0p, o1);
-      xq1 = ldg0(q1p, o1);
-      xq2 = ldg0(q2p, o1);
-      if (ROLE != 0) xu = ldg0(a.in_u, o1);
-      if (GRAV && ROLE == 0) xg = __ldg(a.grav + o1);
-      if (ROLE != 0) {
-        xd = __ldg(a.in_d + o1);
-        xp = __ldg(a.pres + o1);
-      }
-    }
-#else
     nq[0] = ldg0(q0p, off);
     nq[1] = ldg0(q1p, off);
     nq[2] = ldg0(q2p, off);
     const double nu = ROLE == 0 ? nq[2] : ldg0(a.in_u, off);
     const double ng = (GRAV && ROLE == 0) ? __ldg(a.grav + off) : 0.0;
-#endif
     // characteristic distances of cell t (inteuler.F:197-208)
     Prep prC = prB;
     if (t >= is - 1 && t <= ie + 1) {
-#if !PPM_RECON_PREFETCH
       const double nd = ROLE == 0 ? nq[0] : __ldg(a.in_d + off);
       const double npr = ROLE == 0 ? nq[1] : __ldg(a.pres + off);
-#endif
       prC = (COR && a.presfree) ? cell_prep<true>(nd, npr, nu, a.coef[t].dx2i, P)
                                 : cell_prep(nd, npr, nu, a.coef[t].dx2i, P);
     }
