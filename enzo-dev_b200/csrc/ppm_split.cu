@@ -505,8 +505,8 @@ __global__ void __launch_bounds__(RT, (LEARNED ? PPM_RIEMANN_LEARNED_MINBLOCKS
   }
   unsigned trips = 0;  // Newton updates of this lane's face (both starts when rejected)
   if (valid) {
-    const double cl = sqrt(P.gamma * s.pl * s.dl);
-    const double cr = sqrt(P.gamma * s.pr * s.dr);
+    const double cl = qsqrt(P.gamma * s.pl * s.dl);
+    const double cr = qsqrt(P.gamma * s.pr * s.dr);
     const double ps = acoustic_guess(s, cl, cr, P);
     Riemann rs;
     unsigned spent = 0;
@@ -534,7 +534,7 @@ __global__ void __launch_bounds__(RT, (LEARNED ? PPM_RIEMANN_LEARNED_MINBLOCKS
         }
       }
     }
-    const double qc = P.dt / a.coef[a.is + fi].dx;
+    const double qc = qdiv(P.dt, a.coef[a.is + fi].dx);
     load_face_advected<DUAL>(a, idx, s);
     double db;
     const Flux F = flux_twoshock<DUAL>(s, rs.pbar, rs.ubar, qc, P, COL ? &db : nullptr);
@@ -727,8 +727,8 @@ __global__ void __launch_bounds__(kFaceThreads, PPM_FACE_MINBLOCKS)
   const int64_t idx = (int64_t)(c - is) * np + pid;
   unsigned trips = 0;
   if (face_ok) {
-    const double clr = sqrt(P.gamma * st.pl * st.dl);
-    const double crr = sqrt(P.gamma * st.pr * st.dr);
+    const double clr = qsqrt(P.gamma * st.pl * st.dl);
+    const double crr = qsqrt(P.gamma * st.pr * st.dr);
     rs = twoshock_newton(st, clr, crr, acoustic_guess(st, clr, crr, P), P);
     trips = (unsigned)rs.iters;
     if (a.log && a.log_stride > 0) {
@@ -797,7 +797,7 @@ __global__ void __launch_bounds__(kFaceThreads, PPM_FACE_MINBLOCKS)
     st.vl = as.vl; st.vr = as.vr; st.wl = as.wl; st.wr = as.wr;
     st.gel = DUAL ? as.gel : 0.0;
     st.ger = DUAL ? as.ger : 0.0;
-    const double qc = P.dt / cf.dx;
+    const double qc = qdiv(P.dt, cf.dx);
     const Flux F = flux_twoshock<DUAL>(st, rs.pbar, rs.ubar, qc, P);
     double* o = a.fflux + idx;
     o[XDF * plane] = F.df;
@@ -1289,7 +1289,10 @@ __device__ __forceinline__ double cell_dt1(const SweepArgs& a, const Cell& o, do
 #ifndef PPM_STAGE_LD
 #define PPM_STAGE_LD (32 + 8)
 #endif
-enum { kStageCells = 4, kStageLd = PPM_STAGE_LD };
+#ifndef PPM_STAGE_CELLS
+#define PPM_STAGE_CELLS 4
+#endif
+enum { kStageCells = PPM_STAGE_CELLS, kStageLd = PPM_STAGE_LD };
 constexpr int kStageField = kStageCells * kStageLd;
 constexpr int kStageWarp = 6 * kStageField;  // doubles per warp
 
