@@ -15,10 +15,16 @@
 //
 // Measured on a B200 against CUDA's IEEE division and sqrt over 3.2e9 random operands
 // (exponents over +-60, +-1000 and near 1): at most 1 ulp apart for all three.
-// Arguments outside [2^-1000, 2^1000] in magnitude (zero, subnormals, infinities, NaN,
-// extreme exponents) take the IEEE operation instead, decided on the integer pipe from
-// the exponent bits, so the special values behave exactly as in the exact build.
-// In the exact build (PPM_FAST_ALGEBRA 0) the three are the IEEE operations themselves.
+//
+// No branches: the special arguments are picked out on the integer pipe from the
+// exponent bits and their results selected.  Zeros, infinities and NaN give the IEEE
+// results; subnormal arguments count as zero and results that would be subnormal flush
+// to zero (the hardware approximations' ftz).  Branch-free code also keeps the results
+// independent of where the compiler places them: with a branch around the IEEE
+// fallback, the multiply-adds fused around these calls differed between kernel
+// instantiations, and a level solved in one batch stopped matching the same grids
+// solved one at a time.  In the exact build (PPM_FAST_ALGEBRA 0) the three are the
+// IEEE operations themselves.
 #pragma once
 
 #ifndef PPM_FAST_ALGEBRA
@@ -30,10 +36,9 @@
 
 namespace ppm {
 
-__device__ __forceinline__ bool fm_plain_range(double x) {
-  // biased exponent in [23, 2023]: |x| in [2^-1000, 2^1000], normal, finite
-  const unsigned e = ((unsigned)__double2hiint(x) >> 20) & 0x7FFu;
-  return e - 23u <= 2000u;
+// biased exponent of x
+__device__ __forceinline__ unsigned fm_exponent(double x) {
+  return ((unsigned)__double2hiint(x) >> 20) & 0x7FFu;
 }
 
 __device__ __forceinline__ double fm_rcp_approx(double x) {
@@ -50,10 +55,12 @@ __device__ __forceinline__ double fm_rsqrt_approx(double x) {
 // 1/x
 __device__ __forceinline__ double qrcp(double x) {
 #if PPM_FAST_DIVSQRT
-  if (!fm_plain_range(x)) return 1.0 / x;
   const double y0 = fm_rcp_approx(x);
   const double e = fma(-x, y0, 1.0);
-  return fma(y0, fma(e, e, e), y0);
+  const double r = fma(y0, fma(e, e, e), y0);
+  // |x| in [2^-1022, 2^1021): x and 1/x normal; otherwise the approximation itself is
+  // exact (+-0 -> +-inf, +-inf -> +-0, NaN) or flushed (subnormal x, subnormal 1/x)
+  return fm_exponent(x) - 1u <= 2042u ? r : y0;
 #else
   return 1.0 / x;
 #endif
@@ -71,14 +78,20 @@ __device__ __forceinline__ double qdiv(double a, double b) {
 // sqrt(x)
 __device__ __forceinline__ double qsqrt(double x) {
 #if PPM_FAST_DIVSQRT
-  if (!fm_plain_range(x)) return sqrt(x);
-  const double y0 = fm_rsqrt_approx(x);
+  const double y0 = fm_rsqrt_approx(x);  // NaN for x < 0, which the iteration keeps
   double g = x * y0, h = 0.5 * y0;
   double r = fma(-g, h, 0.5);
   g = fma(g, r, g);
   h = fma(h, r, h);
   r = fma(-g, h, 0.5);
-  return fma(g, r, g);
+  const double s = fma(g, r, g);
+  const unsigned ex = fm_exponent(x);
+  const int hi = __double2hiint(x);
+  // exponent 0: +-0 (and subnormals, flushed) -> +-0; exponent 2047: +inf -> +inf,
+  // -inf -> NaN, NaN -> NaN
+  const double special = ex == 0u ? __hiloint2double(hi & (int)0x80000000, 0)
+                                  : (hi < 0 ? __longlong_as_double(0x7FF8000000000000ll) : x);
+  return ex - 1u <= 2045u ? s : special;
 #else
   return sqrt(x);
 #endif
