@@ -691,10 +691,10 @@ __device__ __forceinline__ Cell euler_update(const Cell& c, const Flux& F0, cons
                                              double ges, double gr, const Phys& P, bool& fatal) {
   Cell o;
   double dnu = c.d + (F0.df - F1.df);
-  double dnuinv = 1.0 / dnu;
+  double dnuinv = qrcp(dnu);
   if (P.small_rho > 0.0) {
     dnu = dmax(dnu, P.small_rho);
-    dnuinv = 1.0 / dnu;
+    dnuinv = qrcp(dnu);
   }
   double uold = c.u;
   o.u = (c.u * c.d + (F0.uf - F1.uf)) * dnuinv;
@@ -723,9 +723,9 @@ __device__ __forceinline__ void pgas2d_dual(Cell& c, double de_m, double de_p, c
   double ke = 0.5 * (c.u * c.u + c.v * c.v + c.w * c.w);
   double ge1 = c.e - ke;
   double demax = dmax(dmax(c.d * c.e, de_m), de_p);
-  if (ge1 * c.d / demax > P.eta2) c.ge = ge1;
-  double ge2 = (ge1 / c.e > P.eta1) ? ge1 : c.ge;
-  ge2 = dmax(ge2, P.pmin / (P.gm1 * c.d));
+  if (qdiv(ge1 * c.d, demax) > P.eta2) c.ge = ge1;
+  double ge2 = (qdiv(ge1, c.e) > P.eta1) ? ge1 : c.ge;
+  ge2 = dmax(ge2, qdiv(P.pmin, P.gm1 * c.d));
   c.e = c.e - ge1 + ge2;
 }
 

@@ -17,6 +17,8 @@
 // warp's scratch accesses are contiguous.
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
 #include <atomic>
 
 #include "ppm_device.cuh"
@@ -190,8 +192,11 @@ __device__ __forceinline__ void reconstruct_pencil(const SweepArgs& a, int64_t p
   AdvL aLp = {};   // left data of face t-2 (ROLE 1)
 
   const int tend = ie + 3;  // the last face, ie+1, is assembled at t = ie+3
-#pragma unroll 1
-  for (int t = 0; t <= tend; ++t) {
+  // One step of the march.  ST (steady): cells t-2 .. t all inside the range every stage
+  // touches (t in [is+2, ie+1]), so the range tests drop out and the step is one block
+  // of straight-line code the scheduler can interleave.
+  auto step = [&](const int t, auto steady) {
+    constexpr bool ST = decltype(steady)::value;
     const int64_t off = base + (int64_t)t * sa;
     double nq[3];
     nq[0] = ldg0(q0p, off);
@@ -201,7 +206,7 @@ __device__ __forceinline__ void reconstruct_pencil(const SweepArgs& a, int64_t p
     const double ng = (GRAV && ROLE == 0) ? __ldg(a.grav + off) : 0.0;
     // characteristic distances of cell t (inteuler.F:197-208)
     Prep prC = prB;
-    if (t >= is - 1 && t <= ie + 1) {
+    if (ST || (t >= is - 1 && t <= ie + 1)) {
       const double nd = ROLE == 0 ? nq[0] : __ldg(a.in_d + off);
       const double npr = ROLE == 0 ? nq[1] : __ldg(a.pres + off);
       prC = (COR && a.presfree) ? cell_prep<true>(nd, npr, nu, a.coef[t].dx2i, P)
@@ -213,11 +218,11 @@ __device__ __forceinline__ void reconstruct_pencil(const SweepArgs& a, int64_t p
     for (int v = 0; v < 3; ++v) dqN[v] = qlN[v] = 0.0;
     {
       const int c = t - 1;
-      if (c >= is - 2 && c <= ie + 2) {
+      if (ST || (c >= is - 2 && c <= ie + 2)) {
         const Coef cf = a.coef[c];
 #pragma unroll
         for (int v = 0; v < NV; ++v) dqN[v] = pm_slope(wq1[v], wq2[v], nq[v], cf.c1, cf.c2);
-        if (c >= is - 1) {
+        if (ST || c >= is - 1) {
 #pragma unroll
           for (int v = 0; v < NV; ++v)
             qlN[v] = pm_edge(wq1[v], wq2[v], dqm1[v], dqN[v], cf.c3, cf.c4, cf.c5, cf.c6);
@@ -230,7 +235,7 @@ __device__ __forceinline__ void reconstruct_pencil(const SweepArgs& a, int64_t p
     AdvL aLn = aLp;
     {
       const int c = t - 2;
-      if (c >= is - 1 && c <= ie + 1) {
+      if (ST || (c >= is - 1 && c <= ie + 1)) {
         Para pa[3];
 #pragma unroll
         for (int v = 0; v < 3; ++v) pa[v] = Para{0.0, 0.0, 0.0, 0.0};
@@ -262,7 +267,7 @@ __device__ __forceinline__ void reconstruct_pencil(const SweepArgs& a, int64_t p
           // cell c's left edge gives the right side of face c, its right edge the left
           // side of face c+1; each side is solved on its own (face_side), the left one
           // carried to the next step
-          if (c >= is) {
+          if (ST || c >= is) {
             const SideIn Rin{pm_C(pa[0], prA.char2), pm_B(pa[0], prA.c0),
                              pm_C(pa[1], prA.char2), pm_B(pa[1], prA.c0),
                              pm_B(pa[1], prA.cm),    pm_B(pa[1], prA.cp),
@@ -293,7 +298,7 @@ __device__ __forceinline__ void reconstruct_pencil(const SweepArgs& a, int64_t p
             o[SUL * plane] = sLp.u;
             o[SUR * plane] = r.u;
           }
-          if (c <= ie) {
+          if (ST || c <= ie) {
             const SideIn Lin{pm_A(pa[0], prA.char1), pm_A(pa[0], prA.c0),
                              pm_A(pa[1], prA.char1), pm_A(pa[1], prA.c0),
                              pm_A(pa[1], prA.cm),    pm_A(pa[1], prA.cp),
@@ -306,7 +311,7 @@ __device__ __forceinline__ void reconstruct_pencil(const SweepArgs& a, int64_t p
             ld0n = Lin.d0;
           }
         } else {
-          if (c >= is) {
+          if (ST || c >= is) {
             AdvR R;
             R.vra = pm_C(pa[0], prA.char2);
             R.vr0 = pm_B(pa[0], prA.c0);
@@ -324,7 +329,7 @@ __device__ __forceinline__ void reconstruct_pencil(const SweepArgs& a, int64_t p
               o[SGER * plane] = s.ger;
             }
           }
-          if (c <= ie) {
+          if (ST || c <= ie) {
             aLn.vla = pm_A(pa[0], prA.char1);
             aLn.vl0 = pm_A(pa[0], prA.c0);
             aLn.wla = pm_A(pa[1], prA.char1);
@@ -356,7 +361,17 @@ __device__ __forceinline__ void reconstruct_pencil(const SweepArgs& a, int64_t p
     lda = ldn;
     ld0 = ld0n;
     aLp = aLn;
-  }
+  };
+  using Ramp = std::integral_constant<bool, false>;
+  using Steady = std::integral_constant<bool, true>;
+  const int t_steady0 = is + 2, t_steady1 = ie + 1;
+#pragma unroll 1
+  for (int t = 0; t < t_steady0 && t <= tend; ++t) step(t, Ramp{});
+#pragma unroll 1
+  for (int t = t_steady0; t <= t_steady1; ++t) step(t, Steady{});
+#pragma unroll 1
+  for (int t = t_steady1 + 1 > t_steady0 ? t_steady1 + 1 : t_steady0; t <= tend; ++t)
+    step(t, Ramp{});
 }
 
 // FLAG: only the pencils of the batch's flagged list (the fused sweep's fallback pass,
