@@ -1400,33 +1400,36 @@ __device__ __forceinline__ bool update_pencil(const SweepArgs& a, int64_t pid, c
     for (int q = 0; q < kXBuffers - 1 && q * kXTileCells < n; ++q) x_issue(*xt, q);
   }
 
-#pragma unroll 1
-  for (int t = 0; t <= n; ++t) {
-    if (XT && t < n && t % kXTileCells == 0) x_chunk(*xt, t / kXTileCells, n);
+  // One step of the march.  ST (steady): t in [is+2, ie-1], where cell t, face t+1 and
+  // cells t-1, t-2 are all inside the ranges every stage tests, so the tests drop out.
+  bool handed = false;  // the pencil went to the fallback pass
+  auto step = [&](const int t, auto steady) {
+    constexpr bool ST = decltype(steady)::value;
+    if (XT && (ST || t < n) && t % kXTileCells == 0) x_chunk(*xt, t / kXTileCells, n);
     Cell Cn = Cm;
     double ges_n = 0.0;
     Flux F1 = F0;
     bool gov_next = false;
     double govv_next = 0.0;
     // (1) check of cell t
-    if (live && t < n) {
+    if (live && (ST || t < n)) {
       if (PIPE) {
         cp_async_wait<(PD > 0 ? PD - 1 : 0)>();  // unit t has landed, t+1 .. t+PD-1 may not
         const double* r = ring + (t % (PD + 1)) * (kUnitVals * kMarchThreads);
         Cn = pipe_cell<DUAL>(a, r);
-        if (t >= is && t <= ie) F1 = pipe_flux(r);
+        if (ST || (t >= is && t <= ie)) F1 = pipe_flux(r);
         pipe_issue<DUAL, PD>(a, ring, base, pid, t + PD);  // into the slot read at t-1
       } else {
         Cn = XT ? x_cell<DUAL>(*xt, a, t) : Cpf;
-        if (t >= is && t <= ie) F1 = Fpf;
-        if (t + 1 < n) {
+        if (ST || (t >= is && t <= ie)) F1 = Fpf;
+        if (ST || t + 1 < n) {
           if (!XT)
             Cpf = STAGED ? load_cell_keep<DUAL>(a, base + (int64_t)(t + 1) * sa)
                          : load_cell<DUAL>(a, base + (int64_t)(t + 1) * sa);
-          if (t + 1 >= is && t + 1 <= ie) Fpf = load_flux(a, (int64_t)(t + 2 - is) * np + pid);
+          if (ST || (t + 1 >= is && t + 1 <= ie)) Fpf = load_flux(a, (int64_t)(t + 2 - is) * np + pid);
         }
       }
-      if (t >= is && t <= ie) {
+      if (ST || (t >= is && t <= ie)) {
         if (DUAL) {
           const double pcent = dmax(P.gm1 * Cn.ge * Cn.d, kTiny);
           ges_n = gov ? govv : (RS ? F0.ub : P.dt / a.coef[t].dx * pcent * (F0.ub - F1.ub));
@@ -1437,7 +1440,8 @@ __device__ __forceinline__ bool update_pencil(const SweepArgs& a, int64_t pid, c
         if (bad) {
           if (!FALLBACK && !STAGED) {  // hand the pencil to the fallback pass
             if (PIPE) cp_async_wait<0>();
-            return true;
+            handed = true;
+            return;
           }
           if (!FALLBACK) {  // STAGED: stop computing, keep joining the block's flushes
             live = false;
@@ -1474,7 +1478,7 @@ __device__ __forceinline__ bool update_pencil(const SweepArgs& a, int64_t pid, c
     Cell PEn = Cm;
     if (live) {
       const int c = t - 1;
-      if (c >= is && c <= ie) {
+      if (ST || (c >= is && c <= ie)) {
         bool fatal = false;
         PEn = euler_update<DUAL, GRAV>(Cm, Fm, F0, ges_m,
                                        GRAV ? __ldg(a.grav + base + (int64_t)c * sa) : 0.0, P,
@@ -1485,17 +1489,17 @@ __device__ __forceinline__ bool update_pencil(const SweepArgs& a, int64_t pid, c
     // (3) dual-energy select of cell t-2 and store
     {
       const int c = t - 2;
-      if (live && c >= 0) {
+      if (live && (ST || c >= 0)) {
         Cell o = PEm;
         if (DUAL) {
           const double own = o.d * o.e;
-          const double de_m = (c == 0) ? own : dep;
-          const double de_p = (c == n - 1) ? own : PEn.d * PEn.e;
+          const double de_m = (!ST && c == 0) ? own : dep;
+          const double de_p = (!ST && c == n - 1) ? own : PEn.d * PEn.e;
           pgas2d_dual(o, de_m, de_p, P);
           dep = o.d * o.e;
         }
         if (!isfinite(o.d) || !isfinite(o.e)) nonfin += 1;
-        if (cfl && c >= is && c <= ie)
+        if (cfl && (ST || (c >= is && c <= ie)))
           dtmin = dmin(dtmin, cell_dt1<DUAL>(a, o, a.coef[c].dx, t1, t2, P));
         if (STAGED && PPM_X_STAGE_STORES) {
           double* sp = stage + (c % kStageCells) * kStageLd + (threadIdx.x & 31);
@@ -1516,7 +1520,7 @@ __device__ __forceinline__ bool update_pencil(const SweepArgs& a, int64_t pid, c
         }
       }
       // warp-wide: the same steps on every lane
-      if (STAGED && PPM_X_STAGE_STORES && c >= 0 && c % kStageCells == kStageCells - 1)
+      if (STAGED && PPM_X_STAGE_STORES && (ST || c >= 0) && c % kStageCells == kStageCells - 1)
         flush_stage<DUAL>(a, stage, pid0, c - (kStageCells - 1), kStageCells);
     }
     Fm = F0;
@@ -1526,6 +1530,23 @@ __device__ __forceinline__ bool update_pencil(const SweepArgs& a, int64_t pid, c
     gov = gov_next;
     govv = govv_next;
     PEm = PEn;
+  };
+  using Ramp = std::integral_constant<bool, false>;
+  using Steady = std::integral_constant<bool, true>;
+  // the x sweep's update (TMA tiles) gains from the steady block; the y/z update, with
+  // its cp.async ring, measured slower with it (more registers than its 128)
+  const int t_steady0 = XT ? is + 2 : n + 1, t_steady1 = XT ? ie - 1 : n;
+#pragma unroll 1
+  for (int t = 0; t < t_steady0 && t <= n; ++t) {
+    step(t, Ramp{});
+    if (handed) return true;
+  }
+  if constexpr (XT) {
+#pragma unroll 1
+    for (int t = t_steady0; t <= t_steady1; ++t) step(t, Steady{});
+#pragma unroll 1
+    for (int t = t_steady1 + 1 > t_steady0 ? t_steady1 + 1 : t_steady0; t <= n; ++t)
+      step(t, Ramp{});
   }
   // the last step (t = n) leaves cell n-1 unstored; it is a ghost cell, whose
   // post-euler state is its input, selected against itself and its left neighbour
