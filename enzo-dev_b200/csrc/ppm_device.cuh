@@ -15,6 +15,13 @@
 
 #include "ppm_fastmath.cuh"
 
+// PPM_NEWTON_RSQRT: the tolerance build's Newton update from 1/sqrt of the shock factors
+// (one reciprocal square root each instead of a square root plus a shared reciprocal;
+// Riemann stage 0.77 -> 0.74 ms per 256^3 sweep)
+#ifndef PPM_NEWTON_RSQRT
+#define PPM_NEWTON_RSQRT 1
+#endif
+
 // PPM_FAST_ALGEBRA (the tolerance-mode build): a few quotients with a shared divisor
 // are formed from one reciprocal, and the reconstruction's and the Riemann solvers'
 // divisions and square roots go through qrcp / qdiv / qsqrt (ppm_fastmath.cuh; the
@@ -408,6 +415,31 @@ __device__ __forceinline__ Riemann twoshock_newton(const FaceState& s, double cl
   // division (a/x, b/y = a*y*q, b*x*q with q = 1/(x*y)), and the convergence test as
   // |dp| < tolerance * ps: three divisions per update instead of twelve.
   const double ipl = qrcp(s.pl), ipr = qrcp(s.pr), idl = qrcp(s.dl), idr = qrcp(s.dr);
+#if PPM_NEWTON_RSQRT
+  // zl = cl sqrt(Xl) from yl = 1/sqrt(Xl): zl = cl Xl yl, 1/zl = yl / cl, zl^2 = cl^2 Xl
+  const double icl = qrcp(cl), icr = qrcp(cr), cl2 = cl * cl, cr2 = cr * cr;
+#pragma unroll 1
+  for (int n = 2; n <= kNumIter; n++) {
+    if (active) {
+      const double Xl = 1.0 + P.qa * (ps * ipl - 1.0), Xr = 1.0 + P.qa * (ps * ipr - 1.0);
+      const double yl = qrsqrt(Xl), yr = qrsqrt(Xr);
+      const double zl = cl * (Xl * yl), zr = cr * (Xr * yr);
+      ubl = s.ul - (ps - s.pl) * (yl * icl);
+      ubr = s.ur + (ps - s.pr) * (yr * icr);
+      const double al = 4.0 * (cl2 * Xl) * idl, ar = 4.0 * (cr2 * Xr) * idr;
+      const double dl = al - P.gp1 * (ps - s.pl), dr = ar - P.gp1 * (ps - s.pr);
+      const double qd = qrcp(dl * dr);
+      dpdul = -(zl * al * (dr * qd));
+      dpdur = zr * ar * (dl * qd);
+      ps = ps + qdiv((ubr - ubl) * dpdur * dpdul, dpdur - dpdul);
+      if (ps < P.pmin) ps = P.pmin;
+      const double delta_ps = ps - old_ps;
+      old_ps = ps;
+      it++;
+      if (fabs(delta_ps) < kTolerance * ps) active = false;
+    }
+  }
+#else
 #pragma unroll 1
   for (int n = 2; n <= kNumIter; n++) {
     if (active) {
@@ -429,6 +461,7 @@ __device__ __forceinline__ Riemann twoshock_newton(const FaceState& s, double cl
       if (fabs(delta_ps) < kTolerance * ps) active = false;
     }
   }
+#endif
 #else
 #pragma unroll 1
   for (int n = 2; n <= kNumIter; n++) {

@@ -89,6 +89,38 @@ def test_level_solve_matches_per_grid_solves_and_oracle(torch, dual, grav):
     ctx.close()
 
 
+@pytest.mark.parametrize("dual,grav", [(True, False), (False, False), (True, True)])
+def test_tolerance_build_level_matches_per_grid_solves(torch, dual, grav):
+    # the tolerance build (fused multiply-adds, fast reciprocal and square root) is not
+    # bit-identical to the oracle, but a grid still gives the same bits in a level batch
+    # as alone: the fast reciprocal and square root have no branches, so what the
+    # compiler fuses around them does not depend on the kernel's instantiation (one
+    # grid's record in the kernel parameters, a batch's in shared memory)
+    hp = H.HydroParams(gamma=5.0 / 3.0, cfl=0.5, dual=dual, gravity=grav)
+    grids, host = _level(hp, 300)
+    acc_dev = None
+    if grav:
+        rng = np.random.default_rng(11)
+        acc_dev = [[torch.from_numpy(0.1 * rng.standard_normal(g.shape)).cuda()
+                    for _ in range(g.rank)] for g in grids]
+    ctx = capi.Context(0, variant="fast")
+    per_grid = [_dev(f, torch) for f in host]
+    batched = [_dev(f, torch) for f in host]
+    for cyc in range(4):
+        dt = ctx.compute_timestep_level(grids, hp, batched)
+        for k, g in enumerate(grids):
+            ctx.solve_ppm_de(g, hp, dt, cyc, per_grid[k], memory=capi.MEM_DEVICE,
+                             accel=None if acc_dev is None else acc_dev[k], want_stats=False)
+        rc, _ = ctx.solve_level(grids, hp, dt, cyc, batched, accels=acc_dev, want_stats=True)
+        assert rc == capi.OK
+        for k, g in enumerate(grids):
+            _assert_same(_host(batched[k]), _host(per_grid[k]), g, ("per-grid", cyc, k))
+        ctx.set_boundary_level(grids, batched, dual)
+        for k in range(len(grids)):
+            ctx.set_boundary(grids[k], per_grid[k], dual)
+    ctx.close()
+
+
 def test_level_solve_in_a_fresh_context(torch):
     # the first call sizes every scratch buffer for the level at once; the second
     # sweep direction of these patches needs more face scratch than the first
@@ -195,7 +227,9 @@ def test_level_rejects_mixed_rank(torch):
     ("batched", 128, 1, 4_000_000),  # waves: a few grids at a time
     ("classes", 128, 0, 1),          # every grid its own wave
 ])
-def test_level_schedules_are_bit_identical(torch, schedule, threads, persistent, scratch):
+@pytest.mark.parametrize("variant", ["exact", "fast"])
+def test_level_schedules_are_bit_identical(torch, schedule, threads, persistent, scratch,
+                                           variant):
     # the level schedules (one batch, one batch per size class, one grid at a time), the
     # Riemann stage's block size and persistent launch, and waves under a scratch bound
     # change how the level is launched, never its results: the same fields and the same
@@ -203,12 +237,12 @@ def test_level_schedules_are_bit_identical(torch, schedule, threads, persistent,
     hp = H.HydroParams(gamma=5.0 / 3.0, cfl=0.5, dual=True)
     grids, host = _level(hp, 600)
     ref = [_dev(f, torch) for f in host]
-    a = capi.Context(0)
+    a = capi.Context(0, variant=variant)
     dt_a = torch.zeros(1, dtype=torch.float64, device="cuda")
     a.compute_timestep_level(grids, hp, ref, dt_device=dt_a, want_host=False)
     a.set_cfl(dt_a, courant=hp.cfl)
     for graphs in (False, True):
-        b = capi.Context(0)
+        b = capi.Context(0, variant=variant)
         b.set_graphs(graphs)
         # class bounds inside the test level's range of sizes, so every class has grids
         b.set_level_config(schedule=schedule, riemann_threads=threads, persistent=persistent,
