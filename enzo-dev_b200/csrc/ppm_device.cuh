@@ -23,9 +23,10 @@
 #endif
 
 // PPM_FAST_ALGEBRA (the tolerance-mode build): a few quotients with a shared divisor
-// are formed from one reciprocal, and the reconstruction's and the Riemann solvers'
-// divisions and square roots go through qrcp / qdiv / qsqrt (ppm_fastmath.cuh; the
-// IEEE operations in the exact build); everything else is the reference's expression.
+// are formed from one reciprocal, and the divisions and square roots of the
+// reconstruction, the Riemann solvers and the update (not calc_dt's) go through qrcp /
+// qdiv / qsqrt / qrsqrt (ppm_fastmath.cuh; the IEEE operations in the exact build);
+// everything else is the reference's expression.
 
 namespace ppm {
 
